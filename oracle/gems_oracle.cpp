@@ -1,0 +1,1184 @@
+// gems_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU FP64 restatement of the GEMS force/neighbour hot path (alexispaz/GEMS,
+// Fortran 2003).  It is the checker for the CUDA path and the timed CPU
+// baseline ("port"): only tests/, __graft_entry__.smoke() and bench.py's
+// cpu_baseline / reference legs may load it.  The product library
+// (gems_b200/libgemsgpu.so) never links or calls it.
+//
+// Parity status of this restatement:
+//   * pinned against the reference's golden files examples/XYZ (LJ, PBC,
+//     O(N^2) list), examples/LJ (dimer scan + velocity Verlet),
+//     examples/SMA-TB/bulk (linked cells, SMA-TB, Ermak, LCG stream),
+//     examples/NVE (plj, fill, tempgdist, VV) and examples/NVT (plj, Ermak);
+//     see tests/test_oracle_golden.py.
+//   * Tersoff and FIRE: parity UNPINNED (the reference ships no test for
+//     either, its Tersoff.f90 is internally inconsistent and FIRE.f90 does
+//     not compile).  They are restated from the published methods and
+//     checked by finite differences / energy conservation instead.
+//
+// Every routine cites the reference file:line it restates.  Arithmetic is
+// written in the reference's evaluation order and compiled with
+// -ffp-contract=off so that the neighbour predicate is bit-identical to a
+// gfortran -O2 build on x86-64 (no FMA contraction).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdlib>
+#include <vector>
+#include <algorithm>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------- units
+// Constants.F90:101-175.  Internal units: Angstrom, uma, ps.
+const double axps_mxs = 1.0e2;
+const double uma_kg = 1.6605402e-27;
+const double qe_si = 1.60219e-19;
+const double joule_ev = 1.0 / qe_si;
+const double ui_ev = axps_mxs * axps_mxs * uma_kg * joule_ev;
+const double ev_ui = 1.0 / ui_ev;
+const double kB_ev = 8.617385e-05;
+const double kB_ui = kB_ev * ev_ui;
+const double pi = 3.14159265358979323846264338327950288;
+const double pio2 = pi / 2.0;
+
+// ---------------------------------------------------------------- RNG
+// Random.F90:145-171 (lcg_ranu, lcg_init_ran) and :213-250 (rang, gasdev).
+struct Lcg {
+  int32_t idum = -12345789;
+  int32_t ix = -1, iy = -1;
+  bool gaus_stored = false;
+  double g = 0.0;
+};
+
+// am = nearest(1.0,-1.0)/im is evaluated in single precision
+// (Random.F90:148): (1 - 2^-24) / float(2147483647) = (1 - 2^-24) * 2^-31.
+const double lcg_am = (double)((1.0f - 5.9604644775390625e-8f) / 2147483648.0f);
+
+double lcg_ranu(Lcg& s) {
+  const int32_t ia = 16807, im = 2147483647, iq = 127773, ir = 2836;
+  if (s.idum <= 0 || s.iy < 0) {
+    int32_t a = s.idum < 0 ? -s.idum : s.idum;
+    s.iy = ((int32_t)(888889999 ^ a)) | 1;
+    s.ix = (int32_t)(777755555 ^ a);
+    s.idum = a + 1;
+  }
+  uint32_t x = (uint32_t)s.ix;
+  x ^= x << 13;
+  x ^= x >> 17;
+  x ^= x << 5;
+  s.ix = (int32_t)x;
+  int32_t k = s.iy / iq;
+  s.iy = ia * (s.iy - k * iq) - ir * k;
+  if (s.iy < 0) s.iy += im;
+  return lcg_am * (double)((im & (s.ix ^ s.iy)) | 1);
+}
+
+void lcg_seed(Lcg& s, int seed) {  // lcg_init_ran(lseed): idum=-abs(seed)
+  s.idum = -std::abs(seed);
+}
+
+double gasdev(Lcg& s) {
+  if (s.gaus_stored) {
+    s.gaus_stored = false;
+    return s.g;
+  }
+  double v1, v2, rsq;
+  for (;;) {
+    v1 = 2.0 * lcg_ranu(s) - 1.0;
+    v2 = 2.0 * lcg_ranu(s) - 1.0;
+    rsq = v1 * v1 + v2 * v2;
+    if (rsq > 0.0 && rsq < 1.0) break;
+  }
+  rsq = std::sqrt(-2.0 * std::log(rsq) / rsq);
+  s.g = v2 * rsq;
+  s.gaus_stored = true;
+  return v1 * rsq;
+}
+
+void rang(Lcg& s, double* r1, double* r2) {  // always draws a pair
+  *r1 = gasdev(s);
+  double aux = gasdev(s);
+  if (r2) *r2 = aux;
+}
+
+// ---------------------------------------------------------------- system
+enum FF { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
+enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3 };
+const int MAXT = 8;
+
+// 27-cell stencil in the reference's order (Neighbour.F90:75-83): 0 is the
+// centre, 1..13 the upper half, 14..26 the lower half.
+const int cmap[27][3] = {
+    {0, 0, 0},   {1, 0, 0},   {1, 1, 0},  {0, 1, 0},   {-1, 1, 0},
+    {1, 0, -1},  {1, 1, -1},  {0, 1, -1}, {-1, 1, -1}, {1, 0, 1},
+    {1, 1, 1},   {0, 1, 1},   {-1, 1, 1}, {0, 0, 1},   {-1, 0, 0},
+    {-1, -1, 0}, {0, -1, 0},  {1, -1, 0}, {-1, 0, 1},  {-1, -1, 1},
+    {0, -1, 1},  {1, -1, 1},  {-1, 0, -1}, {-1, -1, -1}, {0, -1, -1},
+    {1, -1, -1}, {0, 0, -1}};
+
+struct LJp {
+  bool on = false;
+  double e = 0, s = 0, rc = 0, rc2 = 0;
+  bool shifted_force = false;  // plj (Pairs.F90:282-370)
+  double prc = 0, frc = 0;
+  double eshift = 0;           // constant energy shift per pair (eV)
+};
+
+struct SMp {  // TB.F90:66-102 per type pair
+  bool on = false;
+  double ca = 0, eps = 0, p = 0, q = 0, r0 = 0, rci = 0, rce = 0;
+  double b1 = 0, b2 = 0, b3 = 0, r1 = 0, r2 = 0, r3 = 0;
+};
+
+struct TSp {  // Tersoff 1988 parameter set (single species)
+  double A = 0, B = 0, l1 = 0, l2 = 0, beta = 0, n = 1, c = 0, d = 1, h = 0,
+         R = 0, D = 0, chi = 1.0;
+};
+
+struct Sys {
+  int n = 0;
+  std::vector<double> pos, vel, acel, force, pos_old, pos_v, vel_v;
+  std::vector<double> epot, mass, one_mass, one_sqrt_mass;
+  std::vector<int> type;
+  bool boxed = false;
+  double box[3] = {0, 0, 0}, one_box[3] = {0, 0, 0};
+  int pbc[3] = {0, 0, 0};
+  bool mic = true;  // Program_Types.F90:98
+  double skin = 1.0;  // nb_dcut, Neighbour.F90:237
+  bool half = false;  // OpenMP default: full lists (Neighbour.F90:160-171)
+  // neighbour list, column-major like list(n1+100,mnb)
+  int cap = 0;
+  std::vector<int> nn, list;
+  bool first = true;
+  long nupd = 0;
+  bool use_cells = false;
+  int ncells[3] = {1, 1, 1};
+  double cell[3] = {0, 0, 0};
+  std::vector<int> head, clist;
+  int overflow = 0, lost = 0;
+  // force field
+  int ff = FF_NONE;
+  int ntypes = 1;
+  LJp lj[MAXT][MAXT];
+  SMp sm[MAXT][MAXT];
+  TSp ts;
+  double rcut = 0;  // intergroup rcut (max over pairs)
+  std::vector<double> band, eband;
+  // integrator
+  int integ = IT_NONE;
+  double dt = 0.002;
+  double cc0 = 0, cc1 = 0, cc2 = 0, sdr = 0, sdv = 0, crv1 = 0, crv2 = 0,
+         skt = 0, gama = 0, temp = 0;
+  Lcg* rng = nullptr;
+  const double* ext_normals = nullptr;  // optional external normal stream
+  // FIRE state
+  double fire_dt = 0, fire_dtmax = 0, fire_alpha = 0.1;
+  int fire_np = 0;
+  double last_epot = 0;
+};
+
+inline double idnint(double x) { return std::round(x); }  // half away from 0
+
+// vdistance(i,j) = pos_i - pos_j with minimum image (Inq_Properties.F90:137-157)
+inline void vdist(const Sys& s, int i, int j, double vd[3]) {
+  for (int l = 0; l < 3; l++) vd[l] = s.pos[3 * i + l] - s.pos[3 * j + l];
+  if (!s.mic) return;
+  for (int l = 0; l < 3; l++)
+    if (s.pbc[l]) vd[l] = vd[l] - s.box[l] * idnint(vd[l] * s.one_box[l]);
+}
+
+inline double dot3(const double v[3]) {  // dot_product(vd,vd), left to right
+  return v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+}
+
+void ensure_cap(Sys& s, int cap) {
+  if (cap <= s.cap && (int)s.nn.size() == s.n) return;
+  s.cap = std::max(cap, s.cap);
+  s.nn.assign(s.n, 0);
+  s.list.assign((size_t)s.n * s.cap, 0);
+}
+
+inline void add_nb(Sys& s, int i, int j) {
+  int m = s.nn[i];
+  if (m >= s.cap) {
+    s.overflow = 1;
+    return;
+  }
+  s.list[(size_t)m * s.n + i] = j;
+  s.nn[i] = m + 1;
+}
+
+// verlet_self / verlet_selfhalf (Neighbour.F90:676-811): keeps rd <= rlist^2
+void verlet_build(Sys& s) {
+  double rcut = s.rcut + s.skin;
+  rcut = rcut * rcut;
+  std::fill(s.nn.begin(), s.nn.end(), 0);
+  const int n = s.n;
+  if (!s.half) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < n; i++) {
+      double vd[3];
+      for (int j = 0; j < n; j++) {
+        if (i == j) continue;
+        vdist(s, i, j, vd);
+        double rd = dot3(vd);
+        if (rd > rcut) continue;
+        add_nb(s, i, j);
+      }
+    }
+  } else {
+    for (int i = 0; i < n; i++) {
+      double vd[3];
+      for (int j = i + 1; j < n; j++) {
+        vdist(s, i, j, vd);
+        double rd = dot3(vd);
+        if (rd > rcut) continue;
+        add_nb(s, i, j);
+      }
+    }
+  }
+}
+
+// cell_pbc (Neighbour.F90:1350-1376), 0-based cells
+inline bool cell_pbc(const Sys& s, int r[3]) {
+  if (s.mic) {
+    for (int l = 0; l < 3; l++) r[l] = ((r[l] + s.ncells[l]) % s.ncells[l]);
+    return true;
+  }
+  for (int l = 0; l < 3; l++)
+    if (r[l] < 0 || r[l] >= s.ncells[l]) return false;
+  return true;
+}
+
+// sort_in_cells (Neighbour.F90:927-989): head/next chain, reversed insertion
+bool sort_in_cells(Sys& s) {
+  int nc = s.ncells[0] * s.ncells[1] * s.ncells[2];
+  s.head.assign(nc, -1);
+  s.clist.assign(s.n, -1);
+  double one_cell[3];
+  for (int l = 0; l < 3; l++) one_cell[l] = 1.0 / s.cell[l];
+  for (int i = 0; i < s.n; i++) {
+    int c[3];
+    for (int l = 0; l < 3; l++) {
+      double v = s.pos[3 * i + l] * one_cell[l];
+      c[l] = (int)v;  // int() truncates toward zero
+      if (c[l] < 0 || c[l] >= s.ncells[l]) {
+        // Out-of-grid atoms are undefined behaviour in the reference; the
+        // restatement clamps them into the grid and records the event.
+        s.lost = 1;
+        c[l] = c[l] < 0 ? 0 : s.ncells[l] - 1;
+      }
+    }
+    int id = c[0] + s.ncells[0] * (c[1] + s.ncells[1] * c[2]);
+    s.clist[i] = s.head[id];
+    s.head[id] = i;
+  }
+  return true;
+}
+
+// linkedcell_self / linkedcell_selfhalf (Neighbour.F90:991-1161): strict <
+void linkedcell_build(Sys& s) {
+  double rcut = s.rcut + s.skin;
+  rcut = rcut * rcut;
+  std::fill(s.nn.begin(), s.nn.end(), 0);
+  sort_in_cells(s);
+  const int nc = s.ncells[0] * s.ncells[1] * s.ncells[2];
+  const int nstencil = s.half ? 14 : 27;
+#pragma omp parallel for schedule(dynamic, 4) if (!s.half)
+  for (int ic = 0; ic < nc; ic++) {
+    int rc[3] = {ic % s.ncells[0], (ic / s.ncells[0]) % s.ncells[1],
+                 ic / (s.ncells[0] * s.ncells[1])};
+    for (int nb = 0; nb < nstencil; nb++) {
+      int c[3] = {rc[0] + cmap[nb][0], rc[1] + cmap[nb][1], rc[2] + cmap[nb][2]};
+      if (!cell_pbc(s, c)) continue;
+      int nid = c[0] + s.ncells[0] * (c[1] + s.ncells[1] * c[2]);
+      for (int i = s.head[ic]; i >= 0; i = s.clist[i]) {
+        int j;
+        if (s.half && nb == 0)
+          j = s.clist[i];
+        else
+          j = s.head[nid];
+        for (; j >= 0; j = s.clist[j]) {
+          if (!s.half && i == j) continue;
+          double vd[3];
+          vdist(s, j, i, vd);  // respetar el orden
+          double rd = dot3(vd);
+          if (rd < rcut) add_nb(s, i, j);
+        }
+      }
+    }
+  }
+}
+
+// intergroup_setcells (Neighbour.F90:587-664) + update (:1242-1299)
+void update(Sys& s) {
+  s.nupd++;
+  s.pos_old = s.pos;
+  s.use_cells = false;
+  if (s.boxed) {
+    double rc = s.rcut + s.skin;
+    bool any4 = false;
+    for (int l = 0; l < 3; l++) {
+      s.ncells[l] = (int)(s.box[l] / rc);
+      if (s.ncells[l] >= 4) any4 = true;
+    }
+    if (any4) {
+      s.use_cells = true;
+      for (int l = 0; l < 3; l++) s.cell[l] = s.box[l] / s.ncells[l];
+    }
+  }
+  if (s.use_cells)
+    linkedcell_build(s);
+  else
+    verlet_build(s);
+}
+
+// test_update (Neighbour.F90:1305-1346)
+bool test_update(Sys& s) {
+  double d1 = 1.e-16, d2 = 1.e-16;
+  for (int i = 0; i < s.n; i++) {
+    double vd[3];
+    for (int l = 0; l < 3; l++) vd[l] = s.pos[3 * i + l] - s.pos_old[3 * i + l];
+    double rd = dot3(vd);
+    if (rd > d1) {
+      d2 = d1;
+      d1 = rd;
+    } else if (rd > d2) {
+      d2 = rd;
+    }
+  }
+  if (std::sqrt(d1) + std::sqrt(d2) > s.skin) {
+    update(s);
+    return true;
+  }
+  return false;
+}
+
+// x**6 the way gfortran expands it (x3 = x2*x, x6 = x3*x3)
+inline double pow6(double x) {
+  double x3 = x * x * x;
+  return x3 * x3;
+}
+
+// lj_interact / plj_interact (Pairs.F90:207-370), full list, newton off
+double lj_interact(Sys& s) {
+  double etot = 0.0;
+  const int n = s.n;
+#pragma omp parallel for schedule(static) reduction(+ : etot)
+  for (int i = 0; i < n; i++) {
+    int ti = s.type[i];
+    double fx = 0, fy = 0, fz = 0, ep = 0;
+    for (int l = 0; l < s.nn[i]; l++) {
+      int j = s.list[(size_t)l * n + i];
+      const LJp& P = s.lj[ti][s.type[j]];
+      if (!P.on) continue;
+      double vd[3];
+      vdist(s, j, i, vd);
+      double dr = dot3(vd);
+      if (dr > P.rc2) continue;
+      dr = std::sqrt(dr);
+      double s_dr = pow6(P.s / dr);
+      double p, f;
+      if (P.shifted_force) {
+        p = 4.0 * P.e * (s_dr * s_dr - s_dr) - P.prc - P.frc * (dr - P.rc);
+        f = P.e * (48.0 * s_dr - 24.0) * s_dr / dr + P.frc;
+      } else {
+        p = 4.0 * P.e * (s_dr * s_dr - s_dr) - P.eshift;
+        f = P.e * (48.0 * s_dr - 24.0) * s_dr / dr;
+      }
+      p = p * ev_ui;
+      f = f * ev_ui;
+      ep = ep + p * 0.5;
+      etot = etot + p * 0.5;
+      fx = fx - f * vd[0] / dr;
+      fy = fy - f * vd[1] / dr;
+      fz = fz - f * vd[2] / dr;
+    }
+    s.force[3 * i] += fx;
+    s.force[3 * i + 1] += fy;
+    s.force[3 * i + 2] += fz;
+    s.epot[i] += ep;
+  }
+  return etot;
+}
+
+// smatb_set (TB.F90:106-170): tail polynomial coefficients (Logsdail 2012)
+void smatb_set(SMp& P, double a, double eps, double p, double q, double r0,
+               double rci, double rce) {
+  P.on = true;
+  P.ca = a; P.eps = eps; P.p = p; P.q = q; P.r0 = r0; P.rci = rci; P.rce = rce;
+  double dcut = rce - rci;
+  double ab = -1.0 / (dcut * dcut * dcut);
+  double bb = -(q / r0) / (dcut * dcut);
+  double cb = -((q / r0) * (q / r0)) / dcut;
+  double aux = eps * std::exp(-q * (rci / r0 - 1.0));
+  P.b1 = aux * (12.0 * ab - 6.0 * bb + cb) / (2.0 * (dcut * dcut));
+  P.b2 = aux * (15.0 * ab - 7.0 * bb + cb) / dcut;
+  P.b3 = aux * (20.0 * ab - 8.0 * bb + cb) / 2.0;
+  aux = a * std::exp(-p * (rci / r0 - 1.0));
+  bb = -(p / r0) / (dcut * dcut);
+  cb = -((p / r0) * (p / r0)) / dcut;
+  P.r1 = aux * (12.0 * ab - 6.0 * bb + cb) / (2.0 * (dcut * dcut));
+  P.r2 = aux * (15.0 * ab - 7.0 * bb + cb) / dcut;
+  P.r3 = aux * (20.0 * ab - 8.0 * bb + cb) / 2.0;
+}
+
+// smatb_preinteraction (TB.F90:367-455) + smatb_interact (TB.F90:457-586)
+double smatb_interact(Sys& s) {
+  const int n = s.n;
+  s.band.assign(n, 0.0);
+  s.eband.assign(n, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    int z1 = s.type[i];
+    double band = 0.0;
+    for (int l = 0; l < s.nn[i]; l++) {
+      int j = s.list[(size_t)l * n + i];
+      const SMp& P = s.sm[z1][s.type[j]];
+      double vd[3];
+      vdist(s, j, i, vd);
+      double dr = std::sqrt(dot3(vd));
+      if (dr > P.rce) continue;
+      double banda;
+      if (dr < P.rci) {
+        double r0 = P.r0;
+        banda = P.eps * P.eps * std::exp(-2.0 * P.q * (dr / r0 - 1.0));
+      } else {
+        double drm = dr - P.rce;
+        double drm2 = drm * drm, drm3 = drm2 * drm, drm4 = drm3 * drm,
+               drm5 = drm4 * drm;
+        banda = P.b1 * drm5 + P.b2 * drm4 + P.b3 * drm3;
+        banda = banda * banda;
+      }
+      band = band + banda;
+    }
+    s.band[i] = band;
+  }
+  for (int i = 0; i < n; i++) s.eband[i] = 1.0 / std::sqrt(s.band[i]);
+
+  const double lev_ui = ev_ui;
+  double epot = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : epot)
+  for (int i = 0; i < n; i++) {
+    int z1 = s.type[i];
+    double f[3] = {0, 0, 0}, ep = 0.0;
+    for (int l = 0; l < s.nn[i]; l++) {
+      int j = s.list[(size_t)l * n + i];
+      const SMp& P = s.sm[z1][s.type[j]];
+      double vd[3];
+      vdist(s, j, i, vd);
+      double dr = std::sqrt(dot3(vd));
+      double factor = 0.0, repul = 0.0;
+      if (dr > P.rce) continue;
+      if (dr <= P.rci) {
+        double r0 = P.r0;
+        repul = P.ca * std::exp(-P.p * (dr / r0 - 1.0));
+        factor = 2.0 * repul * (P.p / r0) -
+                 P.eps * P.eps * 1.0 / 2.0 *
+                     std::exp(-2.0 * P.q * (dr / r0 - 1.0)) *
+                     (2.0 * P.q / r0) * (s.eband[i] + s.eband[j]);
+      } else {
+        double drm = dr - P.rce;
+        double drm2 = drm * drm, drm3 = drm2 * drm, drm4 = drm3 * drm,
+               drm5 = drm4 * drm;
+        factor = (P.b1 * drm5 + P.b2 * drm4 + P.b3 * drm3) *
+                 (5.0 * P.b1 * drm4 + 4.0 * P.b2 * drm3 + 3.0 * P.b3 * drm2) *
+                 (s.eband[i] + s.eband[j]);
+        factor = factor -
+                 2.0 * (5.0 * P.r1 * drm4 + 4.0 * P.r2 * drm3 + 3.0 * P.r3 * drm2);
+        repul = P.r1 * drm5 + P.r2 * drm4 + P.r3 * drm3;
+      }
+      for (int k = 0; k < 3; k++) f[k] = f[k] - factor * lev_ui * vd[k] / dr;
+      ep = ep + repul * lev_ui;
+      epot = epot + repul * lev_ui;
+    }
+    double aux2 = std::sqrt(s.band[i]) * lev_ui;
+    ep = ep - aux2;
+    epot = epot - aux2;
+    for (int k = 0; k < 3; k++) s.force[3 * i + k] += f[k];
+    s.epot[i] += ep;
+  }
+  return epot;
+}
+
+// fcut_dfcut (Algebra.F90:391-409)
+inline double fcut_dfcut(double r, double r1, double r2, double* dfc) {
+  if (r < r1) {
+    *dfc = 0.0;
+    return 1.0;
+  } else if (r > r2) {
+    *dfc = 0.0;
+    return 0.0;
+  }
+  double aux = pi * (r - (r1 + r2) * 0.5) / (r2 - r1);
+  *dfc = -std::cos(aux) * pio2 / (r2 - r1);
+  return 0.5 - 0.5 * std::sin(aux);
+}
+
+// Tersoff 1988 (PRB 37, 6991), restated with forces that are the exact
+// gradient of E = sum_i sum_{j!=i} 1/2 fc(r_ij) [VR(r_ij) + b_ij VA(r_ij)].
+// Same functional form and cutoff as Tersoff.f90:131-341 + Algebra.F90:
+// 391-409 (no lambda3 term, chi prefactor); the reference's missing radial
+// force on j and its unallocated gradb_k are NOT reproduced.
+double tersoff_interact(Sys& s) {
+  const TSp& T = s.ts;
+  const int n = s.n;
+  const double r1 = T.R - T.D, r2 = T.R + T.D;
+  const double c2 = T.c * T.c, d2 = T.d * T.d;
+  const double btnp = std::pow(T.beta, T.n);
+  const double A = T.A * ev_ui, B = T.B * ev_ui;
+  double etot = 0.0;
+  // Per-atom forces are gathered into a private buffer per thread and
+  // reduced in a fixed order afterwards (deterministic).
+  int nth = 1;
+#ifdef _OPENMP
+  nth = omp_get_max_threads();
+#endif
+  std::vector<double> fbuf((size_t)nth * 3 * n, 0.0);
+#pragma omp parallel reduction(+ : etot)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* F = &fbuf[(size_t)tid * 3 * n];
+    std::vector<int> kk;
+    std::vector<double> kv, kr;
+#pragma omp for schedule(static)
+    for (int i = 0; i < n; i++) {
+      // gather bonded neighbours of i (r <= r2)
+      kk.clear(); kv.clear(); kr.clear();
+      for (int m = 0; m < s.nn[i]; m++) {
+        int j = s.list[(size_t)m * n + i];
+        double vd[3];
+        vdist(s, j, i, vd);  // r_j - r_i
+        double rd = std::sqrt(dot3(vd));
+        if (rd > r2) continue;
+        kk.push_back(j);
+        kr.push_back(rd);
+        kv.push_back(vd[0] / rd); kv.push_back(vd[1] / rd); kv.push_back(vd[2] / rd);
+      }
+      const int nb = (int)kk.size();
+      for (int a = 0; a < nb; a++) {
+        int j = kk[a];
+        double rij = kr[a];
+        const double* u = &kv[3 * a];
+        double dfc;
+        double fc = fcut_dfcut(rij, r1, r2, &dfc);
+        double vr = A * std::exp(-T.l1 * rij), dvr = -T.l1 * vr;
+        double va = -B * std::exp(-T.l2 * rij), dva = -T.l2 * va;
+        // zeta_ij and its pieces
+        double zij = 0.0;
+        for (int b = 0; b < nb; b++) {
+          if (b == a) continue;
+          double dfk;
+          double fk = fcut_dfcut(kr[b], r1, r2, &dfk);
+          const double* w = &kv[3 * b];
+          double ct = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
+          double hc = T.h - ct;
+          double g = 1.0 + c2 / d2 - c2 / (d2 + hc * hc);
+          zij += fk * g;
+        }
+        double bij, dbdz;
+        if (zij > 1.0e-15) {
+          double zn = std::pow(zij, T.n);
+          double aux = 1.0 / (1.0 + btnp * zn);
+          bij = T.chi * std::pow(aux, 0.5 / T.n);
+          dbdz = -0.5 * bij * aux * btnp * std::pow(zij, T.n - 1.0);
+        } else {
+          bij = T.chi;
+          dbdz = 0.0;
+        }
+        double e = 0.5 * fc * (vr + bij * va);
+        s.epot[i] += e;
+        etot += e;
+        // radial part: dE/dr_ij along u (u points i->j)
+        double dV = 0.5 * (dfc * (vr + bij * va) + fc * (dvr + bij * dva));
+        for (int k = 0; k < 3; k++) {
+          F[3 * i + k] += dV * u[k];
+          F[3 * j + k] -= dV * u[k];
+        }
+        if (dbdz == 0.0) continue;
+        double pre = 0.5 * fc * va * dbdz;  // dE/dzeta
+        for (int b = 0; b < nb; b++) {
+          if (b == a) continue;
+          int k = kk[b];
+          double rik = kr[b];
+          const double* w = &kv[3 * b];
+          double dfk;
+          double fk = fcut_dfcut(rik, r1, r2, &dfk);
+          double ct = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
+          double hc = T.h - ct;
+          double den = d2 + hc * hc;
+          double g = 1.0 + c2 / d2 - c2 / den;
+          double dg = -2.0 * c2 * hc / (den * den);  // dg/dcos
+          // d cos / d r_j = (w - ct u)/rij ; d cos / d r_k = (u - ct w)/rik
+          for (int q = 0; q < 3; q++) {
+            double dcj = (w[q] - ct * u[q]) / rij;
+            double dck = (u[q] - ct * w[q]) / rik;
+            double gj = fk * dg * dcj;                      // dzeta/dr_j
+            double gk = dfk * g * w[q] + fk * dg * dck;     // dzeta/dr_k
+            F[3 * j + q] -= pre * gj;
+            F[3 * k + q] -= pre * gk;
+            F[3 * i + q] += pre * (gj + gk);
+          }
+        }
+      }
+    }
+  }
+  for (int t = 0; t < nth; t++)
+    for (size_t q = 0; q < (size_t)3 * n; q++) s.force[q] += fbuf[(size_t)t * 3 * n + q];
+  return etot;
+}
+
+// interact (Interaction.f90:135-241): list test/update, zero, force field
+double interact(Sys& s, bool* rebuilt) {
+  bool rb;
+  if (s.first) {
+    s.first = false;
+    update(s);
+    rb = true;
+  } else {
+    rb = test_update(s);
+  }
+  if (rebuilt) *rebuilt = rb;
+  std::fill(s.force.begin(), s.force.end(), 0.0);
+  std::fill(s.epot.begin(), s.epot.end(), 0.0);
+  double e = 0.0;
+  if (s.ff == FF_LJ) e = lj_interact(s);
+  else if (s.ff == FF_SMATB) e = smatb_interact(s);
+  else if (s.ff == FF_TERSOFF) e = tersoff_interact(s);
+  s.last_epot = e;
+  return e;
+}
+
+// do_pbc_1 (Set_Properties.f90:444-470)
+void do_pbc(Sys& s) {
+  if (!s.boxed) return;
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++)
+      if (s.pbc[k]) {
+        if (s.pos[3 * i + k] >= s.box[k])
+          s.pos[3 * i + k] = s.pos[3 * i + k] - s.box[k];
+        else if (s.pos[3 * i + k] < 0.0)
+          s.pos[3 * i + k] = s.pos[3 * i + k] + s.box[k];
+      }
+}
+
+// set_ermak (Integration.F90:909-961)
+void set_ermak(Sys& s, double dt, double gama, double temp) {
+  s.integ = IT_ERMAK;
+  s.dt = dt;
+  s.gama = gama;
+  s.temp = temp;
+  s.cc0 = std::exp(-dt * gama);
+  s.cc1 = (1.0 - s.cc0) / gama;
+  s.cc2 = (1.0 - s.cc1 / dt) / gama;
+  s.sdr = std::sqrt(dt / gama * (2.0 - (3.0 - 4.0 * s.cc0 + s.cc0 * s.cc0) / (dt * gama)));
+  s.sdv = std::sqrt(1.0 - s.cc0 * s.cc0);
+  s.crv1 = (1.0 - s.cc0) * (1.0 - s.cc0) / (gama * s.sdr * s.sdv);
+  s.crv2 = std::sqrt(1.0 - (s.crv1 * s.crv1));
+  s.skt = std::sqrt(kB_ui * temp);
+}
+
+// velocity_verlet_a (Integration.F90:1150-1168)
+void vv_a(Sys& s) {
+  double acel_dv = s.dt * 0.5, acel_dx = acel_dv * s.dt;
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++) {
+      int q = 3 * i + k;
+      s.acel[q] = s.force[q] * s.one_mass[i];
+      s.pos[q] = s.pos[q] + s.dt * s.vel[q] + acel_dx * s.acel[q];
+      s.vel[q] = s.vel[q] + acel_dv * s.acel[q];
+    }
+}
+
+// velocity_verlet_b (Integration.F90:1171-1186)
+void vv_b(Sys& s) {
+  double acel_dv = s.dt * 0.5;
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++) {
+      int q = 3 * i + k;
+      s.acel[q] = s.force[q] * s.one_mass[i];
+      s.vel[q] = s.vel[q] + acel_dv * s.acel[q];
+    }
+}
+
+// ermak_a (Integration.F90:963-1011).  Normals come from the LCG stream
+// (rang, one pair per dimension) or from an external stream of 6 per atom.
+void ermak_a(Sys& s) {
+  for (int i = 0; i < s.n; i++) {
+    double f_lan = s.skt * s.one_sqrt_mass[i];
+    for (int j = 0; j < 3; j++) {
+      double r1, r2;
+      if (s.ext_normals) {
+        r1 = s.ext_normals[6 * i + 2 * j];
+        r2 = s.ext_normals[6 * i + 2 * j + 1];
+      } else {
+        rang(*s.rng, &r1, &r2);
+      }
+      s.pos_v[3 * i + j] = f_lan * s.sdr * r1;
+      s.vel_v[3 * i + j] = f_lan * s.sdv * (s.crv1 * r1 + s.crv2 * r2);
+    }
+    for (int k = 0; k < 3; k++) {
+      int q = 3 * i + k;
+      s.pos[q] = s.pos[q] + s.cc1 * s.vel[q] + s.cc2 * s.dt * s.acel[q] + s.pos_v[q];
+    }
+  }
+}
+
+// ermak_b (Integration.F90:1013-1031)
+void ermak_b(Sys& s) {
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++) {
+      int q = 3 * i + k;
+      s.vel[q] = s.cc0 * s.vel[q] + (s.cc1 - s.cc2) * s.acel[q] +
+                 s.cc2 * s.force[q] * s.one_mass[i] + s.vel_v[q];
+      s.acel[q] = s.force[q] * s.one_mass[i];
+    }
+}
+
+// inq_cm_vel / inq_kin_energy / inq_temperature (Inq_Properties.F90:399-437,
+// 669-698): Ekin with the centre-of-mass velocity removed.
+void kin(const Sys& s, double* ekin, double* temp) {
+  double cm[3] = {0, 0, 0}, mt = 0.0;
+  for (int i = 0; i < s.n; i++) mt = mt + s.mass[i];
+  if (s.n == 1) {
+    for (int k = 0; k < 3; k++) cm[k] = s.vel[k];
+  } else {
+    for (int i = 0; i < s.n; i++)
+      for (int k = 0; k < 3; k++) cm[k] = cm[k] + s.mass[i] * s.vel[3 * i + k];
+    for (int k = 0; k < 3; k++) cm[k] = cm[k] / mt;
+  }
+  double ek = 0.0;
+  for (int i = 0; i < s.n; i++) {
+    double v[3];
+    for (int k = 0; k < 3; k++) v[k] = s.vel[3 * i + k] - cm[k];
+    ek = ek + dot3(v) * s.mass[i];
+  }
+  ek = ek * 0.5;
+  *ekin = ek;
+  *temp = 2.0 * ek / (kB_ui * (3 * s.n));
+}
+
+void cm_vel(const Sys& s, double cm[3]) {
+  double mt = 0.0;
+  for (int i = 0; i < s.n; i++) mt = mt + s.mass[i];
+  cm[0] = cm[1] = cm[2] = 0.0;
+  if (s.n == 1) {
+    for (int k = 0; k < 3; k++) cm[k] = s.vel[k];
+    return;
+  }
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++) cm[k] = cm[k] + s.mass[i] * s.vel[3 * i + k];
+  for (int k = 0; k < 3; k++) cm[k] = cm[k] / mt;
+}
+
+// FIRE (Bitzek et al., PRL 97, 170201 (2006)), following the intent of
+// FIRE.f90:40-141 with its three defects fixed: |v| (not v.v) in the mixing,
+// f_dec applied on P<=0, and every velocity reset.  Parity unpinned.
+const double fire_alpha0 = 0.1, fire_finc = 1.1, fire_fdec = 0.5,
+             fire_falpha = 0.99;
+const int fire_nmin = 5;
+
+void fire_init(Sys& s, double dt0, double dtmax) {
+  s.integ = IT_FIRE;
+  s.dt = dt0;
+  s.fire_dt = dt0;
+  s.fire_dtmax = dtmax;
+  s.fire_alpha = fire_alpha0;
+  s.fire_np = 0;
+  std::fill(s.vel.begin(), s.vel.end(), 0.0);
+}
+
+// one FIRE iteration given current forces: MD half steps use velocity Verlet
+// with the current fire_dt; returns max |F| (eV/A) after the force call.
+void fire_mix(Sys& s) {
+  // P = sum_atoms v.F (FIRE.f90:99-105)
+  double P = 0.0;
+  for (int q = 0; q < 3 * s.n; q++) P = P + s.vel[q] * s.force[q];
+  // per-atom mixing v = (1-a) v + a |v| F/|F| (FIRE.f90:107-114, with |v|)
+  for (int i = 0; i < s.n; i++) {
+    double* v = &s.vel[3 * i];
+    const double* f = &s.force[3 * i];
+    double vn = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    double fn = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    double mixf = fn > 0.0 ? s.fire_alpha * vn / fn : 0.0;
+    for (int k = 0; k < 3; k++) v[k] = v[k] * (1.0 - s.fire_alpha) + mixf * f[k];
+  }
+  if (P > 0.0) {
+    s.fire_np++;
+    if (s.fire_np > fire_nmin) {
+      s.fire_dt = std::min(s.fire_dt * fire_finc, s.fire_dtmax);
+      s.fire_alpha = s.fire_alpha * fire_falpha;
+    }
+  } else {
+    s.fire_np = 0;
+    s.fire_dt = s.fire_dt * fire_fdec;
+    s.fire_alpha = fire_alpha0;
+    std::fill(s.vel.begin(), s.vel.end(), 0.0);
+  }
+  s.dt = s.fire_dt;
+}
+
+double fmax_ev(const Sys& s) {
+  double m = 0.0;
+  for (int i = 0; i < s.n; i++) {
+    double v[3] = {s.force[3 * i], s.force[3 * i + 1], s.force[3 * i + 2]};
+    m = std::max(m, std::sqrt(dot3(v)));
+  }
+  return m * ui_ev;
+}
+
+void stepa(Sys& s) {
+  if (s.integ == IT_VV || s.integ == IT_FIRE) vv_a(s);
+  else if (s.integ == IT_ERMAK) ermak_a(s);
+  do_pbc(s);
+}
+
+void stepb(Sys& s) {
+  if (s.integ == IT_VV || s.integ == IT_FIRE) vv_b(s);
+  else if (s.integ == IT_ERMAK) ermak_b(s);
+  do_pbc(s);
+  if (s.integ == IT_FIRE) fire_mix(s);
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+extern "C" {
+
+double orc_ev_ui() { return ev_ui; }
+double orc_kB_ui() { return kB_ui; }
+int orc_max_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+// ---- RNG objects
+void* orc_rng_new(int seed) {
+  Lcg* r = new Lcg();
+  lcg_seed(*r, seed);
+  return r;
+}
+void orc_rng_free(void* r) { delete (Lcg*)r; }
+double orc_ranu(void* r) { return lcg_ranu(*(Lcg*)r); }
+void orc_rang(void* r, double* r1, double* r2) { rang(*(Lcg*)r, r1, r2); }
+// n pairs from rang, stored r1,r2,r1,r2,... (the Ermak parity stream)
+void orc_rang_stream(void* r, long npairs, double* out) {
+  for (long k = 0; k < npairs; k++) rang(*(Lcg*)r, &out[2 * k], &out[2 * k + 1]);
+}
+void orc_rng_state(void* r, int* st) {
+  Lcg* l = (Lcg*)r;
+  st[0] = l->idum; st[1] = l->ix; st[2] = l->iy; st[3] = l->gaus_stored;
+}
+
+// create_fill (Select_Create.F90:64-135): random sequential addition in
+// [origin, origin+frame) with the reference's overlap rule rd < (s_a+s_b)^2.
+// `pos` holds n_old existing atoms (with radii sig_old) followed by room for
+// `num` new ones.  No minimum image (the created atom has pbc off).
+int orc_fill(void* rng, int n_old, double* pos, const double* sig_old,
+             int num, double sigma, const double frame[3],
+             const double origin[3]) {
+  Lcg& r = *(Lcg*)rng;
+  const int nmax = 1000;
+  std::vector<double> sig(sig_old, sig_old + n_old);
+  int n = n_old;
+  for (int i = 0; i < num; i++) {
+    double a[3];
+    int it;
+    for (it = 1; it <= nmax; it++) {
+      for (int j = 0; j < 3; j++) a[j] = lcg_ranu(r) * frame[j] + origin[j];
+      bool ok = true;
+      for (int k = 0; k < n; k++) {
+        double vd[3] = {a[0] - pos[3 * k], a[1] - pos[3 * k + 1], a[2] - pos[3 * k + 2]};
+        double rd = dot3(vd);
+        double cut = sigma + sig[k];
+        cut = cut * cut;
+        if (rd < cut) { ok = false; break; }
+      }
+      if (ok) break;
+    }
+    if (it > nmax) return -1;
+    for (int j = 0; j < 3; j++) pos[3 * n + j] = a[j];
+    sig.push_back(sigma);
+    n++;
+  }
+  return n;
+}
+
+// ---- systems
+void* orc_sys_new(int n) {
+  Sys* s = new Sys();
+  s->n = n;
+  s->pos.assign(3 * n, 0.0);
+  s->vel.assign(3 * n, 0.0);
+  s->acel.assign(3 * n, 0.0);
+  s->force.assign(3 * n, 0.0);
+  s->pos_v.assign(3 * n, 0.0);
+  s->vel_v.assign(3 * n, 0.0);
+  s->pos_old.assign(3 * n, 0.0);
+  s->epot.assign(n, 0.0);
+  s->mass.assign(n, 1.0);
+  s->one_mass.assign(n, 1.0);
+  s->one_sqrt_mass.assign(n, 1.0);
+  s->type.assign(n, 0);
+  ensure_cap(*s, 256);
+  return s;
+}
+void orc_sys_free(void* p) { delete (Sys*)p; }
+
+void orc_set_pos(void* p, const double* x) { Sys* s = (Sys*)p; std::memcpy(s->pos.data(), x, sizeof(double) * 3 * s->n); }
+void orc_get_pos(void* p, double* x) { Sys* s = (Sys*)p; std::memcpy(x, s->pos.data(), sizeof(double) * 3 * s->n); }
+void orc_set_vel(void* p, const double* x) { Sys* s = (Sys*)p; std::memcpy(s->vel.data(), x, sizeof(double) * 3 * s->n); }
+void orc_get_vel(void* p, double* x) { Sys* s = (Sys*)p; std::memcpy(x, s->vel.data(), sizeof(double) * 3 * s->n); }
+void orc_set_acel(void* p, const double* x) { Sys* s = (Sys*)p; std::memcpy(s->acel.data(), x, sizeof(double) * 3 * s->n); }
+void orc_get_acel(void* p, double* x) { Sys* s = (Sys*)p; std::memcpy(x, s->acel.data(), sizeof(double) * 3 * s->n); }
+void orc_get_force(void* p, double* x) { Sys* s = (Sys*)p; std::memcpy(x, s->force.data(), sizeof(double) * 3 * s->n); }
+void orc_get_epot_atoms(void* p, double* x) { Sys* s = (Sys*)p; std::memcpy(x, s->epot.data(), sizeof(double) * s->n); }
+void orc_get_band(void* p, double* x) { Sys* s = (Sys*)p; std::memcpy(x, s->band.data(), sizeof(double) * s->n); }
+
+// set_mass (Set_Properties.f90:168-191)
+void orc_set_mass(void* p, const double* m) {
+  Sys* s = (Sys*)p;
+  for (int i = 0; i < s->n; i++) {
+    s->mass[i] = m[i];
+    if (m[i] == 0.0) {
+      s->one_mass[i] = 0.0;
+      s->one_sqrt_mass[i] = 0.0;
+    } else {
+      s->one_mass[i] = 1.0 / m[i];
+      s->one_sqrt_mass[i] = std::sqrt(s->one_mass[i]);
+    }
+  }
+}
+void orc_set_types(void* p, const int* t, int ntypes) {
+  Sys* s = (Sys*)p;
+  for (int i = 0; i < s->n; i++) s->type[i] = t[i];
+  s->ntypes = ntypes;
+}
+// box_setvars (Program_Types.F90:126-141); boxed=0 means no box
+void orc_set_box(void* p, int boxed, const double* L, const int* pbc) {
+  Sys* s = (Sys*)p;
+  s->boxed = boxed != 0;
+  for (int k = 0; k < 3; k++) {
+    s->box[k] = boxed ? L[k] : 0.0;
+    s->one_box[k] = boxed ? 1.0 / L[k] : 0.0;
+    s->pbc[k] = pbc ? pbc[k] : 0;
+  }
+}
+void orc_set_mic(void* p, int mic) { ((Sys*)p)->mic = mic != 0; }
+void orc_set_skin(void* p, double skin) { ((Sys*)p)->skin = skin; }
+void orc_set_half(void* p, int half) { ((Sys*)p)->half = half != 0; }
+void orc_set_capacity(void* p, int cap) { ensure_cap(*(Sys*)p, cap); }
+
+static void recompute_rcut(Sys* s) {
+  double rc = 0.0;
+  for (int a = 0; a < MAXT; a++)
+    for (int b = 0; b < MAXT; b++) {
+      if (s->ff == FF_LJ && s->lj[a][b].on) rc = std::max(rc, s->lj[a][b].rc);
+      if (s->ff == FF_SMATB && s->sm[a][b].on) rc = std::max(rc, s->sm[a][b].rce);
+    }
+  if (s->ff == FF_TERSOFF) rc = s->ts.R + s->ts.D;
+  s->rcut = rc;
+}
+
+// lj_set / plj_set (Pairs.F90:198-205, 282-291); eshift is an optional
+// constant energy shift per pair (eV), 0 for the reference's `lj`.
+void orc_set_lj(void* p, int ti, int tj, double e, double sg, double rc,
+                int shifted_force, double eshift) {
+  Sys* s = (Sys*)p;
+  s->ff = FF_LJ;
+  LJp P;
+  P.on = true; P.e = e; P.s = sg; P.rc = rc; P.rc2 = rc * rc;
+  P.shifted_force = shifted_force != 0;
+  P.eshift = eshift;
+  if (P.shifted_force) {
+    double x = sg / rc;
+    double x6 = pow6(x);
+    P.prc = 4.0 * e * (x6 * x6 - x6);
+    double s6 = pow6(sg), s12 = s6 * s6;
+    double rc6 = pow6(rc), rc7 = rc6 * rc, rc13 = rc6 * rc6 * rc;
+    P.frc = 24.0 * e * (2.0 * (s12 / rc13) - (s6 / rc7));
+  }
+  s->lj[ti][tj] = P;
+  s->lj[tj][ti] = P;
+  recompute_rcut(s);
+}
+
+void orc_set_smatb(void* p, int ti, int tj, double a, double eps, double pp,
+                   double q, double r0, double rci, double rce) {
+  Sys* s = (Sys*)p;
+  s->ff = FF_SMATB;
+  SMp P;
+  smatb_set(P, a, eps, pp, q, r0, rci, rce);
+  s->sm[ti][tj] = P;
+  s->sm[tj][ti] = P;
+  recompute_rcut(s);
+}
+// prm: A, B (eV), lambda1, lambda2, beta, n, c, d, h, R, D, chi
+void orc_set_tersoff(void* p, const double* prm) {
+  Sys* s = (Sys*)p;
+  s->ff = FF_TERSOFF;
+  TSp& T = s->ts;
+  T.A = prm[0]; T.B = prm[1]; T.l1 = prm[2]; T.l2 = prm[3]; T.beta = prm[4];
+  T.n = prm[5]; T.c = prm[6]; T.d = prm[7]; T.h = prm[8]; T.R = prm[9];
+  T.D = prm[10]; T.chi = prm[11];
+  recompute_rcut(s);
+}
+void orc_smatb_coeffs(void* p, int ti, int tj, double* out6) {
+  const SMp& P = ((Sys*)p)->sm[ti][tj];
+  out6[0] = P.b1; out6[1] = P.b2; out6[2] = P.b3;
+  out6[3] = P.r1; out6[4] = P.r2; out6[5] = P.r3;
+}
+
+// first call builds the list (update), later calls run test_update
+double orc_interact(void* p, int* rebuilt) {
+  bool rb;
+  double e = interact(*(Sys*)p, &rb);
+  if (rebuilt) *rebuilt = rb;
+  return e;
+}
+void orc_update(void* p) { Sys* s = (Sys*)p; s->first = false; update(*s); }
+long orc_nupd(void* p) { return ((Sys*)p)->nupd; }
+int orc_status(void* p) { Sys* s = (Sys*)p; return (s->overflow ? 1 : 0) | (s->lost ? 2 : 0); }
+int orc_list_cap(void* p) { return ((Sys*)p)->cap; }
+int orc_uses_cells(void* p, int* nc) {
+  Sys* s = (Sys*)p;
+  for (int k = 0; k < 3; k++) nc[k] = s->ncells[k];
+  return s->use_cells;
+}
+// copy out nn(n) and the column-major list (cap x n)
+void orc_get_list(void* p, int* nn, int* list) {
+  Sys* s = (Sys*)p;
+  std::memcpy(nn, s->nn.data(), sizeof(int) * s->n);
+  std::memcpy(list, s->list.data(), sizeof(int) * (size_t)s->n * s->cap);
+}
+
+void orc_set_vv(void* p, double dt) { Sys* s = (Sys*)p; s->integ = IT_VV; s->dt = dt; }
+void orc_set_ermak(void* p, double dt, double gama, double temp, void* rng) {
+  Sys* s = (Sys*)p;
+  set_ermak(*s, dt, gama, temp);
+  s->rng = (Lcg*)rng;
+}
+void orc_ermak_consts(void* p, double* out8) {
+  Sys* s = (Sys*)p;
+  out8[0] = s->cc0; out8[1] = s->cc1; out8[2] = s->cc2; out8[3] = s->sdr;
+  out8[4] = s->sdv; out8[5] = s->crv1; out8[6] = s->crv2; out8[7] = s->skt;
+}
+void orc_set_ext_normals(void* p, const double* nrm) { ((Sys*)p)->ext_normals = nrm; }
+void orc_set_fire(void* p, double dt0, double dtmax) { fire_init(*(Sys*)p, dt0, dtmax); }
+double orc_fire_dt(void* p) { return ((Sys*)p)->fire_dt; }
+double orc_fmax(void* p) { return fmax_ev(*(Sys*)p); }
+
+void orc_stepa(void* p) { stepa(*(Sys*)p); }
+void orc_stepb(void* p) { stepb(*(Sys*)p); }
+void orc_do_pbc(void* p) { do_pbc(*(Sys*)p); }
+
+// kinetic energy (CM removed) and temperature
+void orc_kin(void* p, double* ekin, double* temp) { kin(*(Sys*)p, ekin, temp); }
+double orc_epot_sum(void* p) {  // inq_pot_energy (Inq_Properties.F90:358-375)
+  Sys* s = (Sys*)p;
+  double e = 0.0;
+  for (int i = 0; i < s->n; i++) e = e + s->epot[i];
+  return e;
+}
+
+// set_gdist (Set_Properties.f90:301-349) over the whole system, in atom order
+void orc_gdist(void* p, void* rng, double newtemp) {
+  Sys* s = (Sys*)p;
+  Lcg& r = *(Lcg*)rng;
+  double cm[3];
+  cm_vel(*s, cm);
+  double factor = kB_ui * newtemp;
+  for (int i = 0; i < s->n; i++) {
+    double vel_med = std::sqrt(factor * s->one_mass[i]);
+    for (int j = 0; j < 3; j++) {
+      double r1;
+      rang(r, &r1, nullptr);
+      s->vel[3 * i + j] = vel_med * r1 + cm[j];
+    }
+  }
+  // set_scal_vel (Set_Properties.f90:351-377)
+  double ek, t;
+  kin(*s, &ek, &t);
+  if (t != 0.0) {
+    double f = std::sqrt(newtemp / t);
+    for (int q = 0; q < 3 * s->n; q++) s->vel[q] = s->vel[q] * f;
+  }
+  // remove the centre-of-mass drift (set_add_cmvel)
+  cm_vel(*s, cm);
+  for (int i = 0; i < s->n; i++)
+    for (int k = 0; k < 3; k++) s->vel[3 * i + k] = s->vel[3 * i + k] + (-cm[k]);
+}
+// `box move` (CLInterpreter.F90:1692-1695): subtract the CM velocity
+void orc_remove_cm(void* p) {
+  Sys* s = (Sys*)p;
+  double cm[3];
+  cm_vel(*s, cm);
+  for (int i = 0; i < s->n; i++)
+    for (int k = 0; k < 3; k++) s->vel[3 * i + k] = s->vel[3 * i + k] + (-cm[k]);
+}
+
+// dinamic (Programs.f90:114-167): interact once, then nsteps of
+// stepa / interact / stepb; every `each` steps append (Epot, Ekin, Etot, T)
+// in eV/K to rows.  Returns the number of rows written.
+int orc_dinamica(void* p, int nsteps, int each, double* rows) {
+  Sys* s = (Sys*)p;
+  interact(*s, nullptr);
+  int nr = 0;
+  for (int ns = 1; ns <= nsteps; ns++) {
+    stepa(*s);
+    interact(*s, nullptr);
+    stepb(*s);
+    if (each > 0 && ns % each == 0 && rows) {
+      double ek, t;
+      kin(*s, &ek, &t);
+      double ep = 0.0;
+      for (int i = 0; i < s->n; i++) ep = ep + s->epot[i];
+      rows[4 * nr + 0] = ep * ui_ev;
+      rows[4 * nr + 1] = ek * ui_ev;
+      rows[4 * nr + 2] = rows[4 * nr + 0] + rows[4 * nr + 1];
+      rows[4 * nr + 3] = t;
+      nr++;
+    }
+  }
+  return nr;
+}
+
+// FIRE relaxation to max|F| < fmax_tol (eV/A) or maxit iterations.  Returns
+// the number of iterations; *fmax_out the final max|F| in eV/A.
+int orc_fire_relax(void* p, double fmax_tol, int maxit, double* fmax_out) {
+  Sys* s = (Sys*)p;
+  interact(*s, nullptr);
+  int it = 0;
+  double fm = fmax_ev(*s);
+  while (fm >= fmax_tol && it < maxit) {
+    stepa(*s);
+    interact(*s, nullptr);
+    stepb(*s);
+    fm = fmax_ev(*s);
+    it++;
+  }
+  if (fmax_out) *fmax_out = fm;
+  return it;
+}
+
+}  // extern "C"

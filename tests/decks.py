@@ -1,0 +1,141 @@
+"""Restatements of the reference's regression decks (examples/*/*.gms).
+
+Each function builds the same system the deck builds -- atom order, box,
+periodic flags, potentials, integrator and random stream -- so a run can be
+compared with the golden rows of tests/golden/golden.json under the rule of
+examples/test.sh.  The builders return plain numpy data plus a `setup`
+callable that applies the deck's settings to any engine exposing the
+oracle.System / gems_b200.System setter names, so the same deck drives the
+oracle (CPU) and the CUDA path.
+"""
+import json
+import math
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.json")
+_G = None
+
+
+def golden():
+    global _G
+    if _G is None:
+        with open(GOLDEN) as f:
+            _G = json.load(f)
+    return _G
+
+
+def f32(x):
+    """A default-real Fortran literal widened to real(dp) (e.g. e(47)%mass=107.87)."""
+    return float(np.float32(x))
+
+
+# Elements.F90 masses (single-precision literals assigned to real(dp))
+MASS = {"H": f32(1.008), "He": f32(4.0032), "Ne": f32(20.183), "Si": f32(28.09),
+        "Ag": f32(107.87), "Pt": f32(195.08), "Au": f32(196.97)}
+
+# Fortran `dt=0.002` default (Program_Types.F90:53): a single-precision literal
+DT_DEFAULT = f32(0.002)
+
+# examples/test.sh pass rule: abs(sum((ref-new)^2) / sum(ref)) < 1e-6
+def gems_rule(ref, new):
+    ref = np.asarray(ref, dtype=np.float64)
+    new = np.asarray(new, dtype=np.float64)
+    return abs(np.sum((ref - new) ** 2) / np.sum(ref))
+
+
+def e15(x):
+    """Round like the E15.7 output format (7 significant digits)."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.zeros_like(x)
+    nz = x != 0
+    mag = np.floor(np.log10(np.abs(x[nz]))) + 1
+    out[nz] = np.round(x[nz] / 10.0 ** mag, 7) * 10.0 ** mag
+    return out
+
+
+# --------------------------------------------------------------- XYZ deck
+def xyz_deck():
+    """examples/XYZ/readxyz.gms: LJ energy of 6 frames, PBC box, no RNG."""
+    g = golden()
+    return dict(
+        frames=[np.array(f, dtype=np.float64) for f in g["xyz_frames"]],
+        box=(13.1399, 12.64396, 20.0000),
+        lj=(0.1, 3.890898718140339, 10.0),
+        ref=np.array(g["xyz_energy"])[:, 0],
+    )
+
+
+# --------------------------------------------------------------- LJ dimer
+def lj_dimer_deck():
+    """examples/LJ/lj.gms: dimer scan (251 states) then 1000 VV steps."""
+    g = golden()
+    tau_ps = 0.01018
+    return dict(
+        pos0=np.array([[1.0, 1.0, 1.0], [2.2, 1.0, 1.0]]),
+        mass=3.0,
+        box=(5.78, 5.78, 5.78),
+        lj=(1.0, 0.890898718140339, 2.0),
+        dt=0.002 * tau_ps,
+        ref=np.array(g["lj_energy"]),
+    )
+
+
+# --------------------------------------------------------------- SMA-TB bulk
+def fcc_reply_positions():
+    """bulk.gms atom order: 4-atom cell then `reply` along x, y, z (10 each).
+
+    create_reply (Select_Create.F90:137-165) appends, for every atom of the
+    current selection in order, its times-1 translated copies.
+    """
+    sel = [np.array(p, dtype=np.float64) for p in
+           ([0, 0, 0], [0.5, 0.5, 0], [0, 0.5, 0.5], [0.5, 0, 0.5])]
+    for tras in ([1, 0, 0], [0, 1, 0], [0, 0, 1]):
+        t = np.array(tras, dtype=np.float64)
+        new = []
+        for a in sel:
+            for j in range(1, 10):
+                new.append(a + t * j)
+        sel = sel + new
+    return np.array(sel)
+
+
+def bulk_deck():
+    """examples/SMA-TB/bulk.gms: 4000 Ag fcc, boxed, no PBC, Ermak 1500 K."""
+    g = golden()
+    d0 = math.sqrt(0.5)
+    fact = 2.89 / d0
+    pos = fcc_reply_positions()
+    pos = pos + np.array([1.0, 1.0, 1.0])
+    pos = pos * fact            # expand about the origin
+    box = tuple(12.0 * fact for _ in range(3))
+    # baletto_2003.prm, Ag Ag line
+    ag = (0.1031, 1.1899, 10.85, 3.18, 2.89, 2.89 * math.sqrt(2.0), 2.89 * math.sqrt(3.0))
+    return dict(pos=pos, mass=MASS["Ag"], box=box, pbc=(False, False, False),
+                smatb=ag, dt=DT_DEFAULT, temp=1500.0, gamma=1.0, nsteps=220,
+                each=20, seed=123456, ref=np.array(g["smatb_bulk_energy"]))
+
+
+# --------------------------------------------------------------- NVE / NVT
+def he_ne_gas(rng):
+    """v_verlet.gms / ermak.gms set-up: `fill 100 2.6` He then Ne in 50^3."""
+    box = (50.0, 50.0, 50.0)
+    he = rng.fill(np.zeros((0, 3)), [], 100, 2.6, box)
+    ne = rng.fill(he, [2.6] * 100, 100, 2.6, box)
+    pos = np.concatenate([he, ne])
+    types = np.array([0] * 100 + [1] * 100, dtype=np.int32)
+    mass = np.array([MASS["He"]] * 100 + [MASS["Ne"]] * 100)
+    return pos, types, mass, box
+
+
+def plj_params():
+    """The three plj groups of v_verlet.gms (He-He, Ne-Ne, He-Ne)."""
+    cal_ev = 2.61144768e19
+    na = 6.0221417930e23
+    kcalmol_ev = cal_ev / na * 1000.0
+    return {
+        (0, 0): (0.021270 * kcalmol_ev, 1.4800),
+        (1, 1): (0.086000 * kcalmol_ev, 1.5300),
+        (0, 1): (math.sqrt(0.086000 * 0.021270) * kcalmol_ev, 0.5 * (1.5300 + 1.4800)),
+    }

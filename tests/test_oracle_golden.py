@@ -1,0 +1,137 @@
+"""The FP64 oracle against the reference's golden files (CPU only).
+
+Each test restates one regression deck of examples/ and applies the pass rule
+of examples/test.sh (abs(sum((ref-new)^2)/sum(ref)) < 1e-6 on the Epot
+column); the tests additionally require agreement to the printed 7 digits.
+"""
+import numpy as np
+import pytest
+
+import decks
+from oracle import oracle as O
+
+
+def test_units():
+    # Constants.F90:101-175: ui_ev = 1e4 * 1.6605402e-27 / 1.60219e-19
+    assert abs(1.0 / O.lib().orc_ev_ui() - 1.0364190264575364e-4) < 1e-18
+    assert O.lib().orc_kB_ui() == pytest.approx(8.617385e-05 / 1.0364190264575364e-4, rel=1e-15)
+
+
+def test_lcg_stream_known_values():
+    # lcg_ranu with idum=-123456 (Random.F90:145-171); the first value is
+    # am * ior(iand(im, ieor(ix, iy)), 1) after one xorshift / Schrage step.
+    r = O.Rng(123456)
+    a = 123456
+    iy = (888889999 ^ a) | 1
+    ix = 777755555 ^ a
+    ix &= 0xFFFFFFFF
+    ix ^= (ix << 13) & 0xFFFFFFFF
+    ix ^= ix >> 17
+    ix ^= (ix << 5) & 0xFFFFFFFF
+    ix = ix - (1 << 32) if ix >= (1 << 31) else ix
+    k = iy // 127773
+    iy = 16807 * (iy - k * 127773) - 2836 * k
+    if iy < 0:
+        iy += 2147483647
+    am = float(np.float32(np.float32(1.0) - np.float32(2.0 ** -24)) / np.float32(2147483648.0))
+    expect = am * float((2147483647 & (ix ^ iy)) | 1)
+    assert r.ranu() == expect
+
+
+def test_xyz_frames_lj_pbc():
+    """examples/XYZ: LJ energy of 6 fixed frames (PBC, O(N^2) list)."""
+    d = decks.xyz_deck()
+    s = O.System(d["frames"][0], 12.0)
+    s.set_box(d["box"], (True, True, True))
+    s.set_lj(*d["lj"])
+    out = []
+    for f in d["frames"]:
+        s.set_pos(f)
+        s.interact()
+        out.append(s.epot_sum() * O.UI_EV)
+    assert not s.uses_cells()[0]
+    assert decks.gems_rule(d["ref"], out) < 1e-6
+    np.testing.assert_allclose(out, d["ref"], rtol=2e-7)
+
+
+def lj_dimer_rows(sys_factory, ui_ev):
+    d = decks.lj_dimer_deck()
+    pos = d["pos0"].copy()
+    s = sys_factory(pos, d["mass"])
+    s.set_box(d["box"], (False, False, False))
+    s.set_lj(*d["lj"])
+    rows = []
+
+    def state():
+        s.set_pos(pos)
+        s.interact()
+        ek, _ = s.kin()
+        ep = s.epot_sum()
+        rows.append([ep * ui_ev, ek * ui_ev, (ep + ek) * ui_ev])
+
+    state()
+    for mv in (-1.2, 0.9):
+        pos[1, 0] = pos[1, 0] + mv
+    for _ in range(250):
+        pos[1, 0] = pos[1, 0] + 0.01
+        state()
+    for mv in (-2.5, -0.9, 1.2):
+        pos[1, 0] = pos[1, 0] + mv
+    s.set_pos(pos)
+    s.set_vv(d["dt"])
+    r = s.dinamica(1000, 10)
+    return np.concatenate([np.array(rows), r[:, :3]]), d["ref"]
+
+
+def test_lj_dimer_scan_and_vv():
+    """examples/LJ/lj.gms: 251 dimer states + 1000 velocity-Verlet steps."""
+    got, ref = lj_dimer_rows(O.System, 1.0 / O.lib().orc_ev_ui())
+    assert got.shape == ref.shape
+    assert decks.gems_rule(ref[:, 0], got[:, 0]) < 1e-6
+    np.testing.assert_allclose(got, ref, atol=1e-7, rtol=1e-6)
+
+
+def test_smatb_bulk_linked_cells_ermak():
+    """examples/SMA-TB/bulk.gms: 4000 Ag, linked cells, Ermak 1500 K, LCG."""
+    d = decks.bulk_deck()
+    s = O.System(d["pos"], d["mass"])
+    s.set_box(d["box"], d["pbc"])
+    s.set_smatb(*d["smatb"])
+    s.set_ermak(d["dt"], d["gamma"], d["temp"], O.Rng(d["seed"]))
+    r = s.dinamica(d["nsteps"], d["each"])
+    assert s.uses_cells() == (True, (8, 8, 8))
+    assert decks.gems_rule(d["ref"][:, 0], r[:, 0]) < 1e-6
+    np.testing.assert_allclose(r[:, :3], d["ref"], rtol=1e-6)
+
+
+def _he_ne(kind):
+    g = decks.golden()
+    rng = O.Rng(123456)
+    pos, types, mass, box = decks.he_ne_gas(rng)
+    s = O.System(pos, mass, types, 2)
+    s.set_box(box, (True, True, True))
+    for (a, b), (e, sg) in decks.plj_params().items():
+        s.set_lj(e, sg, 10.0, a, b, shifted_force=True)
+    s.remove_cm()
+    s.gdist(rng, 300.0)
+    if kind == "nve":
+        s.set_vv(0.002)
+        return s.dinamica(5000, 100), np.array(g["nve_energy"])
+    s.set_ermak(0.002, 10.0, 300.0, rng)
+    return s.dinamica(10000, 100), np.array(g["nvt_energy"])
+
+
+def test_nve_plj_fill_gdist_vv():
+    """examples/NVE/v_verlet.gms: fill + tempgdist + 3 plj groups + VV."""
+    r, ref = _he_ne("nve")
+    assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
+    np.testing.assert_allclose(r[:, 0], ref[:, 0], atol=2e-8)
+    np.testing.assert_allclose(r[:, 1:3], ref[:, 1:3], rtol=1e-6)
+
+
+def test_nvt_plj_ermak():
+    """examples/NVT/ermak.gms: same gas under Ermak (gamma=10/ps, 300 K)."""
+    r, ref = _he_ne("nvt")
+    assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
+    np.testing.assert_allclose(r[:, 0], ref[:, 0], atol=2e-8)
+    np.testing.assert_allclose(r[:, 1:4], ref[:, 1:4], rtol=1e-6)
