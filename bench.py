@@ -1,0 +1,383 @@
+"""Benchmark of the GEMS force/neighbour path on B200.
+
+Workload (default): 32000-atom SMA-TB Au bulk (fcc 20^3, a=4.078 A, periodic,
+seeded N(0, 0.02 A) displacements), Ermak Langevin 300 K, gamma=1/ps, dt=2 fs.
+Metric: atom-steps/s (one atom-step = one force evaluation + one integrator
+update for one atom, neighbour rebuilds amortised in).
+
+One bench step = one block of --block MD steps (default 100) run on the
+device through the C ABI (gemsgpu_batch_md_steps).  The L2 is flushed
+(a 256 MiB write) between timed blocks, outside the timed events.
+
+Arms measured in one run:
+  fp64   : the plain FP64 drop-in kernels, one system;
+  mixed  : FP32 pair math with FP64 accumulation, one system;
+  batched: the mixed kernels over --replicas independent 32k-atom replicas
+           (different displacement / noise seeds) packed into one launch.
+`value` is the batched arm; every arm is reported.  `e2e` runs the batched
+arm through the C ABI with host buffers: each block uploads positions and
+velocities from pinned memory and reads positions, velocities and energies
+back.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s on 1 B200 (FP32+FP64-acc vs plain FP64); serve p50/p99 latency"
+UNIT = "atom-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--block", type=int, default=100, help="MD steps per bench step")
+    ap.add_argument("--replicas", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if s[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- workload
+def c2_replica(seed):
+    from gems_b200 import workloads as W
+    return W.smatb_bulk(seed=seed)
+
+
+def make_system(gems, ctx, w, prec, seed):
+    s = gems.System(w["pos"], w["mass"], ctx=ctx)
+    s.set_box(w["L"], (True, True, True))
+    s.set_smatb(*w["smatb"])
+    s.set_skin(w["skin"])
+    s.set_precision(prec)
+    s.set_ermak(w["dt"], w["gamma"], w["temp"], seed=seed)
+    return s
+
+
+def timed_blocks(ctx, torch, systems, block, steps, warmup, flush, ext_stream):
+    """Run warmup + steps blocks of `block` MD steps; returns (ms list, launches)."""
+    for _ in range(warmup):
+        ctx.batch_md_steps(systems, block)
+    torch.cuda.synchronize()
+    times = []
+    l0 = ctx.launches()
+    for _ in range(steps):
+        flush.add_(1.0)  # > L2, on torch's stream
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext_stream)
+        ctx.batch_md_steps(systems, block)
+        e1.record(ext_stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times, ctx.launches() - l0
+
+
+def timed_e2e(ctx, torch, systems, block, steps, warmup, flush, ext_stream):
+    """Same blocks through the C ABI with host buffers (pinned), H2D of
+    positions + velocities and D2H of positions, velocities and energies inside
+    the timed region."""
+    n = sum(s.n for s in systems)
+    host = []
+    for s in systems:
+        p = torch.empty(3 * s.n, dtype=torch.float64).pin_memory()
+        v = torch.empty(3 * s.n, dtype=torch.float64).pin_memory()
+        p.numpy()[:] = s.pos.ravel()
+        v.numpy()[:] = s.vel.ravel()
+        host.append((p, v))
+
+    def one():
+        for s, (p, v) in zip(systems, host):
+            s.set_pos(p.numpy())
+            s.set_vel(v.numpy())
+        ctx.batch_md_steps(systems, block)
+        for s, (p, v) in zip(systems, host):
+            p.numpy()[:] = s.pos.ravel()
+            v.numpy()[:] = s.vel.ravel()
+        return ctx.batch_energy(systems)
+
+    for _ in range(warmup):
+        one()
+    times = []
+    for _ in range(steps):
+        flush.add_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext_stream)
+        one()
+        e1.record(ext_stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    h2d = 2 * 24 * n
+    d2h = 2 * 24 * n + 24 * len(systems)
+    return times, h2d, d2h
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(seconds):
+    """The FP64 OpenMP restatement (oracle port) on all host cores: C2 sample."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    w = c2_replica(2)
+    s = O.System(w["pos"], w["mass"])
+    s.set_box(w["L"], (True, True, True))
+    s.set_smatb(*w["smatb"])
+    s.set_skin(w["skin"])
+    s.set_ermak(w["dt"], w["gamma"], w["temp"], O.Rng(123456))
+    s.interact()
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        s.stepa()
+        s.interact()
+        s.stepb()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and steps >= 3:
+            break
+    return {"value": s.n * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d MD steps of the 32000-atom SMA-TB Ermak workload (FP64 OpenMP restatement)" % steps}
+
+
+def run_reference(args):
+    """The reference's CPU path (the FP64 OpenMP restatement: no Fortran
+    compiler exists to build the reference itself), on this config."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    w = c2_replica(2)
+    s = O.System(w["pos"], w["mass"])
+    s.set_box(w["L"], (True, True, True))
+    s.set_smatb(*w["smatb"])
+    s.set_skin(w["skin"])
+    s.set_ermak(w["dt"], w["gamma"], w["temp"], O.Rng(123456))
+    s.interact()
+    per = max(1, min(args.block, 5))   # bounded sample per bench step
+
+    def blk():
+        for _ in range(per):
+            s.stepa()
+            s.interact()
+            s.stepb()
+
+    for _ in range(args.warmup):
+        blk()
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        blk()
+        ts.append(time.perf_counter() - t0)
+    tot = sum(ts)
+    val = s.n * per * args.steps / tot
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "smatb_au_bulk_32000 (fcc 20^3, Ermak 300 K, dt 2 fs)",
+                       "md_steps_per_bench_step": per, "parallelism": "openmp"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d blocks of %d MD steps, 32000 atoms" % (args.steps, per)},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import gems_b200 as gems
+
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    ctx = gems.Context(device=dev)
+    ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+    blk = args.block
+    arms = {}
+    # --- single-system arms
+    w = c2_replica(2 + 1000 * rank)
+    for name, prec in (("fp64", gems.PREC_FP64), ("mixed", gems.PREC_MIXED)):
+        s = make_system(gems, ctx, w, prec, seed=7 + rank)
+        s.interact()
+        if dist:
+            dist.barrier()
+        ts, nl = timed_blocks(ctx, torch, [s], blk, args.steps, args.warmup, flush, ext)
+        arms[name] = {"value": s.n * blk * len(ts) / (sum(ts) * 1e-3), "ms_per_block": sum(ts) / len(ts),
+                      "atoms": s.n, "launches": nl}
+        if name == "mixed":
+            kern = s.time_kernels(50)
+            mixed_sys = s
+        else:
+            kern64 = s.time_kernels(50)
+            s.destroy()
+    # --- batched arm: replicas in one launch
+    reps = [make_system(gems, ctx, c2_replica(100 + k + 1000 * rank), gems.PREC_MIXED, seed=100 + k)
+            for k in range(args.replicas)]
+    for s in reps:
+        s.interact()
+    clocks = Clocks(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ts, nl = timed_blocks(ctx, torch, reps, blk, args.steps, args.warmup, flush, ext)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    natoms = sum(s.n for s in reps)
+    tot_ms = sum(ts)
+    if dist:
+        t = torch.tensor([tot_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    value = world * natoms * blk * len(ts) / (tot_ms * 1e-3)
+    arms["batched"] = {"value": natoms * blk * len(ts) / (sum(ts) * 1e-3), "ms_per_block": sum(ts) / len(ts),
+                       "atoms": natoms, "replicas": len(reps), "launches": nl}
+    # --- e2e through the C ABI with host buffers
+    te, h2d, d2h = timed_e2e(ctx, torch, reps, blk, args.steps, args.warmup, flush, ext)
+    e2e_ms = sum(te)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * natoms * blk * len(te) / (e2e_ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    # --- roofline of the dominant kernel (mixed SMA-TB force pass)
+    nbar = 54.0
+    force_bytes = 16 + 4 + 8 + 4 * nbar + 32 + 8      # own int4, eband, band, list, force, epot
+    rho_bytes = 16 + 4 * nbar + 8 + 8 + 4
+    peak, peak_kind = measured_peaks()
+    n1 = mixed_sys.n
+    ach = force_bytes * n1 / (kern[1] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "traffic": None, "kernel": "k_smatb_force_mixed<8>", "peak_source": peak_kind,
+                "bytes_per_launch": force_bytes * n1, "ms_per_launch": kern[1],
+                "rho_kernel": {"ms_per_launch": kern[0], "bytes_per_launch": rho_bytes * n1},
+                "rebuild_ms": kern[2], "fp64_force_ms": kern64[1], "fp64_rho_ms": kern64[0],
+                "note": "working set is L2-resident (about 10 MB per replica)"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / len(ts), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",
+            "config": {"workload": "smatb_au_bulk_32000 x %d replicas (fcc 20^3, a=4.078, Ermak 300 K, "
+                                   "gamma 1/ps, dt 2 fs, skin 1.0)" % len(reps),
+                       "md_steps_per_bench_step": blk, "replicas_per_gpu": len(reps),
+                       "l2": "flushed between timed blocks (256 MiB write)", "parallelism": "replicas"},
+            "arms": arms,
+            "speedup_batched_vs_fp64": arms["batched"]["value"] / arms["fp64"]["value"],
+            "speedup_mixed_vs_fp64": arms["mixed"]["value"] / arms["fp64"]["value"],
+            "e2e": e2e, "roofline": roofline, "clocks": ck, "gpu_launches": nl}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for s in reps:
+        s.destroy()
+    mixed_sys.destroy()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,7 @@
+"""B200 (sm_100a) force/neighbour path of the GEMS molecular simulator.
+
+The compute lives in libgemsgpu.so (hand-written CUDA behind the C ABI of
+include/gemsgpu.h); this package is the thin host-side binding.
+"""
+from .gemsgpu import (Context, GemsGpuError, System, PREC_FP64, PREC_MIXED,  # noqa: F401
+                      UI_EV, EV_UI, KB_UI, lib, declared_symbols)

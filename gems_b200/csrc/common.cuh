@@ -1,0 +1,149 @@
+// common.cuh -- data layout shared by the host runtime and the sm_100a kernels.
+//
+// All systems of a context live in one HBM arena (structure of arrays, one
+// slot per atom).  A system owns a contiguous atom range [off, off+n) and a
+// contiguous cell range; single systems and batches use the same kernels,
+// which walk a block map (block -> system, atom range) so that uneven systems
+// pack into one launch without any block straddling two systems.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gg {
+
+constexpr int MAXT = 4;            // species per system
+constexpr int BLOCK = 256;         // threads per block of every kernel
+constexpr int NSTENCIL = 27;
+
+// 27-cell stencil in the reference's order (src/Neighbour.F90:75-83):
+// 0 centre, 1..13 the upper half, 14..26 the lower half.
+__host__ __device__ inline void stencil(int k, int& dx, int& dy, int& dz) {
+  constexpr signed char m[27][3] = {
+      {0, 0, 0},   {1, 0, 0},   {1, 1, 0},   {0, 1, 0},   {-1, 1, 0},
+      {1, 0, -1},  {1, 1, -1},  {0, 1, -1},  {-1, 1, -1}, {1, 0, 1},
+      {1, 1, 1},   {0, 1, 1},   {-1, 1, 1},  {0, 0, 1},   {-1, 0, 0},
+      {-1, -1, 0}, {0, -1, 0},  {1, -1, 0},  {-1, 0, 1},  {-1, -1, 1},
+      {0, -1, 1},  {1, -1, 1},  {-1, 0, -1}, {-1, -1, -1}, {0, -1, -1},
+      {1, -1, -1}, {0, 0, -1}};
+  dx = m[k][0];
+  dy = m[k][1];
+  dz = m[k][2];
+}
+
+enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
+enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3 };
+enum PREC : int { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+// status bits of a system (SysState::status)
+enum ST : int { ST_OVERFLOW = 1, ST_LOST = 2, ST_NAN = 4 };
+
+// Parameters of one species pair.  LJ (Pairs.F90:198-291):
+//   v[0]=e v[1]=s v[2]=rc v[3]=rc2 v[4]=prc v[5]=frc v[6]=eshift
+//   v[7]=shifted_force (0/1)
+// SMA-TB (TB.F90:106-170):
+//   v[0]=A v[1]=xi v[2]=p v[3]=q v[4]=r0 v[5]=rci v[6]=rce
+//   v[7..9]=b1,b2,b3 v[10..12]=r1,r2,r3 v[13]=on
+struct PairP {
+  double v[16];
+};
+
+// Tersoff 1988: A B l1 l2 beta n c d h R D chi  (A, B in eV)
+struct TersoffP {
+  double A, B, l1, l2, beta, n, c, d, h, R, D, chi;
+};
+
+// Static configuration of a system, written by the host.
+struct SysDev {
+  int off, n;          // atom range in the arena
+  int ff, integ, prec, half;
+  int ntypes, param_off;
+  int boxed, use_cells;
+  int pbc[3];
+  int nc[3];
+  int cell_off, ncell;
+  int use_ext_normals;
+  int fx_per[3];       // fixed-point dim is periodic
+  double L[3], invL[3];
+  double cell[3], inv_cell[3];
+  double rlist2, skin, rcut;
+  double fx_scale[3], fx_origin[3];
+  float fx_inv[3];     // fixed-point unit (A), rounded to float ...
+  float fx_inv_lo[3];  // ... and its rounding remainder (hi + lo = unit)
+  int skin_mic;        // skin test on minimum-image displacements
+  int pad0;
+  // integrator
+  double dt;
+  double cc0, cc1, cc2, sdr, sdv, crv1, crv2, skt;
+  uint64_t seed;
+  double fire_dtmax, fire_fmax;
+  int fire_maxit, pad1;
+  TersoffP ts;
+};
+
+// Dynamic state of a system, written only by kernels (and reset by host).
+struct SysState {
+  int rebuild;      // list must be rebuilt this step
+  int status;       // ST_* bits
+  int ticket;       // last-block counters
+  int ticket2;
+  uint64_t step;    // Ermak / Philox counter
+  int64_t nupd;     // rebuild count
+  double fire_dt, fire_alpha, fire_P;
+  int fire_np, fire_done;
+  int fire_iter, fire_zero;
+  double fmax2;     // max |F|^2 (internal units), FIRE convergence
+  unsigned long long fmax2_bits;
+  int maxnn, pad;
+};
+
+// Block map: block b covers atoms [first[b], end[b]) of system sys[b];
+// sys_blk0[s] / sys_nblk[s] give each system's block range (for last-block
+// merges) -- arrays indexed by system id.
+struct BlockMap {
+  int nblk;
+  int apb;             // atoms per block
+  const int* sys;
+  const int* first;
+  const int* end;
+  const int* sys_blk0;
+  const int* sys_nblk;
+};
+
+// Device arena (passed by value to kernels).
+struct Arena {
+  int64_t cap;          // atom capacity (leading dimension of the list)
+  int lcap;             // neighbour capacity per atom
+  double4* pos;         // x, y, z, -
+  double4* pos_old;     // positions at the last rebuild (test_update)
+  double4* vel;
+  double4* acel;
+  double4* force;
+  double4* vel_v;       // Ermak random velocity kick (ermak_a -> ermak_b)
+  double* epot;         // per atom (internal units)
+  double* band;         // SMA-TB density rho_i
+  double* eband;        // 1/sqrt(rho_i)
+  float* ebandf;        // FP32 copy for the mixed kernels
+  int4* fxp;            // fixed-point positions (x, y, z, type) for mixed
+  double2* minv;        // (1/m, 1/sqrt(m))
+  double* mass;
+  int* type;
+  int* nn;              // neighbours per atom
+  int* list;            // column-major: list[m * cap + i]
+  int* cell_of;
+  int* slot;
+  int* cell_count;      // per cell, zero between rebuilds
+  int* cell_n;
+  int* cell_loc;        // exclusive prefix within a 256-cell chunk
+  int* cell_start;      // absolute start in cell_atoms
+  int* chunk_sum;       // per 256-cell chunk
+  int* cell_atoms;      // atom ids sorted by cell (descending within a cell)
+  double* ext_normals;  // parity-mode Ermak normals (6 per atom)
+  double2* blk_top2;    // per-block top-2 displacement^2
+  double* blk_red;      // per-block partial sums
+  SysDev* sys;
+  SysState* st;
+  PairP* prm;
+  int* any_rebuild;     // OR over the systems of the last step
+};
+
+}  // namespace gg

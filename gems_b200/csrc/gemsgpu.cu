@@ -1,0 +1,1612 @@
+// gemsgpu.cu -- host runtime and C ABI of the B200 force/neighbour path.
+//
+// A context owns one CUDA stream and one HBM arena holding every system's
+// atoms (structure of arrays).  Host records mirror the reference's
+// intergroup / integrate objects; the device keeps all per-step state, so a
+// molecular-dynamics step needs no host round trip (the rebuild decision of
+// test_update is taken on the device).  gemsgpu_md_steps captures a chunk of
+// steps in a CUDA graph and replays it.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/gemsgpu.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace gg;
+
+namespace {
+
+constexpr double kB_ev = 8.617385e-05;  // src/Constants.F90:173
+const double UI_EV = c_ui_ev();
+const double EV_UI_H = 1.0 / c_ui_ev();
+const double kB_ui = kB_ev * EV_UI_H;
+
+struct DevMap {
+  BlockMap m{};
+  int* buf = nullptr;  // device storage of the map arrays
+  int nblk = 0;
+};
+
+struct SysHost {
+  bool alive = false;
+  int off = 0, n = 0, ntypes = 1;
+  int cell_off = 0, cell_cap = 0;
+  int param_off = 0;
+  bool first = true;        // next interact builds the list (update)
+  bool pos_dirty = false;   // positions replaced from the host since the skin test
+  bool has_forces = false;
+  int lanes = 8;            // atoms' list split (autotuned)
+  std::vector<PairP> prm;   // ntypes x ntypes
+  SysDev d{};
+  bool ff_set = false;
+};
+
+struct Graph {
+  cudaGraphExec_t exec = nullptr;
+  uint64_t epoch = 0;
+  int64_t nodes = 0;  // kernel nodes per replay
+};
+
+}  // namespace
+
+struct gemsgpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // arena
+  Arena A{};
+  int64_t acap = 0;   // atoms
+  int64_t ccap = 0;   // cells
+  int scap = 0;       // systems
+  int pcap = 0;       // pair-parameter slots
+  int nblk_cap = 0;   // per-block scratch entries
+  int64_t atoms_used = 0, cells_used = 0;
+  int params_used = 0;
+  std::vector<SysHost> sys;
+  std::vector<std::pair<int64_t, int64_t>> free_atoms, free_cells;
+  uint64_t epoch = 1;  // bumps when device pointers or maps change
+  int64_t launches = 0;  // kernels issued (graph replays add their node count)
+  int64_t pending = 0;   // kernels recorded by the capture in progress
+  std::map<std::string, DevMap> maps;
+  std::map<std::string, Graph> graphs;
+  // pinned scratch for small readbacks
+  double* h_red = nullptr;
+  int h_red_cap = 0;
+  double* d_red = nullptr;
+  int* d_sys = nullptr;
+  int d_sys_cap = 0;
+  SysState* h_st = nullptr;
+  double* stage = nullptr;      // 3 doubles per atom, host <-> device staging
+  int64_t stage_cap = 0;
+  int64_t snap_cap = 0;
+  double4* snap = nullptr;      // pos, vel, acel, force
+  SysState* snap_st = nullptr;
+};
+
+namespace {
+
+int fail(gemsgpu_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CU(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? GEMSGPU_ERR_OOM          \
+                                                       : GEMSGPU_ERR_CUDA,        \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,      \
+                  __LINE__);                                                      \
+  } while (0)
+
+#define CHK(expr)          \
+  do {                     \
+    int r_ = (expr);       \
+    if (r_ != 0) return r_; \
+  } while (0)
+
+template <typename T>
+int dalloc(gemsgpu_ctx* ctx, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  CU(cudaMalloc((void**)p, n * sizeof(T)));
+  return 0;
+}
+
+// grow one device array keeping its first `keep` elements
+template <typename T>
+int dgrow(gemsgpu_ctx* ctx, T** p, size_t keep, size_t n) {
+  T* q = nullptr;
+  CHK(dalloc(ctx, &q, n));
+  if (*p && keep) CU(cudaMemcpyAsync(q, *p, keep * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (*p) {
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaFree(*p));
+  }
+  *p = q;
+  return 0;
+}
+
+void drop_graphs(gemsgpu_ctx* c) {
+  for (auto& kv : c->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  c->graphs.clear();
+}
+
+void drop_maps(gemsgpu_ctx* c) {
+  for (auto& kv : c->maps)
+    if (kv.second.buf) cudaFree(kv.second.buf);
+  c->maps.clear();
+}
+
+void invalidate(gemsgpu_ctx* c) {
+  c->epoch++;
+  drop_graphs(c);
+}
+
+// ------------------------------------------------------------- arena
+int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
+  if (need <= ctx->acap) return 0;
+  int64_t nc = std::max<int64_t>(need, ctx->acap + ctx->acap / 2);
+  nc = (nc + 255) / 256 * 256;
+  int64_t keep = ctx->acap;
+  Arena& A = ctx->A;
+  CHK(dgrow(ctx, &A.pos, keep, nc));
+  CHK(dgrow(ctx, &A.pos_old, keep, nc));
+  CHK(dgrow(ctx, &A.vel, keep, nc));
+  CHK(dgrow(ctx, &A.acel, keep, nc));
+  CHK(dgrow(ctx, &A.force, keep, nc));
+  CHK(dgrow(ctx, &A.vel_v, keep, nc));
+  CHK(dgrow(ctx, &A.epot, keep, nc));
+  CHK(dgrow(ctx, &A.band, keep, nc));
+  CHK(dgrow(ctx, &A.eband, keep, nc));
+  CHK(dgrow(ctx, &A.ebandf, keep, nc));
+  CHK(dgrow(ctx, &A.fxp, keep, nc));
+  CHK(dgrow(ctx, &A.minv, keep, nc));
+  CHK(dgrow(ctx, &A.mass, keep, nc));
+  CHK(dgrow(ctx, &A.type, keep, nc));
+  CHK(dgrow(ctx, &A.nn, keep, nc));
+  CHK(dgrow(ctx, &A.cell_of, keep, nc));
+  CHK(dgrow(ctx, &A.slot, keep, nc));
+  CHK(dgrow(ctx, &A.cell_atoms, keep, nc));
+  CHK(dgrow(ctx, &A.ext_normals, 6 * keep, 6 * nc));
+  // the list's leading dimension is the atom capacity: re-lay it out
+  if (A.lcap > 0) {
+    int* nl = nullptr;
+    CHK(dalloc(ctx, &nl, (size_t)A.lcap * nc));
+    if (A.list && keep)
+      CU(cudaMemcpy2DAsync(nl, nc * sizeof(int), A.list, keep * sizeof(int), keep * sizeof(int),
+                           A.lcap, cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (A.list) CU(cudaFree(A.list));
+    A.list = nl;
+  }
+  ctx->acap = nc;
+  A.cap = nc;
+  invalidate(ctx);
+  return 0;
+}
+
+int grow_list(gemsgpu_ctx* ctx, int lcap) {
+  Arena& A = ctx->A;
+  if (lcap <= A.lcap && A.list) return 0;
+  lcap = (lcap + 7) / 8 * 8;
+  int* nl = nullptr;
+  CHK(dalloc(ctx, &nl, (size_t)lcap * std::max<int64_t>(ctx->acap, 1)));
+  CU(cudaStreamSynchronize(ctx->stream));
+  if (A.list) CU(cudaFree(A.list));
+  A.list = nl;
+  A.lcap = lcap;
+  size_t smem = (size_t)LIST_ATOMS * lcap * sizeof(int);
+  if (smem > 48 * 1024) {
+    if (smem > 200 * 1024) return fail(ctx, GEMSGPU_ERR_ARG, "neighbour capacity %d too large", lcap);
+    CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  invalidate(ctx);
+  return 0;
+}
+
+int grow_cells(gemsgpu_ctx* ctx, int64_t need) {
+  if (need <= ctx->ccap) return 0;
+  int64_t nc = std::max<int64_t>(need, ctx->ccap + ctx->ccap / 2);
+  nc = (nc + 255) / 256 * 256;
+  Arena& A = ctx->A;
+  int64_t keep = ctx->ccap;
+  CHK(dgrow(ctx, &A.cell_count, keep, nc));
+  if (keep < nc) CU(cudaMemsetAsync(A.cell_count + keep, 0, (nc - keep) * sizeof(int), ctx->stream));
+  CHK(dgrow(ctx, &A.cell_n, keep, nc));
+  CHK(dgrow(ctx, &A.cell_loc, keep, nc));
+  CHK(dgrow(ctx, &A.cell_start, keep, nc));
+  CHK(dgrow(ctx, &A.chunk_sum, keep / 256, nc / 256));
+  ctx->ccap = nc;
+  invalidate(ctx);
+  return 0;
+}
+
+int grow_systems(gemsgpu_ctx* ctx, int need) {
+  if (need <= ctx->scap) return 0;
+  int nc = std::max(need, std::max(16, ctx->scap * 2));
+  Arena& A = ctx->A;
+  CHK(dgrow(ctx, &A.sys, ctx->scap, nc));
+  CHK(dgrow(ctx, &A.st, ctx->scap, nc));
+  CU(cudaMemsetAsync(A.st + ctx->scap, 0, (nc - ctx->scap) * sizeof(SysState), ctx->stream));
+  if (ctx->h_st) cudaFreeHost(ctx->h_st);
+  CU(cudaMallocHost((void**)&ctx->h_st, nc * sizeof(SysState)));
+  if (ctx->snap_st) cudaFree(ctx->snap_st);
+  CHK(dalloc(ctx, &ctx->snap_st, nc));
+  ctx->scap = nc;
+  invalidate(ctx);
+  return 0;
+}
+
+int grow_params(gemsgpu_ctx* ctx, int need) {
+  if (need <= ctx->pcap) return 0;
+  int nc = std::max(need, std::max(64, ctx->pcap * 2));
+  CHK(dgrow(ctx, &ctx->A.prm, ctx->pcap, nc));
+  ctx->pcap = nc;
+  invalidate(ctx);
+  return 0;
+}
+
+int grow_blocks(gemsgpu_ctx* ctx, int nblk) {
+  if (nblk <= ctx->nblk_cap) return 0;
+  int nc = std::max(nblk, ctx->nblk_cap * 2);
+  CHK(dgrow(ctx, &ctx->A.blk_top2, 0, nc));
+  CHK(dgrow(ctx, &ctx->A.blk_red, 0, 2 * (size_t)nc));
+  ctx->nblk_cap = nc;
+  invalidate(ctx);
+  return 0;
+}
+
+// first-fit range allocation with a bump pointer
+int64_t take_range(std::vector<std::pair<int64_t, int64_t>>& fr, int64_t& used, int64_t n,
+                   int64_t align) {
+  for (size_t k = 0; k < fr.size(); k++) {
+    int64_t b = (fr[k].first + align - 1) / align * align;
+    if (b + n <= fr[k].second) {
+      int64_t e = fr[k].second;
+      int64_t a0 = fr[k].first;
+      fr.erase(fr.begin() + k);
+      if (a0 < b) fr.push_back({a0, b});
+      if (b + n < e) fr.push_back({b + n, e});
+      return b;
+    }
+  }
+  int64_t b = (used + align - 1) / align * align;
+  used = b + n;
+  return b;
+}
+
+// ------------------------------------------------------------- derived config
+void derive(gemsgpu_ctx* ctx, SysHost& h) {
+  SysDev& d = h.d;
+  d.off = h.off;
+  d.n = h.n;
+  d.ntypes = h.ntypes;
+  d.param_off = h.param_off;
+  // rcut: max cut-off over the species pairs (intergroup rcut)
+  double rc = 0.0;
+  if (d.ff == FF_LJ)
+    for (auto& p : h.prm) rc = std::max(rc, p.v[2]);
+  if (d.ff == FF_SMATB)
+    for (auto& p : h.prm)
+      if (p.v[13] != 0.0) rc = std::max(rc, p.v[6]);
+  if (d.ff == FF_TERSOFF) rc = d.ts.R + d.ts.D;
+  d.rcut = rc;
+  double rl = rc + d.skin;
+  d.rlist2 = rl * rl;
+  // intergroup_setcells (src/Neighbour.F90:587-664)
+  d.use_cells = 0;
+  for (int k = 0; k < 3; k++) {
+    d.nc[k] = 1;
+    d.invL[k] = d.boxed ? 1.0 / d.L[k] : 0.0;
+  }
+  if (d.boxed && rl > 0.0) {
+    bool any4 = false;
+    int nc[3];
+    for (int k = 0; k < 3; k++) {
+      nc[k] = (int)(d.L[k] / rl);
+      if (nc[k] >= 4) any4 = true;
+    }
+    if (any4) {
+      d.use_cells = 1;
+      for (int k = 0; k < 3; k++) {
+        d.nc[k] = nc[k];
+        d.cell[k] = d.L[k] / nc[k];
+        d.inv_cell[k] = 1.0 / d.cell[k];
+      }
+    }
+  }
+  d.ncell = d.use_cells ? d.nc[0] * d.nc[1] * d.nc[2] : 0;
+  // fixed-point frame of the mixed kernels
+  for (int k = 0; k < 3; k++) {
+    bool per = d.boxed && d.pbc[k];
+    d.fx_per[k] = per ? 1 : 0;
+    if (per) {
+      d.fx_scale[k] = 4294967296.0 / d.L[k];
+      double u = d.L[k] / 4294967296.0;
+      d.fx_inv[k] = (float)u;
+      d.fx_inv_lo[k] = (float)(u - (double)d.fx_inv[k]);
+      d.fx_origin[k] = 0.0;
+    } else {
+      d.fx_scale[k] = 4194304.0;  // 2^22 per Angstrom
+      d.fx_inv[k] = (float)(1.0 / 4194304.0);
+      d.fx_inv_lo[k] = 0.0f;
+      d.fx_origin[k] = d.boxed ? 0.5 * d.L[k] : d.fx_origin[k];
+    }
+  }
+}
+
+int alloc_cells(gemsgpu_ctx* ctx, SysHost& h) {
+  int need = h.d.use_cells ? h.d.ncell : 0;
+  if (need <= h.cell_cap) {
+    h.d.cell_off = h.cell_off;
+    return 0;
+  }
+  if (h.cell_cap > 0) ctx->free_cells.push_back({h.cell_off, h.cell_off + h.cell_cap});
+  int64_t cap = (need + 255) / 256 * 256;
+  int64_t off = take_range(ctx->free_cells, ctx->cells_used, cap, 256);
+  CHK(grow_cells(ctx, off + cap));
+  h.cell_off = (int)off;
+  h.cell_cap = (int)cap;
+  h.d.cell_off = h.cell_off;
+  invalidate(ctx);
+  return 0;
+}
+
+int push_sys(gemsgpu_ctx* ctx, int s) {
+  SysHost& h = ctx->sys[s];
+  derive(ctx, h);
+  CHK(alloc_cells(ctx, h));
+  CU(cudaMemcpyAsync(ctx->A.sys + s, &h.d, sizeof(SysDev), cudaMemcpyHostToDevice, ctx->stream));
+  if (!h.prm.empty())
+    CU(cudaMemcpyAsync(ctx->A.prm + h.param_off, h.prm.data(), h.prm.size() * sizeof(PairP),
+                       cudaMemcpyHostToDevice, ctx->stream));
+  return 0;
+}
+
+int check_sys(gemsgpu_ctx* ctx, int s) {
+  if (!ctx) return GEMSGPU_ERR_ARG;
+  if (s < 0 || s >= (int)ctx->sys.size() || !ctx->sys[s].alive)
+    return fail(ctx, GEMSGPU_ERR_ARG, "unknown system %d", s);
+  return 0;
+}
+
+// ------------------------------------------------------------- block maps
+// kind 0: atoms, `apb` atoms per block; kind 1: cells, 256 cells per block.
+int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, BlockMap* out) {
+  std::string key = std::to_string(kind) + ":" + std::to_string(apb) + ":";
+  for (int s : ss) key += std::to_string(s) + ",";
+  auto it = ctx->maps.find(key);
+  if (it != ctx->maps.end()) {
+    *out = it->second.m;
+    return 0;
+  }
+  std::vector<int> bs, bf, be;
+  std::vector<int> blk0(ctx->scap, 0), nblk(ctx->scap, 0);
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    int lo, hi;
+    if (kind == 0) {
+      lo = h.off;
+      hi = h.off + h.n;
+    } else {
+      if (!h.d.use_cells) continue;
+      lo = h.cell_off;
+      hi = h.cell_off + h.d.ncell;
+    }
+    blk0[s] = (int)bs.size();
+    for (int a = lo; a < hi; a += apb) {
+      bs.push_back(s);
+      bf.push_back(a);
+      be.push_back(std::min(hi, a + apb));
+    }
+    nblk[s] = (int)bs.size() - blk0[s];
+  }
+  int nb = (int)bs.size();
+  CHK(grow_blocks(ctx, std::max(nb, 1)));
+  std::vector<int> all;
+  all.insert(all.end(), bs.begin(), bs.end());
+  all.insert(all.end(), bf.begin(), bf.end());
+  all.insert(all.end(), be.begin(), be.end());
+  all.insert(all.end(), blk0.begin(), blk0.end());
+  all.insert(all.end(), nblk.begin(), nblk.end());
+  DevMap dm;
+  CHK(dalloc(ctx, &dm.buf, all.size()));
+  CU(cudaMemcpyAsync(dm.buf, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  dm.m.nblk = nb;
+  dm.m.apb = apb;
+  dm.m.sys = dm.buf;
+  dm.m.first = dm.buf + nb;
+  dm.m.end = dm.buf + 2 * nb;
+  dm.m.sys_blk0 = dm.buf + 3 * nb;
+  dm.m.sys_nblk = dm.buf + 3 * nb + ctx->scap;
+  dm.nblk = nb;
+  ctx->maps[key] = dm;
+  *out = dm.m;
+  return 0;
+}
+
+int sys_array(gemsgpu_ctx* ctx, const std::vector<int>& ss, const int** out) {
+  std::string key = "S:";
+  for (int s : ss) key += std::to_string(s) + ",";
+  auto it = ctx->maps.find(key);
+  if (it == ctx->maps.end()) {
+    DevMap dm;
+    CHK(dalloc(ctx, &dm.buf, ss.size()));
+    CU(cudaMemcpyAsync(dm.buf, ss.data(), ss.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    dm.nblk = (int)ss.size();
+    it = ctx->maps.emplace(key, dm).first;
+  }
+  *out = it->second.buf;
+  return 0;
+}
+
+// ------------------------------------------------------------- launches
+template <int K>
+void launch_forces_k(gemsgpu_ctx* ctx, int ff, int prec, const BlockMap& m) {
+  cudaStream_t st = ctx->stream;
+  const Arena& A = ctx->A;
+  if (m.nblk == 0) return;
+  if (ff == FF_SMATB) {
+    if (prec == PREC_MIXED) {
+      k_smatb_rho_mixed<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+      k_smatb_force_mixed<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+    } else {
+      k_smatb_rho_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+      k_smatb_force_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+    }
+  } else if (ff == FF_LJ) {
+    if (prec == PREC_MIXED) {
+      k_lj_mixed<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+    } else {
+      k_lj_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+    }
+  }
+}
+
+// group systems by (ff, prec, lanes) and launch the force kernels
+int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no force field", s);
+    if (h.d.half) return fail(ctx, GEMSGPU_ERR_STATE, "system %d: force kernels need full lists", s);
+    int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
+    groups[{h.d.ff, h.d.prec, K}].push_back(s);
+  }
+  for (auto& kv : groups) {
+    int ff = std::get<0>(kv.first), prec = std::get<1>(kv.first), K = std::get<2>(kv.first);
+    BlockMap m;
+    if (ff == FF_TERSOFF) {
+      CHK(get_map(ctx, kv.second, BLOCK, 0, &m));
+      k_zero_force<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+      if (prec == PREC_MIXED) {
+        k_tersoff<float, true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+      } else {
+        k_tersoff<double, false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+      }
+      continue;
+    }
+    CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
+    switch (K) {
+      case 1: launch_forces_k<1>(ctx, ff, prec, m); break;
+      case 2: launch_forces_k<2>(ctx, ff, prec, m); break;
+      case 4: launch_forces_k<4>(ctx, ff, prec, m); break;
+      case 8: launch_forces_k<8>(ctx, ff, prec, m); break;
+      case 16: launch_forces_k<16>(ctx, ff, prec, m); break;
+      default: launch_forces_k<32>(ctx, ff, prec, m); break;
+    }
+  }
+  CU(cudaGetLastError());
+  return 0;
+}
+
+// the rebuild chain; every kernel returns at once for systems whose
+// rebuild flag is clear, so the chain can sit in a captured step.
+int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  BlockMap ma, mc, mw;
+  const int* sa;
+  CHK(get_map(ctx, ss, BLOCK, 0, &ma));
+  CHK(get_map(ctx, ss, 256, 1, &mc));
+  CHK(get_map(ctx, ss, LIST_ATOMS, 0, &mw));
+  CHK(sys_array(ctx, ss, &sa));
+  cudaStream_t st = ctx->stream;
+  const Arena& A = ctx->A;
+  bool cells = mc.nblk > 0;
+  bool n2 = false;
+  for (int s : ss) n2 |= !ctx->sys[s].d.use_cells;
+  if (cells) {
+    k_bin<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+    k_scan1<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
+    k_scan2<<<(int)ss.size(), BLOCK, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
+    k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+    k_sort_cells<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
+    k_list_cells<<<mw.nblk, BLOCK, LIST_ATOMS * A.lcap * sizeof(int), st>>>(A, mw); ++ctx->launches;
+  }
+  if (n2) {
+    k_list_n2<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  }
+  k_count_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  BlockMap ma;
+  CHK(get_map(ctx, ss, BLOCK, 0, &ma));
+  k_step_a<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int launch_step_b(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  BlockMap ma;
+  CHK(get_map(ctx, ss, BLOCK, 0, &ma));
+  k_step_b<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int read_states(gemsgpu_ctx* ctx) {
+  CU(cudaMemcpyAsync(ctx->h_st, ctx->A.st, ctx->scap * sizeof(SysState), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int clear_status(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  for (int s : ss) {
+    CU(cudaMemsetAsync(&ctx->A.st[s].status, 0, sizeof(int), ctx->stream));
+    CU(cudaMemsetAsync(&ctx->A.st[s].maxnn, 0, sizeof(int), ctx->stream));
+  }
+  return 0;
+}
+
+int status_error(gemsgpu_ctx* ctx, int s, int st) {
+  if (st & ST_NAN) return fail(ctx, GEMSGPU_ERR_NAN, "system %d: non-finite positions", s);
+  if (st & ST_LOST)
+    return fail(ctx, GEMSGPU_ERR_LOST, "system %d: atom outside the cell grid / fixed-point range", s);
+  if (st & ST_OVERFLOW) return fail(ctx, GEMSGPU_ERR_OVERFLOW, "system %d: neighbour list overflow", s);
+  return 0;
+}
+
+// neighbour capacity estimate: 1.5x the ideal count at the system's density
+int estimate_cap(const SysHost& h) {
+  const SysDev& d = h.d;
+  double rl = std::sqrt(d.rlist2);
+  double vol;
+  if (d.boxed)
+    vol = d.L[0] * d.L[1] * d.L[2];
+  else
+    vol = h.n / 0.06;  // close-packed metals ~0.06 atoms / A^3
+  double dens = h.n / std::max(vol, 1e-6);
+  dens = std::max(dens, 0.06);
+  double nb = 4.18879 * rl * rl * rl * dens;
+  int cap = (int)(1.5 * nb) + 16;
+  cap = std::min(cap, std::max(h.n, 16));
+  return std::max(cap, 16);
+}
+
+// interact (src/Interaction.f90:135-241) for a set of systems, host-driven:
+// rebuild if flagged (heal overflow by growing the list), then forces.
+int interact_group(gemsgpu_ctx* ctx, const std::vector<int>& ss, bool sync_check) {
+  std::vector<int> first, dirty;
+  int need = 0;
+  for (int s : ss) {
+    SysHost& h = ctx->sys[s];
+    if (h.first) first.push_back(s);
+    else if (h.pos_dirty) dirty.push_back(s);
+    need = std::max(need, estimate_cap(h));
+  }
+  if (ctx->A.lcap < need) CHK(grow_list(ctx, need));
+  CHK(clear_status(ctx, ss));
+  if (!first.empty()) {
+    const int* sa;
+    CHK(sys_array(ctx, first, &sa));
+    k_force_rebuild<<<((int)first.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa,
+                                                                                 (int)first.size()); ++ctx->launches;
+  }
+  if (!dirty.empty()) {
+    BlockMap m;
+    CHK(get_map(ctx, dirty, BLOCK, 0, &m));
+    k_skin<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  }
+  CHK(launch_rebuild(ctx, ss));
+  if (sync_check) {
+    CHK(read_states(ctx));
+    int grow = 0;
+    for (int s : ss) {
+      const SysState& st = ctx->h_st[s];
+      if (st.status & ST_OVERFLOW) grow = std::max(grow, st.maxnn);
+    }
+    if (grow > 0) {
+      CHK(grow_list(ctx, grow + grow / 4 + 8));
+      CHK(clear_status(ctx, ss));
+      const int* sa;
+      CHK(sys_array(ctx, ss, &sa));
+      k_force_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa,
+                                                                              (int)ss.size()); ++ctx->launches;
+      CHK(launch_rebuild(ctx, ss));
+      CHK(read_states(ctx));
+    }
+    for (int s : ss) CHK(status_error(ctx, s, ctx->h_st[s].status & ~0));
+  }
+  CHK(launch_forces(ctx, ss));
+  for (int s : ss) {
+    SysHost& h = ctx->sys[s];
+    h.first = false;
+    h.pos_dirty = false;
+    h.has_forces = true;
+  }
+  return 0;
+}
+
+int reduce_sys(gemsgpu_ctx* ctx, const std::vector<int>& ss, std::vector<double>& out) {
+  int n = (int)ss.size();
+  if (n > ctx->h_red_cap) {
+    if (ctx->h_red) cudaFreeHost(ctx->h_red);
+    if (ctx->d_red) cudaFree(ctx->d_red);
+    CU(cudaMallocHost((void**)&ctx->h_red, 4 * sizeof(double) * n));
+    CHK(dalloc(ctx, &ctx->d_red, 4 * (size_t)n));
+    ctx->h_red_cap = n;
+  }
+  const int* sa;
+  CHK(sys_array(ctx, ss, &sa));
+  k_sys_reduce<<<n, BLOCK, 0, ctx->stream>>>(ctx->A, sa, n, ctx->d_red); ++ctx->launches;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(ctx->h_red, ctx->d_red, 4 * sizeof(double) * n, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  out.assign(ctx->h_red, ctx->h_red + 4 * n);
+  return 0;
+}
+
+// one captured MD step for a set of systems
+int record_step(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  CHK(launch_step_a(ctx, ss));
+  CHK(launch_rebuild(ctx, ss));
+  CHK(launch_forces(ctx, ss));
+  CHK(launch_step_b(ctx, ss));
+  return 0;
+}
+
+int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGraphExec_t* out) {
+  std::string key = "G" + std::to_string(nsteps) + ":";
+  for (int s : ss) key += std::to_string(s) + ",";
+  auto it = ctx->graphs.find(key);
+  if (it != ctx->graphs.end() && it->second.epoch == ctx->epoch) {
+    *out = it->second.exec;
+    return 0;
+  }
+  // make sure every map exists before capture (map creation copies memory)
+  {
+    BlockMap m;
+    const int* sa;
+    CHK(get_map(ctx, ss, BLOCK, 0, &m));
+    CHK(get_map(ctx, ss, 256, 1, &m));
+    CHK(get_map(ctx, ss, LIST_ATOMS, 0, &m));
+    CHK(sys_array(ctx, ss, &sa));
+    std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+    for (int s : ss) {
+      const SysHost& h = ctx->sys[s];
+      int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
+      groups[{h.d.ff, h.d.prec, K}].push_back(s);
+    }
+    for (auto& kv : groups) {
+      int K = std::get<2>(kv.first);
+      CHK(get_map(ctx, kv.second, std::get<0>(kv.first) == FF_TERSOFF ? BLOCK : BLOCK / K, 0, &m));
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+  }
+  cudaGraph_t g = nullptr;
+  const int64_t before = ctx->launches;
+  CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  for (int k = 0; k < nsteps && rc == 0; k++) rc = record_step(ctx, ss);
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  const int64_t nodes = ctx->launches - before;
+  ctx->launches = before;  // captured, not executed
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(ctx, GEMSGPU_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  cudaGraphExec_t ex = nullptr;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(ctx, GEMSGPU_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  if (it != ctx->graphs.end() && it->second.exec) cudaGraphExecDestroy(it->second.exec);
+  ctx->graphs[key] = Graph{ex, ctx->epoch, nodes};
+  *out = ex;
+  return 0;
+}
+
+int launch_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps) {
+  cudaGraphExec_t ex;
+  CHK(get_graph(ctx, ss, nsteps, &ex));
+  CU(cudaGraphLaunch(ex, ctx->stream));
+  std::string key = "G" + std::to_string(nsteps) + ":";
+  for (int s : ss) key += std::to_string(s) + ",";
+  ctx->launches += ctx->graphs[key].nodes;
+  return 0;
+}
+
+int snapshot(gemsgpu_ctx* ctx, bool restore) {
+  int64_t n = ctx->acap;
+  if (!restore && ctx->snap_cap < n) {
+    if (ctx->snap) cudaFree(ctx->snap);
+    CHK(dalloc(ctx, &ctx->snap, 4 * (size_t)n));
+    ctx->snap_cap = n;
+  }
+  Arena& A = ctx->A;
+  double4* arr[4] = {A.pos, A.vel, A.acel, A.force};
+  for (int k = 0; k < 4; k++) {
+    if (restore)
+      CU(cudaMemcpyAsync(arr[k], ctx->snap + k * n, n * sizeof(double4), cudaMemcpyDeviceToDevice,
+                         ctx->stream));
+    else
+      CU(cudaMemcpyAsync(ctx->snap + k * n, arr[k], n * sizeof(double4), cudaMemcpyDeviceToDevice,
+                         ctx->stream));
+  }
+  if (restore) {
+    CU(cudaMemcpyAsync(A.st, ctx->snap_st, ctx->scap * sizeof(SysState), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+  } else {
+    CU(cudaMemcpyAsync(ctx->snap_st, A.st, ctx->scap * sizeof(SysState), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+  }
+  return 0;
+}
+
+constexpr int CHUNK = 50;
+
+// dinamic (src/Programs.f90:114-167) for a set of systems, device-resident:
+// chunks of CHUNK captured steps; after each chunk the states are checked,
+// and a chunk that overflowed a list is undone, the list grown and redone.
+int md_group(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps) {
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    if (h.d.integ == IT_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no integrator", s);
+  }
+  bool need_first = false;
+  for (int s : ss) need_first |= ctx->sys[s].first || ctx->sys[s].pos_dirty || !ctx->sys[s].has_forces;
+  if (need_first) CHK(interact_group(ctx, ss, true));
+  int done = 0;
+  int retries = 0;
+  while (done < nsteps) {
+    int k = std::min(CHUNK, nsteps - done);
+    CHK(snapshot(ctx, false));
+    CHK(clear_status(ctx, ss));
+    CHK(launch_graph(ctx, ss, k));
+    CHK(read_states(ctx));
+    int grow = 0, bad = 0, bads = -1;
+    for (int s : ss) {
+      int st = ctx->h_st[s].status;
+      if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
+      if (st & (ST_NAN | ST_LOST)) { bad = st; bads = s; }
+    }
+    if (bad) return status_error(ctx, bads, bad);
+    if (grow > 0) {
+      if (++retries > 4) return fail(ctx, GEMSGPU_ERR_OVERFLOW, "neighbour list keeps overflowing");
+      CHK(snapshot(ctx, true));
+      CHK(grow_list(ctx, grow + grow / 4 + 8));
+      const int* sa;
+      CHK(sys_array(ctx, ss, &sa));
+      k_force_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size()); ++ctx->launches;
+      CHK(clear_status(ctx, ss));
+      CHK(launch_rebuild(ctx, ss));
+      CHK(launch_forces(ctx, ss));
+      continue;
+    }
+    done += k;
+  }
+  return 0;
+}
+
+int ensure_stage(gemsgpu_ctx* ctx, int64_t n) {
+  if (ctx->stage_cap >= n) return 0;
+  if (ctx->stage) CU(cudaFree(ctx->stage));
+  ctx->stage = nullptr;
+  CHK(dalloc(ctx, &ctx->stage, 3 * (size_t)n));
+  ctx->stage_cap = n;
+  return 0;
+}
+
+// host interleaved xyz -> arena double4 slots (one H2D copy + a repack kernel)
+int h2d_xyz(gemsgpu_ctx* ctx, const double* src, double4* dst, int n) {
+  CHK(ensure_stage(ctx, n));
+  CU(cudaMemcpyAsync(ctx->stage, src, (size_t)3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  k_unpack3<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->stage, dst, n); ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+// arena double4 slots -> host interleaved xyz (a pack kernel + one D2H copy)
+int d2h_xyz(gemsgpu_ctx* ctx, const double4* src, double* dst, int n) {
+  CHK(ensure_stage(ctx, n));
+  k_pack3<<<(n + 255) / 256, 256, 0, ctx->stream>>>(src, ctx->stage, n); ++ctx->launches;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(dst, ctx->stage, (size_t)3 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  return 0;
+}
+
+void copy_interleaved_to_d4(const double* src, std::vector<double4>& dst, int n) {
+  dst.resize(n);
+  for (int i = 0; i < n; i++) dst[i] = make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0);
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+extern "C" {
+
+const char* gemsgpu_version(void) { return "gemsgpu 0.1 (sm_100a)"; }
+
+int gemsgpu_create(int device, int64_t max_atoms, int max_systems, gemsgpu_ctx** out) {
+  if (!out) return GEMSGPU_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GEMSGPU_ERR_NODEV;
+  if (device < 0 || device >= ndev) return GEMSGPU_ERR_ARG;
+  auto* ctx = new gemsgpu_ctx();
+  ctx->device = device;
+  int rc = 0;
+  do {
+    if (cudaSetDevice(device) != cudaSuccess) { rc = GEMSGPU_ERR_CUDA; break; }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      rc = GEMSGPU_ERR_CUDA;
+      break;
+    }
+    if ((rc = grow_systems(ctx, std::max(max_systems, 16)))) break;
+    if ((rc = grow_atoms(ctx, std::max<int64_t>(max_atoms, 1024)))) break;
+    if ((rc = grow_cells(ctx, 4096))) break;
+    if ((rc = grow_params(ctx, 64))) break;
+    if ((rc = grow_blocks(ctx, 1024))) break;
+    if ((rc = dalloc(ctx, &ctx->A.any_rebuild, 1))) break;
+    cudaMemsetAsync(ctx->A.any_rebuild, 0, sizeof(int), ctx->stream);
+  } while (0);
+  if (rc) {
+    gemsgpu_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return 0;
+}
+
+int gemsgpu_destroy(gemsgpu_ctx* ctx) {
+  if (!ctx) return GEMSGPU_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graphs(ctx);
+  drop_maps(ctx);
+  Arena& A = ctx->A;
+  void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.epot, A.band, A.eband,
+                  A.ebandf, A.fxp, A.minv, A.mass, A.type, A.nn, A.list, A.cell_of, A.slot,
+                  A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
+                  A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild,
+                  ctx->d_red, ctx->snap, ctx->snap_st, ctx->d_sys};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  if (ctx->h_st) cudaFreeHost(ctx->h_st);
+  if (ctx->stage) cudaFree(ctx->stage);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return 0;
+}
+
+int gemsgpu_last_error(gemsgpu_ctx* ctx, char* buf, int len) {
+  if (!ctx || !buf || len <= 0) return GEMSGPU_ERR_ARG;
+  snprintf(buf, len, "%s", ctx->err.c_str());
+  return 0;
+}
+
+int gemsgpu_system_create(gemsgpu_ctx* ctx, int natoms, int ntypes, int* sys) {
+  if (!ctx || !sys || natoms <= 0 || ntypes <= 0 || ntypes > MAXT)
+    return fail(ctx, GEMSGPU_ERR_ARG, "system_create: natoms>0 and 1<=ntypes<=%d", MAXT);
+  cudaSetDevice(ctx->device);
+  int s = -1;
+  for (size_t k = 0; k < ctx->sys.size(); k++)
+    if (!ctx->sys[k].alive) { s = (int)k; break; }
+  if (s < 0) {
+    s = (int)ctx->sys.size();
+    ctx->sys.emplace_back();
+  }
+  CHK(grow_systems(ctx, s + 1));
+  SysHost& h = ctx->sys[s];
+  h = SysHost();
+  h.alive = true;
+  h.n = natoms;
+  h.ntypes = ntypes;
+  int64_t off = take_range(ctx->free_atoms, ctx->atoms_used, natoms, 32);
+  CHK(grow_atoms(ctx, off + natoms));
+  h.off = (int)off;
+  h.param_off = ctx->params_used;
+  ctx->params_used += ntypes * ntypes;
+  CHK(grow_params(ctx, ctx->params_used));
+  h.prm.assign(ntypes * ntypes, PairP{});
+  h.d = SysDev{};
+  h.d.skin = 1.0;
+  h.d.skin_mic = 1;
+  h.d.dt = 0.002;
+  h.d.fx_origin[0] = h.d.fx_origin[1] = h.d.fx_origin[2] = 0.0;
+  SysState z{};
+  CU(cudaMemcpyAsync(ctx->A.st + s, &z, sizeof(z), cudaMemcpyHostToDevice, ctx->stream));
+  CHK(push_sys(ctx, s));
+  invalidate(ctx);
+  drop_maps(ctx);
+  *sys = s;
+  return 0;
+}
+
+int gemsgpu_system_destroy(gemsgpu_ctx* ctx, int sys) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  ctx->free_atoms.push_back({h.off, h.off + h.n});
+  if (h.cell_cap) ctx->free_cells.push_back({h.cell_off, h.cell_off + h.cell_cap});
+  h.alive = false;
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_upload(gemsgpu_ctx* ctx, int sys, const double* pos, const double* vel,
+                   const double* mass, const int* type) {
+  CHK(check_sys(ctx, sys));
+  if (!pos || !mass) return fail(ctx, GEMSGPU_ERR_ARG, "upload: pos and mass are required");
+  cudaSetDevice(ctx->device);
+  SysHost& h = ctx->sys[sys];
+  int n = h.n;
+  std::vector<double4> b;
+  copy_interleaved_to_d4(pos, b, n);
+  // fixed-point origin of open dims: centroid of the first upload
+  double cg[3] = {0, 0, 0};
+  for (int i = 0; i < n; i++) {
+    cg[0] += b[i].x; cg[1] += b[i].y; cg[2] += b[i].z;
+  }
+  for (int k = 0; k < 3; k++) {
+    double c = cg[k] / n;
+    if (!std::isfinite(c)) return fail(ctx, GEMSGPU_ERR_NAN, "upload: non-finite positions");
+    if (!h.d.boxed) h.d.fx_origin[k] = c;
+  }
+  Arena& A = ctx->A;
+  CU(cudaMemcpyAsync(A.pos + h.off, b.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(A.pos_old + h.off, b.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<double4> v(n, make_double4(0, 0, 0, 0));
+  if (vel) copy_interleaved_to_d4(vel, v, n);
+  CU(cudaMemcpyAsync(A.vel + h.off, v.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<double4> z(n, make_double4(0, 0, 0, 0));
+  CU(cudaMemcpyAsync(A.acel + h.off, z.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(A.force + h.off, z.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(A.vel_v + h.off, z.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<double2> mi(n);
+  std::vector<int> t(n, 0);
+  for (int i = 0; i < n; i++) {
+    // set_mass (src/Set_Properties.f90:168-191)
+    double m = mass[i];
+    if (m == 0.0) mi[i] = make_double2(0.0, 0.0);
+    else {
+      double om = 1.0 / m;
+      mi[i] = make_double2(om, std::sqrt(om));
+    }
+    if (type) {
+      if (type[i] < 0 || type[i] >= h.ntypes) return fail(ctx, GEMSGPU_ERR_ARG, "upload: type out of range");
+      t[i] = type[i];
+    }
+  }
+  CU(cudaMemcpyAsync(A.mass + h.off, mass, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(A.minv + h.off, mi.data(), n * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(A.type + h.off, t.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  CHK(push_sys(ctx, sys));
+  BlockMap m;
+  CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
+  k_refresh_fx<<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); ++ctx->launches;
+  h.first = true;
+  h.has_forces = false;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int gemsgpu_set_positions(gemsgpu_ctx* ctx, int sys, const double* pos) {
+  CHK(check_sys(ctx, sys));
+  if (!pos) return fail(ctx, GEMSGPU_ERR_ARG, "set_positions: NULL");
+  SysHost& h = ctx->sys[sys];
+  CHK(h2d_xyz(ctx, pos, ctx->A.pos + h.off, h.n));
+  BlockMap m;
+  CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
+  k_refresh_fx<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  CU(cudaStreamSynchronize(ctx->stream));
+  h.pos_dirty = true;
+  h.has_forces = false;
+  return 0;
+}
+
+static int set_d4(gemsgpu_ctx* ctx, int sys, const double* src, double4* dst) {
+  CHK(check_sys(ctx, sys));
+  if (!src) return fail(ctx, GEMSGPU_ERR_ARG, "NULL array");
+  SysHost& h = ctx->sys[sys];
+  CHK(h2d_xyz(ctx, src, dst + h.off, h.n));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int gemsgpu_set_velocities(gemsgpu_ctx* ctx, int sys, const double* vel) {
+  if (!ctx) return GEMSGPU_ERR_ARG;
+  return set_d4(ctx, sys, vel, ctx->A.vel);
+}
+int gemsgpu_set_accelerations(gemsgpu_ctx* ctx, int sys, const double* acel) {
+  if (!ctx) return GEMSGPU_ERR_ARG;
+  return set_d4(ctx, sys, acel, ctx->A.acel);
+}
+
+static int get_d4(gemsgpu_ctx* ctx, const SysHost& h, const double4* src, double* dst) {
+  CHK(d2h_xyz(ctx, src + h.off, dst, h.n));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int gemsgpu_download(gemsgpu_ctx* ctx, int sys, double* pos, double* vel, double* force,
+                     double* epot_atoms) {
+  CHK(check_sys(ctx, sys));
+  const SysHost& h = ctx->sys[sys];
+  if (pos) CHK(get_d4(ctx, h, ctx->A.pos, pos));
+  if (vel) CHK(get_d4(ctx, h, ctx->A.vel, vel));
+  if (force) CHK(get_d4(ctx, h, ctx->A.force, force));
+  if (epot_atoms) {
+    CU(cudaMemcpyAsync(epot_atoms, ctx->A.epot + h.off, h.n * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}
+
+int gemsgpu_download_acel(gemsgpu_ctx* ctx, int sys, double* acel) {
+  CHK(check_sys(ctx, sys));
+  if (!acel) return fail(ctx, GEMSGPU_ERR_ARG, "NULL array");
+  return get_d4(ctx, ctx->sys[sys], ctx->A.acel, acel);
+}
+
+int gemsgpu_set_box(gemsgpu_ctx* ctx, int sys, int boxed, const double L[3], const int pbc[3]) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (boxed) {
+    if (!L) return fail(ctx, GEMSGPU_ERR_ARG, "set_box: L required");
+    for (int k = 0; k < 3; k++)
+      if (!(L[k] > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "set_box: L must be positive");
+  }
+  h.d.boxed = boxed ? 1 : 0;
+  for (int k = 0; k < 3; k++) {
+    h.d.L[k] = boxed ? L[k] : 0.0;
+    h.d.pbc[k] = (boxed && pbc) ? (pbc[k] ? 1 : 0) : 0;
+  }
+  CHK(push_sys(ctx, sys));
+  h.first = true;
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_set_skin(gemsgpu_ctx* ctx, int sys, double skin) {
+  CHK(check_sys(ctx, sys));
+  if (!(skin >= 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "skin must be >= 0");
+  ctx->sys[sys].d.skin = skin;
+  CHK(push_sys(ctx, sys));
+  ctx->sys[sys].first = true;
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_set_skin_mode(gemsgpu_ctx* ctx, int sys, int mic) {
+  CHK(check_sys(ctx, sys));
+  ctx->sys[sys].d.skin_mic = mic ? 1 : 0;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_set_list_mode(gemsgpu_ctx* ctx, int sys, int half) {
+  CHK(check_sys(ctx, sys));
+  ctx->sys[sys].d.half = half ? 1 : 0;
+  ctx->sys[sys].first = true;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec) {
+  CHK(check_sys(ctx, sys));
+  if (prec != GEMSGPU_PREC_FP64 && prec != GEMSGPU_PREC_MIXED)
+    return fail(ctx, GEMSGPU_ERR_ARG, "unknown precision %d", prec);
+  ctx->sys[sys].d.prec = prec;
+  CHK(push_sys(ctx, sys));
+  BlockMap m;
+  CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
+  k_refresh_fx<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  ctx->sys[sys].has_forces = false;
+  invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_set_lj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, double sigma,
+                   double rcut, int shifted_force, double eshift) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (ti < 0 || tj < 0 || ti >= h.ntypes || tj >= h.ntypes || !(rcut > 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_lj: bad type pair or cut-off");
+  if (h.d.ff != FF_NONE && h.d.ff != FF_LJ)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lj: system already has another force field");
+  h.d.ff = FF_LJ;
+  PairP P{};
+  P.v[0] = eps;
+  P.v[1] = sigma;
+  P.v[2] = rcut;
+  P.v[3] = rcut * rcut;
+  if (shifted_force) {
+    // plj_set (src/Pairs.F90:282-291)
+    double x = sigma / rcut, x3 = x * x * x, x6 = x3 * x3;
+    P.v[4] = 4.0 * eps * (x6 * x6 - x6);
+    double s3 = sigma * sigma * sigma, s6 = s3 * s3, s12 = s6 * s6;
+    double r3 = rcut * rcut * rcut, r6 = r3 * r3, r7 = r6 * rcut, r13 = r6 * r6 * rcut;
+    P.v[5] = 24.0 * eps * (2.0 * (s12 / r13) - (s6 / r7));
+    P.v[7] = 1.0;
+  }
+  P.v[6] = eshift;
+  h.prm[ti * h.ntypes + tj] = P;
+  h.prm[tj * h.ntypes + ti] = P;
+  h.ff_set = true;
+  h.first = true;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_set_smatb(gemsgpu_ctx* ctx, int sys, int ti, int tj, double A, double xi, double p,
+                      double q, double r0, double rci, double rce) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (ti < 0 || tj < 0 || ti >= h.ntypes || tj >= h.ntypes || !(rce > rci) || !(r0 > 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_smatb: bad type pair or cut-offs");
+  if (h.d.ff != FF_NONE && h.d.ff != FF_SMATB)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_smatb: system already has another force field");
+  h.d.ff = FF_SMATB;
+  // smatb_set (src/TB.F90:106-170): tail coefficients of Logsdail et al. 2012
+  PairP P{};
+  double dcut = rce - rci;
+  double ab = -1.0 / (dcut * dcut * dcut);
+  double bb = -(q / r0) / (dcut * dcut);
+  double cb = -((q / r0) * (q / r0)) / dcut;
+  double aux = xi * std::exp(-q * (rci / r0 - 1.0));
+  P.v[7] = aux * (12.0 * ab - 6.0 * bb + cb) / (2.0 * (dcut * dcut));
+  P.v[8] = aux * (15.0 * ab - 7.0 * bb + cb) / dcut;
+  P.v[9] = aux * (20.0 * ab - 8.0 * bb + cb) / 2.0;
+  aux = A * std::exp(-p * (rci / r0 - 1.0));
+  bb = -(p / r0) / (dcut * dcut);
+  cb = -((p / r0) * (p / r0)) / dcut;
+  P.v[10] = aux * (12.0 * ab - 6.0 * bb + cb) / (2.0 * (dcut * dcut));
+  P.v[11] = aux * (15.0 * ab - 7.0 * bb + cb) / dcut;
+  P.v[12] = aux * (20.0 * ab - 8.0 * bb + cb) / 2.0;
+  P.v[0] = A; P.v[1] = xi; P.v[2] = p; P.v[3] = q; P.v[4] = r0; P.v[5] = rci; P.v[6] = rce;
+  P.v[13] = 1.0;
+  h.prm[ti * h.ntypes + tj] = P;
+  h.prm[tj * h.ntypes + ti] = P;
+  h.ff_set = true;
+  h.first = true;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_set_tersoff(gemsgpu_ctx* ctx, int sys, const double prm[12]) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (!prm) return fail(ctx, GEMSGPU_ERR_ARG, "set_tersoff: NULL");
+  if (h.d.ff != FF_NONE && h.d.ff != FF_TERSOFF)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_tersoff: system already has another force field");
+  h.d.ff = FF_TERSOFF;
+  TersoffP& T = h.d.ts;
+  T.A = prm[0]; T.B = prm[1]; T.l1 = prm[2]; T.l2 = prm[3]; T.beta = prm[4]; T.n = prm[5];
+  T.c = prm[6]; T.d = prm[7]; T.h = prm[8]; T.R = prm[9]; T.D = prm[10]; T.chi = prm[11];
+  h.lanes = 1;
+  h.ff_set = true;
+  h.first = true;
+  CHK(push_sys(ctx, sys));
+  BlockMap m;
+  CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
+  k_refresh_fx<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_forces(gemsgpu_ctx* ctx, int sys, double* epot, int* rebuilt) {
+  CHK(check_sys(ctx, sys));
+  cudaSetDevice(ctx->device);
+  int64_t before = 0;
+  if (rebuilt) {
+    CHK(read_states(ctx));
+    before = ctx->h_st[sys].nupd;
+  }
+  CHK(interact_group(ctx, {sys}, true));
+  if (epot || rebuilt) {
+    std::vector<double> r;
+    CHK(reduce_sys(ctx, {sys}, r));
+    if (epot) *epot = r[0];
+    if (rebuilt) {
+      CHK(read_states(ctx));
+      *rebuilt = ctx->h_st[sys].nupd > before;
+    }
+  }
+  return 0;
+}
+
+int gemsgpu_update(gemsgpu_ctx* ctx, int sys) {
+  CHK(check_sys(ctx, sys));
+  ctx->sys[sys].first = true;
+  std::vector<int> ss{sys};
+  int need = estimate_cap(ctx->sys[sys]);
+  if (ctx->A.lcap < need) CHK(grow_list(ctx, need));
+  CHK(clear_status(ctx, ss));
+  const int* sa;
+  CHK(sys_array(ctx, ss, &sa));
+  k_force_rebuild<<<1, 256, 0, ctx->stream>>>(ctx->A, sa, 1); ++ctx->launches;
+  CHK(launch_rebuild(ctx, ss));
+  CHK(read_states(ctx));
+  if (ctx->h_st[sys].status & ST_OVERFLOW) {
+    CHK(grow_list(ctx, ctx->h_st[sys].maxnn + 8));
+    CHK(clear_status(ctx, ss));
+    k_force_rebuild<<<1, 256, 0, ctx->stream>>>(ctx->A, sa, 1); ++ctx->launches;
+    CHK(launch_rebuild(ctx, ss));
+    CHK(read_states(ctx));
+  }
+  CHK(status_error(ctx, sys, ctx->h_st[sys].status));
+  ctx->sys[sys].first = false;
+  ctx->sys[sys].pos_dirty = false;
+  return 0;
+}
+
+int gemsgpu_get_list(gemsgpu_ctx* ctx, int sys, int* nn, int* list, int cap, int* cap_needed) {
+  CHK(check_sys(ctx, sys));
+  const SysHost& h = ctx->sys[sys];
+  std::vector<int> hn(h.n);
+  CU(cudaMemcpyAsync(hn.data(), ctx->A.nn + h.off, h.n * sizeof(int), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  int mx = 0;
+  for (int v : hn) mx = std::max(mx, v);
+  if (cap_needed) *cap_needed = mx;
+  if (nn) memcpy(nn, hn.data(), h.n * sizeof(int));
+  if (list) {
+    if (cap < mx) return fail(ctx, GEMSGPU_ERR_ARG, "get_list: cap %d < needed %d", cap, mx);
+    int rows = std::min(mx, ctx->A.lcap);
+    std::vector<int> tmp((size_t)rows * h.n);
+    if (rows > 0)
+      CU(cudaMemcpy2DAsync(tmp.data(), h.n * sizeof(int), ctx->A.list + h.off, ctx->acap * sizeof(int),
+                           h.n * sizeof(int), rows, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (int m = 0; m < cap; m++)
+      for (int i = 0; i < h.n; i++)
+        list[(size_t)m * h.n + i] = (m < rows && m < hn[i]) ? tmp[(size_t)m * h.n + i] - h.off : 0;
+  }
+  return 0;
+}
+
+int gemsgpu_get_nupd(gemsgpu_ctx* ctx, int sys, int64_t* nupd) {
+  CHK(check_sys(ctx, sys));
+  CHK(read_states(ctx));
+  if (nupd) *nupd = ctx->h_st[sys].nupd;
+  return 0;
+}
+
+int gemsgpu_set_vv(gemsgpu_ctx* ctx, int sys, double dt) {
+  CHK(check_sys(ctx, sys));
+  if (!(dt > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "dt must be > 0");
+  SysHost& h = ctx->sys[sys];
+  h.d.integ = IT_VV;
+  h.d.dt = dt;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_set_ermak(gemsgpu_ctx* ctx, int sys, double dt, double gama, double temp, uint64_t seed) {
+  CHK(check_sys(ctx, sys));
+  if (!(dt > 0.0) || !(gama > 0.0) || !(temp >= 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_ermak: dt>0, gamma>0, T>=0");
+  SysHost& h = ctx->sys[sys];
+  SysDev& d = h.d;
+  // set_ermak (src/Integration.F90:909-961)
+  d.integ = IT_ERMAK;
+  d.dt = dt;
+  d.cc0 = std::exp(-dt * gama);
+  d.cc1 = (1.0 - d.cc0) / gama;
+  d.cc2 = (1.0 - d.cc1 / dt) / gama;
+  d.sdr = std::sqrt(dt / gama * (2.0 - (3.0 - 4.0 * d.cc0 + d.cc0 * d.cc0) / (dt * gama)));
+  d.sdv = std::sqrt(1.0 - d.cc0 * d.cc0);
+  d.crv1 = (1.0 - d.cc0) * (1.0 - d.cc0) / (gama * d.sdr * d.sdv);
+  d.crv2 = std::sqrt(1.0 - (d.crv1 * d.crv1));
+  d.skt = std::sqrt(kB_ui * temp);
+  d.seed = seed;
+  d.use_ext_normals = 0;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_set_ermak_normals(gemsgpu_ctx* ctx, int sys, const double* normals) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (!normals) {
+    h.d.use_ext_normals = 0;
+  } else {
+    CU(cudaMemcpyAsync(ctx->A.ext_normals + (size_t)6 * h.off, normals, (size_t)6 * h.n * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    h.d.use_ext_normals = 1;
+  }
+  CHK(push_sys(ctx, sys));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int gemsgpu_set_fire(gemsgpu_ctx* ctx, int sys, double dt0, double dtmax) {
+  CHK(check_sys(ctx, sys));
+  if (!(dt0 > 0.0) || !(dtmax >= dt0)) return fail(ctx, GEMSGPU_ERR_ARG, "set_fire: 0 < dt0 <= dtmax");
+  SysHost& h = ctx->sys[sys];
+  h.d.integ = IT_FIRE;
+  h.d.dt = dt0;
+  h.d.fire_dtmax = dtmax;
+  h.d.fire_fmax = 0.0;
+  h.d.fire_maxit = 0x7fffffff;
+  CHK(push_sys(ctx, sys));
+  SysState z{};
+  CHK(read_states(ctx));
+  z.nupd = ctx->h_st[sys].nupd;
+  z.fire_dt = dt0;
+  z.fire_alpha = 0.1;
+  CU(cudaMemcpyAsync(ctx->A.st + sys, &z, sizeof(z), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<double4> zero(h.n, make_double4(0, 0, 0, 0));
+  CU(cudaMemcpyAsync(ctx->A.vel + h.off, zero.data(), h.n * sizeof(double4), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_step_a(gemsgpu_ctx* ctx, int sys) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (h.d.integ == IT_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "no integrator");
+  CHK(launch_step_a(ctx, {sys}));
+  h.pos_dirty = false;
+  return 0;
+}
+
+int gemsgpu_step_b(gemsgpu_ctx* ctx, int sys) {
+  CHK(check_sys(ctx, sys));
+  if (ctx->sys[sys].d.integ == IT_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "no integrator");
+  CHK(launch_step_b(ctx, {sys}));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int gemsgpu_md_steps(gemsgpu_ctx* ctx, int sys, int nsteps) {
+  CHK(check_sys(ctx, sys));
+  if (nsteps < 0) return fail(ctx, GEMSGPU_ERR_ARG, "nsteps < 0");
+  cudaSetDevice(ctx->device);
+  return md_group(ctx, {sys}, nsteps);
+}
+
+int gemsgpu_energy(gemsgpu_ctx* ctx, int sys, double* epot_ev, double* ekin_ev, double* temp) {
+  CHK(check_sys(ctx, sys));
+  std::vector<double> r;
+  CHK(reduce_sys(ctx, {sys}, r));
+  const SysHost& h = ctx->sys[sys];
+  if (epot_ev) *epot_ev = r[0] * UI_EV;
+  if (ekin_ev) *ekin_ev = r[1] * UI_EV;
+  if (temp) *temp = 2.0 * r[1] / (kB_ui * (3.0 * h.n));
+  return 0;
+}
+
+int gemsgpu_fmax(gemsgpu_ctx* ctx, int sys, double* fmax_ev) {
+  CHK(check_sys(ctx, sys));
+  std::vector<double> r;
+  CHK(reduce_sys(ctx, {sys}, r));
+  if (fmax_ev) *fmax_ev = std::sqrt(r[2]) * UI_EV;
+  return 0;
+}
+
+static int sys_list(gemsgpu_ctx* ctx, const int* sys, int nsys, std::vector<int>& ss) {
+  if (!ctx || !sys || nsys <= 0) return fail(ctx, GEMSGPU_ERR_ARG, "empty system list");
+  ss.assign(sys, sys + nsys);
+  for (int s : ss) CHK(check_sys(ctx, s));
+  std::vector<int> t = ss;
+  std::sort(t.begin(), t.end());
+  if (std::unique(t.begin(), t.end()) != t.end())
+    return fail(ctx, GEMSGPU_ERR_ARG, "duplicate system in batch");
+  return 0;
+}
+
+int gemsgpu_batch_md_steps(gemsgpu_ctx* ctx, const int* sys, int nsys, int nsteps) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  cudaSetDevice(ctx->device);
+  return md_group(ctx, ss, nsteps);
+}
+
+int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys, double fmax, int maxit, int* iters) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  if (!(fmax > 0.0) || maxit <= 0) return fail(ctx, GEMSGPU_ERR_ARG, "batch_fire: fmax>0, maxit>0");
+  cudaSetDevice(ctx->device);
+  for (int s : ss) {
+    SysHost& h = ctx->sys[s];
+    if (h.d.integ != IT_FIRE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d is not set up for FIRE", s);
+    h.d.fire_fmax = fmax;
+    h.d.fire_maxit = maxit;
+    CHK(push_sys(ctx, s));
+  }
+  invalidate(ctx);
+  // converged systems freeze on the device; poll between chunks
+  CHK(interact_group(ctx, ss, true));
+  {
+    std::vector<double> r;
+    CHK(reduce_sys(ctx, ss, r));
+    CHK(read_states(ctx));
+    for (size_t k = 0; k < ss.size(); k++) {
+      SysState st = ctx->h_st[ss[k]];
+      st.fire_done = std::sqrt(r[4 * k + 2]) * UI_EV < fmax ? 1 : 0;
+      CU(cudaMemcpyAsync(ctx->A.st + ss[k], &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+    }
+  }
+  int total = 0;
+  for (;;) {
+    CHK(read_states(ctx));
+    bool all = true;
+    for (int s : ss) all &= ctx->h_st[s].fire_done != 0;
+    if (all || total >= maxit) break;
+    int k = std::min(CHUNK, maxit - total);
+    CHK(clear_status(ctx, ss));
+    CHK(launch_graph(ctx, ss, k));
+    total += k;
+    CHK(read_states(ctx));
+    for (int s : ss) {
+      int st = ctx->h_st[s].status;
+      if (st & (ST_NAN | ST_LOST)) return status_error(ctx, s, st);
+      if (st & ST_OVERFLOW) {
+        CHK(grow_list(ctx, ctx->h_st[s].maxnn + 16));
+        const int* sa;
+        CHK(sys_array(ctx, ss, &sa));
+        k_force_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size()); ++ctx->launches;
+        CHK(clear_status(ctx, ss));
+        CHK(launch_rebuild(ctx, ss));
+        CHK(launch_forces(ctx, ss));
+        break;
+      }
+    }
+  }
+  if (iters)
+    for (size_t k = 0; k < ss.size(); k++) iters[k] = ctx->h_st[ss[k]].fire_iter;
+  return 0;
+}
+
+int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys, double* epot_ev, double* ekin_ev,
+                         double* temp) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  std::vector<double> r;
+  CHK(reduce_sys(ctx, ss, r));
+  for (int k = 0; k < nsys; k++) {
+    if (epot_ev) epot_ev[k] = r[4 * k] * UI_EV;
+    if (ekin_ev) ekin_ev[k] = r[4 * k + 1] * UI_EV;
+    if (temp) temp[k] = 2.0 * r[4 * k + 1] / (kB_ui * (3.0 * ctx->sys[ss[k]].n));
+  }
+  return 0;
+}
+
+int gemsgpu_get_stream(gemsgpu_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return GEMSGPU_ERR_ARG;
+  *stream = (void*)ctx->stream;
+  return 0;
+}
+
+int gemsgpu_get_launch_count(gemsgpu_ctx* ctx, int64_t* launches) {
+  if (!ctx || !launches) return GEMSGPU_ERR_ARG;
+  *launches = ctx->launches;
+  return 0;
+}
+
+int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms) {
+  CHK(check_sys(ctx, sys));
+  if (reps <= 0 || !out_ms) return fail(ctx, GEMSGPU_ERR_ARG, "time_kernels: reps > 0, out_ms");
+  cudaSetDevice(ctx->device);
+  SysHost& h = ctx->sys[sys];
+  if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "no force field");
+  std::vector<int> ss{sys};
+  if (h.first || h.pos_dirty || !h.has_forces) CHK(interact_group(ctx, ss, true));
+  const int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
+  BlockMap m;
+  CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / K, 0, &m));
+  cudaEvent_t ev[6];
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  const Arena& A = ctx->A;
+  auto first_kernel = [&]() {
+    if (h.d.ff == FF_SMATB) {
+      if (h.d.prec == PREC_MIXED) {
+        switch (K) {
+          case 4: k_smatb_rho_mixed<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+          case 16: k_smatb_rho_mixed<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+          default: k_smatb_rho_mixed<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+        }
+      } else {
+        switch (K) {
+          case 4: k_smatb_rho_fp64<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+          case 16: k_smatb_rho_fp64<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+          default: k_smatb_rho_fp64<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+        }
+      }
+    } else {
+      launch_forces(ctx, ss);
+    }
+  };
+  auto second_kernel = [&]() {
+    if (h.d.ff != FF_SMATB) return;
+    if (h.d.prec == PREC_MIXED) {
+      switch (K) {
+        case 4: k_smatb_force_mixed<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+        case 16: k_smatb_force_mixed<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+        default: k_smatb_force_mixed<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+      }
+    } else {
+      switch (K) {
+        case 4: k_smatb_force_fp64<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+        case 16: k_smatb_force_fp64<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+        default: k_smatb_force_fp64<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
+      }
+    }
+  };
+  first_kernel();
+  second_kernel();
+  const int* sa;
+  CHK(sys_array(ctx, ss, &sa));
+  CU(cudaEventRecord(ev[0], ctx->stream));
+  for (int r = 0; r < reps; r++) first_kernel();
+  CU(cudaEventRecord(ev[1], ctx->stream));
+  for (int r = 0; r < reps; r++) second_kernel();
+  CU(cudaEventRecord(ev[2], ctx->stream));
+  for (int r = 0; r < reps; r++) {
+    k_force_rebuild<<<1, 256, 0, ctx->stream>>>(ctx->A, sa, 1);
+    CHK(launch_rebuild(ctx, ss));
+  }
+  CU(cudaEventRecord(ev[3], ctx->stream));
+  CU(cudaEventSynchronize(ev[3]));
+  float t[3];
+  CU(cudaEventElapsedTime(&t[0], ev[0], ev[1]));
+  CU(cudaEventElapsedTime(&t[1], ev[1], ev[2]));
+  CU(cudaEventElapsedTime(&t[2], ev[2], ev[3]));
+  for (int k = 0; k < 3; k++) out_ms[k] = t[k] / reps;
+  for (auto& e : ev) cudaEventDestroy(e);
+  CU(cudaGetLastError());
+  return 0;
+}
+
+}  // extern "C"

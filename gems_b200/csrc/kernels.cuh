@@ -1,0 +1,1264 @@
+// kernels.cuh -- sm_100a kernels of the force/neighbour path.
+//
+// Conventions
+//  * every kernel runs BLOCK threads and walks a BlockMap: block b belongs to
+//    one system, so per-system branches never diverge inside a block;
+//  * neighbour lists are column-major, list[m * cap + i] (the reference's
+//    list(i,m), src/Neighbour.F90:116-117), which makes the m-th neighbour of
+//    consecutive atoms a coalesced 128-byte row;
+//  * force kernels split an atom's list over K lanes and combine the lanes
+//    with a fixed xor-shuffle tree, so results do not depend on scheduling;
+//  * the list predicate and the skin test use explicitly rounded FP64
+//    operations (no FMA contraction) so they decide exactly as the reference.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace gg {
+
+// GEMS unit conversion (src/Constants.F90:101-127), fixed at compile time
+// in the same operation order as the reference.
+__host__ __device__ constexpr double c_ui_ev() {
+  return 1.0e2 * 1.0e2 * 1.6605402e-27 * (1.0 / 1.60219e-19);
+}
+#define EV_UI (1.0 / gg::c_ui_ev())
+
+__device__ __forceinline__ int blk_sys(const BlockMap& M) { return M.sys[blockIdx.x]; }
+
+// ------------------------------------------------------------------ Philox
+// Counter-based generator Philox4x32-10 (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11).
+__device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+    uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += W0;
+    k.y += W1;
+  }
+  return c;
+}
+
+// two standard normals from one Philox block (Box-Muller, FP64)
+__device__ __forceinline__ void normals2(uint4 r, double& n1, double& n2) {
+  const double inv53 = 1.0 / 9007199254740992.0;  // 2^-53
+  double u1 = ((double)(r.x >> 5) * 67108864.0 + (double)(r.y >> 6)) * inv53;
+  double u2 = ((double)(r.z >> 5) * 67108864.0 + (double)(r.w >> 6)) * inv53;
+  u1 = 1.0 - u1;  // (0, 1]
+  double rr = sqrt(-2.0 * log(u1));
+  double sn, cs;
+  sincospi(2.0 * u2, &sn, &cs);
+  n1 = rr * cs;
+  n2 = rr * sn;
+}
+
+// ------------------------------------------------------------------ helpers
+// top-2 of squared displacements (test_update, src/Neighbour.F90:1305-1346)
+__device__ __forceinline__ double2 top2_merge(double2 a, double2 b) {
+  double hi = fmax(a.x, b.x);
+  double lo = fmax(fmin(a.x, b.x), fmax(a.y, b.y));
+  return make_double2(hi, lo);
+}
+
+__device__ __forceinline__ double2 block_top2(double2 v) {
+  __shared__ double2 sh[BLOCK / 32];
+  for (int o = 16; o; o >>= 1) {
+    double2 w;
+    w.x = __shfl_xor_sync(0xffffffffu, v.x, o);
+    w.y = __shfl_xor_sync(0xffffffffu, v.y, o);
+    v = top2_merge(v, w);
+  }
+  int wid = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  if (ln == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = ln < BLOCK / 32 ? sh[ln] : make_double2(1.e-16, 1.e-16);
+    for (int o = 16; o; o >>= 1) {
+      double2 w;
+      w.x = __shfl_xor_sync(0xffffffffu, v.x, o);
+      w.y = __shfl_xor_sync(0xffffffffu, v.y, o);
+      v = top2_merge(v, w);
+    }
+  }
+  __syncthreads();
+  return v;  // valid in thread 0
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[BLOCK / 32];
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  int wid = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  if (ln == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = ln < BLOCK / 32 ? sh[ln] : 0.0;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;  // valid in thread 0
+}
+
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double sh[BLOCK / 32];
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  int wid = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  if (ln == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = ln < BLOCK / 32 ? sh[ln] : 0.0;
+    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  __syncthreads();
+  return v;
+}
+
+// exact reference predicate: vd = pos_j - pos_i with minimum image
+// (vdistance, src/Inq_Properties.F90:137-157), rd = dot_product(vd, vd)
+__device__ __forceinline__ double rd_exact(const SysDev& S, double4 xi, double4 xj) {
+  double v0 = __dsub_rn(xj.x, xi.x);
+  double v1 = __dsub_rn(xj.y, xi.y);
+  double v2 = __dsub_rn(xj.z, xi.z);
+  if (S.pbc[0]) v0 = __dsub_rn(v0, __dmul_rn(S.L[0], round(__dmul_rn(v0, S.invL[0]))));
+  if (S.pbc[1]) v1 = __dsub_rn(v1, __dmul_rn(S.L[1], round(__dmul_rn(v1, S.invL[1]))));
+  if (S.pbc[2]) v2 = __dsub_rn(v2, __dmul_rn(S.L[2], round(__dmul_rn(v2, S.invL[2]))));
+  return __dadd_rn(__dadd_rn(__dmul_rn(v0, v0), __dmul_rn(v1, v1)), __dmul_rn(v2, v2));
+}
+
+// minimum-image pair vector in FP64 for the FP64 force kernels
+__device__ __forceinline__ void vd_fp64(const SysDev& S, double4 xi, double4 xj,
+                                        double& v0, double& v1, double& v2) {
+  v0 = xj.x - xi.x;
+  v1 = xj.y - xi.y;
+  v2 = xj.z - xi.z;
+  if (S.pbc[0]) v0 = v0 - S.L[0] * round(v0 * S.invL[0]);
+  if (S.pbc[1]) v1 = v1 - S.L[1] * round(v1 * S.invL[1]);
+  if (S.pbc[2]) v2 = v2 - S.L[2] * round(v2 * S.invL[2]);
+}
+
+// fixed-point coordinates for the mixed kernels.  Periodic dims map [0,L)
+// onto the full 32-bit ring (the int32 difference is the minimum image);
+// open dims use 2^22 units per Angstrom around fx_origin (+-512 A).
+__device__ __forceinline__ int fx_coord(const SysDev& S, int d, double x, int& bad) {
+  if (S.fx_per[d]) {
+    double t = floor(x * S.fx_scale[d]);
+    long long q = (long long)t;
+    return (int)(unsigned int)(unsigned long long)q;
+  }
+  double t = rint((x - S.fx_origin[d]) * S.fx_scale[d]);
+  if (!(fabs(t) < 2147483000.0)) {
+    bad = 1;
+    t = 0.0;
+  }
+  return (int)t;
+}
+
+__device__ __forceinline__ void write_fx(const Arena& A, const SysDev& S, int i,
+                                         double4 p, int ti, int& bad) {
+  int4 q;
+  q.x = fx_coord(S, 0, p.x, bad);
+  q.y = fx_coord(S, 1, p.y, bad);
+  q.z = fx_coord(S, 2, p.z, bad);
+  q.w = ti;
+  A.fxp[i] = q;
+}
+
+// squared displacement since the last rebuild.  Reference mode (skin_mic=0)
+// takes the raw difference of test_update (src/Neighbour.F90:1320), so an atom
+// wrapped by do_pbc counts as having moved a box length and forces a rebuild;
+// skin_mic=1 takes the minimum image, which moves no list decision for atoms
+// that did not move, only skips those spurious rebuilds.
+__device__ __forceinline__ double disp2(const SysDev& S, double4 x, double4 q) {
+  double v0 = __dsub_rn(x.x, q.x), v1 = __dsub_rn(x.y, q.y), v2 = __dsub_rn(x.z, q.z);
+  if (S.skin_mic) {
+    if (S.pbc[0]) v0 = __dsub_rn(v0, __dmul_rn(S.L[0], round(__dmul_rn(v0, S.invL[0]))));
+    if (S.pbc[1]) v1 = __dsub_rn(v1, __dmul_rn(S.L[1], round(__dmul_rn(v1, S.invL[1]))));
+    if (S.pbc[2]) v2 = __dsub_rn(v2, __dmul_rn(S.L[2], round(__dmul_rn(v2, S.invL[2]))));
+  }
+  return __dadd_rn(__dadd_rn(__dmul_rn(v0, v0), __dmul_rn(v1, v1)), __dmul_rn(v2, v2));
+}
+
+// last block of a system in a launch: true in thread 0 of that block
+__device__ __forceinline__ bool last_block(const BlockMap& M, SysState* st, int s,
+                                           int* counter) {
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = atomicAdd(counter, 1);
+    last = (t == M.sys_nblk[s] - 1);
+    if (last) *counter = 0;
+  }
+  __syncthreads();
+  return last;
+}
+
+// ------------------------------------------------------------------ skin test
+// Per-block top-2 of |pos - pos_old|^2; the last block of each system
+// decides rebuild = sqrt(d1) + sqrt(d2) > nb_dcut (test_update).
+__device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, int s,
+                                           double2 t) {
+  if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
+  if (last_block(M, A.st, s, &A.st[s].ticket)) {
+    if (threadIdx.x == 0) {
+      double2 v = make_double2(1.e-16, 1.e-16);
+      int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+      for (int b = 0; b < nb; b++) v = top2_merge(v, __ldcg(&A.blk_top2[b0 + b]));
+      const SysDev& S = A.sys[s];
+      int rb = __dadd_rn(__dsqrt_rn(v.x), __dsqrt_rn(v.y)) > S.skin;
+      A.st[s].rebuild = rb;
+      if (rb) atomicOr(A.any_rebuild, 1);
+    }
+  }
+}
+
+__global__ void k_skin(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  double2 t = make_double2(1.e-16, 1.e-16);
+  if (i < M.end[blockIdx.x]) t.x = disp2(A.sys[s], A.pos[i], A.pos_old[i]);
+  t = block_top2(t);
+  skin_finish(A, M, s, t);
+}
+
+// mark systems for rebuild (first interact: update(), Interaction.f90:174)
+__global__ void k_force_rebuild(Arena A, const int* sys, int nsys) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nsys) {
+    A.st[sys[k]].rebuild = 1;
+    atomicOr(A.any_rebuild, 1);
+  }
+}
+
+// refresh fixed-point positions (after an upload or set_positions)
+__global__ void k_refresh_fx(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  if (i >= M.end[blockIdx.x]) return;
+  const SysDev& S = A.sys[s];
+  int bad = 0;
+  write_fx(A, S, i, A.pos[i], A.type[i], bad);
+  if (bad) atomicOr(&A.st[s].status, ST_LOST);
+}
+
+// ------------------------------------------------------------------ binning
+// sort_in_cells (src/Neighbour.F90:927-989) as a counting sort:
+// k_bin (histogram) -> k_scan1/k_scan2 (prefix) -> k_scatter -> k_sort_cells
+__global__ void k_bin(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  if (!A.st[s].rebuild || !S.use_cells) return;
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  if (i >= M.end[blockIdx.x]) return;
+  double4 p = A.pos[i];
+  int c0 = (int)__dmul_rn(p.x, S.inv_cell[0]);
+  int c1 = (int)__dmul_rn(p.y, S.inv_cell[1]);
+  int c2 = (int)__dmul_rn(p.z, S.inv_cell[2]);
+  bool lost = false;
+  // out-of-grid atoms are undefined behaviour in the reference; here they
+  // are clamped into the grid and the system is flagged ST_LOST.
+  if (c0 < 0 || c0 >= S.nc[0]) { lost = true; c0 = c0 < 0 ? 0 : S.nc[0] - 1; }
+  if (c1 < 0 || c1 >= S.nc[1]) { lost = true; c1 = c1 < 0 ? 0 : S.nc[1] - 1; }
+  if (c2 < 0 || c2 >= S.nc[2]) { lost = true; c2 = c2 < 0 ? 0 : S.nc[2] - 1; }
+  if (lost || !(p.x == p.x && p.y == p.y && p.z == p.z)) atomicOr(&A.st[s].status, ST_LOST);
+  int cid = S.cell_off + c0 + S.nc[0] * (c1 + S.nc[1] * c2);
+  A.cell_of[i] = cid;
+  A.slot[i] = atomicAdd(&A.cell_count[cid], 1);
+}
+
+// per 256-cell chunk: local exclusive prefix, chunk total; resets counts
+__global__ void k_scan1(Arena A, BlockMap C) {
+  int s = blk_sys(C);
+  if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
+  int c = C.first[blockIdx.x] + threadIdx.x;
+  bool act = c < C.end[blockIdx.x];
+  int v = act ? A.cell_count[c] : 0;
+  if (act) {
+    A.cell_n[c] = v;
+    A.cell_count[c] = 0;
+  }
+  __shared__ int sh[BLOCK];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < BLOCK; o <<= 1) {
+    int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (act) A.cell_loc[c] = sh[threadIdx.x] - v;
+  if (threadIdx.x == BLOCK - 1) A.chunk_sum[C.first[blockIdx.x] >> 8] = sh[BLOCK - 1];
+}
+
+// one block per system: exclusive prefix of its chunk totals
+__global__ void k_scan2(Arena A, const int* sys, int nsys) {
+  int s = sys[blockIdx.x];
+  const SysDev& S = A.sys[s];
+  if (!A.st[s].rebuild || !S.use_cells) return;
+  int k0 = S.cell_off >> 8;
+  int nk = (S.ncell + BLOCK - 1) / BLOCK;
+  __shared__ int sh[BLOCK];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = S.off;
+  __syncthreads();
+  for (int base = 0; base < nk; base += BLOCK) {
+    int k = base + threadIdx.x;
+    int v = k < nk ? A.chunk_sum[k0 + k] : 0;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < BLOCK; o <<= 1) {
+      int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+      __syncthreads();
+      sh[threadIdx.x] += t;
+      __syncthreads();
+    }
+    int excl = carry + sh[threadIdx.x] - v;
+    int tot = sh[BLOCK - 1];
+    __syncthreads();
+    if (k < nk) A.chunk_sum[k0 + k] = excl;
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+}
+
+__global__ void k_scatter(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  if (i >= M.end[blockIdx.x]) return;
+  int c = A.cell_of[i];
+  int start = A.chunk_sum[c >> 8] + A.cell_loc[c];
+  A.cell_atoms[start + A.slot[i]] = i;
+}
+
+// one warp per cell: absolute start, then order the cell's atoms by
+// descending index -- the order of the reference's head/next chain, which
+// is built by inserting atoms in increasing index order.  Each lane ranks
+// its atom(s) against the whole cell (cells of up to 64 atoms); larger cells
+// fall back to an insertion sort by one lane.
+__global__ void k_sort_cells(Arena A, BlockMap C) {
+  int s = blk_sys(C);
+  if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
+  const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const int first = C.first[blockIdx.x], end = C.end[blockIdx.x];
+  for (int c = first + warp; c < end; c += BLOCK / 32) {
+    int start = A.chunk_sum[c >> 8] + A.cell_loc[c];
+    int n = A.cell_n[c];
+    if (ln == 0) A.cell_start[c] = start;
+    int* a = A.cell_atoms + start;
+    if (n <= 64) {
+      int v0 = ln < n ? a[ln] : -1;
+      int v1 = ln + 32 < n ? a[ln + 32] : -1;
+      int r0 = 0, r1 = 0;
+      for (int k = 0; k < 32; k++) {
+        int w0 = __shfl_sync(0xffffffffu, v0, k);
+        int w1 = __shfl_sync(0xffffffffu, v1, k);
+        r0 += (w0 > v0) + (w1 > v0);
+        r1 += (w0 > v1) + (w1 > v1);
+      }
+      __syncwarp();
+      if (ln < n) a[r0] = v0;
+      if (ln + 32 < n) a[r1] = v1;
+    } else if (ln == 0) {
+      for (int x = 1; x < n; x++) {
+        int v = a[x];
+        int y = x - 1;
+        while (y >= 0 && a[y] < v) {
+          a[y + 1] = a[y];
+          y--;
+        }
+        a[y + 1] = v;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ lists
+__device__ __forceinline__ void list_put(const Arena& A, int i, int m, int j) {
+  if (m < A.lcap) A.list[(size_t)m * A.cap + i] = j;
+}
+
+__device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
+  A.nn[i] = m;
+  A.pos_old[i] = A.pos[i];
+  if (m > A.lcap) atomicOr(&A.st[s].status, ST_OVERFLOW);
+  atomicMax(&A.st[s].maxnn, m);
+}
+
+// linkedcell_self / linkedcell_selfhalf (src/Neighbour.F90:991-1161): the
+// 27 (or 14) stencil cells in the reference's order with periodic cell
+// wrap (cell_pbc, :1350-1376); keep j if rd < (rcut+nb_dcut)^2 (strict).
+// One warp per atom: the lanes test one cell's candidates at once and a
+// ballot keeps the accepted ones in candidate order, so the list comes out
+// in the reference's order.  The block's lists are staged in shared memory
+// (LIST_ATOMS atoms x lcap) and written out as coalesced column rows.
+constexpr int LIST_ATOMS = BLOCK / 32;
+
+__global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  if (!A.st[s].rebuild || !S.use_cells) return;
+  extern __shared__ int stage[];  // [LIST_ATOMS][lcap]
+  const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const int i0 = M.first[blockIdx.x];
+  const int i = i0 + warp;
+  const bool act = i < M.end[blockIdx.x];
+  int m = 0;
+  if (act) {
+    const double4 xi = A.pos[i];
+    int c = A.cell_of[i] - S.cell_off;
+    int cx = c % S.nc[0], cy = (c / S.nc[0]) % S.nc[1], cz = c / (S.nc[0] * S.nc[1]);
+    const int nst = S.half ? 14 : 27;
+    int* row = stage + warp * A.lcap;
+    for (int k = 0; k < nst; k++) {
+      int dx, dy, dz;
+      stencil(k, dx, dy, dz);
+      int x = (cx + dx + S.nc[0]) % S.nc[0];
+      int y = (cy + dy + S.nc[1]) % S.nc[1];
+      int z = (cz + dz + S.nc[2]) % S.nc[2];
+      int cid = S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
+      int beg = A.cell_start[cid], cnt = A.cell_n[cid];
+      int t0 = 0;
+      if (S.half && k == 0) {
+        // same cell: only atoms after i in the chain (smaller indices)
+        int pos_i = cnt;
+        for (int base = 0; base < cnt; base += 32) {
+          int t = base + ln;
+          unsigned b = __ballot_sync(0xffffffffu, t < cnt && A.cell_atoms[beg + t] == i);
+          if (b) pos_i = min(pos_i, base + __ffs(b) - 1);
+        }
+        t0 = pos_i + 1;
+      }
+      for (int t = t0; t < cnt; t += 32) {
+        int tt = t + ln;
+        bool ok = false;
+        int j = -1;
+        if (tt < cnt) {
+          j = A.cell_atoms[beg + tt];
+          ok = (j != i) && rd_exact(S, xi, A.pos[j]) < S.rlist2;
+        }
+        unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+          int mm = m + __popc(b & ((1u << ln) - 1u));
+          if (mm < A.lcap) row[mm] = j;
+        }
+        m += __popc(b);
+      }
+    }
+  }
+  __syncthreads();
+  // coalesced write-out: row m of the block's atoms, LIST_ATOMS ints at a time
+  __shared__ int cnt_sh[LIST_ATOMS];
+  if (ln == 0) cnt_sh[warp] = act ? m : 0;
+  __syncthreads();
+  int mx = 0;
+  for (int w = 0; w < LIST_ATOMS; w++) mx = max(mx, cnt_sh[w]);
+  mx = min(mx, A.lcap);
+  for (int e = threadIdx.x; e < mx * LIST_ATOMS; e += BLOCK) {
+    int mm = e / LIST_ATOMS, w = e % LIST_ATOMS;
+    int ii = i0 + w;
+    if (ii < M.end[blockIdx.x] && mm < cnt_sh[w]) A.list[(size_t)mm * A.cap + ii] = stage[w * A.lcap + mm];
+  }
+  if (act && ln == 0) list_done(A, s, i, m);
+}
+
+// verlet_self / verlet_selfhalf (src/Neighbour.F90:676-811): O(N^2) over the
+// system in increasing index, keep j if rd <= (rcut+nb_dcut)^2.  Candidate
+// positions are staged through shared memory one BLOCK-wide tile at a time.
+__global__ void k_list_n2(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  if (!A.st[s].rebuild || S.use_cells) return;
+  __shared__ double4 tile[BLOCK];
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  bool act = i < M.end[blockIdx.x];
+  double4 xi = act ? A.pos[i] : make_double4(0, 0, 0, 0);
+  int m = 0;
+  const int j0 = S.off, j1 = S.off + S.n;
+  for (int base = j0; base < j1; base += BLOCK) {
+    int j = base + threadIdx.x;
+    __syncthreads();
+    if (j < j1) tile[threadIdx.x] = A.pos[j];
+    __syncthreads();
+    int nt = min(BLOCK, j1 - base);
+    if (act) {
+      for (int t = 0; t < nt; t++) {
+        int jj = base + t;
+        if (S.half ? (jj <= i) : (jj == i)) continue;
+        double rd = rd_exact(S, xi, tile[t]);
+        if (rd > S.rlist2) continue;
+        list_put(A, i, m++, jj);
+      }
+    }
+  }
+  if (act) list_done(A, s, i, m);
+}
+
+__global__ void k_count_rebuild(Arena A, const int* sys, int nsys) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nsys && A.st[sys[k]].rebuild) A.st[sys[k]].nupd++;
+}
+
+// ------------------------------------------------------------------ SMA-TB
+// Per species-pair constants of the FP64 kernels.
+struct SmFP64 {
+  double A, eps2, p, q, r0, rci, rce, b1, b2, b3, r1, r2, r3, pr0, q2r0;
+};
+__device__ __forceinline__ SmFP64 sm_load(const PairP& P) {
+  SmFP64 c;
+  c.A = P.v[0];
+  c.eps2 = P.v[1] * P.v[1];
+  c.p = P.v[2];
+  c.q = P.v[3];
+  c.r0 = P.v[4];
+  c.rci = P.v[5];
+  c.rce = P.v[6];
+  c.b1 = P.v[7]; c.b2 = P.v[8]; c.b3 = P.v[9];
+  c.r1 = P.v[10]; c.r2 = P.v[11]; c.r3 = P.v[12];
+  c.pr0 = P.v[2] / P.v[4];
+  c.q2r0 = 2.0 * P.v[3] / P.v[4];
+  return c;
+}
+
+template <int K>
+__device__ __forceinline__ double lane_sum(double v) {
+#pragma unroll
+  for (int o = K / 2; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int K>
+__device__ __forceinline__ float lane_sumf(float v) {
+#pragma unroll
+  for (int o = K / 2; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// smatb_preinteraction (src/TB.F90:367-455), FP64: rho_i = sum_j
+//   xi^2 exp(-2q(r/r0-1))            r <  rci
+//   (b1 d^5 + b2 d^4 + b3 d^3)^2     rci <= r <= rce, d = r - rce
+template <int K>
+__global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x / K;
+  int lane = threadIdx.x % K;
+  bool act = i < M.end[blockIdx.x];
+  double band = 0.0;
+  if (act) {
+    const double4 xi = A.pos[i];
+    const int ti = A.type[i];
+    const int nn = min(A.nn[i], A.lcap);
+    const bool one = S.ntypes == 1;
+    SmFP64 c = sm_load(A.prm[S.param_off]);
+    for (int m = lane; m < nn; m += K) {
+      int j = A.list[(size_t)m * A.cap + i];
+      if (!one) c = sm_load(A.prm[S.param_off + ti * S.ntypes + A.type[j]]);
+      double v0, v1, v2;
+      vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+      double dr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+      if (dr > c.rce) continue;
+      double banda;
+      if (dr < c.rci) {
+        banda = c.eps2 * exp(-2.0 * c.q * (dr / c.r0 - 1.0));
+      } else {
+        double d = dr - c.rce, d2 = d * d, d3 = d2 * d;
+        banda = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+        banda = banda * banda;
+      }
+      band += banda;
+    }
+  }
+  band = lane_sum<K>(band);
+  if (act && lane == 0) {
+    A.band[i] = band;
+    double eb = 1.0 / sqrt(band);
+    A.eband[i] = eb;
+    A.ebandf[i] = (float)eb;
+  }
+}
+
+// smatb_interact (src/TB.F90:457-586), FP64, full list (newton off):
+//   r <= rci : factor = 2 A e^{-p(r/r0-1)} p/r0
+//                       - xi^2/2 e^{-2q(r/r0-1)} (2q/r0)(eb_i + eb_j)
+//   tail     : factor = P P' (eb_i + eb_j) - 2 R'
+//   F_i -= factor * ev_ui * vd / r ;  e_i += repul ; e_i -= sqrt(rho_i)
+template <int K>
+__global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x / K;
+  int lane = threadIdx.x % K;
+  bool act = i < M.end[blockIdx.x];
+  double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  if (act) {
+    const double4 xi = A.pos[i];
+    const int ti = A.type[i];
+    const double ebi = A.eband[i];
+    const int nn = min(A.nn[i], A.lcap);
+    const bool one = S.ntypes == 1;
+    SmFP64 c = sm_load(A.prm[S.param_off]);
+    for (int m = lane; m < nn; m += K) {
+      int j = A.list[(size_t)m * A.cap + i];
+      if (!one) c = sm_load(A.prm[S.param_off + ti * S.ntypes + A.type[j]]);
+      double v0, v1, v2;
+      vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+      double dr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+      if (dr > c.rce) continue;
+      double factor, repul;
+      double ebs = ebi + A.eband[j];
+      if (dr <= c.rci) {
+        double x = dr / c.r0 - 1.0;
+        repul = c.A * exp(-c.p * x);
+        factor = 2.0 * repul * c.pr0 - c.eps2 * 0.5 * exp(-2.0 * c.q * x) * c.q2r0 * ebs;
+      } else {
+        double d = dr - c.rce, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
+        double P = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+        double dP = 5.0 * c.b1 * d4 + 4.0 * c.b2 * d3 + 3.0 * c.b3 * d2;
+        double dR = 5.0 * c.r1 * d4 + 4.0 * c.r2 * d3 + 3.0 * c.r3 * d2;
+        factor = P * dP * ebs - 2.0 * dR;
+        repul = (c.r1 * d2 + c.r2 * d + c.r3) * d3;
+      }
+      double fr = factor * EV_UI / dr;
+      f0 -= fr * v0;
+      f1 -= fr * v1;
+      f2 -= fr * v2;
+      ep += repul;
+    }
+  }
+  f0 = lane_sum<K>(f0);
+  f1 = lane_sum<K>(f1);
+  f2 = lane_sum<K>(f2);
+  ep = lane_sum<K>(ep);
+  if (act && lane == 0) {
+    A.force[i] = make_double4(f0, f1, f2, 0.0);
+    A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
+  }
+}
+
+// ---- mixed precision: FP32 pair math, FP64 accumulation.
+// Pair vectors come from fixed-point coordinates, so the subtraction is
+// exact and the minimum image is the int32 wrap of periodic dims.
+struct SmF32 {
+  float kp, kq, r0;    // e1 = 2^(kp (r0 - r)) = exp(-p(r/r0-1)),
+                       // e2 = 2^(kq (r0 - r)) = exp(-2q(r/r0-1)); r0 - r is exact
+  float A, eps2, c1, c2;
+  float rci, rce, rci2, rce2;
+  float b1, b2, b3, r1, r2, r3;
+};
+__device__ __forceinline__ SmF32 smf_load(const PairP& P) {
+  const double log2e = 1.4426950408889634;
+  SmF32 c;
+  double A = P.v[0], xi = P.v[1], p = P.v[2], q = P.v[3], r0 = P.v[4];
+  c.kp = (float)(p / r0 * log2e);
+  c.kq = (float)(2.0 * q / r0 * log2e);
+  c.r0 = (float)r0;
+  c.A = (float)A;
+  c.eps2 = (float)(xi * xi);
+  c.c1 = (float)(2.0 * A * p / r0);          // 2 A p/r0 (times e1)
+  c.c2 = (float)(xi * xi * q / r0);          // xi^2/2 * 2q/r0 (times e2 * ebs)
+  c.rci = (float)P.v[5];
+  c.rce = (float)P.v[6];
+  c.rci2 = (float)(P.v[5] * P.v[5]);
+  c.rce2 = (float)(P.v[6] * P.v[6]);
+  c.b1 = (float)P.v[7]; c.b2 = (float)P.v[8]; c.b3 = (float)P.v[9];
+  c.r1 = (float)P.v[10]; c.r2 = (float)P.v[11]; c.r3 = (float)P.v[12];
+  return c;
+}
+
+// exact integer difference, one rounding in the conversion; the unit is
+// applied as hi + lo so its float rounding adds no systematic scale error
+__device__ __forceinline__ void vd_fx(const SysDev& S, int4 a, int4 b, float& x, float& y,
+                                      float& z) {
+  float fx = (float)(b.x - a.x), fy = (float)(b.y - a.y), fz = (float)(b.z - a.z);
+  x = fmaf(fx, S.fx_inv[0], fx * S.fx_inv_lo[0]);
+  y = fmaf(fy, S.fx_inv[1], fy * S.fx_inv_lo[1]);
+  z = fmaf(fz, S.fx_inv[2], fz * S.fx_inv_lo[2]);
+}
+
+__device__ __forceinline__ float ex2f(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+template <int K>
+__global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x / K;
+  int lane = threadIdx.x % K;
+  bool act = i < M.end[blockIdx.x];
+  double band = 0.0;
+  if (act) {
+    const int4 xi = A.fxp[i];
+    const int nn = min(A.nn[i], A.lcap);
+    const bool one = S.ntypes == 1;
+    SmF32 c = smf_load(A.prm[S.param_off]);
+    for (int m = lane; m < nn; m += K) {
+      int j = A.list[(size_t)m * A.cap + i];
+      int4 xj = A.fxp[j];
+      if (!one) c = smf_load(A.prm[S.param_off + xi.w * S.ntypes + xj.w]);
+      float v0, v1, v2;
+      vd_fx(S, xi, xj, v0, v1, v2);
+      float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+      if (r2 > c.rce2) continue;
+      float dr = sqrtf(r2);
+      float banda;
+      if (dr < c.rci) {
+        banda = c.eps2 * ex2f(c.kq * (c.r0 - dr));
+      } else {
+        float d = dr - c.rce, d2 = d * d, d3 = d2 * d;
+        banda = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+        banda = banda * banda;
+      }
+      band += (double)banda;
+    }
+  }
+  band = lane_sum<K>(band);
+  if (act && lane == 0) {
+    A.band[i] = band;
+    double eb = 1.0 / sqrt(band);
+    A.eband[i] = eb;
+    A.ebandf[i] = (float)eb;
+  }
+}
+
+template <int K>
+__global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x / K;
+  int lane = threadIdx.x % K;
+  bool act = i < M.end[blockIdx.x];
+  double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  if (act) {
+    const int4 xi = A.fxp[i];
+    const float ebi = A.ebandf[i];
+    const int nn = min(A.nn[i], A.lcap);
+    const bool one = S.ntypes == 1;
+    SmF32 c = smf_load(A.prm[S.param_off]);
+    const float evui = (float)EV_UI;
+    for (int m = lane; m < nn; m += K) {
+      int j = A.list[(size_t)m * A.cap + i];
+      int4 xj = A.fxp[j];
+      if (!one) c = smf_load(A.prm[S.param_off + xi.w * S.ntypes + xj.w]);
+      float v0, v1, v2;
+      vd_fx(S, xi, xj, v0, v1, v2);
+      float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+      if (r2 > c.rce2) continue;
+      float dr = sqrtf(r2);
+      float rinv = __frcp_rn(dr);
+      float ebs = ebi + A.ebandf[j];
+      float factor, repul;
+      if (dr <= c.rci) {
+        float x = c.r0 - dr;
+        float e1 = ex2f(c.kp * x);
+        float e2 = ex2f(c.kq * x);
+        repul = c.A * e1;
+        factor = c.c1 * e1 - c.c2 * e2 * ebs;
+      } else {
+        float d = dr - c.rce, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
+        float P = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+        float dP = 5.0f * c.b1 * d4 + 4.0f * c.b2 * d3 + 3.0f * c.b3 * d2;
+        float dR = 5.0f * c.r1 * d4 + 4.0f * c.r2 * d3 + 3.0f * c.r3 * d2;
+        factor = P * dP * ebs - 2.0f * dR;
+        repul = (c.r1 * d2 + c.r2 * d + c.r3) * d3;
+      }
+      float fr = factor * evui * rinv;
+      f0 -= (double)(fr * v0);
+      f1 -= (double)(fr * v1);
+      f2 -= (double)(fr * v2);
+      ep += (double)repul;
+    }
+  }
+  f0 = lane_sum<K>(f0);
+  f1 = lane_sum<K>(f1);
+  f2 = lane_sum<K>(f2);
+  ep = lane_sum<K>(ep);
+  if (act && lane == 0) {
+    A.force[i] = make_double4(f0, f1, f2, 0.0);
+    A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
+  }
+}
+
+// ------------------------------------------------------------------ LJ
+// lj_interact / plj_interact (src/Pairs.F90:207-370), full list:
+//   s6 = (s/r)^6 ; p = 4e(s6^2 - s6) [- prc - frc (r - rc)] [- eshift]
+//   f = e(48 s6 - 24) s6 / r [+ frc] ; F_i -= f vd / r ; e_i += p/2
+template <int K>
+__global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x / K;
+  int lane = threadIdx.x % K;
+  bool act = i < M.end[blockIdx.x];
+  double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  if (act) {
+    const double4 xi = A.pos[i];
+    const int ti = A.type[i];
+    const int nn = min(A.nn[i], A.lcap);
+    for (int m = lane; m < nn; m += K) {
+      int j = A.list[(size_t)m * A.cap + i];
+      const PairP& P = A.prm[S.param_off + ti * S.ntypes + A.type[j]];
+      double e = P.v[0];
+      if (e == 0.0 && P.v[1] == 0.0) continue;
+      double v0, v1, v2;
+      vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+      double dr = v0 * v0 + v1 * v1 + v2 * v2;
+      if (dr > P.v[3]) continue;
+      dr = sqrt(dr);
+      double t = P.v[1] / dr;
+      double t3 = t * t * t;
+      double s6 = t3 * t3;
+      double p = 4.0 * e * (s6 * s6 - s6);
+      double f = e * (48.0 * s6 - 24.0) * s6 / dr;
+      if (P.v[7] != 0.0) {
+        p = p - P.v[4] - P.v[5] * (dr - P.v[2]);
+        f = f + P.v[5];
+      } else {
+        p = p - P.v[6];
+      }
+      double fr = f * EV_UI / dr;
+      f0 -= fr * v0;
+      f1 -= fr * v1;
+      f2 -= fr * v2;
+      ep += p;
+    }
+  }
+  f0 = lane_sum<K>(f0);
+  f1 = lane_sum<K>(f1);
+  f2 = lane_sum<K>(f2);
+  ep = lane_sum<K>(ep);
+  if (act && lane == 0) {
+    A.force[i] = make_double4(f0, f1, f2, 0.0);
+    A.epot[i] = ep * 0.5 * EV_UI;
+  }
+}
+
+template <int K>
+__global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x / K;
+  int lane = threadIdx.x % K;
+  bool act = i < M.end[blockIdx.x];
+  double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  if (act) {
+    const int4 xi = A.fxp[i];
+    const int nn = min(A.nn[i], A.lcap);
+    const float evui = (float)EV_UI;
+    for (int m = lane; m < nn; m += K) {
+      int j = A.list[(size_t)m * A.cap + i];
+      int4 xj = A.fxp[j];
+      const PairP& P = A.prm[S.param_off + xi.w * S.ntypes + xj.w];
+      float e = (float)P.v[0];
+      float rc2 = (float)P.v[3];
+      float v0, v1, v2;
+      vd_fx(S, xi, xj, v0, v1, v2);
+      float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+      if (r2 > rc2 || e == 0.0f) continue;
+      float sg = (float)P.v[1];
+      float ir2 = 1.0f / r2;
+      float t2 = sg * sg * ir2;
+      float s6 = t2 * t2 * t2;
+      float p = 4.0f * e * (s6 * s6 - s6);
+      float fr = e * (48.0f * s6 - 24.0f) * s6 * ir2;  // f / r
+      if (P.v[7] != 0.0) {
+        float dr = sqrtf(r2);
+        p = p - (float)P.v[4] - (float)P.v[5] * (dr - (float)P.v[2]);
+        fr = fr + (float)P.v[5] / dr;
+      } else {
+        p = p - (float)P.v[6];
+      }
+      fr = fr * evui;
+      f0 -= (double)(fr * v0);
+      f1 -= (double)(fr * v1);
+      f2 -= (double)(fr * v2);
+      ep += (double)p;
+    }
+  }
+  f0 = lane_sum<K>(f0);
+  f1 = lane_sum<K>(f1);
+  f2 = lane_sum<K>(f2);
+  ep = lane_sum<K>(ep);
+  if (act && lane == 0) {
+    A.force[i] = make_double4(f0, f1, f2, 0.0);
+    A.epot[i] = ep * 0.5 * EV_UI;
+  }
+}
+
+// ------------------------------------------------------------------ Tersoff
+// Tersoff 1988 with the functional form of src/Tersoff.f90:131-341 and the
+// cut-off of src/Algebra.F90:391-409, forces = exact gradient of
+// E = sum_i sum_j 1/2 fc(r_ij) [VR(r_ij) + b_ij VA(r_ij)].  One thread per
+// atom i gathers its bonds into registers, then scatters the three-body
+// terms to j and k with FP64 atomics.
+constexpr int TS_MAXB = 12;
+
+template <typename R>
+__device__ __forceinline__ R ts_fc(R r, R r1, R r2, R& dfc) {
+  if (r < r1) { dfc = R(0); return R(1); }
+  if (r > r2) { dfc = R(0); return R(0); }
+  const R pi = R(3.14159265358979323846);
+  R aux = pi * (r - (r1 + r2) * R(0.5)) / (r2 - r1);
+  R sn, cs;
+  if constexpr (sizeof(R) == 8) { sincos(aux, &sn, &cs); } else { __sincosf(aux, &sn, &cs); }
+  dfc = -cs * (pi * R(0.5)) / (r2 - r1);
+  return R(0.5) - R(0.5) * sn;
+}
+
+template <typename R, bool MIXED>
+__global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  if (i >= M.end[blockIdx.x]) return;
+  const TersoffP& T = S.ts;
+  const R r1 = R(T.R - T.D), r2 = R(T.R + T.D);
+  const R c2 = R(T.c * T.c), d2 = R(T.d * T.d), h = R(T.h);
+  const R nexp = R(T.n);
+  const R btnp = R(pow(T.beta, T.n));
+  const R Aa = R(T.A * EV_UI), Bb = R(T.B * EV_UI), l1 = R(T.l1), l2 = R(T.l2);
+  const R chi = R(T.chi);
+  int bj[TS_MAXB];
+  R br[TS_MAXB], bu[TS_MAXB][3], bfc[TS_MAXB], bdfc[TS_MAXB];
+  int nb = 0;
+  const int nn = min(A.nn[i], A.lcap);
+  const double4 xi = A.pos[i];
+  const int4 qi = A.fxp[i];
+  for (int m = 0; m < nn; m++) {
+    int j = A.list[(size_t)m * A.cap + i];
+    R v0, v1, v2;
+    if constexpr (MIXED) {
+      float a, b, c;
+      vd_fx(S, qi, A.fxp[j], a, b, c);
+      v0 = a; v1 = b; v2 = c;
+    } else {
+      double a, b, c;
+      vd_fp64(S, xi, A.pos[j], a, b, c);
+      v0 = a; v1 = b; v2 = c;
+    }
+    R rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    if (rr > r2) continue;
+    if (nb == TS_MAXB) {
+      atomicOr(&A.st[s].status, ST_OVERFLOW);
+      break;
+    }
+    bj[nb] = j;
+    br[nb] = rr;
+    R ir = R(1) / rr;
+    bu[nb][0] = v0 * ir; bu[nb][1] = v1 * ir; bu[nb][2] = v2 * ir;
+    bfc[nb] = ts_fc<R>(rr, r1, r2, bdfc[nb]);
+    nb++;
+  }
+  double ei = 0.0;
+  double fi0 = 0, fi1 = 0, fi2 = 0;
+  for (int a = 0; a < nb; a++) {
+    const R rij = br[a];
+    const R* u = bu[a];
+    R zij = R(0);
+    for (int b = 0; b < nb; b++) {
+      if (b == a) continue;
+      R ct = u[0] * bu[b][0] + u[1] * bu[b][1] + u[2] * bu[b][2];
+      R hc = h - ct;
+      R g = R(1) + c2 / d2 - c2 / (d2 + hc * hc);
+      zij += bfc[b] * g;
+    }
+    R vr = Aa * exp(-l1 * rij), dvr = -l1 * vr;
+    R va = -Bb * exp(-l2 * rij), dva = -l2 * va;
+    R bij, dbdz;
+    if (zij > R(1.0e-15)) {
+      R zn = pow(zij, nexp);
+      R aux = R(1) / (R(1) + btnp * zn);
+      bij = chi * pow(aux, R(0.5) / nexp);
+      dbdz = R(-0.5) * bij * aux * btnp * zn / zij;
+    } else {
+      bij = chi;
+      dbdz = R(0);
+    }
+    ei += (double)(R(0.5) * bfc[a] * (vr + bij * va));
+    R dV = R(0.5) * (bdfc[a] * (vr + bij * va) + bfc[a] * (dvr + bij * dva));
+    double g0 = (double)(dV * u[0]), g1 = (double)(dV * u[1]), g2 = (double)(dV * u[2]);
+    fi0 += g0; fi1 += g1; fi2 += g2;
+    double* fj = reinterpret_cast<double*>(&A.force[bj[a]]);
+    atomicAdd(fj + 0, -g0);
+    atomicAdd(fj + 1, -g1);
+    atomicAdd(fj + 2, -g2);
+    if (dbdz == R(0)) continue;
+    R pre = R(0.5) * bfc[a] * va * dbdz;
+    double gj0 = 0, gj1 = 0, gj2 = 0;
+    for (int b = 0; b < nb; b++) {
+      if (b == a) continue;
+      const R* w = bu[b];
+      R rik = br[b];
+      R ct = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
+      R hc = h - ct;
+      R den = d2 + hc * hc;
+      R g = R(1) + c2 / d2 - c2 / den;
+      R dg = R(-2) * c2 * hc / (den * den);
+      R ka = pre * bfc[b] * dg / rij;
+      R kb = pre * dg / rik * bfc[b];
+      R kc = pre * bdfc[b] * g;
+      double gk0 = (double)(kb * (u[0] - ct * w[0]) + kc * w[0]);
+      double gk1 = (double)(kb * (u[1] - ct * w[1]) + kc * w[1]);
+      double gk2 = (double)(kb * (u[2] - ct * w[2]) + kc * w[2]);
+      gj0 += (double)(ka * (w[0] - ct * u[0]));
+      gj1 += (double)(ka * (w[1] - ct * u[1]));
+      gj2 += (double)(ka * (w[2] - ct * u[2]));
+      double* fk = reinterpret_cast<double*>(&A.force[bj[b]]);
+      atomicAdd(fk + 0, -gk0);
+      atomicAdd(fk + 1, -gk1);
+      atomicAdd(fk + 2, -gk2);
+      fi0 += gk0; fi1 += gk1; fi2 += gk2;
+    }
+    atomicAdd(fj + 0, -gj0);
+    atomicAdd(fj + 1, -gj1);
+    atomicAdd(fj + 2, -gj2);
+    fi0 += gj0; fi1 += gj1; fi2 += gj2;
+  }
+  double* f = reinterpret_cast<double*>(&A.force[i]);
+  atomicAdd(f + 0, fi0);
+  atomicAdd(f + 1, fi1);
+  atomicAdd(f + 2, fi2);
+  A.epot[i] = ei;
+}
+
+// interleaved [x1,y1,z1,...] staging <-> double4 arena slots
+__global__ void k_unpack3(const double* __restrict__ src, double4* __restrict__ dst, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0);
+}
+__global__ void k_pack3(const double4* __restrict__ src, double* __restrict__ dst, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    double4 v = src[i];
+    dst[3 * i] = v.x;
+    dst[3 * i + 1] = v.y;
+    dst[3 * i + 2] = v.z;
+  }
+}
+
+__global__ void k_zero_force(Arena A, BlockMap M) {
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  if (i < M.end[blockIdx.x]) A.force[i] = make_double4(0, 0, 0, 0);
+}
+
+// ------------------------------------------------------------------ integrators
+// integration_stepa (src/Integration.F90:243-262): the algorithm's half
+// step, do_pbc (Set_Properties.f90:444-470), then the displacement test of
+// test_update fused in (the list decision for this step's interact).
+__global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  SysState& st = A.st[s];
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  bool act = i < M.end[blockIdx.x];
+  bool frozen = S.integ == IT_FIRE && st.fire_done;
+  double2 t = make_double2(1.e-16, 1.e-16);
+  if (act && S.integ != IT_NONE && !frozen) {
+    double4 x = A.pos[i], v = A.vel[i], a = A.acel[i];
+    const double2 mi = A.minv[i];
+    if (S.integ == IT_VV || S.integ == IT_FIRE) {
+      // velocity_verlet_a (Integration.F90:1150-1168)
+      const double dt = S.integ == IT_FIRE ? st.fire_dt : S.dt;
+      if (S.integ == IT_FIRE && st.fire_zero) v = make_double4(0, 0, 0, 0);
+      const double4 F = A.force[i];
+      const double adv = dt * 0.5, adx = adv * dt;
+      a.x = F.x * mi.x; a.y = F.y * mi.x; a.z = F.z * mi.x;
+      x.x = x.x + dt * v.x + adx * a.x;
+      x.y = x.y + dt * v.y + adx * a.y;
+      x.z = x.z + dt * v.z + adx * a.z;
+      v.x = v.x + adv * a.x;
+      v.y = v.y + adv * a.y;
+      v.z = v.z + adv * a.z;
+      A.acel[i] = a;
+    } else if (S.integ == IT_ERMAK) {
+      // ermak_a (Integration.F90:963-1011)
+      double r[6];
+      if (S.use_ext_normals) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) r[k] = A.ext_normals[(size_t)6 * i + k];
+      } else {
+        const uint32_t loc = (uint32_t)(i - S.off);
+        const uint64_t step = st.step;
+        const uint2 key = make_uint2((uint32_t)S.seed, (uint32_t)(S.seed >> 32));
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          uint4 c = make_uint4(loc, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)k);
+          normals2(philox10(c, key), r[2 * k], r[2 * k + 1]);
+        }
+      }
+      const double f_lan = S.skt * mi.y;
+      const double pr = f_lan * S.sdr, pv = f_lan * S.sdv;
+      double4 vv;
+      vv.x = pv * (S.crv1 * r[0] + S.crv2 * r[1]);
+      vv.y = pv * (S.crv1 * r[2] + S.crv2 * r[3]);
+      vv.z = pv * (S.crv1 * r[4] + S.crv2 * r[5]);
+      vv.w = 0.0;
+      const double c2dt = S.cc2 * S.dt;
+      x.x = x.x + S.cc1 * v.x + c2dt * a.x + pr * r[0];
+      x.y = x.y + S.cc1 * v.y + c2dt * a.y + pr * r[2];
+      x.z = x.z + S.cc1 * v.z + c2dt * a.z + pr * r[4];
+      A.vel_v[i] = vv;
+    }
+    // do_pbc_1: a single wrap into [0, box)
+    if (S.boxed) {
+      if (S.pbc[0]) { if (x.x >= S.L[0]) x.x = x.x - S.L[0]; else if (x.x < 0.0) x.x = x.x + S.L[0]; }
+      if (S.pbc[1]) { if (x.y >= S.L[1]) x.y = x.y - S.L[1]; else if (x.y < 0.0) x.y = x.y + S.L[1]; }
+      if (S.pbc[2]) { if (x.z >= S.L[2]) x.z = x.z - S.L[2]; else if (x.z < 0.0) x.z = x.z + S.L[2]; }
+    }
+    A.pos[i] = x;
+    A.vel[i] = v;
+    if (S.prec == PREC_MIXED || S.ff == FF_TERSOFF) {
+      int bad = 0;
+      write_fx(A, S, i, x, A.type[i], bad);
+      if (bad) atomicOr(&st.status, ST_LOST);
+    }
+    t.x = disp2(S, x, A.pos_old[i]);
+    if (!(t.x == t.x)) atomicOr(&st.status, ST_NAN);
+  }
+  t = block_top2(t);
+  if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
+  if (last_block(M, A.st, s, &st.ticket)) {
+    if (threadIdx.x == 0) {
+      double2 w = make_double2(1.e-16, 1.e-16);
+      int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+      for (int b = 0; b < nb; b++) w = top2_merge(w, __ldcg(&A.blk_top2[b0 + b]));
+      int rb = __dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)) > S.skin;
+      if (frozen) rb = 0;
+      st.rebuild = rb;
+      if (rb) atomicOr(A.any_rebuild, 1);
+      if (S.integ == IT_ERMAK && !S.use_ext_normals) st.step++;
+      if (S.integ == IT_FIRE) st.fire_zero = 0;
+    }
+  }
+}
+
+// integration_stepb (src/Integration.F90:264-301): velocity_verlet_b
+// (:1171-1186) or ermak_b (:1013-1031); FIRE adds P = sum v.F, the per-atom
+// mixing v = (1-a) v + a |v| F/|F| (FIRE.f90:99-114, with |v|) and the
+// dt / alpha control (:116-131) in the system's last block.
+__global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  const SysDev& S = A.sys[s];
+  SysState& st = A.st[s];
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  bool act = i < M.end[blockIdx.x];
+  bool frozen = S.integ == IT_FIRE && st.fire_done;
+  double P = 0.0, f2max = 0.0;
+  if (act && S.integ != IT_NONE && !frozen) {
+    double4 v = A.vel[i], a = A.acel[i];
+    const double4 F = A.force[i];
+    const double om = A.minv[i].x;
+    if (S.integ == IT_VV || S.integ == IT_FIRE) {
+      const double dt = S.integ == IT_FIRE ? st.fire_dt : S.dt;
+      const double adv = dt * 0.5;
+      a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+      v.x = v.x + adv * a.x;
+      v.y = v.y + adv * a.y;
+      v.z = v.z + adv * a.z;
+      if (S.integ == IT_FIRE) {
+        P = v.x * F.x + v.y * F.y + v.z * F.z;
+        double fn2 = F.x * F.x + F.y * F.y + F.z * F.z;
+        f2max = fn2;
+        double vn = sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+        double fn = sqrt(fn2);
+        double al = st.fire_alpha;
+        double mixf = fn > 0.0 ? al * vn / fn : 0.0;
+        v.x = v.x * (1.0 - al) + mixf * F.x;
+        v.y = v.y * (1.0 - al) + mixf * F.y;
+        v.z = v.z * (1.0 - al) + mixf * F.z;
+      }
+    } else if (S.integ == IT_ERMAK) {
+      const double4 vv = A.vel_v[i];
+      const double c12 = S.cc1 - S.cc2;
+      v.x = S.cc0 * v.x + c12 * a.x + S.cc2 * F.x * om + vv.x;
+      v.y = S.cc0 * v.y + c12 * a.y + S.cc2 * F.y * om + vv.y;
+      v.z = S.cc0 * v.z + c12 * a.z + S.cc2 * F.z * om + vv.z;
+      a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+    }
+    A.vel[i] = v;
+    A.acel[i] = a;
+  }
+  if (S.integ != IT_FIRE) return;  // uniform per block
+  double Pb = block_sum(P);
+  double Fb = block_max(f2max);
+  if (threadIdx.x == 0) A.blk_red[2 * blockIdx.x] = Pb, A.blk_red[2 * blockIdx.x + 1] = Fb;
+  if (last_block(M, A.st, s, &st.ticket2)) {
+    if (threadIdx.x == 0 && !frozen) {
+      int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+      double Pt = 0.0, Ft = 0.0;
+      for (int b = 0; b < nb; b++) {
+        Pt += __ldcg(&A.blk_red[2 * (b0 + b)]);
+        Ft = fmax(Ft, __ldcg(&A.blk_red[2 * (b0 + b) + 1]));
+      }
+      st.fire_P = Pt;
+      st.fmax2 = Ft;
+      st.fire_iter++;
+      const double alpha0 = 0.1, finc = 1.1, fdec = 0.5, falf = 0.99;
+      if (Pt > 0.0) {
+        st.fire_np++;
+        if (st.fire_np > 5) {
+          st.fire_dt = fmin(st.fire_dt * finc, S.fire_dtmax);
+          st.fire_alpha = st.fire_alpha * falf;
+        }
+      } else {
+        st.fire_np = 0;
+        st.fire_dt = st.fire_dt * fdec;
+        st.fire_alpha = alpha0;
+        st.fire_zero = 1;  // velocities are zeroed by the next step_a
+      }
+      double fm = sqrt(Ft) * c_ui_ev();
+      if (fm < S.fire_fmax || st.fire_iter >= S.fire_maxit) st.fire_done = 1;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ reductions
+// Per-system sums in a fixed order (one block per system): Epot, sum m v,
+// total mass, then Ekin with the centre-of-mass velocity removed
+// (inq_kin_energy, src/Inq_Properties.F90:399-422) and max |F|^2.
+__global__ void k_sys_reduce(Arena A, const int* sys, int nsys, double* out) {
+  int s = sys[blockIdx.x];
+  const SysDev& S = A.sys[s];
+  double ep = 0, mx = 0, my = 0, mz = 0, mt = 0, f2 = 0;
+  for (int i = S.off + threadIdx.x; i < S.off + S.n; i += BLOCK) {
+    ep += A.epot[i];
+    double m = A.mass[i];
+    double4 v = A.vel[i];
+    mx += m * v.x; my += m * v.y; mz += m * v.z; mt += m;
+    double4 F = A.force[i];
+    f2 = fmax(f2, F.x * F.x + F.y * F.y + F.z * F.z);
+  }
+  ep = block_sum(ep);
+  __shared__ double cm[4];
+  double bx = block_sum(mx), by = block_sum(my), bz = block_sum(mz), bm = block_sum(mt);
+  double bf = block_max(f2);
+  if (threadIdx.x == 0) {
+    if (S.n == 1) {
+      double4 v = A.vel[S.off];
+      cm[0] = v.x; cm[1] = v.y; cm[2] = v.z;
+    } else {
+      cm[0] = bx / bm; cm[1] = by / bm; cm[2] = bz / bm;
+    }
+  }
+  __syncthreads();
+  double ek = 0.0;
+  for (int i = S.off + threadIdx.x; i < S.off + S.n; i += BLOCK) {
+    double4 v = A.vel[i];
+    double a = v.x - cm[0], b = v.y - cm[1], c = v.z - cm[2];
+    ek += (a * a + b * b + c * c) * A.mass[i];
+  }
+  ek = block_sum(ek);
+  if (threadIdx.x == 0) {
+    out[4 * blockIdx.x + 0] = ep;
+    out[4 * blockIdx.x + 1] = ek * 0.5;
+    out[4 * blockIdx.x + 2] = bf;
+    out[4 * blockIdx.x + 3] = (double)A.st[s].status;
+  }
+}
+
+}  // namespace gg

@@ -1,0 +1,377 @@
+"""ctypes binding of libgemsgpu.so (the C ABI declared in include/gemsgpu.h).
+
+`System` mirrors a GEMS group carrying one interaction group (intergroup,
+src/Neighbour.F90:93-208) and one integrator (integrate,
+src/Integration.F90:32-49): the setters take the same arguments as the
+reference's `interact ... under lj|tb|tersoff` and `evolve v_verlet|ermak`
+commands, `interact()` is the reference's interact(), `stepa()/stepb()` are
+integration_stepa/b and `dinamica()` is dinamic().  Every call runs on the
+GPU through the C ABI; there is no CPU fallback, and importing this module
+without the built library raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libgemsgpu.so")
+
+OK = 0
+ERRORS = {-1: "ERR_ARG", -2: "ERR_OOM", -3: "ERR_CUDA", -4: "ERR_OVERFLOW", -5: "ERR_LOST",
+          -6: "ERR_NAN", -7: "ERR_STATE", -8: "ERR_TIMEOUT", -9: "ERR_NODEV", -10: "ERR_FULL"}
+PREC_FP64, PREC_MIXED = 0, 1
+
+# GEMS internal units (src/Constants.F90:101-175)
+UI_EV = 1.0e2 * 1.0e2 * 1.6605402e-27 * (1.0 / 1.60219e-19)
+EV_UI = 1.0 / UI_EV
+KB_UI = 8.617385e-05 * EV_UI
+
+_lib = None
+_d, _i, _p, _l = ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+_SIGS = {
+    "gemsgpu_version": (ctypes.c_char_p, []),
+    "gemsgpu_create": (_i, [_i, _l, _i, ctypes.POINTER(_p)]),
+    "gemsgpu_destroy": (_i, [_p]),
+    "gemsgpu_last_error": (_i, [_p, ctypes.c_char_p, _i]),
+    "gemsgpu_system_create": (_i, [_p, _i, _i, _ip]),
+    "gemsgpu_system_destroy": (_i, [_p, _i]),
+    "gemsgpu_upload": (_i, [_p, _i, _dp, _dp, _dp, _ip]),
+    "gemsgpu_set_positions": (_i, [_p, _i, _dp]),
+    "gemsgpu_set_velocities": (_i, [_p, _i, _dp]),
+    "gemsgpu_set_accelerations": (_i, [_p, _i, _dp]),
+    "gemsgpu_download": (_i, [_p, _i, _dp, _dp, _dp, _dp]),
+    "gemsgpu_download_acel": (_i, [_p, _i, _dp]),
+    "gemsgpu_set_box": (_i, [_p, _i, _i, _dp, _ip]),
+    "gemsgpu_set_skin": (_i, [_p, _i, _d]),
+    "gemsgpu_set_list_mode": (_i, [_p, _i, _i]),
+    "gemsgpu_set_skin_mode": (_i, [_p, _i, _i]),
+    "gemsgpu_set_precision": (_i, [_p, _i, _i]),
+    "gemsgpu_set_lj": (_i, [_p, _i, _i, _i, _d, _d, _d, _i, _d]),
+    "gemsgpu_set_smatb": (_i, [_p, _i, _i, _i, _d, _d, _d, _d, _d, _d, _d]),
+    "gemsgpu_set_tersoff": (_i, [_p, _i, _dp]),
+    "gemsgpu_forces": (_i, [_p, _i, _dp, _ip]),
+    "gemsgpu_update": (_i, [_p, _i]),
+    "gemsgpu_get_list": (_i, [_p, _i, _ip, _ip, _i, _ip]),
+    "gemsgpu_get_nupd": (_i, [_p, _i, ctypes.POINTER(_l)]),
+    "gemsgpu_set_vv": (_i, [_p, _i, _d]),
+    "gemsgpu_set_ermak": (_i, [_p, _i, _d, _d, _d, ctypes.c_uint64]),
+    "gemsgpu_set_ermak_normals": (_i, [_p, _i, _dp]),
+    "gemsgpu_set_fire": (_i, [_p, _i, _d, _d]),
+    "gemsgpu_step_a": (_i, [_p, _i]),
+    "gemsgpu_step_b": (_i, [_p, _i]),
+    "gemsgpu_md_steps": (_i, [_p, _i, _i]),
+    "gemsgpu_energy": (_i, [_p, _i, _dp, _dp, _dp]),
+    "gemsgpu_fmax": (_i, [_p, _i, _dp]),
+    "gemsgpu_batch_md_steps": (_i, [_p, _ip, _i, _i]),
+    "gemsgpu_batch_fire": (_i, [_p, _ip, _i, _d, _i, _ip]),
+    "gemsgpu_batch_energy": (_i, [_p, _ip, _i, _dp, _dp, _dp]),
+    "gemsgpu_get_launch_count": (_i, [_p, ctypes.POINTER(_l)]),
+    "gemsgpu_get_stream": (_i, [_p, ctypes.POINTER(_p)]),
+    "gemsgpu_time_kernels": (_i, [_p, _i, _i, _dp]),
+}
+
+
+def declared_symbols():
+    """Every entry point this binding expects the library to export."""
+    return sorted(_SIGS)
+
+
+def lib():
+    """Load libgemsgpu.so; raises if it was not built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise ImportError("libgemsgpu.so is not built: run __graft_entry__.build() "
+                          "(nvcc, sm_100a); there is no CPU fallback")
+    L = ctypes.CDLL(LIBPATH)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+class GemsGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "?"), code, msg))
+        self.code = code
+
+
+def _ptr(a, ct=ctypes.c_double):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    if n is not None and a.size != n:
+        raise ValueError("expected %d values, got %d" % (n, a.size))
+    return a
+
+
+class Context:
+    """One CUDA stream + HBM arena on one device (gemsgpu_ctx)."""
+
+    def __init__(self, device=0, max_atoms=0, max_systems=16):
+        h = _p()
+        rc = lib().gemsgpu_create(int(device), int(max_atoms), int(max_systems), ctypes.byref(h))
+        if rc != OK:
+            raise GemsGpuError(rc, "gemsgpu_create failed on device %d" % device)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gemsgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        if rc != OK:
+            buf = ctypes.create_string_buffer(512)
+            lib().gemsgpu_last_error(self.h, buf, 512)
+            raise GemsGpuError(rc, buf.value.decode(errors="replace"))
+
+    # batches ---------------------------------------------------------------
+    def _ids(self, systems):
+        return np.ascontiguousarray([s.sid for s in systems], dtype=np.int32)
+
+    def batch_md_steps(self, systems, nsteps):
+        ids = self._ids(systems)
+        self.check(lib().gemsgpu_batch_md_steps(self.h, _ptr(ids, ctypes.c_int), len(ids), int(nsteps)))
+
+    def batch_fire(self, systems, fmax, maxit):
+        ids = self._ids(systems)
+        it = np.zeros(len(ids), dtype=np.int32)
+        self.check(lib().gemsgpu_batch_fire(self.h, _ptr(ids, ctypes.c_int), len(ids), float(fmax),
+                                            int(maxit), _ptr(it, ctypes.c_int)))
+        return it
+
+    def stream_ptr(self):
+        """cudaStream_t of this context (int), e.g. for torch.cuda.ExternalStream."""
+        v = _p()
+        self.check(lib().gemsgpu_get_stream(self.h, ctypes.byref(v)))
+        return v.value or 0
+
+    def launches(self):
+        v = ctypes.c_int64()
+        self.check(lib().gemsgpu_get_launch_count(self.h, ctypes.byref(v)))
+        return v.value
+
+    def batch_energy(self, systems):
+        ids = self._ids(systems)
+        n = len(ids)
+        ep, ek, t = np.zeros(n), np.zeros(n), np.zeros(n)
+        self.check(lib().gemsgpu_batch_energy(self.h, _ptr(ids, ctypes.c_int), n, _ptr(ep), _ptr(ek), _ptr(t)))
+        return ep, ek, t
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context()
+    return _default_ctx
+
+
+class System:
+    """A GEMS system on the GPU; setter names follow oracle.System."""
+
+    def __init__(self, pos, mass, types=None, ntypes=1, ctx=None, vel=None):
+        self.ctx = ctx or default_context()
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        self.n = pos.shape[0]
+        sid = ctypes.c_int()
+        self.ctx.check(lib().gemsgpu_system_create(self.ctx.h, self.n, int(ntypes), ctypes.byref(sid)))
+        self.sid = sid.value
+        self.ntypes = ntypes
+        m = _f64(np.broadcast_to(np.asarray(mass, dtype=np.float64), (self.n,)))
+        t = None if types is None else np.ascontiguousarray(types, dtype=np.int32)
+        v = None if vel is None else _f64(vel, 3 * self.n)
+        self._mass = m
+        self.ctx.check(lib().gemsgpu_upload(self.ctx.h, self.sid, _ptr(_f64(pos)), _ptr(v), _ptr(m),
+                                            _ptr(t, ctypes.c_int)))
+
+    def destroy(self):
+        if self.sid is not None:
+            self.ctx.check(lib().gemsgpu_system_destroy(self.ctx.h, self.sid))
+            self.sid = None
+
+    def _c(self, rc):
+        self.ctx.check(rc)
+
+    # state -------------------------------------------------------------------
+    def set_pos(self, x):
+        self._c(lib().gemsgpu_set_positions(self.ctx.h, self.sid, _ptr(_f64(x, 3 * self.n))))
+
+    def set_vel(self, v):
+        self._c(lib().gemsgpu_set_velocities(self.ctx.h, self.sid, _ptr(_f64(v, 3 * self.n))))
+
+    def set_acel(self, a):
+        self._c(lib().gemsgpu_set_accelerations(self.ctx.h, self.sid, _ptr(_f64(a, 3 * self.n))))
+
+    def _down(self, which):
+        out = np.empty(3 * self.n if which != 3 else self.n, dtype=np.float64)
+        args = [None, None, None, None]
+        args[which] = _ptr(out)
+        self._c(lib().gemsgpu_download(self.ctx.h, self.sid, *args))
+        return out.reshape(self.n, 3) if which != 3 else out
+
+    @property
+    def pos(self):
+        return self._down(0)
+
+    @property
+    def vel(self):
+        return self._down(1)
+
+    @property
+    def force(self):
+        return self._down(2)
+
+    @property
+    def epot_atoms(self):
+        return self._down(3)
+
+    @property
+    def acel(self):
+        out = np.empty(3 * self.n, dtype=np.float64)
+        self._c(lib().gemsgpu_download_acel(self.ctx.h, self.sid, _ptr(out)))
+        return out.reshape(self.n, 3)
+
+    # setup -------------------------------------------------------------------
+    def set_box(self, L=None, pbc=(True, True, True)):
+        if L is None:
+            self._c(lib().gemsgpu_set_box(self.ctx.h, self.sid, 0, None, None))
+            return
+        Lb = _f64(L, 3)
+        pb = np.asarray([1 if b else 0 for b in pbc], dtype=np.int32)
+        self._c(lib().gemsgpu_set_box(self.ctx.h, self.sid, 1, _ptr(Lb), _ptr(pb, ctypes.c_int)))
+
+    def set_skin(self, skin):
+        self._c(lib().gemsgpu_set_skin(self.ctx.h, self.sid, float(skin)))
+
+    def set_skin_mode(self, mic):
+        """mic=False: the reference's raw-displacement skin test."""
+        self._c(lib().gemsgpu_set_skin_mode(self.ctx.h, self.sid, 1 if mic else 0))
+
+    def set_half(self, half):
+        self._c(lib().gemsgpu_set_list_mode(self.ctx.h, self.sid, 1 if half else 0))
+
+    def set_precision(self, prec):
+        self._c(lib().gemsgpu_set_precision(self.ctx.h, self.sid, int(prec)))
+
+    def set_lj(self, e, s, rc, ti=0, tj=0, shifted_force=False, eshift=0.0):
+        self._c(lib().gemsgpu_set_lj(self.ctx.h, self.sid, ti, tj, e, s, rc, 1 if shifted_force else 0, eshift))
+
+    def set_smatb(self, A, xi, p, q, r0, rci, rce, ti=0, tj=0):
+        self._c(lib().gemsgpu_set_smatb(self.ctx.h, self.sid, ti, tj, A, xi, p, q, r0, rci, rce))
+
+    def set_tersoff(self, prm):
+        a = _f64(prm, 12)
+        self._c(lib().gemsgpu_set_tersoff(self.ctx.h, self.sid, _ptr(a)))
+
+    # compute -----------------------------------------------------------------
+    def interact(self):
+        """interact(): forces, per-atom energies; returns Epot (internal units)."""
+        e = ctypes.c_double()
+        self._c(lib().gemsgpu_forces(self.ctx.h, self.sid, ctypes.byref(e), None))
+        return e.value
+
+    def update(self):
+        self._c(lib().gemsgpu_update(self.ctx.h, self.sid))
+
+    @property
+    def nupd(self):
+        v = ctypes.c_int64()
+        self._c(lib().gemsgpu_get_nupd(self.ctx.h, self.sid, ctypes.byref(v)))
+        return v.value
+
+    def neighbour_list(self):
+        need = ctypes.c_int()
+        nn = np.empty(self.n, dtype=np.int32)
+        self._c(lib().gemsgpu_get_list(self.ctx.h, self.sid, _ptr(nn, ctypes.c_int), None, 0, ctypes.byref(need)))
+        cap = max(need.value, 1)
+        lst = np.empty(cap * self.n, dtype=np.int32)
+        self._c(lib().gemsgpu_get_list(self.ctx.h, self.sid, _ptr(nn, ctypes.c_int), _ptr(lst, ctypes.c_int),
+                                       cap, ctypes.byref(need)))
+        return nn, lst.reshape(cap, self.n)
+
+    def pair_set(self):
+        nn, lst = self.neighbour_list()
+        i_idx = np.repeat(np.arange(self.n, dtype=np.int64), nn)
+        j_idx = np.concatenate([lst[:c, i].astype(np.int64) for i, c in enumerate(nn)]) if self.n else np.zeros(0, np.int64)
+        return np.sort(i_idx * self.n + j_idx)
+
+    # integrators -------------------------------------------------------------
+    def set_vv(self, dt):
+        self._c(lib().gemsgpu_set_vv(self.ctx.h, self.sid, float(dt)))
+
+    def set_ermak(self, dt, gama, temp, seed=12345):
+        self._c(lib().gemsgpu_set_ermak(self.ctx.h, self.sid, float(dt), float(gama), float(temp), int(seed)))
+
+    def set_ermak_normals(self, nrm):
+        a = None if nrm is None else _f64(nrm, 6 * self.n)
+        self._c(lib().gemsgpu_set_ermak_normals(self.ctx.h, self.sid, _ptr(a)))
+
+    def set_fire(self, dt0, dtmax):
+        self._c(lib().gemsgpu_set_fire(self.ctx.h, self.sid, float(dt0), float(dtmax)))
+
+    def stepa(self):
+        self._c(lib().gemsgpu_step_a(self.ctx.h, self.sid))
+
+    def stepb(self):
+        self._c(lib().gemsgpu_step_b(self.ctx.h, self.sid))
+
+    def md_steps(self, n):
+        self._c(lib().gemsgpu_md_steps(self.ctx.h, self.sid, int(n)))
+
+    def energy(self):
+        """(Epot eV, Ekin eV with CM removed, T K)."""
+        ep, ek, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._c(lib().gemsgpu_energy(self.ctx.h, self.sid, ctypes.byref(ep), ctypes.byref(ek), ctypes.byref(t)))
+        return ep.value, ek.value, t.value
+
+    def kin(self):
+        _, ek, t = self.energy()
+        return ek * EV_UI, t
+
+    def epot_sum(self):
+        return self.energy()[0] * EV_UI
+
+    def time_kernels(self, reps=20):
+        """Mean ms of (first force kernel, second force kernel, list rebuild)."""
+        out = np.zeros(3)
+        self._c(lib().gemsgpu_time_kernels(self.ctx.h, self.sid, int(reps), _ptr(out)))
+        return out
+
+    def fmax(self):
+        v = ctypes.c_double()
+        self._c(lib().gemsgpu_fmax(self.ctx.h, self.sid, ctypes.byref(v)))
+        return v.value
+
+    def dinamica(self, nsteps, each):
+        """dinamic(): interact once, then nsteps on the device; every `each`
+        steps one row (Epot, Ekin, Etot in eV, T in K)."""
+        self.interact()
+        rows = []
+        done = 0
+        while done < nsteps:
+            k = min(each, nsteps - done) if each > 0 else nsteps
+            self.md_steps(k)
+            done += k
+            if each > 0 and done % each == 0:
+                ep, ek, t = self.energy()
+                rows.append([ep, ek, ep + ek, t])
+        return np.array(rows).reshape(-1, 4)

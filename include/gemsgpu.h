@@ -1,0 +1,216 @@
+/*
+ * gemsgpu.h -- C ABI of the B200 (sm_100a) force/neighbour path of GEMS.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes.  A
+ * Fortran `bind(C)` interface module binds these names directly (see the
+ * integration notes shipped with this library).  Every entry point replaces
+ * one reference routine or plug point, cited as file:line within
+ * alexispaz/GEMS.
+ *
+ * Units are GEMS internal units (Angstrom, uma, ps; energy uma*A^2/ps^2)
+ * unless a function says eV.  Per-atom vectors use the GEMS interleaved
+ * layout [x1, y1, z1, x2, ...] of group_switch_vectorial
+ * (src/Groups.F90:553-585).  The library owns all device memory; the caller
+ * owns host buffers, which are copied and never retained past a call.
+ *
+ * Status codes: 0 on success, a negative GEMSGPU_ERR_* otherwise; the text of
+ * the last error of a context is returned by gemsgpu_last_error.  No entry
+ * point aborts, traps or exits the process.
+ *
+ * Threading: one host thread per context at a time; every context owns one
+ * CUDA stream and all of its work is ordered on that stream.
+ */
+#ifndef GEMSGPU_H
+#define GEMSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GEMSGPU_OK 0
+#define GEMSGPU_ERR_ARG (-1)      /* bad argument / unknown handle          */
+#define GEMSGPU_ERR_OOM (-2)      /* device allocation failed               */
+#define GEMSGPU_ERR_CUDA (-3)     /* CUDA runtime error                      */
+#define GEMSGPU_ERR_OVERFLOW (-4) /* neighbour capacity exceeded, not healed */
+#define GEMSGPU_ERR_LOST (-5)     /* atom outside the cell grid of a box     */
+#define GEMSGPU_ERR_NAN (-6)      /* non-finite position or force            */
+#define GEMSGPU_ERR_STATE (-7)    /* call out of order (no force field, ...) */
+#define GEMSGPU_ERR_TIMEOUT (-8)  /* bounded device wait expired             */
+#define GEMSGPU_ERR_NODEV (-9)    /* no usable CUDA device                   */
+#define GEMSGPU_ERR_FULL (-10)    /* arena has no room for the request       */
+
+/* force-field kinds (the `interact ... under <pot>` keywords) */
+#define GEMSGPU_FF_NONE 0
+#define GEMSGPU_FF_LJ 1      /* lj / plj, Pairs.F90:198-370      */
+#define GEMSGPU_FF_SMATB 2   /* tb, TB.F90:106-586               */
+#define GEMSGPU_FF_TERSOFF 3 /* tersoff, Tersoff.f90:131-341     */
+
+/* integrators (the `evolve <alg>` keywords) */
+#define GEMSGPU_INT_NONE 0
+#define GEMSGPU_INT_VV 1    /* v_verlet, Integration.F90:1150-1186 */
+#define GEMSGPU_INT_ERMAK 2 /* ermak, Integration.F90:909-1031     */
+#define GEMSGPU_INT_FIRE 3  /* fire, FIRE.f90:40-141 (intent)      */
+
+/* arithmetic of the force kernels */
+#define GEMSGPU_PREC_FP64 0  /* plain FP64: the drop-in                  */
+#define GEMSGPU_PREC_MIXED 1 /* FP32 pair math, FP64 accumulation        */
+
+typedef struct gemsgpu_ctx gemsgpu_ctx;
+
+/* ------------------------------------------------------------ context */
+
+/* Create a context on CUDA device `device`.  max_atoms / max_systems size
+ * the HBM arena (0 = grow on demand). */
+int gemsgpu_create(int device, int64_t max_atoms, int max_systems,
+                   gemsgpu_ctx** out);
+int gemsgpu_destroy(gemsgpu_ctx* ctx);
+/* Copy the last error message of ctx (NUL-terminated) into buf. */
+int gemsgpu_last_error(gemsgpu_ctx* ctx, char* buf, int len);
+/* Library version string (static storage). */
+const char* gemsgpu_version(void);
+
+/* ------------------------------------------------------------ systems */
+
+/* A system is one GEMS group with its interaction group(s) and integrator.
+ * Replaces the intergroup constructor (src/Neighbour.F90:255-295) and the
+ * atom arrays of group_switch_vectorial (src/Groups.F90:553-585). */
+int gemsgpu_system_create(gemsgpu_ctx* ctx, int natoms, int ntypes, int* sys);
+int gemsgpu_system_destroy(gemsgpu_ctx* ctx, int sys);
+
+/* Copy positions (3n), velocities (3n, may be NULL = zero), masses (n) and
+ * 0-based types (n, may be NULL = all 0) to the device.  Masses follow
+ * set_mass (src/Set_Properties.f90:168-191).  acel is reset to zero, as for
+ * freshly created atoms (src/Atoms.F90:184). */
+int gemsgpu_upload(gemsgpu_ctx* ctx, int sys, const double* pos,
+                   const double* vel, const double* mass, const int* type);
+/* Replace positions only (dinamic_from_xyz, src/Programs.f90:38-85). */
+int gemsgpu_set_positions(gemsgpu_ctx* ctx, int sys, const double* pos);
+/* Replace velocities / accelerations only. */
+int gemsgpu_set_velocities(gemsgpu_ctx* ctx, int sys, const double* vel);
+int gemsgpu_set_accelerations(gemsgpu_ctx* ctx, int sys, const double* acel);
+/* Copy state back; any pointer may be NULL.  epot_atoms is per atom (n). */
+int gemsgpu_download(gemsgpu_ctx* ctx, int sys, double* pos, double* vel,
+                     double* force, double* epot_atoms);
+int gemsgpu_download_acel(gemsgpu_ctx* ctx, int sys, double* acel);
+
+/* box_setvars (src/Program_Types.F90:126-141) + set pbc: boxed=0 removes
+ * the box (O(N^2) lists, src/Neighbour.F90:591-606). */
+int gemsgpu_set_box(gemsgpu_ctx* ctx, int sys, int boxed, const double L[3],
+                    const int pbc[3]);
+/* nb_dcut, the Verlet skin (src/Neighbour.F90:237). */
+int gemsgpu_set_skin(gemsgpu_ctx* ctx, int sys, double skin);
+/* Displacement measure of the skin test.  mic=0 is the reference's
+ * test_update (src/Neighbour.F90:1305-1346): raw pos - pos_old, so an atom
+ * wrapped into the box by do_pbc triggers a rebuild; mic=1 (default) takes
+ * the minimum image and skips those rebuilds (same forces, fewer rebuilds). */
+int gemsgpu_set_skin_mode(gemsgpu_ctx* ctx, int sys, int mic);
+/* 0 = full list, newton off (OpenMP default); 1 = half list
+ * (src/Neighbour.F90:160-171).  Half lists are built for export/parity;
+ * force kernels require full lists. */
+int gemsgpu_set_list_mode(gemsgpu_ctx* ctx, int sys, int half);
+int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec);
+
+/* lj_set / plj_set (src/Pairs.F90:198-205, 282-291) for the type pair
+ * (ti,tj): epsilon (eV), sigma (A), cut-off (A).  shifted_force=1 selects
+ * plj; eshift (eV) is an optional constant energy shift per pair (0 = lj). */
+int gemsgpu_set_lj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
+                   double sigma, double rcut, int shifted_force,
+                   double eshift);
+/* smatb_set (src/TB.F90:106-170): A, xi (eV), p, q, r0, rci, rce (A).  The
+ * device derives the tail polynomial coefficients. */
+int gemsgpu_set_smatb(gemsgpu_ctx* ctx, int sys, int ti, int tj, double A,
+                      double xi, double p, double q, double r0, double rci,
+                      double rce);
+/* Tersoff 1988 parameters (Tersoff.f90:56-59 form): A, B (eV), lambda1,
+ * lambda2, beta, n, c, d, h, R, D, chi. */
+int gemsgpu_set_tersoff(gemsgpu_ctx* ctx, int sys, const double prm[12]);
+
+/* ------------------------------------------------------------ forces */
+
+/* interact (src/Interaction.f90:135-241): on the first call build the list
+ * (update, Neighbour.F90:1242-1299), later run test_update
+ * (Neighbour.F90:1305-1346); zero and compute forces and per-atom energies.
+ * *epot (may be NULL) receives the system's potential energy (internal
+ * units), *rebuilt (may be NULL) whether the list was rebuilt. */
+int gemsgpu_forces(gemsgpu_ctx* ctx, int sys, double* epot, int* rebuilt);
+/* update: rebuild the neighbour list now. */
+int gemsgpu_update(gemsgpu_ctx* ctx, int sys);
+/* Export the list: nn[n] and the column-major list (cap x n) like
+ * ig%list(i,m) (src/Neighbour.F90:116-117); indices are 0-based atom
+ * indices of the system.  *cap_needed gets the largest nn. */
+int gemsgpu_get_list(gemsgpu_ctx* ctx, int sys, int* nn, int* list, int cap,
+                     int* cap_needed);
+/* Number of list rebuilds so far (nupd_vlist, src/Neighbour.F90:246). */
+int gemsgpu_get_nupd(gemsgpu_ctx* ctx, int sys, int64_t* nupd);
+
+/* ------------------------------------------------------------ integrators */
+
+int gemsgpu_set_vv(gemsgpu_ctx* ctx, int sys, double dt);
+/* set_ermak (src/Integration.F90:909-961): dt (ps), gamma (1/ps), T (K).
+ * The device draws its normals from a counter-based Philox4x32-10 stream
+ * keyed by seed (production mode). */
+int gemsgpu_set_ermak(gemsgpu_ctx* ctx, int sys, double dt, double gamma,
+                      double temp, uint64_t seed);
+/* Parity mode: the next step_a of an Ermak system consumes these normals
+ * (6 per atom: r1,r2 for x, y, z in atom order, as rang() draws them in
+ * ermak_a, Integration.F90:988-993) instead of the device stream. */
+int gemsgpu_set_ermak_normals(gemsgpu_ctx* ctx, int sys,
+                              const double* normals);
+/* FIRE (Bitzek 2006) with the per-atom mixing of FIRE.f90:107-114: dt0,
+ * dt_max (ps).  Velocities are zeroed. */
+int gemsgpu_set_fire(gemsgpu_ctx* ctx, int sys, double dt0, double dtmax);
+
+/* integration_stepa / integration_stepb (src/Integration.F90:243-301):
+ * the algorithm's half step followed by do_pbc (Set_Properties.f90:444-470). */
+int gemsgpu_step_a(gemsgpu_ctx* ctx, int sys);
+int gemsgpu_step_b(gemsgpu_ctx* ctx, int sys);
+/* dinamic (src/Programs.f90:114-167) without output: nsteps of
+ * step_a / interact / step_b on the device, no host round trip per step
+ * (CUDA-graph captured).  Requires a prior gemsgpu_forces call or runs one. */
+int gemsgpu_md_steps(gemsgpu_ctx* ctx, int sys, int nsteps);
+
+/* Potential energy, kinetic energy with the centre-of-mass velocity removed
+ * and temperature (inq_pot_energy, inq_kin_energy, inq_temperature,
+ * src/Inq_Properties.F90:358-437).  Energies in eV, T in K. */
+int gemsgpu_energy(gemsgpu_ctx* ctx, int sys, double* epot_ev,
+                   double* ekin_ev, double* temp);
+/* max |F| over the system's atoms, eV/A. */
+int gemsgpu_fmax(gemsgpu_ctx* ctx, int sys, double* fmax_ev);
+
+/* ------------------------------------------------------------ batches */
+
+/* Advance nsys systems together: every kernel of a step covers all of them
+ * in one launch (uneven sizes packed by a block map). */
+int gemsgpu_batch_md_steps(gemsgpu_ctx* ctx, const int* sys, int nsys,
+                           int nsteps);
+/* FIRE-relax nsys systems together to max|F| < fmax (eV/A) or maxit
+ * iterations; iters[k] (may be NULL) receives each system's count. */
+int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys,
+                       double fmax, int maxit, int* iters);
+/* Energies of nsys systems (arrays of nsys; any may be NULL). */
+int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys,
+                         double* epot_ev, double* ekin_ev, double* temp);
+
+/* ------------------------------------------------------------ measurement */
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or CUDA events against the library's.  No reference counterpart. */
+int gemsgpu_get_stream(gemsgpu_ctx* ctx, void** stream);
+/* Kernel launches issued by ctx so far (graph replays count their kernel
+ * nodes).  No reference counterpart: GEMS has no device code. */
+int gemsgpu_get_launch_count(gemsgpu_ctx* ctx, int64_t* launches);
+/* Time the force kernels of `sys` on the context's stream with CUDA events:
+ * reps back-to-back evaluations after one warm-up; out_ms[0] = mean time of
+ * the first force kernel (density pass for SMA-TB), out_ms[1] = mean time of
+ * the second (force pass; 0 if none), out_ms[2] = mean list rebuild time.
+ * Replaces timer_dump's per-step wall time (src/Errors.f90:128-172). */
+int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GEMSGPU_H */

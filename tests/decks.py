@@ -139,3 +139,69 @@ def plj_params():
         (1, 1): (0.086000 * kcalmol_ev, 1.5300),
         (0, 1): (math.sqrt(0.086000 * 0.021270) * kcalmol_ev, 0.5 * (1.5300 + 1.4800)),
     }
+
+
+def lj_dimer_rows(sys_factory, ui_ev):
+    """Run the lj.gms deck on an engine; returns (rows, golden rows)."""
+    d = lj_dimer_deck()
+    pos = d["pos0"].copy()
+    s = sys_factory(pos, d["mass"])
+    s.set_box(d["box"], (False, False, False))
+    s.set_lj(*d["lj"])
+    rows = []
+
+    def state():
+        s.set_pos(pos)
+        s.interact()
+        ek, _ = s.kin()
+        ep = s.epot_sum()
+        rows.append([ep * ui_ev, ek * ui_ev, (ep + ek) * ui_ev])
+
+    state()
+    for mv in (-1.2, 0.9):
+        pos[1, 0] = pos[1, 0] + mv
+    for _ in range(250):
+        pos[1, 0] = pos[1, 0] + 0.01
+        state()
+    for mv in (-2.5, -0.9, 1.2):
+        pos[1, 0] = pos[1, 0] + mv
+    s.set_pos(pos)
+    s.set_vv(d["dt"])
+    r = s.dinamica(1000, 10)
+    return np.concatenate([np.array(rows), r[:, :3]]), d["ref"]
+
+
+def he_ne_setup(O):
+    """NVE/NVT initial state from the oracle's stream (fill, box move,
+    tempgdist 300); returns positions, velocities, types, masses, box, rng."""
+    rng = O.Rng(123456)
+    pos, types, mass, box = he_ne_gas(rng)
+    s = O.System(pos, mass, types, 2)
+    s.set_box(box, (True, True, True))
+    for (a, b), (e, sg) in plj_params().items():
+        s.set_lj(e, sg, 10.0, a, b, shifted_force=True)
+    s.remove_cm()
+    s.gdist(rng, 300.0)
+    return pos, s.vel, types, mass, box, rng
+
+
+def apply_plj(s):
+    for (a, b), (e, sg) in plj_params().items():
+        s.set_lj(e, sg, 10.0, a, b, shifted_force=True)
+
+
+def ermak_parity_run(s, rng, nsteps, each):
+    """dinamic with the Ermak normals taken from the LCG stream (rang pairs in
+    atom order), fed to the engine step by step."""
+    s.interact()
+    rows = []
+    for ns in range(1, nsteps + 1):
+        s.set_ermak_normals(rng.rang_stream(3 * s.n))
+        s.stepa()
+        s.interact()
+        s.stepb()
+        if ns % each == 0:
+            ek, t = s.kin()
+            ep = s.epot_sum()
+            rows.append([ep, ek, ep + ek, t])
+    return np.array(rows)

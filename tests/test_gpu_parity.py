@@ -1,0 +1,323 @@
+"""CUDA path (through the C ABI) against the FP64 oracle and the golden files.
+
+Tolerances:
+  * neighbour lists: identical, entry by entry (bit-exact integer sets and
+    the reference's order);
+  * plain FP64 kernels: forces to 1e-10 relative RMS, energies to 1e-9 eV
+    per atom (summation order and exp/sqrt implementations differ);
+  * mixed kernels (FP32 pair math, FP64 accumulation): forces <= 1e-5
+    relative RMS, energies <= 1e-6 eV per atom;
+  * trajectories against golden files: the rule of examples/test.sh.
+"""
+import numpy as np
+import pytest
+
+import decks
+from oracle import oracle as O
+
+gems = pytest.importorskip("gems_b200")
+pytestmark = pytest.mark.gpu
+
+RMS_FP64 = 1e-10
+E_FP64 = 1e-9        # eV per atom
+RMS_MIXED = 1e-5
+E_MIXED = 1e-6       # eV per atom
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = gems.Context()
+    yield c
+    c.close()
+
+
+def relrms(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def both(pos, mass, ctx, types=None, ntypes=1, setup=None):
+    o = O.System(pos, mass, types, ntypes)
+    g = gems.System(pos, mass, types, ntypes, ctx=ctx)
+    for s in (o, g):
+        setup(s)
+    return o, g
+
+
+def compare_lists(o, g):
+    no, lo = o.neighbour_list()
+    ng, lg = g.neighbour_list()
+    np.testing.assert_array_equal(ng, no)
+    m = int(no.max()) if len(no) else 0
+    for k in range(m):
+        mask = no > k
+        np.testing.assert_array_equal(lg[k][mask], lo[k][mask])
+
+
+# ------------------------------------------------------------------ lists
+def smatb_bulk_setup(s, half=False):
+    d = decks.bulk_deck()
+    s.set_box(d["box"], d["pbc"])
+    s.set_smatb(*d["smatb"])
+    s.set_half(half)
+
+
+@pytest.mark.parametrize("half", [False, True])
+def test_list_cells_open_box(ctx, half):
+    """bulk.gms geometry: boxed, no PBC, 8^3 linked cells."""
+    d = decks.bulk_deck()
+    rng = np.random.default_rng(7)
+    pos = d["pos"] + rng.normal(0, 0.05, d["pos"].shape)
+    o, g = both(pos, d["mass"], ctx, setup=lambda s: smatb_bulk_setup(s, half))
+    o.update()
+    g.update()
+    assert o.uses_cells()[0]
+    compare_lists(o, g)
+
+
+@pytest.mark.parametrize("half", [False, True])
+def test_list_cells_pbc_32k(ctx, half):
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk()
+
+    def setup(s):
+        s.set_box(w["L"], (True, True, True))
+        s.set_smatb(*w["smatb"])
+        s.set_half(half)
+
+    o, g = both(w["pos"], w["mass"], ctx, setup=setup)
+    o.update()
+    g.update()
+    assert o.uses_cells() == (True, (13, 13, 13))
+    compare_lists(o, g)
+
+
+@pytest.mark.parametrize("half", [False, True])
+def test_list_n2_mic(ctx, half):
+    """readxyz.gms geometry: rc+skin > box/2, O(N^2) list with minimum image."""
+    d = decks.xyz_deck()
+
+    def setup(s):
+        s.set_box(d["box"], (True, True, True))
+        s.set_lj(*d["lj"])
+        s.set_half(half)
+
+    o, g = both(d["frames"][0], 12.0, ctx, setup=setup)
+    o.update()
+    g.update()
+    assert not o.uses_cells()[0]
+    compare_lists(o, g)
+
+
+def test_list_boundary_ties(ctx):
+    """A pair exactly at rlist: kept by the O(N^2) list (<=), dropped by the
+    linked cells (<), as in the reference."""
+    rl = 5.0 + 1.0
+    pos = np.array([[1.0, 1.0, 1.0], [1.0 + rl, 1.0, 1.0], [3.0, 4.0, 1.0]])
+    for boxed in (False, True):
+        def setup(s):
+            if boxed:
+                s.set_box((40.0, 40.0, 40.0), (False, False, False))
+            s.set_smatb(0.2061, 1.79, 10.229, 4.036, 2.884, 4.4, 5.0)
+        o, g = both(pos, 196.97, ctx, setup=setup)
+        o.update()
+        g.update()
+        assert o.uses_cells()[0] == boxed
+        compare_lists(o, g)
+
+
+def test_list_single_atom_and_cluster(ctx):
+    from gems_b200 import workloads as W
+    for n in (1, 2, 500):
+        pos = W.cluster(n, np.random.default_rng(n)) if n > 2 else np.array([[0.0, 0, 0], [2.8, 0, 0]])[:n]
+        o, g = both(pos, 196.97, ctx, setup=lambda s: s.set_smatb(*W.SMATB["Au"]))
+        o.update()
+        g.update()
+        compare_lists(o, g)
+
+
+# ------------------------------------------------------------------ forces
+def check_forces(o, g, rms, etol):
+    """forces: relative RMS; energies: total per atom and per-atom RMS <= etol,
+    largest single-atom deviation <= 5 etol."""
+    eo = o.interact()
+    eg = g.interact()
+    fo, fg = o.force, g.force
+    assert relrms(fg, fo) <= rms, relrms(fg, fo)
+    d = (g.epot_atoms - o.epot_atoms) * gems.UI_EV
+    assert abs(eg - eo) * gems.UI_EV / o.n <= etol, abs(eg - eo) * gems.UI_EV / o.n
+    assert np.sqrt(np.mean(d * d)) <= etol, np.sqrt(np.mean(d * d))
+    assert np.abs(d).max() <= 5 * etol, np.abs(d).max()
+
+
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_smatb_forces_32k(ctx, prec, rms, etol):
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk()
+
+    def setup(s):
+        s.set_box(w["L"], (True, True, True))
+        s.set_smatb(*w["smatb"])
+    o, g = both(w["pos"], w["mass"], ctx, setup=setup)
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+
+
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_smatb_alloy_cluster(ctx, prec, rms, etol):
+    """Two species (Au/Ag cross pair by arithmetic means), free cluster."""
+    from gems_b200 import workloads as W
+    rng = np.random.default_rng(11)
+    pos = W.cluster(800, rng)
+    types = (rng.random(800) < 0.4).astype(np.int32)
+    mass = np.where(types == 0, W.MASS["Au"], W.MASS["Ag"])
+    au, ag = W.SMATB["Au"], W.SMATB["Ag"]
+    cross = tuple(0.5 * (a + b) for a, b in zip(au, ag))
+
+    def setup(s):
+        s.set_smatb(*au, ti=0, tj=0)
+        s.set_smatb(*ag, ti=1, tj=1)
+        s.set_smatb(*cross, ti=0, tj=1)
+    o, g = both(pos, mass, ctx, types, 2, setup=setup)
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+
+
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_lj_fluid_forces(ctx, prec, rms, etol):
+    from gems_b200 import workloads as W
+    w = W.lj_fluid()
+    rng = np.random.default_rng(3)
+    pos = np.mod(w["pos"] + rng.normal(0, 0.05, w["pos"].shape), w["L"][0])
+
+    def setup(s):
+        s.set_box(w["L"], (True, True, True))
+        e, sg, rc, sh = w["lj"]
+        s.set_lj(e, sg, rc, eshift=sh)
+        s.set_skin(w["skin"])
+    o, g = both(pos, 1.0, ctx, setup=setup)
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+
+
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, 5e-5, 2e-6)])
+def test_tersoff_forces(ctx, prec, rms, etol):
+    from gems_b200 import workloads as W
+    rng = np.random.default_rng(5)
+    pos = W.diamond(4, 5.431)
+    L = 4 * 5.431
+    pos = np.mod(pos + rng.normal(0, 0.05, pos.shape), L)
+
+    def setup(s):
+        s.set_box((L, L, L), (True, True, True))
+        s.set_tersoff(W.TERSOFF_SI)
+    o, g = both(pos, W.MASS["Si"], ctx, setup=setup)
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+
+
+# ------------------------------------------------------------------ golden decks
+def gpu_ref_sys(*a, **k):
+    """A GPU system with the reference's raw-displacement skin test."""
+    g = gems.System(*a, **k)
+    g.set_skin_mode(False)
+    return g
+
+
+def test_gpu_xyz_frames(ctx):
+    d = decks.xyz_deck()
+    g = gpu_ref_sys(d["frames"][0], 12.0, ctx=ctx)
+    g.set_box(d["box"], (True, True, True))
+    g.set_lj(*d["lj"])
+    out = []
+    for f in d["frames"]:
+        g.set_pos(f)
+        out.append(g.interact() * gems.UI_EV)
+    assert decks.gems_rule(d["ref"], out) < 1e-6
+    np.testing.assert_allclose(out, d["ref"], rtol=2e-7)
+
+
+def test_gpu_lj_dimer(ctx):
+    got, ref = decks.lj_dimer_rows(lambda p, m: gpu_ref_sys(p, m, ctx=ctx), gems.UI_EV)
+    assert decks.gems_rule(ref[:, 0], got[:, 0]) < 1e-6
+    np.testing.assert_allclose(got, ref, atol=2e-7, rtol=1e-6)
+
+
+def test_gpu_smatb_bulk_ermak_parity_stream(ctx):
+    d = decks.bulk_deck()
+    g = gpu_ref_sys(d["pos"], d["mass"], ctx=ctx)
+    smatb_bulk_setup(g)
+    g.set_ermak(d["dt"], d["gamma"], d["temp"])
+    rows = decks.ermak_parity_run(g, O.Rng(d["seed"]), d["nsteps"], d["each"])
+    ref = d["ref"]
+    assert decks.gems_rule(ref[:, 0], rows[:, 0] * gems.UI_EV) < 1e-6
+    np.testing.assert_allclose(rows[:, :3] * gems.UI_EV, ref, rtol=2e-6)
+
+
+def test_gpu_nve_plj(ctx):
+    pos, vel, types, mass, box, _ = decks.he_ne_setup(O)
+    g = gpu_ref_sys(pos, mass, types, 2, ctx=ctx, vel=vel)
+    g.set_box(box, (True, True, True))
+    decks.apply_plj(g)
+    g.set_vv(0.002)
+    r = g.dinamica(5000, 100)
+    ref = np.array(decks.golden()["nve_energy"])
+    assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
+    np.testing.assert_allclose(r[:, 1:3], ref[:, 1:3], rtol=1e-5)
+
+
+def test_gpu_nvt_plj_parity_stream(ctx):
+    pos, vel, types, mass, box, rng = decks.he_ne_setup(O)
+    g = gpu_ref_sys(pos, mass, types, 2, ctx=ctx, vel=vel)
+    g.set_box(box, (True, True, True))
+    decks.apply_plj(g)
+    g.set_ermak(0.002, 10.0, 300.0)
+    rows = decks.ermak_parity_run(g, rng, 10000, 100)
+    ref = np.array(decks.golden()["nvt_energy"])
+    assert decks.gems_rule(ref[:, 0], rows[:, 0] * gems.UI_EV) < 1e-6
+    np.testing.assert_allclose(rows[:, 3], ref[:, 3], rtol=1e-5)
+
+
+# ------------------------------------------------------------------ engine invariants
+def test_md_steps_equals_stepwise(ctx):
+    """The captured md_steps loop runs the same kernels as step_a/interact/step_b."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=8)
+    sys = []
+    for _ in range(2):
+        g = gems.System(w["pos"], w["mass"], ctx=ctx)
+        g.set_box(w["L"], (True, True, True))
+        g.set_smatb(*w["smatb"])
+        g.set_ermak(w["dt"], w["gamma"], w["temp"], seed=99)
+        g.interact()
+        sys.append(g)
+    sys[0].md_steps(120)
+    for _ in range(120):
+        sys[1].stepa()
+        sys[1].interact()
+        sys[1].stepb()
+    np.testing.assert_array_equal(sys[0].pos, sys[1].pos)
+    np.testing.assert_array_equal(sys[0].vel, sys[1].vel)
+    assert sys[0].nupd == sys[1].nupd
+
+
+def test_skin_modes_same_trajectory(ctx):
+    """The minimum-image skin test skips the rebuilds that wrapped atoms
+    trigger in the reference's test, without changing the dynamics."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=8)
+    runs = []
+    for mic in (False, True):
+        g = gems.System(w["pos"], w["mass"], ctx=ctx)
+        g.set_box(w["L"], (True, True, True))
+        g.set_smatb(*w["smatb"])
+        g.set_skin_mode(mic)
+        g.set_vv(0.002)
+        g.interact()
+        g.md_steps(200)
+        runs.append((g.nupd, g.pos, g.energy()))
+    (n_ref, p_ref, e_ref), (n_mic, p_mic, e_mic) = runs
+    assert n_mic < n_ref
+    d = p_mic - p_ref
+    d -= w["L"][0] * np.round(d / w["L"][0])
+    assert np.abs(d).max() < 1e-9
+    assert abs(e_mic[0] - e_ref[0]) / len(p_ref) < 1e-10

@@ -54,38 +54,9 @@ def test_xyz_frames_lj_pbc():
     np.testing.assert_allclose(out, d["ref"], rtol=2e-7)
 
 
-def lj_dimer_rows(sys_factory, ui_ev):
-    d = decks.lj_dimer_deck()
-    pos = d["pos0"].copy()
-    s = sys_factory(pos, d["mass"])
-    s.set_box(d["box"], (False, False, False))
-    s.set_lj(*d["lj"])
-    rows = []
-
-    def state():
-        s.set_pos(pos)
-        s.interact()
-        ek, _ = s.kin()
-        ep = s.epot_sum()
-        rows.append([ep * ui_ev, ek * ui_ev, (ep + ek) * ui_ev])
-
-    state()
-    for mv in (-1.2, 0.9):
-        pos[1, 0] = pos[1, 0] + mv
-    for _ in range(250):
-        pos[1, 0] = pos[1, 0] + 0.01
-        state()
-    for mv in (-2.5, -0.9, 1.2):
-        pos[1, 0] = pos[1, 0] + mv
-    s.set_pos(pos)
-    s.set_vv(d["dt"])
-    r = s.dinamica(1000, 10)
-    return np.concatenate([np.array(rows), r[:, :3]]), d["ref"]
-
-
 def test_lj_dimer_scan_and_vv():
     """examples/LJ/lj.gms: 251 dimer states + 1000 velocity-Verlet steps."""
-    got, ref = lj_dimer_rows(O.System, 1.0 / O.lib().orc_ev_ui())
+    got, ref = decks.lj_dimer_rows(O.System, 1.0 / O.lib().orc_ev_ui())
     assert got.shape == ref.shape
     assert decks.gems_rule(ref[:, 0], got[:, 0]) < 1e-6
     np.testing.assert_allclose(got, ref, atol=1e-7, rtol=1e-6)
