@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--block", type=int, default=100, help="MD steps per bench step")
     ap.add_argument("--replicas", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--arms", default="fp64,mixed,batched",
+                    help="comma list of arms to run (profiling); the full line needs all three")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -295,6 +297,28 @@ def main():
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
     blk = args.block
     arms = {}
+    want = set(args.arms.split(","))
+    if want != {"fp64", "mixed", "batched"}:
+        # profiling run: time the requested arms only, print a short line
+        w = c2_replica(2)
+        out = {}
+        for name in ("fp64", "mixed", "batched"):
+            if name not in want:
+                continue
+            prec = gems.PREC_FP64 if name == "fp64" else gems.PREC_MIXED
+            nrep = args.replicas if name == "batched" else 1
+            ss = [make_system(gems, ctx, c2_replica(100 + k) if nrep > 1 else w, prec, seed=100 + k)
+                  for k in range(nrep)]
+            for s_ in ss:
+                s_.interact()
+            ts, nl = timed_blocks(ctx, torch, ss, blk, args.steps, args.warmup, flush, ext)
+            out[name] = {"atom_steps_per_s": sum(x.n for x in ss) * blk * len(ts) / (sum(ts) * 1e-3),
+                         "launches": nl}
+            for s_ in ss:
+                s_.destroy()
+        print(json.dumps({"profile_arms": out}), flush=True)
+        ctx.close()
+        return
     # --- single-system arms
     w = c2_replica(2 + 1000 * rank)
     for name, prec in (("fp64", gems.PREC_FP64), ("mixed", gems.PREC_MIXED)):

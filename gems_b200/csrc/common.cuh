@@ -144,6 +144,7 @@ struct Arena {
   SysState* st;
   PairP* prm;
   int* any_rebuild;     // OR over the systems of the last step
+  unsigned long long* body_runs;  // executions of graph-captured rebuild chains
 };
 
 }  // namespace gg

@@ -52,7 +52,8 @@ struct SysHost {
 struct Graph {
   cudaGraphExec_t exec = nullptr;
   uint64_t epoch = 0;
-  int64_t nodes = 0;  // kernel nodes per replay
+  int64_t nodes = 0;       // unconditional kernel nodes per replay
+  int64_t body_nodes = 0;  // kernels of one conditional rebuild body
 };
 
 }  // namespace
@@ -74,6 +75,9 @@ struct gemsgpu_ctx {
   std::vector<std::pair<int64_t, int64_t>> free_atoms, free_cells;
   uint64_t epoch = 1;  // bumps when device pointers or maps change
   int64_t launches = 0;  // kernels issued (graph replays add their node count)
+  bool use_cond = true;  // conditional graph nodes guard the rebuild chain
+  int64_t body_nodes = 0;  // kernels in one captured rebuild chain
+  unsigned long long body_seen = 0;  // body_runs already accounted
   int64_t pending = 0;   // kernels recorded by the capture in progress
   std::map<std::string, DevMap> maps;
   std::map<std::string, Graph> graphs;
@@ -498,9 +502,9 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
       CHK(get_map(ctx, kv.second, BLOCK, 0, &m));
       k_zero_force<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
       if (prec == PREC_MIXED) {
-        k_tersoff<float, true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+        k_tersoff<float><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
       } else {
-        k_tersoff<double, false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+        k_tersoff<double><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
       }
       continue;
     }
@@ -520,7 +524,7 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
 
 // the rebuild chain; every kernel returns at once for systems whose
 // rebuild flag is clear, so the chain can sit in a captured step.
-int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 0) {
   BlockMap ma, mc, mw;
   const int* sa;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
@@ -543,15 +547,16 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   if (n2) {
     k_list_n2<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   }
-  k_count_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
+  k_count_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, st>>>(A, sa, (int)ss.size(), in_graph); ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
 }
 
-int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss,
+                  cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
-  k_step_a<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
+  k_step_a<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond, use_cond); ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
 }
@@ -687,6 +692,102 @@ int record_step(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   return 0;
 }
 
+// Capture `nsteps` MD steps into one graph.  Each step is
+//   [step_a] -> IF(rebuild needed) { rebuild chain } -> [forces, step_b]
+// where the IF node's handle is raised by k_step_a; the rebuild kernels
+// therefore cost nothing on steps that keep their list.
+int capture_into(gemsgpu_ctx* ctx, cudaGraph_t g, std::vector<cudaGraphNode_t>& deps,
+                 int (*fn)(gemsgpu_ctx*, const std::vector<int>&, void*),
+                 const std::vector<int>& ss, void* arg) {
+  CU(cudaStreamBeginCaptureToGraph(ctx->stream, g, deps.empty() ? nullptr : deps.data(), nullptr,
+                                   deps.size(), cudaStreamCaptureModeThreadLocal));
+  int rc = fn(ctx, ss, arg);
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* d = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, nullptr, &d, &nd);
+  std::vector<cudaGraphNode_t> nd_copy;
+  if (e == cudaSuccess) nd_copy.assign(d, d + nd);
+  cudaGraph_t out = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &out);
+  if (rc) return rc;
+  if (e != cudaSuccess || e2 != cudaSuccess)
+    return fail(ctx, GEMSGPU_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  deps = nd_copy;
+  return 0;
+}
+
+struct CondArg {
+  cudaGraphConditionalHandle h;
+};
+
+int cap_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
+  return launch_step_a(ctx, ss, ((CondArg*)arg)->h, 1);
+}
+int cap_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
+  const int64_t before = ctx->launches;
+  int rc = launch_rebuild(ctx, ss, 1);
+  ctx->body_nodes = ctx->launches - before;
+  return rc;
+}
+int cap_forces_b(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
+  CHK(launch_forces(ctx, ss));
+  return launch_step_b(ctx, ss);
+}
+int cap_plain(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
+  int n = *(int*)arg;
+  for (int k = 0; k < n; k++) CHK(record_step(ctx, ss));
+  return 0;
+}
+
+int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGraph_t* out) {
+  cudaGraph_t g = nullptr;
+  CU(cudaGraphCreate(&g, 0));
+  std::vector<cudaGraphNode_t> deps;
+  int rc = 0;
+  bool cond_ok = ctx->use_cond;
+  for (int k = 0; k < nsteps && rc == 0 && cond_ok; k++) {
+    CondArg ca{};
+    if (cudaGraphConditionalHandleCreate(&ca.h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+      cond_ok = false;
+      break;
+    }
+    rc = capture_into(ctx, g, deps, cap_step_a, ss, &ca);
+    if (rc) break;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = ca.h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    if (cudaGraphAddNode(&cn, g, deps.data(), deps.size(), &cp) != cudaSuccess) {
+      cond_ok = false;
+      break;
+    }
+    std::vector<cudaGraphNode_t> none;
+    rc = capture_into(ctx, cp.conditional.phGraph_out[0], none, cap_rebuild, ss, nullptr);
+    if (rc) break;
+    deps.assign(1, cn);
+    rc = capture_into(ctx, g, deps, cap_forces_b, ss, nullptr);
+  }
+  cudaGetLastError();
+  if (rc == 0 && !cond_ok) {
+    // conditional nodes unavailable: plain capture, rebuild kernels exit early
+    cudaGraphDestroy(g);
+    ctx->use_cond = false;
+    CU(cudaGraphCreate(&g, 0));
+    deps.clear();
+    int n = nsteps;
+    rc = capture_into(ctx, g, deps, cap_plain, ss, &n);
+  }
+  if (rc) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  *out = g;
+  return 0;
+}
+
 int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGraphExec_t* out) {
   std::string key = "G" + std::to_string(nsteps) + ":";
   for (int s : ss) key += std::to_string(s) + ",";
@@ -717,23 +818,23 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
   }
   cudaGraph_t g = nullptr;
   const int64_t before = ctx->launches;
-  CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = 0;
-  for (int k = 0; k < nsteps && rc == 0; k++) rc = record_step(ctx, ss);
-  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-  const int64_t nodes = ctx->launches - before;
+  ctx->body_nodes = 0;
+  int rc = build_chunk_graph(ctx, ss, nsteps, &g);
+  int64_t nodes = ctx->launches - before;
+  const int64_t body = ctx->use_cond ? ctx->body_nodes : 0;
+  nodes -= body * nsteps;  // the bodies run only on rebuild steps
   ctx->launches = before;  // captured, not executed
   if (rc) {
     if (g) cudaGraphDestroy(g);
     return rc;
   }
-  if (e != cudaSuccess) return fail(ctx, GEMSGPU_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  cudaError_t e;
   cudaGraphExec_t ex = nullptr;
   e = cudaGraphInstantiate(&ex, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(ctx, GEMSGPU_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
   if (it != ctx->graphs.end() && it->second.exec) cudaGraphExecDestroy(it->second.exec);
-  ctx->graphs[key] = Graph{ex, ctx->epoch, nodes};
+  ctx->graphs[key] = Graph{ex, ctx->epoch, nodes, body};
   *out = ex;
   return 0;
 }
@@ -745,6 +846,13 @@ int launch_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps) {
   std::string key = "G" + std::to_string(nsteps) + ":";
   for (int s : ss) key += std::to_string(s) + ",";
   ctx->launches += ctx->graphs[key].nodes;
+  if (ctx->graphs[key].body_nodes) {
+    unsigned long long runs = 0;
+    CU(cudaMemcpyAsync(&runs, ctx->A.body_runs, sizeof(runs), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->launches += (int64_t)(runs - ctx->body_seen) * ctx->graphs[key].body_nodes;
+    ctx->body_seen = runs;
+  }
   return 0;
 }
 
@@ -880,7 +988,9 @@ int gemsgpu_create(int device, int64_t max_atoms, int max_systems, gemsgpu_ctx**
     if ((rc = grow_params(ctx, 64))) break;
     if ((rc = grow_blocks(ctx, 1024))) break;
     if ((rc = dalloc(ctx, &ctx->A.any_rebuild, 1))) break;
+    if ((rc = dalloc(ctx, &ctx->A.body_runs, 1))) break;
     cudaMemsetAsync(ctx->A.any_rebuild, 0, sizeof(int), ctx->stream);
+    cudaMemsetAsync(ctx->A.body_runs, 0, sizeof(unsigned long long), ctx->stream);
   } while (0);
   if (rc) {
     gemsgpu_destroy(ctx);
@@ -900,7 +1010,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.epot, A.band, A.eband,
                   A.ebandf, A.fxp, A.minv, A.mass, A.type, A.nn, A.list, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
-                  A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild,
+                  A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->d_sys};
   for (void* p : ptrs)
     if (p) cudaFree(p);

@@ -43,17 +43,26 @@ __device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
   return c;
 }
 
-// two standard normals from one Philox block (Box-Muller, FP64)
-__device__ __forceinline__ void normals2(uint4 r, double& n1, double& n2) {
-  const double inv53 = 1.0 / 9007199254740992.0;  // 2^-53
-  double u1 = ((double)(r.x >> 5) * 67108864.0 + (double)(r.y >> 6)) * inv53;
-  double u2 = ((double)(r.z >> 5) * 67108864.0 + (double)(r.w >> 6)) * inv53;
-  u1 = 1.0 - u1;  // (0, 1]
-  double rr = sqrt(-2.0 * log(u1));
-  double sn, cs;
-  sincospi(2.0 * u2, &sn, &cs);
-  n1 = rr * cs;
-  n2 = rr * sn;
+// Box-Muller on two 32-bit uniforms: u1 in (0,1], u2 in [0,1).  FP32 is
+// ample for a Langevin kick (the kick is applied in FP64).
+__device__ __forceinline__ void bm_pair(uint32_t a, uint32_t b, double& n1, double& n2) {
+  float u1 = ((float)(a >> 8) + 1.0f) * 5.9604644775390625e-8f;  // (0, 1]
+  float u2 = (float)(b >> 8) * 5.9604644775390625e-8f;            // [0, 1)
+  float rr = sqrtf(-2.0f * logf(u1));
+  float sn, cs;
+  sincospif(2.0f * u2, &sn, &cs);
+  n1 = (double)(rr * cs);
+  n2 = (double)(rr * sn);
+}
+
+// six standard normals for (atom, step) from two Philox blocks
+__device__ __forceinline__ void normals6(uint32_t atom, uint64_t step, uint64_t seed, double r[6]) {
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  uint4 a = philox10(make_uint4(atom, (uint32_t)step, (uint32_t)(step >> 32), 0u), key);
+  uint4 b = philox10(make_uint4(atom, (uint32_t)step, (uint32_t)(step >> 32), 1u), key);
+  bm_pair(a.x, a.y, r[0], r[1]);
+  bm_pair(a.z, a.w, r[2], r[3]);
+  bm_pair(b.x, b.y, r[4], r[5]);
 }
 
 // ------------------------------------------------------------------ helpers
@@ -196,17 +205,29 @@ __device__ __forceinline__ bool last_block(const BlockMap& M, SysState* st, int 
   return last;
 }
 
+// warp 0 of a system's last block: top-2 over that system's block results
+__device__ __forceinline__ double2 sys_top2(const Arena& A, const BlockMap& M, int s) {
+  double2 w = make_double2(1.e-16, 1.e-16);
+  const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+  for (int b = threadIdx.x; b < nb; b += 32) w = top2_merge(w, __ldcg(&A.blk_top2[b0 + b]));
+  for (int o = 16; o; o >>= 1) {
+    double2 q;
+    q.x = __shfl_xor_sync(0xffffffffu, w.x, o);
+    q.y = __shfl_xor_sync(0xffffffffu, w.y, o);
+    w = top2_merge(w, q);
+  }
+  return w;
+}
+
 // ------------------------------------------------------------------ skin test
 // Per-block top-2 of |pos - pos_old|^2; the last block of each system
 // decides rebuild = sqrt(d1) + sqrt(d2) > nb_dcut (test_update).
 __device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, int s,
                                            double2 t) {
   if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
-  if (last_block(M, A.st, s, &A.st[s].ticket)) {
+  if (last_block(M, A.st, s, &A.st[s].ticket) && threadIdx.x < 32) {
+    double2 v = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
-      double2 v = make_double2(1.e-16, 1.e-16);
-      int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
-      for (int b = 0; b < nb; b++) v = top2_merge(v, __ldcg(&A.blk_top2[b0 + b]));
       const SysDev& S = A.sys[s];
       int rb = __dadd_rn(__dsqrt_rn(v.x), __dsqrt_rn(v.y)) > S.skin;
       A.st[s].rebuild = rb;
@@ -497,9 +518,12 @@ __global__ void k_list_n2(Arena A, BlockMap M) {
   if (act) list_done(A, s, i, m);
 }
 
-__global__ void k_count_rebuild(Arena A, const int* sys, int nsys) {
+// rebuild counters; in_graph marks the copy captured inside a conditional
+// node, whose executions are counted for the launch statistics
+__global__ void k_count_rebuild(Arena A, const int* sys, int nsys, int in_graph) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < nsys && A.st[sys[k]].rebuild) A.st[sys[k]].nupd++;
+  if (in_graph && k == 0) atomicAdd(A.body_runs, 1ull);
 }
 
 // ------------------------------------------------------------------ SMA-TB
@@ -536,6 +560,32 @@ __device__ __forceinline__ float lane_sumf(float v) {
   return v;
 }
 
+// Pair loops of the force kernels: lane `lane` of an atom takes list slots
+// lane, lane+K, ...; UNR slots are loaded, then gathered, then computed, so a
+// lane keeps UNR independent gathers in flight (the kernels are bound by
+// gather latency, not arithmetic).
+constexpr int UNR = 4;
+
+#define PAIR_LOOP_BEGIN(GATHER_T, GATHER)                                      \
+  for (int m0 = lane; m0 < nn; m0 += UNR * K) {                               \
+    int jj[UNR];                                                              \
+    _Pragma("unroll") for (int u = 0; u < UNR; u++) {                         \
+      int m = m0 + u * K;                                                     \
+      jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;            \
+    }                                                                         \
+    GATHER_T gj[UNR];                                                         \
+    _Pragma("unroll") for (int u = 0; u < UNR; u++) if (jj[u] >= 0) gj[u] = GATHER(jj[u]); \
+    _Pragma("unroll") for (int u = 0; u < UNR; u++) {                         \
+      if (jj[u] < 0) continue;                                                \
+      const int j = jj[u];                                                    \
+      (void)j;
+#define PAIR_LOOP_END \
+    }                 \
+  }
+
+struct GPos { double4 x; double eb; };
+struct GFx { int4 x; float eb; };
+
 // smatb_preinteraction (src/TB.F90:367-455), FP64: rho_i = sum_j
 //   xi^2 exp(-2q(r/r0-1))            r <  rci
 //   (b1 d^5 + b2 d^4 + b3 d^3)^2     rci <= r <= rce, d = r - rce
@@ -553,11 +603,11 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
     const int nn = min(A.nn[i], A.lcap);
     const bool one = S.ntypes == 1;
     SmFP64 c = sm_load(A.prm[S.param_off]);
-    for (int m = lane; m < nn; m += K) {
-      int j = A.list[(size_t)m * A.cap + i];
+    auto gat = [&](int j) { return A.pos[j]; };
+    PAIR_LOOP_BEGIN(double4, gat)
       if (!one) c = sm_load(A.prm[S.param_off + ti * S.ntypes + A.type[j]]);
       double v0, v1, v2;
-      vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+      vd_fp64(S, xi, gj[u], v0, v1, v2);
       double dr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
       if (dr > c.rce) continue;
       double banda;
@@ -569,7 +619,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
         banda = banda * banda;
       }
       band += banda;
-    }
+    PAIR_LOOP_END
   }
   band = lane_sum<K>(band);
   if (act && lane == 0) {
@@ -600,15 +650,15 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
     const int nn = min(A.nn[i], A.lcap);
     const bool one = S.ntypes == 1;
     SmFP64 c = sm_load(A.prm[S.param_off]);
-    for (int m = lane; m < nn; m += K) {
-      int j = A.list[(size_t)m * A.cap + i];
+    auto gat = [&](int j) { GPos g; g.x = A.pos[j]; g.eb = A.eband[j]; return g; };
+    PAIR_LOOP_BEGIN(GPos, gat)
       if (!one) c = sm_load(A.prm[S.param_off + ti * S.ntypes + A.type[j]]);
       double v0, v1, v2;
-      vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+      vd_fp64(S, xi, gj[u].x, v0, v1, v2);
       double dr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
       if (dr > c.rce) continue;
       double factor, repul;
-      double ebs = ebi + A.eband[j];
+      double ebs = ebi + gj[u].eb;
       if (dr <= c.rci) {
         double x = dr / c.r0 - 1.0;
         repul = c.A * exp(-c.p * x);
@@ -626,7 +676,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
       f1 -= fr * v1;
       f2 -= fr * v2;
       ep += repul;
-    }
+    PAIR_LOOP_END
   }
   f0 = lane_sum<K>(f0);
   f1 = lane_sum<K>(f1);
@@ -697,9 +747,9 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
     const int nn = min(A.nn[i], A.lcap);
     const bool one = S.ntypes == 1;
     SmF32 c = smf_load(A.prm[S.param_off]);
-    for (int m = lane; m < nn; m += K) {
-      int j = A.list[(size_t)m * A.cap + i];
-      int4 xj = A.fxp[j];
+    auto gat = [&](int j) { return A.fxp[j]; };
+    PAIR_LOOP_BEGIN(int4, gat)
+      const int4 xj = gj[u];
       if (!one) c = smf_load(A.prm[S.param_off + xi.w * S.ntypes + xj.w]);
       float v0, v1, v2;
       vd_fx(S, xi, xj, v0, v1, v2);
@@ -715,7 +765,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
         banda = banda * banda;
       }
       band += (double)banda;
-    }
+    PAIR_LOOP_END
   }
   band = lane_sum<K>(band);
   if (act && lane == 0) {
@@ -741,9 +791,9 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M
     const bool one = S.ntypes == 1;
     SmF32 c = smf_load(A.prm[S.param_off]);
     const float evui = (float)EV_UI;
-    for (int m = lane; m < nn; m += K) {
-      int j = A.list[(size_t)m * A.cap + i];
-      int4 xj = A.fxp[j];
+    auto gat = [&](int j) { GFx g; g.x = A.fxp[j]; g.eb = A.ebandf[j]; return g; };
+    PAIR_LOOP_BEGIN(GFx, gat)
+      const int4 xj = gj[u].x;
       if (!one) c = smf_load(A.prm[S.param_off + xi.w * S.ntypes + xj.w]);
       float v0, v1, v2;
       vd_fx(S, xi, xj, v0, v1, v2);
@@ -751,7 +801,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M
       if (r2 > c.rce2) continue;
       float dr = sqrtf(r2);
       float rinv = __frcp_rn(dr);
-      float ebs = ebi + A.ebandf[j];
+      float ebs = ebi + gj[u].eb;
       float factor, repul;
       if (dr <= c.rci) {
         float x = c.r0 - dr;
@@ -772,7 +822,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M
       f1 -= (double)(fr * v1);
       f2 -= (double)(fr * v2);
       ep += (double)repul;
-    }
+    PAIR_LOOP_END
   }
   f0 = lane_sum<K>(f0);
   f1 = lane_sum<K>(f1);
@@ -800,13 +850,13 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
     const double4 xi = A.pos[i];
     const int ti = A.type[i];
     const int nn = min(A.nn[i], A.lcap);
-    for (int m = lane; m < nn; m += K) {
-      int j = A.list[(size_t)m * A.cap + i];
+    auto gat = [&](int j) { return A.pos[j]; };
+    PAIR_LOOP_BEGIN(double4, gat)
       const PairP& P = A.prm[S.param_off + ti * S.ntypes + A.type[j]];
       double e = P.v[0];
       if (e == 0.0 && P.v[1] == 0.0) continue;
       double v0, v1, v2;
-      vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+      vd_fp64(S, xi, gj[u], v0, v1, v2);
       double dr = v0 * v0 + v1 * v1 + v2 * v2;
       if (dr > P.v[3]) continue;
       dr = sqrt(dr);
@@ -826,7 +876,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
       f1 -= fr * v1;
       f2 -= fr * v2;
       ep += p;
-    }
+    PAIR_LOOP_END
   }
   f0 = lane_sum<K>(f0);
   f1 = lane_sum<K>(f1);
@@ -850,9 +900,9 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
     const int4 xi = A.fxp[i];
     const int nn = min(A.nn[i], A.lcap);
     const float evui = (float)EV_UI;
-    for (int m = lane; m < nn; m += K) {
-      int j = A.list[(size_t)m * A.cap + i];
-      int4 xj = A.fxp[j];
+    auto gat = [&](int j) { return A.fxp[j]; };
+    PAIR_LOOP_BEGIN(int4, gat)
+      const int4 xj = gj[u];
       const PairP& P = A.prm[S.param_off + xi.w * S.ntypes + xj.w];
       float e = (float)P.v[0];
       float rc2 = (float)P.v[3];
@@ -878,7 +928,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
       f1 -= (double)(fr * v1);
       f2 -= (double)(fr * v2);
       ep += (double)p;
-    }
+    PAIR_LOOP_END
   }
   f0 = lane_sum<K>(f0);
   f1 = lane_sum<K>(f1);
@@ -894,54 +944,48 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
 // Tersoff 1988 with the functional form of src/Tersoff.f90:131-341 and the
 // cut-off of src/Algebra.F90:391-409, forces = exact gradient of
 // E = sum_i sum_j 1/2 fc(r_ij) [VR(r_ij) + b_ij VA(r_ij)].  One thread per
-// atom i gathers its bonds into registers, then scatters the three-body
-// terms to j and k with FP64 atomics.
+// atom i gathers its bonds (r <= R+D) into registers and scatters the
+// three-body terms to j and k with FP64 atomics.  Bond geometry, the pair
+// terms fc, VR, VA and the bond order b_ij = chi (1 + beta^n zeta^n)^(-1/2n)
+// are FP64; the angular sums zeta_ij and their derivatives (the triplet
+// work) run in R = float for the mixed kernel, double for the FP64 kernel.
 constexpr int TS_MAXB = 12;
 
-template <typename R>
-__device__ __forceinline__ R ts_fc(R r, R r1, R r2, R& dfc) {
-  if (r < r1) { dfc = R(0); return R(1); }
-  if (r > r2) { dfc = R(0); return R(0); }
-  const R pi = R(3.14159265358979323846);
-  R aux = pi * (r - (r1 + r2) * R(0.5)) / (r2 - r1);
-  R sn, cs;
-  if constexpr (sizeof(R) == 8) { sincos(aux, &sn, &cs); } else { __sincosf(aux, &sn, &cs); }
-  dfc = -cs * (pi * R(0.5)) / (r2 - r1);
-  return R(0.5) - R(0.5) * sn;
+__device__ __forceinline__ double ts_fc(double r, double r1, double r2, double& dfc) {
+  if (r < r1) { dfc = 0.0; return 1.0; }
+  if (r > r2) { dfc = 0.0; return 0.0; }
+  const double pi = 3.14159265358979323846;
+  double aux = pi * (r - (r1 + r2) * 0.5) / (r2 - r1);
+  double sn, cs;
+  sincos(aux, &sn, &cs);
+  dfc = -cs * (pi * 0.5) / (r2 - r1);
+  return 0.5 - 0.5 * sn;
 }
 
-template <typename R, bool MIXED>
+template <typename R>
 __global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
   int s = blk_sys(M);
   const SysDev& S = A.sys[s];
   int i = M.first[blockIdx.x] + threadIdx.x;
   if (i >= M.end[blockIdx.x]) return;
   const TersoffP& T = S.ts;
-  const R r1 = R(T.R - T.D), r2 = R(T.R + T.D);
+  const double r1 = T.R - T.D, r2 = T.R + T.D;
   const R c2 = R(T.c * T.c), d2 = R(T.d * T.d), h = R(T.h);
-  const R nexp = R(T.n);
-  const R btnp = R(pow(T.beta, T.n));
-  const R Aa = R(T.A * EV_UI), Bb = R(T.B * EV_UI), l1 = R(T.l1), l2 = R(T.l2);
-  const R chi = R(T.chi);
+  const R c2d2 = R(T.c * T.c / (T.d * T.d));
+  const double nexp = T.n;
+  const double btnp = pow(T.beta, T.n);
+  const double Aa = T.A * EV_UI, Bb = T.B * EV_UI;
   int bj[TS_MAXB];
-  R br[TS_MAXB], bu[TS_MAXB][3], bfc[TS_MAXB], bdfc[TS_MAXB];
+  double br[TS_MAXB], bfc[TS_MAXB];
+  R bu[TS_MAXB][3], bfcr[TS_MAXB], bdfcr[TS_MAXB];
   int nb = 0;
   const int nn = min(A.nn[i], A.lcap);
   const double4 xi = A.pos[i];
-  const int4 qi = A.fxp[i];
   for (int m = 0; m < nn; m++) {
     int j = A.list[(size_t)m * A.cap + i];
-    R v0, v1, v2;
-    if constexpr (MIXED) {
-      float a, b, c;
-      vd_fx(S, qi, A.fxp[j], a, b, c);
-      v0 = a; v1 = b; v2 = c;
-    } else {
-      double a, b, c;
-      vd_fp64(S, xi, A.pos[j], a, b, c);
-      v0 = a; v1 = b; v2 = c;
-    }
-    R rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    double v0, v1, v2;
+    vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+    double rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
     if (rr > r2) continue;
     if (nb == TS_MAXB) {
       atomicOr(&A.st[s].status, ST_OVERFLOW);
@@ -949,59 +993,67 @@ __global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
     }
     bj[nb] = j;
     br[nb] = rr;
-    R ir = R(1) / rr;
-    bu[nb][0] = v0 * ir; bu[nb][1] = v1 * ir; bu[nb][2] = v2 * ir;
-    bfc[nb] = ts_fc<R>(rr, r1, r2, bdfc[nb]);
+    double ir = 1.0 / rr;
+    bu[nb][0] = R(v0 * ir); bu[nb][1] = R(v1 * ir); bu[nb][2] = R(v2 * ir);
+    double dfc;
+    bfc[nb] = ts_fc(rr, r1, r2, dfc);
+    bfcr[nb] = R(bfc[nb]);
+    bdfcr[nb] = R(dfc);
     nb++;
   }
   double ei = 0.0;
   double fi0 = 0, fi1 = 0, fi2 = 0;
   for (int a = 0; a < nb; a++) {
-    const R rij = br[a];
+    const double rij = br[a];
     const R* u = bu[a];
     R zij = R(0);
     for (int b = 0; b < nb; b++) {
       if (b == a) continue;
       R ct = u[0] * bu[b][0] + u[1] * bu[b][1] + u[2] * bu[b][2];
       R hc = h - ct;
-      R g = R(1) + c2 / d2 - c2 / (d2 + hc * hc);
-      zij += bfc[b] * g;
+      R g = R(1) + c2d2 - c2 / (d2 + hc * hc);
+      zij += bfcr[b] * g;
     }
-    R vr = Aa * exp(-l1 * rij), dvr = -l1 * vr;
-    R va = -Bb * exp(-l2 * rij), dva = -l2 * va;
-    R bij, dbdz;
-    if (zij > R(1.0e-15)) {
-      R zn = pow(zij, nexp);
-      R aux = R(1) / (R(1) + btnp * zn);
-      bij = chi * pow(aux, R(0.5) / nexp);
-      dbdz = R(-0.5) * bij * aux * btnp * zn / zij;
+    double dfc_a;
+    const double fc_a = ts_fc(rij, r1, r2, dfc_a);
+    const double vr = Aa * exp(-T.l1 * rij), dvr = -T.l1 * vr;
+    const double va = -Bb * exp(-T.l2 * rij), dva = -T.l2 * va;
+    double bij, dbdz;
+    const double z = (double)zij;
+    if (z > 1.0e-15) {
+      double zn = pow(z, nexp);
+      double aux = 1.0 / (1.0 + btnp * zn);
+      bij = T.chi * pow(aux, 0.5 / nexp);
+      dbdz = -0.5 * bij * aux * btnp * zn / z;
     } else {
-      bij = chi;
-      dbdz = R(0);
+      bij = T.chi;
+      dbdz = 0.0;
     }
-    ei += (double)(R(0.5) * bfc[a] * (vr + bij * va));
-    R dV = R(0.5) * (bdfc[a] * (vr + bij * va) + bfc[a] * (dvr + bij * dva));
-    double g0 = (double)(dV * u[0]), g1 = (double)(dV * u[1]), g2 = (double)(dV * u[2]);
+    ei += 0.5 * fc_a * (vr + bij * va);
+    const double dV = 0.5 * (dfc_a * (vr + bij * va) + fc_a * (dvr + bij * dva));
+    const double ua0 = (double)u[0], ua1 = (double)u[1], ua2 = (double)u[2];
+    double g0 = dV * ua0, g1 = dV * ua1, g2 = dV * ua2;
     fi0 += g0; fi1 += g1; fi2 += g2;
     double* fj = reinterpret_cast<double*>(&A.force[bj[a]]);
     atomicAdd(fj + 0, -g0);
     atomicAdd(fj + 1, -g1);
     atomicAdd(fj + 2, -g2);
-    if (dbdz == R(0)) continue;
-    R pre = R(0.5) * bfc[a] * va * dbdz;
+    if (dbdz == 0.0) continue;
+    const R pre = R(0.5 * fc_a * va * dbdz);  // dE / dzeta
+    const R irij = R(1.0 / rij);
     double gj0 = 0, gj1 = 0, gj2 = 0;
     for (int b = 0; b < nb; b++) {
       if (b == a) continue;
       const R* w = bu[b];
-      R rik = br[b];
+      const R irik = R(1.0 / br[b]);
       R ct = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
       R hc = h - ct;
       R den = d2 + hc * hc;
-      R g = R(1) + c2 / d2 - c2 / den;
+      R g = R(1) + c2d2 - c2 / den;
       R dg = R(-2) * c2 * hc / (den * den);
-      R ka = pre * bfc[b] * dg / rij;
-      R kb = pre * dg / rik * bfc[b];
-      R kc = pre * bdfc[b] * g;
+      R ka = pre * bfcr[b] * dg * irij;
+      R kb = pre * bfcr[b] * dg * irik;
+      R kc = pre * bdfcr[b] * g;
       double gk0 = (double)(kb * (u[0] - ct * w[0]) + kc * w[0]);
       double gk1 = (double)(kb * (u[1] - ct * w[1]) + kc * w[1]);
       double gk2 = (double)(kb * (u[2] - ct * w[2]) + kc * w[2]);
@@ -1050,7 +1102,11 @@ __global__ void k_zero_force(Arena A, BlockMap M) {
 // integration_stepa (src/Integration.F90:243-262): the algorithm's half
 // step, do_pbc (Set_Properties.f90:444-470), then the displacement test of
 // test_update fused in (the list decision for this step's interact).
-__global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M) {
+// When the step is replayed from a CUDA graph, `cond` is the handle of the
+// conditional node that guards the rebuild kernels: any system that needs a
+// rebuild raises it, so steps without a rebuild skip those launches.
+__global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraphConditionalHandle cond,
+                                                   int use_cond) {
   int s = blk_sys(M);
   const SysDev& S = A.sys[s];
   SysState& st = A.st[s];
@@ -1082,14 +1138,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M) {
 #pragma unroll
         for (int k = 0; k < 6; k++) r[k] = A.ext_normals[(size_t)6 * i + k];
       } else {
-        const uint32_t loc = (uint32_t)(i - S.off);
-        const uint64_t step = st.step;
-        const uint2 key = make_uint2((uint32_t)S.seed, (uint32_t)(S.seed >> 32));
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          uint4 c = make_uint4(loc, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)k);
-          normals2(philox10(c, key), r[2 * k], r[2 * k + 1]);
-        }
+        normals6((uint32_t)(i - S.off), st.step, S.seed, r);
       }
       const double f_lan = S.skt * mi.y;
       const double pr = f_lan * S.sdr, pv = f_lan * S.sdv;
@@ -1122,15 +1171,16 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M) {
   }
   t = block_top2(t);
   if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
-  if (last_block(M, A.st, s, &st.ticket)) {
+  if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
+    double2 w = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
-      double2 w = make_double2(1.e-16, 1.e-16);
-      int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
-      for (int b = 0; b < nb; b++) w = top2_merge(w, __ldcg(&A.blk_top2[b0 + b]));
       int rb = __dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)) > S.skin;
       if (frozen) rb = 0;
       st.rebuild = rb;
-      if (rb) atomicOr(A.any_rebuild, 1);
+      if (rb) {
+        atomicOr(A.any_rebuild, 1);
+        if (use_cond) cudaGraphSetConditional(cond, 1u);
+      }
       if (S.integ == IT_ERMAK && !S.use_ext_normals) st.step++;
       if (S.integ == IT_FIRE) st.fire_zero = 0;
     }
@@ -1187,14 +1237,18 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
   double Pb = block_sum(P);
   double Fb = block_max(f2max);
   if (threadIdx.x == 0) A.blk_red[2 * blockIdx.x] = Pb, A.blk_red[2 * blockIdx.x + 1] = Fb;
-  if (last_block(M, A.st, s, &st.ticket2)) {
+  if (last_block(M, A.st, s, &st.ticket2) && threadIdx.x < 32) {
+    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+    double Pt = 0.0, Ft = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 32) {
+      Pt += __ldcg(&A.blk_red[2 * (b0 + b)]);
+      Ft = fmax(Ft, __ldcg(&A.blk_red[2 * (b0 + b) + 1]));
+    }
+    for (int o = 16; o; o >>= 1) {
+      Pt += __shfl_xor_sync(0xffffffffu, Pt, o);
+      Ft = fmax(Ft, __shfl_xor_sync(0xffffffffu, Ft, o));
+    }
     if (threadIdx.x == 0 && !frozen) {
-      int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
-      double Pt = 0.0, Ft = 0.0;
-      for (int b = 0; b < nb; b++) {
-        Pt += __ldcg(&A.blk_red[2 * (b0 + b)]);
-        Ft = fmax(Ft, __ldcg(&A.blk_red[2 * (b0 + b) + 1]));
-      }
       st.fire_P = Pt;
       st.fmax2 = Ft;
       st.fire_iter++;
