@@ -123,13 +123,20 @@ def c2_replica(seed):
     return W.smatb_bulk(seed=seed)
 
 
-def make_system(gems, ctx, w, prec, seed):
+def make_system(gems, ctx, w, prec, seed, tune=None):
+    """One C2 system; `tune` copies a launch shape, else the autotuner picks."""
     s = gems.System(w["pos"], w["mass"], ctx=ctx)
     s.set_box(w["L"], (True, True, True))
     s.set_smatb(*w["smatb"])
     s.set_skin(w["skin"])
     s.set_precision(prec)
     s.set_ermak(w["dt"], w["gamma"], w["temp"], seed=seed)
+    s.interact()
+    if tune is None:
+        s.tuned = s.autotune(10)
+    else:
+        s.set_lanes(tune[0], tune[1])
+        s.tuned = tune
     return s
 
 
@@ -307,8 +314,9 @@ def main():
                 continue
             prec = gems.PREC_FP64 if name == "fp64" else gems.PREC_MIXED
             nrep = args.replicas if name == "batched" else 1
-            ss = [make_system(gems, ctx, c2_replica(100 + k) if nrep > 1 else w, prec, seed=100 + k)
-                  for k in range(nrep)]
+            first = make_system(gems, ctx, c2_replica(100) if nrep > 1 else w, prec, seed=100)
+            ss = [first] + [make_system(gems, ctx, c2_replica(100 + k), prec, seed=100 + k, tune=first.tuned)
+                            for k in range(1, nrep)]
             for s_ in ss:
                 s_.interact()
             ts, nl = timed_blocks(ctx, torch, ss, blk, args.steps, args.warmup, flush, ext)
@@ -328,7 +336,7 @@ def main():
             dist.barrier()
         ts, nl = timed_blocks(ctx, torch, [s], blk, args.steps, args.warmup, flush, ext)
         arms[name] = {"value": s.n * blk * len(ts) / (sum(ts) * 1e-3), "ms_per_block": sum(ts) / len(ts),
-                      "atoms": s.n, "launches": nl}
+                      "atoms": s.n, "launches": nl, "lanes_variant": list(s.tuned[:2])}
         if name == "mixed":
             kern = s.time_kernels(50)
             mixed_sys = s
@@ -336,8 +344,9 @@ def main():
             kern64 = s.time_kernels(50)
             s.destroy()
     # --- batched arm: replicas in one launch
-    reps = [make_system(gems, ctx, c2_replica(100 + k + 1000 * rank), gems.PREC_MIXED, seed=100 + k)
-            for k in range(args.replicas)]
+    reps = [make_system(gems, ctx, c2_replica(100 + 1000 * rank), gems.PREC_MIXED, seed=100)]
+    reps += [make_system(gems, ctx, c2_replica(100 + k + 1000 * rank), gems.PREC_MIXED, seed=100 + k,
+                         tune=reps[0].tuned) for k in range(1, args.replicas)]
     for s in reps:
         s.interact()
     clocks = Clocks(dev)
@@ -356,7 +365,8 @@ def main():
         tot_ms = float(t.item())
     value = world * natoms * blk * len(ts) / (tot_ms * 1e-3)
     arms["batched"] = {"value": natoms * blk * len(ts) / (sum(ts) * 1e-3), "ms_per_block": sum(ts) / len(ts),
-                       "atoms": natoms, "replicas": len(reps), "launches": nl}
+                       "atoms": natoms, "replicas": len(reps), "launches": nl,
+                       "lanes_variant": list(reps[0].tuned[:2])}
     # --- e2e through the C ABI with host buffers
     te, h2d, d2h = timed_e2e(ctx, torch, reps, blk, args.steps, args.warmup, flush, ext)
     e2e_ms = sum(te)
@@ -374,10 +384,11 @@ def main():
     n1 = mixed_sys.n
     ach = force_bytes * n1 / (kern[1] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": None, "kernel": "k_smatb_force_mixed<8>", "peak_source": peak_kind,
+                "traffic": None, "kernel": "k_smatb_force_mixed", "peak_source": peak_kind,
                 "bytes_per_launch": force_bytes * n1, "ms_per_launch": kern[1],
                 "rho_kernel": {"ms_per_launch": kern[0], "bytes_per_launch": rho_bytes * n1},
                 "rebuild_ms": kern[2], "fp64_force_ms": kern64[1], "fp64_rho_ms": kern64[0],
+                "kernel_lanes_variant": list(mixed_sys.tuned[:2]),
                 "note": "working set is L2-resident (about 10 MB per replica)"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_ms / len(ts), "higher_is_better": True,

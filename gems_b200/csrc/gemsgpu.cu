@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -43,7 +44,9 @@ struct SysHost {
   bool first = true;        // next interact builds the list (update)
   bool pos_dirty = false;   // positions replaced from the host since the skin test
   bool has_forces = false;
-  int lanes = 8;            // atoms' list split (autotuned)
+  int lanes = 8;            // lanes per atom in the force kernels (autotuned)
+  int variant = 1;          // 1: species table in shared memory, 0: constants in
+                            //    registers (single-species mixed SMA-TB; autotuned)
   std::vector<PairP> prm;   // ntypes x ntypes
   SysDev d{};
   bool ff_set = false;
@@ -463,40 +466,69 @@ int sys_array(gemsgpu_ctx* ctx, const std::vector<int>& ss, const int** out) {
 }
 
 // ------------------------------------------------------------- launches
+// one SMA-TB pass (0: density, 1: force) for a block map of K lanes per atom
 template <int K>
-void launch_forces_k(gemsgpu_ctx* ctx, int ff, int prec, const BlockMap& m) {
+void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, const BlockMap& m) {
   cudaStream_t st = ctx->stream;
   const Arena& A = ctx->A;
-  if (m.nblk == 0) return;
-  if (ff == FF_SMATB) {
-    if (prec == PREC_MIXED) {
-      k_smatb_rho_mixed<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
-      k_smatb_force_mixed<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+  if (prec == PREC_MIXED) {
+    if (pass == 0) {
+      if (regs) k_smatb_rho_mixed<K, true><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else k_smatb_rho_mixed<K, false><<<m.nblk, BLOCK, 0, st>>>(A, m);
     } else {
-      k_smatb_rho_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
-      k_smatb_force_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
+      if (regs) k_smatb_force_mixed<K, true><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else k_smatb_force_mixed<K, false><<<m.nblk, BLOCK, 0, st>>>(A, m);
     }
-  } else if (ff == FF_LJ) {
-    if (prec == PREC_MIXED) {
-      k_lj_mixed<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
-    } else {
-      k_lj_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m); ++ctx->launches;
-    }
+  } else {
+    if (pass == 0) k_smatb_rho_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m);
+    else k_smatb_force_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m);
+  }
+  ++ctx->launches;
+}
+
+template <int K>
+void lj_k(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
+  if (prec == PREC_MIXED) k_lj_mixed<K><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  else k_lj_fp64<K><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  ++ctx->launches;
+}
+
+void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, bool regs, int K, const BlockMap& m) {
+  switch (K) {
+    case 2: smatb_pass_k<2>(ctx, pass, prec, regs, m); break;
+    case 4: smatb_pass_k<4>(ctx, pass, prec, regs, m); break;
+    case 8: smatb_pass_k<8>(ctx, pass, prec, regs, m); break;
+    case 16: smatb_pass_k<16>(ctx, pass, prec, regs, m); break;
+    case 32: smatb_pass_k<32>(ctx, pass, prec, regs, m); break;
+    default: smatb_pass_k<1>(ctx, pass, prec, regs, m); break;
+  }
+}
+
+void lj_pass(gemsgpu_ctx* ctx, int prec, int K, const BlockMap& m) {
+  switch (K) {
+    case 2: lj_k<2>(ctx, prec, m); break;
+    case 4: lj_k<4>(ctx, prec, m); break;
+    case 8: lj_k<8>(ctx, prec, m); break;
+    case 16: lj_k<16>(ctx, prec, m); break;
+    case 32: lj_k<32>(ctx, prec, m); break;
+    default: lj_k<1>(ctx, prec, m); break;
   }
 }
 
 // group systems by (ff, prec, lanes) and launch the force kernels
 int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
-  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+  std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;
   for (int s : ss) {
     const SysHost& h = ctx->sys[s];
     if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no force field", s);
     if (h.d.half) return fail(ctx, GEMSGPU_ERR_STATE, "system %d: force kernels need full lists", s);
     int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
-    groups[{h.d.ff, h.d.prec, K}].push_back(s);
+    int regs = (h.ntypes == 1 && h.variant == 0) ? 1 : 0;
+    groups[{h.d.ff, h.d.prec, K, regs}].push_back(s);
   }
   for (auto& kv : groups) {
     int ff = std::get<0>(kv.first), prec = std::get<1>(kv.first), K = std::get<2>(kv.first);
+    bool one = std::get<3>(kv.first) != 0;
     BlockMap m;
     if (ff == FF_TERSOFF) {
       CHK(get_map(ctx, kv.second, BLOCK, 0, &m));
@@ -509,13 +541,11 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
       continue;
     }
     CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
-    switch (K) {
-      case 1: launch_forces_k<1>(ctx, ff, prec, m); break;
-      case 2: launch_forces_k<2>(ctx, ff, prec, m); break;
-      case 4: launch_forces_k<4>(ctx, ff, prec, m); break;
-      case 8: launch_forces_k<8>(ctx, ff, prec, m); break;
-      case 16: launch_forces_k<16>(ctx, ff, prec, m); break;
-      default: launch_forces_k<32>(ctx, ff, prec, m); break;
+    if (ff == FF_SMATB) {
+      smatb_pass(ctx, 0, prec, one, K, m);
+      smatb_pass(ctx, 1, prec, one, K, m);
+    } else if (ff == FF_LJ) {
+      lj_pass(ctx, prec, K, m);
     }
   }
   CU(cudaGetLastError());
@@ -525,11 +555,12 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
 // the rebuild chain; every kernel returns at once for systems whose
 // rebuild flag is clear, so the chain can sit in a captured step.
 int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 0) {
-  BlockMap ma, mc, mw;
+  BlockMap ma, mc, mw, mc8;
   const int* sa;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
   CHK(get_map(ctx, ss, 256, 1, &mc));
   CHK(get_map(ctx, ss, LIST_ATOMS, 0, &mw));
+  CHK(get_map(ctx, ss, BLOCK / 32, 1, &mc8));
   CHK(sys_array(ctx, ss, &sa));
   cudaStream_t st = ctx->stream;
   const Arena& A = ctx->A;
@@ -541,7 +572,7 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 
     k_scan1<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
     k_scan2<<<(int)ss.size(), BLOCK, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
     k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
-    k_sort_cells<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
+    k_sort_cells<<<mc8.nblk, BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
     k_list_cells<<<mw.nblk, BLOCK, LIST_ATOMS * A.lcap * sizeof(int), st>>>(A, mw); ++ctx->launches;
   }
   if (n2) {
@@ -803,6 +834,7 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
     CHK(get_map(ctx, ss, BLOCK, 0, &m));
     CHK(get_map(ctx, ss, 256, 1, &m));
     CHK(get_map(ctx, ss, LIST_ATOMS, 0, &m));
+    CHK(get_map(ctx, ss, BLOCK / 32, 1, &m));
     CHK(sys_array(ctx, ss, &sa));
     std::map<std::tuple<int, int, int>, std::vector<int>> groups;
     for (int s : ss) {
@@ -975,6 +1007,9 @@ int gemsgpu_create(int device, int64_t max_atoms, int max_systems, gemsgpu_ctx**
   if (device < 0 || device >= ndev) return GEMSGPU_ERR_ARG;
   auto* ctx = new gemsgpu_ctx();
   ctx->device = device;
+  // profilers cannot replay kernels of graphs with conditional nodes:
+  // GEMSGPU_NO_COND=1 captures plain steps (rebuild kernels exit early)
+  if (const char* e = getenv("GEMSGPU_NO_COND")) ctx->use_cond = !(e[0] == '1');
   int rc = 0;
   do {
     if (cudaSetDevice(device) != cudaSuccess) { rc = GEMSGPU_ERR_CUDA; break; }
@@ -1633,6 +1668,66 @@ int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys, double* epo
   return 0;
 }
 
+int gemsgpu_autotune(gemsgpu_ctx* ctx, int sys, int reps, int* lanes_out, int* variant_out,
+                     double* best_ms) {
+  CHK(check_sys(ctx, sys));
+  if (reps <= 0) reps = 10;
+  cudaSetDevice(ctx->device);
+  SysHost& h = ctx->sys[sys];
+  if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "autotune: no force field");
+  std::vector<int> ss{sys};
+  if (h.first || h.pos_dirty || !h.has_forces) CHK(interact_group(ctx, ss, true));
+  std::vector<std::pair<int, int>> cand;
+  if (h.d.ff == FF_TERSOFF) {
+    cand.push_back({1, 1});
+  } else {
+    for (int K : {2, 4, 8, 16, 32}) {
+      cand.push_back({K, 1});
+      if (h.d.ff == FF_SMATB && h.ntypes == 1 && h.d.prec == PREC_MIXED) cand.push_back({K, 0});
+    }
+  }
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  double best = 1e30;
+  std::pair<int, int> pick = {h.lanes, h.variant};
+  for (auto c : cand) {
+    h.lanes = c.first;
+    h.variant = c.second;
+    CHK(launch_forces(ctx, ss));  // warm-up (and map creation)
+    CU(cudaEventRecord(e0, ctx->stream));
+    for (int r = 0; r < reps; r++) CHK(launch_forces(ctx, ss));
+    CU(cudaEventRecord(e1, ctx->stream));
+    CU(cudaEventSynchronize(e1));
+    float ms;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms / reps < best) {
+      best = ms / reps;
+      pick = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h.lanes = pick.first;
+  h.variant = pick.second;
+  invalidate(ctx);
+  if (lanes_out) *lanes_out = h.lanes;
+  if (variant_out) *variant_out = h.variant;
+  if (best_ms) *best_ms = best;
+  return 0;
+}
+
+int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant) {
+  CHK(check_sys(ctx, sys));
+  if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(ctx, GEMSGPU_ERR_ARG, "lanes must be a power of two <= 32");
+  SysHost& h = ctx->sys[sys];
+  if (h.d.ff != FF_TERSOFF) h.lanes = lanes;
+  h.variant = variant ? 1 : 0;
+  invalidate(ctx);
+  return 0;
+}
+
 int gemsgpu_get_stream(gemsgpu_ctx* ctx, void** stream) {
   if (!ctx || !stream) return GEMSGPU_ERR_ARG;
   *stream = (void*)ctx->stream;
@@ -1658,41 +1753,13 @@ int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms) {
   CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / K, 0, &m));
   cudaEvent_t ev[6];
   for (auto& e : ev) CU(cudaEventCreate(&e));
-  const Arena& A = ctx->A;
+  const bool regs = h.ntypes == 1 && h.variant == 0;
   auto first_kernel = [&]() {
-    if (h.d.ff == FF_SMATB) {
-      if (h.d.prec == PREC_MIXED) {
-        switch (K) {
-          case 4: k_smatb_rho_mixed<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-          case 16: k_smatb_rho_mixed<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-          default: k_smatb_rho_mixed<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-        }
-      } else {
-        switch (K) {
-          case 4: k_smatb_rho_fp64<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-          case 16: k_smatb_rho_fp64<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-          default: k_smatb_rho_fp64<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-        }
-      }
-    } else {
-      launch_forces(ctx, ss);
-    }
+    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 0, h.d.prec, regs, K, m);
+    else launch_forces(ctx, ss);
   };
   auto second_kernel = [&]() {
-    if (h.d.ff != FF_SMATB) return;
-    if (h.d.prec == PREC_MIXED) {
-      switch (K) {
-        case 4: k_smatb_force_mixed<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-        case 16: k_smatb_force_mixed<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-        default: k_smatb_force_mixed<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-      }
-    } else {
-      switch (K) {
-        case 4: k_smatb_force_fp64<4><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-        case 16: k_smatb_force_fp64<16><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-        default: k_smatb_force_fp64<8><<<m.nblk, BLOCK, 0, ctx->stream>>>(A, m); break;
-      }
-    }
+    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 1, h.d.prec, regs, K, m);
   };
   first_kernel();
   second_kernel();

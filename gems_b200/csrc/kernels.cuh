@@ -365,7 +365,7 @@ __global__ void k_sort_cells(Arena A, BlockMap C) {
   if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
   const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int first = C.first[blockIdx.x], end = C.end[blockIdx.x];
-  for (int c = first + warp; c < end; c += BLOCK / 32) {
+  for (int c = first + warp; c < end; c += BLOCK / 32) {  // C: 8 cells per block
     int start = A.chunk_sum[c >> 8] + A.cell_loc[c];
     int n = A.cell_n[c];
     if (ln == 0) A.cell_start[c] = start;
@@ -589,10 +589,19 @@ struct GFx { int4 x; float eb; };
 // smatb_preinteraction (src/TB.F90:367-455), FP64: rho_i = sum_j
 //   xi^2 exp(-2q(r/r0-1))            r <  rci
 //   (b1 d^5 + b2 d^4 + b3 d^3)^2     rci <= r <= rce, d = r - rce
+__device__ __forceinline__ const SmFP64* sm_table(const Arena& A, const SysDev& S, SmFP64* sh) {
+  const int np = S.ntypes * S.ntypes;
+  for (int t = threadIdx.x; t < np; t += BLOCK) sh[t] = sm_load(A.prm[S.param_off + t]);
+  __syncthreads();
+  return sh;
+}
+
 template <int K>
 __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
   int s = blk_sys(M);
   const SysDev& S = A.sys[s];
+  __shared__ SmFP64 tab_sh[MAXT * MAXT];
+  const SmFP64* tab = sm_table(A, S, tab_sh);
   int i = M.first[blockIdx.x] + threadIdx.x / K;
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
@@ -602,10 +611,9 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
     const int ti = A.type[i];
     const int nn = min(A.nn[i], A.lcap);
     const bool one = S.ntypes == 1;
-    SmFP64 c = sm_load(A.prm[S.param_off]);
     auto gat = [&](int j) { return A.pos[j]; };
     PAIR_LOOP_BEGIN(double4, gat)
-      if (!one) c = sm_load(A.prm[S.param_off + ti * S.ntypes + A.type[j]]);
+      const SmFP64& c = tab[one ? 0 : ti * S.ntypes + A.type[j]];
       double v0, v1, v2;
       vd_fp64(S, xi, gj[u], v0, v1, v2);
       double dr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
@@ -639,6 +647,8 @@ template <int K>
 __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M) {
   int s = blk_sys(M);
   const SysDev& S = A.sys[s];
+  __shared__ SmFP64 tab_sh[MAXT * MAXT];
+  const SmFP64* tab = sm_table(A, S, tab_sh);
   int i = M.first[blockIdx.x] + threadIdx.x / K;
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
@@ -649,10 +659,9 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
     const double ebi = A.eband[i];
     const int nn = min(A.nn[i], A.lcap);
     const bool one = S.ntypes == 1;
-    SmFP64 c = sm_load(A.prm[S.param_off]);
     auto gat = [&](int j) { GPos g; g.x = A.pos[j]; g.eb = A.eband[j]; return g; };
     PAIR_LOOP_BEGIN(GPos, gat)
-      if (!one) c = sm_load(A.prm[S.param_off + ti * S.ntypes + A.type[j]]);
+      const SmFP64& c = tab[one ? 0 : ti * S.ntypes + A.type[j]];
       double v0, v1, v2;
       vd_fp64(S, xi, gj[u].x, v0, v1, v2);
       double dr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
@@ -734,10 +743,33 @@ __device__ __forceinline__ float ex2f(float x) {
   return y;
 }
 
-template <int K>
+// r = sqrt(r2) and 1/r from one MUFU rsqrt plus a Newton step on r
+// (accurate to ~1 ulp without the IEEE sqrt / rcp instruction sequences)
+__device__ __forceinline__ float sqrt_nr(float r2, float& rinv) {
+  rinv = rsqrtf(r2);
+  float r = r2 * rinv;
+  return fmaf(0.5f * rinv, fmaf(-r, r, r2), r);
+}
+
+// Mixed kernels sum the FP32 pair terms of one UNR group in FP32 and add the
+// group sums to FP64 per-atom accumulators (one conversion per group).
+// ONE: single-species system, constants held in registers; otherwise the
+// species-pair table sits in shared memory and is read per pair.
+template <bool ONE>
+__device__ __forceinline__ const SmF32* smf_table(const Arena& A, const SysDev& S, SmF32* sh) {
+  if (ONE) return nullptr;
+  const int np = S.ntypes * S.ntypes;
+  for (int t = threadIdx.x; t < np; t += BLOCK) sh[t] = smf_load(A.prm[S.param_off + t]);
+  __syncthreads();
+  return sh;
+}
+
+template <int K, bool ONE>
 __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
   const SysDev& S = A.sys[s];
+  __shared__ SmF32 tab_sh[ONE ? 1 : MAXT * MAXT];
+  const SmF32* tab = smf_table<ONE>(A, S, tab_sh);
   int i = M.first[blockIdx.x] + threadIdx.x / K;
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
@@ -745,27 +777,42 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
   if (act) {
     const int4 xi = A.fxp[i];
     const int nn = min(A.nn[i], A.lcap);
-    const bool one = S.ntypes == 1;
-    SmF32 c = smf_load(A.prm[S.param_off]);
-    auto gat = [&](int j) { return A.fxp[j]; };
-    PAIR_LOOP_BEGIN(int4, gat)
-      const int4 xj = gj[u];
-      if (!one) c = smf_load(A.prm[S.param_off + xi.w * S.ntypes + xj.w]);
-      float v0, v1, v2;
-      vd_fx(S, xi, xj, v0, v1, v2);
-      float r2 = v0 * v0 + v1 * v1 + v2 * v2;
-      if (r2 > c.rce2) continue;
-      float dr = sqrtf(r2);
-      float banda;
-      if (dr < c.rci) {
-        banda = c.eps2 * ex2f(c.kq * (c.r0 - dr));
-      } else {
-        float d = dr - c.rce, d2 = d * d, d3 = d2 * d;
-        banda = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
-        banda = banda * banda;
+    const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
+    for (int m0 = lane; m0 < nn; m0 += UNR * K) {
+      int jj[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        int m = m0 + u * K;
+        jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;
       }
-      band += (double)banda;
-    PAIR_LOOP_END
+      int4 gj[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; u++)
+        if (jj[u] >= 0) gj[u] = A.fxp[jj[u]];
+      float grp = 0.0f;
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        if (jj[u] < 0) continue;
+        const int4 xj = gj[u];
+        const SmF32& c = ONE ? c1 : tab[xi.w * S.ntypes + xj.w];
+        float v0, v1, v2;
+        vd_fx(S, xi, xj, v0, v1, v2);
+        float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+        if (r2 > c.rce2) continue;
+        float rinv;
+        float dr = sqrt_nr(r2, rinv);
+        float banda;
+        if (dr < c.rci) {
+          banda = c.eps2 * ex2f(c.kq * (c.r0 - dr));
+        } else {
+          float d = dr - c.rce, d2 = d * d, d3 = d2 * d;
+          banda = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+          banda = banda * banda;
+        }
+        grp += banda;
+      }
+      band += (double)grp;
+    }
   }
   band = lane_sum<K>(band);
   if (act && lane == 0) {
@@ -776,10 +823,12 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
   }
 }
 
-template <int K>
+template <int K, bool ONE>
 __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
   const SysDev& S = A.sys[s];
+  __shared__ SmF32 tab_sh[ONE ? 1 : MAXT * MAXT];
+  const SmF32* tab = smf_table<ONE>(A, S, tab_sh);
   int i = M.first[blockIdx.x] + threadIdx.x / K;
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
@@ -788,41 +837,62 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M
     const int4 xi = A.fxp[i];
     const float ebi = A.ebandf[i];
     const int nn = min(A.nn[i], A.lcap);
-    const bool one = S.ntypes == 1;
-    SmF32 c = smf_load(A.prm[S.param_off]);
+    const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
     const float evui = (float)EV_UI;
-    auto gat = [&](int j) { GFx g; g.x = A.fxp[j]; g.eb = A.ebandf[j]; return g; };
-    PAIR_LOOP_BEGIN(GFx, gat)
-      const int4 xj = gj[u].x;
-      if (!one) c = smf_load(A.prm[S.param_off + xi.w * S.ntypes + xj.w]);
-      float v0, v1, v2;
-      vd_fx(S, xi, xj, v0, v1, v2);
-      float r2 = v0 * v0 + v1 * v1 + v2 * v2;
-      if (r2 > c.rce2) continue;
-      float dr = sqrtf(r2);
-      float rinv = __frcp_rn(dr);
-      float ebs = ebi + gj[u].eb;
-      float factor, repul;
-      if (dr <= c.rci) {
-        float x = c.r0 - dr;
-        float e1 = ex2f(c.kp * x);
-        float e2 = ex2f(c.kq * x);
-        repul = c.A * e1;
-        factor = c.c1 * e1 - c.c2 * e2 * ebs;
-      } else {
-        float d = dr - c.rce, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
-        float P = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
-        float dP = 5.0f * c.b1 * d4 + 4.0f * c.b2 * d3 + 3.0f * c.b3 * d2;
-        float dR = 5.0f * c.r1 * d4 + 4.0f * c.r2 * d3 + 3.0f * c.r3 * d2;
-        factor = P * dP * ebs - 2.0f * dR;
-        repul = (c.r1 * d2 + c.r2 * d + c.r3) * d3;
+    for (int m0 = lane; m0 < nn; m0 += UNR * K) {
+      int jj[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        int m = m0 + u * K;
+        jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;
       }
-      float fr = factor * evui * rinv;
-      f0 -= (double)(fr * v0);
-      f1 -= (double)(fr * v1);
-      f2 -= (double)(fr * v2);
-      ep += (double)repul;
-    PAIR_LOOP_END
+      int4 gj[UNR];
+      float gb[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; u++)
+        if (jj[u] >= 0) {
+          gj[u] = A.fxp[jj[u]];
+          gb[u] = A.ebandf[jj[u]];
+        }
+      float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, ge = 0.0f;
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        if (jj[u] < 0) continue;
+        const int4 xj = gj[u];
+        const SmF32& c = ONE ? c1 : tab[xi.w * S.ntypes + xj.w];
+        float v0, v1, v2;
+        vd_fx(S, xi, xj, v0, v1, v2);
+        float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+        if (r2 > c.rce2) continue;
+        float rinv;
+        float dr = sqrt_nr(r2, rinv);
+        float ebs = ebi + gb[u];
+        float factor, repul;
+        if (dr <= c.rci) {
+          float x = c.r0 - dr;
+          float e1 = ex2f(c.kp * x);
+          float e2 = ex2f(c.kq * x);
+          repul = c.A * e1;
+          factor = c.c1 * e1 - c.c2 * e2 * ebs;
+        } else {
+          float d = dr - c.rce, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
+          float P = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+          float dP = 5.0f * c.b1 * d4 + 4.0f * c.b2 * d3 + 3.0f * c.b3 * d2;
+          float dR = 5.0f * c.r1 * d4 + 4.0f * c.r2 * d3 + 3.0f * c.r3 * d2;
+          factor = P * dP * ebs - 2.0f * dR;
+          repul = (c.r1 * d2 + c.r2 * d + c.r3) * d3;
+        }
+        float fr = factor * evui * rinv;
+        g0 = fmaf(fr, v0, g0);
+        g1 = fmaf(fr, v1, g1);
+        g2 = fmaf(fr, v2, g2);
+        ge += repul;
+      }
+      f0 -= (double)g0;
+      f1 -= (double)g1;
+      f2 -= (double)g2;
+      ep += (double)ge;
+    }
   }
   f0 = lane_sum<K>(f0);
   f1 = lane_sum<K>(f1);
@@ -1011,7 +1081,8 @@ __global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
       if (b == a) continue;
       R ct = u[0] * bu[b][0] + u[1] * bu[b][1] + u[2] * bu[b][2];
       R hc = h - ct;
-      R g = R(1) + c2d2 - c2 / (d2 + hc * hc);
+      R hc2 = hc * hc;
+      R g = R(1) + c2d2 * hc2 / (d2 + hc2);  // = 1 + c2/d2 - c2/(d2+hc2), no cancellation
       zij += bfcr[b] * g;
     }
     double dfc_a;
@@ -1049,7 +1120,7 @@ __global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
       R ct = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
       R hc = h - ct;
       R den = d2 + hc * hc;
-      R g = R(1) + c2d2 - c2 / den;
+      R g = R(1) + c2d2 * (hc * hc) / den;
       R dg = R(-2) * c2 * hc / (den * den);
       R ka = pre * bfcr[b] * dg * irij;
       R kb = pre * bfcr[b] * dg * irik;

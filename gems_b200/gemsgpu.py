@@ -71,6 +71,8 @@ _SIGS = {
     "gemsgpu_batch_energy": (_i, [_p, _ip, _i, _dp, _dp, _dp]),
     "gemsgpu_get_launch_count": (_i, [_p, ctypes.POINTER(_l)]),
     "gemsgpu_get_stream": (_i, [_p, ctypes.POINTER(_p)]),
+    "gemsgpu_autotune": (_i, [_p, _i, _i, _ip, _ip, _dp]),
+    "gemsgpu_set_lanes": (_i, [_p, _i, _i, _i]),
     "gemsgpu_time_kernels": (_i, [_p, _i, _i, _dp]),
 }
 
@@ -349,6 +351,16 @@ class System:
 
     def epot_sum(self):
         return self.energy()[0] * EV_UI
+
+    def autotune(self, reps=10):
+        """Pick the fastest force-kernel launch shape; returns (lanes, variant, ms)."""
+        k, v, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._c(lib().gemsgpu_autotune(self.ctx.h, self.sid, int(reps), ctypes.byref(k), ctypes.byref(v),
+                                       ctypes.byref(ms)))
+        return k.value, v.value, ms.value
+
+    def set_lanes(self, lanes, variant=1):
+        self._c(lib().gemsgpu_set_lanes(self.ctx.h, self.sid, int(lanes), int(variant)))
 
     def time_kernels(self, reps=20):
         """Mean ms of (first force kernel, second force kernel, list rebuild)."""

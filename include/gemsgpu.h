@@ -194,6 +194,18 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys,
 int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys,
                          double* epot_ev, double* ekin_ev, double* temp);
 
+/* ------------------------------------------------------------ tuning */
+
+/* Time the system's force kernels over the candidate launch shapes (lanes
+ * per atom 2..32 and, for single-species mixed SMA-TB, species constants in
+ * registers or in shared memory) and keep the fastest.  reps timed
+ * evaluations per candidate.  No reference counterpart (GEMS has no device
+ * code); the choice changes summation order only. */
+int gemsgpu_autotune(gemsgpu_ctx* ctx, int sys, int reps, int* lanes_out,
+                     int* variant_out, double* best_ms);
+/* Set the launch shape by hand (lanes: 1,2,4,...,32; variant 0/1). */
+int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant);
+
 /* ------------------------------------------------------------ measurement */
 
 /* The context's CUDA stream (a cudaStream_t), for callers that order their

@@ -321,3 +321,26 @@ def test_skin_modes_same_trajectory(ctx):
     d -= w["L"][0] * np.round(d / w["L"][0])
     assert np.abs(d).max() < 1e-9
     assert abs(e_mic[0] - e_ref[0]) / len(p_ref) < 1e-10
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_launch_shapes_agree(ctx, prec):
+    """Every lanes-per-atom / constant-placement shape the autotuner may pick
+    gives the same forces within the precision's tolerance."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=6)
+
+    def setup(s):
+        s.set_box(w["L"], (True, True, True))
+        s.set_smatb(*w["smatb"])
+    o, g = both(w["pos"], w["mass"], ctx, setup=setup)
+    g.set_precision(prec)
+    o.interact()
+    fo = o.force
+    for lanes in (1, 2, 4, 8, 16, 32):
+        for variant in (0, 1):
+            g.set_lanes(lanes, variant)
+            g.interact()
+            assert relrms(g.force, fo) <= (RMS_FP64 if prec == 0 else RMS_MIXED)
+    k, v, ms = g.autotune(3)
+    assert k in (2, 4, 8, 16, 32) and ms > 0
