@@ -9,9 +9,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(HERE, "csrc", "gemsgpu.cu")
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu")]
 OUT = os.path.join(HERE, "libgemsgpu.so")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "kernels.cuh", "common.cuh")] + [
+DEPS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu", "kernels.cuh", "common.cuh")] + [
     os.path.join(os.path.dirname(HERE), "include", "gemsgpu.h")]
 
 NVCC_FLAGS = [
@@ -39,7 +39,7 @@ def stale():
 def build(force=False, verbose=False, extra=()):
     if not force and not stale():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", OUT, SRC]
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", OUT, *SRCS]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -73,6 +73,7 @@ _SIGS = {
     "gemsgpu_get_stream": (_i, [_p, ctypes.POINTER(_p)]),
     "gemsgpu_autotune": (_i, [_p, _i, _i, _ip, _ip, _dp]),
     "gemsgpu_set_lanes": (_i, [_p, _i, _i, _i]),
+    "gemsgpu_smatb_forces_noalloc": (_i, [_p, _i, _i, _dp, _ip, _d, _d, _d, _d, _d, _d, _d, _p, _p, _p]),
     "gemsgpu_time_kernels": (_i, [_p, _i, _i, _dp]),
 }
 

@@ -194,6 +194,37 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys,
 int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys,
                          double* epot_ev, double* ekin_ev, double* temp);
 
+/* ------------------------------------------------------------ no allocation */
+
+/* Largest system gemsgpu_smatb_forces_noalloc accepts. */
+#define GEMSGPU_NOALLOC_MAX_ATOMS 16384
+
+/* SMA-TB forces for callers that cannot allocate device memory -- a host
+ * that hands the library only buffers from its own fixed device budget, or
+ * code running where cudaMalloc/cudaFree are not allowed (they synchronise
+ * the device and are refused during CUDA-graph stream capture).  This entry
+ * point has no counterpart in the reference (GEMS has no device code); it
+ * computes what smatb_interact computes for one species (A, xi, p, q, r0,
+ * rci, rce as in gemsgpu_set_smatb) from caller-owned DEVICE buffers:
+ *   d_pos   positions, 3n doubles, GEMS interleaved layout (read);
+ *   d_force forces, 3n doubles (written), internal units;
+ *   d_epot  per-atom potential energy, n doubles (written), internal units.
+ * boxed/L/pbc as in gemsgpu_set_box.  Work is queued on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream) and not waited for.
+ * It allocates nothing: its only scratch is a fixed file-scope device array
+ * of 2 x GEMSGPU_NOALLOC_MAX_ATOMS doubles (256 KiB) that every GPU loading
+ * the library holds until exit.  n > GEMSGPU_NOALLOC_MAX_ATOMS returns
+ * GEMSGPU_ERR_FULL without launching.  The first call on a device looks up
+ * the array's device address, so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (two
+ * streams, or two host threads) race; calls ordered on one stream do not. */
+int gemsgpu_smatb_forces_noalloc(const double* d_pos, int n, int boxed,
+                                 const double L[3], const int pbc[3],
+                                 double A, double xi, double p, double q,
+                                 double r0, double rci, double rce,
+                                 double* d_force, double* d_epot,
+                                 void* stream);
+
 /* ------------------------------------------------------------ tuning */
 
 /* Time the system's force kernels over the candidate launch shapes (lanes
