@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--arms", default="fp64,mixed,batched",
                     help="comma list of arms to run (profiling); the full line needs all three")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--tune", default=None,
+                    help="lanes,variant for every mixed system instead of the autotuner (profiling)")
     return ap.parse_args()
 
 
@@ -123,6 +125,9 @@ def c2_replica(seed):
     return W.smatb_bulk(seed=seed)
 
 
+FIXED_TUNE = None
+
+
 def make_system(gems, ctx, w, prec, seed, tune=None):
     """One C2 system; `tune` copies a launch shape, else the autotuner picks."""
     s = gems.System(w["pos"], w["mass"], ctx=ctx)
@@ -132,6 +137,8 @@ def make_system(gems, ctx, w, prec, seed, tune=None):
     s.set_precision(prec)
     s.set_ermak(w["dt"], w["gamma"], w["temp"], seed=seed)
     s.interact()
+    if tune is None and FIXED_TUNE is not None:
+        tune = FIXED_TUNE
     if tune is None:
         s.tuned = s.autotune(10)
     else:
@@ -282,7 +289,10 @@ def run_reference(args):
 
 
 def main():
+    global FIXED_TUNE
     args = parse()
+    if args.tune:
+        FIXED_TUNE = tuple(int(v) for v in args.tune.split(","))
     if args.impl == "reference":
         run_reference(args)
         return

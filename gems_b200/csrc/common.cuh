@@ -16,18 +16,20 @@ constexpr int BLOCK = 256;         // threads per block of every kernel
 constexpr int NSTENCIL = 27;
 
 // 27-cell stencil in the reference's order (src/Neighbour.F90:75-83):
-// 0 centre, 1..13 the upper half, 14..26 the lower half.
-__host__ __device__ inline void stencil(int k, int& dx, int& dy, int& dz) {
-  constexpr signed char m[27][3] = {
-      {0, 0, 0},   {1, 0, 0},   {1, 1, 0},   {0, 1, 0},   {-1, 1, 0},
-      {1, 0, -1},  {1, 1, -1},  {0, 1, -1},  {-1, 1, -1}, {1, 0, 1},
-      {1, 1, 1},   {0, 1, 1},   {-1, 1, 1},  {0, 0, 1},   {-1, 0, 0},
-      {-1, -1, 0}, {0, -1, 0},  {1, -1, 0},  {-1, 0, 1},  {-1, -1, 1},
-      {0, -1, 1},  {1, -1, 1},  {-1, 0, -1}, {-1, -1, -1}, {0, -1, -1},
-      {1, -1, -1}, {0, 0, -1}};
-  dx = m[k][0];
-  dy = m[k][1];
-  dz = m[k][2];
+// 0 centre, 1..13 the upper half, 14..26 the lower half.  Kept in constant
+// memory: a function-local table would be rebuilt in local memory per call.
+__constant__ signed char c_stencil[27][3] = {
+    {0, 0, 0},   {1, 0, 0},   {1, 1, 0},   {0, 1, 0},   {-1, 1, 0},
+    {1, 0, -1},  {1, 1, -1},  {0, 1, -1},  {-1, 1, -1}, {1, 0, 1},
+    {1, 1, 1},   {0, 1, 1},   {-1, 1, 1},  {0, 0, 1},   {-1, 0, 0},
+    {-1, -1, 0}, {0, -1, 0},  {1, -1, 0},  {-1, 0, 1},  {-1, -1, 1},
+    {0, -1, 1},  {1, -1, 1},  {-1, 0, -1}, {-1, -1, -1}, {0, -1, -1},
+    {1, -1, -1}, {0, 0, -1}};
+
+__device__ __forceinline__ void stencil(int k, int& dx, int& dy, int& dz) {
+  dx = c_stencil[k][0];
+  dy = c_stencil[k][1];
+  dz = c_stencil[k][2];
 }
 
 enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
