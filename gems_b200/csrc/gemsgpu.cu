@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <string>
@@ -50,6 +51,7 @@ struct SysHost {
   std::vector<PairP> prm;   // ntypes x ntypes
   SysDev d{};
   bool ff_set = false;
+  double temp = 0.0;        // Ermak bath temperature (K)
 };
 
 struct Graph {
@@ -96,6 +98,57 @@ struct gemsgpu_ctx {
   int64_t snap_cap = 0;
   double4* snap = nullptr;      // pos, vel, acel, force
   SysState* snap_st = nullptr;
+};
+
+// A pool: a fixed-capacity batch of systems sharing one force-field kind and
+// launch shape.  Its block maps live in device buffers sized for the
+// capacity and padded with empty blocks, so one captured graph serves any
+// active set -- changing the set rewrites the maps, not the graph.
+struct gemsgpu_pool {
+  gemsgpu_ctx* ctx = nullptr;
+  int max_systems = 0;
+  int64_t max_atoms = 0, max_cells = 0;
+  int ff = 0, prec = 0, lanes = 8, variant = 1, chunk = 50;
+  std::vector<int> active;  // system ids
+  // map kinds: 0 atoms/256, 1 cells/256, 2 atoms/LIST_ATOMS, 3 cells/8, 4 atoms/(256/K)
+  int cap[5] = {0, 0, 0, 0, 0};
+  int* dmap[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int* dsys = nullptr;      // padded system array
+  int scap = 0;             // system-id capacity of the per-system map arrays
+  gg::BlockMap maps[5];
+  bool maps_dirty = true;
+  cudaGraphExec_t exec = nullptr;
+  gg::Arena captured{};     // arena the graph was captured against
+  int64_t nodes = 0, body_nodes = 0;
+  std::vector<int> host_buf;
+};
+
+// Serving loop: jobs (FIRE relaxations, short Langevin runs) arrive at any
+// time, wait in a queue, are admitted into the pool while memory and slots
+// allow, advance together chunk by chunk, and leave when done.
+struct ServerJob {
+  int64_t id = 0;
+  gemsgpu_job spec{};
+  std::vector<double> pos;   // input copy, then the final positions
+  int state = 0;             // GEMSGPU_JOB_*
+  int sys = -1;
+  int done_steps = 0;
+  double epot_ev = 0.0, ekin_ev = 0.0, fmax_ev = 0.0;
+  int iters = 0;
+  int error = 0;
+};
+
+struct gemsgpu_server {
+  gemsgpu_ctx* ctx = nullptr;
+  gemsgpu_pool* pool = nullptr;
+  int max_jobs = 0;
+  int64_t max_atoms = 0;
+  int chunk = 50;
+  int64_t next_id = 1;
+  int64_t atoms_in = 0;
+  std::deque<int64_t> queue;
+  std::vector<int64_t> running;
+  std::map<int64_t, ServerJob> jobs;
 };
 
 namespace {
@@ -587,7 +640,9 @@ int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss,
                   cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
-  k_step_a<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond, use_cond); ++ctx->launches;
+  if (use_cond) k_step_a<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  else k_step_a<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
 }
@@ -608,10 +663,12 @@ int read_states(gemsgpu_ctx* ctx) {
 }
 
 int clear_status(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
-  for (int s : ss) {
-    CU(cudaMemsetAsync(&ctx->A.st[s].status, 0, sizeof(int), ctx->stream));
-    CU(cudaMemsetAsync(&ctx->A.st[s].maxnn, 0, sizeof(int), ctx->stream));
-  }
+  if (ss.empty()) return 0;
+  const int* sa;
+  CHK(sys_array(ctx, ss, &sa));
+  k_clear_status<<<((int)ss.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size());
+  ++ctx->launches;
+  CU(cudaGetLastError());
   return 0;
 }
 
@@ -990,6 +1047,292 @@ int d2h_xyz(gemsgpu_ctx* ctx, const double4* src, double* dst, int n) {
 void copy_interleaved_to_d4(const double* src, std::vector<double4>& dst, int n) {
   dst.resize(n);
   for (int i = 0; i < n; i++) dst[i] = make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0);
+}
+
+// ------------------------------------------------------------- pools
+int pool_kind_apb(const gemsgpu_pool* P, int kind) {
+  switch (kind) {
+    case 0: return BLOCK;
+    case 1: return 256;
+    case 2: return LIST_ATOMS;
+    case 3: return BLOCK / 32;
+    default: return BLOCK / P->lanes;
+  }
+}
+
+int pool_alloc(gemsgpu_pool* P) {
+  gemsgpu_ctx* ctx = P->ctx;
+  for (int k = 0; k < 5; k++) {
+    int64_t units = (k == 1 || k == 3) ? P->max_cells : P->max_atoms;
+    int apb = pool_kind_apb(P, k);
+    P->cap[k] = (int)((units + apb - 1) / apb + P->max_systems);
+    if (P->cap[k] < 1) P->cap[k] = 1;
+    // sys, first, end (cap each) + sys_blk0, sys_nblk (scap each)
+    CHK(dalloc(ctx, &P->dmap[k], 3 * (size_t)P->cap[k] + 2 * (size_t)P->scap));
+    BlockMap& m = P->maps[k];
+    m.nblk = P->cap[k];
+    m.apb = apb;
+    m.sys = P->dmap[k];
+    m.first = P->dmap[k] + P->cap[k];
+    m.end = P->dmap[k] + 2 * P->cap[k];
+    m.sys_blk0 = P->dmap[k] + 3 * P->cap[k];
+    m.sys_nblk = P->dmap[k] + 3 * P->cap[k] + P->scap;
+  }
+  CHK(dalloc(ctx, &P->dsys, P->max_systems));
+  CHK(grow_blocks(ctx, *std::max_element(P->cap, P->cap + 5)));
+  return 0;
+}
+
+// write the padded maps of the current active set
+int pool_upload_maps(gemsgpu_pool* P) {
+  gemsgpu_ctx* ctx = P->ctx;
+  for (int k = 0; k < 5; k++) {
+    const int cap = P->cap[k], apb = pool_kind_apb(P, k);
+    std::vector<int>& b = P->host_buf;
+    b.assign(3 * (size_t)cap + 2 * (size_t)P->scap, 0);
+    int* bs = b.data();
+    int* bf = bs + cap;
+    int* be = bs + 2 * cap;
+    int* b0 = bs + 3 * cap;
+    int* nb = b0 + P->scap;
+    int n = 0;
+    for (int s : P->active) {
+      const SysHost& h = ctx->sys[s];
+      int lo, hi;
+      if (k == 1 || k == 3) {
+        if (!h.d.use_cells) continue;
+        lo = h.cell_off;
+        hi = h.cell_off + h.d.ncell;
+      } else {
+        lo = h.off;
+        hi = h.off + h.n;
+      }
+      b0[s] = n;
+      for (int a = lo; a < hi; a += apb) {
+        if (n >= cap) return fail(ctx, GEMSGPU_ERR_FULL, "pool map capacity exceeded");
+        bs[n] = s;
+        bf[n] = a;
+        be[n] = std::min(hi, a + apb);
+        n++;
+      }
+      nb[s] = n - b0[s];
+    }
+    for (int q = n; q < cap; q++) bs[q] = -1;
+    CU(cudaMemcpyAsync(P->dmap[k], b.data(), b.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  std::vector<int> sa(P->max_systems, -1);
+  for (size_t q = 0; q < P->active.size(); q++) sa[q] = P->active[q];
+  CU(cudaMemcpyAsync(P->dsys, sa.data(), sa.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));  // host buffers are reused
+  P->maps_dirty = false;
+  return 0;
+}
+
+// kernels of one pooled step (capacity grids; padding blocks return at once)
+int pool_step_a(gemsgpu_pool* P, cudaGraphConditionalHandle h, bool cond) {
+  gemsgpu_ctx* ctx = P->ctx;
+  const BlockMap& m = P->maps[0];
+  if (cond) k_step_a<true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, h);
+  else k_step_a<false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, h);
+  ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int pool_rebuild(gemsgpu_pool* P, int in_graph) {
+  gemsgpu_ctx* ctx = P->ctx;
+  cudaStream_t st = ctx->stream;
+  const Arena& A = ctx->A;
+  const BlockMap &ma = P->maps[0], &mc = P->maps[1], &mw = P->maps[2], &mc8 = P->maps[3];
+  const int ns = P->max_systems;
+  k_bin<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  k_scan1<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
+  k_scan2<<<ns, BLOCK, 0, st>>>(A, P->dsys, ns); ++ctx->launches;
+  k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  k_sort_cells<<<mc8.nblk, BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
+  k_list_cells<<<mw.nblk, BLOCK, LIST_ATOMS * A.lcap * sizeof(int), st>>>(A, mw); ++ctx->launches;
+  k_list_n2<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  k_count_rebuild<<<(ns + 255) / 256, 256, 0, st>>>(A, P->dsys, ns, in_graph); ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int pool_forces(gemsgpu_pool* P) {
+  gemsgpu_ctx* ctx = P->ctx;
+  const BlockMap& mk = P->maps[4];
+  const BlockMap& ma = P->maps[0];
+  const bool regs = P->variant == 0;
+  if (P->ff == FF_SMATB) {
+    smatb_pass(ctx, 0, P->prec, regs, P->lanes, mk);
+    smatb_pass(ctx, 1, P->prec, regs, P->lanes, mk);
+  } else if (P->ff == FF_LJ) {
+    lj_pass(ctx, P->prec, P->lanes, mk);
+  } else if (P->ff == FF_TERSOFF) {
+    k_zero_force<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
+    if (P->prec == PREC_MIXED) k_tersoff<float><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+    else k_tersoff<double><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+    ++ctx->launches;
+  }
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int pool_step_b(gemsgpu_pool* P) {
+  gemsgpu_ctx* ctx = P->ctx;
+  const BlockMap& m = P->maps[0];
+  k_step_b<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+struct PoolArg {
+  gemsgpu_pool* P;
+  cudaGraphConditionalHandle h;
+  int n;
+};
+int pcap_a(gemsgpu_ctx*, const std::vector<int>&, void* a) {
+  PoolArg* q = (PoolArg*)a;
+  return pool_step_a(q->P, q->h, true);
+}
+int pcap_rebuild(gemsgpu_ctx* ctx, const std::vector<int>&, void* a) {
+  const int64_t before = ctx->launches;
+  int rc = pool_rebuild(((PoolArg*)a)->P, 1);
+  ((PoolArg*)a)->P->body_nodes = ctx->launches - before;
+  return rc;
+}
+int pcap_fb(gemsgpu_ctx*, const std::vector<int>&, void* a) {
+  CHK(pool_forces(((PoolArg*)a)->P));
+  return pool_step_b(((PoolArg*)a)->P);
+}
+int pcap_plain(gemsgpu_ctx*, const std::vector<int>&, void* a) {
+  PoolArg* q = (PoolArg*)a;
+  for (int k = 0; k < q->n; k++) {
+    CHK(pool_step_a(q->P, 0, false));
+    CHK(pool_rebuild(q->P, 0));
+    CHK(pool_forces(q->P));
+    CHK(pool_step_b(q->P));
+  }
+  return 0;
+}
+
+int pool_capture(gemsgpu_pool* P) {
+  gemsgpu_ctx* ctx = P->ctx;
+  if (P->exec) {
+    cudaGraphExecDestroy(P->exec);
+    P->exec = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CU(cudaGraphCreate(&g, 0));
+  const int64_t before = ctx->launches;
+  std::vector<cudaGraphNode_t> deps;
+  std::vector<int> none_ss;
+  int rc = 0;
+  bool cond = ctx->use_cond;
+  P->body_nodes = 0;
+  for (int k = 0; k < P->chunk && rc == 0 && cond; k++) {
+    PoolArg pa{P, 0, 0};
+    if (cudaGraphConditionalHandleCreate(&pa.h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+      cond = false;
+      break;
+    }
+    rc = capture_into(ctx, g, deps, pcap_a, none_ss, &pa);
+    if (rc) break;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = pa.h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    if (cudaGraphAddNode(&cn, g, deps.data(), deps.size(), &cp) != cudaSuccess) {
+      cond = false;
+      break;
+    }
+    std::vector<cudaGraphNode_t> none;
+    rc = capture_into(ctx, cp.conditional.phGraph_out[0], none, pcap_rebuild, none_ss, &pa);
+    if (rc) break;
+    deps.assign(1, cn);
+    rc = capture_into(ctx, g, deps, pcap_fb, none_ss, &pa);
+  }
+  cudaGetLastError();
+  if (rc == 0 && !cond) {
+    cudaGraphDestroy(g);
+    CU(cudaGraphCreate(&g, 0));
+    deps.clear();
+    PoolArg pa{P, 0, P->chunk};
+    P->body_nodes = 0;
+    rc = capture_into(ctx, g, deps, pcap_plain, none_ss, &pa);
+  }
+  int64_t nodes = ctx->launches - before;
+  ctx->launches = before;
+  if (rc) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  P->nodes = nodes - P->body_nodes * P->chunk;
+  cudaError_t e = cudaGraphInstantiate(&P->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(ctx, GEMSGPU_ERR_CUDA, "pool graph instantiate: %s", cudaGetErrorString(e));
+  P->captured = ctx->A;
+  return 0;
+}
+
+bool same_arena(const Arena& a, const Arena& b) { return memcmp(&a, &b, sizeof(Arena)) == 0; }
+
+// one pooled chunk: (re)capture if the arena moved, launch, check states;
+// undo and redo a chunk whose lists overflowed.
+int pool_chunk(gemsgpu_pool* P) {
+  gemsgpu_ctx* ctx = P->ctx;
+  if (P->active.empty()) return 0;
+  if (P->maps_dirty) CHK(pool_upload_maps(P));
+  for (int attempt = 0; attempt < 5; attempt++) {
+    if (!P->exec || !same_arena(P->captured, ctx->A)) CHK(pool_capture(P));
+    CHK(snapshot(ctx, false));
+    k_clear_status<<<(P->max_systems + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, P->dsys, P->max_systems);
+    ++ctx->launches;
+    CU(cudaGraphLaunch(P->exec, ctx->stream));
+    ctx->launches += P->nodes;
+    if (P->body_nodes) {
+      unsigned long long runs = 0;
+      CU(cudaMemcpyAsync(&runs, ctx->A.body_runs, sizeof(runs), cudaMemcpyDeviceToHost, ctx->stream));
+      CU(cudaStreamSynchronize(ctx->stream));
+      ctx->launches += (int64_t)(runs - ctx->body_seen) * P->body_nodes;
+      ctx->body_seen = runs;
+    }
+    CHK(read_states(ctx));
+    int grow = 0;
+    for (int s : P->active) {
+      int st = ctx->h_st[s].status;
+      if (st & (ST_NAN | ST_LOST)) return status_error(ctx, s, st);
+      if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
+    }
+    if (!grow) return 0;
+    CHK(snapshot(ctx, true));
+    CHK(grow_list(ctx, grow + grow / 4 + 8));
+    if (ctx->A.lcap * LIST_ATOMS * sizeof(int) > 48 * 1024)
+      CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(ctx->A.lcap * LIST_ATOMS * sizeof(int))));
+    k_force_rebuild<<<(P->max_systems + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, P->dsys, P->max_systems);
+    ++ctx->launches;
+    k_clear_status<<<(P->max_systems + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, P->dsys, P->max_systems);
+    ++ctx->launches;
+    CHK(pool_rebuild(P, 0));
+    CHK(pool_forces(P));
+  }
+  return fail(ctx, GEMSGPU_ERR_OVERFLOW, "neighbour list keeps overflowing");
+}
+
+// systems entering a pool get their first list and forces (interact)
+int pool_prepare(gemsgpu_pool* P, const std::vector<int>& fresh) {
+  gemsgpu_ctx* ctx = P->ctx;
+  if (fresh.empty()) return 0;
+  for (int s : fresh) {
+    SysHost& h = ctx->sys[s];
+    if (h.d.ff != P->ff || h.d.prec != P->prec)
+      return fail(ctx, GEMSGPU_ERR_STATE, "system %d does not match the pool's force field / precision", s);
+    h.lanes = P->lanes;
+    h.variant = P->variant;
+  }
+  return interact_group(ctx, fresh, true);
 }
 
 }  // namespace
@@ -1491,6 +1834,7 @@ int gemsgpu_set_ermak(gemsgpu_ctx* ctx, int sys, double dt, double gama, double 
   d.crv1 = (1.0 - d.cc0) * (1.0 - d.cc0) / (gama * d.sdr * d.sdv);
   d.crv2 = std::sqrt(1.0 - (d.crv1 * d.crv1));
   d.skt = std::sqrt(kB_ui * temp);
+  h.temp = temp;
   d.seed = seed;
   d.use_ext_normals = 0;
   CHK(push_sys(ctx, sys));
@@ -1624,31 +1968,63 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys, double fmax, 
     }
   }
   int total = 0;
-  for (;;) {
-    CHK(read_states(ctx));
-    bool all = true;
-    for (int s : ss) all &= ctx->h_st[s].fire_done != 0;
-    if (all || total >= maxit) break;
-    int k = std::min(CHUNK, maxit - total);
-    CHK(clear_status(ctx, ss));
-    CHK(launch_graph(ctx, ss, k));
-    total += k;
-    CHK(read_states(ctx));
-    for (int s : ss) {
-      int st = ctx->h_st[s].status;
-      if (st & (ST_NAN | ST_LOST)) return status_error(ctx, s, st);
-      if (st & ST_OVERFLOW) {
-        CHK(grow_list(ctx, ctx->h_st[s].maxnn + 16));
-        const int* sa;
-        CHK(sys_array(ctx, ss, &sa));
-        k_force_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size()); ++ctx->launches;
-        CHK(clear_status(ctx, ss));
-        CHK(launch_rebuild(ctx, ss));
-        CHK(launch_forces(ctx, ss));
-        break;
+  bool uniform = true;
+  int64_t atoms = 0, cells = 0;
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    uniform &= h.d.ff == ctx->sys[ss[0]].d.ff && h.d.prec == ctx->sys[ss[0]].d.prec &&
+               h.lanes == ctx->sys[ss[0]].lanes && h.variant == ctx->sys[ss[0]].variant;
+    atoms += h.n;
+    cells += h.d.use_cells ? h.d.ncell : 0;
+  }
+  if (uniform) {
+    // converged systems leave the pool's active set between chunks
+    const SysHost& h0 = ctx->sys[ss[0]];
+    gemsgpu_pool* P = nullptr;
+    CHK(gemsgpu_pool_create(ctx, (int)ss.size(), atoms, cells, h0.d.ff, h0.d.prec, h0.lanes, h0.variant,
+                            CHUNK, &P));
+    int rc = 0;
+    for (;;) {
+      if ((rc = read_states(ctx))) break;
+      std::vector<int> act;
+      for (int s : ss)
+        if (!ctx->h_st[s].fire_done) act.push_back(s);
+      if (act.empty() || total >= maxit) break;
+      if ((rc = gemsgpu_pool_set(P, act.data(), (int)act.size()))) break;
+      if ((rc = gemsgpu_pool_run(P, 1))) break;
+      total += CHUNK;
+    }
+    gemsgpu_pool_destroy(P);
+    CHK(rc);
+  } else {
+    for (;;) {
+      CHK(read_states(ctx));
+      bool all = true;
+      for (int s : ss) all &= ctx->h_st[s].fire_done != 0;
+      if (all || total >= maxit) break;
+      int k = std::min(CHUNK, maxit - total);
+      CHK(clear_status(ctx, ss));
+      CHK(launch_graph(ctx, ss, k));
+      total += k;
+      CHK(read_states(ctx));
+      for (int s : ss) {
+        int st = ctx->h_st[s].status;
+        if (st & (ST_NAN | ST_LOST)) return status_error(ctx, s, st);
+        if (st & ST_OVERFLOW) {
+          CHK(grow_list(ctx, ctx->h_st[s].maxnn + 16));
+          const int* sa;
+          CHK(sys_array(ctx, ss, &sa));
+          k_force_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size());
+          ++ctx->launches;
+          CHK(clear_status(ctx, ss));
+          CHK(launch_rebuild(ctx, ss));
+          CHK(launch_forces(ctx, ss));
+          break;
+        }
       }
     }
   }
+  CHK(read_states(ctx));
   if (iters)
     for (size_t k = 0; k < ss.size(); k++) iters[k] = ctx->h_st[ss[k]].fire_iter;
   return 0;
@@ -1725,6 +2101,338 @@ int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant) {
   if (h.d.ff != FF_TERSOFF) h.lanes = lanes;
   h.variant = variant ? 1 : 0;
   invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_replica_exchange(gemsgpu_ctx* ctx, int nrep, int* sys_of_temp, const double* temps,
+                             int round, uint64_t seed, const double* uniforms, int* accepted) {
+  if (!ctx || nrep <= 0 || !sys_of_temp || !temps) return fail(ctx, GEMSGPU_ERR_ARG, "replica_exchange: arguments");
+  std::vector<int> ss(sys_of_temp, sys_of_temp + nrep);
+  for (int k = 0; k < nrep; k++) {
+    CHK(check_sys(ctx, ss[k]));
+    if (ctx->sys[ss[k]].d.integ != IT_ERMAK)
+      return fail(ctx, GEMSGPU_ERR_STATE, "replica_exchange: system %d is not an Ermak system", ss[k]);
+    if (!(temps[k] > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "replica_exchange: temperatures > 0");
+  }
+  {
+    std::vector<int> t = ss;
+    std::sort(t.begin(), t.end());
+    if (std::unique(t.begin(), t.end()) != t.end()) return fail(ctx, GEMSGPU_ERR_ARG, "duplicate replica");
+  }
+  cudaSetDevice(ctx->device);
+  // inq_pot_energy of every replica at its current configuration
+  std::vector<double> r;
+  CHK(reduce_sys(ctx, ss, r));
+  // parallel_tempering2 (src/ReplicaExchange.f90:55-138): in round ns the
+  // temperature index k pairs with k+par (even k) or k-par (odd k), par = +1
+  // for even ns and -1 for odd ns; the lower index accepts with
+  // min(1, exp(-(beta_k - beta_k')(U_k' - U_k))).
+  const int par = (round % 2 == 0) ? 1 : -1;
+  int nacc = 0;
+  std::vector<int> perm = ss;
+  for (int k = 0; k < nrep; k++) {
+    int p = (k % 2 == 0) ? k + par : k - par;
+    if (p < 0 || p >= nrep || p < k) continue;  // k is the lower index of the pair
+    double bk = 1.0 / (kB_ui * temps[k]), bp = 1.0 / (kB_ui * temps[p]);
+    double du = (r[4 * p] - r[4 * k]) * (bk - bp);
+    bool swap = true;
+    if (du > 0.0) {
+      double u;
+      if (uniforms) {
+        u = uniforms[k];
+      } else {
+        uint4 q = philox10(make_uint4((uint32_t)k, (uint32_t)round, (uint32_t)((uint64_t)round >> 32), 7u),
+                           make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+        u = ((double)(q.x >> 5) * 67108864.0 + (double)(q.y >> 6)) / 9007199254740992.0;
+      }
+      swap = u < std::exp(-du);
+    }
+    if (!swap) continue;
+    nacc++;
+    std::swap(perm[k], perm[p]);
+  }
+  // apply: each system takes its new temperature; velocities scale by
+  // sqrt(T_new / T_old) (the reference rescales after exchanging configurations)
+  std::vector<double> fac(ctx->scap, 1.0);
+  bool any = false;
+  for (int k = 0; k < nrep; k++) {
+    int sid = perm[k];
+    SysHost& h = ctx->sys[sid];
+    double told = h.temp;
+    double tnew = temps[k];
+    if (told != tnew) {
+      fac[sid] = std::sqrt(tnew / told);
+      h.d.skt = std::sqrt(kB_ui * tnew);
+      h.temp = tnew;
+      CHK(push_sys(ctx, sid));
+      any = true;
+    }
+    sys_of_temp[k] = sid;
+  }
+  if (any) {
+    double* dfac = nullptr;
+    CHK(dalloc(ctx, &dfac, ctx->scap));
+    CU(cudaMemcpyAsync(dfac, fac.data(), ctx->scap * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    BlockMap m;
+    CHK(get_map(ctx, ss, BLOCK, 0, &m));
+    k_scale_vel<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, dfac); ++ctx->launches;
+    CU(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dfac);
+  }
+  if (accepted) *accepted = nacc;
+  return 0;
+}
+
+int gemsgpu_pool_create(gemsgpu_ctx* ctx, int max_systems, int64_t max_atoms, int64_t max_cells, int ff,
+                        int prec, int lanes, int variant, int chunk_steps, gemsgpu_pool** out) {
+  if (!ctx || !out || max_systems <= 0 || max_atoms <= 0 || max_cells < 0 || chunk_steps <= 0)
+    return fail(ctx, GEMSGPU_ERR_ARG, "pool_create: arguments");
+  if (ff < FF_LJ || ff > FF_TERSOFF || (prec != PREC_FP64 && prec != PREC_MIXED))
+    return fail(ctx, GEMSGPU_ERR_ARG, "pool_create: force field / precision");
+  if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(ctx, GEMSGPU_ERR_ARG, "pool_create: lanes");
+  cudaSetDevice(ctx->device);
+  auto* P = new gemsgpu_pool();
+  P->ctx = ctx;
+  P->max_systems = max_systems;
+  P->max_atoms = max_atoms;
+  P->max_cells = max_cells;
+  P->ff = ff;
+  P->prec = prec;
+  P->lanes = ff == FF_TERSOFF ? 1 : lanes;
+  P->variant = variant ? 1 : 0;
+  P->chunk = chunk_steps;
+  int rc = grow_systems(ctx, std::max((int)ctx->sys.size(), 0) + max_systems + 1);
+  P->scap = ctx->scap;
+  if (!rc) rc = pool_alloc(P);
+  if (rc) {
+    gemsgpu_pool_destroy(P);
+    return rc;
+  }
+  *out = P;
+  return 0;
+}
+
+int gemsgpu_pool_destroy(gemsgpu_pool* P) {
+  if (!P) return GEMSGPU_ERR_ARG;
+  if (P->exec) cudaGraphExecDestroy(P->exec);
+  for (int k = 0; k < 5; k++)
+    if (P->dmap[k]) cudaFree(P->dmap[k]);
+  if (P->dsys) cudaFree(P->dsys);
+  delete P;
+  return 0;
+}
+
+int gemsgpu_pool_set(gemsgpu_pool* P, const int* sys, int nsys) {
+  if (!P) return GEMSGPU_ERR_ARG;
+  gemsgpu_ctx* ctx = P->ctx;
+  if (nsys < 0 || nsys > P->max_systems || (nsys > 0 && !sys))
+    return fail(ctx, GEMSGPU_ERR_ARG, "pool_set: 0 <= nsys <= %d", P->max_systems);
+  std::vector<int> ss(sys, sys + nsys);
+  int64_t atoms = 0;
+  for (int s : ss) {
+    CHK(check_sys(ctx, s));
+    if (s >= P->scap) return fail(ctx, GEMSGPU_ERR_FULL, "system id beyond the pool's capacity");
+    atoms += ctx->sys[s].n;
+  }
+  if (atoms > P->max_atoms) return fail(ctx, GEMSGPU_ERR_FULL, "pool_set: %lld atoms > capacity", (long long)atoms);
+  std::vector<int> fresh;
+  for (int s : ss)
+    if (std::find(P->active.begin(), P->active.end(), s) == P->active.end() &&
+        (ctx->sys[s].first || ctx->sys[s].pos_dirty || !ctx->sys[s].has_forces))
+      fresh.push_back(s);
+  CHK(pool_prepare(P, fresh));
+  P->active = ss;
+  P->maps_dirty = true;
+  return 0;
+}
+
+int gemsgpu_pool_run(gemsgpu_pool* P, int nchunks) {
+  if (!P || nchunks < 0) return GEMSGPU_ERR_ARG;
+  cudaSetDevice(P->ctx->device);
+  for (int c = 0; c < nchunks; c++) CHK(pool_chunk(P));
+  return 0;
+}
+
+int gemsgpu_server_create(gemsgpu_ctx* ctx, int max_jobs, int64_t max_atoms, int prec, int lanes,
+                          int variant, int chunk_steps, gemsgpu_server** out) {
+  if (!ctx || !out || max_jobs <= 0 || max_atoms <= 0 || chunk_steps <= 0)
+    return fail(ctx, GEMSGPU_ERR_ARG, "server_create: arguments");
+  cudaSetDevice(ctx->device);
+  auto* S = new gemsgpu_server();
+  S->ctx = ctx;
+  S->max_jobs = max_jobs;
+  S->max_atoms = max_atoms;
+  S->chunk = chunk_steps;
+  // room for every admitted job without moving the arena (no re-capture)
+  int rc = grow_atoms(ctx, ctx->atoms_used + max_atoms + 32 * (int64_t)max_jobs);
+  if (!rc) rc = gemsgpu_pool_create(ctx, max_jobs, max_atoms, 1, FF_SMATB, prec, lanes, variant, chunk_steps,
+                                    &S->pool);
+  if (rc) {
+    delete S;
+    return rc;
+  }
+  *out = S;
+  return 0;
+}
+
+int gemsgpu_server_destroy(gemsgpu_server* S) {
+  if (!S) return GEMSGPU_ERR_ARG;
+  for (int64_t id : S->running) {
+    ServerJob& j = S->jobs[id];
+    if (j.sys >= 0) gemsgpu_system_destroy(S->ctx, j.sys);
+  }
+  if (S->pool) gemsgpu_pool_destroy(S->pool);
+  delete S;
+  return 0;
+}
+
+int gemsgpu_server_submit(gemsgpu_server* S, const gemsgpu_job* job, int64_t* id) {
+  if (!S || !job || !job->pos || job->natoms <= 0) return GEMSGPU_ERR_ARG;
+  gemsgpu_ctx* ctx = S->ctx;
+  if (job->natoms > S->max_atoms) return fail(ctx, GEMSGPU_ERR_FULL, "job larger than the server's atom budget");
+  if ((job->kind != GEMSGPU_JOB_FIRE && job->kind != GEMSGPU_JOB_MD) || job->steps <= 0 || !(job->dt > 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "submit: kind, steps > 0, dt > 0");
+  ServerJob j;
+  j.id = S->next_id++;
+  j.spec = *job;
+  j.pos.assign(job->pos, job->pos + 3 * (size_t)job->natoms);
+  j.spec.pos = nullptr;
+  j.state = GEMSGPU_JOB_QUEUED;
+  S->jobs[j.id] = std::move(j);
+  S->queue.push_back(S->jobs.rbegin()->first);
+  if (id) *id = S->queue.back();
+  return 0;
+}
+
+static int server_admit(gemsgpu_server* S, int64_t id) {
+  gemsgpu_ctx* ctx = S->ctx;
+  ServerJob& j = S->jobs[id];
+  const gemsgpu_job& q = j.spec;
+  int sys = -1;
+  CHK(gemsgpu_system_create(ctx, q.natoms, 1, &sys));
+  j.sys = sys;
+  std::vector<double> m(q.natoms, q.mass);
+  CHK(gemsgpu_upload(ctx, sys, j.pos.data(), nullptr, m.data(), nullptr));
+  CHK(gemsgpu_set_smatb(ctx, sys, 0, 0, q.smatb[0], q.smatb[1], q.smatb[2], q.smatb[3], q.smatb[4], q.smatb[5],
+                        q.smatb[6]));
+  CHK(gemsgpu_set_precision(ctx, sys, S->pool->prec));
+  if (q.kind == GEMSGPU_JOB_FIRE) {
+    CHK(gemsgpu_set_fire(ctx, sys, q.dt, 10.0 * q.dt));
+    SysHost& h = ctx->sys[sys];
+    h.d.fire_fmax = q.fmax;
+    h.d.fire_maxit = q.steps;
+    CHK(push_sys(ctx, sys));
+  } else {
+    CHK(gemsgpu_set_ermak(ctx, sys, q.dt, q.gamma, q.temp, q.seed));
+  }
+  j.state = GEMSGPU_JOB_RUNNING;
+  S->atoms_in += q.natoms;
+  S->running.push_back(id);
+  return 0;
+}
+
+static int server_retire(gemsgpu_server* S, int64_t id, const SysState& st) {
+  gemsgpu_ctx* ctx = S->ctx;
+  ServerJob& j = S->jobs[id];
+  double ep = 0, ek = 0, t = 0, fm = 0;
+  CHK(gemsgpu_energy(ctx, j.sys, &ep, &ek, &t));
+  CHK(gemsgpu_fmax(ctx, j.sys, &fm));
+  j.epot_ev = ep;
+  j.ekin_ev = ek;
+  j.fmax_ev = fm;
+  j.iters = j.spec.kind == GEMSGPU_JOB_FIRE ? st.fire_iter : j.done_steps;
+  CHK(gemsgpu_download(ctx, j.sys, j.pos.data(), nullptr, nullptr, nullptr));
+  CHK(gemsgpu_system_destroy(ctx, j.sys));
+  S->atoms_in -= j.spec.natoms;
+  j.sys = -1;
+  j.state = GEMSGPU_JOB_DONE;
+  return 0;
+}
+
+int gemsgpu_server_step(gemsgpu_server* S, int* n_running, int* n_queued, int* n_finished) {
+  if (!S) return GEMSGPU_ERR_ARG;
+  gemsgpu_ctx* ctx = S->ctx;
+  cudaSetDevice(ctx->device);
+  // admission by memory footprint: first fit over the queue (FIFO order)
+  bool changed = false;
+  for (auto it = S->queue.begin(); it != S->queue.end();) {
+    if ((int)S->running.size() >= S->max_jobs) break;
+    ServerJob& j = S->jobs[*it];
+    if (S->atoms_in + j.spec.natoms > S->max_atoms) {
+      ++it;
+      continue;
+    }
+    int rc = server_admit(S, *it);
+    if (rc) {
+      j.state = GEMSGPU_JOB_FAILED;
+      j.error = rc;
+      if (j.sys >= 0) {
+        gemsgpu_system_destroy(ctx, j.sys);
+        j.sys = -1;
+      }
+    }
+    changed = true;
+    it = S->queue.erase(it);
+  }
+  int finished = 0;
+  if (!S->running.empty()) {
+    std::vector<int> act;
+    for (int64_t id : S->running) act.push_back(S->jobs[id].sys);
+    if (changed || act.size() != S->pool->active.size() || !std::equal(act.begin(), act.end(),
+                                                                        S->pool->active.begin()))
+      CHK(gemsgpu_pool_set(S->pool, act.data(), (int)act.size()));
+    CHK(gemsgpu_pool_run(S->pool, 1));
+    CHK(read_states(ctx));
+    std::vector<int64_t> keep;
+    for (int64_t id : S->running) {
+      ServerJob& j = S->jobs[id];
+      j.done_steps += S->chunk;
+      const SysState st = ctx->h_st[j.sys];
+      bool done = j.spec.kind == GEMSGPU_JOB_FIRE ? st.fire_done != 0 : j.done_steps >= j.spec.steps;
+      if (done) {
+        CHK(server_retire(S, id, st));
+        finished++;
+      } else {
+        keep.push_back(id);
+      }
+    }
+    if (keep.size() != S->running.size()) {
+      S->running = keep;
+      std::vector<int> act2;
+      for (int64_t id : S->running) act2.push_back(S->jobs[id].sys);
+      CHK(gemsgpu_pool_set(S->pool, act2.data(), (int)act2.size()));
+    }
+  }
+  if (n_running) *n_running = (int)S->running.size();
+  if (n_queued) *n_queued = (int)S->queue.size();
+  if (n_finished) *n_finished = finished;
+  return 0;
+}
+
+int gemsgpu_server_poll(gemsgpu_server* S, int64_t id, int* state, double* epot_ev, double* fmax_ev,
+                        int* iters, double* pos_out) {
+  if (!S) return GEMSGPU_ERR_ARG;
+  auto it = S->jobs.find(id);
+  if (it == S->jobs.end()) return fail(S->ctx, GEMSGPU_ERR_ARG, "unknown job %lld", (long long)id);
+  ServerJob& j = it->second;
+  if (state) *state = j.state;
+  if (j.state == GEMSGPU_JOB_DONE) {
+    if (epot_ev) *epot_ev = j.epot_ev;
+    if (fmax_ev) *fmax_ev = j.fmax_ev;
+    if (iters) *iters = j.iters;
+    if (pos_out) memcpy(pos_out, j.pos.data(), j.pos.size() * sizeof(double));
+  }
+  if (j.state == GEMSGPU_JOB_FAILED) return j.error;
+  return 0;
+}
+
+int gemsgpu_server_forget(gemsgpu_server* S, int64_t id) {
+  if (!S) return GEMSGPU_ERR_ARG;
+  auto it = S->jobs.find(id);
+  if (it == S->jobs.end() || (it->second.state != GEMSGPU_JOB_DONE && it->second.state != GEMSGPU_JOB_FAILED))
+    return GEMSGPU_ERR_ARG;
+  S->jobs.erase(it);
   return 0;
 }
 

@@ -29,13 +29,21 @@ __device__ __forceinline__ int blk_sys(const BlockMap& M) { return M.sys[blockId
 // ------------------------------------------------------------------ Philox
 // Counter-based generator Philox4x32-10 (Salmon, Moraes, Dror, Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC'11).
-__device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
+__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
+#endif
+}
+
+__host__ __device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
   const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
   const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
 #pragma unroll
   for (int r = 0; r < 10; r++) {
-    uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
-    uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    uint32_t hi0 = mulhi32(M0, c.x), lo0 = M0 * c.x;
+    uint32_t hi1 = mulhi32(M1, c.z), lo1 = M1 * c.z;
     c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
     k.x += W0;
     k.y += W1;
@@ -238,6 +246,7 @@ __device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, i
 
 __global__ void k_skin(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   int i = M.first[blockIdx.x] + threadIdx.x;
   double2 t = make_double2(1.e-16, 1.e-16);
   if (i < M.end[blockIdx.x]) t.x = disp2(A.sys[s], A.pos[i], A.pos_old[i]);
@@ -248,15 +257,25 @@ __global__ void k_skin(Arena A, BlockMap M) {
 // mark systems for rebuild (first interact: update(), Interaction.f90:174)
 __global__ void k_force_rebuild(Arena A, const int* sys, int nsys) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < nsys) {
+  if (k < nsys && sys[k] >= 0) {
     A.st[sys[k]].rebuild = 1;
     atomicOr(A.any_rebuild, 1);
+  }
+}
+
+// clear the per-chunk status words of a set of systems
+__global__ void k_clear_status(Arena A, const int* sys, int nsys) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nsys && sys[k] >= 0) {
+    A.st[sys[k]].status = 0;
+    A.st[sys[k]].maxnn = 0;
   }
 }
 
 // refresh fixed-point positions (after an upload or set_positions)
 __global__ void k_refresh_fx(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   int i = M.first[blockIdx.x] + threadIdx.x;
   if (i >= M.end[blockIdx.x]) return;
   const SysDev& S = A.sys[s];
@@ -270,6 +289,7 @@ __global__ void k_refresh_fx(Arena A, BlockMap M) {
 // k_bin (histogram) -> k_scan1/k_scan2 (prefix) -> k_scatter -> k_sort_cells
 __global__ void k_bin(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   if (!A.st[s].rebuild || !S.use_cells) return;
   int i = M.first[blockIdx.x] + threadIdx.x;
@@ -293,6 +313,7 @@ __global__ void k_bin(Arena A, BlockMap M) {
 // per 256-cell chunk: local exclusive prefix, chunk total; resets counts
 __global__ void k_scan1(Arena A, BlockMap C) {
   int s = blk_sys(C);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
   int c = C.first[blockIdx.x] + threadIdx.x;
   bool act = c < C.end[blockIdx.x];
@@ -317,6 +338,7 @@ __global__ void k_scan1(Arena A, BlockMap C) {
 // one block per system: exclusive prefix of its chunk totals
 __global__ void k_scan2(Arena A, const int* sys, int nsys) {
   int s = sys[blockIdx.x];
+  if (s < 0) return;
   const SysDev& S = A.sys[s];
   if (!A.st[s].rebuild || !S.use_cells) return;
   int k0 = S.cell_off >> 8;
@@ -347,6 +369,7 @@ __global__ void k_scan2(Arena A, const int* sys, int nsys) {
 
 __global__ void k_scatter(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
   int i = M.first[blockIdx.x] + threadIdx.x;
   if (i >= M.end[blockIdx.x]) return;
@@ -362,6 +385,7 @@ __global__ void k_scatter(Arena A, BlockMap M) {
 // fall back to an insertion sort by one lane.
 __global__ void k_sort_cells(Arena A, BlockMap C) {
   int s = blk_sys(C);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
   const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int first = C.first[blockIdx.x], end = C.end[blockIdx.x];
@@ -420,6 +444,7 @@ constexpr int LIST_ATOMS = BLOCK / 32;
 
 __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   if (!A.st[s].rebuild || !S.use_cells) return;
   extern __shared__ int stage[];  // [LIST_ATOMS][lcap]
@@ -491,6 +516,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap M) {
 // positions are staged through shared memory one BLOCK-wide tile at a time.
 __global__ void k_list_n2(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   if (!A.st[s].rebuild || S.use_cells) return;
   __shared__ double4 tile[BLOCK];
@@ -522,7 +548,7 @@ __global__ void k_list_n2(Arena A, BlockMap M) {
 // node, whose executions are counted for the launch statistics
 __global__ void k_count_rebuild(Arena A, const int* sys, int nsys, int in_graph) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < nsys && A.st[sys[k]].rebuild) A.st[sys[k]].nupd++;
+  if (k < nsys && sys[k] >= 0 && A.st[sys[k]].rebuild) A.st[sys[k]].nupd++;
   if (in_graph && k == 0) atomicAdd(A.body_runs, 1ull);
 }
 
@@ -599,6 +625,7 @@ __device__ __forceinline__ const SmFP64* sm_table(const Arena& A, const SysDev& 
 template <int K>
 __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   __shared__ SmFP64 tab_sh[MAXT * MAXT];
   const SmFP64* tab = sm_table(A, S, tab_sh);
@@ -646,6 +673,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
 template <int K>
 __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   __shared__ SmFP64 tab_sh[MAXT * MAXT];
   const SmFP64* tab = sm_table(A, S, tab_sh);
@@ -767,6 +795,7 @@ __device__ __forceinline__ const SmF32* smf_table(const Arena& A, const SysDev& 
 template <int K, bool ONE>
 __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   __shared__ SmF32 tab_sh[ONE ? 1 : MAXT * MAXT];
   const SmF32* tab = smf_table<ONE>(A, S, tab_sh);
@@ -826,6 +855,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
 template <int K, bool ONE>
 __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   __shared__ SmF32 tab_sh[ONE ? 1 : MAXT * MAXT];
   const SmF32* tab = smf_table<ONE>(A, S, tab_sh);
@@ -911,6 +941,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M
 template <int K>
 __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   int i = M.first[blockIdx.x] + threadIdx.x / K;
   int lane = threadIdx.x % K;
@@ -961,6 +992,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
 template <int K>
 __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   int i = M.first[blockIdx.x] + threadIdx.x / K;
   int lane = threadIdx.x % K;
@@ -1035,6 +1067,7 @@ __device__ __forceinline__ double ts_fc(double r, double r1, double r2, double& 
 template <typename R>
 __global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   int i = M.first[blockIdx.x] + threadIdx.x;
   if (i >= M.end[blockIdx.x]) return;
@@ -1164,6 +1197,18 @@ __global__ void k_pack3(const double4* __restrict__ src, double* __restrict__ ds
   }
 }
 
+// velocity rescale of whole systems (replica exchange): v *= f[k]
+__global__ void k_scale_vel(Arena A, BlockMap M, const double* fac_by_sys) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  if (i >= M.end[blockIdx.x]) return;
+  double f = fac_by_sys[s];
+  double4 v = A.vel[i];
+  v.x *= f; v.y *= f; v.z *= f;
+  A.vel[i] = v;
+}
+
 __global__ void k_zero_force(Arena A, BlockMap M) {
   int i = M.first[blockIdx.x] + threadIdx.x;
   if (i < M.end[blockIdx.x]) A.force[i] = make_double4(0, 0, 0, 0);
@@ -1176,9 +1221,12 @@ __global__ void k_zero_force(Arena A, BlockMap M) {
 // When the step is replayed from a CUDA graph, `cond` is the handle of the
 // conditional node that guards the rebuild kernels: any system that needs a
 // rebuild raises it, so steps without a rebuild skip those launches.
-__global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraphConditionalHandle cond,
-                                                   int use_cond) {
+// COND=false builds a copy without the device-side graph call, for plain
+// launches (profilers do not replay kernels that contain it).
+template <bool COND>
+__global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraphConditionalHandle cond) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   SysState& st = A.st[s];
   int i = M.first[blockIdx.x] + threadIdx.x;
@@ -1250,7 +1298,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
       st.rebuild = rb;
       if (rb) {
         atomicOr(A.any_rebuild, 1);
-        if (use_cond) cudaGraphSetConditional(cond, 1u);
+        if constexpr (COND) cudaGraphSetConditional(cond, 1u);
       }
       if (S.integ == IT_ERMAK && !S.use_ext_normals) st.step++;
       if (S.integ == IT_FIRE) st.fire_zero = 0;
@@ -1264,6 +1312,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
 // dt / alpha control (:116-131) in the system's last block.
 __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
   int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   SysState& st = A.st[s];
   int i = M.first[blockIdx.x] + threadIdx.x;

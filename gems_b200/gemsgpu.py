@@ -73,6 +73,17 @@ _SIGS = {
     "gemsgpu_get_stream": (_i, [_p, ctypes.POINTER(_p)]),
     "gemsgpu_autotune": (_i, [_p, _i, _i, _ip, _ip, _dp]),
     "gemsgpu_set_lanes": (_i, [_p, _i, _i, _i]),
+    "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
+    "gemsgpu_pool_create": (_i, [_p, _i, _l, _l, _i, _i, _i, _i, _i, ctypes.POINTER(_p)]),
+    "gemsgpu_pool_destroy": (_i, [_p]),
+    "gemsgpu_pool_set": (_i, [_p, _ip, _i]),
+    "gemsgpu_pool_run": (_i, [_p, _i]),
+    "gemsgpu_server_create": (_i, [_p, _i, _l, _i, _i, _i, _i, ctypes.POINTER(_p)]),
+    "gemsgpu_server_destroy": (_i, [_p]),
+    "gemsgpu_server_submit": (_i, [_p, _p, ctypes.POINTER(_l)]),
+    "gemsgpu_server_step": (_i, [_p, _ip, _ip, _ip]),
+    "gemsgpu_server_poll": (_i, [_p, _l, _ip, _dp, _dp, _ip, _dp]),
+    "gemsgpu_server_forget": (_i, [_p, _l]),
     "gemsgpu_smatb_forces_noalloc": (_i, [_p, _i, _i, _dp, _ip, _d, _d, _d, _d, _d, _d, _d, _p, _p, _p]),
     "gemsgpu_time_kernels": (_i, [_p, _i, _i, _dp]),
 }
@@ -164,6 +175,17 @@ class Context:
         v = _p()
         self.check(lib().gemsgpu_get_stream(self.h, ctypes.byref(v)))
         return v.value or 0
+
+    def replica_exchange(self, systems_of_temp, temps, rnd, seed=1, uniforms=None):
+        """One parallel-tempering round; returns (systems ordered by temperature, accepted)."""
+        ids = self._ids(systems_of_temp)
+        t = np.ascontiguousarray(temps, dtype=np.float64)
+        u = None if uniforms is None else np.ascontiguousarray(uniforms, dtype=np.float64)
+        acc = ctypes.c_int()
+        self.check(lib().gemsgpu_replica_exchange(self.h, len(ids), _ptr(ids, ctypes.c_int), _ptr(t), int(rnd),
+                                                  int(seed), _ptr(u), ctypes.byref(acc)))
+        by_id = {s.sid: s for s in systems_of_temp}
+        return [by_id[int(k)] for k in ids], acc.value
 
     def launches(self):
         v = ctypes.c_int64()
@@ -388,3 +410,89 @@ class System:
                 ep, ek, t = self.energy()
                 rows.append([ep, ek, ep + ek, t])
         return np.array(rows).reshape(-1, 4)
+
+
+FF_LJ, FF_SMATB, FF_TERSOFF = 1, 2, 3
+JOB_FIRE, JOB_MD = 0, 1
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
+class Pool:
+    """A fixed-capacity set of systems advanced through one captured graph."""
+
+    def __init__(self, ctx, max_systems, max_atoms, max_cells=1, ff=FF_SMATB, prec=PREC_MIXED, lanes=8,
+                 variant=1, chunk=50):
+        self.ctx = ctx
+        h = _p()
+        ctx.check(lib().gemsgpu_pool_create(ctx.h, int(max_systems), int(max_atoms), int(max_cells), int(ff),
+                                            int(prec), int(lanes), int(variant), int(chunk), ctypes.byref(h)))
+        self.h = h
+
+    def set(self, systems):
+        ids = np.ascontiguousarray([s.sid for s in systems], dtype=np.int32)
+        self.ctx.check(lib().gemsgpu_pool_set(self.h, _ptr(ids, ctypes.c_int), len(ids)))
+
+    def run(self, nchunks=1):
+        self.ctx.check(lib().gemsgpu_pool_run(self.h, int(nchunks)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gemsgpu_pool_destroy(self.h)
+            self.h = None
+
+
+class _Job(ctypes.Structure):
+    _fields_ = [("natoms", ctypes.c_int), ("pos", ctypes.POINTER(ctypes.c_double)), ("mass", ctypes.c_double),
+                ("smatb", ctypes.c_double * 7), ("kind", ctypes.c_int), ("steps", ctypes.c_int),
+                ("dt", ctypes.c_double), ("temp", ctypes.c_double), ("gamma", ctypes.c_double),
+                ("fmax", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
+class Server:
+    """The serving loop (gemsgpu_server_*): submit jobs, step, poll."""
+
+    def __init__(self, ctx, max_jobs, max_atoms, prec=PREC_MIXED, lanes=4, variant=1, chunk=50):
+        self.ctx = ctx
+        h = _p()
+        ctx.check(lib().gemsgpu_server_create(ctx.h, int(max_jobs), int(max_atoms), int(prec), int(lanes),
+                                              int(variant), int(chunk), ctypes.byref(h)))
+        self.h = h
+        self.sizes = {}
+
+    def submit(self, pos, mass, smatb, kind, steps, dt=0.002, temp=300.0, gamma=1.0, fmax=1e-3, seed=1):
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        j = _Job()
+        j.natoms = p.size // 3
+        j.pos = _ptr(p)
+        j.mass = float(mass)
+        for k in range(7):
+            j.smatb[k] = float(smatb[k])
+        j.kind, j.steps, j.dt, j.temp, j.gamma, j.fmax, j.seed = (int(kind), int(steps), float(dt), float(temp),
+                                                                  float(gamma), float(fmax), int(seed))
+        jid = ctypes.c_int64()
+        self.ctx.check(lib().gemsgpu_server_submit(self.h, ctypes.byref(j), ctypes.byref(jid)))
+        self.sizes[jid.value] = j.natoms
+        return jid.value
+
+    def step(self):
+        r, q, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self.ctx.check(lib().gemsgpu_server_step(self.h, ctypes.byref(r), ctypes.byref(q), ctypes.byref(f)))
+        return r.value, q.value, f.value
+
+    def poll(self, jid, want_pos=False):
+        st, ep, fm, it = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        pos = np.zeros(3 * self.sizes[jid]) if want_pos else None
+        self.ctx.check(lib().gemsgpu_server_poll(self.h, int(jid), ctypes.byref(st), ctypes.byref(ep),
+                                                 ctypes.byref(fm), ctypes.byref(it), _ptr(pos)))
+        out = {"state": st.value, "epot_ev": ep.value, "fmax_ev": fm.value, "iters": it.value}
+        if want_pos:
+            out["pos"] = pos.reshape(-1, 3)
+        return out
+
+    def forget(self, jid):
+        self.ctx.check(lib().gemsgpu_server_forget(self.h, int(jid)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gemsgpu_server_destroy(self.h)
+            self.h = None

@@ -59,6 +59,28 @@ extern "C" {
 #define GEMSGPU_PREC_MIXED 1 /* FP32 pair math, FP64 accumulation        */
 
 typedef struct gemsgpu_ctx gemsgpu_ctx;
+typedef struct gemsgpu_pool gemsgpu_pool;
+typedef struct gemsgpu_server gemsgpu_server;
+
+/* a job of the serving loop: one free SMA-TB cluster */
+#define GEMSGPU_JOB_FIRE 0   /* relax with FIRE to max|F| < fmax, <= steps iterations */
+#define GEMSGPU_JOB_MD 1     /* `steps` Ermak steps at temp (rounded up to whole chunks) */
+#define GEMSGPU_JOB_QUEUED 0
+#define GEMSGPU_JOB_RUNNING 1
+#define GEMSGPU_JOB_DONE 2
+#define GEMSGPU_JOB_FAILED 3
+typedef struct gemsgpu_job {
+  int natoms;
+  const double* pos;   /* 3 natoms, copied at submit */
+  double mass;         /* uma */
+  double smatb[7];     /* A, xi, p, q, r0, rci, rce as gemsgpu_set_smatb */
+  int kind;            /* GEMSGPU_JOB_FIRE or GEMSGPU_JOB_MD */
+  int steps;
+  double dt;           /* ps; FIRE: initial dt, dt_max = 10 dt */
+  double temp, gamma;  /* MD: Ermak bath */
+  double fmax;         /* FIRE: convergence, eV/A */
+  uint64_t seed;       /* MD: Philox stream */
+} gemsgpu_job;
 
 /* ------------------------------------------------------------ context */
 
@@ -193,6 +215,69 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys,
 /* Energies of nsys systems (arrays of nsys; any may be NULL). */
 int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys,
                          double* epot_ev, double* ekin_ev, double* temp);
+
+/* ------------------------------------------------------------ pools */
+
+/* A pool runs a changing set of systems (one force-field kind and precision)
+ * through one captured CUDA graph: its launch maps have fixed capacity and
+ * are rewritten when the set changes, so admitting or retiring a system
+ * costs no graph capture.  Capacity: max_systems systems, max_atoms atoms
+ * and max_cells cells in total; each run advances chunk_steps MD steps.
+ * lanes / variant fix the force kernels' launch shape (see gemsgpu_autotune).
+ * Replaces the per-rank dinamic loops of parallel_tempering2 and drives the
+ * serving loop; no single reference routine corresponds. */
+int gemsgpu_pool_create(gemsgpu_ctx* ctx, int max_systems, int64_t max_atoms,
+                        int64_t max_cells, int ff, int prec, int lanes,
+                        int variant, int chunk_steps, gemsgpu_pool** out);
+int gemsgpu_pool_destroy(gemsgpu_pool* pool);
+/* Set the active systems (replaces the previous set); new members get their
+ * first list and forces. */
+int gemsgpu_pool_set(gemsgpu_pool* pool, const int* sys, int nsys);
+/* Advance the active set by nchunks x chunk_steps steps (FIRE systems that
+ * have converged stay frozen). */
+int gemsgpu_pool_run(gemsgpu_pool* pool, int nchunks);
+
+/* ------------------------------------------------------------ serving */
+
+/* A serving loop over one pool.  Jobs wait in a queue and are admitted, in
+ * arrival order but skipping jobs that do not fit, while the running jobs
+ * hold at most max_atoms atoms and max_jobs slots (admission by memory
+ * footprint).  Every gemsgpu_server_step admits what fits, advances all
+ * running jobs by one chunk on the device (their work overlaps in the same
+ * kernels), and retires finished jobs: their energy, max|F|, iterations and
+ * final positions stay on the host until gemsgpu_server_forget.  Each job's
+ * result does not depend on which other jobs share its chunks.  GEMS itself
+ * has no serving mode; this sits on the same kernels as gemsgpu_md_steps. */
+int gemsgpu_server_create(gemsgpu_ctx* ctx, int max_jobs, int64_t max_atoms,
+                          int prec, int lanes, int variant, int chunk_steps,
+                          gemsgpu_server** out);
+int gemsgpu_server_destroy(gemsgpu_server* srv);
+int gemsgpu_server_submit(gemsgpu_server* srv, const gemsgpu_job* job,
+                          int64_t* job_id);
+int gemsgpu_server_step(gemsgpu_server* srv, int* n_running, int* n_queued,
+                        int* n_finished);
+/* state: GEMSGPU_JOB_*; results are filled once DONE (pos_out: 3n). */
+int gemsgpu_server_poll(gemsgpu_server* srv, int64_t job_id, int* state,
+                        double* epot_ev, double* fmax_ev, int* iters,
+                        double* pos_out);
+int gemsgpu_server_forget(gemsgpu_server* srv, int64_t job_id);
+
+/* ------------------------------------------------------------ replicas */
+
+/* One exchange round of parallel tempering (parallel_tempering2,
+ * src/ReplicaExchange.f90:27-150) among nrep Ermak systems.  temps[k] is the
+ * k-th temperature (any order the caller keeps fixed) and sys_of_temp[k] the
+ * system currently at temps[k].  In round `round` index k pairs with k+par
+ * (k even) or k-par (k odd), par = +1 for even rounds and -1 for odd ones;
+ * the lower index accepts with min(1, exp(-(b_k - b_k')(U_k' - U_k))).  An
+ * accepted swap exchanges the two systems' temperature labels and rescales
+ * their velocities by sqrt(T_new/T_old) -- the configurations stay on the
+ * device (the reference moves them between MPI ranks).  Uniforms come from
+ * Philox(seed, round, k) or, if `uniforms` is not NULL, from uniforms[k].
+ * sys_of_temp is updated in place; *accepted gets the number of swaps. */
+int gemsgpu_replica_exchange(gemsgpu_ctx* ctx, int nrep, int* sys_of_temp,
+                             const double* temps, int round, uint64_t seed,
+                             const double* uniforms, int* accepted);
 
 /* ------------------------------------------------------------ no allocation */
 

@@ -205,3 +205,53 @@ def ermak_parity_run(s, rng, nsteps, each):
             ep = s.epot_sum()
             rows.append([ep, ek, ep + ek, t])
     return np.array(rows)
+
+
+def repex_rows(O):
+    """examples/RepExchange/lj.gms on the oracle: 4 replicas (one per MPI rank
+    of the reference, each with its own LCG stream seeded 123456*rank), Ermak
+    at 30/35/40/45, `dinamica 1000`, `out state`, then `partemp2 100 100`
+    with the swap rule of parallel_tempering2 (src/ReplicaExchange.f90:55-138).
+    Like the reference, a swap exchanges positions and velocities (not acel)
+    and rescales the velocities by sqrt(T_self/T_partner)."""
+    import math
+    tau_ps = 0.01018
+    dt = 0.002 * tau_ps
+    gam = 1.0 / tau_ps
+    kB_ui = O.lib().orc_kB_ui()
+    reps = []
+    for pc in range(4):
+        rng = O.Rng(123456 * pc)
+        s = O.System(np.array([[1.0, 1, 1], [2.2, 1, 1]]) + 1.0, 3.0)
+        s.set_box((5.78,) * 3, (False,) * 3)
+        s.set_lj(1.0, 0.890898718140339, 2.0)
+        T = pc * 5.0 + 30
+        s.gdist(rng, T)
+        s.set_ermak(dt, gam, T, rng)
+        reps.append((s, rng, T))
+    for s, _, _ in reps:
+        s.dinamica(1000, 0)
+    rows = [[] for _ in range(4)]
+    for pc, (s, _, _) in enumerate(reps):
+        e = s.interact()
+        ek, _ = s.kin()
+        rows[pc].append(e * O.UI_EV)
+    for ns in range(1, 101):
+        for pc, (s, _, _) in enumerate(reps):
+            rows[pc] += list(s.dinamica(100, 10)[:, 0])
+        par = 1 if ns % 2 == 0 else -1
+        ep = [s.interact() for s, _, _ in reps]
+        for pc in range(4):
+            p = pc + par if pc % 2 == 0 else pc - par
+            if p < 0 or p >= 4 or p < pc:
+                continue
+            (a, ra, ta), (b, _, tb) = reps[pc], reps[p]
+            du = (ep[p] - ep[pc]) * (1.0 / (kB_ui * ta) - 1.0 / (kB_ui * tb))
+            if du > 0 and not ra.ranu() < math.exp(-du):
+                continue
+            pa, va, pb, vb = a.pos, a.vel, b.pos, b.vel
+            a.set_pos(pb)
+            a.set_vel(vb * math.sqrt(ta / tb))
+            b.set_pos(pa)
+            b.set_vel(va * math.sqrt(tb / ta))
+    return [np.array(r) for r in rows]

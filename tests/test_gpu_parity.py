@@ -344,3 +344,114 @@ def test_launch_shapes_agree(ctx, prec):
             assert relrms(g.force, fo) <= (RMS_FP64 if prec == 0 else RMS_MIXED)
     k, v, ms = g.autotune(3)
     assert k in (2, 4, 8, 16, 32) and ms > 0
+
+
+def _cluster_replicas(ctx, nrep, temps, seed0=7):
+    from gems_b200 import workloads as W
+    pos = W.cluster(147, np.random.default_rng(3))
+    reps = []
+    for k in range(nrep):
+        g = gems.System(pos + np.random.default_rng(seed0 + k).normal(0, 0.05, pos.shape), W.MASS["Au"],
+                        ctx=ctx)
+        g.set_smatb(*W.SMATB["Au"])
+        g.set_ermak(0.002, 1.0, temps[k], seed=seed0 + k)
+        reps.append(g)
+    return reps
+
+
+def test_replica_exchange_rule(ctx):
+    """The GPU exchange follows parallel_tempering2's pairing and Metropolis
+    rule (restated here from the replicas' energies and the same uniforms)
+    and swaps temperature labels with a velocity rescale."""
+    nrep = 8
+    temps = 200.0 * (900.0 / 200.0) ** (np.arange(nrep) / (nrep - 1))
+    reps = _cluster_replicas(ctx, nrep, temps)
+    ctx.batch_md_steps(reps, 200)
+    order = list(reps)
+    rng = np.random.default_rng(0)
+    kB = 8.617385e-05
+    for rnd in range(1, 7):
+        ep, _, _ = ctx.batch_energy(order)
+        vel_before = {s.sid: s.vel for s in order}
+        u = rng.random(nrep)
+        expect = list(order)
+        par = 1 if rnd % 2 == 0 else -1
+        for k in range(nrep):
+            p = k + par if k % 2 == 0 else k - par
+            if p < 0 or p >= nrep or p < k:
+                continue
+            du = (ep[p] - ep[k]) * (1.0 / (kB * temps[k]) - 1.0 / (kB * temps[p]))
+            if du <= 0 or u[k] < np.exp(-du):
+                expect[k], expect[p] = expect[p], expect[k]
+        prev = [s.sid for s in order]
+        order, acc = ctx.replica_exchange(order, temps, rnd, uniforms=u)
+        assert [s.sid for s in order] == [s.sid for s in expect]
+        for k, s in enumerate(order):
+            k_old = prev.index(s.sid)
+            np.testing.assert_allclose(s.vel, vel_before[s.sid] * np.sqrt(temps[k] / temps[k_old]), rtol=1e-13)
+        ctx.batch_md_steps(order, 50)
+    assert sorted(s.sid for s in order) == sorted(s.sid for s in reps)
+
+
+def test_replica_exchange_identical_replicas_always_swap(ctx):
+    temps = [300.0, 400.0, 500.0, 600.0]
+    reps = _cluster_replicas(ctx, 4, temps, seed0=50)
+    from gems_b200 import workloads as W
+    pos = W.cluster(147, np.random.default_rng(3))
+    for g in reps:
+        g.set_pos(pos)
+    for g in reps:
+        g.interact()
+    v0 = {g.sid: g.vel for g in reps}
+    order, acc = ctx.replica_exchange(reps, temps, 2, seed=3)
+    assert acc == 2  # pairs (0,1) and (2,3): equal energies, always accepted
+    assert [s.sid for s in order] == [reps[1].sid, reps[0].sid, reps[3].sid, reps[2].sid]
+    # velocities rescaled by sqrt(T_new / T_old)
+    np.testing.assert_allclose(order[0].vel, v0[reps[1].sid] * np.sqrt(300.0 / 400.0), rtol=1e-14)
+    np.testing.assert_allclose(order[3].vel, v0[reps[2].sid] * np.sqrt(600.0 / 500.0), rtol=1e-14)
+
+
+def test_fire_single_cluster_vs_oracle(ctx):
+    """FIRE (the intent of src/FIRE.f90 with its defects fixed) relaxes a
+    perturbed 55-atom Au cluster to the oracle's minimum."""
+    from gems_b200 import workloads as W
+    pos = W.cluster(55, np.random.default_rng(21), jitter=0.12)
+    o = O.System(pos, W.MASS["Au"])
+    o.set_smatb(*W.SMATB["Au"])
+    o.set_fire(0.002, 0.02)
+    it_o, fm_o = o.fire_relax(1e-3, 5000)
+    g = gems.System(pos, W.MASS["Au"], ctx=ctx)
+    g.set_smatb(*W.SMATB["Au"])
+    g.set_fire(0.002, 0.02)
+    it_g = ctx.batch_fire([g], 1e-3, 5000)[0]
+    assert fm_o < 1e-3 and g.fmax() < 1e-3
+    eo = o.epot_sum() * gems.UI_EV / 55
+    eg = g.energy()[0] / 55
+    assert abs(eo - eg) < 1e-6, (eo, eg)
+    assert abs(it_g - it_o) <= max(50, 0.2 * it_o)
+
+
+def test_fire_batch_equals_alone(ctx):
+    """Uneven clusters relaxed in one batch give bit-identical results to the
+    same clusters relaxed one at a time."""
+    from gems_b200 import workloads as W
+    sizes = [13, 80, 300, 38]
+    cl = [W.cluster(n, np.random.default_rng(100 + n), jitter=0.1) for n in sizes]
+
+    def mk(p):
+        g = gems.System(p, W.MASS["Au"], ctx=ctx)
+        g.set_smatb(*W.SMATB["Au"])
+        g.set_precision(gems.PREC_MIXED)
+        g.set_lanes(4, 1)
+        g.set_fire(0.002, 0.02)
+        return g
+
+    batch = [mk(p) for p in cl]
+    it_b = ctx.batch_fire(batch, 1e-3, 3000)
+    for p, gb, itb in zip(cl, batch, it_b):
+        ga = mk(p)
+        it_a = ctx.batch_fire([ga], 1e-3, 3000)[0]
+        assert it_a == itb
+        np.testing.assert_array_equal(ga.pos, gb.pos)
+        assert ga.energy()[0] == gb.energy()[0]
+        ga.destroy()

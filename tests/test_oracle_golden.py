@@ -106,3 +106,14 @@ def test_nvt_plj_ermak():
     assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
     np.testing.assert_allclose(r[:, 0], ref[:, 0], atol=2e-8)
     np.testing.assert_allclose(r[:, 1:4], ref[:, 1:4], rtol=1e-6)
+
+
+def test_replica_exchange_four_ranks():
+    """examples/RepExchange/lj.gms: 4-rank parallel tempering, 100 rounds."""
+    rows = decks.repex_rows(O)
+    ref = [np.array(r)[:, 0] for r in decks.golden()["repex_energy"]]
+    a = sum(np.sum((r - n) ** 2) for r, n in zip(ref, rows))
+    b = sum(np.sum(r) for r in ref)
+    assert abs(a / b) < 1e-6
+    for r, n in zip(ref, rows):
+        np.testing.assert_allclose(n, r, atol=1e-7)
