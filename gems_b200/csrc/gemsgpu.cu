@@ -248,6 +248,7 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   if (A.lcap > 0) {
     int* nl = nullptr;
     CHK(dalloc(ctx, &nl, (size_t)A.lcap * nc));
+    CU(cudaMemsetAsync(nl, 0, (size_t)A.lcap * nc * sizeof(int), ctx->stream));
     if (A.list && keep)
       CU(cudaMemcpy2DAsync(nl, nc * sizeof(int), A.list, keep * sizeof(int), keep * sizeof(int),
                            A.lcap, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -266,7 +267,12 @@ int grow_list(gemsgpu_ctx* ctx, int lcap) {
   if (lcap <= A.lcap && A.list) return 0;
   lcap = (lcap + 7) / 8 * 8;
   int* nl = nullptr;
-  CHK(dalloc(ctx, &nl, (size_t)lcap * std::max<int64_t>(ctx->acap, 1)));
+  const size_t ld = (size_t)std::max<int64_t>(ctx->acap, 1);
+  CHK(dalloc(ctx, &nl, (size_t)lcap * ld));
+  CU(cudaMemsetAsync(nl, 0, (size_t)lcap * ld * sizeof(int), ctx->stream));
+  // keep every system's current list: rows 0..lcap_old-1 are contiguous
+  if (A.list && A.lcap > 0)
+    CU(cudaMemcpyAsync(nl, A.list, (size_t)A.lcap * ld * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   if (A.list) CU(cudaFree(A.list));
   A.list = nl;

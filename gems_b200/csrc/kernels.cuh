@@ -598,6 +598,7 @@ constexpr int UNR = 4;
     _Pragma("unroll") for (int u = 0; u < UNR; u++) {                         \
       int m = m0 + u * K;                                                     \
       jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;            \
+      if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;                     \
     }                                                                         \
     GATHER_T gj[UNR];                                                         \
     _Pragma("unroll") for (int u = 0; u < UNR; u++) if (jj[u] >= 0) gj[u] = GATHER(jj[u]); \
@@ -813,6 +814,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
       for (int u = 0; u < UNR; u++) {
         int m = m0 + u * K;
         jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;
+        if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;  // never gather outside the arena
       }
       int4 gj[UNR];
 #pragma unroll
@@ -875,6 +877,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M
       for (int u = 0; u < UNR; u++) {
         int m = m0 + u * K;
         jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;
+        if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;  // never gather outside the arena
       }
       int4 gj[UNR];
       float gb[UNR];
@@ -1086,6 +1089,7 @@ __global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
   const double4 xi = A.pos[i];
   for (int m = 0; m < nn; m++) {
     int j = A.list[(size_t)m * A.cap + i];
+    if ((unsigned)j >= (unsigned)A.cap) continue;  // never gather outside the arena
     double v0, v1, v2;
     vd_fp64(S, xi, A.pos[j], v0, v1, v2);
     double rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
