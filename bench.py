@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--arms", default="fp64,mixed,batched",
                     help="comma list of arms to run (profiling); the full line needs all three")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2 (default, the headline line) or one of the other configurations")
+    ap.add_argument("--serve-seconds", type=float, default=20.0,
+                    help="c4: length of the Poisson arrival window (the full configuration is 120 s)")
     ap.add_argument("--tune", default=None,
                     help="lanes,variant for every mixed system instead of the autotuner (profiling)")
     return ap.parse_args()
@@ -288,6 +292,208 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- other configs
+def _line(metric, value, unit, args, config, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+         "data": "synthetic", "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def _time_md(ctx, torch, systems, block, steps, warmup, ext):
+    for _ in range(warmup):
+        ctx.batch_md_steps(systems, block)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(steps):
+        ctx.batch_md_steps(systems, block)
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    return sum(s.n for s in systems) * block * steps / (ms * 1e-3), ms / steps
+
+
+def run_c1(args, gems, torch, ctx, ext):
+    """LJ fluid, 4000 atoms, NVE velocity Verlet: FP64, mixed, and 16 mixed
+    replicas; energy drift over the timed steps."""
+    from gems_b200 import workloads as W
+    w = W.lj_fluid()
+    out = {}
+    for name, prec, nrep in (("fp64", gems.PREC_FP64, 1), ("mixed", gems.PREC_MIXED, 1),
+                             ("batched", gems.PREC_MIXED, 16)):
+        ss = []
+        for k in range(nrep):
+            wk = W.lj_fluid(seed=1 + k)
+            g = gems.System(wk["pos"], 1.0, ctx=ctx, vel=wk["vel"])
+            g.set_box(wk["L"], (True, True, True))
+            e, sg, rc, sh = wk["lj"]
+            g.set_lj(e, sg, rc, eshift=sh)
+            g.set_skin(wk["skin"])
+            g.set_precision(prec)
+            g.set_vv(wk["dt"])
+            g.interact()
+            if k == 0:
+                g.tuned = g.autotune(5)
+            else:
+                g.set_lanes(*ss[0].tuned[:2])
+                g.tuned = ss[0].tuned
+            ss.append(g)
+        e0 = sum(x.energy()[0] + x.energy()[1] for x in ss)
+        val, ms = _time_md(ctx, torch, ss, args.block, args.steps, args.warmup, ext)
+        e1 = sum(x.energy()[0] + x.energy()[1] for x in ss)
+        out[name] = {"value": val, "ms_per_block": ms, "atoms": sum(x.n for x in ss),
+                     "drift_ev_per_atom": (e1 - e0) / sum(x.n for x in ss),
+                     "lanes_variant": list(ss[0].tuned[:2])}
+        for g in ss:
+            g.destroy()
+    _line("atom-steps/s (LJ fluid 4000, NVE VV)", out["batched"]["value"], UNIT, args,
+          {"workload": "lj_fluid_4000 (fcc 10^3, rho*=0.8442, T*=0.72, rc 2.5 shifted, skin 0.3)",
+           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out)
+
+
+def run_c5(args, gems, torch, ctx, ext):
+    """Tersoff Si(C), 1,000,000 atoms on a diamond lattice, NVE VV dt=1 fs."""
+    from gems_b200 import workloads as W
+    w = W.tersoff_si()
+    out = {}
+    for name, prec in (("fp64", gems.PREC_FP64), ("mixed", gems.PREC_MIXED)):
+        g = gems.System(w["pos"], w["mass"], ctx=ctx, vel=w["vel"])
+        g.set_box(w["L"], (True, True, True))
+        g.set_tersoff(w["tersoff"])
+        g.set_skin(w["skin"])
+        g.set_precision(prec)
+        g.set_vv(w["dt"])
+        g.interact()
+        ep0, ek0, _ = g.energy()
+        val, ms = _time_md(ctx, torch, [g], args.block, args.steps, args.warmup, ext)
+        ep1, ek1, _ = g.energy()
+        kern = g.time_kernels(5)
+        nsteps = args.block * (args.steps + args.warmup)
+        out[name] = {"value": val, "ms_per_block": ms, "atoms": g.n, "steps_run": nsteps,
+                     "etot_drift_ev_per_atom": ((ep1 + ek1) - (ep0 + ek0)) / g.n,
+                     "force_kernel_ms": kern[0], "rebuild_ms": kern[2]}
+        g.destroy()
+    _line("atom-steps/s (Tersoff Si 1M, NVE VV)", out["mixed"]["value"], UNIT, args,
+          {"workload": "tersoff_si_1000000 (diamond 50^3, a=5.431, 1000 K, dt 1 fs, skin 1.0)",
+           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out)
+
+
+def run_c3(args, gems, torch, ctx, ext):
+    """1024 free Au clusters relaxed with FIRE in one batch, then 64
+    replica-exchange replicas of a 147-atom cluster (200-900 K)."""
+    from gems_b200 import workloads as W
+    sm, m = W.SMATB["Au"], W.MASS["Au"]
+    clusters = W.batched_clusters()
+    ss = []
+    for k, p in enumerate(clusters):
+        g = gems.System(p, m, ctx=ctx)
+        g.set_smatb(*sm)
+        g.set_precision(gems.PREC_MIXED)
+        g.set_lanes(4, 1)
+        g.set_fire(0.002, 0.02)
+        ss.append(g)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    iters = ctx.batch_fire(ss, 1e-3, 5000)
+    torch.cuda.synchronize()
+    t_fire = time.perf_counter() - t0
+    atom_iters = float(sum(int(i) * g.n for i, g in zip(iters, ss)))
+    fmax = [g.fmax() for g in ss[:64]]
+    fire = {"systems": len(ss), "atoms": sum(g.n for g in ss), "seconds": t_fire,
+            "atom_steps_per_s": atom_iters / t_fire, "iters_median": float(np.median(iters)),
+            "iters_max": int(max(iters)), "converged": int(sum(int(i) < 5000 for i in iters)),
+            "fmax_first64_max": max(fmax)}
+    for g in ss:
+        g.destroy()
+    # replica exchange
+    nrep = 64
+    temps = 200.0 * (900.0 / 200.0) ** (np.arange(nrep) / (nrep - 1))
+    base = W.cluster(147, np.random.default_rng(147))
+    reps = []
+    for k in range(nrep):
+        g = gems.System(base, m, ctx=ctx)
+        g.set_smatb(*sm)
+        g.set_precision(gems.PREC_MIXED)
+        g.set_lanes(4, 1)
+        g.set_ermak(0.002, 1.0, temps[k], seed=500 + k)
+        g.interact()
+        reps.append(g)
+    order = list(reps)
+    rounds, acc, attempted = 10, 0, 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in range(1, rounds + 1):
+        ctx.batch_md_steps(order, 500)
+        order, a = ctx.replica_exchange(order, temps, r, seed=77)
+        acc += a
+        par = 1 if r % 2 == 0 else -1
+        attempted += sum(1 for q in range(nrep) if q % 2 == 0 and 0 <= q + par < nrep and q + par > q) + \
+            sum(1 for q in range(nrep) if q % 2 == 1 and 0 <= q - par < nrep and q - par > q)
+    torch.cuda.synchronize()
+    t_rex = time.perf_counter() - t0
+    rex = {"replicas": nrep, "atoms_each": 147, "rounds": rounds, "steps_per_round": 500,
+           "seconds": t_rex, "atom_steps_per_s": nrep * 147 * 500 * rounds / t_rex,
+           "accepted": acc, "attempted": attempted}
+    for g in reps:
+        g.destroy()
+    _line("atom-steps/s (1024 Au clusters FIRE + 64-replica exchange, batched)", fire["atom_steps_per_s"], UNIT,
+          args, {"workload": "1024 Au clusters 13-2000 atoms (log-uniform, seed 3), FIRE to 1e-3 eV/A cap 5000; "
+                             "64 x 147-atom replicas 200-900 K, swaps every 500 steps"},
+          dtype="f32+f64acc", fire=fire, replica_exchange=rex)
+
+
+def run_c4(args, gems, torch, ctx, ext):
+    """Served stream: Poisson 200 req/s of Au/Ag/Pt cluster jobs."""
+    from gems_b200 import workloads as W
+    srv = gems.Server(ctx, max_jobs=384, max_atoms=600000, lanes=4, variant=1, chunk=50)
+    stream = list(W.serve_stream(seconds=args.serve_seconds))
+    prepared = []
+    for j in stream:
+        rng = np.random.default_rng(j["pos_seed"])
+        a0 = {"Au": 4.078, "Ag": 4.086, "Pt": 3.924}[j["element"]]
+        prepared.append((j, W.cluster(j["n"], rng, a=a0, check=False)))
+    lat, done_atoms_steps = [], 0.0
+    pending = {}
+    k = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while k < len(prepared) or pending:
+        now = time.perf_counter() - t0
+        while k < len(prepared) and prepared[k][0]["t"] <= now:
+            j, pos = prepared[k]
+            el = j["element"]
+            kind = gems.JOB_FIRE if j["kind"] == "fire" else gems.JOB_MD
+            jid = srv.submit(pos, W.MASS[el], W.SMATB[el], kind, 5000 if kind == gems.JOB_FIRE else 2000,
+                             dt=0.002, temp=j["temp"], gamma=1.0, fmax=1e-3, seed=j["seed"])
+            pending[jid] = (j["t"], j["n"])
+            k += 1
+        running, queued, fin = srv.step()
+        if fin or not running:
+            now = time.perf_counter() - t0
+            for jid in list(pending):
+                r = srv.poll(jid)
+                if r["state"] == gems.JOB_DONE:
+                    t_arr, n = pending.pop(jid)
+                    lat.append(now - t_arr)
+                    done_atoms_steps += n * r["iters"]
+                    srv.forget(jid)
+        if not running and not queued and k < len(prepared):
+            time.sleep(max(0.0, prepared[k][0]["t"] - (time.perf_counter() - t0)))
+    wall = time.perf_counter() - t0
+    srv.close()
+    lat = np.array(lat)
+    _line("serve latency and throughput (Au/Ag/Pt cluster jobs, Poisson 200 req/s)", float(np.percentile(lat, 50)),
+          "s (p50 latency)", args,
+          {"workload": "Poisson 200 req/s for %.0f s, Au/Ag/Pt clusters 13-5000 atoms, 70%% FIRE / 30%% 2000-step "
+                       "Ermak 300-800 K" % args.serve_seconds}, dtype="f32+f64acc",
+          higher_is_better=False, p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)),
+          jobs=len(lat), wall_s=wall, throughput_jobs_per_s=len(lat) / wall,
+          throughput_atom_steps_per_s=done_atoms_steps / wall)
+
+
 def main():
     global FIXED_TUNE
     args = parse()
@@ -295,6 +501,15 @@ def main():
         FIXED_TUNE = tuple(int(v) for v in args.tune.split(","))
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.config != "c2":
+        import torch
+        import gems_b200 as gems
+        torch.cuda.set_device(0)
+        ctx = gems.Context(device=0)
+        ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=0)
+        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args, gems, torch, ctx, ext)
+        ctx.close()
         return
     import torch
     import gems_b200 as gems

@@ -105,7 +105,7 @@ def tersoff_si(seed=5, ncell=50):
                 pbc=(1, 1, 1), tersoff=TERSOFF_SI, skin=1.0, dt=0.001, nsteps=2000)
 
 
-def cluster(n, rng, dmin=2.5, a=4.078, jitter=0.05):
+def cluster(n, rng, dmin=2.5, a=4.078, jitter=0.05, check=True):
     """A compact n-atom blob at bulk fcc density: the n sites of a randomly
     rotated and shifted fcc lattice (lattice constant a) nearest to the
     centre, each displaced by N(0, jitter); every pair stays >= dmin apart.
@@ -121,7 +121,7 @@ def cluster(n, rng, dmin=2.5, a=4.078, jitter=0.05):
     pos = pos[np.argsort(r2, kind="stable")[:n]]
     for _ in range(20):
         trial = pos + rng.normal(0.0, jitter, pos.shape)
-        if n < 2:
+        if n < 2 or not check:
             return trial
         d2 = ((trial[:, None, :] - trial[None, :, :]) ** 2).sum(-1) if n <= 3000 else None
         if d2 is None:
@@ -135,3 +135,30 @@ def cluster(n, rng, dmin=2.5, a=4.078, jitter=0.05):
 def cluster_sizes(count, lo, hi, rng):
     """log-uniform sizes in [lo, hi], rounded."""
     return np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), count))).astype(int)
+
+
+def batched_clusters(seed=3, count=1024, lo=13, hi=2000):
+    """C3 part 1: `count` free Au clusters, log-uniform sizes in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    sizes = cluster_sizes(count, lo, hi, rng)
+    return [cluster(int(n), rng, check=False) for n in sizes]
+
+
+def serve_stream(seed=4, rate=200.0, seconds=120.0, lo=13, hi=5000):
+    """C4: Poisson arrivals of Au/Ag/Pt cluster jobs; 70 % FIRE relaxations,
+    30 % 2000-step Langevin runs at U(300, 800) K.  Yields dicts with the
+    arrival time (s), element, size, kind, temperature and seed."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    k = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            return
+        el = ("Au", "Ag", "Pt")[int(rng.integers(0, 3))]
+        n = int(np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        fire = rng.random() < 0.7
+        yield dict(t=t, element=el, n=n, kind="fire" if fire else "md",
+                   temp=float(rng.uniform(300.0, 800.0)), seed=1000 + k,
+                   pos_seed=int(rng.integers(0, 2 ** 31)))
+        k += 1
