@@ -130,7 +130,10 @@ struct Arena {
   double* mass;
   int* type;
   int* nn;              // neighbours per atom
-  int* list;            // column-major: list[m * cap + i]
+  int* list;            // column-major: list[m * cap + i], the reference's order
+  int* flist;           // the same pairs sorted by distance at the rebuild
+                        // (force kernels: a warp's atoms meet the same shell
+                        // at the same slot, so the distance classes do not diverge)
   int* cell_of;
   int* slot;
   int* cell_count;      // per cell, zero between rebuilds

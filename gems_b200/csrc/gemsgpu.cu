@@ -244,17 +244,20 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   CHK(dgrow(ctx, &A.slot, keep, nc));
   CHK(dgrow(ctx, &A.cell_atoms, keep, nc));
   CHK(dgrow(ctx, &A.ext_normals, 6 * keep, 6 * nc));
-  // the list's leading dimension is the atom capacity: re-lay it out
+  // the lists' leading dimension is the atom capacity: re-lay them out
   if (A.lcap > 0) {
-    int* nl = nullptr;
-    CHK(dalloc(ctx, &nl, (size_t)A.lcap * nc));
-    CU(cudaMemsetAsync(nl, 0, (size_t)A.lcap * nc * sizeof(int), ctx->stream));
-    if (A.list && keep)
-      CU(cudaMemcpy2DAsync(nl, nc * sizeof(int), A.list, keep * sizeof(int), keep * sizeof(int),
-                           A.lcap, cudaMemcpyDeviceToDevice, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
-    if (A.list) CU(cudaFree(A.list));
-    A.list = nl;
+    int** lists[2] = {&A.list, &A.flist};
+    for (int q = 0; q < 2; q++) {
+      int* nl = nullptr;
+      CHK(dalloc(ctx, &nl, (size_t)A.lcap * nc));
+      CU(cudaMemsetAsync(nl, 0, (size_t)A.lcap * nc * sizeof(int), ctx->stream));
+      if (*lists[q] && keep)
+        CU(cudaMemcpy2DAsync(nl, nc * sizeof(int), *lists[q], keep * sizeof(int), keep * sizeof(int), A.lcap,
+                             cudaMemcpyDeviceToDevice, ctx->stream));
+      CU(cudaStreamSynchronize(ctx->stream));
+      if (*lists[q]) CU(cudaFree(*lists[q]));
+      *lists[q] = nl;
+    }
   }
   ctx->acap = nc;
   A.cap = nc;
@@ -266,18 +269,21 @@ int grow_list(gemsgpu_ctx* ctx, int lcap) {
   Arena& A = ctx->A;
   if (lcap <= A.lcap && A.list) return 0;
   lcap = (lcap + 7) / 8 * 8;
-  int* nl = nullptr;
   const size_t ld = (size_t)std::max<int64_t>(ctx->acap, 1);
-  CHK(dalloc(ctx, &nl, (size_t)lcap * ld));
-  CU(cudaMemsetAsync(nl, 0, (size_t)lcap * ld * sizeof(int), ctx->stream));
-  // keep every system's current list: rows 0..lcap_old-1 are contiguous
-  if (A.list && A.lcap > 0)
-    CU(cudaMemcpyAsync(nl, A.list, (size_t)A.lcap * ld * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
-  CU(cudaStreamSynchronize(ctx->stream));
-  if (A.list) CU(cudaFree(A.list));
-  A.list = nl;
+  int** lists[2] = {&A.list, &A.flist};
+  for (int q = 0; q < 2; q++) {
+    int* nl = nullptr;
+    CHK(dalloc(ctx, &nl, (size_t)lcap * ld));
+    CU(cudaMemsetAsync(nl, 0, (size_t)lcap * ld * sizeof(int), ctx->stream));
+    // keep every system's current list: rows 0..lcap_old-1 are contiguous
+    if (*lists[q] && A.lcap > 0)
+      CU(cudaMemcpyAsync(nl, *lists[q], (size_t)A.lcap * ld * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (*lists[q]) CU(cudaFree(*lists[q]));
+    *lists[q] = nl;
+  }
   A.lcap = lcap;
-  size_t smem = (size_t)LIST_ATOMS * lcap * sizeof(int);
+  size_t smem = list_smem(lcap);
   if (smem > 48 * 1024) {
     if (smem > 200 * 1024) return fail(ctx, GEMSGPU_ERR_ARG, "neighbour capacity %d too large", lcap);
     CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -632,7 +638,7 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 
     k_scan2<<<(int)ss.size(), BLOCK, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
     k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
     k_sort_cells<<<mc8.nblk, BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
-    k_list_cells<<<mw.nblk, BLOCK, LIST_ATOMS * A.lcap * sizeof(int), st>>>(A, mw); ++ctx->launches;
+    k_list_cells<<<mw.nblk, BLOCK, list_smem(A.lcap), st>>>(A, mw); ++ctx->launches;
   }
   if (n2) {
     k_list_n2<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
@@ -1156,7 +1162,7 @@ int pool_rebuild(gemsgpu_pool* P, int in_graph) {
   k_scan2<<<ns, BLOCK, 0, st>>>(A, P->dsys, ns); ++ctx->launches;
   k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   k_sort_cells<<<mc8.nblk, BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
-  k_list_cells<<<mw.nblk, BLOCK, LIST_ATOMS * A.lcap * sizeof(int), st>>>(A, mw); ++ctx->launches;
+  k_list_cells<<<mw.nblk, BLOCK, list_smem(A.lcap), st>>>(A, mw); ++ctx->launches;
   k_list_n2<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   k_count_rebuild<<<(ns + 255) / 256, 256, 0, st>>>(A, P->dsys, ns, in_graph); ++ctx->launches;
   CU(cudaGetLastError());
@@ -1314,9 +1320,9 @@ int pool_chunk(gemsgpu_pool* P) {
     if (!grow) return 0;
     CHK(snapshot(ctx, true));
     CHK(grow_list(ctx, grow + grow / 4 + 8));
-    if (ctx->A.lcap * LIST_ATOMS * sizeof(int) > 48 * 1024)
+    if (list_smem(ctx->A.lcap) > 48 * 1024)
       CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(ctx->A.lcap * LIST_ATOMS * sizeof(int))));
+                              (int)list_smem(ctx->A.lcap)));
     k_force_rebuild<<<(P->max_systems + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, P->dsys, P->max_systems);
     ++ctx->launches;
     k_clear_status<<<(P->max_systems + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, P->dsys, P->max_systems);
@@ -1392,7 +1398,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   drop_maps(ctx);
   Arena& A = ctx->A;
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.epot, A.band, A.eband,
-                  A.ebandf, A.fxp, A.minv, A.mass, A.type, A.nn, A.list, A.cell_of, A.slot,
+                  A.ebandf, A.fxp, A.minv, A.mass, A.type, A.nn, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->d_sys};

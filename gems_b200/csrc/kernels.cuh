@@ -423,7 +423,10 @@ __global__ void k_sort_cells(Arena A, BlockMap C) {
 
 // ------------------------------------------------------------------ lists
 __device__ __forceinline__ void list_put(const Arena& A, int i, int m, int j) {
-  if (m < A.lcap) A.list[(size_t)m * A.cap + i] = j;
+  if (m < A.lcap) {
+    A.list[(size_t)m * A.cap + i] = j;
+    A.flist[(size_t)m * A.cap + i] = j;  // O(N^2) lists keep index order for the forces too
+  }
 }
 
 __device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
@@ -442,12 +445,18 @@ __device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
 // (LIST_ATOMS atoms x lcap) and written out as coalesced column rows.
 constexpr int LIST_ATOMS = BLOCK / 32;
 
+// dynamic shared memory of k_list_cells: ids and distances of the staged lists
+__host__ __device__ constexpr size_t list_smem(int lcap) {
+  return (size_t)LIST_ATOMS * lcap * (sizeof(int) + sizeof(float));
+}
+
 __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   if (!A.st[s].rebuild || !S.use_cells) return;
-  extern __shared__ int stage[];  // [LIST_ATOMS][lcap]
+  extern __shared__ int stage[];  // [LIST_ATOMS][lcap] ids, then [LIST_ATOMS][lcap] distances
+  float* stage_rd = reinterpret_cast<float*>(stage + LIST_ATOMS * A.lcap);
   const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int i0 = M.first[blockIdx.x];
   const int i = i0 + warp;
@@ -459,6 +468,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap M) {
     int cx = c % S.nc[0], cy = (c / S.nc[0]) % S.nc[1], cz = c / (S.nc[0] * S.nc[1]);
     const int nst = S.half ? 14 : 27;
     int* row = stage + warp * A.lcap;
+    float* rrow = stage_rd + warp * A.lcap;
     for (int k = 0; k < nst; k++) {
       int dx, dy, dz;
       stencil(k, dx, dy, dz);
@@ -482,31 +492,52 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap M) {
         int tt = t + ln;
         bool ok = false;
         int j = -1;
+        double rd = 0.0;
         if (tt < cnt) {
           j = A.cell_atoms[beg + tt];
-          ok = (j != i) && rd_exact(S, xi, A.pos[j]) < S.rlist2;
+          if (j != i) {
+            rd = rd_exact(S, xi, A.pos[j]);
+            ok = rd < S.rlist2;
+          }
         }
         unsigned b = __ballot_sync(0xffffffffu, ok);
         if (ok) {
           int mm = m + __popc(b & ((1u << ln) - 1u));
-          if (mm < A.lcap) row[mm] = j;
+          if (mm < A.lcap) {
+            row[mm] = j;
+            rrow[mm] = (float)rd;
+          }
         }
         m += __popc(b);
       }
     }
   }
   __syncthreads();
-  // coalesced write-out: row m of the block's atoms, LIST_ATOMS ints at a time
   __shared__ int cnt_sh[LIST_ATOMS];
-  if (ln == 0) cnt_sh[warp] = act ? m : 0;
+  if (ln == 0) cnt_sh[warp] = act ? min(m, A.lcap) : 0;
   __syncthreads();
   int mx = 0;
   for (int w = 0; w < LIST_ATOMS; w++) mx = max(mx, cnt_sh[w]);
-  mx = min(mx, A.lcap);
+  // reference order, written out as coalesced column rows
   for (int e = threadIdx.x; e < mx * LIST_ATOMS; e += BLOCK) {
     int mm = e / LIST_ATOMS, w = e % LIST_ATOMS;
     int ii = i0 + w;
     if (ii < M.end[blockIdx.x] && mm < cnt_sh[w]) A.list[(size_t)mm * A.cap + ii] = stage[w * A.lcap + mm];
+  }
+  // force order: each warp ranks its atom's entries by distance (ties by slot)
+  if (act) {
+    const int n = cnt_sh[warp];
+    const int* row = stage + warp * A.lcap;
+    const float* rrow = stage_rd + warp * A.lcap;
+    for (int e = ln; e < n; e += 32) {
+      const float re = rrow[e];
+      int rank = 0;
+      for (int f = 0; f < n; f++) {
+        float rf = rrow[f];
+        rank += (rf < re) || (rf == re && f < e);
+      }
+      A.flist[(size_t)rank * A.cap + i] = row[e];
+    }
   }
   if (act && ln == 0) list_done(A, s, i, m);
 }
@@ -597,7 +628,7 @@ constexpr int UNR = 4;
     int jj[UNR];                                                              \
     _Pragma("unroll") for (int u = 0; u < UNR; u++) {                         \
       int m = m0 + u * K;                                                     \
-      jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;            \
+      jj[u] = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;            \
       if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;                     \
     }                                                                         \
     GATHER_T gj[UNR];                                                         \
@@ -813,7 +844,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
 #pragma unroll
       for (int u = 0; u < UNR; u++) {
         int m = m0 + u * K;
-        jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;
+        jj[u] = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;
         if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;  // never gather outside the arena
       }
       int4 gj[UNR];
@@ -876,7 +907,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M
 #pragma unroll
       for (int u = 0; u < UNR; u++) {
         int m = m0 + u * K;
-        jj[u] = m < nn ? __ldg(&A.list[(size_t)m * A.cap + i]) : -1;
+        jj[u] = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;
         if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;  // never gather outside the arena
       }
       int4 gj[UNR];
@@ -1088,7 +1119,7 @@ __global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
   const int nn = min(A.nn[i], A.lcap);
   const double4 xi = A.pos[i];
   for (int m = 0; m < nn; m++) {
-    int j = A.list[(size_t)m * A.cap + i];
+    int j = A.flist[(size_t)m * A.cap + i];
     if ((unsigned)j >= (unsigned)A.cap) continue;  // never gather outside the arena
     double v0, v1, v2;
     vd_fp64(S, xi, A.pos[j], v0, v1, v2);
