@@ -569,9 +569,10 @@ def main():
             kern64 = s.time_kernels(50)
             s.destroy()
     # --- batched arm: replicas in one launch
-    reps = [make_system(gems, ctx, c2_replica(100 + 1000 * rank), gems.PREC_MIXED, seed=100)]
-    reps += [make_system(gems, ctx, c2_replica(100 + k + 1000 * rank), gems.PREC_MIXED, seed=100 + k,
-                         tune=reps[0].tuned) for k in range(1, args.replicas)]
+    reps = [make_system(gems, ctx, c2_replica(100 + k + 1000 * rank), gems.PREC_MIXED, seed=100 + k,
+                        tune=(2, 0)) for k in range(args.replicas)]
+    if FIXED_TUNE is None:
+        ctx.batch_autotune(reps, 10)   # the batch's own best launch shape
     for s in reps:
         s.interact()
     clocks = Clocks(dev)

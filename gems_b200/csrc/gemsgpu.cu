@@ -531,18 +531,24 @@ int sys_array(gemsgpu_ctx* ctx, const std::vector<int>& ss, const int** out) {
 }
 
 // ------------------------------------------------------------- launches
-// one SMA-TB pass (0: density, 1: force) for a block map of K lanes per atom
+// one SMA-TB pass (0: density, 1: force) for a block map of K lanes per atom.
+// variant bit 0: species constants in shared memory (1) or registers (0,
+// single species only); bit 1: register-capped build for more warps per SM.
 template <int K>
-void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, const BlockMap& m) {
+void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, const BlockMap& m) {
   cudaStream_t st = ctx->stream;
   const Arena& A = ctx->A;
   if (prec == PREC_MIXED) {
     if (pass == 0) {
-      if (regs) k_smatb_rho_mixed<K, true><<<m.nblk, BLOCK, 0, st>>>(A, m);
-      else k_smatb_rho_mixed<K, false><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      if (regs && tight) k_smatb_rho_mixed<K, true, 5><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else if (regs) k_smatb_rho_mixed<K, true, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else if (tight) k_smatb_rho_mixed<K, false, 5><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else k_smatb_rho_mixed<K, false, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
     } else {
-      if (regs) k_smatb_force_mixed<K, true><<<m.nblk, BLOCK, 0, st>>>(A, m);
-      else k_smatb_force_mixed<K, false><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      if (regs && tight) k_smatb_force_mixed<K, true, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else if (regs) k_smatb_force_mixed<K, true, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else if (tight) k_smatb_force_mixed<K, false, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else k_smatb_force_mixed<K, false, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
     }
   } else {
     if (pass == 0) k_smatb_rho_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m);
@@ -558,14 +564,16 @@ void lj_k(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
   ++ctx->launches;
 }
 
-void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, bool regs, int K, const BlockMap& m) {
+void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, int K, const BlockMap& m) {
+  const bool regs = single && (variant & 1) == 0;
+  const bool tight = (variant & 2) != 0;
   switch (K) {
-    case 2: smatb_pass_k<2>(ctx, pass, prec, regs, m); break;
-    case 4: smatb_pass_k<4>(ctx, pass, prec, regs, m); break;
-    case 8: smatb_pass_k<8>(ctx, pass, prec, regs, m); break;
-    case 16: smatb_pass_k<16>(ctx, pass, prec, regs, m); break;
-    case 32: smatb_pass_k<32>(ctx, pass, prec, regs, m); break;
-    default: smatb_pass_k<1>(ctx, pass, prec, regs, m); break;
+    case 1: smatb_pass_k<1>(ctx, pass, prec, regs, tight, m); break;
+    case 2: smatb_pass_k<2>(ctx, pass, prec, regs, tight, m); break;
+    case 4: smatb_pass_k<4>(ctx, pass, prec, regs, tight, m); break;
+    case 8: smatb_pass_k<8>(ctx, pass, prec, regs, tight, m); break;
+    case 16: smatb_pass_k<16>(ctx, pass, prec, regs, tight, m); break;
+    default: smatb_pass_k<32>(ctx, pass, prec, regs, tight, m); break;
   }
 }
 
@@ -588,12 +596,13 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
     if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no force field", s);
     if (h.d.half) return fail(ctx, GEMSGPU_ERR_STATE, "system %d: force kernels need full lists", s);
     int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
-    int regs = (h.ntypes == 1 && h.variant == 0) ? 1 : 0;
-    groups[{h.d.ff, h.d.prec, K, regs}].push_back(s);
+    int key = h.variant * 2 + (h.ntypes == 1 ? 1 : 0);
+    groups[{h.d.ff, h.d.prec, K, key}].push_back(s);
   }
   for (auto& kv : groups) {
     int ff = std::get<0>(kv.first), prec = std::get<1>(kv.first), K = std::get<2>(kv.first);
-    bool one = std::get<3>(kv.first) != 0;
+    const int variant = std::get<3>(kv.first) / 2;
+    const bool single = (std::get<3>(kv.first) & 1) != 0;
     BlockMap m;
     if (ff == FF_TERSOFF) {
       CHK(get_map(ctx, kv.second, BLOCK, 0, &m));
@@ -607,8 +616,8 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
     }
     CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
     if (ff == FF_SMATB) {
-      smatb_pass(ctx, 0, prec, one, K, m);
-      smatb_pass(ctx, 1, prec, one, K, m);
+      smatb_pass(ctx, 0, prec, variant, single, K, m);
+      smatb_pass(ctx, 1, prec, variant, single, K, m);
     } else if (ff == FF_LJ) {
       lj_pass(ctx, prec, K, m);
     }
@@ -1173,10 +1182,12 @@ int pool_forces(gemsgpu_pool* P) {
   gemsgpu_ctx* ctx = P->ctx;
   const BlockMap& mk = P->maps[4];
   const BlockMap& ma = P->maps[0];
-  const bool regs = P->variant == 0;
   if (P->ff == FF_SMATB) {
-    smatb_pass(ctx, 0, P->prec, regs, P->lanes, mk);
-    smatb_pass(ctx, 1, P->prec, regs, P->lanes, mk);
+    // the graph is captured once: the register variant (bit 0 clear) is only
+    // allowed for single-species members (checked in gemsgpu_pool_set)
+    const bool single = (P->variant & 1) == 0;
+    smatb_pass(ctx, 0, P->prec, P->variant, single, P->lanes, mk);
+    smatb_pass(ctx, 1, P->prec, P->variant, single, P->lanes, mk);
   } else if (P->ff == FF_LJ) {
     lj_pass(ctx, P->prec, P->lanes, mk);
   } else if (P->ff == FF_TERSOFF) {
@@ -2056,32 +2067,52 @@ int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys, double* epo
   return 0;
 }
 
-int gemsgpu_autotune(gemsgpu_ctx* ctx, int sys, int reps, int* lanes_out, int* variant_out,
-                     double* best_ms) {
-  CHK(check_sys(ctx, sys));
+static int sys_list(gemsgpu_ctx* ctx, const int* sys, int nsys, std::vector<int>& ss);
+
+// time launch_forces over the candidate shapes for a set of systems that
+// share one force field / precision, keep the fastest for all of them
+static int autotune_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, int* lanes_out, int* variant_out,
+                        double* best_ms) {
   if (reps <= 0) reps = 10;
   cudaSetDevice(ctx->device);
-  SysHost& h = ctx->sys[sys];
-  if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "autotune: no force field");
-  std::vector<int> ss{sys};
-  if (h.first || h.pos_dirty || !h.has_forces) CHK(interact_group(ctx, ss, true));
+  const SysHost& h0 = ctx->sys[ss[0]];
+  bool single = true;
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "autotune: no force field");
+    if (h.d.ff != h0.d.ff || h.d.prec != h0.d.prec)
+      return fail(ctx, GEMSGPU_ERR_ARG, "autotune: systems differ in force field or precision");
+    single &= h.ntypes == 1;
+  }
+  std::vector<int> need;
+  for (int s : ss)
+    if (ctx->sys[s].first || ctx->sys[s].pos_dirty || !ctx->sys[s].has_forces) need.push_back(s);
+  if (!need.empty()) CHK(interact_group(ctx, need, true));
   std::vector<std::pair<int, int>> cand;
-  if (h.d.ff == FF_TERSOFF) {
+  if (h0.d.ff == FF_TERSOFF) {
     cand.push_back({1, 1});
   } else {
-    for (int K : {2, 4, 8, 16, 32}) {
+    for (int K : {1, 2, 4, 8, 16, 32}) {
       cand.push_back({K, 1});
-      if (h.d.ff == FF_SMATB && h.ntypes == 1 && h.d.prec == PREC_MIXED) cand.push_back({K, 0});
+      if (h0.d.ff == FF_SMATB && h0.d.prec == PREC_MIXED) {
+        cand.push_back({K, 3});
+        if (single) {
+          cand.push_back({K, 0});
+          cand.push_back({K, 2});
+        }
+      }
     }
   }
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
   double best = 1e30;
-  std::pair<int, int> pick = {h.lanes, h.variant};
+  std::pair<int, int> pick = {h0.lanes, h0.variant};
   for (auto c : cand) {
-    h.lanes = c.first;
-    h.variant = c.second;
+    for (int s : ss) {
+      ctx->sys[s].lanes = c.first;
+      ctx->sys[s].variant = c.second;
+    }
     CHK(launch_forces(ctx, ss));  // warm-up (and map creation)
     CU(cudaEventRecord(e0, ctx->stream));
     for (int r = 0; r < reps; r++) CHK(launch_forces(ctx, ss));
@@ -2096,22 +2127,38 @@ int gemsgpu_autotune(gemsgpu_ctx* ctx, int sys, int reps, int* lanes_out, int* v
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  h.lanes = pick.first;
-  h.variant = pick.second;
+  for (int s : ss) {
+    ctx->sys[s].lanes = ctx->sys[s].d.ff == FF_TERSOFF ? 1 : pick.first;
+    ctx->sys[s].variant = pick.second;
+  }
   invalidate(ctx);
-  if (lanes_out) *lanes_out = h.lanes;
-  if (variant_out) *variant_out = h.variant;
+  if (lanes_out) *lanes_out = pick.first;
+  if (variant_out) *variant_out = pick.second;
   if (best_ms) *best_ms = best;
   return 0;
+}
+
+int gemsgpu_autotune(gemsgpu_ctx* ctx, int sys, int reps, int* lanes_out, int* variant_out,
+                     double* best_ms) {
+  CHK(check_sys(ctx, sys));
+  return autotune_set(ctx, {sys}, reps, lanes_out, variant_out, best_ms);
+}
+
+int gemsgpu_batch_autotune(gemsgpu_ctx* ctx, const int* sys, int nsys, int reps, int* lanes_out,
+                           int* variant_out, double* best_ms) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  return autotune_set(ctx, ss, reps, lanes_out, variant_out, best_ms);
 }
 
 int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant) {
   CHK(check_sys(ctx, sys));
   if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
     return fail(ctx, GEMSGPU_ERR_ARG, "lanes must be a power of two <= 32");
+  if (variant < 0 || variant > 3) return fail(ctx, GEMSGPU_ERR_ARG, "variant must be 0..3");
   SysHost& h = ctx->sys[sys];
   if (h.d.ff != FF_TERSOFF) h.lanes = lanes;
-  h.variant = variant ? 1 : 0;
+  h.variant = variant;
   invalidate(ctx);
   return 0;
 }
@@ -2212,7 +2259,7 @@ int gemsgpu_pool_create(gemsgpu_ctx* ctx, int max_systems, int64_t max_atoms, in
   P->ff = ff;
   P->prec = prec;
   P->lanes = ff == FF_TERSOFF ? 1 : lanes;
-  P->variant = variant ? 1 : 0;
+  P->variant = (variant >= 0 && variant <= 3) ? variant : 1;
   P->chunk = chunk_steps;
   int rc = grow_systems(ctx, std::max((int)ctx->sys.size(), 0) + max_systems + 1);
   P->scap = ctx->scap;
@@ -2245,6 +2292,8 @@ int gemsgpu_pool_set(gemsgpu_pool* P, const int* sys, int nsys) {
   for (int s : ss) {
     CHK(check_sys(ctx, s));
     if (s >= P->scap) return fail(ctx, GEMSGPU_ERR_FULL, "system id beyond the pool's capacity");
+    if ((P->variant & 1) == 0 && ctx->sys[s].ntypes != 1)
+      return fail(ctx, GEMSGPU_ERR_STATE, "pool variant %d needs single-species systems", P->variant);
     atoms += ctx->sys[s].n;
   }
   if (atoms > P->max_atoms) return fail(ctx, GEMSGPU_ERR_FULL, "pool_set: %lld atoms > capacity", (long long)atoms);
@@ -2473,13 +2522,12 @@ int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms) {
   CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / K, 0, &m));
   cudaEvent_t ev[6];
   for (auto& e : ev) CU(cudaEventCreate(&e));
-  const bool regs = h.ntypes == 1 && h.variant == 0;
   auto first_kernel = [&]() {
-    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 0, h.d.prec, regs, K, m);
+    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 0, h.d.prec, h.variant, h.ntypes == 1, K, m);
     else launch_forces(ctx, ss);
   };
   auto second_kernel = [&]() {
-    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 1, h.d.prec, regs, K, m);
+    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 1, h.d.prec, h.variant, h.ntypes == 1, K, m);
   };
   first_kernel();
   second_kernel();

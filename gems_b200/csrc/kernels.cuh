@@ -824,8 +824,10 @@ __device__ __forceinline__ const SmF32* smf_table(const Arena& A, const SysDev& 
   return sh;
 }
 
-template <int K, bool ONE>
-__global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) {
+// MINB > 1 asks the compiler to fit MINB blocks per SM (fewer registers,
+// more warps to hide gather latency); the autotuner tries both.
+template <int K, bool ONE, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
@@ -885,8 +887,8 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_mixed(Arena A, BlockMap M) 
   }
 }
 
-template <int K, bool ONE>
-__global__ void __launch_bounds__(BLOCK) k_smatb_force_mixed(Arena A, BlockMap M) {
+template <int K, bool ONE, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];

@@ -73,6 +73,7 @@ _SIGS = {
     "gemsgpu_get_stream": (_i, [_p, ctypes.POINTER(_p)]),
     "gemsgpu_autotune": (_i, [_p, _i, _i, _ip, _ip, _dp]),
     "gemsgpu_set_lanes": (_i, [_p, _i, _i, _i]),
+    "gemsgpu_batch_autotune": (_i, [_p, _ip, _i, _i, _ip, _ip, _dp]),
     "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
     "gemsgpu_pool_create": (_i, [_p, _i, _l, _l, _i, _i, _i, _i, _i, ctypes.POINTER(_p)]),
     "gemsgpu_pool_destroy": (_i, [_p]),
@@ -186,6 +187,16 @@ class Context:
                                                   int(seed), _ptr(u), ctypes.byref(acc)))
         by_id = {s.sid: s for s in systems_of_temp}
         return [by_id[int(k)] for k in ids], acc.value
+
+    def batch_autotune(self, systems, reps=10):
+        """One force-kernel launch shape for systems launched together."""
+        ids = self._ids(systems)
+        k, v, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self.check(lib().gemsgpu_batch_autotune(self.h, _ptr(ids, ctypes.c_int), len(ids), int(reps),
+                                                ctypes.byref(k), ctypes.byref(v), ctypes.byref(ms)))
+        for s in systems:
+            s.tuned = (k.value, v.value, ms.value)
+        return k.value, v.value, ms.value
 
     def launches(self):
         v = ctypes.c_int64()
