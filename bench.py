@@ -67,6 +67,16 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(value, dist, device=None):
+    """The largest value over all ranks (timings are the slowest rank's)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------- clocks
 class Clocks:
     """nvidia-smi samples of SM clock and throttle reasons during a region."""
@@ -584,38 +594,39 @@ def main():
     torch.cuda.synchronize()
     ck = clocks.stop()
     natoms = sum(s.n for s in reps)
-    tot_ms = sum(ts)
-    if dist:
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = max_over_ranks(sum(ts), dist, "cuda")
     value = world * natoms * blk * len(ts) / (tot_ms * 1e-3)
     arms["batched"] = {"value": natoms * blk * len(ts) / (sum(ts) * 1e-3), "ms_per_block": sum(ts) / len(ts),
                        "atoms": natoms, "replicas": len(reps), "launches": nl,
                        "lanes_variant": list(reps[0].tuned[:2])}
     # --- e2e through the C ABI with host buffers
     te, h2d, d2h = timed_e2e(ctx, torch, reps, blk, args.steps, args.warmup, flush, ext)
-    e2e_ms = sum(te)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(sum(te), dist, "cuda")
     e2e = {"value": world * natoms * blk * len(te) / (e2e_ms * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
-    # --- roofline of the dominant kernel (mixed SMA-TB force pass)
-    nbar = 54.0
-    force_bytes = 16 + 4 + 8 + 4 * nbar + 32 + 8      # own int4, eband, band, list, force, epot
+    # --- roofline of the dominant kernel: the mixed SMA-TB force pass as the
+    # batched arm launches it (all replicas in one launch, its tuned shape)
+    nbar = 54.0   # list entries per atom (fcc shells within 6.0 A)
+    force_bytes = 16 + 4 + 8 + 4 * nbar + 32 + 8      # own int4, rho^-1/2, rho, list, force, epot
     rho_bytes = 16 + 4 * nbar + 8 + 8 + 4
     peak, peak_kind = measured_peaks()
-    n1 = mixed_sys.n
-    ach = force_bytes * n1 / (kern[1] * 1e-3) / 1e9
+    kb = ctx.batch_time_kernels(reps, 50)
+    ach = force_bytes * natoms / (kb[1] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f)["k_smatb_force_mixed"]["dram_bytes_per_atom"] * natoms
     roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": None, "kernel": "k_smatb_force_mixed", "peak_source": peak_kind,
-                "bytes_per_launch": force_bytes * n1, "ms_per_launch": kern[1],
-                "rho_kernel": {"ms_per_launch": kern[0], "bytes_per_launch": rho_bytes * n1},
-                "rebuild_ms": kern[2], "fp64_force_ms": kern64[1], "fp64_rho_ms": kern64[0],
-                "kernel_lanes_variant": list(mixed_sys.tuned[:2]),
-                "note": "working set is L2-resident (about 10 MB per replica)"}
+                "traffic": traffic, "kernel": "k_smatb_force_mixed", "peak_source": peak_kind,
+                "bytes_per_launch": force_bytes * natoms, "ms_per_launch": kb[1], "atoms_per_launch": natoms,
+                "launch_shape": list(reps[0].tuned[:2]),
+                "rho_kernel": {"ms_per_launch": kb[0], "bytes_per_launch": rho_bytes * natoms},
+                "rebuild_ms": kb[2],
+                "single_32k": {"mixed_force_ms": kern[1], "mixed_rho_ms": kern[0],
+                               "fp64_force_ms": kern64[1], "fp64_rho_ms": kern64[0]},
+                "note": "working set L2-resident (about 10 MB per replica); the kernel is bound by "
+                        "neighbour-gather latency, see profiles/smatb_mixed_batched_8x32k.txt"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_ms / len(ts), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",

@@ -2509,37 +2509,46 @@ int gemsgpu_get_launch_count(gemsgpu_ctx* ctx, int64_t* launches) {
   return 0;
 }
 
-int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms) {
-  CHK(check_sys(ctx, sys));
+static int time_kernels_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, double* out_ms) {
   if (reps <= 0 || !out_ms) return fail(ctx, GEMSGPU_ERR_ARG, "time_kernels: reps > 0, out_ms");
   cudaSetDevice(ctx->device);
-  SysHost& h = ctx->sys[sys];
-  if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "no force field");
-  std::vector<int> ss{sys};
-  if (h.first || h.pos_dirty || !h.has_forces) CHK(interact_group(ctx, ss, true));
+  const SysHost& h = ctx->sys[ss[0]];
+  for (int s : ss) {
+    const SysHost& q = ctx->sys[s];
+    if (q.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "no force field");
+    if (q.d.ff != h.d.ff || q.d.prec != h.d.prec || q.lanes != h.lanes || q.variant != h.variant)
+      return fail(ctx, GEMSGPU_ERR_ARG, "time_kernels: systems differ in force field or launch shape");
+  }
+  std::vector<int> need;
+  for (int s : ss)
+    if (ctx->sys[s].first || ctx->sys[s].pos_dirty || !ctx->sys[s].has_forces) need.push_back(s);
+  if (!need.empty()) CHK(interact_group(ctx, need, true));
   const int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
+  bool single = true;
+  for (int s : ss) single &= ctx->sys[s].ntypes == 1;
   BlockMap m;
   CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / K, 0, &m));
-  cudaEvent_t ev[6];
+  const int* sa;
+  CHK(sys_array(ctx, ss, &sa));
+  cudaEvent_t ev[4];
   for (auto& e : ev) CU(cudaEventCreate(&e));
   auto first_kernel = [&]() {
-    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 0, h.d.prec, h.variant, h.ntypes == 1, K, m);
+    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 0, h.d.prec, h.variant, single, K, m);
     else launch_forces(ctx, ss);
   };
   auto second_kernel = [&]() {
-    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 1, h.d.prec, h.variant, h.ntypes == 1, K, m);
+    if (h.d.ff == FF_SMATB) smatb_pass(ctx, 1, h.d.prec, h.variant, single, K, m);
   };
   first_kernel();
   second_kernel();
-  const int* sa;
-  CHK(sys_array(ctx, ss, &sa));
   CU(cudaEventRecord(ev[0], ctx->stream));
   for (int r = 0; r < reps; r++) first_kernel();
   CU(cudaEventRecord(ev[1], ctx->stream));
   for (int r = 0; r < reps; r++) second_kernel();
   CU(cudaEventRecord(ev[2], ctx->stream));
   for (int r = 0; r < reps; r++) {
-    k_force_rebuild<<<1, 256, 0, ctx->stream>>>(ctx->A, sa, 1);
+    k_force_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size());
+    ++ctx->launches;
     CHK(launch_rebuild(ctx, ss));
   }
   CU(cudaEventRecord(ev[3], ctx->stream));
@@ -2552,6 +2561,17 @@ int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms) {
   for (auto& e : ev) cudaEventDestroy(e);
   CU(cudaGetLastError());
   return 0;
+}
+
+int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms) {
+  CHK(check_sys(ctx, sys));
+  return time_kernels_set(ctx, {sys}, reps, out_ms);
+}
+
+int gemsgpu_batch_time_kernels(gemsgpu_ctx* ctx, const int* sys, int nsys, int reps, double* out_ms) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  return time_kernels_set(ctx, ss, reps, out_ms);
 }
 
 }  // extern "C"

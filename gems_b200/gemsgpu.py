@@ -74,6 +74,7 @@ _SIGS = {
     "gemsgpu_autotune": (_i, [_p, _i, _i, _ip, _ip, _dp]),
     "gemsgpu_set_lanes": (_i, [_p, _i, _i, _i]),
     "gemsgpu_batch_autotune": (_i, [_p, _ip, _i, _i, _ip, _ip, _dp]),
+    "gemsgpu_batch_time_kernels": (_i, [_p, _ip, _i, _i, _dp]),
     "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
     "gemsgpu_pool_create": (_i, [_p, _i, _l, _l, _i, _i, _i, _i, _i, ctypes.POINTER(_p)]),
     "gemsgpu_pool_destroy": (_i, [_p]),
@@ -197,6 +198,13 @@ class Context:
         for s in systems:
             s.tuned = (k.value, v.value, ms.value)
         return k.value, v.value, ms.value
+
+    def batch_time_kernels(self, systems, reps=20):
+        """Mean ms of (first force kernel, second, list rebuild) over the set."""
+        ids = self._ids(systems)
+        out = np.zeros(3)
+        self.check(lib().gemsgpu_batch_time_kernels(self.h, _ptr(ids, ctypes.c_int), len(ids), int(reps), _ptr(out)))
+        return out
 
     def launches(self):
         v = ctypes.c_int64()

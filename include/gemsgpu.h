@@ -341,6 +341,9 @@ int gemsgpu_get_launch_count(gemsgpu_ctx* ctx, int64_t* launches);
  * the second (force pass; 0 if none), out_ms[2] = mean list rebuild time.
  * Replaces timer_dump's per-step wall time (src/Errors.f90:128-172). */
 int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms);
+/* The same for nsys systems launched together (one launch shape). */
+int gemsgpu_batch_time_kernels(gemsgpu_ctx* ctx, const int* sys, int nsys,
+                               int reps, double* out_ms);
 
 #ifdef __cplusplus
 }
