@@ -2497,6 +2497,95 @@ int gemsgpu_server_forget(gemsgpu_server* S, int64_t id) {
   return 0;
 }
 
+// ------------------------------------------------------------ checkpoints
+// write_chp / read_chp (src/Checkpoint.F90:154-244): the per-system state a
+// run resumes from -- positions, velocities, accelerations (GEMS layout), the
+// Ermak/Philox step counter, the FIRE state and the rebuild count.  Resuming
+// forces a neighbour rebuild, as the reference's interact does after
+// read_chp (src/Checkpoint.F90:232-241).
+namespace {
+struct ChpHeader {
+  char magic[8];
+  int32_t version, n, ff, integ;
+  uint64_t step;
+  int64_t nupd;
+  double fire_dt, fire_alpha;
+  int32_t fire_np, fire_done, fire_iter, fire_zero;
+};
+}  // namespace
+
+int gemsgpu_checkpoint_size(gemsgpu_ctx* ctx, int sys, size_t* bytes) {
+  CHK(check_sys(ctx, sys));
+  if (!bytes) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_size: NULL");
+  *bytes = sizeof(ChpHeader) + 9 * sizeof(double) * (size_t)ctx->sys[sys].n;
+  return 0;
+}
+
+int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes) {
+  size_t need = 0;
+  CHK(gemsgpu_checkpoint_size(ctx, sys, &need));
+  if (!buf || bytes < need) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_save: buffer of %zu bytes needed", need);
+  const SysHost& h = ctx->sys[sys];
+  CHK(read_states(ctx));
+  const SysState& st = ctx->h_st[sys];
+  ChpHeader hd{};
+  memcpy(hd.magic, "GEMSGPU", 8);
+  hd.version = 1;
+  hd.n = h.n;
+  hd.ff = h.d.ff;
+  hd.integ = h.d.integ;
+  hd.step = st.step;
+  hd.nupd = st.nupd;
+  hd.fire_dt = st.fire_dt;
+  hd.fire_alpha = st.fire_alpha;
+  hd.fire_np = st.fire_np;
+  hd.fire_done = st.fire_done;
+  hd.fire_iter = st.fire_iter;
+  hd.fire_zero = st.fire_zero;
+  char* p = static_cast<char*>(buf);
+  memcpy(p, &hd, sizeof(hd));
+  double* x = reinterpret_cast<double*>(p + sizeof(hd));
+  CHK(get_d4(ctx, h, ctx->A.pos, x));
+  CHK(get_d4(ctx, h, ctx->A.vel, x + 3 * (size_t)h.n));
+  CHK(get_d4(ctx, h, ctx->A.acel, x + 6 * (size_t)h.n));
+  return 0;
+}
+
+int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t bytes) {
+  size_t need = 0;
+  CHK(gemsgpu_checkpoint_size(ctx, sys, &need));
+  if (!buf || bytes < need) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %zu bytes expected", need);
+  SysHost& h = ctx->sys[sys];
+  ChpHeader hd;
+  memcpy(&hd, buf, sizeof(hd));
+  if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || hd.version != 1)
+    return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: not a checkpoint of this library");
+  if (hd.n != h.n) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %d atoms, system has %d", hd.n, h.n);
+  const double* x = reinterpret_cast<const double*>(static_cast<const char*>(buf) + sizeof(hd));
+  CHK(h2d_xyz(ctx, x, ctx->A.pos + h.off, h.n));
+  CHK(h2d_xyz(ctx, x + 3 * (size_t)h.n, ctx->A.vel + h.off, h.n));
+  CHK(h2d_xyz(ctx, x + 6 * (size_t)h.n, ctx->A.acel + h.off, h.n));
+  CHK(read_states(ctx));
+  SysState st = ctx->h_st[sys];
+  st.step = hd.step;
+  st.nupd = hd.nupd;
+  st.fire_dt = hd.fire_dt;
+  st.fire_alpha = hd.fire_alpha;
+  st.fire_np = hd.fire_np;
+  st.fire_done = hd.fire_done;
+  st.fire_iter = hd.fire_iter;
+  st.fire_zero = hd.fire_zero;
+  st.status = 0;
+  CU(cudaMemcpyAsync(ctx->A.st + sys, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+  BlockMap m;
+  CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
+  k_refresh_fx<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  CU(cudaStreamSynchronize(ctx->stream));
+  h.first = true;        // the resumed interact rebuilds the list
+  h.has_forces = false;
+  return 0;
+}
+
 int gemsgpu_get_stream(gemsgpu_ctx* ctx, void** stream) {
   if (!ctx || !stream) return GEMSGPU_ERR_ARG;
   *stream = (void*)ctx->stream;

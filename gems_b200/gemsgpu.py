@@ -75,6 +75,9 @@ _SIGS = {
     "gemsgpu_set_lanes": (_i, [_p, _i, _i, _i]),
     "gemsgpu_batch_autotune": (_i, [_p, _ip, _i, _i, _ip, _ip, _dp]),
     "gemsgpu_batch_time_kernels": (_i, [_p, _ip, _i, _i, _dp]),
+    "gemsgpu_checkpoint_size": (_i, [_p, _i, ctypes.POINTER(ctypes.c_size_t)]),
+    "gemsgpu_checkpoint_save": (_i, [_p, _i, _p, ctypes.c_size_t]),
+    "gemsgpu_checkpoint_load": (_i, [_p, _i, _p, ctypes.c_size_t]),
     "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
     "gemsgpu_pool_create": (_i, [_p, _i, _l, _l, _i, _i, _i, _i, _i, ctypes.POINTER(_p)]),
     "gemsgpu_pool_destroy": (_i, [_p]),
@@ -409,6 +412,19 @@ class System:
         out = np.zeros(3)
         self._c(lib().gemsgpu_time_kernels(self.ctx.h, self.sid, int(reps), _ptr(out)))
         return out
+
+    def checkpoint(self):
+        """write_chp: the system's resumable state as bytes."""
+        n = ctypes.c_size_t()
+        self._c(lib().gemsgpu_checkpoint_size(self.ctx.h, self.sid, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        self._c(lib().gemsgpu_checkpoint_save(self.ctx.h, self.sid, buf, n.value))
+        return buf.raw
+
+    def restore(self, data):
+        """read_chp: resume from checkpoint bytes (the next interact rebuilds the list)."""
+        buf = ctypes.create_string_buffer(data, len(data))
+        self._c(lib().gemsgpu_checkpoint_load(self.ctx.h, self.sid, buf, len(data)))
 
     def fmax(self):
         v = ctypes.c_double()

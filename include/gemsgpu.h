@@ -216,6 +216,20 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys,
 int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys,
                          double* epot_ev, double* ekin_ev, double* temp);
 
+/* ------------------------------------------------------------ checkpoints */
+
+/* Per-system checkpoint (write_chp / read_chp, src/Checkpoint.F90:154-244):
+ * positions, velocities and accelerations in the GEMS layout plus the
+ * integrator state (Philox step counter, FIRE dt/alpha/counters) and the
+ * rebuild count, in a caller-owned host buffer of gemsgpu_checkpoint_size
+ * bytes.  Loading into a system of the same size restores that state; the
+ * next interact rebuilds the neighbour list, as the reference's does after
+ * read_chp. */
+int gemsgpu_checkpoint_size(gemsgpu_ctx* ctx, int sys, size_t* bytes);
+int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes);
+int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf,
+                            size_t bytes);
+
 /* ------------------------------------------------------------ pools */
 
 /* A pool runs a changing set of systems (one force-field kind and precision)
