@@ -161,6 +161,48 @@ def make_system(gems, ctx, w, prec, seed, tune=None):
     return s
 
 
+def smatb_pair_stats(s, L, rci, rce):
+    """List entries, pairs with r <= rci and pairs with rci < r <= rce of one
+    periodic system at its current positions (minimum image)."""
+    nn, lst = s.neighbour_list()
+    x = s.pos
+    i = np.repeat(np.arange(s.n), nn)
+    j = np.concatenate([lst[:c, a] for a, c in enumerate(nn)]).astype(np.int64)
+    d = x[j] - x[i]
+    Lv = np.asarray(L, dtype=np.float64)
+    d -= Lv * np.round(d / Lv)
+    r = np.sqrt((d * d).sum(1))
+    return {"entries": int(nn.sum()), "inner": int((r <= rci).sum()),
+            "tail": int(((r > rci) & (r <= rce)).sum())}
+
+
+def smatb_compute_counts(st):
+    """Algorithmic FP32 flops (FMA = 2) and MUFU operations of the two mixed
+    SMA-TB passes for the pair statistics `st`:
+      every list entry: pair vector and r^2 (8 flops);
+      density, r <= rci: rsqrt + Newton (4), exp argument and scale (3), sum (1); 2 MUFU
+      density, tail:      rsqrt + Newton (4), quintic and square (8), sum (1);    1 MUFU
+      force,   r <= rci: rsqrt + Newton (4), eband sum (1), two exps and factor (8),
+                         force and energy sums (9);                                3 MUFU
+      force,   tail:      rsqrt + Newton (4), eband sum (1), three polynomials and
+                         factor (34), force and energy sums (9);                   1 MUFU"""
+    e, a, b = st["entries"], st["inner"], st["tail"]
+    rho = {"flops": 8 * e + 8 * a + 13 * b, "mufu": 2 * a + b}
+    force = {"flops": 8 * e + 22 * a + 48 * b, "mufu": 3 * a + b}
+    return rho, force
+
+
+def compute_roof(counts, bytes_, ms, peaks, hbm):
+    """Time each roof allows for one launch, and the fraction of the binding one."""
+    t = {"hbm_us": bytes_ / (hbm * 1e9) * 1e6,
+         "fp32_us": counts["flops"] / (peaks["fp32_tflops"] * 1e12) * 1e6,
+         "mufu_us": counts["mufu"] / (peaks["ex2_gops"] * 1e9) * 1e6}
+    bind = max(t, key=t.get)
+    return {"flops_per_launch": counts["flops"], "mufu_per_launch": counts["mufu"],
+            "roof_times_us": t, "binding": bind.replace("_us", ""), "measured_us": ms * 1e3,
+            "frac_of_binding_roof": t[bind] / (ms * 1e3)}
+
+
 def timed_blocks(ctx, torch, systems, block, steps, warmup, flush, ext_stream):
     """Run warmup + steps blocks of `block` MD steps; returns (ms list, launches)."""
     for _ in range(warmup):
@@ -255,6 +297,81 @@ def cpu_baseline(seconds):
             break
     return {"value": s.n * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": "%d MD steps of the 32000-atom SMA-TB Ermak workload (FP64 OpenMP restatement)" % steps}
+
+
+def _cpu_steps(s, seconds):
+    """Step an oracle system (stepa, interact, stepb) for about `seconds`."""
+    s.interact()
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        s.stepa()
+        s.interact()
+        s.stepb()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and steps >= 3:
+            return steps, el
+
+
+def cpu_baseline_c1(seconds):
+    from oracle import oracle as O
+    from gems_b200 import workloads as W
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    w = W.lj_fluid()
+    s = O.System(w["pos"], 1.0)
+    s.set_vel(w["vel"])
+    s.set_box(w["L"], (True, True, True))
+    e, sg, rc, sh = w["lj"]
+    s.set_lj(e, sg, rc, eshift=sh)
+    s.set_skin(w["skin"])
+    s.set_vv(w["dt"])
+    steps, el = _cpu_steps(s, seconds)
+    return {"value": s.n * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d VV steps of the 4000-atom LJ fluid (FP64 OpenMP restatement)" % steps}
+
+
+def cpu_baseline_c5(seconds):
+    from oracle import oracle as O
+    from gems_b200 import workloads as W
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    w = W.tersoff_si()
+    s = O.System(w["pos"], w["mass"])
+    s.set_vel(w["vel"])
+    s.set_box(w["L"], (True, True, True))
+    s.set_tersoff(w["tersoff"])
+    s.set_skin(w["skin"])
+    s.set_vv(w["dt"])
+    steps, el = _cpu_steps(s, seconds)
+    return {"value": s.n * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d VV steps of the 1,000,000-atom Tersoff Si crystal (FP64 OpenMP restatement)" % steps}
+
+
+def cpu_baseline_c3(seconds):
+    """FIRE relaxations of the batch's first clusters, one after another."""
+    from oracle import oracle as O
+    from gems_b200 import workloads as W
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    sm, m = W.SMATB["Au"], W.MASS["Au"]
+    clusters = W.batched_clusters()
+    t0 = time.perf_counter()
+    work, done = 0.0, 0
+    for p in clusters[:64]:
+        s = O.System(p, m)
+        s.set_smatb(*sm)
+        s.set_fire(0.002, 0.02)
+        it, _ = s.fire_relax(1e-3, 5000)
+        work += it * s.n
+        done += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": work / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "FIRE to 1e-3 eV/A of the first %d clusters of the batch, one after another "
+                      "(FP64 OpenMP restatement)" % done}
 
 
 def run_reference(args):
@@ -361,7 +478,8 @@ def run_c1(args, gems, torch, ctx, ext):
             g.destroy()
     _line("atom-steps/s (LJ fluid 4000, NVE VV)", out["batched"]["value"], UNIT, args,
           {"workload": "lj_fluid_4000 (fcc 10^3, rho*=0.8442, T*=0.72, rc 2.5 shifted, skin 0.3)",
-           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out)
+           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out,
+          **({} if args.no_cpu else {"cpu_baseline": cpu_baseline_c1(args.cpu_seconds)}))
 
 
 def run_c5(args, gems, torch, ctx, ext):
@@ -388,7 +506,8 @@ def run_c5(args, gems, torch, ctx, ext):
         g.destroy()
     _line("atom-steps/s (Tersoff Si 1M, NVE VV)", out["mixed"]["value"], UNIT, args,
           {"workload": "tersoff_si_1000000 (diamond 50^3, a=5.431, 1000 K, dt 1 fs, skin 1.0)",
-           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out)
+           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out,
+          **({} if args.no_cpu else {"cpu_baseline": cpu_baseline_c5(args.cpu_seconds)}))
 
 
 def run_c3(args, gems, torch, ctx, ext):
@@ -452,7 +571,8 @@ def run_c3(args, gems, torch, ctx, ext):
     _line("atom-steps/s (1024 Au clusters FIRE + 64-replica exchange, batched)", fire["atom_steps_per_s"], UNIT,
           args, {"workload": "1024 Au clusters 13-2000 atoms (log-uniform, seed 3), FIRE to 1e-3 eV/A cap 5000; "
                              "64 x 147-atom replicas 200-900 K, swaps every 500 steps"},
-          dtype="f32+f64acc", fire=fire, replica_exchange=rex)
+          dtype="f32+f64acc", fire=fire, replica_exchange=rex,
+          **({} if args.no_cpu else {"cpu_baseline": cpu_baseline_c3(args.cpu_seconds)}))
 
 
 def run_c4(args, gems, torch, ctx, ext):
@@ -617,12 +737,22 @@ def main():
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f)["k_smatb_force_mixed"]["dram_bytes_per_atom"] * natoms
+    # compute roofs: measured FP32 / MUFU issue rates against the algorithmic
+    # flop and MUFU counts of the same launch
+    peaks = gems.measure_peaks(dev)
+    sm = c2_replica(2)["smatb"]
+    pst = [smatb_pair_stats(r_, c2_replica(2)["L"], sm[5], sm[6]) for r_ in reps]
+    tot = {k: sum(p_[k] for p_ in pst) for k in pst[0]}
+    c_rho, c_force = smatb_compute_counts(tot)
+    roofs = {"peaks": peaks, "pairs_per_launch": tot,
+             "force": compute_roof(c_force, force_bytes * natoms, kb[1], peaks, peak),
+             "rho": compute_roof(c_rho, rho_bytes * natoms, kb[0], peaks, peak)}
     roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "traffic": traffic, "kernel": "k_smatb_force_mixed", "peak_source": peak_kind,
                 "bytes_per_launch": force_bytes * natoms, "ms_per_launch": kb[1], "atoms_per_launch": natoms,
                 "launch_shape": list(reps[0].tuned[:2]),
                 "rho_kernel": {"ms_per_launch": kb[0], "bytes_per_launch": rho_bytes * natoms},
-                "rebuild_ms": kb[2],
+                "rebuild_ms": kb[2], "compute_roofs": roofs,
                 "single_32k": {"mixed_force_ms": kern[1], "mixed_rho_ms": kern[0],
                                "fp64_force_ms": kern64[1], "fp64_rho_ms": kern64[0]},
                 "note": "working set L2-resident (about 10 MB per replica); the kernel is bound by "

@@ -9,9 +9,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRCS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu")]
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu", "peaks.cu")]
 OUT = os.path.join(HERE, "libgemsgpu.so")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu", "kernels.cuh", "common.cuh")] + [
+DEPS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu", "peaks.cu", "kernels.cuh",
+                                                             "common.cuh")] + [
     os.path.join(os.path.dirname(HERE), "include", "gemsgpu.h")]
 
 NVCC_FLAGS = [

@@ -668,6 +668,27 @@ int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss,
   return 0;
 }
 
+int launch_step_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss,
+                   cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
+  BlockMap ma;
+  CHK(get_map(ctx, ss, BLOCK, 0, &ma));
+  if (use_cond) k_step_ba<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  else k_step_ba<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  ++ctx->launches;
+  CU(cudaGetLastError());
+  return 0;
+}
+
+// step_b of one step and step_a of the next fuse into one kernel when every
+// system integrates with velocity Verlet or Ermak
+bool can_fuse_steps(const gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  for (int s : ss) {
+    const int it = ctx->sys[s].d.integ;
+    if (it != IT_VV && it != IT_ERMAK) return false;
+  }
+  return true;
+}
+
 int launch_step_b(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
@@ -793,18 +814,26 @@ int reduce_sys(gemsgpu_ctx* ctx, const std::vector<int>& ss, std::vector<double>
 }
 
 // one captured MD step for a set of systems
-int record_step(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
-  CHK(launch_step_a(ctx, ss));
-  CHK(launch_rebuild(ctx, ss));
-  CHK(launch_forces(ctx, ss));
-  CHK(launch_step_b(ctx, ss));
+// n plain steps; with fusion, step k > 0 opens with step_b(k-1)+step_a(k)
+// and only the last step closes with its own step_b
+int record_steps(gemsgpu_ctx* ctx, const std::vector<int>& ss, int n) {
+  const bool fuse = can_fuse_steps(ctx, ss);
+  for (int k = 0; k < n; k++) {
+    if (k == 0 || !fuse) CHK(launch_step_a(ctx, ss));
+    else CHK(launch_step_ba(ctx, ss));
+    CHK(launch_rebuild(ctx, ss));
+    CHK(launch_forces(ctx, ss));
+    if (!fuse || k == n - 1) CHK(launch_step_b(ctx, ss));
+  }
   return 0;
 }
 
 // Capture `nsteps` MD steps into one graph.  Each step is
 //   [step_a] -> IF(rebuild needed) { rebuild chain } -> [forces, step_b]
 // where the IF node's handle is raised by k_step_a; the rebuild kernels
-// therefore cost nothing on steps that keep their list.
+// therefore cost nothing on steps that keep their list.  For velocity
+// Verlet and Ermak systems step_b and the next step_a are one kernel:
+//   [step_a] IF [forces] ([step_ba] IF [forces])... [step_b]
 int capture_into(gemsgpu_ctx* ctx, cudaGraph_t g, std::vector<cudaGraphNode_t>& deps,
                  int (*fn)(gemsgpu_ctx*, const std::vector<int>&, void*),
                  const std::vector<int>& ss, void* arg) {
@@ -833,6 +862,9 @@ struct CondArg {
 int cap_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
   return launch_step_a(ctx, ss, ((CondArg*)arg)->h, 1);
 }
+int cap_step_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
+  return launch_step_ba(ctx, ss, ((CondArg*)arg)->h, 1);
+}
 int cap_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
   const int64_t before = ctx->launches;
   int rc = launch_rebuild(ctx, ss, 1);
@@ -843,10 +875,11 @@ int cap_forces_b(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
   CHK(launch_forces(ctx, ss));
   return launch_step_b(ctx, ss);
 }
+int cap_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
+  return launch_forces(ctx, ss);
+}
 int cap_plain(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
-  int n = *(int*)arg;
-  for (int k = 0; k < n; k++) CHK(record_step(ctx, ss));
-  return 0;
+  return record_steps(ctx, ss, *(int*)arg);
 }
 
 int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGraph_t* out) {
@@ -855,13 +888,14 @@ int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, 
   std::vector<cudaGraphNode_t> deps;
   int rc = 0;
   bool cond_ok = ctx->use_cond;
+  const bool fuse = can_fuse_steps(ctx, ss);
   for (int k = 0; k < nsteps && rc == 0 && cond_ok; k++) {
     CondArg ca{};
     if (cudaGraphConditionalHandleCreate(&ca.h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
       cond_ok = false;
       break;
     }
-    rc = capture_into(ctx, g, deps, cap_step_a, ss, &ca);
+    rc = capture_into(ctx, g, deps, (k == 0 || !fuse) ? cap_step_a : cap_step_ba, ss, &ca);
     if (rc) break;
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
@@ -877,7 +911,7 @@ int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, 
     rc = capture_into(ctx, cp.conditional.phGraph_out[0], none, cap_rebuild, ss, nullptr);
     if (rc) break;
     deps.assign(1, cn);
-    rc = capture_into(ctx, g, deps, cap_forces_b, ss, nullptr);
+    rc = capture_into(ctx, g, deps, (fuse && k < nsteps - 1) ? cap_forces : cap_forces_b, ss, nullptr);
   }
   cudaGetLastError();
   if (rc == 0 && !cond_ok) {
@@ -1024,6 +1058,12 @@ int md_group(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps) {
     if (grow > 0) {
       if (++retries > 4) return fail(ctx, GEMSGPU_ERR_OVERFLOW, "neighbour list keeps overflowing");
       CHK(snapshot(ctx, true));
+      {
+        // the fixed-point copies were left at the undone chunk's positions
+        BlockMap mr;
+        CHK(get_map(ctx, ss, BLOCK, 0, &mr));
+        k_refresh_fx<<<mr.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, mr); ++ctx->launches;
+      }
       CHK(grow_list(ctx, grow + grow / 4 + 8));
       const int* sa;
       CHK(sys_array(ctx, ss, &sa));
@@ -1330,6 +1370,8 @@ int pool_chunk(gemsgpu_pool* P) {
     }
     if (!grow) return 0;
     CHK(snapshot(ctx, true));
+    // the fixed-point copies were left at the undone chunk's positions
+    k_refresh_fx<<<P->maps[0].nblk, BLOCK, 0, ctx->stream>>>(ctx->A, P->maps[0]); ++ctx->launches;
     CHK(grow_list(ctx, grow + grow / 4 + 8));
     if (list_smem(ctx->A.lcap) > 48 * 1024)
       CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -1252,6 +1252,110 @@ __global__ void k_zero_force(Arena A, BlockMap M) {
 }
 
 // ------------------------------------------------------------------ integrators
+// ---- per-atom integrator updates, shared by the split and fused kernels
+// velocity_verlet_b (src/Integration.F90:1171-1186)
+__device__ __forceinline__ void vv_b_atom(double dt, double om, const double4& F, double4& v, double4& a) {
+  const double adv = dt * 0.5;
+  a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+  v.x = v.x + adv * a.x;
+  v.y = v.y + adv * a.y;
+  v.z = v.z + adv * a.z;
+}
+
+// ermak_b (src/Integration.F90:1013-1031)
+__device__ __forceinline__ void ermak_b_atom(const SysDev& S, double om, const double4& F, const double4& vv,
+                                             double4& v, double4& a) {
+  const double c12 = S.cc1 - S.cc2;
+  v.x = S.cc0 * v.x + c12 * a.x + S.cc2 * F.x * om + vv.x;
+  v.y = S.cc0 * v.y + c12 * a.y + S.cc2 * F.y * om + vv.y;
+  v.z = S.cc0 * v.z + c12 * a.z + S.cc2 * F.z * om + vv.z;
+  a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+}
+
+// velocity_verlet_a (src/Integration.F90:1150-1168)
+__device__ __forceinline__ void vv_a_atom(double dt, double om, const double4& F, double4& x, double4& v,
+                                          double4& a) {
+  const double adv = dt * 0.5, adx = adv * dt;
+  a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+  x.x = x.x + dt * v.x + adx * a.x;
+  x.y = x.y + dt * v.y + adx * a.y;
+  x.z = x.z + dt * v.z + adx * a.z;
+  v.x = v.x + adv * a.x;
+  v.y = v.y + adv * a.y;
+  v.z = v.z + adv * a.z;
+}
+
+// ermak_a (src/Integration.F90:963-1011): position update and the velocity
+// kick vel_v that ermak_b adds
+__device__ __forceinline__ void ermak_a_atom(const Arena& A, const SysDev& S, const SysState& st, int i,
+                                             double2 mi, const double4& v, const double4& a, double4& x,
+                                             double4& vv) {
+  double r[6];
+  if (S.use_ext_normals) {
+#pragma unroll
+    for (int k = 0; k < 6; k++) r[k] = A.ext_normals[(size_t)6 * i + k];
+  } else {
+    normals6((uint32_t)(i - S.off), st.step, S.seed, r);
+  }
+  const double f_lan = S.skt * mi.y;
+  const double pr = f_lan * S.sdr, pv = f_lan * S.sdv;
+  vv.x = pv * (S.crv1 * r[0] + S.crv2 * r[1]);
+  vv.y = pv * (S.crv1 * r[2] + S.crv2 * r[3]);
+  vv.z = pv * (S.crv1 * r[4] + S.crv2 * r[5]);
+  vv.w = 0.0;
+  const double c2dt = S.cc2 * S.dt;
+  x.x = x.x + S.cc1 * v.x + c2dt * a.x + pr * r[0];
+  x.y = x.y + S.cc1 * v.y + c2dt * a.y + pr * r[2];
+  x.z = x.z + S.cc1 * v.z + c2dt * a.z + pr * r[4];
+}
+
+// do_pbc_1 (src/Set_Properties.f90:444-470): a single wrap into [0, box)
+__device__ __forceinline__ void wrap_atom(const SysDev& S, double4& x) {
+  if (S.boxed) {
+    if (S.pbc[0]) { if (x.x >= S.L[0]) x.x = x.x - S.L[0]; else if (x.x < 0.0) x.x = x.x + S.L[0]; }
+    if (S.pbc[1]) { if (x.y >= S.L[1]) x.y = x.y - S.L[1]; else if (x.y < 0.0) x.y = x.y + S.L[1]; }
+    if (S.pbc[2]) { if (x.z >= S.L[2]) x.z = x.z - S.L[2]; else if (x.z < 0.0) x.z = x.z + S.L[2]; }
+  }
+}
+
+// the moved atom's outputs: position, fixed-point copy, skin displacement
+__device__ __forceinline__ double moved_atom(Arena& A, const SysDev& S, SysState& st, int i, const double4& x) {
+  A.pos[i] = x;
+  if (S.prec == PREC_MIXED || S.ff == FF_TERSOFF) {
+    int bad = 0;
+    write_fx(A, S, i, x, A.type[i], bad);
+    if (bad) atomicOr(&st.status, ST_LOST);
+  }
+  double d = disp2(S, x, A.pos_old[i]);
+  if (!(d == d)) atomicOr(&st.status, ST_NAN);
+  return d;
+}
+
+// test_update (src/Neighbour.F90:1305-1346) over the system: block top-2 of
+// the squared displacements, merged by the system's last block, which sets
+// the rebuild flag (and raises the graph's rebuild condition) and closes
+// the step's integrator bookkeeping.
+template <bool COND>
+__device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, const SysDev& S, SysState& st,
+                                           bool frozen, double2 t, cudaGraphConditionalHandle cond) {
+  t = block_top2(t);
+  if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
+  if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
+    double2 w = sys_top2(A, M, s);
+    if (threadIdx.x == 0) {
+      int rb = __dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)) > S.skin;
+      if (frozen) rb = 0;
+      st.rebuild = rb;
+      if (rb) {
+        atomicOr(A.any_rebuild, 1);
+        if constexpr (COND) cudaGraphSetConditional(cond, 1u);
+      }
+      if (S.integ == IT_ERMAK && !S.use_ext_normals) st.step++;
+      if (S.integ == IT_FIRE) st.fire_zero = 0;
+    }
+  }
+}
+
 // integration_stepa (src/Integration.F90:243-262): the algorithm's half
 // step, do_pbc (Set_Properties.f90:444-470), then the displacement test of
 // test_update fused in (the list decision for this step's interact).
@@ -1274,73 +1378,55 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
     double4 x = A.pos[i], v = A.vel[i], a = A.acel[i];
     const double2 mi = A.minv[i];
     if (S.integ == IT_VV || S.integ == IT_FIRE) {
-      // velocity_verlet_a (Integration.F90:1150-1168)
       const double dt = S.integ == IT_FIRE ? st.fire_dt : S.dt;
       if (S.integ == IT_FIRE && st.fire_zero) v = make_double4(0, 0, 0, 0);
-      const double4 F = A.force[i];
-      const double adv = dt * 0.5, adx = adv * dt;
-      a.x = F.x * mi.x; a.y = F.y * mi.x; a.z = F.z * mi.x;
-      x.x = x.x + dt * v.x + adx * a.x;
-      x.y = x.y + dt * v.y + adx * a.y;
-      x.z = x.z + dt * v.z + adx * a.z;
-      v.x = v.x + adv * a.x;
-      v.y = v.y + adv * a.y;
-      v.z = v.z + adv * a.z;
+      vv_a_atom(dt, mi.x, A.force[i], x, v, a);
       A.acel[i] = a;
+      A.vel[i] = v;
     } else if (S.integ == IT_ERMAK) {
-      // ermak_a (Integration.F90:963-1011)
-      double r[6];
-      if (S.use_ext_normals) {
-#pragma unroll
-        for (int k = 0; k < 6; k++) r[k] = A.ext_normals[(size_t)6 * i + k];
-      } else {
-        normals6((uint32_t)(i - S.off), st.step, S.seed, r);
-      }
-      const double f_lan = S.skt * mi.y;
-      const double pr = f_lan * S.sdr, pv = f_lan * S.sdv;
       double4 vv;
-      vv.x = pv * (S.crv1 * r[0] + S.crv2 * r[1]);
-      vv.y = pv * (S.crv1 * r[2] + S.crv2 * r[3]);
-      vv.z = pv * (S.crv1 * r[4] + S.crv2 * r[5]);
-      vv.w = 0.0;
-      const double c2dt = S.cc2 * S.dt;
-      x.x = x.x + S.cc1 * v.x + c2dt * a.x + pr * r[0];
-      x.y = x.y + S.cc1 * v.y + c2dt * a.y + pr * r[2];
-      x.z = x.z + S.cc1 * v.z + c2dt * a.z + pr * r[4];
+      ermak_a_atom(A, S, st, i, mi, v, a, x, vv);
       A.vel_v[i] = vv;
     }
-    // do_pbc_1: a single wrap into [0, box)
-    if (S.boxed) {
-      if (S.pbc[0]) { if (x.x >= S.L[0]) x.x = x.x - S.L[0]; else if (x.x < 0.0) x.x = x.x + S.L[0]; }
-      if (S.pbc[1]) { if (x.y >= S.L[1]) x.y = x.y - S.L[1]; else if (x.y < 0.0) x.y = x.y + S.L[1]; }
-      if (S.pbc[2]) { if (x.z >= S.L[2]) x.z = x.z - S.L[2]; else if (x.z < 0.0) x.z = x.z + S.L[2]; }
+    wrap_atom(S, x);
+    t.x = moved_atom(A, S, st, i, x);
+  }
+  skin_close<COND>(A, M, s, S, st, frozen, t, cond);
+}
+
+// step_b of one step fused with step_a of the next, for velocity Verlet and
+// Ermak systems (FIRE needs its system-wide P between the two and keeps the
+// split kernels).  Per atom it is exactly k_step_b followed by k_step_a:
+// the same operations in the same order, with each array read and written
+// once instead of twice.
+template <bool COND>
+__global__ void __launch_bounds__(BLOCK) k_step_ba(Arena A, BlockMap M, cudaGraphConditionalHandle cond) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  const SysDev& S = A.sys[s];
+  SysState& st = A.st[s];
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  bool act = i < M.end[blockIdx.x];
+  double2 t = make_double2(1.e-16, 1.e-16);
+  if (act && (S.integ == IT_VV || S.integ == IT_ERMAK)) {
+    double4 x = A.pos[i], v = A.vel[i], a = A.acel[i];
+    const double4 F = A.force[i];
+    const double2 mi = A.minv[i];
+    if (S.integ == IT_VV) {
+      vv_b_atom(S.dt, mi.x, F, v, a);
+      vv_a_atom(S.dt, mi.x, F, x, v, a);
+    } else {
+      ermak_b_atom(S, mi.x, F, A.vel_v[i], v, a);
+      double4 vv;
+      ermak_a_atom(A, S, st, i, mi, v, a, x, vv);
+      A.vel_v[i] = vv;
     }
-    A.pos[i] = x;
+    A.acel[i] = a;
     A.vel[i] = v;
-    if (S.prec == PREC_MIXED || S.ff == FF_TERSOFF) {
-      int bad = 0;
-      write_fx(A, S, i, x, A.type[i], bad);
-      if (bad) atomicOr(&st.status, ST_LOST);
-    }
-    t.x = disp2(S, x, A.pos_old[i]);
-    if (!(t.x == t.x)) atomicOr(&st.status, ST_NAN);
+    wrap_atom(S, x);
+    t.x = moved_atom(A, S, st, i, x);
   }
-  t = block_top2(t);
-  if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
-  if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
-    double2 w = sys_top2(A, M, s);
-    if (threadIdx.x == 0) {
-      int rb = __dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)) > S.skin;
-      if (frozen) rb = 0;
-      st.rebuild = rb;
-      if (rb) {
-        atomicOr(A.any_rebuild, 1);
-        if constexpr (COND) cudaGraphSetConditional(cond, 1u);
-      }
-      if (S.integ == IT_ERMAK && !S.use_ext_normals) st.step++;
-      if (S.integ == IT_FIRE) st.fire_zero = 0;
-    }
-  }
+  skin_close<COND>(A, M, s, S, st, false, t, cond);
 }
 
 // integration_stepb (src/Integration.F90:264-301): velocity_verlet_b
@@ -1361,12 +1447,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
     const double4 F = A.force[i];
     const double om = A.minv[i].x;
     if (S.integ == IT_VV || S.integ == IT_FIRE) {
-      const double dt = S.integ == IT_FIRE ? st.fire_dt : S.dt;
-      const double adv = dt * 0.5;
-      a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
-      v.x = v.x + adv * a.x;
-      v.y = v.y + adv * a.y;
-      v.z = v.z + adv * a.z;
+      vv_b_atom(S.integ == IT_FIRE ? st.fire_dt : S.dt, om, F, v, a);
       if (S.integ == IT_FIRE) {
         P = v.x * F.x + v.y * F.y + v.z * F.z;
         double fn2 = F.x * F.x + F.y * F.y + F.z * F.z;
@@ -1380,12 +1461,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
         v.z = v.z * (1.0 - al) + mixf * F.z;
       }
     } else if (S.integ == IT_ERMAK) {
-      const double4 vv = A.vel_v[i];
-      const double c12 = S.cc1 - S.cc2;
-      v.x = S.cc0 * v.x + c12 * a.x + S.cc2 * F.x * om + vv.x;
-      v.y = S.cc0 * v.y + c12 * a.y + S.cc2 * F.y * om + vv.y;
-      v.z = S.cc0 * v.z + c12 * a.z + S.cc2 * F.z * om + vv.z;
-      a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+      ermak_b_atom(S, om, F, A.vel_v[i], v, a);
     }
     A.vel[i] = v;
     A.acel[i] = a;

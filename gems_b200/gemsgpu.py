@@ -75,6 +75,7 @@ _SIGS = {
     "gemsgpu_set_lanes": (_i, [_p, _i, _i, _i]),
     "gemsgpu_batch_autotune": (_i, [_p, _ip, _i, _i, _ip, _ip, _dp]),
     "gemsgpu_batch_time_kernels": (_i, [_p, _ip, _i, _i, _dp]),
+    "gemsgpu_measure_peaks": (_i, [_i, _dp]),
     "gemsgpu_checkpoint_size": (_i, [_p, _i, ctypes.POINTER(ctypes.c_size_t)]),
     "gemsgpu_checkpoint_save": (_i, [_p, _i, _p, ctypes.c_size_t]),
     "gemsgpu_checkpoint_load": (_i, [_p, _i, _p, ctypes.c_size_t]),
@@ -223,6 +224,16 @@ class Context:
 
 
 _default_ctx = None
+
+
+def measure_peaks(device=0):
+    """Measured FP32 / FP64 FMA TFLOP/s and MUFU ex2 / rsqrt Gop/s of one device."""
+    out = np.zeros(4)
+    rc = lib().gemsgpu_measure_peaks(int(device), _ptr(out))
+    if rc != 0:
+        raise GemsGpuError("measure_peaks failed (%d)" % rc)
+    return {"fp32_tflops": float(out[0]), "fp64_tflops": float(out[1]), "ex2_gops": float(out[2]),
+            "rsqrt_gops": float(out[3])}
 
 
 def default_context():

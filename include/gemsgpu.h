@@ -359,6 +359,12 @@ int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms);
 int gemsgpu_batch_time_kernels(gemsgpu_ctx* ctx, const int* sys, int nsys,
                                int reps, double* out_ms);
 
+/* Measured issue-rate roofs of the pipes the force kernels use, on one
+ * device: out[0] FP32 FMA TFLOP/s, out[1] FP64 FMA TFLOP/s, out[2] MUFU
+ * ex2 Gop/s, out[3] MUFU rsqrt Gop/s.  No counterpart in the reference: it
+ * gives the compute roofs that the kernels' achieved rates are set against. */
+int gemsgpu_measure_peaks(int device, double* out);
+
 #ifdef __cplusplus
 }
 #endif

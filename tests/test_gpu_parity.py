@@ -278,16 +278,25 @@ def test_gpu_nvt_plj_parity_stream(ctx):
 
 
 # ------------------------------------------------------------------ engine invariants
-def test_md_steps_equals_stepwise(ctx):
-    """The captured md_steps loop runs the same kernels as step_a/interact/step_b."""
+@pytest.mark.parametrize("integ", ["ermak", "vv"])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_md_steps_equals_stepwise(ctx, integ, prec):
+    """The captured md_steps loop (step_b and the next step_a fused into one
+    kernel) gives the trajectory of separate step_a / interact / step_b calls
+    bit for bit."""
     from gems_b200 import workloads as W
     w = W.smatb_bulk(ncell=8)
+    vel = W.maxwell(len(w["pos"]), w["mass"], 600.0, np.random.default_rng(3))
     sys = []
     for _ in range(2):
-        g = gems.System(w["pos"], w["mass"], ctx=ctx)
+        g = gems.System(w["pos"], w["mass"], ctx=ctx, vel=vel)
         g.set_box(w["L"], (True, True, True))
         g.set_smatb(*w["smatb"])
-        g.set_ermak(w["dt"], w["gamma"], w["temp"], seed=99)
+        g.set_precision(prec)
+        if integ == "ermak":
+            g.set_ermak(w["dt"], w["gamma"], w["temp"], seed=99)
+        else:
+            g.set_vv(w["dt"])
         g.interact()
         sys.append(g)
     sys[0].md_steps(120)
@@ -298,6 +307,8 @@ def test_md_steps_equals_stepwise(ctx):
     np.testing.assert_array_equal(sys[0].pos, sys[1].pos)
     np.testing.assert_array_equal(sys[0].vel, sys[1].vel)
     assert sys[0].nupd == sys[1].nupd
+    for g in sys:
+        g.destroy()
 
 
 def test_skin_modes_same_trajectory(ctx):
