@@ -126,6 +126,8 @@ struct Arena {
   double* eband;        // 1/sqrt(rho_i)
   float* ebandf;        // FP32 copy for the mixed kernels
   int4* fxp;            // fixed-point positions (x, y, z, type) for mixed
+  double4* pose;        // FP64 force pass: (x, y, z, 1/sqrt(rho)) from the density pass
+  int4* fxe;            // mixed force pass: (fixed-point x, y, z, bits of float 1/sqrt(rho))
   double2* minv;        // (1/m, 1/sqrt(m))
   double* mass;
   int* type;

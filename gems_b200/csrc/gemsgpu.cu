@@ -236,6 +236,8 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   CHK(dgrow(ctx, &A.eband, keep, nc));
   CHK(dgrow(ctx, &A.ebandf, keep, nc));
   CHK(dgrow(ctx, &A.fxp, keep, nc));
+  CHK(dgrow(ctx, &A.pose, keep, nc));
+  CHK(dgrow(ctx, &A.fxe, keep, nc));
   CHK(dgrow(ctx, &A.minv, keep, nc));
   CHK(dgrow(ctx, &A.mass, keep, nc));
   CHK(dgrow(ctx, &A.type, keep, nc));
@@ -533,20 +535,24 @@ int sys_array(gemsgpu_ctx* ctx, const std::vector<int>& ss, const int** out) {
 // ------------------------------------------------------------- launches
 // one SMA-TB pass (0: density, 1: force) for a block map of K lanes per atom.
 // variant bit 0: species constants in shared memory (1) or registers (0,
-// single species only); bit 1: register-capped build for more warps per SM.
+// single species only); bit 1: register-capped build for more warps per SM
+// (four 256-thread blocks); bit 2 with bit 1: the force pass capped at three
+// blocks instead (no spills, fewer warps).
 template <int K>
-void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, const BlockMap& m) {
+void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, bool tight3, const BlockMap& m) {
   cudaStream_t st = ctx->stream;
   const Arena& A = ctx->A;
   if (prec == PREC_MIXED) {
     if (pass == 0) {
-      if (regs && tight) k_smatb_rho_mixed<K, true, 5><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      if (regs && tight) k_smatb_rho_mixed<K, true, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else if (regs) k_smatb_rho_mixed<K, true, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
-      else if (tight) k_smatb_rho_mixed<K, false, 5><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else if (tight) k_smatb_rho_mixed<K, false, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else k_smatb_rho_mixed<K, false, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
     } else {
-      if (regs && tight) k_smatb_force_mixed<K, true, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      if (regs && tight && tight3) k_smatb_force_mixed<K, true, 3><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else if (regs && tight) k_smatb_force_mixed<K, true, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else if (regs) k_smatb_force_mixed<K, true, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else if (tight && tight3) k_smatb_force_mixed<K, false, 3><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else if (tight) k_smatb_force_mixed<K, false, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else k_smatb_force_mixed<K, false, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
     }
@@ -567,13 +573,14 @@ void lj_k(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
 void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, int K, const BlockMap& m) {
   const bool regs = single && (variant & 1) == 0;
   const bool tight = (variant & 2) != 0;
+  const bool tight3 = (variant & 4) != 0;
   switch (K) {
-    case 1: smatb_pass_k<1>(ctx, pass, prec, regs, tight, m); break;
-    case 2: smatb_pass_k<2>(ctx, pass, prec, regs, tight, m); break;
-    case 4: smatb_pass_k<4>(ctx, pass, prec, regs, tight, m); break;
-    case 8: smatb_pass_k<8>(ctx, pass, prec, regs, tight, m); break;
-    case 16: smatb_pass_k<16>(ctx, pass, prec, regs, tight, m); break;
-    default: smatb_pass_k<32>(ctx, pass, prec, regs, tight, m); break;
+    case 1: smatb_pass_k<1>(ctx, pass, prec, regs, tight, tight3, m); break;
+    case 2: smatb_pass_k<2>(ctx, pass, prec, regs, tight, tight3, m); break;
+    case 4: smatb_pass_k<4>(ctx, pass, prec, regs, tight, tight3, m); break;
+    case 8: smatb_pass_k<8>(ctx, pass, prec, regs, tight, tight3, m); break;
+    case 16: smatb_pass_k<16>(ctx, pass, prec, regs, tight, tight3, m); break;
+    default: smatb_pass_k<32>(ctx, pass, prec, regs, tight, tight3, m); break;
   }
 }
 
@@ -1451,7 +1458,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   drop_maps(ctx);
   Arena& A = ctx->A;
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.epot, A.band, A.eband,
-                  A.ebandf, A.fxp, A.minv, A.mass, A.type, A.nn, A.list, A.flist, A.cell_of, A.slot,
+                  A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->d_sys};
@@ -2138,9 +2145,11 @@ static int autotune_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, 
       cand.push_back({K, 1});
       if (h0.d.ff == FF_SMATB && h0.d.prec == PREC_MIXED) {
         cand.push_back({K, 3});
+        cand.push_back({K, 7});
         if (single) {
           cand.push_back({K, 0});
           cand.push_back({K, 2});
+          cand.push_back({K, 6});
         }
       }
     }
@@ -2197,7 +2206,8 @@ int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant) {
   CHK(check_sys(ctx, sys));
   if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
     return fail(ctx, GEMSGPU_ERR_ARG, "lanes must be a power of two <= 32");
-  if (variant < 0 || variant > 3) return fail(ctx, GEMSGPU_ERR_ARG, "variant must be 0..3");
+  if (variant < 0 || variant > 7 || variant == 4 || variant == 5)
+    return fail(ctx, GEMSGPU_ERR_ARG, "variant must be 0..3, 6 or 7");
   SysHost& h = ctx->sys[sys];
   if (h.d.ff != FF_TERSOFF) h.lanes = lanes;
   h.variant = variant;
@@ -2301,7 +2311,7 @@ int gemsgpu_pool_create(gemsgpu_ctx* ctx, int max_systems, int64_t max_atoms, in
   P->ff = ff;
   P->prec = prec;
   P->lanes = ff == FF_TERSOFF ? 1 : lanes;
-  P->variant = (variant >= 0 && variant <= 3) ? variant : 1;
+  P->variant = (variant >= 0 && variant <= 7 && variant != 4 && variant != 5) ? variant : 1;
   P->chunk = chunk_steps;
   int rc = grow_systems(ctx, std::max((int)ctx->sys.size(), 0) + max_systems + 1);
   P->scap = ctx->scap;

@@ -51,14 +51,17 @@ __host__ __device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
   return c;
 }
 
-// Box-Muller on two 32-bit uniforms: u1 in (0,1], u2 in [0,1).  FP32 is
-// ample for a Langevin kick (the kick is applied in FP64).
+// Box-Muller on two 32-bit uniforms: u1 in (0,1], u2 in [0,1).  The kick
+// needs normal variates, not correctly rounded ones, so the FP32 hardware
+// approximations serve (log2, sin, cos on the multi-function unit; the angle
+// 2 pi u2 - pi stays in [-pi, pi), where they are accurate, and the shift by
+// pi only flips both signs of a symmetric pair).  The kick is applied in FP64.
 __device__ __forceinline__ void bm_pair(uint32_t a, uint32_t b, double& n1, double& n2) {
   float u1 = ((float)(a >> 8) + 1.0f) * 5.9604644775390625e-8f;  // (0, 1]
   float u2 = (float)(b >> 8) * 5.9604644775390625e-8f;            // [0, 1)
-  float rr = sqrtf(-2.0f * logf(u1));
+  float rr = sqrtf(-2.0f * __logf(u1));
   float sn, cs;
-  sincospif(2.0f * u2, &sn, &cs);
+  __sincosf(fmaf(6.2831853071795865f, u2, -3.14159265358979f), &sn, &cs);
   n1 = (double)(rr * cs);
   n2 = (double)(rr * sn);
 }
@@ -198,13 +201,15 @@ __device__ __forceinline__ double disp2(const SysDev& S, double4 x, double4 q) {
   return __dadd_rn(__dadd_rn(__dmul_rn(v0, v0), __dmul_rn(v1, v1)), __dmul_rn(v2, v2));
 }
 
-// last block of a system in a launch: true in thread 0 of that block
+// last block of a system in a launch (the value is the same in every thread
+// of the block).  Thread 0 has written the block's partial result; its fence
+// orders that write before the ticket, so the last block sees every partial.
 __device__ __forceinline__ bool last_block(const BlockMap& M, SysState* st, int s,
                                            int* counter) {
   __shared__ int last;
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
+    __threadfence();
     int t = atomicAdd(counter, 1);
     last = (t == M.sys_nblk[s] - 1);
     if (last) *counter = 0;
@@ -623,16 +628,30 @@ __device__ __forceinline__ float lane_sumf(float v) {
 // gather latency, not arithmetic).
 constexpr int UNR = 4;
 
+// list slots m0, m0+K, ... (UNR of them) of atom i; slots past nn, and ids
+// outside the arena (never gather outside it), read as -1
+template <int K>
+__device__ __forceinline__ void list_group(const Arena& A, int i, int nn, int m0, int (&jj)[UNR]) {
+#pragma unroll
+  for (int u = 0; u < UNR; u++) {
+    int m = m0 + u * K;
+    int j = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;
+    jj[u] = (unsigned)j < (unsigned)A.cap ? j : -1;
+  }
+}
+
+// The indices of the next group are loaded while the current group is
+// gathered and computed, so a lane waits on one memory latency per group
+// instead of two (list load, then the gathers it feeds).
 #define PAIR_LOOP_BEGIN(GATHER_T, GATHER)                                      \
+  int jn_[UNR];                                                               \
+  list_group<K>(A, i, nn, lane, jn_);                                         \
   for (int m0 = lane; m0 < nn; m0 += UNR * K) {                               \
     int jj[UNR];                                                              \
-    _Pragma("unroll") for (int u = 0; u < UNR; u++) {                         \
-      int m = m0 + u * K;                                                     \
-      jj[u] = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;            \
-      if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;                     \
-    }                                                                         \
+    _Pragma("unroll") for (int u = 0; u < UNR; u++) jj[u] = jn_[u];           \
     GATHER_T gj[UNR];                                                         \
     _Pragma("unroll") for (int u = 0; u < UNR; u++) if (jj[u] >= 0) gj[u] = GATHER(jj[u]); \
+    list_group<K>(A, i, nn, m0 + UNR * K, jn_);                               \
     _Pragma("unroll") for (int u = 0; u < UNR; u++) {                         \
       if (jj[u] < 0) continue;                                                \
       const int j = jj[u];                                                    \
@@ -641,8 +660,6 @@ constexpr int UNR = 4;
     }                 \
   }
 
-struct GPos { double4 x; double eb; };
-struct GFx { int4 x; float eb; };
 
 // smatb_preinteraction (src/TB.F90:367-455), FP64: rho_i = sum_j
 //   xi^2 exp(-2q(r/r0-1))            r <  rci
@@ -694,6 +711,8 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
     double eb = 1.0 / sqrt(band);
     A.eband[i] = eb;
     A.ebandf[i] = (float)eb;
+    const double4 xi = A.pos[i];
+    A.pose[i] = make_double4(xi.x, xi.y, xi.z, eb);  // one gather per neighbour in the force pass
   }
 }
 
@@ -719,15 +738,15 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
     const double ebi = A.eband[i];
     const int nn = min(A.nn[i], A.lcap);
     const bool one = S.ntypes == 1;
-    auto gat = [&](int j) { GPos g; g.x = A.pos[j]; g.eb = A.eband[j]; return g; };
-    PAIR_LOOP_BEGIN(GPos, gat)
+    auto gat = [&](int j) { return A.pose[j]; };
+    PAIR_LOOP_BEGIN(double4, gat)
       const SmFP64& c = tab[one ? 0 : ti * S.ntypes + A.type[j]];
       double v0, v1, v2;
-      vd_fp64(S, xi, gj[u].x, v0, v1, v2);
+      vd_fp64(S, xi, gj[u], v0, v1, v2);
       double dr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
       if (dr > c.rce) continue;
       double factor, repul;
-      double ebs = ebi + gj[u].eb;
+      double ebs = ebi + gj[u].w;
       if (dr <= c.rci) {
         double x = dr / c.r0 - 1.0;
         repul = c.A * exp(-c.p * x);
@@ -841,18 +860,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
     const int4 xi = A.fxp[i];
     const int nn = min(A.nn[i], A.lcap);
     const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
+    int jn[UNR];
+    list_group<K>(A, i, nn, lane, jn);
     for (int m0 = lane; m0 < nn; m0 += UNR * K) {
       int jj[UNR];
 #pragma unroll
-      for (int u = 0; u < UNR; u++) {
-        int m = m0 + u * K;
-        jj[u] = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;
-        if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;  // never gather outside the arena
-      }
+      for (int u = 0; u < UNR; u++) jj[u] = jn[u];
       int4 gj[UNR];
 #pragma unroll
       for (int u = 0; u < UNR; u++)
         if (jj[u] >= 0) gj[u] = A.fxp[jj[u]];
+      list_group<K>(A, i, nn, m0 + UNR * K, jn);  // next group's ids, in flight meanwhile
       float grp = 0.0f;
 #pragma unroll
       for (int u = 0; u < UNR; u++) {
@@ -883,7 +901,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
     A.band[i] = band;
     double eb = 1.0 / sqrt(band);
     A.eband[i] = eb;
-    A.ebandf[i] = (float)eb;
+    const float ebf = (float)eb;
+    A.ebandf[i] = ebf;
+    const int4 xi = A.fxp[i];
+    A.fxe[i] = make_int4(xi.x, xi.y, xi.z, __float_as_int(ebf));  // one gather per neighbour
   }
 }
 
@@ -904,35 +925,35 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
     const int nn = min(A.nn[i], A.lcap);
     const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
     const float evui = (float)EV_UI;
+    const int ti = xi.w;
+    int jn[UNR];
+    list_group<K>(A, i, nn, lane, jn);
     for (int m0 = lane; m0 < nn; m0 += UNR * K) {
       int jj[UNR];
 #pragma unroll
-      for (int u = 0; u < UNR; u++) {
-        int m = m0 + u * K;
-        jj[u] = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;
-        if ((unsigned)jj[u] >= (unsigned)A.cap) jj[u] = -1;  // never gather outside the arena
-      }
+      for (int u = 0; u < UNR; u++) jj[u] = jn[u];
       int4 gj[UNR];
-      float gb[UNR];
+      int tj[UNR];
 #pragma unroll
       for (int u = 0; u < UNR; u++)
         if (jj[u] >= 0) {
-          gj[u] = A.fxp[jj[u]];
-          gb[u] = A.ebandf[jj[u]];
+          gj[u] = A.fxe[jj[u]];
+          if (!ONE) tj[u] = A.type[jj[u]];
         }
+      list_group<K>(A, i, nn, m0 + UNR * K, jn);  // next group's ids, in flight meanwhile
       float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, ge = 0.0f;
 #pragma unroll
       for (int u = 0; u < UNR; u++) {
         if (jj[u] < 0) continue;
         const int4 xj = gj[u];
-        const SmF32& c = ONE ? c1 : tab[xi.w * S.ntypes + xj.w];
+        const SmF32& c = ONE ? c1 : tab[ti * S.ntypes + tj[u]];
         float v0, v1, v2;
         vd_fx(S, xi, xj, v0, v1, v2);
         float r2 = v0 * v0 + v1 * v1 + v2 * v2;
         if (r2 > c.rce2) continue;
         float rinv;
         float dr = sqrt_nr(r2, rinv);
-        float ebs = ebi + gb[u];
+        float ebs = ebi + __int_as_float(xj.w);
         float factor, repul;
         if (dr <= c.rci) {
           float x = c.r0 - dr;
@@ -1319,14 +1340,16 @@ __device__ __forceinline__ void wrap_atom(const SysDev& S, double4& x) {
 }
 
 // the moved atom's outputs: position, fixed-point copy, skin displacement
-__device__ __forceinline__ double moved_atom(Arena& A, const SysDev& S, SysState& st, int i, const double4& x) {
+// (xo = its position at the last rebuild, ty = its species)
+__device__ __forceinline__ double moved_atom(Arena& A, const SysDev& S, SysState& st, int i, const double4& x,
+                                             const double4& xo, int ty) {
   A.pos[i] = x;
   if (S.prec == PREC_MIXED || S.ff == FF_TERSOFF) {
     int bad = 0;
-    write_fx(A, S, i, x, A.type[i], bad);
+    write_fx(A, S, i, x, ty, bad);
     if (bad) atomicOr(&st.status, ST_LOST);
   }
-  double d = disp2(S, x, A.pos_old[i]);
+  double d = disp2(S, x, xo);
   if (!(d == d)) atomicOr(&st.status, ST_NAN);
   return d;
 }
@@ -1389,7 +1412,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
       A.vel_v[i] = vv;
     }
     wrap_atom(S, x);
-    t.x = moved_atom(A, S, st, i, x);
+    t.x = moved_atom(A, S, st, i, x, A.pos_old[i], A.type[i]);
   }
   skin_close<COND>(A, M, s, S, st, frozen, t, cond);
 }
@@ -1400,7 +1423,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
 // the same operations in the same order, with each array read and written
 // once instead of twice.
 template <bool COND>
-__global__ void __launch_bounds__(BLOCK) k_step_ba(Arena A, BlockMap M, cudaGraphConditionalHandle cond) {
+__global__ void __launch_bounds__(BLOCK, 4) k_step_ba(Arena A, BlockMap M, cudaGraphConditionalHandle cond) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
@@ -1408,15 +1431,20 @@ __global__ void __launch_bounds__(BLOCK) k_step_ba(Arena A, BlockMap M, cudaGrap
   int i = M.first[blockIdx.x] + threadIdx.x;
   bool act = i < M.end[blockIdx.x];
   double2 t = make_double2(1.e-16, 1.e-16);
-  if (act && (S.integ == IT_VV || S.integ == IT_ERMAK)) {
+  const int integ = S.integ;
+  if (act && (integ == IT_VV || integ == IT_ERMAK)) {
+    // every input is loaded before the first store, so all loads are in flight together
     double4 x = A.pos[i], v = A.vel[i], a = A.acel[i];
     const double4 F = A.force[i];
     const double2 mi = A.minv[i];
-    if (S.integ == IT_VV) {
+    const double4 xo = A.pos_old[i];
+    const int ty = A.type[i];
+    const double4 vv0 = integ == IT_ERMAK ? A.vel_v[i] : make_double4(0, 0, 0, 0);
+    if (integ == IT_VV) {
       vv_b_atom(S.dt, mi.x, F, v, a);
       vv_a_atom(S.dt, mi.x, F, x, v, a);
     } else {
-      ermak_b_atom(S, mi.x, F, A.vel_v[i], v, a);
+      ermak_b_atom(S, mi.x, F, vv0, v, a);
       double4 vv;
       ermak_a_atom(A, S, st, i, mi, v, a, x, vv);
       A.vel_v[i] = vv;
@@ -1424,7 +1452,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_ba(Arena A, BlockMap M, cudaGrap
     A.acel[i] = a;
     A.vel[i] = v;
     wrap_atom(S, x);
-    t.x = moved_atom(A, S, st, i, x);
+    t.x = moved_atom(A, S, st, i, x, xo, ty);
   }
   skin_close<COND>(A, M, s, S, st, false, t, cond);
 }

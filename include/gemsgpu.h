@@ -329,7 +329,8 @@ int gemsgpu_smatb_forces_noalloc(const double* d_pos, int n, int boxed,
 /* Time the system's force kernels over the candidate launch shapes (lanes
  * per atom 1..32; for mixed SMA-TB the variant bits: bit 0 species
  * constants in shared memory (1) or registers (0, single species), bit 1 a
- * register-capped build with more blocks per SM) and keep the fastest.  reps timed
+ * register-capped build with more blocks per SM (four per SM), bit 2 with
+ * bit 1 a force pass capped at three blocks per SM) and keep the fastest.  reps timed
  * evaluations per candidate.  No reference counterpart (GEMS has no device
  * code); the choice changes summation order only. */
 int gemsgpu_autotune(gemsgpu_ctx* ctx, int sys, int reps, int* lanes_out,
@@ -338,7 +339,7 @@ int gemsgpu_autotune(gemsgpu_ctx* ctx, int sys, int reps, int* lanes_out,
  * all of them: the best shape of a batch differs from a lone system's). */
 int gemsgpu_batch_autotune(gemsgpu_ctx* ctx, const int* sys, int nsys, int reps,
                            int* lanes_out, int* variant_out, double* best_ms);
-/* Set the launch shape by hand (lanes: 1,2,4,...,32; variant 0..3). */
+/* Set the launch shape by hand (lanes: 1,2,4,...,32; variant 0..3, 6, 7). */
 int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant);
 
 /* ------------------------------------------------------------ measurement */

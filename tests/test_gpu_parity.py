@@ -349,12 +349,12 @@ def test_launch_shapes_agree(ctx, prec):
     o.interact()
     fo = o.force
     for lanes in (1, 2, 4, 8, 16, 32):
-        for variant in (0, 1, 2, 3):
+        for variant in (0, 1, 2, 3, 6, 7):
             g.set_lanes(lanes, variant)
             g.interact()
             assert relrms(g.force, fo) <= (RMS_FP64 if prec == 0 else RMS_MIXED)
     k, v, ms = g.autotune(3)
-    assert k in (1, 2, 4, 8, 16, 32) and v in (0, 1, 2, 3) and ms > 0
+    assert k in (1, 2, 4, 8, 16, 32) and v in (0, 1, 2, 3, 6, 7) and ms > 0
 
 
 def _cluster_replicas(ctx, nrep, temps, seed0=7):
