@@ -728,7 +728,7 @@ def main():
     # batched arm launches it (all replicas in one launch, its tuned shape)
     nbar = 54.0   # list entries per atom (fcc shells within 6.0 A)
     force_bytes = 16 + 4 + 8 + 4 * nbar + 32 + 8      # own int4, rho^-1/2, rho, list, force, epot
-    rho_bytes = 16 + 4 * nbar + 8 + 8 + 4
+    rho_bytes = 16 + 4 * nbar + 8 + 8 + 4 + 16       # own int4, list, rho, rho^-1/2 (f64, f32), fxe
     peak, peak_kind = measured_peaks()
     kb = ctx.batch_time_kernels(reps, 50)
     ach = force_bytes * natoms / (kb[1] * 1e-3) / 1e9
