@@ -512,8 +512,15 @@ def run_c5(args, gems, torch, ctx, ext):
 
 def run_c3(args, gems, torch, ctx, ext):
     """1024 free Au clusters relaxed with FIRE in one batch, then 64
-    replica-exchange replicas of a 147-atom cluster (200-900 K)."""
+    replica-exchange replicas of a 147-atom cluster (200-900 K).  Under
+    torchrun every rank relaxes its own 1024 clusters and holds 64 replicas of
+    one ladder of 64 x ranks temperatures; the exchange all-gathers energies."""
     from gems_b200 import workloads as W
+    from gems_b200.remd import ReplicaExchange
+    rank, world, _ = dist_env()
+    tdist = None
+    if world > 1:
+        import torch.distributed as tdist
     sm, m = W.SMATB["Au"], W.MASS["Au"]
     clusters = W.batched_clusters()
     ss = []
@@ -525,54 +532,63 @@ def run_c3(args, gems, torch, ctx, ext):
         g.set_fire(0.002, 0.02)
         ss.append(g)
     torch.cuda.synchronize()
+    if tdist:
+        tdist.barrier()
     t0 = time.perf_counter()
     iters = ctx.batch_fire(ss, 1e-3, 5000)
     torch.cuda.synchronize()
-    t_fire = time.perf_counter() - t0
+    t_fire = max_over_ranks(time.perf_counter() - t0, tdist, "cuda")
     atom_iters = float(sum(int(i) * g.n for i, g in zip(iters, ss)))
     fmax = [g.fmax() for g in ss[:64]]
-    fire = {"systems": len(ss), "atoms": sum(g.n for g in ss), "seconds": t_fire,
-            "atom_steps_per_s": atom_iters / t_fire, "iters_median": float(np.median(iters)),
-            "iters_max": int(max(iters)), "converged": int(sum(int(i) < 5000 for i in iters)),
+    fire = {"systems": len(ss) * world, "atoms": sum(g.n for g in ss) * world, "seconds": t_fire,
+            "atom_steps_per_s": world * atom_iters / t_fire, "iters_median": float(np.median(iters)),
+            "iters_max": int(max(iters)), "converged": int(sum(int(i) < 5000 for i in iters)) * world,
             "fmax_first64_max": max(fmax)}
     for g in ss:
         g.destroy()
-    # replica exchange
-    nrep = 64
+    # replica exchange: this rank's 64 replicas of one ladder over all ranks
+    nloc = 64
+    nrep = nloc * world
     temps = 200.0 * (900.0 / 200.0) ** (np.arange(nrep) / (nrep - 1))
     base = W.cluster(147, np.random.default_rng(147))
     reps = []
-    for k in range(nrep):
+    for k in range(nloc):
+        gid = rank * nloc + k
         g = gems.System(base, m, ctx=ctx)
         g.set_smatb(*sm)
         g.set_precision(gems.PREC_MIXED)
         g.set_lanes(4, 1)
-        g.set_ermak(0.002, 1.0, temps[k], seed=500 + k)
+        g.set_ermak(0.002, 1.0, temps[gid], seed=500 + gid)
         g.interact()
         reps.append(g)
-    order = list(reps)
-    rounds, acc, attempted = 10, 0, 0
+    rex = ReplicaExchange(ctx, reps, temps, seed=77)
+    rounds = 10
     torch.cuda.synchronize()
+    if tdist:
+        tdist.barrier()
     t0 = time.perf_counter()
     for r in range(1, rounds + 1):
-        ctx.batch_md_steps(order, 500)
-        order, a = ctx.replica_exchange(order, temps, r, seed=77)
-        acc += a
-        par = 1 if r % 2 == 0 else -1
-        attempted += sum(1 for q in range(nrep) if q % 2 == 0 and 0 <= q + par < nrep and q + par > q) + \
-            sum(1 for q in range(nrep) if q % 2 == 1 and 0 <= q - par < nrep and q - par > q)
+        ctx.batch_md_steps(reps, 500)
+        rex.exchange(r)
     torch.cuda.synchronize()
-    t_rex = time.perf_counter() - t0
-    rex = {"replicas": nrep, "atoms_each": 147, "rounds": rounds, "steps_per_round": 500,
-           "seconds": t_rex, "atom_steps_per_s": nrep * 147 * 500 * rounds / t_rex,
-           "accepted": acc, "attempted": attempted}
+    t_rex = max_over_ranks(time.perf_counter() - t0, tdist, "cuda")
+    attempted = 0
+    for r in range(1, rounds + 1):
+        par = 1 if r % 2 == 0 else -1
+        attempted += sum(1 for q in range(nrep) if 0 <= (q + par if q % 2 == 0 else q - par) < nrep
+                         and (q + par if q % 2 == 0 else q - par) > q)
+    rex_d = {"replicas": nrep, "atoms_each": 147, "rounds": rounds, "steps_per_round": 500,
+             "seconds": t_rex, "atom_steps_per_s": nrep * 147 * 500 * rounds / t_rex,
+             "accepted": rex.accepted, "attempted": attempted, "ranks": world}
     for g in reps:
         g.destroy()
+    if rank != 0:
+        return
     _line("atom-steps/s (1024 Au clusters FIRE + 64-replica exchange, batched)", fire["atom_steps_per_s"], UNIT,
-          args, {"workload": "1024 Au clusters 13-2000 atoms (log-uniform, seed 3), FIRE to 1e-3 eV/A cap 5000; "
-                             "64 x 147-atom replicas 200-900 K, swaps every 500 steps"},
-          dtype="f32+f64acc", fire=fire, replica_exchange=rex,
-          **({} if args.no_cpu else {"cpu_baseline": cpu_baseline_c3(args.cpu_seconds)}))
+          args, {"workload": "1024 Au clusters 13-2000 atoms (log-uniform, seed 3) per GPU, FIRE to 1e-3 eV/A cap "
+                             "5000; 64 x 147-atom replicas per GPU on one 200-900 K ladder, swaps every 500 steps"},
+          dtype="f32+f64acc", fire=fire, replica_exchange=rex_d, n_gpus=world,
+          **({} if args.no_cpu or world > 1 else {"cpu_baseline": cpu_baseline_c3(args.cpu_seconds)}))
 
 
 def run_c4(args, gems, torch, ctx, ext):
@@ -635,11 +651,27 @@ def main():
     if args.config != "c2":
         import torch
         import gems_b200 as gems
-        torch.cuda.set_device(0)
-        ctx = gems.Context(device=0)
-        ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=0)
+        rank, world, local = dist_env()
+        if args.config == "c3" and world > 1:
+            # replica exchange across ranks: one all-gather of energies per round
+            import datetime
+            import torch.distributed as tdist
+            torch.cuda.set_device(local)
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        elif world > 1:
+            if rank == 0:
+                print(json.dumps({"config": args.config, "unavailable": "multi-GPU runs cover c2 and c3"}))
+            return
+        else:
+            torch.cuda.set_device(0)
+        dev = torch.cuda.current_device()
+        ctx = gems.Context(device=dev)
+        ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
         {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args, gems, torch, ctx, ext)
         ctx.close()
+        if world > 1:
+            tdist.barrier()
+            tdist.destroy_process_group()
         return
     import torch
     import gems_b200 as gems

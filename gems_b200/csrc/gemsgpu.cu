@@ -2215,6 +2215,85 @@ int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant) {
   return 0;
 }
 
+// parallel_tempering2 (src/ReplicaExchange.f90:55-138): in round ns the
+// temperature index k pairs with k+par (even k) or k-par (odd k), par = +1
+// for even ns and -1 for odd ns; the lower index accepts with
+// min(1, exp(-(beta_k - beta_k')(U_k' - U_k))).  Host arithmetic only, so
+// every rank of a multi-GPU run reaches the same decisions from the same
+// energies.
+int gemsgpu_remd_decide(int nrep, const double* epot_ev, const double* temps, int round, uint64_t seed,
+                        const double* uniforms, int* partner, int* accepted) {
+  if (nrep <= 0 || !epot_ev || !temps || !partner) return GEMSGPU_ERR_ARG;
+  for (int k = 0; k < nrep; k++) {
+    if (!(temps[k] > 0.0)) return GEMSGPU_ERR_ARG;
+    partner[k] = k;
+  }
+  const double kB_ev = 8.617385e-5;
+  const int par = (round % 2 == 0) ? 1 : -1;
+  int nacc = 0;
+  for (int k = 0; k < nrep; k++) {
+    int p = (k % 2 == 0) ? k + par : k - par;
+    if (p < 0 || p >= nrep || p < k) continue;  // k is the lower index of the pair
+    double bk = 1.0 / (kB_ev * temps[k]), bp = 1.0 / (kB_ev * temps[p]);
+    double du = (epot_ev[p] - epot_ev[k]) * (bk - bp);
+    bool swap = true;
+    if (du > 0.0) {
+      double u;
+      if (uniforms) {
+        u = uniforms[k];
+      } else {
+        uint4 q = philox10(make_uint4((uint32_t)k, (uint32_t)round, (uint32_t)((uint64_t)round >> 32), 7u),
+                           make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+        u = ((double)(q.x >> 5) * 67108864.0 + (double)(q.y >> 6)) / 9007199254740992.0;
+      }
+      swap = u < std::exp(-du);
+    }
+    if (!swap) continue;
+    nacc++;
+    partner[k] = p;
+    partner[p] = k;
+  }
+  if (accepted) *accepted = nacc;
+  return 0;
+}
+
+// each system takes its new Ermak temperature; velocities scale by
+// sqrt(T_new / T_old) (the reference rescales after exchanging configurations)
+int gemsgpu_retemper(gemsgpu_ctx* ctx, int nsys, const int* sys, const double* temps) {
+  if (!ctx || nsys <= 0 || !sys || !temps) return fail(ctx, GEMSGPU_ERR_ARG, "retemper: arguments");
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  for (int k = 0; k < nsys; k++) {
+    if (ctx->sys[ss[k]].d.integ != IT_ERMAK)
+      return fail(ctx, GEMSGPU_ERR_STATE, "retemper: system %d is not an Ermak system", ss[k]);
+    if (!(temps[k] > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "retemper: temperatures > 0");
+  }
+  cudaSetDevice(ctx->device);
+  std::vector<double> fac(ctx->scap, 1.0);
+  bool any = false;
+  for (int k = 0; k < nsys; k++) {
+    SysHost& h = ctx->sys[ss[k]];
+    if (h.temp != temps[k]) {
+      fac[ss[k]] = std::sqrt(temps[k] / h.temp);
+      h.d.skt = std::sqrt(kB_ui * temps[k]);
+      h.temp = temps[k];
+      CHK(push_sys(ctx, ss[k]));
+      any = true;
+    }
+  }
+  if (any) {
+    double* dfac = nullptr;
+    CHK(dalloc(ctx, &dfac, ctx->scap));
+    CU(cudaMemcpyAsync(dfac, fac.data(), ctx->scap * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    BlockMap m;
+    CHK(get_map(ctx, ss, BLOCK, 0, &m));
+    k_scale_vel<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, dfac); ++ctx->launches;
+    CU(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dfac);
+  }
+  return 0;
+}
+
 int gemsgpu_replica_exchange(gemsgpu_ctx* ctx, int nrep, int* sys_of_temp, const double* temps,
                              int round, uint64_t seed, const double* uniforms, int* accepted) {
   if (!ctx || nrep <= 0 || !sys_of_temp || !temps) return fail(ctx, GEMSGPU_ERR_ARG, "replica_exchange: arguments");
@@ -2230,66 +2309,17 @@ int gemsgpu_replica_exchange(gemsgpu_ctx* ctx, int nrep, int* sys_of_temp, const
     std::sort(t.begin(), t.end());
     if (std::unique(t.begin(), t.end()) != t.end()) return fail(ctx, GEMSGPU_ERR_ARG, "duplicate replica");
   }
-  cudaSetDevice(ctx->device);
-  // inq_pot_energy of every replica at its current configuration
-  std::vector<double> r;
-  CHK(reduce_sys(ctx, ss, r));
-  // parallel_tempering2 (src/ReplicaExchange.f90:55-138): in round ns the
-  // temperature index k pairs with k+par (even k) or k-par (odd k), par = +1
-  // for even ns and -1 for odd ns; the lower index accepts with
-  // min(1, exp(-(beta_k - beta_k')(U_k' - U_k))).
-  const int par = (round % 2 == 0) ? 1 : -1;
+  // inq_pot_energy of every replica at its current configuration (eV, as
+  // gemsgpu_batch_energy reports it)
+  std::vector<double> ep(nrep);
+  CHK(gemsgpu_batch_energy(ctx, ss.data(), nrep, ep.data(), nullptr, nullptr));
+  std::vector<int> partner(nrep);
   int nacc = 0;
-  std::vector<int> perm = ss;
-  for (int k = 0; k < nrep; k++) {
-    int p = (k % 2 == 0) ? k + par : k - par;
-    if (p < 0 || p >= nrep || p < k) continue;  // k is the lower index of the pair
-    double bk = 1.0 / (kB_ui * temps[k]), bp = 1.0 / (kB_ui * temps[p]);
-    double du = (r[4 * p] - r[4 * k]) * (bk - bp);
-    bool swap = true;
-    if (du > 0.0) {
-      double u;
-      if (uniforms) {
-        u = uniforms[k];
-      } else {
-        uint4 q = philox10(make_uint4((uint32_t)k, (uint32_t)round, (uint32_t)((uint64_t)round >> 32), 7u),
-                           make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
-        u = ((double)(q.x >> 5) * 67108864.0 + (double)(q.y >> 6)) / 9007199254740992.0;
-      }
-      swap = u < std::exp(-du);
-    }
-    if (!swap) continue;
-    nacc++;
-    std::swap(perm[k], perm[p]);
-  }
-  // apply: each system takes its new temperature; velocities scale by
-  // sqrt(T_new / T_old) (the reference rescales after exchanging configurations)
-  std::vector<double> fac(ctx->scap, 1.0);
-  bool any = false;
-  for (int k = 0; k < nrep; k++) {
-    int sid = perm[k];
-    SysHost& h = ctx->sys[sid];
-    double told = h.temp;
-    double tnew = temps[k];
-    if (told != tnew) {
-      fac[sid] = std::sqrt(tnew / told);
-      h.d.skt = std::sqrt(kB_ui * tnew);
-      h.temp = tnew;
-      CHK(push_sys(ctx, sid));
-      any = true;
-    }
-    sys_of_temp[k] = sid;
-  }
-  if (any) {
-    double* dfac = nullptr;
-    CHK(dalloc(ctx, &dfac, ctx->scap));
-    CU(cudaMemcpyAsync(dfac, fac.data(), ctx->scap * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    BlockMap m;
-    CHK(get_map(ctx, ss, BLOCK, 0, &m));
-    k_scale_vel<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, dfac); ++ctx->launches;
-    CU(cudaStreamSynchronize(ctx->stream));
-    cudaFree(dfac);
-  }
+  if (gemsgpu_remd_decide(nrep, ep.data(), temps, round, seed, uniforms, partner.data(), &nacc))
+    return fail(ctx, GEMSGPU_ERR_ARG, "replica_exchange: decision arguments");
+  // the replica at temperature partner[k] moves to temperature k
+  for (int k = 0; k < nrep; k++) sys_of_temp[k] = ss[partner[k]];
+  CHK(gemsgpu_retemper(ctx, nrep, sys_of_temp, temps));
   if (accepted) *accepted = nacc;
   return 0;
 }

@@ -80,6 +80,8 @@ _SIGS = {
     "gemsgpu_checkpoint_save": (_i, [_p, _i, _p, ctypes.c_size_t]),
     "gemsgpu_checkpoint_load": (_i, [_p, _i, _p, ctypes.c_size_t]),
     "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
+    "gemsgpu_remd_decide": (_i, [_i, _dp, _dp, _i, ctypes.c_uint64, _dp, _ip, _ip]),
+    "gemsgpu_retemper": (_i, [_p, _i, _ip, _dp]),
     "gemsgpu_pool_create": (_i, [_p, _i, _l, _l, _i, _i, _i, _i, _i, ctypes.POINTER(_p)]),
     "gemsgpu_pool_destroy": (_i, [_p]),
     "gemsgpu_pool_set": (_i, [_p, _ip, _i]),
@@ -193,6 +195,12 @@ class Context:
         by_id = {s.sid: s for s in systems_of_temp}
         return [by_id[int(k)] for k in ids], acc.value
 
+    def retemper(self, systems, temps):
+        """New Ermak temperatures, velocities rescaled by sqrt(T_new/T_old)."""
+        ids = self._ids(systems)
+        t = np.ascontiguousarray(temps, dtype=np.float64)
+        self.check(lib().gemsgpu_retemper(self.h, len(ids), _ptr(ids, ctypes.c_int), _ptr(t)))
+
     def batch_autotune(self, systems, reps=10):
         """One force-kernel launch shape for systems launched together."""
         ids = self._ids(systems)
@@ -224,6 +232,23 @@ class Context:
 
 
 _default_ctx = None
+
+
+def remd_decide(epot_ev, temps, rnd, seed=1, uniforms=None):
+    """parallel_tempering2's decision for one round (host arithmetic): returns
+    (partner, accepted), partner[k] = the temperature index whose replica
+    moves to temps[k]."""
+    e = np.ascontiguousarray(epot_ev, dtype=np.float64)
+    t = np.ascontiguousarray(temps, dtype=np.float64)
+    u = None if uniforms is None else np.ascontiguousarray(uniforms, dtype=np.float64)
+    n = len(e)
+    part = np.zeros(n, dtype=np.int32)
+    acc = ctypes.c_int()
+    rc = lib().gemsgpu_remd_decide(n, _ptr(e), _ptr(t), int(rnd), int(seed), _ptr(u), _ptr(part, ctypes.c_int),
+                                   ctypes.byref(acc))
+    if rc != 0:
+        raise GemsGpuError("remd_decide: bad arguments (%d)" % rc)
+    return part, acc.value
 
 
 def measure_peaks(device=0):

@@ -293,6 +293,20 @@ int gemsgpu_replica_exchange(gemsgpu_ctx* ctx, int nrep, int* sys_of_temp,
                              const double* temps, int round, uint64_t seed,
                              const double* uniforms, int* accepted);
 
+/* The decision of one exchange round alone, in host arithmetic (no device,
+ * no context): epot_ev[k] is the potential energy (eV) of the replica at
+ * temps[k]; partner[k] receives the temperature index whose replica moves
+ * to temps[k] (k itself when no swap).  Same rule and uniforms as
+ * gemsgpu_replica_exchange, so every rank of a multi-GPU run that has
+ * gathered the same energies reaches the same decisions. */
+int gemsgpu_remd_decide(int nrep, const double* epot_ev, const double* temps,
+                        int round, uint64_t seed, const double* uniforms,
+                        int* partner, int* accepted);
+/* Give nsys Ermak systems new temperatures, rescaling each one's velocities
+ * by sqrt(T_new/T_old) (the second half of an accepted exchange). */
+int gemsgpu_retemper(gemsgpu_ctx* ctx, int nsys, const int* sys,
+                     const double* temps);
+
 /* ------------------------------------------------------------ no allocation */
 
 /* Largest system gemsgpu_smatb_forces_noalloc accepts. */

@@ -422,6 +422,33 @@ def test_replica_exchange_identical_replicas_always_swap(ctx):
     np.testing.assert_allclose(order[3].vel, v0[reps[2].sid] * np.sqrt(600.0 / 500.0), rtol=1e-14)
 
 
+def test_replica_exchange_driver_equals_context_call(ctx):
+    """The multi-rank driver (here one rank) takes the same decisions as
+    gemsgpu_replica_exchange and leaves the same temperatures and velocities."""
+    from gems_b200.remd import ReplicaExchange
+    nrep = 6
+    temps = 250.0 * (800.0 / 250.0) ** (np.arange(nrep) / (nrep - 1))
+    a = _cluster_replicas(ctx, nrep, temps, seed0=21)
+    b = _cluster_replicas(ctx, nrep, temps, seed0=21)
+    rex = ReplicaExchange(ctx, b, temps, seed=13)
+    order = list(a)
+    acc_a = acc_b = 0
+    for rnd in range(1, 9):
+        ctx.batch_md_steps(a, 40)
+        ctx.batch_md_steps(b, 40)
+        order, acc = ctx.replica_exchange(order, temps, rnd, seed=13)
+        acc_a += acc
+        acc_b += rex.exchange(rnd)
+    assert acc_a == acc_b and acc_a > 0
+    t_a = {s.sid: temps[k] for k, s in enumerate(order)}
+    np.testing.assert_array_equal(rex.local_temperatures(), [t_a[s.sid] for s in a])
+    for sa, sb in zip(a, b):
+        np.testing.assert_array_equal(sa.vel, sb.vel)
+        np.testing.assert_array_equal(sa.pos, sb.pos)
+    for g in a + b:
+        g.destroy()
+
+
 def test_fire_single_cluster_vs_oracle(ctx):
     """FIRE (the intent of src/FIRE.f90 with its defects fixed) relaxes a
     perturbed 55-atom Au cluster to the oracle's minimum."""
