@@ -21,6 +21,7 @@
 #include "../../include/gemsgpu.h"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "lbfgs.cuh"
 
 using namespace gg;
 
@@ -2666,6 +2667,132 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   h.first = true;        // the resumed interact rebuilds the list
   h.has_forces = false;
   return 0;
+}
+
+// ------------------------------------------------------------------ L-BFGS
+// lbfgs_minimizator (src/Quasi_Newton.f90:77-160) for nsys systems at once;
+// the kernels and the method are in lbfgs.cuh.  Rounds of function
+// evaluations run in chunks; after each chunk the host reads the systems'
+// phases, drops finished systems from the launches, and heals a list
+// overflow by growing the list and restarting the affected searches from
+// their current points (the L-BFGS history is then discarded).
+int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m, double eps, double xtol, int itermax,
+                        int* iters, int* nfun, int* status, double* emin_ev) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  if (m < 1 || m > LB_MAXM) return fail(ctx, GEMSGPU_ERR_ARG, "lbfgs: m must be 1..%d", LB_MAXM);
+  if (!(eps > 0.0) || !(xtol >= 0.0) || itermax < 1) return fail(ctx, GEMSGPU_ERR_ARG, "lbfgs: eps, xtol, itermax");
+  for (int s : ss)
+    if (ctx->sys[s].d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "lbfgs: system %d has no force field", s);
+  cudaSetDevice(ctx->device);
+  // workspace, indexed like the arena
+  const int64_t cap = ctx->acap;
+  LbWork W{};
+  W.cap = cap;
+  std::vector<void*> bufs;
+  auto take = [&](double4** p, size_t n) -> int {
+    CHK(dalloc(ctx, p, n));
+    bufs.push_back(*p);
+    return 0;
+  };
+  auto release = [&]() {
+    for (void* b : bufs) cudaFree(b);
+    bufs.clear();
+  };
+  int rc = 0;
+  if ((rc = take(&W.x0, cap)) || (rc = take(&W.g, cap)) || (rc = take(&W.gold, cap)) || (rc = take(&W.d, cap)) ||
+      (rc = take(&W.S, (size_t)m * cap)) || (rc = take(&W.Y, (size_t)m * cap))) {
+    release();
+    return rc;
+  }
+  if ((rc = dalloc(ctx, &W.st, ctx->scap))) {
+    release();
+    return rc;
+  }
+  bufs.push_back(W.st);
+  std::vector<LbState> hs(ctx->scap);
+  for (auto& L : hs) {
+    L = LbState{};
+    L.phase = LB_IDLE;
+    L.m = m;
+    L.eps = eps;
+    L.xtol = xtol;
+    L.itermax = itermax;
+  }
+  auto fail_clean = [&](int code) {
+    release();
+    return code;
+  };
+  if (cudaMemcpyAsync(W.st, hs.data(), hs.size() * sizeof(LbState), cudaMemcpyHostToDevice, ctx->stream) !=
+      cudaSuccess)
+    return fail_clean(fail(ctx, GEMSGPU_ERR_CUDA, "lbfgs: state upload"));
+  if ((rc = interact_group(ctx, ss, true))) return fail_clean(rc);
+  const int* sa;
+  if ((rc = sys_array(ctx, ss, &sa))) return fail_clean(rc);
+  k_lb_init<<<(int)ss.size(), LB_THREADS, 0, ctx->stream>>>(ctx->A, W, sa, 0); ++ctx->launches;
+  const int ROUND = 16;
+  const int64_t budget = (int64_t)itermax * (LB_MAXFEV + 1) + ROUND;
+  std::vector<int> active = ss;
+  int heals = 0;
+  for (int64_t rounds = 0; rounds < budget && !active.empty(); rounds += ROUND) {
+    BlockMap ma;
+    if ((rc = get_map(ctx, active, BLOCK, 0, &ma)) || (rc = sys_array(ctx, active, &sa)) ||
+        (rc = clear_status(ctx, active)))
+      return fail_clean(rc);
+    const int na = (int)active.size();
+    for (int r = 0; r < ROUND; r++) {
+      k_lb_dir<<<na, LB_THREADS, 0, ctx->stream>>>(ctx->A, W, sa); ++ctx->launches;
+      k_lb_move<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, W, ma); ++ctx->launches;
+      k_skin<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
+      if ((rc = launch_rebuild(ctx, active)) || (rc = launch_forces(ctx, active))) return fail_clean(rc);
+      k_lb_eval<<<na, LB_THREADS, 0, ctx->stream>>>(ctx->A, W, sa); ++ctx->launches;
+    }
+    if (cudaMemcpyAsync(hs.data(), W.st, hs.size() * sizeof(LbState), cudaMemcpyDeviceToHost, ctx->stream) !=
+        cudaSuccess)
+      return fail_clean(fail(ctx, GEMSGPU_ERR_CUDA, "lbfgs: state readback"));
+    if ((rc = read_states(ctx))) return fail_clean(rc);
+    int grow = 0;
+    for (int s : active) {
+      const int st = ctx->h_st[s].status;
+      if (st & (ST_NAN | ST_LOST)) return fail_clean(status_error(ctx, s, st));
+      if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
+    }
+    if (grow > 0) {
+      // forces of this chunk may come from truncated lists: grow, rebuild,
+      // and restart the unfinished searches from where they stand
+      if (++heals > 4) return fail_clean(fail(ctx, GEMSGPU_ERR_OVERFLOW, "lbfgs: neighbour list keeps overflowing"));
+      if ((rc = grow_list(ctx, grow + grow / 4 + 8))) return fail_clean(rc);
+      for (int s : active) ctx->sys[s].first = true;
+      if ((rc = interact_group(ctx, active, true)) || (rc = sys_array(ctx, active, &sa))) return fail_clean(rc);
+      k_lb_init<<<(int)active.size(), LB_THREADS, 0, ctx->stream>>>(ctx->A, W, sa, 1); ++ctx->launches;
+      continue;
+    }
+    std::vector<int> next;
+    for (int s : active) {
+      const int ph = hs[s].phase;
+      if (ph == LB_EVAL || ph == LB_ACCEPT) next.push_back(s);
+    }
+    active.swap(next);
+  }
+  CU(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < nsys; k++) {
+    const LbState& L = hs[ss[k]];
+    SysHost& h = ctx->sys[ss[k]];
+    h.has_forces = true;  // the last evaluation was at the final positions
+    h.pos_dirty = false;
+    if (iters) iters[k] = L.iter;
+    if (nfun) nfun[k] = L.nfun;
+    if (status) status[k] = L.phase == LB_DONE ? 0 : (L.phase == LB_FAIL ? -1 : 1);
+    if (emin_ev) emin_ev[k] = L.f;
+  }
+  release();
+  return 0;
+}
+
+int gemsgpu_lbfgs(gemsgpu_ctx* ctx, int sys, int m, double eps, double xtol, int itermax, int* iters, int* nfun,
+                  int* status, double* emin_ev) {
+  CHK(check_sys(ctx, sys));
+  return gemsgpu_batch_lbfgs(ctx, &sys, 1, m, eps, xtol, itermax, iters, nfun, status, emin_ev);
 }
 
 int gemsgpu_get_stream(gemsgpu_ctx* ctx, void** stream) {

@@ -80,6 +80,8 @@ _SIGS = {
     "gemsgpu_checkpoint_save": (_i, [_p, _i, _p, ctypes.c_size_t]),
     "gemsgpu_checkpoint_load": (_i, [_p, _i, _p, ctypes.c_size_t]),
     "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
+    "gemsgpu_lbfgs": (_i, [_p, _i, _i, _d, _d, _i, _ip, _ip, _ip, _dp]),
+    "gemsgpu_batch_lbfgs": (_i, [_p, _ip, _i, _i, _d, _d, _i, _ip, _ip, _ip, _dp]),
     "gemsgpu_remd_decide": (_i, [_i, _dp, _dp, _i, ctypes.c_uint64, _dp, _ip, _ip]),
     "gemsgpu_retemper": (_i, [_p, _i, _ip, _dp]),
     "gemsgpu_pool_create": (_i, [_p, _i, _l, _l, _i, _i, _i, _i, _i, ctypes.POINTER(_p)]),
@@ -194,6 +196,18 @@ class Context:
                                                   int(seed), _ptr(u), ctypes.byref(acc)))
         by_id = {s.sid: s for s in systems_of_temp}
         return [by_id[int(k)] for k in ids], acc.value
+
+    def batch_lbfgs(self, systems, m=5, eps=1e-8, xtol=1e-15, itermax=1000):
+        """L-BFGS-relax systems together; returns (status, iters, nfun, emin_ev)
+        arrays (status 0 converged, 1 iteration limit, -1 line search failed)."""
+        ids = self._ids(systems)
+        n = len(ids)
+        it, nf, stt = (np.zeros(n, dtype=np.int32) for _ in range(3))
+        em = np.zeros(n)
+        self.check(lib().gemsgpu_batch_lbfgs(self.h, _ptr(ids, ctypes.c_int), n, int(m), float(eps), float(xtol),
+                                             int(itermax), _ptr(it, ctypes.c_int), _ptr(nf, ctypes.c_int),
+                                             _ptr(stt, ctypes.c_int), _ptr(em)))
+        return stt, it, nf, em
 
     def retemper(self, systems, temps):
         """New Ermak temperatures, velocities rescaled by sqrt(T_new/T_old)."""
@@ -461,6 +475,15 @@ class System:
         """read_chp: resume from checkpoint bytes (the next interact rebuilds the list)."""
         buf = ctypes.create_string_buffer(data, len(data))
         self._c(lib().gemsgpu_checkpoint_load(self.ctx.h, self.sid, buf, len(data)))
+
+    def lbfgs(self, m=5, eps=1e-8, xtol=1e-15, itermax=1000):
+        """lbfgs_minimizator: minimise in place; returns (status, iterations,
+        function evaluations, E_pot in eV) -- status 0 converged, 1 iteration
+        limit, -1 line search failed."""
+        it, nf, st, em = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._c(lib().gemsgpu_lbfgs(self.ctx.h, self.sid, int(m), float(eps), float(xtol), int(itermax),
+                                    ctypes.byref(it), ctypes.byref(nf), ctypes.byref(st), ctypes.byref(em)))
+        return st.value, it.value, nf.value, em.value
 
     def fmax(self):
         v = ctypes.c_double()

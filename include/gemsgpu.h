@@ -216,6 +216,26 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys,
 int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys,
                          double* epot_ev, double* ekin_ev, double* temp);
 
+/* ------------------------------------------------------------ minimisation */
+
+/* L-BFGS minimisation in place (lbfgs_minimizator + lbfgs,
+ * src/Quasi_Newton.f90:77-160, 349-663): Liu-Nocedal limited-memory BFGS
+ * with m correction pairs (1..8; the reference uses 5) and the More-Thuente
+ * line search of mcsrch/mcstep (ftol 1e-4, gtol 0.9, 100 evaluations per
+ * search); f is E_pot in eV, g = -F in eV/A (get_fg).  Stops when
+ * |g| / int(max(1, |x|)) <= eps (the reference: 1e-8), after itermax
+ * iterations, or when a line search fails (xtol: relative interval width,
+ * 1e-15 in the reference).  The systems end at their last evaluated point
+ * with its forces.  Per system (arrays of nsys, any may be NULL): iters =
+ * iterations, nfun = function evaluations, status = 0 converged, 1
+ * iteration limit, -1 line search failed; emin_ev = final E_pot (eV).  The
+ * batch form relaxes nsys systems together, each with its own search. */
+int gemsgpu_lbfgs(gemsgpu_ctx* ctx, int sys, int m, double eps, double xtol,
+                  int itermax, int* iters, int* nfun, int* status, double* emin_ev);
+int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m,
+                        double eps, double xtol, int itermax, int* iters,
+                        int* nfun, int* status, double* emin_ev);
+
 /* ------------------------------------------------------------ checkpoints */
 
 /* Per-system checkpoint (write_chp / read_chp, src/Checkpoint.F90:154-244):

@@ -850,6 +850,244 @@ void stepb(Sys& s) {
   if (s.integ == IT_FIRE) fire_mix(s);
 }
 
+// ------------------------------------------------------------------ L-BFGS
+// lbfgs (Quasi_Newton.f90:349-663): limited-memory BFGS of Liu & Nocedal
+// (Math. Prog. B 45, 1989) with the line search of More & Thuente (ACM TOMS
+// 20, 1994) as mcsrch (:703-901) / mcstep (:903-1096) state it.  The
+// objective is get_fg (:1110-1120): f = interact * ui_ev (eV) and g = -F * ui_ev
+// (eV/A).  Constants: lbfgs_minimizator's m = 5, eps = 1e-8, xtol = 1e-15
+// (:77-110); gtol = 0.9, stpmin = 1e-20, stpmax = 1e20 (module :14-20);
+// ftol = 1e-4, maxfev = 100 (:467-469); itermax = 1000 (:391).
+
+void get_fg(Sys& s, double& f, std::vector<double>& g) {
+  f = interact(s, nullptr) * ui_ev;
+  for (int q = 0; q < 3 * s.n; q++) g[q] = -s.force[q] * ui_ev;
+}
+
+double dotv(const std::vector<double>& a, const std::vector<double>& b, int n) {
+  double d = 0.0;
+  for (int q = 0; q < n; q++) d += a[q] * b[q];
+  return d;
+}
+
+// one safeguarded cubic/quadratic step of the interval of uncertainty
+// [stx, sty] towards a point satisfying the strong Wolfe conditions (the
+// four cases of More & Thuente section 4, as mcstep orders them)
+void mt_step(double& stx, double& fx, double& dx, double& sty, double& fy, double& dy, double& stp, double fp,
+             double dp, bool& brackt, double stmin, double stmax, int& info) {
+  info = 0;
+  if ((brackt && (stp <= std::min(stx, sty) || stp >= std::max(stx, sty))) || dx * (stp - stx) >= 0.0 ||
+      stmax < stmin)
+    return;
+  const double sgnd = dp * (dx / std::fabs(dx));
+  double stpf, stpc, stpq;
+  bool bound;
+  auto gamma_of = [](double theta, double a, double b, bool clip) {
+    const double sc = std::max(std::fabs(theta), std::max(std::fabs(a), std::fabs(b)));
+    double disc = (theta / sc) * (theta / sc) - (a / sc) * (b / sc);
+    if (clip) disc = std::max(0.0, disc);
+    return sc * std::sqrt(disc);
+  };
+  if (fp > fx) {
+    // case 1: higher function value; the minimum is bracketed
+    info = 1;
+    bound = true;
+    const double theta = 3.0 * (fx - fp) / (stp - stx) + dx + dp;
+    double gam = gamma_of(theta, dx, dp, false);
+    if (stp < stx) gam = -gam;
+    const double r = ((gam - dx) + theta) / (((gam - dx) + gam) + dp);
+    stpc = stx + r * (stp - stx);
+    stpq = stx + ((dx / ((fx - fp) / (stp - stx) + dx)) / 2.0) * (stp - stx);
+    stpf = (std::fabs(stpc - stx) < std::fabs(stpq - stx)) ? stpc : stpc + (stpq - stpc) / 2.0;
+    brackt = true;
+  } else if (sgnd < 0.0) {
+    // case 2: lower value, derivatives of opposite sign; bracketed
+    info = 2;
+    bound = false;
+    const double theta = 3.0 * (fx - fp) / (stp - stx) + dx + dp;
+    double gam = gamma_of(theta, dx, dp, false);
+    if (stp > stx) gam = -gam;
+    const double r = ((gam - dp) + theta) / (((gam - dp) + gam) + dx);
+    stpc = stp + r * (stx - stp);
+    stpq = stp + (dp / (dp - dx)) * (stx - stp);
+    stpf = (std::fabs(stpc - stp) > std::fabs(stpq - stp)) ? stpc : stpq;
+    brackt = true;
+  } else if (std::fabs(dp) < std::fabs(dx)) {
+    // case 3: lower value, same sign, derivative magnitude decreases
+    info = 3;
+    bound = true;
+    const double theta = 3.0 * (fx - fp) / (stp - stx) + dx + dp;
+    double gam = gamma_of(theta, dx, dp, true);
+    if (stp > stx) gam = -gam;
+    const double r = ((gam - dp) + theta) / ((gam + (dx - dp)) + gam);
+    if (r < 0.0 && gam != 0.0) stpc = stp + r * (stx - stp);
+    else if (stp > stx) stpc = stmax;
+    else stpc = stmin;
+    stpq = stp + (dp / (dp - dx)) * (stx - stp);
+    if (brackt) stpf = (std::fabs(stp - stpc) < std::fabs(stp - stpq)) ? stpc : stpq;
+    else stpf = (std::fabs(stp - stpc) > std::fabs(stp - stpq)) ? stpc : stpq;
+  } else {
+    // case 4: lower value, same sign, derivative does not decrease
+    info = 4;
+    bound = false;
+    if (brackt) {
+      const double theta = 3.0 * (fp - fy) / (sty - stp) + dy + dp;
+      double gam = gamma_of(theta, dy, dp, false);
+      if (stp > sty) gam = -gam;
+      const double r = ((gam - dp) + theta) / (((gam - dp) + gam) + dy);
+      stpf = stp + r * (sty - stp);
+    } else {
+      stpf = (stp > stx) ? stmax : stmin;
+    }
+  }
+  // update the interval
+  if (fp > fx) {
+    sty = stp; fy = fp; dy = dp;
+  } else {
+    if (sgnd < 0.0) { sty = stx; fy = fx; dy = dx; }
+    stx = stp; fx = fp; dx = dp;
+  }
+  stpf = std::max(stmin, std::min(stmax, stpf));
+  stp = stpf;
+  if (brackt && bound) {
+    const double lim = stx + 0.66 * (sty - stx);
+    stp = (sty > stx) ? std::min(lim, stp) : std::max(lim, stp);
+  }
+}
+
+// mcsrch: from x (f, g at x) along s; on return x = x0 + stp s with f, g
+// there; info 1 = strong Wolfe conditions met, other values = failure kinds
+int mt_search(Sys& s, std::vector<double>& x, double& f, std::vector<double>& g, const std::vector<double>& dir,
+              double& stp, double ftol, double gtol, double xtol, double stpmin, double stpmax, int maxfev,
+              int& nfev) {
+  const int n = 3 * s.n;
+  const double dginit = dotv(g, dir, n);
+  nfev = 0;
+  if (dginit >= 0.0) return 0;  // not a descent direction
+  bool brackt = false, stage1 = true;
+  int infoc = 1;
+  const double finit = f, dgtest = ftol * dginit;
+  double width = stpmax - stpmin, width1 = width / 0.5;
+  const std::vector<double> x0 = x;
+  double stx = 0.0, fx = finit, dgx = dginit;
+  double sty = 0.0, fy = finit, dgy = dginit;
+  for (nfev = 1; nfev <= maxfev; nfev++) {
+    double stmin, stmax;
+    if (brackt) {
+      stmin = std::min(stx, sty);
+      stmax = std::max(stx, sty);
+    } else {
+      stmin = stx;
+      stmax = stp + 4.0 * (stp - stx);
+    }
+    stp = std::min(std::max(stp, stpmin), stpmax);
+    if ((brackt && (stp <= stmin || stp >= stmax)) || nfev == maxfev || infoc == 0 ||
+        (brackt && stmax - stmin <= xtol * stmax))
+      stp = stx;
+    for (int q = 0; q < n; q++) x[q] = x0[q] + stp * dir[q];
+    s.pos = x;
+    get_fg(s, f, g);
+    int info = 0;
+    const double dg = dotv(g, dir, n);
+    const double ftest1 = finit + stp * dgtest;
+    if ((brackt && (stp <= stmin || stp >= stmax)) || infoc == 0) info = 6;
+    if (stp == stpmax && f <= ftest1 && dg <= dgtest) info = 5;
+    if (stp == stpmin && (f > ftest1 || dg >= dgtest)) info = 4;
+    if (nfev == maxfev) return 3;
+    if (brackt && stmax - stmin <= xtol * stmax) info = 2;
+    if (f <= ftest1 && std::fabs(dg) <= gtol * (-dginit)) info = 1;
+    if (info != 0) return info;
+    if (stage1 && f <= ftest1 && dg >= std::min(ftol, gtol) * dginit) stage1 = false;
+    if (stage1 && f <= fx && f > ftest1) {
+      // modified function psi(stp) = f - stp * dgtest while in the first stage
+      double fm = f - stp * dgtest, fxm = fx - stx * dgtest, fym = fy - sty * dgtest;
+      double dgm = dg - dgtest, dgxm = dgx - dgtest, dgym = dgy - dgtest;
+      mt_step(stx, fxm, dgxm, sty, fym, dgym, stp, fm, dgm, brackt, stmin, stmax, infoc);
+      fx = fxm + stx * dgtest;
+      fy = fym + sty * dgtest;
+      dgx = dgxm + dgtest;
+      dgy = dgym + dgtest;
+    } else {
+      mt_step(stx, fx, dgx, sty, fy, dgy, stp, f, dg, brackt, stmin, stmax, infoc);
+    }
+    if (brackt) {
+      if (std::fabs(sty - stx) >= 0.66 * width1) stp = stx + 0.5 * (sty - stx);
+      width1 = width;
+      width = std::fabs(sty - stx);
+    }
+  }
+  return 3;
+}
+
+// returns iflag: 0 converged, -1 line search failed, 1 iteration limit;
+// *iters = L-BFGS iterations, *nfun = function evaluations, *fmin = f (eV)
+int lbfgs_min(Sys& s, int m, double eps, double xtol, int itermax, int* iters, int* nfun, double* fmin) {
+  const int n = 3 * s.n;
+  const double ftol = 1e-4, gtol = 0.9, stpmin = 1e-20, stpmax = 1e20;
+  const int maxfev = 100;
+  std::vector<double> x = s.pos, g(n), gold(n), d(n), q(n);
+  std::vector<std::vector<double>> S(m, std::vector<double>(n)), Y(m, std::vector<double>(n));
+  std::vector<double> rho(m), alpha(m);
+  double f;
+  get_fg(s, f, g);
+  int nf = 1, point = 0, flag = 1, it = 0;
+  for (int k = 0; k < n; k++) d[k] = -g[k];
+  double gnorm = std::sqrt(dotv(g, g, n));
+  for (it = 1; it <= itermax; it++) {
+    double stp = 1.0;
+    if (it == 1) {
+      stp = 1.0 / gnorm;
+    } else {
+      // two-loop recursion over the last min(it-1, m) pairs, newest first;
+      // H0 = (y.s / y.y) I with the newest pair
+      const int bound = std::min(it - 1, m);
+      const int newest = (point + m - 1) % m;
+      const double ys = dotv(Y[newest], S[newest], n);
+      const double yy = dotv(Y[newest], Y[newest], n);
+      const double h0 = ys / yy;
+      rho[newest] = 1.0 / ys;
+      for (int k = 0; k < n; k++) q[k] = -g[k];
+      int cp = point;
+      for (int b = 0; b < bound; b++) {
+        cp = (cp + m - 1) % m;
+        alpha[cp] = rho[cp] * dotv(S[cp], q, n);
+        for (int k = 0; k < n; k++) q[k] -= alpha[cp] * Y[cp][k];
+      }
+      for (int k = 0; k < n; k++) q[k] *= h0;
+      for (int b = 0; b < bound; b++) {
+        const double beta = alpha[cp] - rho[cp] * dotv(Y[cp], q, n);
+        for (int k = 0; k < n; k++) q[k] += beta * S[cp][k];
+        cp = (cp + 1) % m;
+      }
+      d = q;
+    }
+    gold = g;
+    int nfev = 0;
+    const int info = mt_search(s, x, f, g, d, stp, ftol, gtol, xtol, stpmin, stpmax, maxfev, nfev);
+    nf += nfev;
+    if (info != 1) {
+      flag = -1;
+      break;
+    }
+    for (int k = 0; k < n; k++) {
+      S[point][k] = stp * d[k];
+      Y[point][k] = g[k] - gold[k];
+    }
+    point = (point + 1) % m;
+    gnorm = std::sqrt(dotv(g, g, n));
+    double xnorm = std::sqrt(dotv(x, x, n));
+    xnorm = (double)(long)std::max(1.0, xnorm);  // int(max(1, xnorm)), :633
+    if (gnorm / xnorm <= eps) {
+      flag = 0;
+      break;
+    }
+  }
+  if (iters) *iters = std::min(it, itermax);
+  if (nfun) *nfun = nf;
+  if (fmin) *fmin = f;
+  return flag;
+}
+
 }  // namespace
 
 // ===================================================================== C ABI
@@ -1165,6 +1403,10 @@ int orc_dinamica(void* p, int nsteps, int each, double* rows) {
 
 // FIRE relaxation to max|F| < fmax_tol (eV/A) or maxit iterations.  Returns
 // the number of iterations; *fmax_out the final max|F| in eV/A.
+int orc_lbfgs(void* p, int m, double eps, double xtol, int itermax, int* iters, int* nfun, double* fmin) {
+  return lbfgs_min(*(Sys*)p, m, eps, xtol, itermax, iters, nfun, fmin);
+}
+
 int orc_fire_relax(void* p, double fmax_tol, int maxit, double* fmax_out) {
   Sys* s = (Sys*)p;
   interact(*s, nullptr);

@@ -88,6 +88,7 @@ def lib():
         "orc_remove_cm": (None, [_p]),
         "orc_dinamica": (_i, [_p, _i, _i, _dp]),
         "orc_fire_relax": (_i, [_p, _d, _i, _dp]),
+        "orc_lbfgs": (_i, [_p, _i, _d, _d, _i, _ip, _ip, _dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -366,3 +367,11 @@ class System:
 
     def fmax(self):
         return lib().orc_fmax(self.h)
+
+    def lbfgs(self, m=5, eps=1e-8, xtol=1e-15, itermax=1000):
+        """lbfgs_minimizator: minimise in place; returns (iflag, iterations,
+        function evaluations, f in eV)."""
+        it, nf, fm = ctypes.c_int(), ctypes.c_int(), _d()
+        flag = lib().orc_lbfgs(self.h, int(m), float(eps), float(xtol), int(itermax), ctypes.byref(it),
+                               ctypes.byref(nf), ctypes.byref(fm))
+        return flag, it.value, nf.value, fm.value

@@ -111,10 +111,23 @@ def bulk_deck():
     pos = pos * fact            # expand about the origin
     box = tuple(12.0 * fact for _ in range(3))
     # baletto_2003.prm, Ag Ag line
-    ag = (0.1031, 1.1899, 10.85, 3.18, 2.89, 2.89 * math.sqrt(2.0), 2.89 * math.sqrt(3.0))
     return dict(pos=pos, mass=MASS["Ag"], box=box, pbc=(False, False, False),
-                smatb=ag, dt=DT_DEFAULT, temp=1500.0, gamma=1.0, nsteps=220,
+                smatb=AG_BALETTO, dt=DT_DEFAULT, temp=1500.0, gamma=1.0, nsteps=220,
                 each=20, seed=123456, ref=np.array(g["smatb_bulk_energy"]))
+
+
+AG_BALETTO = (0.1031, 1.1899, 10.85, 3.18, 2.89, 2.89 * math.sqrt(2.0), 2.89 * math.sqrt(3.0))
+
+
+def md_deck():
+    """examples/SMA-TB/md.gms: 13 Ag read from coords.xyz (no box: O(N^2)
+    list), baletto_2003 Ag-Ag, `lbfgs` (lbfgs_minimizator, positions stay at
+    the minimum), then Ermak 300 K, gamma 1/ps, dt 1 fs on the LCG stream of
+    seed 123456, 1000 steps, a row every 100."""
+    g = golden()
+    return dict(pos=np.array(g["smatb_md_coords"], dtype=float), mass=MASS["Ag"], smatb=AG_BALETTO,
+                dt=0.001, temp=300.0, gamma=1.0, nsteps=1000, each=100, seed=123456,
+                ref=np.array(g["smatb_md_energy"]))
 
 
 # --------------------------------------------------------------- NVE / NVT

@@ -75,6 +75,21 @@ def test_smatb_bulk_linked_cells_ermak():
     np.testing.assert_allclose(r[:, :3], d["ref"], rtol=1e-6)
 
 
+def test_smatb_md_lbfgs_then_ermak():
+    """examples/SMA-TB/md.gms: L-BFGS relaxation of 13 Ag, then 1000 Ermak
+    steps at 300 K on the LCG stream."""
+    d = decks.md_deck()
+    s = O.System(d["pos"], d["mass"])
+    s.set_smatb(*d["smatb"])
+    flag, iters, nfun, fmin = s.lbfgs()
+    assert flag == 0 and nfun < 100      # converged; no energy row written during the search
+    assert s.fmax() < 1e-4
+    s.set_ermak(d["dt"], d["gamma"], d["temp"], O.Rng(d["seed"]))
+    r = s.dinamica(d["nsteps"], d["each"])
+    assert decks.gems_rule(d["ref"][:, 0], r[:, 0]) < 1e-6
+    np.testing.assert_allclose(r[:, :3], d["ref"], rtol=1e-6, atol=1e-6)
+
+
 def _he_ne(kind):
     g = decks.golden()
     rng = O.Rng(123456)
