@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRCS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu", "peaks.cu")]
 OUT = os.path.join(HERE, "libgemsgpu.so")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu", "peaks.cu", "kernels.cuh", "lbfgs.cuh",
+DEPS = [os.path.join(HERE, "csrc", f) for f in ("gemsgpu.cu", "noalloc.cu", "peaks.cu", "kernels.cuh", "lbfgs.cuh", "neb.cuh",
                                                              "common.cuh")] + [
     os.path.join(os.path.dirname(HERE), "include", "gemsgpu.h")]
 

@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "lbfgs.cuh"
+#include "neb.cuh"
 
 using namespace gg;
 
@@ -2793,6 +2794,133 @@ int gemsgpu_lbfgs(gemsgpu_ctx* ctx, int sys, int m, double eps, double xtol, int
                   int* status, double* emin_ev) {
   CHK(check_sys(ctx, sys));
   return gemsgpu_batch_lbfgs(ctx, &sys, 1, m, eps, xtol, itermax, iters, nfun, status, emin_ev);
+}
+
+// ------------------------------------------------------------------ NEB
+// neb (src/NEB.f90:58-220) over nimg image systems; kernels in neb.cuh.
+// Reproduced as the reference runs it: the last image's energy is not
+// evaluated before the final report (its loop ends at nimg-1, :110), so it
+// enters the tangent choice as 0; the time step is set once from the RMS
+// NEB force of the interpolated band, dt = sqrt(2 m 5e-5 / F_rms) (:133).
+int gemsgpu_neb(gemsgpu_ctx* ctx, const int* sys, int nimg, const int* fixed, int nfixed, double k_ev, int iters,
+                double* dt_out, double* eimg_ev) {
+  if (!ctx || nimg < 3 || !fixed || nfixed < 2 || iters < 0)
+    return fail(ctx, GEMSGPU_ERR_ARG, "neb: nimg >= 3, two or more fixed images, iters >= 0");
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nimg, ss));
+  const SysHost& h0 = ctx->sys[ss[0]];
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "neb: system %d has no force field", s);
+    if (h.n != h0.n || h.ntypes != h0.ntypes || h.d.ff != h0.d.ff)
+      return fail(ctx, GEMSGPU_ERR_ARG, "neb: the images must be systems of the same atoms and force field");
+  }
+  for (int j = 0; j < nfixed; j++) {
+    if (fixed[j] < 0 || fixed[j] >= nimg || (j > 0 && fixed[j] <= fixed[j - 1]))
+      return fail(ctx, GEMSGPU_ERR_ARG, "neb: fixed images must be increasing indices in [0, nimg)");
+  }
+  cudaSetDevice(ctx->device);
+  const int n = h0.n;
+  std::vector<int> off(nimg);
+  for (int k = 0; k < nimg; k++) off[k] = ctx->sys[ss[k]].off;
+  int *d_sys = nullptr, *d_off = nullptr;
+  double *d_e = nullptr, *d_f = nullptr;
+  auto release = [&]() {
+    cudaFree(d_sys);
+    cudaFree(d_off);
+    cudaFree(d_e);
+    cudaFree(d_f);
+  };
+  int rc = 0;
+  if ((rc = dalloc(ctx, &d_sys, nimg)) || (rc = dalloc(ctx, &d_off, nimg)) || (rc = dalloc(ctx, &d_e, nimg)) ||
+      (rc = dalloc(ctx, &d_f, nimg))) {
+    release();
+    return rc;
+  }
+  auto bail = [&](int code) {
+    release();
+    return code;
+  };
+  if (cudaMemcpyAsync(d_sys, ss.data(), nimg * sizeof(int), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+      cudaMemcpyAsync(d_off, off.data(), nimg * sizeof(int), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+      cudaMemsetAsync(d_e, 0, nimg * sizeof(double), ctx->stream) != cudaSuccess ||
+      cudaMemsetAsync(d_f, 0, nimg * sizeof(double), ctx->stream) != cudaSuccess)
+    return bail(fail(ctx, GEMSGPU_ERR_CUDA, "neb: set-up copies"));
+  NebDev N{d_sys, d_off, d_e, d_f, nimg, n, k_ev / c_ui_ev()};
+  // neb_linin, then unit masses at rest
+  for (int j = 0; j + 1 < nfixed; j++) {
+    if (fixed[j + 1] - fixed[j] < 2) continue;
+    k_neb_interp<<<(3 * n + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, N, fixed[j], fixed[j + 1]);
+    ++ctx->launches;
+  }
+  for (int k = 1; k < nimg - 1; k++) {
+    if (cudaMemsetAsync(ctx->A.vel + off[k], 0, (size_t)n * sizeof(double4), ctx->stream) != cudaSuccess)
+      return bail(fail(ctx, GEMSGPU_ERR_CUDA, "neb: velocity reset"));
+    ctx->sys[ss[k]].pos_dirty = true;
+  }
+  {
+    BlockMap mr;
+    std::vector<int> inner(ss.begin() + 1, ss.end() - 1);
+    if ((rc = get_map(ctx, inner, BLOCK, 0, &mr))) return bail(rc);
+    k_refresh_fx<<<mr.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, mr); ++ctx->launches;
+  }
+  // forces and energies of images 0 .. nimg-2 (:110-118), the NEB force, dt
+  std::vector<int> first(ss.begin(), ss.end() - 1);
+  if ((rc = interact_group(ctx, first, true))) return bail(rc);
+  k_neb_energy<<<nimg - 1, LB_THREADS, 0, ctx->stream>>>(ctx->A, N, 0); ++ctx->launches;
+  k_neb_force<<<nimg - 2, LB_THREADS, 0, ctx->stream>>>(ctx->A, N); ++ctx->launches;
+  std::vector<double> fsum(nimg);
+  if (cudaMemcpyAsync(fsum.data(), d_f, nimg * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return bail(fail(ctx, GEMSGPU_ERR_CUDA, "neb: force readback"));
+  double fprom = 0.0;
+  for (int k = 1; k < nimg - 1; k++) fprom += fsum[k];
+  fprom = std::sqrt(fprom / ((double)(nimg - 2) * (double)(3 * n)));
+  if (!(fprom > 0.0)) return bail(fail(ctx, GEMSGPU_ERR_STATE, "neb: the band has no force"));
+  const double mass = 1.0;
+  const double dt = std::sqrt(2.0 * mass * 5e-5 / fprom);
+  std::vector<int> inner(ss.begin() + 1, ss.end() - 1);
+  const int ni = nimg - 2;
+  const int vv_grid = (int)(((int64_t)ni * n + 255) / 256);
+  for (int it = 0; it < iters; it++) {
+    BlockMap mi;
+    if ((rc = get_map(ctx, inner, BLOCK, 0, &mi)) || (rc = clear_status(ctx, inner))) return bail(rc);
+    k_neb_vel<<<ni, LB_THREADS, 0, ctx->stream>>>(ctx->A, N); ++ctx->launches;
+    k_neb_vv<true><<<vv_grid, 256, 0, ctx->stream>>>(ctx->A, N, dt); ++ctx->launches;
+    k_skin<<<mi.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, mi); ++ctx->launches;
+    if ((rc = launch_rebuild(ctx, inner))) return bail(rc);
+    if ((rc = read_states(ctx))) return bail(rc);
+    int grow = 0;
+    for (int s : inner) {
+      const int st = ctx->h_st[s].status;
+      if (st & (ST_NAN | ST_LOST)) return bail(status_error(ctx, s, st));
+      if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
+    }
+    if (grow > 0) {  // the lists of this step would be truncated: grow and rebuild them
+      if ((rc = grow_list(ctx, grow + grow / 4 + 8))) return bail(rc);
+      for (int s : inner) ctx->sys[s].first = true;
+      if ((rc = interact_group(ctx, inner, true))) return bail(rc);
+    } else if ((rc = launch_forces(ctx, inner))) {
+      return bail(rc);
+    }
+    k_neb_energy<<<ni, LB_THREADS, 0, ctx->stream>>>(ctx->A, N, 1); ++ctx->launches;
+    k_neb_force<<<ni, LB_THREADS, 0, ctx->stream>>>(ctx->A, N); ++ctx->launches;
+    k_neb_vel<<<ni, LB_THREADS, 0, ctx->stream>>>(ctx->A, N); ++ctx->launches;
+    k_neb_vv<false><<<vv_grid, 256, 0, ctx->stream>>>(ctx->A, N, dt); ++ctx->launches;
+  }
+  // write_neb (:376-414): every image's forces and energy at the final band
+  for (int s : ss) ctx->sys[s].pos_dirty = true;
+  if ((rc = interact_group(ctx, ss, true))) return bail(rc);
+  k_neb_energy<<<nimg, LB_THREADS, 0, ctx->stream>>>(ctx->A, N, 0); ++ctx->launches;
+  std::vector<double> e(nimg);
+  if (cudaMemcpyAsync(e.data(), d_e, nimg * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return bail(fail(ctx, GEMSGPU_ERR_CUDA, "neb: energy readback"));
+  if (eimg_ev)
+    for (int k = 0; k < nimg; k++) eimg_ev[k] = e[k] * c_ui_ev();
+  if (dt_out) *dt_out = dt;
+  release();
+  return 0;
 }
 
 int gemsgpu_get_stream(gemsgpu_ctx* ctx, void** stream) {

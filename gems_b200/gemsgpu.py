@@ -82,6 +82,7 @@ _SIGS = {
     "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
     "gemsgpu_lbfgs": (_i, [_p, _i, _i, _d, _d, _i, _ip, _ip, _ip, _dp]),
     "gemsgpu_batch_lbfgs": (_i, [_p, _ip, _i, _i, _d, _d, _i, _ip, _ip, _ip, _dp]),
+    "gemsgpu_neb": (_i, [_p, _ip, _i, _ip, _i, _d, _i, _dp, _dp]),
     "gemsgpu_remd_decide": (_i, [_i, _dp, _dp, _i, ctypes.c_uint64, _dp, _ip, _ip]),
     "gemsgpu_retemper": (_i, [_p, _i, _ip, _dp]),
     "gemsgpu_pool_create": (_i, [_p, _i, _l, _l, _i, _i, _i, _i, _i, ctypes.POINTER(_p)]),
@@ -208,6 +209,18 @@ class Context:
                                              int(itermax), _ptr(it, ctypes.c_int), _ptr(nf, ctypes.c_int),
                                              _ptr(stt, ctypes.c_int), _ptr(em)))
         return stt, it, nf, em
+
+    def neb(self, images, fixed, k_ev, iters):
+        """Nudged elastic band over image systems (their fixed images set);
+        returns (dt in ps, per-image E_pot in eV) and leaves the final band
+        in the systems."""
+        ids = self._ids(images)
+        fx = np.ascontiguousarray(fixed, dtype=np.int32)
+        dt = ctypes.c_double()
+        e = np.zeros(len(ids))
+        self.check(lib().gemsgpu_neb(self.h, _ptr(ids, ctypes.c_int), len(ids), _ptr(fx, ctypes.c_int), len(fx),
+                                     float(k_ev), int(iters), ctypes.byref(dt), _ptr(e)))
+        return dt.value, e
 
     def retemper(self, systems, temps):
         """New Ermak temperatures, velocities rescaled by sqrt(T_new/T_old)."""

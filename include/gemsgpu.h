@@ -236,6 +236,24 @@ int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m,
                         double eps, double xtol, int itermax, int* iters,
                         int* nfun, int* status, double* emin_ev);
 
+/* ------------------------------------------------------------ NEB */
+
+/* Nudged elastic band (neb, neb_linin, nebfce, nebvel: src/NEB.f90:58-355)
+ * on nimg image systems sys[0..nimg-1] of the same atoms and force field.
+ * The images listed in `fixed` (increasing 0-based indices, two or more)
+ * hold their positions; the others are first set on the straight line
+ * between the neighbouring fixed ones.  iters iterations of velocity Verlet
+ * with unit masses on the NEB force (improved tangent, spring constant k_ev
+ * in eV/A^2) with the quick-min velocity projection, time step
+ * sqrt(2 * 5e-5 / F_rms) from the initial band; the end images do not move.
+ * As in the reference the last image's energy enters the tangent choice as
+ * 0 until the end.  On return the systems hold the final band with its
+ * forces; dt_out (may be NULL) gets the time step (ps) and eimg_ev (nimg,
+ * may be NULL) each image's potential energy (eV). */
+int gemsgpu_neb(gemsgpu_ctx* ctx, const int* sys, int nimg, const int* fixed,
+                int nfixed, double k_ev, int iters, double* dt_out,
+                double* eimg_ev);
+
 /* ------------------------------------------------------------ checkpoints */
 
 /* Per-system checkpoint (write_chp / read_chp, src/Checkpoint.F90:154-244):

@@ -1088,6 +1088,151 @@ int lbfgs_min(Sys& s, int m, double eps, double xtol, int itermax, int* iters, i
   return flag;
 }
 
+// ------------------------------------------------------------------ NEB
+// neb (NEB.f90:58-220): nimg images of one group, the end points fixed;
+// neb_linin (:331-355) fills the images between consecutive fixed ones
+// linearly; each iteration is velocity Verlet with unit masses
+// (change_atom_mas, :222-234) on the NEB force, with the quick-min velocity
+// projection nebvel (:314-329) before stepa and before stepb.  nebfce
+// (:236-312) is the improved tangent of Henkelman & Jonsson (J. Chem. Phys.
+// 113, 9978, 2000) with a spring force along it.  Kept as the reference has
+// them: the last image's energy is never evaluated (the first loop runs to
+// nimg-1, :110) and so stays 0 in the tangent choice, and the tangent vector
+// keeps its last value when no branch of the choice applies.  The time step
+// is set once from the initial RMS NEB force, dt = sqrt(2 m 5e-5 / F_rms)
+// (:133).  pneb: nimg x 3n positions, updated in place.
+struct Neb {
+  int nimg = 0, dim = 0;
+  std::vector<double> p, f, v, e, q;
+  double ks = 0.0;
+};
+
+void neb_load_eval(Sys& s, Neb& N, int i) {
+  std::copy(N.p.begin() + (size_t)i * N.dim, N.p.begin() + (size_t)(i + 1) * N.dim, s.pos.begin());
+  N.e[i] = interact(s, nullptr);
+  std::copy(s.force.begin(), s.force.end(), N.f.begin() + (size_t)i * N.dim);
+}
+
+void neb_forces(Neb& N) {
+  const int d = N.dim;
+  std::vector<double> tp(d), tm(d);
+  for (int i = 1; i < N.nimg - 1; i++) {
+    const double* pm = &N.p[(size_t)(i - 1) * d];
+    const double* pi = &N.p[(size_t)i * d];
+    const double* pp = &N.p[(size_t)(i + 1) * d];
+    for (int k = 0; k < d; k++) {
+      tp[k] = pp[k] - pi[k];
+      tm[k] = pi[k] - pm[k];
+    }
+    const double em = N.e[i - 1], ei = N.e[i], ep = N.e[i + 1];
+    const double dmin = std::fabs(ei - em), dplus = std::fabs(ep - ei);
+    const double dmax = std::max(dmin, dplus), dinf = std::min(dmin, dplus);
+    // the tangent: towards the higher neighbour, or an energy-weighted mix at an extremum
+    int kind = -1;  // 0: t+, 1: t-, 2: dmax t+ + dinf t-, 3: dinf t+ + dmax t-
+    if (ep > ei) {
+      if (ei > em) kind = 0;
+      else if (ep > em) kind = 2;
+      else if (ep < em) kind = 3;
+    } else {
+      if (ei > em) {
+        if (ep > em) kind = 2;
+        else if (ep < em) kind = 3;
+      } else {
+        kind = 1;
+      }
+    }
+    for (int k = 0; k < d; k++) {
+      if (kind == 0) N.q[k] = tp[k];
+      else if (kind == 1) N.q[k] = tm[k];
+      else if (kind == 2) N.q[k] = dmax * tp[k] + dinf * tm[k];
+      else if (kind == 3) N.q[k] = dinf * tp[k] + dmax * tm[k];
+    }
+    double nq = 0.0;
+    for (int k = 0; k < d; k++) nq += N.q[k] * N.q[k];
+    const double inv = std::sqrt(nq);
+    for (int k = 0; k < d; k++) N.q[k] = N.q[k] / inv;
+    double* fi = &N.f[(size_t)i * d];
+    double fq = 0.0, tpp = 0.0, tmm = 0.0;
+    for (int k = 0; k < d; k++) {
+      fq += fi[k] * N.q[k];
+      tpp += tp[k] * tp[k];
+      tmm += tm[k] * tm[k];
+    }
+    const double fs = N.ks * (std::sqrt(tpp) - std::sqrt(tmm));
+    for (int k = 0; k < d; k++) fi[k] = fi[k] - fq * N.q[k] + N.q[k] * fs;
+  }
+}
+
+void neb_velocities(Neb& N) {
+  const int d = N.dim;
+  for (int i = 1; i < N.nimg - 1; i++) {
+    double* vi = &N.v[(size_t)i * d];
+    const double* fi = &N.f[(size_t)i * d];
+    double vf = 0.0, ff = 0.0;
+    for (int k = 0; k < d; k++) vf += vi[k] * fi[k];
+    if (vf > 0.0) {
+      for (int k = 0; k < d; k++) ff += fi[k] * fi[k];
+      for (int k = 0; k < d; k++) vi[k] = vf * fi[k] / ff;
+    } else {
+      for (int k = 0; k < d; k++) vi[k] = 0.0;
+    }
+  }
+}
+
+// returns dt; images between fixed ones are interpolated first
+double neb_run(Sys& s, int nimg, double* pneb, const int* fixed, int nfixed, double k_ev, int iter) {
+  Neb N;
+  N.nimg = nimg;
+  N.dim = 3 * s.n;
+  const int d = N.dim;
+  N.p.assign(pneb, pneb + (size_t)nimg * d);
+  std::vector<int> fx(fixed, fixed + nfixed);
+  std::sort(fx.begin(), fx.end());
+  for (int j = 0; j + 1 < nfixed; j++) {
+    const int a = fx[j], b = fx[j + 1];
+    for (int i = a + 1; i < b; i++)
+      for (int k = 0; k < d; k++)
+        N.p[(size_t)i * d + k] = N.p[(size_t)(i - 1) * d + k] + (N.p[(size_t)b * d + k] - N.p[(size_t)a * d + k]) / (double)(b - a);
+  }
+  N.f.assign((size_t)nimg * d, 0.0);
+  N.v.assign((size_t)nimg * d, 0.0);
+  N.e.assign(nimg, 0.0);
+  N.q.assign(d, 0.0);
+  N.ks = k_ev * ev_ui;
+  for (int i = 0; i < nimg - 1; i++) neb_load_eval(s, N, i);
+  neb_forces(N);
+  double fprom = 0.0;
+  for (int i = 1; i < nimg - 1; i++)
+    for (int k = 0; k < d; k++) fprom += N.f[(size_t)i * d + k] * N.f[(size_t)i * d + k];
+  fprom = std::sqrt(fprom / ((double)(nimg - 2) * (double)d));
+  const double mass = 1.0;
+  const double dt = std::sqrt(2.0 * mass * 5e-5 / fprom);
+  const double adv = dt * 0.5, adx = adv * dt;
+  for (int ns = 1; ns <= iter; ns++) {
+    neb_velocities(N);
+    for (int i = 1; i < nimg - 1; i++) {
+      double* pi = &N.p[(size_t)i * d];
+      double* vi = &N.v[(size_t)i * d];
+      const double* fi = &N.f[(size_t)i * d];
+      for (int k = 0; k < d; k++) {  // velocity_verlet_a with one_mass = 1
+        const double a = fi[k] * 1.0;
+        pi[k] = pi[k] + dt * vi[k] + adx * a;
+        vi[k] = vi[k] + adv * a;
+      }
+      neb_load_eval(s, N, i);
+    }
+    neb_forces(N);
+    neb_velocities(N);
+    for (int i = 1; i < nimg - 1; i++) {
+      double* vi = &N.v[(size_t)i * d];
+      const double* fi = &N.f[(size_t)i * d];
+      for (int k = 0; k < d; k++) vi[k] = vi[k] + adv * (fi[k] * 1.0);  // velocity_verlet_b
+    }
+  }
+  std::copy(N.p.begin(), N.p.end(), pneb);
+  return dt;
+}
+
 }  // namespace
 
 // ===================================================================== C ABI
@@ -1405,6 +1550,10 @@ int orc_dinamica(void* p, int nsteps, int each, double* rows) {
 // the number of iterations; *fmax_out the final max|F| in eV/A.
 int orc_lbfgs(void* p, int m, double eps, double xtol, int itermax, int* iters, int* nfun, double* fmin) {
   return lbfgs_min(*(Sys*)p, m, eps, xtol, itermax, iters, nfun, fmin);
+}
+
+double orc_neb(void* p, int nimg, double* pneb, const int* fixed, int nfixed, double k_ev, int iter) {
+  return neb_run(*(Sys*)p, nimg, pneb, fixed, nfixed, k_ev, iter);
 }
 
 int orc_fire_relax(void* p, double fmax_tol, int maxit, double* fmax_out) {

@@ -89,6 +89,7 @@ def lib():
         "orc_dinamica": (_i, [_p, _i, _i, _dp]),
         "orc_fire_relax": (_i, [_p, _d, _i, _dp]),
         "orc_lbfgs": (_i, [_p, _i, _d, _d, _i, _ip, _ip, _dp]),
+        "orc_neb": (_d, [_p, _i, _dp, _ip, _i, _d, _i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -367,6 +368,14 @@ class System:
 
     def fmax(self):
         return lib().orc_fmax(self.h)
+
+    def neb(self, images, fixed, k_ev, iters):
+        """neb_run: images (nimg x n x 3; the fixed ones set) -> (relaxed
+        images, dt).  `fixed` holds 0-based image indices."""
+        im = np.ascontiguousarray(images, dtype=np.float64).copy()
+        fx = np.ascontiguousarray(fixed, dtype=np.int32)
+        dt = lib().orc_neb(self.h, im.shape[0], _ptr(im), _ptr(fx, ctypes.c_int), len(fx), float(k_ev), int(iters))
+        return im, dt
 
     def lbfgs(self, m=5, eps=1e-8, xtol=1e-15, itermax=1000):
         """lbfgs_minimizator: minimise in place; returns (iflag, iterations,

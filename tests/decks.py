@@ -130,6 +130,70 @@ def md_deck():
                 ref=np.array(g["smatb_md_energy"]))
 
 
+# --------------------------------------------------------------- NEB
+NEB_BOX = (12.195, 15.0, 12.195)
+# test.prm (examples/NEB): Au-Au Rossi 2005, Pt-Pt Cleri 1993, Au-Pt Logsdail 2009
+NEB_PRM = {(0, 0): (0.2096, 1.8153, 10.139, 4.033, 2.8850, 2.8850 * math.sqrt(2.0), 2.8850 * math.sqrt(3.0)),
+           (1, 1): (0.2975, 2.695, 10.612, 4.004, 3.924 / math.sqrt(2.0), 3.924, 3.924 * math.sqrt(3.0 / 2.0)),
+           (0, 1): (0.25, 2.2, 10.42, 4.02, 2.830, 2.830 * math.sqrt(2.0), 2.830 * math.sqrt(3.0))}
+
+
+def neb_deck():
+    """examples/NEB/neb.gms: the 72-atom Au slab of configs/ref/gold_cube.xyz
+    plus a Pt adatom at (0.2 Lx, 9.13, 0.2 Lz), all moved by 0.5 A, in a
+    non-periodic 12.195 x 15 x 12.195 box; three fixed images, each relaxed
+    by lbfgs after moving the Pt by (2, 0, 2) and then (2, 0, -2): images 1,
+    15 and 30 of 30; neb_run 20 iterations, spring 5 eV/A^2."""
+    g = golden()
+    au = np.array(g["neb_gold_cube"], dtype=float)
+    pt = np.array([[NEB_BOX[0] * 0.2, 9.13, NEB_BOX[2] * 0.2]])
+    pos = np.vstack([au, pt]) + 0.5
+    types = np.array([0] * len(au) + [1], dtype=np.int32)
+    mass = np.array([MASS["Au"]] * len(au) + [MASS["Pt"]])
+    return dict(pos=pos, types=types, mass=mass, box=NEB_BOX, prm=NEB_PRM, nimg=30, fixed=(0, 14, 29),
+                moves=((2.0, 0.0, 2.0), (2.0, 0.0, -2.0)), k=5.0, iters=20, ref=np.array(g["neb_energy"]))
+
+
+def neb_setup(s, d):
+    s.set_box(d["box"], (False, False, False))
+    for (a, b), prm in d["prm"].items():
+        s.set_smatb(*prm, a, b)
+
+
+def neb_fixed_images(s, d, relax):
+    """The three fixed images: relax, store, move the Pt, relax, ...
+    `relax(s)` runs the engine's L-BFGS on s."""
+    imgs = np.zeros((d["nimg"],) + d["pos"].shape)
+    relax(s)
+    imgs[d["fixed"][0]] = s.pos
+    for mv, k in zip(d["moves"], d["fixed"][1:]):
+        p = s.pos
+        p[-1] += mv
+        s.set_pos(p)
+        relax(s)
+        imgs[k] = s.pos
+    return imgs
+
+
+def neb_rows(images, energy_ev):
+    """write_neb (src/NEB.f90:376-414): per image the path length fraction
+    and its potential energy (eV); energy_ev is a function of an image's
+    positions or the energies themselves."""
+    gc = [0.0]
+    for i in range(1, len(images)):
+        gc.append(gc[-1] + float(np.sqrt(((images[i] - images[i - 1]) ** 2).sum())))
+    gc = np.array(gc) / gc[-1]
+    e = [energy_ev(im) for im in images] if callable(energy_ev) else list(energy_ev)
+    return np.c_[gc, np.asarray(e, dtype=float)]
+
+
+def neb_rule(ref, got):
+    """examples/test.sh for NEB: sum of squared differences of the first two
+    columns over the sum of the first column, < 1e-4."""
+    a = ((ref[:, 1] - got[:, 1]) ** 2).sum() + ((ref[:, 0] - got[:, 0]) ** 2).sum()
+    return abs(a / ref[:, 0].sum())
+
+
 # --------------------------------------------------------------- NVE / NVT
 def he_ne_gas(rng):
     """v_verlet.gms / ermak.gms set-up: `fill 100 2.6` He then Ne in 50^3."""

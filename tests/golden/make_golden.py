@@ -51,6 +51,8 @@ def main():
         "nve_energy": rows("examples/NVE/ref/Energy.v_verlet.dat"),
         "nvt_energy": rows("examples/NVT/ref/Energy.ermak.dat"),
         "repex_energy": [rows("examples/RepExchange/ref/Energy.lj.mpi%d.dat" % k) for k in range(4)],
+        "neb_gold_cube": xyz_frames("examples/configs/ref/gold_cube.xyz")[0],
+        "neb_energy": rows("examples/NEB/ref/Energy.neb.dat.NebF"),
     }
     with open(OUT, "w") as f:
         json.dump(g, f)
