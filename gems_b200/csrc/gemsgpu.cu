@@ -67,6 +67,7 @@ struct Graph {
 
 struct gemsgpu_ctx {
   int device = 0;
+  int nsm = 148;             // multiprocessors of the device
   cudaStream_t stream = nullptr;
   std::string err;
   // arena
@@ -637,12 +638,14 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
 
 // the rebuild chain; every kernel returns at once for systems whose
 // rebuild flag is clear, so the chain can sit in a captured step.
+// grid of the rebuild kernels that visit only flagged systems' blocks
+int rebuild_grid(const gemsgpu_ctx* ctx, int nblk) { return std::max(1, std::min(nblk, 8 * ctx->nsm)); }
+
 int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 0) {
-  BlockMap ma, mc, mw, mc8;
+  BlockMap ma, mc, mc8;
   const int* sa;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
   CHK(get_map(ctx, ss, 256, 1, &mc));
-  CHK(get_map(ctx, ss, LIST_ATOMS, 0, &mw));
   CHK(get_map(ctx, ss, BLOCK / 32, 1, &mc8));
   CHK(sys_array(ctx, ss, &sa));
   cudaStream_t st = ctx->stream;
@@ -655,11 +658,12 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 
     k_scan1<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
     k_scan2<<<(int)ss.size(), BLOCK, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
     k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
-    k_sort_cells<<<mc8.nblk, BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
-    k_list_cells<<<mw.nblk, BLOCK, list_smem(A.lcap), st>>>(A, mw); ++ctx->launches;
+    const int ns = (int)ss.size();
+    k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8, sa, ns); ++ctx->launches;
+    k_list_cells<<<4 * ctx->nsm, BLOCK, list_smem(A.lcap), st>>>(A, sa, ns); ++ctx->launches;
   }
   if (n2) {
-    k_list_n2<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+    k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma, sa, (int)ss.size()); ++ctx->launches;
   }
   k_count_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, st>>>(A, sa, (int)ss.size(), in_graph); ++ctx->launches;
   CU(cudaGetLastError());
@@ -954,7 +958,6 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
     const int* sa;
     CHK(get_map(ctx, ss, BLOCK, 0, &m));
     CHK(get_map(ctx, ss, 256, 1, &m));
-    CHK(get_map(ctx, ss, LIST_ATOMS, 0, &m));
     CHK(get_map(ctx, ss, BLOCK / 32, 1, &m));
     CHK(sys_array(ctx, ss, &sa));
     std::map<std::tuple<int, int, int>, std::vector<int>> groups;
@@ -1213,15 +1216,16 @@ int pool_rebuild(gemsgpu_pool* P, int in_graph) {
   gemsgpu_ctx* ctx = P->ctx;
   cudaStream_t st = ctx->stream;
   const Arena& A = ctx->A;
-  const BlockMap &ma = P->maps[0], &mc = P->maps[1], &mw = P->maps[2], &mc8 = P->maps[3];
+  const BlockMap &ma = P->maps[0], &mc = P->maps[1], &mc8 = P->maps[3];
   const int ns = P->max_systems;
   k_bin<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   k_scan1<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
   k_scan2<<<ns, BLOCK, 0, st>>>(A, P->dsys, ns); ++ctx->launches;
   k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
-  k_sort_cells<<<mc8.nblk, BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
-  k_list_cells<<<mw.nblk, BLOCK, list_smem(A.lcap), st>>>(A, mw); ++ctx->launches;
-  k_list_n2<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8, P->dsys, ns); ++ctx->launches;
+  k_list_cells<<<4 * ctx->nsm, BLOCK, list_smem(A.lcap), st>>>(A, P->dsys, ns);
+  ++ctx->launches;
+  k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma, P->dsys, ns); ++ctx->launches;
   k_count_rebuild<<<(ns + 255) / 256, 256, 0, st>>>(A, P->dsys, ns, in_graph); ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
@@ -1430,6 +1434,10 @@ int gemsgpu_create(int device, int64_t max_atoms, int max_systems, gemsgpu_ctx**
   int rc = 0;
   do {
     if (cudaSetDevice(device) != cudaSuccess) { rc = GEMSGPU_ERR_CUDA; break; }
+    if (cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+      rc = GEMSGPU_ERR_CUDA;
+      break;
+    }
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
       rc = GEMSGPU_ERR_CUDA;
       break;
@@ -2114,6 +2122,89 @@ int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys, double* epo
     if (epot_ev) epot_ev[k] = r[4 * k] * UI_EV;
     if (ekin_ev) ekin_ev[k] = r[4 * k + 1] * UI_EV;
     if (temp) temp[k] = 2.0 * r[4 * k + 1] / (kB_ui * (3.0 * ctx->sys[ss[k]].n));
+  }
+  return 0;
+}
+
+// Host <-> device state of many systems in one call: every copy and repack
+// is queued on the context's stream and the call synchronises once (the
+// per-system calls synchronise each time).  The staging buffer holds two
+// regions of 3 doubles per atom of the whole set, so no copy waits for
+// another's repack.
+int gemsgpu_batch_set_state(gemsgpu_ctx* ctx, const int* sys, int nsys, const double* const* pos,
+                            const double* const* vel) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  if (!pos && !vel) return fail(ctx, GEMSGPU_ERR_ARG, "batch_set_state: nothing to set");
+  cudaSetDevice(ctx->device);
+  int64_t total = 0;
+  for (int s : ss) total += ctx->sys[s].n;
+  CHK(ensure_stage(ctx, 2 * total));
+  int64_t o = 0;
+  std::vector<int> moved;
+  for (int k = 0; k < nsys; k++) {
+    SysHost& h = ctx->sys[ss[k]];
+    double* sp = ctx->stage + 3 * o;
+    double* sv = ctx->stage + 3 * (total + o);
+    if (pos && pos[k]) {
+      CU(cudaMemcpyAsync(sp, pos[k], (size_t)3 * h.n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      k_unpack3<<<(h.n + 255) / 256, 256, 0, ctx->stream>>>(sp, ctx->A.pos + h.off, h.n); ++ctx->launches;
+      moved.push_back(ss[k]);
+    }
+    if (vel && vel[k]) {
+      CU(cudaMemcpyAsync(sv, vel[k], (size_t)3 * h.n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      k_unpack3<<<(h.n + 255) / 256, 256, 0, ctx->stream>>>(sv, ctx->A.vel + h.off, h.n); ++ctx->launches;
+    }
+    o += h.n;
+  }
+  if (!moved.empty()) {
+    BlockMap m;
+    CHK(get_map(ctx, moved, BLOCK, 0, &m));
+    k_refresh_fx<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  }
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(ctx->stream));
+  for (int s : moved) {
+    ctx->sys[s].pos_dirty = true;
+    ctx->sys[s].has_forces = false;
+  }
+  return 0;
+}
+
+int gemsgpu_batch_get_state(gemsgpu_ctx* ctx, const int* sys, int nsys, double* const* pos, double* const* vel,
+                            double* epot_ev, double* ekin_ev, double* temp) {
+  std::vector<int> ss;
+  CHK(sys_list(ctx, sys, nsys, ss));
+  cudaSetDevice(ctx->device);
+  int64_t total = 0;
+  for (int s : ss) total += ctx->sys[s].n;
+  CHK(ensure_stage(ctx, 2 * total));
+  int64_t o = 0;
+  for (int k = 0; k < nsys; k++) {
+    const SysHost& h = ctx->sys[ss[k]];
+    double* sp = ctx->stage + 3 * o;
+    double* sv = ctx->stage + 3 * (total + o);
+    if (pos && pos[k]) {
+      k_pack3<<<(h.n + 255) / 256, 256, 0, ctx->stream>>>(ctx->A.pos + h.off, sp, h.n); ++ctx->launches;
+      CU(cudaMemcpyAsync(pos[k], sp, (size_t)3 * h.n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (vel && vel[k]) {
+      k_pack3<<<(h.n + 255) / 256, 256, 0, ctx->stream>>>(ctx->A.vel + h.off, sv, h.n); ++ctx->launches;
+      CU(cudaMemcpyAsync(vel[k], sv, (size_t)3 * h.n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    o += h.n;
+  }
+  CU(cudaGetLastError());
+  if (epot_ev || ekin_ev || temp) {
+    std::vector<double> r;
+    CHK(reduce_sys(ctx, ss, r));  // synchronises the stream
+    for (int k = 0; k < nsys; k++) {
+      if (epot_ev) epot_ev[k] = r[4 * k] * UI_EV;
+      if (ekin_ev) ekin_ev[k] = r[4 * k + 1] * UI_EV;
+      if (temp) temp[k] = 2.0 * r[4 * k + 1] / (kB_ui * (3.0 * ctx->sys[ss[k]].n));
+    }
+  } else {
+    CU(cudaStreamSynchronize(ctx->stream));
   }
   return 0;
 }

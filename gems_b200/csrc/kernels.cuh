@@ -388,42 +388,56 @@ __global__ void k_scatter(Arena A, BlockMap M) {
 // is built by inserting atoms in increasing index order.  Each lane ranks
 // its atom(s) against the whole cell (cells of up to 64 atoms); larger cells
 // fall back to an insertion sort by one lane.
-__global__ void k_sort_cells(Arena A, BlockMap C) {
-  int s = blk_sys(C);
-  if (s < 0) return;  // padding block of a fixed-capacity map
-  if (!A.st[s].rebuild || !A.sys[s].use_cells) return;
-  const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
-  const int first = C.first[blockIdx.x], end = C.end[blockIdx.x];
-  for (int c = first + warp; c < end; c += BLOCK / 32) {  // C: 8 cells per block
-    int start = A.chunk_sum[c >> 8] + A.cell_loc[c];
-    int n = A.cell_n[c];
-    if (ln == 0) A.cell_start[c] = start;
-    int* a = A.cell_atoms + start;
-    if (n <= 64) {
-      int v0 = ln < n ? a[ln] : -1;
-      int v1 = ln + 32 < n ? a[ln + 32] : -1;
-      int r0 = 0, r1 = 0;
-      for (int k = 0; k < 32; k++) {
-        int w0 = __shfl_sync(0xffffffffu, v0, k);
-        int w1 = __shfl_sync(0xffffffffu, v1, k);
-        r0 += (w0 > v0) + (w1 > v0);
-        r1 += (w0 > v1) + (w1 > v1);
-      }
-      __syncwarp();
-      if (ln < n) a[r0] = v0;
-      if (ln + 32 < n) a[r1] = v1;
-    } else if (ln == 0) {
-      for (int x = 1; x < n; x++) {
-        int v = a[x];
-        int y = x - 1;
-        while (y >= 0 && a[y] < v) {
-          a[y + 1] = a[y];
-          y--;
+// The rebuild kernels run on a fixed grid and visit only the map blocks of
+// systems whose rebuild flag is set: CTA x takes blocks x, x + gridDim.x, ...
+// of each flagged system in turn.  A rebuild of one system in a large batch
+// then costs that system's work, not a launch of every system's blocks.
+template <class F>
+__device__ __forceinline__ void for_rebuild_blocks(const Arena& A, const BlockMap& M, const int* sys, int nsys,
+                                                   bool cells, F body) {
+  for (int q = 0; q < nsys; q++) {
+    const int s = sys[q];
+    if (s < 0 || !A.st[s].rebuild || A.sys[s].use_cells != cells) continue;  // uniform per CTA
+    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+    for (int b = b0 + (int)blockIdx.x; b < b0 + nb; b += (int)gridDim.x) body(s, b);
+  }
+}
+
+__global__ void k_sort_cells(Arena A, BlockMap C, const int* sys, int nsys) {
+  for_rebuild_blocks(A, C, sys, nsys, true, [&](int s, int b) {
+    const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    const int first = C.first[b], end = C.end[b];
+    for (int c = first + warp; c < end; c += BLOCK / 32) {  // C: 8 cells per block
+      int start = A.chunk_sum[c >> 8] + A.cell_loc[c];
+      int n = A.cell_n[c];
+      if (ln == 0) A.cell_start[c] = start;
+      int* a = A.cell_atoms + start;
+      if (n <= 64) {
+        int v0 = ln < n ? a[ln] : -1;
+        int v1 = ln + 32 < n ? a[ln + 32] : -1;
+        int r0 = 0, r1 = 0;
+        for (int k = 0; k < 32; k++) {
+          int w0 = __shfl_sync(0xffffffffu, v0, k);
+          int w1 = __shfl_sync(0xffffffffu, v1, k);
+          r0 += (w0 > v0) + (w1 > v0);
+          r1 += (w0 > v1) + (w1 > v1);
         }
-        a[y + 1] = v;
+        __syncwarp();
+        if (ln < n) a[r0] = v0;
+        if (ln + 32 < n) a[r1] = v1;
+      } else if (ln == 0) {
+        for (int x = 1; x < n; x++) {
+          int v = a[x];
+          int y = x - 1;
+          while (y >= 0 && a[y] < v) {
+            a[y + 1] = a[y];
+            y--;
+          }
+          a[y + 1] = v;
+        }
       }
     }
-  }
+    });
 }
 
 // ------------------------------------------------------------------ lists
@@ -444,140 +458,166 @@ __device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
 // linkedcell_self / linkedcell_selfhalf (src/Neighbour.F90:991-1161): the
 // 27 (or 14) stencil cells in the reference's order with periodic cell
 // wrap (cell_pbc, :1350-1376); keep j if rd < (rcut+nb_dcut)^2 (strict).
-// One warp per atom: the lanes test one cell's candidates at once and a
-// ballot keeps the accepted ones in candidate order, so the list comes out
-// in the reference's order.  The block's lists are staged in shared memory
-// (LIST_ATOMS atoms x lcap) and written out as coalesced column rows.
-constexpr int LIST_ATOMS = BLOCK / 32;
-
-// dynamic shared memory of k_list_cells: ids and distances of the staged lists
+// For every atom of a cell the candidates are the same sequence: the
+// stencil cells of that cell in stencil order, each in its chain order.  So
+// one CTA takes one cell: it stages that sequence in shared memory
+// (LIST_TILE candidates at a time) and its warps test the cell's atoms
+// against it, one atom per warp; the lanes test 32 consecutive candidates
+// and a ballot keeps the accepted ones in candidate order, so each list
+// comes out in the reference's order.  A warp stages its atom's row (ids
+// and distances), then writes it to `list` as it is and to `flist` ranked
+// by distance.
+constexpr int LIST_ATOMS = BLOCK / 32;  // atoms per pass: one per warp
+constexpr int LIST_TILE = 1024;         // candidates staged at a time
 __host__ __device__ constexpr size_t list_smem(int lcap) {
-  return (size_t)LIST_ATOMS * lcap * (sizeof(int) + sizeof(float));
+  return (size_t)LIST_TILE * (sizeof(double4) + sizeof(int)) +
+         (size_t)LIST_ATOMS * lcap * (sizeof(int) + sizeof(float));
 }
 
-__global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap M) {
-  int s = blk_sys(M);
-  if (s < 0) return;  // padding block of a fixed-capacity map
-  const SysDev& S = A.sys[s];
-  if (!A.st[s].rebuild || !S.use_cells) return;
-  extern __shared__ int stage[];  // [LIST_ATOMS][lcap] ids, then [LIST_ATOMS][lcap] distances
-  float* stage_rd = reinterpret_cast<float*>(stage + LIST_ATOMS * A.lcap);
+__global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, const int* sys, int nsys) {
+  extern __shared__ __align__(32) unsigned char list_sh[];
+  double4* cpos = reinterpret_cast<double4*>(list_sh);                      // LIST_TILE positions
+  int* cidx = reinterpret_cast<int*>(cpos + LIST_TILE);                     // LIST_TILE atom ids
+  int* stage = cidx + LIST_TILE;                                            // LIST_ATOMS x lcap ids
+  float* stage_rd = reinterpret_cast<float*>(stage + LIST_ATOMS * A.lcap);  // and their rd
+  __shared__ int nb_start[27], nb_cnt[27], nb_pref[28];
   const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
-  const int i0 = M.first[blockIdx.x];
-  const int i = i0 + warp;
-  const bool act = i < M.end[blockIdx.x];
-  int m = 0;
-  if (act) {
-    const double4 xi = A.pos[i];
-    int c = A.cell_of[i] - S.cell_off;
-    int cx = c % S.nc[0], cy = (c / S.nc[0]) % S.nc[1], cz = c / (S.nc[0] * S.nc[1]);
+  // every cell of every flagged system, spread over the grid one cell per CTA
+  for (int qs = 0; qs < nsys; qs++) {
+    const int s = sys[qs];
+    if (s < 0 || !A.st[s].rebuild || !A.sys[s].use_cells) continue;  // uniform per CTA
+    const SysDev& S = A.sys[s];
     const int nst = S.half ? 14 : 27;
-    int* row = stage + warp * A.lcap;
-    float* rrow = stage_rd + warp * A.lcap;
-    for (int k = 0; k < nst; k++) {
-      int dx, dy, dz;
-      stencil(k, dx, dy, dz);
-      int x = (cx + dx + S.nc[0]) % S.nc[0];
-      int y = (cy + dy + S.nc[1]) % S.nc[1];
-      int z = (cz + dz + S.nc[2]) % S.nc[2];
-      int cid = S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
-      int beg = A.cell_start[cid], cnt = A.cell_n[cid];
-      int t0 = 0;
-      if (S.half && k == 0) {
-        // same cell: only atoms after i in the chain (smaller indices)
-        int pos_i = cnt;
-        for (int base = 0; base < cnt; base += 32) {
-          int t = base + ln;
-          unsigned b = __ballot_sync(0xffffffffu, t < cnt && A.cell_atoms[beg + t] == i);
-          if (b) pos_i = min(pos_i, base + __ffs(b) - 1);
-        }
-        t0 = pos_i + 1;
+    for (int c = S.cell_off + (int)blockIdx.x; c < S.cell_off + S.ncell; c += (int)gridDim.x) {
+      const int cnt0 = A.cell_n[c];
+      if (cnt0 == 0) continue;  // uniform per CTA
+      const int cl = c - S.cell_off;
+      const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
+      if ((int)threadIdx.x < nst) {
+        int dx, dy, dz;
+        stencil(threadIdx.x, dx, dy, dz);
+        const int x = (cx + dx + S.nc[0]) % S.nc[0];
+        const int y = (cy + dy + S.nc[1]) % S.nc[1];
+        const int z = (cz + dz + S.nc[2]) % S.nc[2];
+        const int cid = S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
+        nb_start[threadIdx.x] = A.cell_start[cid];
+        nb_cnt[threadIdx.x] = A.cell_n[cid];
       }
-      for (int t = t0; t < cnt; t += 32) {
-        int tt = t + ln;
-        bool ok = false;
-        int j = -1;
-        double rd = 0.0;
-        if (tt < cnt) {
-          j = A.cell_atoms[beg + tt];
-          if (j != i) {
-            rd = rd_exact(S, xi, A.pos[j]);
-            ok = rd < S.rlist2;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < nst; k++) {
+          nb_pref[k] = acc;
+          acc += nb_cnt[k];
+        }
+        nb_pref[nst] = acc;
+      }
+      __syncthreads();
+      const int T = nb_pref[nst];     // candidates of every atom of the cell
+      const int own = nb_pref[1];     // the first cell of the stencil is the cell itself
+      const int beg0 = nb_start[0];
+      for (int a0 = 0; a0 < cnt0; a0 += LIST_ATOMS) {
+        const int a = a0 + warp;      // this warp's atom: chain position a of the cell
+        const bool act = a < cnt0;
+        const int i = act ? A.cell_atoms[beg0 + a] : -1;
+        const double4 xi = act ? A.pos[i] : make_double4(0, 0, 0, 0);
+        int* row = stage + warp * A.lcap;
+        float* rrow = stage_rd + warp * A.lcap;
+        int m = 0;
+        for (int t0 = 0; t0 < T; t0 += LIST_TILE) {
+          const int tn = min(LIST_TILE, T - t0);
+          if (T > LIST_TILE || a0 == 0) {  // one tile stays staged for all the cell's atoms
+            __syncthreads();
+            for (int q = threadIdx.x; q < tn; q += BLOCK) {
+              const int g = t0 + q;
+              int k = 0;
+              while (nb_pref[k + 1] <= g) k++;
+              const int j = A.cell_atoms[nb_start[k] + (g - nb_pref[k])];
+              cidx[q] = j;
+              cpos[q] = A.pos[j];
+            }
+            __syncthreads();
+          }
+          for (int q0 = 0; q0 < tn; q0 += 32) {
+            const int q = q0 + ln;
+            bool ok = false;
+            int j = -1;
+            double rd = 0.0;
+            if (act && q < tn) {
+              const int g = t0 + q;
+              j = cidx[q];
+              // half lists take only the atoms after i in its own cell's chain
+              const bool skip = (S.half && g < own) ? (g <= a) : (j == i);
+              if (!skip) {
+                rd = rd_exact(S, xi, cpos[q]);
+                ok = rd < S.rlist2;
+              }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+              const int mm = m + __popc(bal & ((1u << ln) - 1u));
+              if (mm < A.lcap) {
+                row[mm] = j;
+                rrow[mm] = (float)rd;
+              }
+            }
+            m += __popc(bal);
           }
         }
-        unsigned b = __ballot_sync(0xffffffffu, ok);
-        if (ok) {
-          int mm = m + __popc(b & ((1u << ln) - 1u));
-          if (mm < A.lcap) {
-            row[mm] = j;
-            rrow[mm] = (float)rd;
+        __syncwarp();
+        if (act) {
+          const int n = min(m, A.lcap);
+          for (int e = ln; e < n; e += 32) {
+            A.list[(size_t)e * A.cap + i] = row[e];
+            // force order: rank by distance, ties by slot
+            const float re = rrow[e];
+            int rank = 0;
+            for (int f = 0; f < n; f++) {
+              const float rf = rrow[f];
+              rank += (rf < re) || (rf == re && f < e);
+            }
+            A.flist[(size_t)rank * A.cap + i] = row[e];
           }
+          if (ln == 0) list_done(A, s, i, m);
         }
-        m += __popc(b);
+        __syncwarp();
       }
+      __syncthreads();  // nb_* and the tile are rewritten for the next cell
     }
   }
-  __syncthreads();
-  __shared__ int cnt_sh[LIST_ATOMS];
-  if (ln == 0) cnt_sh[warp] = act ? min(m, A.lcap) : 0;
-  __syncthreads();
-  int mx = 0;
-  for (int w = 0; w < LIST_ATOMS; w++) mx = max(mx, cnt_sh[w]);
-  // reference order, written out as coalesced column rows
-  for (int e = threadIdx.x; e < mx * LIST_ATOMS; e += BLOCK) {
-    int mm = e / LIST_ATOMS, w = e % LIST_ATOMS;
-    int ii = i0 + w;
-    if (ii < M.end[blockIdx.x] && mm < cnt_sh[w]) A.list[(size_t)mm * A.cap + ii] = stage[w * A.lcap + mm];
-  }
-  // force order: each warp ranks its atom's entries by distance (ties by slot)
-  if (act) {
-    const int n = cnt_sh[warp];
-    const int* row = stage + warp * A.lcap;
-    const float* rrow = stage_rd + warp * A.lcap;
-    for (int e = ln; e < n; e += 32) {
-      const float re = rrow[e];
-      int rank = 0;
-      for (int f = 0; f < n; f++) {
-        float rf = rrow[f];
-        rank += (rf < re) || (rf == re && f < e);
-      }
-      A.flist[(size_t)rank * A.cap + i] = row[e];
-    }
-  }
-  if (act && ln == 0) list_done(A, s, i, m);
 }
 
 // verlet_self / verlet_selfhalf (src/Neighbour.F90:676-811): O(N^2) over the
 // system in increasing index, keep j if rd <= (rcut+nb_dcut)^2.  Candidate
 // positions are staged through shared memory one BLOCK-wide tile at a time.
-__global__ void k_list_n2(Arena A, BlockMap M) {
-  int s = blk_sys(M);
-  if (s < 0) return;  // padding block of a fixed-capacity map
-  const SysDev& S = A.sys[s];
-  if (!A.st[s].rebuild || S.use_cells) return;
+__global__ void k_list_n2(Arena A, BlockMap M, const int* sys, int nsys) {
   __shared__ double4 tile[BLOCK];
-  int i = M.first[blockIdx.x] + threadIdx.x;
-  bool act = i < M.end[blockIdx.x];
-  double4 xi = act ? A.pos[i] : make_double4(0, 0, 0, 0);
-  int m = 0;
-  const int j0 = S.off, j1 = S.off + S.n;
-  for (int base = j0; base < j1; base += BLOCK) {
-    int j = base + threadIdx.x;
-    __syncthreads();
-    if (j < j1) tile[threadIdx.x] = A.pos[j];
-    __syncthreads();
-    int nt = min(BLOCK, j1 - base);
-    if (act) {
-      for (int t = 0; t < nt; t++) {
-        int jj = base + t;
-        if (S.half ? (jj <= i) : (jj == i)) continue;
-        double rd = rd_exact(S, xi, tile[t]);
-        if (rd > S.rlist2) continue;
-        list_put(A, i, m++, jj);
+  for_rebuild_blocks(A, M, sys, nsys, false, [&](int s, int b) {
+    const SysDev& S = A.sys[s];
+    int i = M.first[b] + threadIdx.x;
+    bool act = i < M.end[b];
+    double4 xi = act ? A.pos[i] : make_double4(0, 0, 0, 0);
+    int m = 0;
+    const int j0 = S.off, j1 = S.off + S.n;
+    for (int base = j0; base < j1; base += BLOCK) {
+      int j = base + threadIdx.x;
+      __syncthreads();
+      if (j < j1) tile[threadIdx.x] = A.pos[j];
+      __syncthreads();
+      int nt = min(BLOCK, j1 - base);
+      if (act) {
+        for (int t = 0; t < nt; t++) {
+          int jj = base + t;
+          if (S.half ? (jj <= i) : (jj == i)) continue;
+          double rd = rd_exact(S, xi, tile[t]);
+          if (rd > S.rlist2) continue;
+          list_put(A, i, m++, jj);
+        }
       }
     }
-  }
-  if (act) list_done(A, s, i, m);
+    if (act) list_done(A, s, i, m);
+    __syncthreads();  // the tile is reused by the next block
+  });
 }
 
 // rebuild counters; in_graph marks the copy captured inside a conditional

@@ -82,6 +82,8 @@ _SIGS = {
     "gemsgpu_replica_exchange": (_i, [_p, _i, _ip, _dp, _i, ctypes.c_uint64, _dp, _ip]),
     "gemsgpu_lbfgs": (_i, [_p, _i, _i, _d, _d, _i, _ip, _ip, _ip, _dp]),
     "gemsgpu_batch_lbfgs": (_i, [_p, _ip, _i, _i, _d, _d, _i, _ip, _ip, _ip, _dp]),
+    "gemsgpu_batch_set_state": (_i, [_p, _ip, _i, _p, _p]),
+    "gemsgpu_batch_get_state": (_i, [_p, _ip, _i, _p, _p, _dp, _dp, _dp]),
     "gemsgpu_neb": (_i, [_p, _ip, _i, _ip, _i, _d, _i, _dp, _dp]),
     "gemsgpu_remd_decide": (_i, [_i, _dp, _dp, _i, ctypes.c_uint64, _dp, _ip, _ip]),
     "gemsgpu_retemper": (_i, [_p, _i, _ip, _dp]),
@@ -221,6 +223,45 @@ class Context:
         self.check(lib().gemsgpu_neb(self.h, _ptr(ids, ctypes.c_int), len(ids), _ptr(fx, ctypes.c_int), len(fx),
                                      float(k_ev), int(iters), ctypes.byref(dt), _ptr(e)))
         return dt.value, e
+
+    @staticmethod
+    def _ptrs(arrays, n):
+        if arrays is None:
+            return None
+        out = (ctypes.c_void_p * n)()
+        for k, a in enumerate(arrays):
+            if a is not None:
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]):
+                    raise TypeError("state arrays must be C-contiguous float64 numpy arrays")
+                out[k] = a.ctypes.data
+        return out
+
+    def batch_set_state(self, systems, pos=None, vel=None):
+        """Upload positions and/or velocities (lists of (n, 3) or 3n float64
+        arrays, entries may be None) of many systems with one synchronisation."""
+        ids = self._ids(systems)
+        for arrs in (pos, vel):
+            if arrs is not None:
+                for s, a in zip(systems, arrs):
+                    if a is not None and a.size != 3 * s.n:
+                        raise ValueError("system %d needs %d values" % (s.sid, 3 * s.n))
+        self.check(lib().gemsgpu_batch_set_state(self.h, _ptr(ids, ctypes.c_int), len(ids),
+                                                 self._ptrs(pos, len(ids)), self._ptrs(vel, len(ids))))
+
+    def batch_get_state(self, systems, pos=None, vel=None):
+        """Download positions and/or velocities into the given arrays (as in
+        batch_set_state) and return (epot_ev, ekin_ev, temp) per system."""
+        ids = self._ids(systems)
+        n = len(ids)
+        for arrs in (pos, vel):
+            if arrs is not None:
+                for s, a in zip(systems, arrs):
+                    if a is not None and a.size != 3 * s.n:
+                        raise ValueError("system %d needs %d values" % (s.sid, 3 * s.n))
+        ep, ek, t = np.zeros(n), np.zeros(n), np.zeros(n)
+        self.check(lib().gemsgpu_batch_get_state(self.h, _ptr(ids, ctypes.c_int), n, self._ptrs(pos, n),
+                                                 self._ptrs(vel, n), _ptr(ep), _ptr(ek), _ptr(t)))
+        return ep, ek, t
 
     def retemper(self, systems, temps):
         """New Ermak temperatures, velocities rescaled by sqrt(T_new/T_old)."""

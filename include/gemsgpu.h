@@ -215,6 +215,20 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys,
 /* Energies of nsys systems (arrays of nsys; any may be NULL). */
 int gemsgpu_batch_energy(gemsgpu_ctx* ctx, const int* sys, int nsys,
                          double* epot_ev, double* ekin_ev, double* temp);
+/* Positions and/or velocities of nsys systems in one call (the state
+ * hand-off of group_switch_vectorial, src/Groups.F90:553-585, for a whole
+ * batch): pos[k] / vel[k] are interleaved xyz host arrays of system k (the
+ * pointer arrays or any entry may be NULL).  All copies are queued together
+ * and the call synchronises once; with page-locked host arrays the copies
+ * run at the link's DMA speed.  Setting positions makes the next force
+ * call test the skin, as gemsgpu_set_positions does. */
+int gemsgpu_batch_set_state(gemsgpu_ctx* ctx, const int* sys, int nsys,
+                            const double* const* pos, const double* const* vel);
+/* The reverse, plus the energies of gemsgpu_batch_energy (any output may be
+ * NULL). */
+int gemsgpu_batch_get_state(gemsgpu_ctx* ctx, const int* sys, int nsys,
+                            double* const* pos, double* const* vel,
+                            double* epot_ev, double* ekin_ev, double* temp);
 
 /* ------------------------------------------------------------ minimisation */
 

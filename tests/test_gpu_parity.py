@@ -311,6 +311,48 @@ def test_md_steps_equals_stepwise(ctx, integ, prec):
         g.destroy()
 
 
+def test_batch_state_transfer_equals_per_system_calls(ctx):
+    """gemsgpu_batch_set_state / _get_state move the same bytes as the
+    per-system calls, and a run after a batched upload equals one after
+    per-system uploads."""
+    from gems_b200 import workloads as W
+    sm, m = W.SMATB["Au"], W.MASS["Au"]
+    cl = [W.cluster(n, np.random.default_rng(n)) for n in (40, 200, 90)]
+    rng = np.random.default_rng(1)
+    runs = []
+    for batched in (False, True):
+        ss = []
+        for p in cl:
+            g = gems.System(np.zeros_like(p), m, ctx=ctx)
+            g.set_smatb(*sm)
+            g.set_ermak(0.002, 1.0, 400.0, seed=3)
+            ss.append(g)
+        vel = [W.maxwell(len(p), m, 400.0, np.random.default_rng(len(p))) for p in cl]
+        if batched:
+            ctx.batch_set_state(ss, [np.ascontiguousarray(p) for p in cl], [np.ascontiguousarray(v) for v in vel])
+        else:
+            for g, p, v in zip(ss, cl, vel):
+                g.set_pos(p)
+                g.set_vel(v)
+        for g, p, v in zip(ss, cl, vel):
+            np.testing.assert_array_equal(g.pos, p)
+            np.testing.assert_array_equal(g.vel, v)
+        ctx.batch_md_steps(ss, 60)
+        pos_out = [np.empty(3 * g.n) for g in ss]
+        vel_out = [np.empty(3 * g.n) for g in ss]
+        ep, ek, t = ctx.batch_get_state(ss, pos_out, vel_out)
+        e_ref = ctx.batch_energy(ss)
+        for g, po, vo in zip(ss, pos_out, vel_out):
+            np.testing.assert_array_equal(po.reshape(-1, 3), g.pos)
+            np.testing.assert_array_equal(vo.reshape(-1, 3), g.vel)
+        np.testing.assert_array_equal(ep, e_ref[0])
+        runs.append(pos_out)
+        for g in ss:
+            g.destroy()
+    for a, b in zip(*runs):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_skin_modes_same_trajectory(ctx):
     """The minimum-image skin test skips the rebuilds that wrapped atoms
     trigger in the reference's test, without changing the dynamics."""
