@@ -642,11 +642,12 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
 int rebuild_grid(const gemsgpu_ctx* ctx, int nblk) { return std::max(1, std::min(nblk, 8 * ctx->nsm)); }
 
 int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 0) {
-  BlockMap ma, mc, mc8;
+  BlockMap ma, mc, mc8, mc1;
   const int* sa;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
   CHK(get_map(ctx, ss, 256, 1, &mc));
   CHK(get_map(ctx, ss, BLOCK / 32, 1, &mc8));
+  CHK(get_map(ctx, ss, 1, 1, &mc1));
   CHK(sys_array(ctx, ss, &sa));
   cudaStream_t st = ctx->stream;
   const Arena& A = ctx->A;
@@ -658,12 +659,12 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 
     k_scan1<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
     k_scan2<<<(int)ss.size(), BLOCK, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
     k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
-    const int ns = (int)ss.size();
-    k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8, sa, ns); ++ctx->launches;
-    k_list_cells<<<4 * ctx->nsm, BLOCK, list_smem(A.lcap), st>>>(A, sa, ns); ++ctx->launches;
+    k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
+    k_list_cells<<<rebuild_grid(ctx, mc1.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc1);
+    ++ctx->launches;
   }
   if (n2) {
-    k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma, sa, (int)ss.size()); ++ctx->launches;
+    k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   }
   k_count_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, st>>>(A, sa, (int)ss.size(), in_graph); ++ctx->launches;
   CU(cudaGetLastError());
@@ -959,6 +960,7 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
     CHK(get_map(ctx, ss, BLOCK, 0, &m));
     CHK(get_map(ctx, ss, 256, 1, &m));
     CHK(get_map(ctx, ss, BLOCK / 32, 1, &m));
+    CHK(get_map(ctx, ss, 1, 1, &m));
     CHK(sys_array(ctx, ss, &sa));
     std::map<std::tuple<int, int, int>, std::vector<int>> groups;
     for (int s : ss) {
@@ -1222,10 +1224,10 @@ int pool_rebuild(gemsgpu_pool* P, int in_graph) {
   k_scan1<<<mc.nblk, BLOCK, 0, st>>>(A, mc); ++ctx->launches;
   k_scan2<<<ns, BLOCK, 0, st>>>(A, P->dsys, ns); ++ctx->launches;
   k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
-  k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8, P->dsys, ns); ++ctx->launches;
-  k_list_cells<<<4 * ctx->nsm, BLOCK, list_smem(A.lcap), st>>>(A, P->dsys, ns);
+  k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
+  k_list_cells<<<rebuild_grid(ctx, mc8.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc8);
   ++ctx->launches;
-  k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma, P->dsys, ns); ++ctx->launches;
+  k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   k_count_rebuild<<<(ns + 255) / 256, 256, 0, st>>>(A, P->dsys, ns, in_graph); ++ctx->launches;
   CU(cudaGetLastError());
   return 0;

@@ -388,23 +388,38 @@ __global__ void k_scatter(Arena A, BlockMap M) {
 // is built by inserting atoms in increasing index order.  Each lane ranks
 // its atom(s) against the whole cell (cells of up to 64 atoms); larger cells
 // fall back to an insertion sort by one lane.
-// The rebuild kernels run on a fixed grid and visit only the map blocks of
-// systems whose rebuild flag is set: CTA x takes blocks x, x + gridDim.x, ...
-// of each flagged system in turn.  A rebuild of one system in a large batch
-// then costs that system's work, not a launch of every system's blocks.
-template <class F>
-__device__ __forceinline__ void for_rebuild_blocks(const Arena& A, const BlockMap& M, const int* sys, int nsys,
-                                                   bool cells, F body) {
-  for (int q = 0; q < nsys; q++) {
-    const int s = sys[q];
-    if (s < 0 || !A.st[s].rebuild || A.sys[s].use_cells != cells) continue;  // uniform per CTA
-    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
-    for (int b = b0 + (int)blockIdx.x; b < b0 + nb; b += (int)gridDim.x) body(s, b);
+// The rebuild kernels run on a fixed grid.  CTA x owns work items x, x + G,
+// x + 2G, ... (G = gridDim.x, so live items spread evenly over the CTAs); it
+// tests BLOCK of them at once, one per thread, keeps the live ones in shared
+// memory and works through those.  A rebuild of a few systems in a large
+// batch, or of a system with many cells, thus costs its work plus one
+// parallel test per BLOCK items, not a launch or a serial test per item.
+// Items are independent, so the order in which a CTA takes them is free.
+template <class Check, class Body>
+__device__ __forceinline__ void rebuild_items(int nitems, Check live, Body body) {
+  __shared__ int items[BLOCK];
+  __shared__ int nlive;
+  const int G = gridDim.x;
+  for (int base = 0; (int64_t)blockIdx.x + (int64_t)base * G < nitems; base += BLOCK) {
+    const int64_t w = (int64_t)blockIdx.x + (int64_t)(base + threadIdx.x) * G;
+    if (threadIdx.x == 0) nlive = 0;
+    __syncthreads();
+    if (w < nitems && live((int)w)) items[atomicAdd(&nlive, 1)] = (int)w;
+    __syncthreads();
+    const int n = nlive;
+    for (int k = 0; k < n; k++) body(items[k]);
+    __syncthreads();
   }
 }
 
-__global__ void k_sort_cells(Arena A, BlockMap C, const int* sys, int nsys) {
-  for_rebuild_blocks(A, C, sys, nsys, true, [&](int s, int b) {
+// map block b of a system flagged for a rebuild (cells or O(N^2) lists)
+__device__ __forceinline__ bool rebuild_block(const Arena& A, const BlockMap& M, int b, bool cells) {
+  const int s = M.sys[b];
+  return s >= 0 && A.st[s].rebuild && (A.sys[s].use_cells != 0) == cells;
+}
+
+__global__ void k_sort_cells(Arena A, BlockMap C) {
+  rebuild_items(C.nblk, [&](int b) { return rebuild_block(A, C, b, true); }, [&](int b) {
     const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
     const int first = C.first[b], end = C.end[b];
     for (int c = first + warp; c < end; c += BLOCK / 32) {  // C: 8 cells per block
@@ -469,12 +484,13 @@ __device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
 // by distance.
 constexpr int LIST_ATOMS = BLOCK / 32;  // atoms per pass: one per warp
 constexpr int LIST_TILE = 1024;         // candidates staged at a time
+constexpr int LIST_SPLIT = 4;           // CTAs that may share one cell's atoms
 __host__ __device__ constexpr size_t list_smem(int lcap) {
   return (size_t)LIST_TILE * (sizeof(double4) + sizeof(int)) +
          (size_t)LIST_ATOMS * lcap * (sizeof(int) + sizeof(float));
 }
 
-__global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, const int* sys, int nsys) {
+__global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
   extern __shared__ __align__(32) unsigned char list_sh[];
   double4* cpos = reinterpret_cast<double4*>(list_sh);                      // LIST_TILE positions
   int* cidx = reinterpret_cast<int*>(cpos + LIST_TILE);                     // LIST_TILE atom ids
@@ -482,15 +498,26 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, const int* sys, i
   float* stage_rd = reinterpret_cast<float*>(stage + LIST_ATOMS * A.lcap);  // and their rd
   __shared__ int nb_start[27], nb_cnt[27], nb_pref[28];
   const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
-  // every cell of every flagged system, spread over the grid one cell per CTA
-  for (int qs = 0; qs < nsys; qs++) {
-    const int s = sys[qs];
-    if (s < 0 || !A.st[s].rebuild || !A.sys[s].use_cells) continue;  // uniform per CTA
+  // work item w = (map block w % nblk, part w / nblk): the part
+  // takes atom passes part, part + LIST_SPLIT, ... of each of the block's
+  // cells, so a cell of many atoms is shared by up to LIST_SPLIT CTAs
+  // part-major numbering: the live items of sparse cells (part 0) spread
+  // over every CTA whatever the grid size
+  auto live = [&](int w) {
+    const int b = w % C.nblk, part = w / C.nblk;
+    if (!rebuild_block(A, C, b, true)) return false;
+    // one-cell blocks: is there an atom pass for this part?
+    return C.end[b] - C.first[b] != 1 || part * LIST_ATOMS < A.cell_n[C.first[b]];
+  };
+  rebuild_items(C.nblk * LIST_SPLIT, live, [&](int w) {
+    const int b = w % C.nblk, part = w / C.nblk;
+    const int s = C.sys[b];
     const SysDev& S = A.sys[s];
     const int nst = S.half ? 14 : 27;
-    for (int c = S.cell_off + (int)blockIdx.x; c < S.cell_off + S.ncell; c += (int)gridDim.x) {
+    for (int c = C.first[b]; c < C.end[b]; c++) {
       const int cnt0 = A.cell_n[c];
-      if (cnt0 == 0) continue;  // uniform per CTA
+      const int a_first = part * LIST_ATOMS;
+      if (a_first >= cnt0) continue;  // uniform per CTA
       const int cl = c - S.cell_off;
       const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
       if ((int)threadIdx.x < nst) {
@@ -516,7 +543,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, const int* sys, i
       const int T = nb_pref[nst];     // candidates of every atom of the cell
       const int own = nb_pref[1];     // the first cell of the stencil is the cell itself
       const int beg0 = nb_start[0];
-      for (int a0 = 0; a0 < cnt0; a0 += LIST_ATOMS) {
+      for (int a0 = a_first; a0 < cnt0; a0 += LIST_ATOMS * LIST_SPLIT) {
         const int a = a0 + warp;      // this warp's atom: chain position a of the cell
         const bool act = a < cnt0;
         const int i = act ? A.cell_atoms[beg0 + a] : -1;
@@ -526,7 +553,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, const int* sys, i
         int m = 0;
         for (int t0 = 0; t0 < T; t0 += LIST_TILE) {
           const int tn = min(LIST_TILE, T - t0);
-          if (T > LIST_TILE || a0 == 0) {  // one tile stays staged for all the cell's atoms
+          if (T > LIST_TILE || a0 == a_first) {  // one tile stays staged for all this CTA's passes
             __syncthreads();
             for (int q = threadIdx.x; q < tn; q += BLOCK) {
               const int g = t0 + q;
@@ -584,15 +611,16 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, const int* sys, i
       }
       __syncthreads();  // nb_* and the tile are rewritten for the next cell
     }
-  }
+  });
 }
 
 // verlet_self / verlet_selfhalf (src/Neighbour.F90:676-811): O(N^2) over the
 // system in increasing index, keep j if rd <= (rcut+nb_dcut)^2.  Candidate
 // positions are staged through shared memory one BLOCK-wide tile at a time.
-__global__ void k_list_n2(Arena A, BlockMap M, const int* sys, int nsys) {
+__global__ void k_list_n2(Arena A, BlockMap M) {
   __shared__ double4 tile[BLOCK];
-  for_rebuild_blocks(A, M, sys, nsys, false, [&](int s, int b) {
+  rebuild_items(M.nblk, [&](int b) { return rebuild_block(A, M, b, false); }, [&](int b) {
+    const int s = M.sys[b];
     const SysDev& S = A.sys[s];
     int i = M.first[b] + threadIdx.x;
     bool act = i < M.end[b];
