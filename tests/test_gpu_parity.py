@@ -91,6 +91,41 @@ def test_list_cells_pbc_32k(ctx, half):
     compare_lists(o, g)
 
 
+def test_list_cells_batch_rebuild(ctx):
+    """A batch of periodic cell-list systems rebuilt together (the force
+    rebuild of a kernel timing call, then md steps that rebuild each system
+    at its own time): every system's list equals the oracle's, entry by
+    entry, at its own positions."""
+    from gems_b200 import workloads as W
+    ss, os_ = [], []
+    for k in range(4):
+        w = W.smatb_bulk(seed=40 + k, ncell=8)
+
+        def setup(s, w=w):
+            s.set_box(w["L"], (True, True, True))
+            s.set_smatb(*w["smatb"])
+        o, g = both(w["pos"], w["mass"], ctx, setup=setup)
+        g.set_ermak(0.002, 1.0, 900.0 + 100 * k, seed=7 + k)
+        g.interact()
+        ss.append(g)
+        os_.append(o)
+    ctx.batch_time_kernels(ss, 1)          # forces a rebuild of all four
+    for o, g in zip(os_, ss):
+        o.set_pos(g.pos)
+        o.update()
+        compare_lists(o, g)
+    n0 = [g.nupd for g in ss]
+    ctx.batch_md_steps(ss, 400)            # hot: each rebuilds on its own skin test
+    assert all(g.nupd > n for g, n in zip(ss, n0))
+    ctx.batch_time_kernels(ss, 1)
+    for o, g in zip(os_, ss):
+        o.set_pos(g.pos)
+        o.update()
+        compare_lists(o, g)
+    for g in ss:
+        g.destroy()
+
+
 @pytest.mark.parametrize("half", [False, True])
 def test_list_n2_mic(ctx, half):
     """readxyz.gms geometry: rc+skin > box/2, O(N^2) list with minimum image."""
