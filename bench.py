@@ -159,15 +159,15 @@ def make_system(gems, ctx, w, prec, seed, tune=None, therm=THERM_STEPS):
     s.set_precision(prec)
     s.set_ermak(w["dt"], w["gamma"], w["temp"], seed=seed)
     s.interact()
-    if therm:
-        s.md_steps(therm)
     if tune is None and FIXED_TUNE is not None:
         tune = FIXED_TUNE
-    if tune is None:
-        s.tuned = s.autotune(10)
-    else:
+    if tune is not None:
         s.set_lanes(tune[0], tune[1])
         s.tuned = tune
+    if therm:
+        s.md_steps(therm)
+    if tune is None:
+        s.tuned = s.autotune(10)
     return s
 
 
