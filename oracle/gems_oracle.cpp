@@ -109,8 +109,8 @@ void rang(Lcg& s, double* r1, double* r2) {  // always draws a pair
 }
 
 // ---------------------------------------------------------------- system
-enum FF { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
-enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3 };
+enum FF { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3, FF_SLJ = 4 };
+enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4 };
 const int MAXT = 8;
 
 // 27-cell stencil in the reference's order (Neighbour.F90:75-83): 0 is the
@@ -129,6 +129,11 @@ struct LJp {
   bool shifted_force = false;  // plj (Pairs.F90:282-370)
   double prc = 0, frc = 0;
   double eshift = 0;           // constant energy shift per pair (eV)
+};
+
+struct SLJp {  // slj (Pairs.F90:374-401): LJ with a splined tail from rs to rc
+  bool on = false;
+  double e = 0, s = 0, rs = 0, rc = 0, rc2 = 0, sa4 = 0, sa8 = 0;
 };
 
 struct SMp {  // TB.F90:66-102 per type pair
@@ -167,7 +172,9 @@ struct Sys {
   int ff = FF_NONE;
   int ntypes = 1;
   LJp lj[MAXT][MAXT];
+  SLJp slj[MAXT][MAXT];
   SMp sm[MAXT][MAXT];
+  double virial[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // pair virial of the last interact (internal units)
   TSp ts;
   double rcut = 0;  // intergroup rcut (max over pairs)
   std::vector<double> band, eband;
@@ -178,6 +185,11 @@ struct Sys {
          skt = 0, gama = 0, temp = 0;
   Lcg* rng = nullptr;
   const double* ext_normals = nullptr;  // optional external normal stream
+  // G-JF constant-pressure state (set_lgf, Integration.F90:486-525)
+  double lgf_fac0 = 0, lgf_facg0 = 0, lgf_kinetic = 0, lgf_press = 0, lgf_inv_pmass = 0, lgf_bv = 0,
+         lgf_facv = 0, lgf_av = 0, lgf_rangv = 0, pvel = 0, pistonf = 0;
+  bool lgf_first = true;
+  int ext_used = 0;  // normals of the external stream used this step
   // FIRE state
   double fire_dt = 0, fire_dtmax = 0, fire_alpha = 0.1;
   int fire_np = 0;
@@ -406,6 +418,72 @@ double lj_interact(Sys& s) {
     s.force[3 * i + 2] += fz;
     s.epot[i] += ep;
   }
+  return etot;
+}
+
+// slj_set (Pairs.F90:374-401): cut-off and spline coefficients
+void slj_set(SLJp& P, double e, double sg, double rs) {
+  P.on = true;
+  P.e = e;
+  P.s = sg;
+  P.rs = rs;
+  const double s_dr = pow6(sg / rs);
+  const double urs = 4.0 * e * (s_dr * s_dr - s_dr);
+  const double dudrs = -e * (48.0 * s_dr - 24.0) * s_dr / rs;
+  P.rc = rs - 32.0 * urs / (11.0 * dudrs);
+  P.rc2 = P.rc * P.rc;
+  const double d = P.rc - rs;
+  P.sa4 = (8.0 * urs + d * dudrs) / (4 * (d * d * d * d));
+  P.sa8 = -(4.0 * urs + d * dudrs) / (4 * (d * d * d * d * d * d * d * d));
+}
+
+// slj_interact (Pairs.F90:403-470) over the full list, with the pair virial
+// W = sum_i r_i (x) F_i, which with minimum image is 1/2 sum over the
+// ordered pairs of vd (x) factor2 (vd = r_j - r_i): the virial the reference
+// builds from local and ghost atoms (inq_virial, Inq_Properties.F90:439-527)
+double slj_interact(Sys& s) {
+  double etot = 0.0;
+  const int n = s.n;
+  double W[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < n; i++) {
+    int ti = s.type[i];
+    double fx = 0, fy = 0, fz = 0, ep = 0;
+    for (int l = 0; l < s.nn[i]; l++) {
+      int j = s.list[(size_t)l * n + i];
+      const SLJp& P = s.slj[ti][s.type[j]];
+      if (!P.on) continue;
+      double vd[3];
+      vdist(s, j, i, vd);
+      double dr = dot3(vd);
+      if (dr > P.rc2) continue;
+      dr = std::sqrt(dr);
+      double p, f;
+      if (dr < P.rs) {
+        const double s_dr = pow6(P.s / dr);
+        p = 4.0 * P.e * (s_dr - 1.0) * s_dr;
+        f = P.e * (48.0 * s_dr - 24.0) * s_dr / dr;
+      } else {
+        const double s4 = (dr - P.rc) * (dr - P.rc) * (dr - P.rc) * (dr - P.rc);
+        p = P.sa4 * s4 + P.sa8 * s4 * s4;
+        f = -(4.0 * P.sa4 * s4 + 8.0 * P.sa8 * s4 * s4) / (dr - P.rc);
+      }
+      p = p * ev_ui;
+      f = f * ev_ui;
+      ep = ep + p * 0.5;
+      etot = etot + p * 0.5;
+      const double f2[3] = {f * vd[0] / dr, f * vd[1] / dr, f * vd[2] / dr};
+      fx = fx - f2[0];
+      fy = fy - f2[1];
+      fz = fz - f2[2];
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) W[3 * a + b] += 0.5 * vd[a] * f2[b];
+    }
+    s.force[3 * i] += fx;
+    s.force[3 * i + 1] += fy;
+    s.force[3 * i + 2] += fz;
+    s.epot[i] += ep;
+  }
+  for (int k = 0; k < 9; k++) s.virial[k] = W[k];
   return etot;
 }
 
@@ -655,6 +733,7 @@ double interact(Sys& s, bool* rebuilt) {
   if (s.ff == FF_LJ) e = lj_interact(s);
   else if (s.ff == FF_SMATB) e = smatb_interact(s);
   else if (s.ff == FF_TERSOFF) e = tersoff_interact(s);
+  else if (s.ff == FF_SLJ) e = slj_interact(s);
   s.last_epot = e;
   return e;
 }
@@ -837,17 +916,121 @@ double fmax_ev(const Sys& s) {
   return m * ui_ev;
 }
 
+// ------------------------------------------------------------------ G-JF NPT
+// Constant pressure and temperature Langevin dynamics of Gronbech-Jensen &
+// Farago (J. Chem. Phys. 141, 194108, 2014) as set_lgf / lgf_stepa /
+// lgf_stepb state it (Integration.F90:486-650): an isotropic piston on the
+// box volume with friction pgamav and mass pmass, particles with friction
+// pgama0, target pressure press (internal units) and temperature temp.
+// Noise: one rang pair for the piston, then one per atom and coordinate, of
+// which the first value is used (rang, Random.F90:213-226).
+const double atm_ui = 1.01325 * 1.e5 * ((1.0 / (ui_ev * 1.60219e-19)) * 1e-30);  // Constants.F90:186-193
+
+void set_lgf(Sys& s, double dt, double temp, double press, double pgama0, double pgamav, double pmass) {
+  s.integ = IT_LGF;
+  s.dt = dt;
+  s.temp = temp;
+  s.lgf_fac0 = std::sqrt(2.0 * pgama0 * kB_ui * temp * dt);
+  s.lgf_facg0 = 0.5 * dt * pgama0;
+  s.lgf_kinetic = s.n * temp * kB_ui;
+  s.lgf_press = press;
+  s.lgf_inv_pmass = 1.0 / pmass;
+  s.lgf_bv = 1.0 / (1.0 + 0.5 * dt * s.lgf_inv_pmass * pgamav);
+  s.lgf_facv = std::sqrt(2.0 * pgamav * kB_ui * temp * dt);
+  s.lgf_av = (1.0 - 0.5 * dt * s.lgf_inv_pmass * pgamav) * s.lgf_bv;
+  s.lgf_first = true;
+  s.pvel = 0.0;
+  s.pistonf = 0.0;
+  if ((int)s.pos_v.size() < 3 * s.n) s.pos_v.assign(3 * s.n, 0.0);
+}
+
+double lgf_normal(Sys& s, int q) {  // q: 0 = piston, 1 + 3i + k = atom i, coordinate k
+  if (s.ext_normals) return s.ext_normals[2 * q];
+  double r1, r2;
+  rang(*s.rng, &r1, &r2);
+  return r1;
+}
+
+void lgf_a(Sys& s) {
+  const double dt = s.dt;
+  const double vol0 = s.box[0] * s.box[1] * s.box[2];
+  if (s.lgf_first) {
+    s.lgf_first = false;
+    const double sv = (s.virial[0] + s.virial[4] + s.virial[8]) / 3;
+    s.pistonf = (sv + s.lgf_kinetic) / vol0 - s.lgf_press;
+  }
+  // the box volume, then the lengths: L (V/V_old)^(1/3) with the exponent
+  // the single-precision 1./dd of the reference
+  const double rangv = lgf_normal(s, 0) * s.lgf_facv;
+  double vol = vol0 + s.lgf_bv * dt * (s.pvel + 0.5 * s.lgf_inv_pmass * (dt * s.pistonf + rangv));
+  s.lgf_rangv = rangv;
+  double box_old[3];
+  const double expo = (double)(1.0f / 3.0f);
+  for (int k = 0; k < 3; k++) {
+    box_old[k] = s.box[k];
+    s.box[k] = box_old[k] * std::pow(vol / vol0, expo);
+    s.one_box[k] = 1.0 / s.box[k];
+  }
+  for (int i = 0; i < s.n; i++) {
+    const double b0 = 1.0 / (1.0 + s.lgf_facg0 * s.one_mass[i]);
+    for (int k = 0; k < 3; k++) {
+      const int q = 3 * i + k;
+      const double r1 = lgf_normal(s, 1 + q);
+      s.pos_v[q] = s.one_mass[i] * s.lgf_fac0 * r1;
+      s.acel[q] = s.force[q] * s.one_mass[i];
+      s.pos[q] = s.box[k] / box_old[k] * s.pos[q] +
+                 2.0 * s.box[k] / (box_old[k] + s.box[k]) * b0 * dt * (s.vel[q] + 0.5 * dt * s.acel[q] + 0.5 * s.pos_v[q]);
+    }
+  }
+}
+
+void lgf_b(Sys& s) {
+  const double dt = s.dt;
+  const double vol = s.box[0] * s.box[1] * s.box[2];
+  const double sv = (s.virial[0] + s.virial[4] + s.virial[8]) / 3;
+  const double pf_old = s.pistonf;
+  s.pistonf = (sv + s.lgf_kinetic) / vol - s.lgf_press;
+  s.pvel = s.lgf_av * s.pvel + 0.5 * s.lgf_inv_pmass * dt * (s.lgf_av * pf_old + s.pistonf) +
+           s.lgf_bv * s.lgf_inv_pmass * s.lgf_rangv;
+  for (int i = 0; i < s.n; i++) {
+    const double b0 = 1.0 / (1.0 + s.lgf_facg0 * s.one_mass[i]);
+    const double a0 = (1.0 - s.lgf_facg0 * s.one_mass[i]) * b0;
+    for (int k = 0; k < 3; k++) {
+      const int q = 3 * i + k;
+      s.vel[q] = a0 * s.vel[q] + 0.5 * dt * (a0 * s.acel[q] + s.one_mass[i] * s.force[q]) + b0 * s.pos_v[q];
+      s.acel[q] = s.force[q] * s.one_mass[i];
+    }
+  }
+}
+
 void stepa(Sys& s) {
   if (s.integ == IT_VV || s.integ == IT_FIRE) vv_a(s);
   else if (s.integ == IT_ERMAK) ermak_a(s);
+  else if (s.integ == IT_LGF) lgf_a(s);
   do_pbc(s);
 }
 
 void stepb(Sys& s) {
   if (s.integ == IT_VV || s.integ == IT_FIRE) vv_b(s);
   else if (s.integ == IT_ERMAK) ermak_b(s);
+  else if (s.integ == IT_LGF) lgf_b(s);
   do_pbc(s);
   if (s.integ == IT_FIRE) fire_mix(s);
+}
+
+// pressure tensor (inq_pressure, Inq_Properties.F90:529-573) in atm: the
+// kinetic tensor sum m v v plus the virial, over the volume
+void pressure_atm(const Sys& s, double out[9]) {
+  double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < s.n; i++)
+    for (int a = 0; a < 3; a++)
+      for (int b = a; b < 3; b++) K[3 * a + b] += s.vel[3 * i + a] * s.vel[3 * i + b] * s.mass[i];
+  for (int a = 1; a < 3; a++)
+    for (int b = 0; b < a; b++) K[3 * a + b] = K[3 * b + a];
+  const double vol = s.box[0] * s.box[1] * s.box[2];
+  const double ui_pa = 1.0 / ((1.0 / (ui_ev * 1.60219e-19)) * 1e-30);
+  const double ui_atm_out = ui_pa * 1e-5 * (1.0 / 1.01325);  // write_pressure (Output.F90:767-770)
+  for (int k = 0; k < 9; k++) out[k] = (K[k] + s.virial[k]) / vol * ui_atm_out;
 }
 
 // ------------------------------------------------------------------ L-BFGS
@@ -1551,6 +1734,35 @@ int orc_dinamica(void* p, int nsteps, int each, double* rows) {
 int orc_lbfgs(void* p, int m, double eps, double xtol, int itermax, int* iters, int* nfun, double* fmin) {
   return lbfgs_min(*(Sys*)p, m, eps, xtol, itermax, iters, nfun, fmin);
 }
+
+void orc_set_slj(void* p, int ti, int tj, double e, double sg, double rs) {
+  Sys* s = (Sys*)p;
+  s->ff = FF_SLJ;
+  SLJp P;
+  slj_set(P, e, sg, rs);
+  s->slj[ti][tj] = P;
+  s->slj[tj][ti] = P;
+  s->rcut = std::max(s->rcut, P.rc);
+}
+
+// press in atm (the reference reads it with atm_ui, Integration.F90:157-172)
+void orc_set_lgf(void* p, double dt, double temp, double press_atm, double pgama0, double pgamav, double pmass,
+                 void* rng) {
+  Sys* s = (Sys*)p;
+  s->rng = (Lcg*)rng;
+  set_lgf(*s, dt, temp, press_atm * atm_ui, pgama0, pgamav, pmass);
+}
+
+void orc_virial_ev(void* p, double* out9) {
+  Sys* s = (Sys*)p;
+  for (int k = 0; k < 9; k++) out9[k] = s->virial[k] * ui_ev;
+}
+void orc_pressure_atm(void* p, double* out9) { pressure_atm(*(Sys*)p, out9); }
+void orc_get_box(void* p, double* out3) {
+  Sys* s = (Sys*)p;
+  for (int k = 0; k < 3; k++) out3[k] = s->box[k];
+}
+double orc_atm_ui() { return atm_ui; }
 
 double orc_neb(void* p, int nimg, double* pneb, const int* fixed, int nfixed, double k_ev, int iter) {
   return neb_run(*(Sys*)p, nimg, pneb, fixed, nfixed, k_ev, iter);

@@ -90,6 +90,12 @@ def lib():
         "orc_fire_relax": (_i, [_p, _d, _i, _dp]),
         "orc_lbfgs": (_i, [_p, _i, _d, _d, _i, _ip, _ip, _dp]),
         "orc_neb": (_d, [_p, _i, _dp, _ip, _i, _d, _i]),
+        "orc_set_slj": (None, [_p, _i, _i, _d, _d, _d]),
+        "orc_set_lgf": (None, [_p, _d, _d, _d, _d, _d, _d, _p]),
+        "orc_virial_ev": (None, [_p, _dp]),
+        "orc_pressure_atm": (None, [_p, _dp]),
+        "orc_get_box": (None, [_p, _dp]),
+        "orc_atm_ui": (_d, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -368,6 +374,30 @@ class System:
 
     def fmax(self):
         return lib().orc_fmax(self.h)
+
+    def set_slj(self, e, sg, rs, ti=0, tj=0):
+        lib().orc_set_slj(self.h, int(ti), int(tj), float(e), float(sg), float(rs))
+
+    def set_lgf(self, dt, temp, press_atm, pgama0, pgamav, pmass, rng=None):
+        """set_lgf (G-JF constant pressure): press in atm as the deck gives it."""
+        self._rng = rng
+        lib().orc_set_lgf(self.h, float(dt), float(temp), float(press_atm), float(pgama0), float(pgamav),
+                          float(pmass), rng.h if rng is not None else None)
+
+    def virial_ev(self):
+        out = np.zeros(9)
+        lib().orc_virial_ev(self.h, _ptr(out))
+        return out
+
+    def pressure_atm(self):
+        out = np.zeros(9)
+        lib().orc_pressure_atm(self.h, _ptr(out))
+        return out
+
+    def box_now(self):
+        out = np.zeros(3)
+        lib().orc_get_box(self.h, _ptr(out))
+        return out
 
     def neb(self, images, fixed, k_ev, iters):
         """neb_run: images (nimg x n x 3; the fixed ones set) -> (relaxed

@@ -83,7 +83,7 @@ def lj_dimer_deck():
 
 
 # --------------------------------------------------------------- SMA-TB bulk
-def fcc_reply_positions():
+def fcc_reply_positions(times=10):
     """bulk.gms atom order: 4-atom cell then `reply` along x, y, z (10 each).
 
     create_reply (Select_Create.F90:137-165) appends, for every atom of the
@@ -95,7 +95,7 @@ def fcc_reply_positions():
         t = np.array(tras, dtype=np.float64)
         new = []
         for a in sel:
-            for j in range(1, 10):
+            for j in range(1, times):
                 new.append(a + t * j)
         sel = sel + new
     return np.array(sel)
@@ -192,6 +192,57 @@ def neb_rule(ref, got):
     columns over the sum of the first column, < 1e-4."""
     a = ((ref[:, 1] - got[:, 1]) ** 2).sum() + ((ref[:, 0] - got[:, 0]) ** 2).sum()
     return abs(a / ref[:, 0].sum())
+
+
+# --------------------------------------------------------------- NPT
+def npt_lgf_deck():
+    """examples/NPT/lgf.gms: fcc 6^3 (864 atoms of mass 1.008) expanded by
+    sqrt(2) in a 6 sqrt(2) periodic box, moved by 0.2; slj(1 eV, 2^(-1/6) A,
+    rs 1.108683); G-JF constant pressure and temperature (piston_lgf xyz*) at
+    0.3 e0/kB, particle friction 1/tau, piston friction 1e-4/tau, piston mass
+    1e-5, pressure 0.1 e0/r0^3 given in atm; dt = 0.01 tau (tau = 0.01018 ps);
+    100 steps on the LCG stream of seed 123456, a row every 10.  The deck
+    sets `box mic F` (ghost atoms); at this box size the minimum image gives
+    the same interactions and virial."""
+    g = golden()
+    f = math.sqrt(2.0)
+    pos = fcc_reply_positions(6) * f + 0.2
+    tau = 0.01018
+    return dict(pos=pos, mass=MASS["H"], box=(6.0 * f,) * 3, slj=(1.0, 2.0 ** (-1.0 / 6.0), 1.108683),
+                dt=0.01 * tau, temp=0.3 * 11604.45, press_atm=0.1 * 1581225.25240563, pgama0=1.0 / tau,
+                pgamav=0.0001 / tau, pmass=0.00001, nsteps=100, each=10, seed=123456,
+                ref_energy=np.array(g["npt_lgf_energy"]), ref_press=np.array(g["npt_lgf_press"]),
+                ref_virial=np.array(g["npt_lgf_virial"]))
+
+
+def npt_setup(s, d, rng):
+    s.set_box(d["box"], (True, True, True))
+    s.set_slj(*d["slj"])
+    s.set_lgf(d["dt"], d["temp"], d["press_atm"], d["pgama0"], d["pgamav"], d["pmass"], rng)
+
+
+def npt_run(s, d, rng, nsteps=None, each=None, feed=None):
+    """dinamic with per-step rows of (Epot, Ekin, Etot in eV, T), pressure
+    (atm) and virial (eV).  `feed(s, normals)` hands each step's LCG normals
+    to an engine in parity mode (one pair for the piston, then one pair per
+    atom coordinate)."""
+    nsteps = nsteps or d["nsteps"]
+    each = each or d["each"]
+    s.interact()
+    E, P, V = [], [], []
+    for ns in range(1, nsteps + 1):
+        if feed is not None:
+            feed(s, rng.rang_stream(1 + 3 * s.n))
+        s.stepa()
+        s.interact()
+        s.stepb()
+        if ns % each == 0:
+            ek, t = s.kin()
+            ep = s.epot_sum()
+            E.append([ep, ek, ep + ek, t])
+            P.append(s.pressure_atm())
+            V.append(s.virial_ev())
+    return np.array(E), np.array(P), np.array(V)
 
 
 # --------------------------------------------------------------- NVE / NVT

@@ -53,6 +53,9 @@ def main():
         "repex_energy": [rows("examples/RepExchange/ref/Energy.lj.mpi%d.dat" % k) for k in range(4)],
         "neb_gold_cube": xyz_frames("examples/configs/ref/gold_cube.xyz")[0],
         "neb_energy": rows("examples/NEB/ref/Energy.neb.dat.NebF"),
+        "npt_lgf_energy": rows("examples/NPT/ref/Energy.lgf.dat"),
+        "npt_lgf_press": rows("examples/NPT/ref/Press.lgf.dat"),
+        "npt_lgf_virial": rows("examples/NPT/ref/Viri.lgf.dat"),
     }
     with open(OUT, "w") as f:
         json.dump(g, f)

@@ -158,3 +158,20 @@ def test_replica_exchange_four_ranks():
     assert abs(a / b) < 1e-6
     for r, n in zip(ref, rows):
         np.testing.assert_allclose(n, r, atol=1e-7)
+
+
+def test_npt_lgf_slj_piston():
+    """examples/NPT/lgf.gms: slj fcc 6^3 under the G-JF piston, 100 steps,
+    against Energy.lgf.dat, Press.lgf.dat and Viri.lgf.dat (written with 7
+    significant digits)."""
+    d = decks.npt_lgf_deck()
+    s = O.System(d["pos"], d["mass"])
+    rng = O.Rng(d["seed"])
+    decks.npt_setup(s, d, rng)
+    E, P, V = decks.npt_run(s, d, rng)
+    E[:, :3] *= O.UI_EV
+    assert decks.gems_rule(d["ref_energy"][:, 0], E[:, 0]) < 1e-6
+    np.testing.assert_allclose(E, d["ref_energy"], rtol=2e-6)
+    np.testing.assert_allclose(P, d["ref_press"], rtol=2e-6, atol=1e-2)
+    np.testing.assert_allclose(V, d["ref_virial"], rtol=2e-6, atol=1e-6)
+    assert abs(s.box_now()[0] - d["box"][0]) > 1e-3  # the piston moved the box
