@@ -33,15 +33,20 @@ __device__ __forceinline__ void stencil(int k, int& dx, int& dy, int& dz) {
 }
 
 enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
-enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3 };
+enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4 };
 enum PREC : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 
 // status bits of a system (SysState::status)
-enum ST : int { ST_OVERFLOW = 1, ST_LOST = 2, ST_NAN = 4 };
+// ST_BOX: a constant-pressure box shrank below three list cut-offs in a
+// dimension, or its volume collapsed
+enum ST : int { ST_OVERFLOW = 1, ST_LOST = 2, ST_NAN = 4, ST_BOX = 8 };
 
 // Parameters of one species pair.  LJ (Pairs.F90:198-291):
 //   v[0]=e v[1]=s v[2]=rc v[3]=rc2 v[4]=prc v[5]=frc v[6]=eshift
 //   v[7]=shifted_force (0/1)
+// slj, LJ with a splined tail (Pairs.F90:374-470), in the same slots:
+//   v[0]=e v[1]=s v[2]=rc v[3]=rc2 v[8]=1 (slj form) v[9]=sa4 v[10]=sa8
+//   v[11]=rs
 // SMA-TB (TB.F90:106-170):
 //   v[0]=A v[1]=xi v[2]=p v[3]=q v[4]=r0 v[5]=rci v[6]=rce
 //   v[7..9]=b1,b2,b3 v[10..12]=r1,r2,r3 v[13]=on
@@ -80,6 +85,14 @@ struct SysDev {
   double fire_dtmax, fire_fmax;
   int fire_maxit, pad1;
   TersoffP ts;
+  // pair virial (pressure) and the G-JF constant-pressure piston
+  // (set_lgf, Integration.F90:486-525): particle noise amplitude fac0 and
+  // friction half-step facg0, kinetic term N kB T, target pressure,
+  // 1/piston mass, piston b, noise amplitude and a
+  int virial;          // force kernels accumulate the pair virial
+  int cell_cap;        // cells allocated (a moving box may re-grid within them)
+  double rlist;        // rcut + skin
+  double lgf_fac0, lgf_facg0, lgf_kin, lgf_press, lgf_ipm, lgf_bv, lgf_facv, lgf_av;
 };
 
 // Dynamic state of a system, written only by kernels (and reset by host).
@@ -96,6 +109,16 @@ struct SysState {
   double fmax2;     // max |F|^2 (internal units), FIRE convergence
   unsigned long long fmax2_bits;
   int maxnn, pad;
+  // pair virial W = sum_i r_i (x) F_i of the last force evaluation
+  // (internal units; xx yy zz xy xz yz), kinetic tensor sum m v (x) v
+  double vir[6], ktens[6];
+  // G-JF piston: force (pistonf), velocity, this step's noise, the box
+  // ratio and the drift factor 2 L / (L_old + L) of the last box move
+  double lgf_pf, lgf_pvel, lgf_rangv, ext_piston;
+  double lgf_sc[3], lgf_f2[3];
+  double box_b[3];   // box at the last rebuild (list skin vs box motion)
+  int lgf_phase;     // 0 until the first piston step (pistonf from the virial)
+  int pad2;
 };
 
 // Block map: block b covers atoms [first[b], end[b]) of system sys[b];

@@ -54,6 +54,7 @@ struct SysHost {
   SysDev d{};
   bool ff_set = false;
   double temp = 0.0;        // Ermak bath temperature (K)
+  bool box_live = false;    // the device moved the box (constant pressure)
 };
 
 struct Graph {
@@ -101,6 +102,7 @@ struct gemsgpu_ctx {
   int64_t snap_cap = 0;
   double4* snap = nullptr;      // pos, vel, acel, force
   SysState* snap_st = nullptr;
+  SysDev* snap_sys = nullptr;   // boxes moved by constant-pressure steps
 };
 
 // A pool: a fixed-capacity batch of systems sharing one force-field kind and
@@ -325,6 +327,8 @@ int grow_systems(gemsgpu_ctx* ctx, int need) {
   CU(cudaMallocHost((void**)&ctx->h_st, nc * sizeof(SysState)));
   if (ctx->snap_st) cudaFree(ctx->snap_st);
   CHK(dalloc(ctx, &ctx->snap_st, nc));
+  if (ctx->snap_sys) cudaFree(ctx->snap_sys);
+  CHK(dalloc(ctx, &ctx->snap_sys, nc));
   ctx->scap = nc;
   invalidate(ctx);
   return 0;
@@ -343,7 +347,7 @@ int grow_blocks(gemsgpu_ctx* ctx, int nblk) {
   if (nblk <= ctx->nblk_cap) return 0;
   int nc = std::max(nblk, ctx->nblk_cap * 2);
   CHK(dgrow(ctx, &ctx->A.blk_top2, 0, nc));
-  CHK(dgrow(ctx, &ctx->A.blk_red, 0, 2 * (size_t)nc));
+  CHK(dgrow(ctx, &ctx->A.blk_red, 0, 8 * (size_t)nc));
   ctx->nblk_cap = nc;
   invalidate(ctx);
   return 0;
@@ -385,6 +389,7 @@ void derive(gemsgpu_ctx* ctx, SysHost& h) {
   if (d.ff == FF_TERSOFF) rc = d.ts.R + d.ts.D;
   d.rcut = rc;
   double rl = rc + d.skin;
+  d.rlist = rl;
   d.rlist2 = rl * rl;
   // intergroup_setcells (src/Neighbour.F90:587-664)
   d.use_cells = 0;
@@ -428,10 +433,22 @@ void derive(gemsgpu_ctx* ctx, SysHost& h) {
   }
 }
 
+// cells a system's grid may use: its grid, or for a constant-pressure box
+// the grid of a box 15% longer in every dimension, which it may re-plan
+// into as the box moves
+int cells_needed(const SysHost& h) {
+  if (!h.d.use_cells) return 0;
+  if (h.d.integ != IT_LGF) return h.d.ncell;
+  int64_t m = 1;
+  for (int k = 0; k < 3; k++) m *= std::max(h.d.nc[k], (int)(1.15 * h.d.L[k] / h.d.rlist));
+  return (int)std::min<int64_t>(m, 1 << 26);
+}
+
 int alloc_cells(gemsgpu_ctx* ctx, SysHost& h) {
-  int need = h.d.use_cells ? h.d.ncell : 0;
+  int need = cells_needed(h);
   if (need <= h.cell_cap) {
     h.d.cell_off = h.cell_off;
+    h.d.cell_cap = h.cell_cap;
     return 0;
   }
   if (h.cell_cap > 0) ctx->free_cells.push_back({h.cell_off, h.cell_off + h.cell_cap});
@@ -441,12 +458,23 @@ int alloc_cells(gemsgpu_ctx* ctx, SysHost& h) {
   h.cell_off = (int)off;
   h.cell_cap = (int)cap;
   h.d.cell_off = h.cell_off;
+  h.d.cell_cap = h.cell_cap;
   invalidate(ctx);
+  return 0;
+}
+
+// the box lengths a constant-pressure system has on the device
+int live_box(gemsgpu_ctx* ctx, int s, double L[3]) {
+  SysDev d;
+  CU(cudaMemcpyAsync(&d, ctx->A.sys + s, sizeof(SysDev), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < 3; k++) L[k] = d.L[k];
   return 0;
 }
 
 int push_sys(gemsgpu_ctx* ctx, int s) {
   SysHost& h = ctx->sys[s];
+  if (h.box_live) CHK(live_box(ctx, s, h.d.L));  // keep the box the pistons moved
   derive(ctx, h);
   CHK(alloc_cells(ctx, h));
   CU(cudaMemcpyAsync(ctx->A.sys + s, &h.d, sizeof(SysDev), cudaMemcpyHostToDevice, ctx->stream));
@@ -484,7 +512,8 @@ int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, Blo
     } else {
       if (!h.d.use_cells) continue;
       lo = h.cell_off;
-      hi = h.cell_off + h.d.ncell;
+      // a moving box re-plans its grid on the device within its allocation
+      hi = h.cell_off + (h.d.integ == IT_LGF ? h.cell_cap : h.d.ncell);
     }
     blk0[s] = (int)bs.size();
     for (int a = lo; a < hi; a += apb) {
@@ -567,9 +596,10 @@ void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, b
 }
 
 template <int K>
-void lj_k(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
+void lj_k(gemsgpu_ctx* ctx, int prec, bool vir, const BlockMap& m) {
   if (prec == PREC_MIXED) k_lj_mixed<K><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
-  else k_lj_fp64<K><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  else if (vir) k_lj_fp64<K, true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  else k_lj_fp64<K, false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
   ++ctx->launches;
 }
 
@@ -587,32 +617,33 @@ void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, 
   }
 }
 
-void lj_pass(gemsgpu_ctx* ctx, int prec, int K, const BlockMap& m) {
+void lj_pass(gemsgpu_ctx* ctx, int prec, int K, bool vir, const BlockMap& m) {
   switch (K) {
-    case 2: lj_k<2>(ctx, prec, m); break;
-    case 4: lj_k<4>(ctx, prec, m); break;
-    case 8: lj_k<8>(ctx, prec, m); break;
-    case 16: lj_k<16>(ctx, prec, m); break;
-    case 32: lj_k<32>(ctx, prec, m); break;
-    default: lj_k<1>(ctx, prec, m); break;
+    case 2: lj_k<2>(ctx, prec, vir, m); break;
+    case 4: lj_k<4>(ctx, prec, vir, m); break;
+    case 8: lj_k<8>(ctx, prec, vir, m); break;
+    case 16: lj_k<16>(ctx, prec, vir, m); break;
+    case 32: lj_k<32>(ctx, prec, vir, m); break;
+    default: lj_k<1>(ctx, prec, vir, m); break;
   }
 }
 
 // group systems by (ff, prec, lanes) and launch the force kernels
 int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
-  std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;
+  std::map<std::tuple<int, int, int, int, int>, std::vector<int>> groups;
   for (int s : ss) {
     const SysHost& h = ctx->sys[s];
     if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no force field", s);
     if (h.d.half) return fail(ctx, GEMSGPU_ERR_STATE, "system %d: force kernels need full lists", s);
     int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
     int key = h.variant * 2 + (h.ntypes == 1 ? 1 : 0);
-    groups[{h.d.ff, h.d.prec, K, key}].push_back(s);
+    groups[{h.d.ff, h.d.prec, K, key, h.d.virial}].push_back(s);
   }
   for (auto& kv : groups) {
     int ff = std::get<0>(kv.first), prec = std::get<1>(kv.first), K = std::get<2>(kv.first);
     const int variant = std::get<3>(kv.first) / 2;
     const bool single = (std::get<3>(kv.first) & 1) != 0;
+    const bool vir = std::get<4>(kv.first) != 0;
     BlockMap m;
     if (ff == FF_TERSOFF) {
       CHK(get_map(ctx, kv.second, BLOCK, 0, &m));
@@ -629,7 +660,7 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
       smatb_pass(ctx, 0, prec, variant, single, K, m);
       smatb_pass(ctx, 1, prec, variant, single, K, m);
     } else if (ff == FF_LJ) {
-      lj_pass(ctx, prec, K, m);
+      lj_pass(ctx, prec, K, vir, m);
     }
   }
   CU(cudaGetLastError());
@@ -675,6 +706,16 @@ int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss,
                   cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
+  bool piston = false;
+  for (int s : ss) piston |= ctx->sys[s].d.integ == IT_LGF;
+  if (piston) {
+    const int* sa;
+    CHK(sys_array(ctx, ss, &sa));
+    k_lgf_sys<<<((int)ss.size() + 127) / 128, 128, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size());
+    ++ctx->launches;
+    for (int s : ss)
+      if (ctx->sys[s].d.integ == IT_LGF) ctx->sys[s].box_live = true;
+  }
   if (use_cond) k_step_a<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
   else k_step_a<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
   ++ctx->launches;
@@ -733,6 +774,10 @@ int status_error(gemsgpu_ctx* ctx, int s, int st) {
   if (st & ST_LOST)
     return fail(ctx, GEMSGPU_ERR_LOST, "system %d: atom outside the cell grid / fixed-point range", s);
   if (st & ST_OVERFLOW) return fail(ctx, GEMSGPU_ERR_OVERFLOW, "system %d: neighbour list overflow", s);
+  if (st & ST_BOX)
+    return fail(ctx, GEMSGPU_ERR_STATE,
+                "system %d: the constant-pressure box left its cell grid (under three list cut-offs "
+                "or a collapsed volume)", s);
   return 0;
 }
 
@@ -1034,8 +1079,12 @@ int snapshot(gemsgpu_ctx* ctx, bool restore) {
   if (restore) {
     CU(cudaMemcpyAsync(A.st, ctx->snap_st, ctx->scap * sizeof(SysState), cudaMemcpyDeviceToDevice,
                        ctx->stream));
+    CU(cudaMemcpyAsync(A.sys, ctx->snap_sys, ctx->scap * sizeof(SysDev), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
   } else {
     CU(cudaMemcpyAsync(ctx->snap_st, A.st, ctx->scap * sizeof(SysState), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(ctx->snap_sys, A.sys, ctx->scap * sizeof(SysDev), cudaMemcpyDeviceToDevice,
                        ctx->stream));
   }
   return 0;
@@ -1066,7 +1115,7 @@ int md_group(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps) {
     for (int s : ss) {
       int st = ctx->h_st[s].status;
       if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
-      if (st & (ST_NAN | ST_LOST)) { bad = st; bads = s; }
+      if (st & (ST_NAN | ST_LOST | ST_BOX)) { bad = st; bads = s; }
     }
     if (bad) return status_error(ctx, bads, bad);
     if (grow > 0) {
@@ -1244,7 +1293,7 @@ int pool_forces(gemsgpu_pool* P) {
     smatb_pass(ctx, 0, P->prec, P->variant, single, P->lanes, mk);
     smatb_pass(ctx, 1, P->prec, P->variant, single, P->lanes, mk);
   } else if (P->ff == FF_LJ) {
-    lj_pass(ctx, P->prec, P->lanes, mk);
+    lj_pass(ctx, P->prec, P->lanes, false, mk);
   } else if (P->ff == FF_TERSOFF) {
     k_zero_force<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
     if (P->prec == PREC_MIXED) k_tersoff<float><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
@@ -1473,7 +1522,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
                   A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
-                  ctx->d_red, ctx->snap, ctx->snap_st, ctx->d_sys};
+                  ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
@@ -1664,6 +1713,8 @@ int gemsgpu_set_box(gemsgpu_ctx* ctx, int sys, int boxed, const double L[3], con
     for (int k = 0; k < 3; k++)
       if (!(L[k] > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "set_box: L must be positive");
   }
+  if (h.d.integ == IT_LGF && !boxed) return fail(ctx, GEMSGPU_ERR_STATE, "set_box: a piston system keeps its box");
+  h.box_live = false;  // the given box replaces the one the pistons moved
   h.d.boxed = boxed ? 1 : 0;
   for (int k = 0; k < 3; k++) {
     h.d.L[k] = boxed ? L[k] : 0.0;
@@ -1708,6 +1759,11 @@ int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec) {
   CHK(check_sys(ctx, sys));
   if (prec != GEMSGPU_PREC_FP64 && prec != GEMSGPU_PREC_MIXED)
     return fail(ctx, GEMSGPU_ERR_ARG, "unknown precision %d", prec);
+  if (prec != GEMSGPU_PREC_FP64 && (ctx->sys[sys].d.integ == IT_LGF || ctx->sys[sys].d.virial))
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: the virial and the piston are FP64 only");
+  if (prec != GEMSGPU_PREC_FP64 && ctx->sys[sys].d.ff == FF_LJ)
+    for (const PairP& P : ctx->sys[sys].prm)
+      if (P.v[8] != 0.0) return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: slj pairs are FP64 only");
   ctx->sys[sys].d.prec = prec;
   CHK(push_sys(ctx, sys));
   BlockMap m;
@@ -1962,6 +2018,169 @@ int gemsgpu_set_fire(gemsgpu_ctx* ctx, int sys, double dt0, double dtmax) {
                      ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   invalidate(ctx);
+  return 0;
+}
+
+// slj_set (src/Pairs.F90:374-401): LJ core to rs, then the tail
+// sa4 (r - rc)^4 + sa8 (r - rc)^8 that reaches zero with zero slope at rc
+int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, double sigma, double rs) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (ti < 0 || tj < 0 || ti >= h.ntypes || tj >= h.ntypes || !(rs > 0.0) || !(sigma > 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_slj: bad type pair, sigma or rs");
+  if (h.d.ff != FF_NONE && h.d.ff != FF_LJ)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_slj: system already has another force field");
+  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_slj: FP64 systems only");
+  const double x = sigma / rs, x3 = x * x * x, s_dr = x3 * x3;
+  const double urs = 4.0 * eps * (s_dr * s_dr - s_dr);
+  const double dudrs = -eps * (48.0 * s_dr - 24.0) * s_dr / rs;
+  const double rc = rs - 32.0 * urs / (11.0 * dudrs);
+  if (!(rc > rs)) return fail(ctx, GEMSGPU_ERR_ARG, "set_slj: rs must lie in the attractive part of the core");
+  const double d = rc - rs, d4 = d * d * d * d;
+  h.d.ff = FF_LJ;
+  PairP P{};
+  P.v[0] = eps;
+  P.v[1] = sigma;
+  P.v[2] = rc;
+  P.v[3] = rc * rc;
+  P.v[8] = 1.0;
+  P.v[9] = (8.0 * urs + d * dudrs) / (4 * d4);
+  P.v[10] = -(4.0 * urs + d * dudrs) / (4 * (d4 * d4));
+  P.v[11] = rs;
+  h.prm[ti * h.ntypes + tj] = P;
+  h.prm[tj * h.ntypes + ti] = P;
+  h.ff_set = true;
+  h.first = true;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (on && h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "virial: pair potentials (lj, plj, slj) only");
+  if (on && h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "virial: FP64 systems only");
+  if (!on && h.d.integ == IT_LGF) return fail(ctx, GEMSGPU_ERR_STATE, "virial: the piston needs it");
+  h.d.virial = on ? 1 : 0;
+  h.has_forces = false;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+namespace {
+// pressure units (src/Constants.F90:186-193): atm -> internal on input,
+// internal -> atm on output (write_pressure, src/Output.F90:767-770)
+double atm_ui() { return 1.01325 * 1.e5 * ((1.0 / (UI_EV * 1.60219e-19)) * 1e-30); }
+double ui_atm() { return 1.0 / ((1.0 / (UI_EV * 1.60219e-19)) * 1e-30) * 1e-5 * (1.0 / 1.01325); }
+}  // namespace
+
+// set_lgf (src/Integration.F90:486-525): the isotropic G-JF piston
+int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp, double press_atm, double pgama0,
+                    double pgamav, double pmass, uint64_t seed) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (!(dt > 0.0) || !(temp >= 0.0) || !(pgama0 >= 0.0) || !(pgamav >= 0.0) || !(pmass > 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_lgf: dt>0, T>=0, gammas>=0, piston mass>0");
+  if (!h.d.boxed || !h.d.pbc[0] || !h.d.pbc[1] || !h.d.pbc[2])
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: the piston needs a box periodic in x, y and z");
+  if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: pair potentials (lj, plj, slj) only");
+  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: FP64 systems only");
+  SysDev& d = h.d;
+  d.integ = IT_LGF;
+  d.dt = dt;
+  d.lgf_fac0 = std::sqrt(2.0 * pgama0 * kB_ui * temp * dt);
+  d.lgf_facg0 = 0.5 * dt * pgama0;
+  d.lgf_kin = h.n * temp * kB_ui;
+  d.lgf_press = press_atm * atm_ui();
+  d.lgf_ipm = 1.0 / pmass;
+  d.lgf_bv = 1.0 / (1.0 + 0.5 * dt * d.lgf_ipm * pgamav);
+  d.lgf_facv = std::sqrt(2.0 * pgamav * kB_ui * temp * dt);
+  d.lgf_av = (1.0 - 0.5 * dt * d.lgf_ipm * pgamav) * d.lgf_bv;
+  d.virial = 1;
+  d.seed = seed;
+  d.use_ext_normals = 0;
+  h.temp = temp;
+  h.has_forces = false;  // the first piston step needs the virial
+  CHK(push_sys(ctx, sys));
+  CHK(read_states(ctx));
+  SysState st = ctx->h_st[sys];
+  st.lgf_phase = 0;
+  st.lgf_pf = st.lgf_pvel = st.lgf_rangv = 0.0;
+  for (int k = 0; k < 3; k++) st.box_b[k] = d.L[k];
+  CU(cudaMemcpyAsync(ctx->A.st + sys, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (h.d.integ != IT_LGF) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf_normals: not a piston system");
+  if (!normals) {
+    h.d.use_ext_normals = 0;
+  } else {
+    CU(cudaMemcpyAsync(ctx->A.ext_normals + (size_t)6 * h.off, normals + 2, (size_t)6 * h.n * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(&ctx->A.st[sys].ext_piston, normals, sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    h.d.use_ext_normals = 1;
+  }
+  CHK(push_sys(ctx, sys));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int gemsgpu_get_box(gemsgpu_ctx* ctx, int sys, double L[3]) {
+  CHK(check_sys(ctx, sys));
+  if (!L) return fail(ctx, GEMSGPU_ERR_ARG, "get_box: NULL");
+  SysHost& h = ctx->sys[sys];
+  if (h.box_live) return live_box(ctx, sys, L);
+  for (int k = 0; k < 3; k++) L[k] = h.d.L[k];
+  return 0;
+}
+
+static void sym9(const double w[6], double f, double* out) {
+  const int idx[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+  for (int k = 0; k < 9; k++) out[k] = w[idx[k]] * f;
+}
+
+// inq_virial (src/Inq_Properties.F90:439-527) of the last force evaluation,
+// eV, row-major 3x3
+int gemsgpu_virial(gemsgpu_ctx* ctx, int sys, double* out9) {
+  CHK(check_sys(ctx, sys));
+  if (!out9) return fail(ctx, GEMSGPU_ERR_ARG, "virial: NULL");
+  const SysHost& h = ctx->sys[sys];
+  if (!h.d.virial || h.d.ff != FF_LJ || !h.has_forces)
+    return fail(ctx, GEMSGPU_ERR_STATE, "virial: not computed (set_virial, forces)");
+  CHK(read_states(ctx));
+  sym9(ctx->h_st[sys].vir, UI_EV, out9);
+  return 0;
+}
+
+// inq_pressure (src/Inq_Properties.F90:529-573): (sum m v v + W) / V, atm
+int gemsgpu_pressure(gemsgpu_ctx* ctx, int sys, double* out9) {
+  CHK(check_sys(ctx, sys));
+  if (!out9) return fail(ctx, GEMSGPU_ERR_ARG, "pressure: NULL");
+  const SysHost& h = ctx->sys[sys];
+  if (!h.d.virial || h.d.ff != FF_LJ || !h.has_forces)
+    return fail(ctx, GEMSGPU_ERR_STATE, "pressure: virial not computed");
+  if (!h.d.boxed) return fail(ctx, GEMSGPU_ERR_STATE, "pressure: no box");
+  BlockMap m;
+  CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
+  k_kin_tensor<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  CU(cudaGetLastError());
+  CHK(read_states(ctx));
+  double L[3];
+  CHK(gemsgpu_get_box(ctx, sys, L));
+  const SysState& st = ctx->h_st[sys];
+  double w[6];
+  for (int k = 0; k < 6; k++) w[k] = st.ktens[k] + st.vir[k];
+  sym9(w, ui_atm() / (L[0] * L[1] * L[2]), out9);
   return 0;
 }
 
@@ -2471,6 +2690,8 @@ int gemsgpu_pool_set(gemsgpu_pool* P, const int* sys, int nsys) {
     if (s >= P->scap) return fail(ctx, GEMSGPU_ERR_FULL, "system id beyond the pool's capacity");
     if ((P->variant & 1) == 0 && ctx->sys[s].ntypes != 1)
       return fail(ctx, GEMSGPU_ERR_STATE, "pool variant %d needs single-species systems", P->variant);
+    if (ctx->sys[s].d.integ == IT_LGF || ctx->sys[s].d.virial)
+      return fail(ctx, GEMSGPU_ERR_STATE, "pool_set: pools run fixed boxes without the virial");
     atoms += ctx->sys[s].n;
   }
   if (atoms > P->max_atoms) return fail(ctx, GEMSGPU_ERR_FULL, "pool_set: %lld atoms > capacity", (long long)atoms);
@@ -2688,6 +2909,10 @@ struct ChpHeader {
   int64_t nupd;
   double fire_dt, fire_alpha;
   int32_t fire_np, fire_done, fire_iter, fire_zero;
+  // the box and the G-JF piston (force, velocity, last noise, phase)
+  double box[3];
+  double lgf_pf, lgf_pvel, lgf_rangv;
+  int32_t lgf_phase, pad;
 };
 }  // namespace
 
@@ -2707,7 +2932,7 @@ int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes) 
   const SysState& st = ctx->h_st[sys];
   ChpHeader hd{};
   memcpy(hd.magic, "GEMSGPU", 8);
-  hd.version = 1;
+  hd.version = 2;
   hd.n = h.n;
   hd.ff = h.d.ff;
   hd.integ = h.d.integ;
@@ -2719,6 +2944,11 @@ int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes) 
   hd.fire_done = st.fire_done;
   hd.fire_iter = st.fire_iter;
   hd.fire_zero = st.fire_zero;
+  CHK(gemsgpu_get_box(ctx, sys, hd.box));
+  hd.lgf_pf = st.lgf_pf;
+  hd.lgf_pvel = st.lgf_pvel;
+  hd.lgf_rangv = st.lgf_rangv;
+  hd.lgf_phase = st.lgf_phase;
   char* p = static_cast<char*>(buf);
   memcpy(p, &hd, sizeof(hd));
   double* x = reinterpret_cast<double*>(p + sizeof(hd));
@@ -2735,9 +2965,17 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   SysHost& h = ctx->sys[sys];
   ChpHeader hd;
   memcpy(&hd, buf, sizeof(hd));
-  if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || hd.version != 1)
+  if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || hd.version != 2)
     return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: not a checkpoint of this library");
   if (hd.n != h.n) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %d atoms, system has %d", hd.n, h.n);
+  if (h.d.boxed && (h.d.integ == IT_LGF || hd.integ == IT_LGF)) {
+    // the box the piston had reached
+    h.box_live = false;
+    for (int k = 0; k < 3; k++) h.d.L[k] = hd.box[k];
+    CHK(push_sys(ctx, sys));
+    drop_maps(ctx);
+    invalidate(ctx);
+  }
   const double* x = reinterpret_cast<const double*>(static_cast<const char*>(buf) + sizeof(hd));
   CHK(h2d_xyz(ctx, x, ctx->A.pos + h.off, h.n));
   CHK(h2d_xyz(ctx, x + 3 * (size_t)h.n, ctx->A.vel + h.off, h.n));
@@ -2752,6 +2990,11 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   st.fire_done = hd.fire_done;
   st.fire_iter = hd.fire_iter;
   st.fire_zero = hd.fire_zero;
+  st.lgf_pf = hd.lgf_pf;
+  st.lgf_pvel = hd.lgf_pvel;
+  st.lgf_rangv = hd.lgf_rangv;
+  st.lgf_phase = hd.lgf_phase;
+  for (int k = 0; k < 3; k++) st.box_b[k] = h.d.L[k];
   st.status = 0;
   CU(cudaMemcpyAsync(ctx->A.st + sys, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
   BlockMap m;

@@ -652,7 +652,11 @@ __global__ void k_list_n2(Arena A, BlockMap M) {
 // node, whose executions are counted for the launch statistics
 __global__ void k_count_rebuild(Arena A, const int* sys, int nsys, int in_graph) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < nsys && sys[k] >= 0 && A.st[sys[k]].rebuild) A.st[sys[k]].nupd++;
+  if (k < nsys && sys[k] >= 0 && A.st[sys[k]].rebuild) {
+    SysState& st = A.st[sys[k]];
+    st.nupd++;
+    for (int d = 0; d < 3; d++) st.box_b[d] = A.sys[sys[k]].L[d];
+  }
   if (in_graph && k == 0) atomicAdd(A.body_runs, 1ull);
 }
 
@@ -1060,10 +1064,65 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
 }
 
 // ------------------------------------------------------------------ LJ
+// Six per-system sums (xx yy zz xy xz yz of a tensor): each block sums its
+// threads' values; the system's last block adds the block partials in
+// block order, so the result is the same bits on every run.
+__device__ __forceinline__ void sys6_close(Arena& A, const BlockMap& M, int s, const double w[6], double* dst) {
+  double b[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) b[k] = block_sum(w[k]);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 6; k++) A.blk_red[8 * blockIdx.x + k] = b[k];
+  if (last_block(M, A.st, s, &A.st[s].ticket2) && threadIdx.x < 32) {
+    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = threadIdx.x; q < nb; q += 32)
+#pragma unroll
+      for (int k = 0; k < 6; k++) t[k] += __ldcg(&A.blk_red[8 * (b0 + q) + k]);
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      for (int o = 16; o; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 6; k++) dst[k] = t[k];
+  }
+}
+
+// Pair virial W = sum_i r_i (x) F_i.  With minimum-image pairs it is half
+// the sum over the full list of vd (x) f vd / r (vd = r_j - r_i), the
+// virial inq_virial (Inq_Properties.F90:439-527) builds from local and
+// ghost atoms.
+__device__ __forceinline__ void virial_close(Arena& A, const BlockMap& M, int s, const double w[6]) {
+  sys6_close(A, M, s, w, A.st[s].vir);
+}
+
+// kinetic tensor sum_i m v (x) v of each system (inq_pressure,
+// Inq_Properties.F90:529-573), into SysState::ktens
+__global__ void k_kin_tensor(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  if (i < M.end[blockIdx.x]) {
+    const double4 v = A.vel[i];
+    const double m = A.mass[i];
+    w[0] = v.x * v.x * m;
+    w[1] = v.y * v.y * m;
+    w[2] = v.z * v.z * m;
+    w[3] = v.x * v.y * m;
+    w[4] = v.x * v.z * m;
+    w[5] = v.y * v.z * m;
+  }
+  sys6_close(A, M, s, w, A.st[s].ktens);
+}
+
 // lj_interact / plj_interact (src/Pairs.F90:207-370), full list:
 //   s6 = (s/r)^6 ; p = 4e(s6^2 - s6) [- prc - frc (r - rc)] [- eshift]
 //   f = e(48 s6 - 24) s6 / r [+ frc] ; F_i -= f vd / r ; e_i += p/2
-template <int K>
+// slj_interact (src/Pairs.F90:403-470) for pairs of the slj form:
+//   r < rs: p = 4e (s6 - 1) s6, f as LJ;  rs <= r <= rc, d = r - rc:
+//   p = sa4 d^4 + sa8 d^8, f = -(4 sa4 d^4 + 8 sa8 d^8) / d
+// VIR: also the pair virial of the system (virial_close).
+template <int K, bool VIR>
 __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
@@ -1072,6 +1131,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
   if (act) {
     const double4 xi = A.pos[i];
     const int ti = A.type[i];
@@ -1086,22 +1146,39 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
       double dr = v0 * v0 + v1 * v1 + v2 * v2;
       if (dr > P.v[3]) continue;
       dr = sqrt(dr);
-      double t = P.v[1] / dr;
-      double t3 = t * t * t;
-      double s6 = t3 * t3;
-      double p = 4.0 * e * (s6 * s6 - s6);
-      double f = e * (48.0 * s6 - 24.0) * s6 / dr;
-      if (P.v[7] != 0.0) {
-        p = p - P.v[4] - P.v[5] * (dr - P.v[2]);
-        f = f + P.v[5];
+      double p, f;
+      if (P.v[8] != 0.0 && dr >= P.v[11]) {
+        const double d = dr - P.v[2];
+        const double s4 = d * d * d * d;
+        p = P.v[9] * s4 + P.v[10] * s4 * s4;
+        f = -(4.0 * P.v[9] * s4 + 8.0 * P.v[10] * s4 * s4) / d;
       } else {
-        p = p - P.v[6];
+        double t = P.v[1] / dr;
+        double t3 = t * t * t;
+        double s6 = t3 * t3;
+        p = P.v[8] != 0.0 ? 4.0 * e * (s6 - 1.0) * s6 : 4.0 * e * (s6 * s6 - s6);
+        f = e * (48.0 * s6 - 24.0) * s6 / dr;
+        if (P.v[7] != 0.0) {
+          p = p - P.v[4] - P.v[5] * (dr - P.v[2]);
+          f = f + P.v[5];
+        } else {
+          p = p - P.v[6];
+        }
       }
       double fr = f * EV_UI / dr;
       f0 -= fr * v0;
       f1 -= fr * v1;
       f2 -= fr * v2;
       ep += p;
+      if constexpr (VIR) {
+        const double h = 0.5 * fr;
+        w[0] += h * v0 * v0;
+        w[1] += h * v1 * v1;
+        w[2] += h * v2 * v2;
+        w[3] += h * v0 * v1;
+        w[4] += h * v0 * v2;
+        w[5] += h * v1 * v2;
+      }
     PAIR_LOOP_END
   }
   f0 = lane_sum<K>(f0);
@@ -1112,6 +1189,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
     A.force[i] = make_double4(f0, f1, f2, 0.0);
     A.epot[i] = ep * 0.5 * EV_UI;
   }
+  if constexpr (VIR) virial_close(A, M, s, w);
 }
 
 template <int K>
@@ -1407,6 +1485,123 @@ __device__ __forceinline__ void wrap_atom(const SysDev& S, double4& x) {
   }
 }
 
+// lgf_stepa (src/Integration.F90:527-598) per atom, after k_lgf_sys moved
+// the box: the noise displacement pos_v = fac0 / m r, acel = F / m, and
+// x = (L / L_old) x + 2 L / (L_old + L) b dt (v + dt/2 acel + pos_v / 2)
+// with b = 1 / (1 + dt/2 gamma / m)
+__device__ __forceinline__ void lgf_a_atom(const Arena& A, const SysDev& S, const SysState& st, int i, double om,
+                                           const double4& F, const double4& v, double4& a, double4& x,
+                                           double4& pv) {
+  double r0, r1, r2;
+  if (S.use_ext_normals) {
+    r0 = A.ext_normals[(size_t)6 * i];
+    r1 = A.ext_normals[(size_t)6 * i + 2];
+    r2 = A.ext_normals[(size_t)6 * i + 4];
+  } else {
+    double q[6];
+    normals6((uint32_t)(i - S.off), st.step, S.seed, q);
+    r0 = q[0], r1 = q[2], r2 = q[4];
+  }
+  const double b0 = 1.0 / (1.0 + S.lgf_facg0 * om);
+  const double c = om * S.lgf_fac0;
+  pv = make_double4(c * r0, c * r1, c * r2, 0.0);
+  a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+  const double hdt = 0.5 * S.dt;
+  x.x = st.lgf_sc[0] * x.x + st.lgf_f2[0] * b0 * S.dt * (v.x + hdt * a.x + 0.5 * pv.x);
+  x.y = st.lgf_sc[1] * x.y + st.lgf_f2[1] * b0 * S.dt * (v.y + hdt * a.y + 0.5 * pv.y);
+  x.z = st.lgf_sc[2] * x.z + st.lgf_f2[2] * b0 * S.dt * (v.z + hdt * a.z + 0.5 * pv.z);
+}
+
+// lgf_stepb (src/Integration.F90:600-650) per atom:
+// v = a v + dt/2 (a acel + F / m) + b pos_v, a = (1 - dt/2 gamma / m) b
+__device__ __forceinline__ void lgf_b_atom(const SysDev& S, double om, const double4& F, const double4& pv,
+                                           double4& v, double4& a) {
+  const double b0 = 1.0 / (1.0 + S.lgf_facg0 * om);
+  const double a0 = (1.0 - S.lgf_facg0 * om) * b0;
+  const double hdt = 0.5 * S.dt;
+  v.x = a0 * v.x + hdt * (a0 * a.x + om * F.x) + b0 * pv.x;
+  v.y = a0 * v.y + hdt * (a0 * a.y + om * F.y) + b0 * pv.y;
+  v.z = a0 * v.z + hdt * (a0 * a.z + om * F.z) + b0 * pv.z;
+  a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+}
+
+// The G-JF piston of each constant-pressure system (one thread per system),
+// ahead of the atoms' half step.  It first closes the previous step's
+// piston (lgf_stepb: pistonf from the virial of the last force evaluation
+// and pvel), which needs the whole system's virial and so waits for this
+// launch, then moves the box (lgf_stepa): the volume
+//   V = V0 + b dt (pvel + (dt pistonf + rangv) / (2 Q)),
+// each length L (V / V0)^(1/3) with the single-precision exponent 1./dd of
+// the reference, and the cell grid of the next rebuild re-planned for the
+// new lengths within the cells allocated.  The first step takes pistonf
+// from the virial of the initial interact and leaves pvel at 0.
+__global__ void k_lgf_sys(Arena A, const int* sys, int nsys) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nsys) return;
+  const int s = sys[k];
+  if (s < 0) return;
+  SysDev& S = A.sys[s];
+  SysState& st = A.st[s];
+  if (S.integ != IT_LGF) return;
+  const double dt = S.dt;
+  const double vol0 = S.L[0] * S.L[1] * S.L[2];
+  const double sv = (st.vir[0] + st.vir[1] + st.vir[2]) / 3;
+  const double pf = (sv + S.lgf_kin) / vol0 - S.lgf_press;
+  if (st.lgf_phase == 0) {
+    st.lgf_phase = 1;
+  } else {
+    st.lgf_pvel = S.lgf_av * st.lgf_pvel + 0.5 * S.lgf_ipm * dt * (S.lgf_av * st.lgf_pf + pf) +
+                  S.lgf_bv * S.lgf_ipm * st.lgf_rangv;
+  }
+  st.lgf_pf = pf;
+  double r;
+  if (S.use_ext_normals) {
+    r = st.ext_piston;
+  } else {
+    double q[6];
+    normals6((uint32_t)S.n, st.step, S.seed, q);
+    r = q[0];
+  }
+  const double rangv = r * S.lgf_facv;
+  st.lgf_rangv = rangv;
+  const double vol = vol0 + S.lgf_bv * dt * (st.lgf_pvel + 0.5 * S.lgf_ipm * (dt * pf + rangv));
+  if (!(vol > 0.0)) {
+    atomicOr(&st.status, ST_BOX);
+    for (int d = 0; d < 3; d++) st.lgf_sc[d] = st.lgf_f2[d] = 1.0;
+    return;
+  }
+  const double g = pow(vol / vol0, (double)(1.0f / 3.0f));
+  for (int d = 0; d < 3; d++) {
+    const double Lo = S.L[d], Ln = Lo * g;
+    st.lgf_sc[d] = Ln / Lo;
+    st.lgf_f2[d] = 2.0 * Ln / (Lo + Ln);
+    S.L[d] = Ln;
+    S.invL[d] = 1.0 / Ln;
+  }
+  if (S.use_cells) {
+    // intergroup_setcells for the new box (cells no smaller than the list
+    // cut-off); fewer, larger cells where the allocation is short; below
+    // three cells a dimension's stencil would visit a cell twice
+    int nc[3];
+    for (int d = 0; d < 3; d++) nc[d] = (int)(S.L[d] / S.rlist);
+    while ((int64_t)nc[0] * nc[1] * nc[2] > S.cell_cap) {
+      int m = nc[1] > nc[0] ? 1 : 0;
+      if (nc[2] > nc[m]) m = 2;
+      nc[m]--;
+    }
+    if (nc[0] < 3 || nc[1] < 3 || nc[2] < 3) {
+      atomicOr(&st.status, ST_BOX);
+    } else {
+      for (int d = 0; d < 3; d++) {
+        S.nc[d] = nc[d];
+        S.cell[d] = S.L[d] / nc[d];
+        S.inv_cell[d] = 1.0 / S.cell[d];
+      }
+      S.ncell = nc[0] * nc[1] * nc[2];
+    }
+  }
+}
+
 // the moved atom's outputs: position, fixed-point copy, skin displacement
 // (xo = its position at the last rebuild, ty = its species)
 __device__ __forceinline__ double moved_atom(Arena& A, const SysDev& S, SysState& st, int i, const double4& x,
@@ -1426,7 +1621,8 @@ __device__ __forceinline__ double moved_atom(Arena& A, const SysDev& S, SysState
 // the squared displacements, merged by the system's last block, which sets
 // the rebuild flag (and raises the graph's rebuild condition) and closes
 // the step's integrator bookkeeping.
-template <bool COND>
+// PISTON=false: a kernel that never sees a constant-pressure system
+template <bool COND, bool PISTON = true>
 __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, const SysDev& S, SysState& st,
                                            bool frozen, double2 t, cudaGraphConditionalHandle cond) {
   t = block_top2(t);
@@ -1434,14 +1630,20 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
   if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
     double2 w = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
-      int rb = __dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)) > S.skin;
+      // a moving box (constant pressure) shifts periodic images by up to
+      // the change of its lengths since the build, on top of the atoms'
+      // own displacements
+      double box = 0.0;
+      if (PISTON && S.integ == IT_LGF)
+        box = fabs(S.L[0] - st.box_b[0]) + fabs(S.L[1] - st.box_b[1]) + fabs(S.L[2] - st.box_b[2]);
+      int rb = __dadd_rn(__dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)), box) > S.skin;
       if (frozen) rb = 0;
       st.rebuild = rb;
       if (rb) {
         atomicOr(A.any_rebuild, 1);
         if constexpr (COND) cudaGraphSetConditional(cond, 1u);
       }
-      if (S.integ == IT_ERMAK && !S.use_ext_normals) st.step++;
+      if ((S.integ == IT_ERMAK || S.integ == IT_LGF) && !S.use_ext_normals) st.step++;
       if (S.integ == IT_FIRE) st.fire_zero = 0;
     }
   }
@@ -1478,6 +1680,11 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
       double4 vv;
       ermak_a_atom(A, S, st, i, mi, v, a, x, vv);
       A.vel_v[i] = vv;
+    } else if (S.integ == IT_LGF) {
+      double4 pv;
+      lgf_a_atom(A, S, st, i, mi.x, A.force[i], v, a, x, pv);
+      A.acel[i] = a;
+      A.vel_v[i] = pv;
     }
     wrap_atom(S, x);
     t.x = moved_atom(A, S, st, i, x, A.pos_old[i], A.type[i]);
@@ -1522,7 +1729,7 @@ __global__ void __launch_bounds__(BLOCK, 4) k_step_ba(Arena A, BlockMap M, cudaG
     wrap_atom(S, x);
     t.x = moved_atom(A, S, st, i, x, xo, ty);
   }
-  skin_close<COND>(A, M, s, S, st, false, t, cond);
+  skin_close<COND, false>(A, M, s, S, st, false, t, cond);
 }
 
 // integration_stepb (src/Integration.F90:264-301): velocity_verlet_b
@@ -1558,6 +1765,8 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
       }
     } else if (S.integ == IT_ERMAK) {
       ermak_b_atom(S, om, F, A.vel_v[i], v, a);
+    } else if (S.integ == IT_LGF) {
+      lgf_b_atom(S, om, F, A.vel_v[i], v, a);
     }
     A.vel[i] = v;
     A.acel[i] = a;

@@ -61,6 +61,13 @@ _SIGS = {
     "gemsgpu_set_ermak": (_i, [_p, _i, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_set_ermak_normals": (_i, [_p, _i, _dp]),
     "gemsgpu_set_fire": (_i, [_p, _i, _d, _d]),
+    "gemsgpu_set_slj": (_i, [_p, _i, _i, _i, _d, _d, _d]),
+    "gemsgpu_set_virial": (_i, [_p, _i, _i]),
+    "gemsgpu_set_lgf": (_i, [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
+    "gemsgpu_set_lgf_normals": (_i, [_p, _i, _dp]),
+    "gemsgpu_get_box": (_i, [_p, _i, _dp]),
+    "gemsgpu_virial": (_i, [_p, _i, _dp]),
+    "gemsgpu_pressure": (_i, [_p, _i, _dp]),
     "gemsgpu_step_a": (_i, [_p, _i]),
     "gemsgpu_step_b": (_i, [_p, _i]),
     "gemsgpu_md_steps": (_i, [_p, _i, _i]),
@@ -426,6 +433,13 @@ class System:
     def set_lj(self, e, s, rc, ti=0, tj=0, shifted_force=False, eshift=0.0):
         self._c(lib().gemsgpu_set_lj(self.ctx.h, self.sid, ti, tj, e, s, rc, 1 if shifted_force else 0, eshift))
 
+    def set_slj(self, e, sg, rs, ti=0, tj=0):
+        """slj_set: LJ core to rs, polynomial tail to the derived cut-off."""
+        self._c(lib().gemsgpu_set_slj(self.ctx.h, self.sid, ti, tj, float(e), float(sg), float(rs)))
+
+    def set_virial(self, on=True):
+        self._c(lib().gemsgpu_set_virial(self.ctx.h, self.sid, 1 if on else 0))
+
     def set_smatb(self, A, xi, p, q, r0, rci, rce, ti=0, tj=0):
         self._c(lib().gemsgpu_set_smatb(self.ctx.h, self.sid, ti, tj, A, xi, p, q, r0, rci, rce))
 
@@ -478,6 +492,35 @@ class System:
 
     def set_fire(self, dt0, dtmax):
         self._c(lib().gemsgpu_set_fire(self.ctx.h, self.sid, float(dt0), float(dtmax)))
+
+    def set_lgf(self, dt, temp, press_atm, pgama0, pgamav, pmass, seed=12345):
+        """set_lgf (`evolve piston_lgf xyz*`): G-JF constant pressure and
+        temperature; pressure in atm, frictions in 1/ps."""
+        self._c(lib().gemsgpu_set_lgf(self.ctx.h, self.sid, float(dt), float(temp), float(press_atm),
+                                      float(pgama0), float(pgamav), float(pmass), int(seed)))
+
+    def set_lgf_normals(self, nrm):
+        """Next step's normals: the piston's rang pair, then a pair per atom
+        coordinate (2 + 6 n values; None returns to the device stream)."""
+        a = None if nrm is None else _f64(nrm, 2 + 6 * self.n)
+        self._c(lib().gemsgpu_set_lgf_normals(self.ctx.h, self.sid, _ptr(a)))
+
+    def box_now(self):
+        L = np.empty(3, dtype=np.float64)
+        self._c(lib().gemsgpu_get_box(self.ctx.h, self.sid, _ptr(L)))
+        return L
+
+    def virial_ev(self):
+        """Pair virial of the last force evaluation (eV, xx xy xz yx ... zz)."""
+        out = np.empty(9, dtype=np.float64)
+        self._c(lib().gemsgpu_virial(self.ctx.h, self.sid, _ptr(out)))
+        return out
+
+    def pressure_atm(self):
+        """Pressure tensor (sum m v v + W) / V in atm, row-major."""
+        out = np.empty(9, dtype=np.float64)
+        self._c(lib().gemsgpu_pressure(self.ctx.h, self.sid, _ptr(out)))
+        return out
 
     def stepa(self):
         self._c(lib().gemsgpu_step_a(self.ctx.h, self.sid))

@@ -141,6 +141,16 @@ int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec);
 int gemsgpu_set_lj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
                    double sigma, double rcut, int shifted_force,
                    double eshift);
+/* slj_set (src/Pairs.F90:374-401): LJ to rs (A), then a polynomial tail
+ * sa4 (r - rc)^4 + sa8 (r - rc)^8 that vanishes with its slope at the
+ * derived cut-off rc = rs - 32 u(rs) / (11 u'(rs)).  Pairs of a system may
+ * mix lj, plj and slj (slj_interact, Pairs.F90:403-470); FP64 systems. */
+int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
+                    double sigma, double rs);
+/* Pair virial W = sum_i r_i (x) F_i (inq_virial, Inq_Properties.F90:439-527)
+ * accumulated by the force kernels of an FP64 pair-potential system (on=1);
+ * the G-JF piston switches it on. */
+int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on);
 /* smatb_set (src/TB.F90:106-170): A, xi (eV), p, q, r0, rci, rce (A).  The
  * device derives the tail polynomial coefficients. */
 int gemsgpu_set_smatb(gemsgpu_ctx* ctx, int sys, int ti, int tj, double A,
@@ -184,6 +194,30 @@ int gemsgpu_set_ermak_normals(gemsgpu_ctx* ctx, int sys,
 /* FIRE (Bitzek 2006) with the per-atom mixing of FIRE.f90:107-114: dt0,
  * dt_max (ps).  Velocities are zeroed. */
 int gemsgpu_set_fire(gemsgpu_ctx* ctx, int sys, double dt0, double dtmax);
+/* set_lgf (src/Integration.F90:486-525), `evolve piston_lgf xyz*`: constant
+ * pressure and temperature Langevin dynamics of Gronbech-Jensen & Farago
+ * (J. Chem. Phys. 141, 194108, 2014) with an isotropic piston on the
+ * volume.  dt (ps), T (K), target pressure (atm), particle friction pgama0
+ * and piston friction pgamav (1/ps), piston mass pmass; lgf_stepa/stepb
+ * (:527-650) per step.  The box moves on the device every step (its cell
+ * grid re-planned within 15% growth); FP64 pair-potential systems in a box
+ * periodic in x, y and z.  Production noise: Philox4x32-10 keyed by seed. */
+int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp,
+                    double press_atm, double pgama0, double pgamav,
+                    double pmass, uint64_t seed);
+/* Parity mode: the next step_a of a piston system consumes these normals,
+ * 2 + 6 n values in the order rang() draws them in lgf_stepa
+ * (Integration.F90:561-590): the piston's pair, then a pair per atom and
+ * coordinate (the first value of each pair is used).  NULL returns to the
+ * device stream. */
+int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals);
+/* The box lengths (A) as the device holds them (moved by a piston). */
+int gemsgpu_get_box(gemsgpu_ctx* ctx, int sys, double L[3]);
+/* The pair virial of the last force evaluation (eV, row-major 3x3) and the
+ * pressure tensor (sum m v v + W) / V in atm (inq_pressure,
+ * Inq_Properties.F90:529-573; write_pressure, Output.F90:767-770). */
+int gemsgpu_virial(gemsgpu_ctx* ctx, int sys, double* out9);
+int gemsgpu_pressure(gemsgpu_ctx* ctx, int sys, double* out9);
 
 /* integration_stepa / integration_stepb (src/Integration.F90:243-301):
  * the algorithm's half step followed by do_pbc (Set_Properties.f90:444-470). */
@@ -272,7 +306,8 @@ int gemsgpu_neb(gemsgpu_ctx* ctx, const int* sys, int nimg, const int* fixed,
 
 /* Per-system checkpoint (write_chp / read_chp, src/Checkpoint.F90:154-244):
  * positions, velocities and accelerations in the GEMS layout plus the
- * integrator state (Philox step counter, FIRE dt/alpha/counters) and the
+ * integrator state (Philox step counter, FIRE dt/alpha/counters, the box
+ * and the G-JF piston's force, velocity and last noise) and the
  * rebuild count, in a caller-owned host buffer of gemsgpu_checkpoint_size
  * bytes.  Loading into a system of the same size restores that state; the
  * next interact rebuilds the neighbour list, as the reference's does after

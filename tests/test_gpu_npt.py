@@ -1,0 +1,159 @@
+"""Constant pressure on the GPU: slj forces with the pair virial, and the
+G-JF piston (set_lgf / lgf_stepa / lgf_stepb, src/Integration.F90:486-650)
+against the oracle and the examples/NPT/lgf.gms golden files."""
+import numpy as np
+import pytest
+
+import decks
+from oracle import oracle as O
+
+gems = pytest.importorskip("gems_b200")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = gems.Context()
+    yield c
+    c.close()
+
+
+def _gpu(ctx, d, pos=None, seed=12345, skin=None):
+    g = gems.System(d["pos"] if pos is None else pos, d["mass"], ctx=ctx)
+    g.set_skin_mode(False)  # the reference's raw-displacement skin test
+    if skin is not None:
+        g.set_skin(skin)
+    g.set_box(d["box"], (True, True, True))
+    g.set_slj(*d["slj"])
+    g.set_lgf(d["dt"], d["temp"], d["press_atm"], d["pgama0"], d["pgamav"], d["pmass"], seed=seed)
+    return g
+
+
+def _oracle(d, pos=None, skin=None):
+    s = O.System(d["pos"] if pos is None else pos, d["mass"])
+    if skin is not None:
+        s.set_skin(skin)
+    rng = O.Rng(d["seed"])
+    decks.npt_setup(s, d, rng)
+    return s, rng
+
+
+def _feed(g, nrm):
+    g.set_lgf_normals(nrm)
+
+
+def test_slj_forces_and_virial_equal_oracle(ctx):
+    """One interact of the lgf.gms crystal, displaced: forces, energy and
+    virial."""
+    d = decks.npt_lgf_deck()
+    rng = np.random.default_rng(5)
+    pos = d["pos"] + rng.normal(0.0, 0.05, d["pos"].shape)
+    s, _ = _oracle(d, pos)
+    s.interact()
+    g = _gpu(ctx, d, pos)
+    g.interact()
+    f_ref = s.force
+    np.testing.assert_allclose(g.force, f_ref, rtol=0, atol=1e-10 * np.abs(f_ref).max())
+    assert abs(g.epot_sum() - s.epot_sum()) < 1e-10 * abs(s.epot_sum())
+    np.testing.assert_allclose(g.virial_ev(), s.virial_ev(), rtol=1e-10, atol=1e-8)
+    g.destroy()
+
+
+def test_lgf_trajectory_equals_oracle(ctx):
+    """100 piston steps with the oracle's normals fed to the device: energy,
+    pressure, virial and box at every 10th step."""
+    d = decks.npt_lgf_deck()
+    s, rng_o = _oracle(d)
+    E0, P0, V0 = decks.npt_run(s, d, rng_o)
+    g = _gpu(ctx, d)
+    E1, P1, V1 = decks.npt_run(g, d, O.Rng(d["seed"]), feed=_feed)
+    np.testing.assert_allclose(E1, E0, rtol=1e-9)
+    np.testing.assert_allclose(P1, P0, rtol=1e-8, atol=1e-3)
+    np.testing.assert_allclose(V1, V0, rtol=1e-8, atol=1e-8)
+    np.testing.assert_allclose(g.box_now(), s.box_now(), rtol=1e-12)
+    g.destroy()
+
+
+def test_lgf_deck_golden(ctx):
+    """lgf.gms on the GPU against Energy.lgf.dat, Press.lgf.dat and
+    Viri.lgf.dat (7 significant digits)."""
+    d = decks.npt_lgf_deck()
+    g = _gpu(ctx, d)
+    E, P, V = decks.npt_run(g, d, O.Rng(d["seed"]), feed=_feed)
+    E[:, :3] *= O.UI_EV
+    assert decks.gems_rule(d["ref_energy"][:, 0], E[:, 0]) < 1e-6
+    np.testing.assert_allclose(E, d["ref_energy"], rtol=2e-6)
+    np.testing.assert_allclose(P, d["ref_press"], rtol=2e-6, atol=1e-2)
+    np.testing.assert_allclose(V, d["ref_virial"], rtol=2e-6, atol=1e-6)
+    g.destroy()
+
+
+def test_lgf_md_steps_equals_stepwise(ctx):
+    """The captured md_steps loop (piston kernel, half steps, conditional
+    rebuilds) gives the trajectory of separate step calls bit for bit, with
+    the device's own noise."""
+    d = decks.npt_lgf_deck()
+    a = _gpu(ctx, d, seed=7)
+    b = _gpu(ctx, d, seed=7)
+    a.interact()
+    b.interact()
+    a.md_steps(120)
+    for _ in range(120):
+        b.stepa()
+        b.interact()
+        b.stepb()
+    np.testing.assert_array_equal(a.pos, b.pos)
+    np.testing.assert_array_equal(a.vel, b.vel)
+    np.testing.assert_array_equal(a.box_now(), b.box_now())
+    assert a.nupd == b.nupd
+    assert abs(a.box_now()[0] - d["box"][0]) > 1e-3
+    a.destroy()
+    b.destroy()
+
+
+def test_lgf_checkpoint_resume(ctx):
+    """lgf_flex_a/b style: 60 steps, checkpoint, a fresh system restored from
+    it runs 60 more; the straight 120-step run ends at the same state (the
+    resumed interact rebuilds the list, so the pair sums may round in
+    another order)."""
+    d = decks.npt_lgf_deck()
+    a = _gpu(ctx, d, seed=11)
+    a.md_steps(120)
+    b = _gpu(ctx, d, seed=11)
+    b.md_steps(60)
+    chp = b.checkpoint()
+    b.destroy()
+    c = _gpu(ctx, d, pos=np.zeros_like(d["pos"]), seed=11)
+    c.restore(chp)
+    c.md_steps(60)
+    np.testing.assert_allclose(c.box_now(), a.box_now(), rtol=1e-10)
+    np.testing.assert_allclose(c.pos, a.pos, rtol=0, atol=1e-8)
+    np.testing.assert_allclose(c.vel, a.vel, rtol=0, atol=1e-8 * np.abs(a.vel).max())
+    a.destroy()
+    c.destroy()
+
+
+def test_lgf_cell_grid_follows_the_box(ctx):
+    """A crystal of 12^3 fcc cells (6912 atoms) whose box is 5.01 list
+    cut-offs long, compressed at 1 e0/r0^3: between list builds the box
+    shrinks below five cut-offs, so the linked-cell grid must drop from 5^3
+    to 4^3 cells (the device re-plans it within the cells allocated, the
+    oracle recomputes it at each list update), and the trajectory stays the
+    oracle's."""
+    d = decks.npt_lgf_deck()
+    f = np.sqrt(2.0)
+    L0 = 12.0 * f
+    rc = 1.959794718597571  # slj cut-off of (1, 2^(-1/6), 1.108683)
+    skin = L0 / 5.01 - rc
+    d = dict(d, pos=decks.fcc_reply_positions(12) * f + 0.2, box=(L0,) * 3, press_atm=1.0 * 1581225.25240563)
+    s, rng_o = _oracle(d, skin=skin)
+    s.interact()
+    assert s.uses_cells() == (True, (5, 5, 5))
+    E0, P0, V0 = decks.npt_run(s, d, rng_o, nsteps=100, each=20)
+    assert s.uses_cells() == (True, (4, 4, 4)), "the compression did not change the oracle's grid"
+    g = _gpu(ctx, d, skin=skin)
+    E1, P1, V1 = decks.npt_run(g, d, O.Rng(d["seed"]), nsteps=100, each=20, feed=_feed)
+    np.testing.assert_allclose(g.box_now(), s.box_now(), rtol=1e-10)
+    np.testing.assert_allclose(E1, E0, rtol=1e-8)
+    np.testing.assert_allclose(V1, V0, rtol=1e-7, atol=1e-6)
+    g.destroy()
