@@ -110,7 +110,22 @@ void rang(Lcg& s, double* r1, double* r2) {  // always draws a pair
 
 // ---------------------------------------------------------------- system
 enum FF { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3, FF_SLJ = 4 };
-enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4 };
+enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5 };
+
+// One integrator acting on one coordinate of every atom (integrate objects
+// set by `evolve piston_lgf x|y|z` and `evolve ermak_x|y|z`,
+// Integration.F90:157-186): a G-JF piston on that box length
+// (set_lgf_flex, :652-696) or Ermak Langevin dynamics (set_ermak with a
+// coordinate, :909-961).  The reference runs a system's integrators in
+// the order they were added.
+enum AXMODE { AX_FLEX = 1, AX_ERMAK = 2 };
+struct AxisInt {
+  int mode = 0, d = 0;
+  double fac0 = 0, facg0 = 0, kin = 0, press = 0, ipm = 0, bv = 0, facv = 0, av = 0;  // piston
+  double pf = 0, pvel = 0, rangv = 0;
+  bool first = true;
+  double cc0 = 0, cc1 = 0, cc2 = 0, sdr = 0, sdv = 0, crv1 = 0, crv2 = 0, skt = 0;  // Ermak
+};
 const int MAXT = 8;
 
 // 27-cell stencil in the reference's order (Neighbour.F90:75-83): 0 is the
@@ -189,6 +204,7 @@ struct Sys {
   double lgf_fac0 = 0, lgf_facg0 = 0, lgf_kinetic = 0, lgf_press = 0, lgf_inv_pmass = 0, lgf_bv = 0,
          lgf_facv = 0, lgf_av = 0, lgf_rangv = 0, pvel = 0, pistonf = 0;
   bool lgf_first = true;
+  std::vector<AxisInt> axes;  // IT_AXES: the per-coordinate integrators in order
   int ext_used = 0;  // normals of the external stream used this step
   // FIRE state
   double fire_dt = 0, fire_dtmax = 0, fire_alpha = 0.1;
@@ -1003,10 +1019,91 @@ void lgf_b(Sys& s) {
   }
 }
 
+// lgf_flex_stepa (Integration.F90:698-776) and ermak_a_x (:1033-1082) for
+// each coordinate integrator in turn; every piston sees the volume of the
+// step's start (box_setvars runs once all have moved their lengths,
+// integration_stepa :243-264).  A piston draws its pair, then one pair per
+// atom; an Ermak coordinate one pair per atom.
+void axes_a(Sys& s) {
+  const double dt = s.dt;
+  const double vol0 = s.box[0] * s.box[1] * s.box[2];
+  for (AxisInt& a : s.axes) {
+    const int d = a.d;
+    if (a.mode == AX_FLEX) {
+      if (a.first) {
+        a.first = false;
+        a.pf = (s.virial[4 * d] + a.kin) / vol0 - a.press;
+      }
+      double r1, r2;
+      rang(*s.rng, &r1, &r2);
+      const double rangv = r1 * a.facv;
+      const double Lo = s.box[d];
+      s.box[d] = Lo + a.bv * dt * (a.pvel + 0.5 * a.ipm * (dt * a.pf * vol0 / Lo + rangv));
+      a.rangv = rangv;
+      for (int i = 0; i < s.n; i++) {
+        const double b0 = 1.0 / (1.0 + a.facg0 * s.one_mass[i]);
+        rang(*s.rng, &r1, &r2);
+        const int q = 3 * i + d;
+        s.pos_v[q] = s.one_mass[i] * a.fac0 * r1;
+        s.acel[q] = s.force[q] * s.one_mass[i];
+        s.pos[q] = s.box[d] / Lo * s.pos[q] +
+                   2.0 * s.box[d] / (Lo + s.box[d]) * b0 * dt * (s.vel[q] + 0.5 * dt * s.acel[q] + 0.5 * s.pos_v[q]);
+      }
+    } else {
+      for (int i = 0; i < s.n; i++) {
+        const double f_lan = a.skt * s.one_sqrt_mass[i];
+        double r1, r2;
+        rang(*s.rng, &r1, &r2);
+        const int q = 3 * i + d;
+        s.pos_v[q] = f_lan * a.sdr * r1;
+        s.vel_v[q] = f_lan * a.sdv * (a.crv1 * r1 + a.crv2 * r2);
+        s.pos[q] = s.pos[q] + a.cc1 * s.vel[q] + a.cc2 * dt * s.acel[q] + s.pos_v[q];
+      }
+    }
+  }
+  for (int k = 0; k < 3; k++) s.one_box[k] = 1.0 / s.box[k];
+}
+
+// lgf_flex_stepb (Integration.F90:778-830) and ermak_b_x (:1084-1105)
+void axes_b(Sys& s) {
+  const double dt = s.dt;
+  const double vol = s.box[0] * s.box[1] * s.box[2];
+  for (AxisInt& a : s.axes) {
+    const int d = a.d;
+    if (a.mode == AX_FLEX) {
+      const double pf_old = a.pf;
+      a.pf = (s.virial[4 * d] + a.kin) / vol - a.press;
+      a.pvel = a.av * a.pvel + 0.5 * a.ipm * dt * (a.av * pf_old + a.pf) * vol / s.box[d] + a.bv * a.ipm * a.rangv;
+      for (int i = 0; i < s.n; i++) {
+        const double b0 = 1.0 / (1.0 + a.facg0 * s.one_mass[i]);
+        const double a0 = (1.0 - a.facg0 * s.one_mass[i]) * b0;
+        const int q = 3 * i + d;
+        s.vel[q] = a0 * s.vel[q] + 0.5 * dt * (a0 * s.acel[q] + s.one_mass[i] * s.force[q]) + b0 * s.pos_v[q];
+        s.acel[q] = s.force[q] * s.one_mass[i];
+      }
+    } else {
+      for (int i = 0; i < s.n; i++) {
+        const int q = 3 * i + d;
+        s.vel[q] = a.cc0 * s.vel[q] + (a.cc1 - a.cc2) * s.acel[q] + a.cc2 * s.force[q] * s.one_mass[i] + s.vel_v[q];
+        s.acel[q] = s.force[q] * s.one_mass[i];
+      }
+    }
+  }
+}
+
+void add_axis(Sys& s, const AxisInt& a) {
+  if (s.integ != IT_AXES) s.axes.clear();
+  s.integ = IT_AXES;
+  if ((int)s.pos_v.size() < 3 * s.n) s.pos_v.assign(3 * s.n, 0.0);
+  if ((int)s.vel_v.size() < 3 * s.n) s.vel_v.assign(3 * s.n, 0.0);
+  s.axes.push_back(a);
+}
+
 void stepa(Sys& s) {
   if (s.integ == IT_VV || s.integ == IT_FIRE) vv_a(s);
   else if (s.integ == IT_ERMAK) ermak_a(s);
   else if (s.integ == IT_LGF) lgf_a(s);
+  else if (s.integ == IT_AXES) axes_a(s);
   do_pbc(s);
 }
 
@@ -1014,6 +1111,7 @@ void stepb(Sys& s) {
   if (s.integ == IT_VV || s.integ == IT_FIRE) vv_b(s);
   else if (s.integ == IT_ERMAK) ermak_b(s);
   else if (s.integ == IT_LGF) lgf_b(s);
+  else if (s.integ == IT_AXES) axes_b(s);
   do_pbc(s);
   if (s.integ == IT_FIRE) fire_mix(s);
 }
@@ -1751,6 +1849,47 @@ void orc_set_lgf(void* p, double dt, double temp, double press_atm, double pgama
   Sys* s = (Sys*)p;
   s->rng = (Lcg*)rng;
   set_lgf(*s, dt, temp, press_atm * atm_ui, pgama0, pgamav, pmass);
+}
+
+// `evolve piston_lgf x|y|z T gamma0 P gammav pmass` (Integration.F90:157-172;
+// set_lgf_flex :652-696), press in atm; the system's dt is dt
+void orc_add_lgf_axis(void* p, int d, double dt, double temp, double press_atm, double pgama0, double pgamav,
+                      double pmass, void* rng) {
+  Sys* s = (Sys*)p;
+  s->rng = (Lcg*)rng;
+  s->dt = dt;
+  AxisInt a;
+  a.mode = AX_FLEX;
+  a.d = d;
+  a.fac0 = std::sqrt(2.0 * pgama0 * kB_ui * temp * dt);
+  a.facg0 = 0.5 * dt * pgama0;
+  a.kin = s->n * temp * kB_ui;
+  a.press = press_atm * atm_ui;
+  a.ipm = 1.0 / pmass;
+  a.bv = 1.0 / (1.0 + 0.5 * dt * a.ipm * pgamav);
+  a.facv = std::sqrt(2.0 * pgamav * kB_ui * temp * dt);
+  a.av = (1.0 - 0.5 * dt * a.ipm * pgamav) * a.bv;
+  add_axis(*s, a);
+}
+
+// `evolve ermak_x|y|z T gamma` (Integration.F90:179-186; set_ermak with a
+// coordinate, :909-961)
+void orc_add_ermak_axis(void* p, int d, double dt, double gama, double temp, void* rng) {
+  Sys* s = (Sys*)p;
+  s->rng = (Lcg*)rng;
+  s->dt = dt;
+  AxisInt a;
+  a.mode = AX_ERMAK;
+  a.d = d;
+  a.cc0 = std::exp(-dt * gama);
+  a.cc1 = (1.0 - a.cc0) / gama;
+  a.cc2 = (1.0 - a.cc1 / dt) / gama;
+  a.sdr = std::sqrt(dt / gama * (2.0 - (3.0 - 4.0 * a.cc0 + a.cc0 * a.cc0) / (dt * gama)));
+  a.sdv = std::sqrt(1.0 - a.cc0 * a.cc0);
+  a.crv1 = (1.0 - a.cc0) * (1.0 - a.cc0) / (gama * a.sdr * a.sdv);
+  a.crv2 = std::sqrt(1.0 - (a.crv1 * a.crv1));
+  a.skt = std::sqrt(kB_ui * temp);
+  add_axis(*s, a);
 }
 
 void orc_virial_ev(void* p, double* out9) {

@@ -93,6 +93,8 @@ def lib():
         "orc_set_slj": (None, [_p, _i, _i, _d, _d, _d]),
         "orc_set_lgf": (None, [_p, _d, _d, _d, _d, _d, _d, _p]),
         "orc_virial_ev": (None, [_p, _dp]),
+        "orc_add_lgf_axis": (None, [_p, _i, _d, _d, _d, _d, _d, _d, _p]),
+        "orc_add_ermak_axis": (None, [_p, _i, _d, _d, _d, _p]),
         "orc_pressure_atm": (None, [_p, _dp]),
         "orc_get_box": (None, [_p, _dp]),
         "orc_atm_ui": (_d, []),
@@ -383,6 +385,17 @@ class System:
         self._rng = rng
         lib().orc_set_lgf(self.h, float(dt), float(temp), float(press_atm), float(pgama0), float(pgamav),
                           float(pmass), rng.h if rng is not None else None)
+
+    def add_lgf_axis(self, axis, dt, temp, press_atm, pgama0, pgamav, pmass, rng):
+        """`evolve piston_lgf x|y|z`: a G-JF piston on one box length."""
+        self._rng = rng
+        lib().orc_add_lgf_axis(self.h, int(axis), float(dt), float(temp), float(press_atm), float(pgama0),
+                               float(pgamav), float(pmass), rng.h)
+
+    def add_ermak_axis(self, axis, dt, gama, temp, rng):
+        """`evolve ermak_x|y|z`: Ermak dynamics of one coordinate."""
+        self._rng = rng
+        lib().orc_add_ermak_axis(self.h, int(axis), float(dt), float(gama), float(temp), rng.h)
 
     def virial_ev(self):
         out = np.zeros(9)

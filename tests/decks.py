@@ -215,24 +215,66 @@ def npt_lgf_deck():
                 ref_virial=np.array(g["npt_lgf_virial"]))
 
 
+def npt_axes_deck(kind):
+    """examples/NPT/lgf_flex.gms ("flex": a G-JF piston on each of x, y, z,
+    piston friction 1/tau and mass 0.1) and lgf_x.gms ("x": a piston on x
+    at 1 e0/r0^3, Ermak on y and z at 1/tau): the lgf.gms crystal and
+    potential otherwise.  `axes` lists the per-coordinate integrators in
+    deck order: ("lgf", axis, T, gamma0, P atm, gammav, pmass) or
+    ("ermak", axis, T, gamma)."""
+    g = golden()
+    d = npt_lgf_deck()
+    tau = 0.01018
+    T = 0.3 * 11604.45
+    e0r0 = 1581225.25240563
+    if kind == "flex":
+        d["axes"] = [("lgf", k, T, 1.0 / tau, 0.1 * e0r0, 1.0 / tau, 0.1) for k in range(3)]
+        d.update(ref_energy=np.array(g["npt_flex_energy"]), ref_press=np.array(g["npt_flex_press"]),
+                 ref_virial=np.array(g["npt_flex_virial"]), ref_box=None)
+    else:
+        d["axes"] = [("lgf", 0, T, 1.0 / tau, 1.0 * e0r0, 1.0 / tau, 0.1),
+                     ("ermak", 1, T, 1.0 / tau), ("ermak", 2, T, 1.0 / tau)]
+        d.update(ref_energy=np.array(g["npt_x_energy"]), ref_press=np.array(g["npt_x_press"]),
+                 ref_virial=None, ref_box=np.array(g["npt_x_box"]))
+    return d
+
+
+def npt_axes_setup(s, d, rng):
+    """The per-coordinate integrators of an npt_axes_deck, oracle or GPU
+    (`rng` is the oracle's stream or a GPU seed)."""
+    s.set_box(d["box"], (True, True, True))
+    s.set_slj(*d["slj"])
+    for a in d["axes"]:
+        if a[0] == "lgf":
+            s.add_lgf_axis(a[1], d["dt"], a[2], a[4], a[3], a[5], a[6], rng)
+        else:
+            s.add_ermak_axis(a[1], d["dt"], a[3], a[2], rng)
+
+
+def npt_axes_pairs(d, n):
+    """LCG pairs one step draws: a piston takes 1 + n, an Ermak coordinate n."""
+    return sum(1 + n if a[0] == "lgf" else n for a in d["axes"])
+
+
 def npt_setup(s, d, rng):
     s.set_box(d["box"], (True, True, True))
     s.set_slj(*d["slj"])
     s.set_lgf(d["dt"], d["temp"], d["press_atm"], d["pgama0"], d["pgamav"], d["pmass"], rng)
 
 
-def npt_run(s, d, rng, nsteps=None, each=None, feed=None):
+def npt_run(s, d, rng, nsteps=None, each=None, feed=None, boxes=None):
     """dinamic with per-step rows of (Epot, Ekin, Etot in eV, T), pressure
     (atm) and virial (eV).  `feed(s, normals)` hands each step's LCG normals
-    to an engine in parity mode (one pair for the piston, then one pair per
-    atom coordinate)."""
+    to an engine in parity mode (the pairs of one step in the order the
+    reference draws them); `boxes`, a list, receives the box lengths of each
+    row."""
     nsteps = nsteps or d["nsteps"]
     each = each or d["each"]
     s.interact()
     E, P, V = [], [], []
     for ns in range(1, nsteps + 1):
         if feed is not None:
-            feed(s, rng.rang_stream(1 + 3 * s.n))
+            feed(s, rng.rang_stream(npt_axes_pairs(d, s.n) if "axes" in d else 1 + 3 * s.n))
         s.stepa()
         s.interact()
         s.stepb()
@@ -242,6 +284,8 @@ def npt_run(s, d, rng, nsteps=None, each=None, feed=None):
             E.append([ep, ek, ep + ek, t])
             P.append(s.pressure_atm())
             V.append(s.virial_ev())
+            if boxes is not None:
+                boxes.append(s.box_now())
     return np.array(E), np.array(P), np.array(V)
 
 

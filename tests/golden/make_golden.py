@@ -56,6 +56,12 @@ def main():
         "npt_lgf_energy": rows("examples/NPT/ref/Energy.lgf.dat"),
         "npt_lgf_press": rows("examples/NPT/ref/Press.lgf.dat"),
         "npt_lgf_virial": rows("examples/NPT/ref/Viri.lgf.dat"),
+        "npt_flex_energy": rows("examples/NPT/ref/Energy.lgf_flex.dat"),
+        "npt_flex_press": rows("examples/NPT/ref/Press.lgf_flex.dat"),
+        "npt_flex_virial": rows("examples/NPT/ref/Viri.lgf_flex.dat"),
+        "npt_x_energy": rows("examples/NPT/ref/Energy.lgf_x.dat"),
+        "npt_x_press": rows("examples/NPT/ref/Press.lgf_x.dat"),
+        "npt_x_box": rows("examples/NPT/ref/Caja.lgf_x.dat"),
     }
     with open(OUT, "w") as f:
         json.dump(g, f)

@@ -175,3 +175,24 @@ def test_npt_lgf_slj_piston():
     np.testing.assert_allclose(P, d["ref_press"], rtol=2e-6, atol=1e-2)
     np.testing.assert_allclose(V, d["ref_virial"], rtol=2e-6, atol=1e-6)
     assert abs(s.box_now()[0] - d["box"][0]) > 1e-3  # the piston moved the box
+
+
+@pytest.mark.parametrize("kind", ["flex", "x"])
+def test_npt_per_coordinate_integrators(kind):
+    """examples/NPT/lgf_flex.gms (a G-JF piston on each box length) and
+    lgf_x.gms (a piston on x, Ermak on y and z): energies, pressure tensor,
+    and the virial (flex) or the box lengths (x) of each written row."""
+    d = decks.npt_axes_deck(kind)
+    s = O.System(d["pos"], d["mass"])
+    rng = O.Rng(d["seed"])
+    decks.npt_axes_setup(s, d, rng)
+    B = []
+    E, P, V = decks.npt_run(s, d, rng, boxes=B)
+    E[:, :3] *= O.UI_EV
+    assert decks.gems_rule(d["ref_energy"][:, 0], E[:, 0]) < 1e-6
+    np.testing.assert_allclose(E, d["ref_energy"], rtol=2e-6)
+    np.testing.assert_allclose(P, d["ref_press"], rtol=2e-6, atol=1e-2)
+    if d["ref_virial"] is not None:
+        np.testing.assert_allclose(V, d["ref_virial"], rtol=2e-6, atol=1e-6)
+    if d["ref_box"] is not None:
+        np.testing.assert_allclose(np.array(B), d["ref_box"], rtol=2e-7)
