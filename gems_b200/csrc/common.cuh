@@ -33,7 +33,10 @@ __device__ __forceinline__ void stencil(int k, int& dx, int& dy, int& dz) {
 }
 
 enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
-enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4 };
+enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5 };
+// IT_AXES: one integrator per coordinate -- a G-JF piston on that box length
+// (AX_FLEX) or Ermak dynamics of that coordinate (AX_ERMAK)
+enum AX : int { AX_NONE = 0, AX_FLEX = 1, AX_ERMAK = 2 };
 enum PREC : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 
 // status bits of a system (SysState::status)
@@ -93,6 +96,13 @@ struct SysDev {
   int cell_cap;        // cells allocated (a moving box may re-grid within them)
   double rlist;        // rcut + skin
   double lgf_fac0, lgf_facg0, lgf_kin, lgf_press, lgf_ipm, lgf_bv, lgf_facv, lgf_av;
+  // IT_AXES, per coordinate: the mode and its constants --
+  // AX_FLEX (set_lgf_flex, Integration.F90:652-696):
+  //   fac0 facg0 kin press 1/pmass bv facv av
+  // AX_ERMAK (set_ermak, :909-961): cc0 cc1 cc2 sdr sdv crv1 crv2 sqrt(kB T)
+  int ax_mode[3];
+  int pad3;
+  double ax_p[3][8];
 };
 
 // Dynamic state of a system, written only by kernels (and reset by host).
@@ -119,6 +129,11 @@ struct SysState {
   double box_b[3];   // box at the last rebuild (list skin vs box motion)
   int lgf_phase;     // 0 until the first piston step (pistonf from the virial)
   int pad2;
+  // IT_AXES pistons, per coordinate: force, velocity, last noise, fed
+  // normal, phase
+  double ax_pf[3], ax_pvel[3], ax_rangv[3], ax_ext[3];
+  int ax_phase[3];
+  int pad4;
 };
 
 // Block map: block b covers atoms [first[b], end[b]) of system sys[b];

@@ -55,7 +55,16 @@ struct SysHost {
   bool ff_set = false;
   double temp = 0.0;        // Ermak bath temperature (K)
   bool box_live = false;    // the device moved the box (constant pressure)
+  std::vector<int> ax_order;  // IT_AXES: coordinates in the order their integrators were added
 };
+
+// a system whose box the device moves (a G-JF piston on the volume or on
+// a length)
+bool moving_box(const SysDev& d) {
+  if (d.integ == IT_LGF) return true;
+  if (d.integ != IT_AXES) return false;
+  return d.ax_mode[0] == AX_FLEX || d.ax_mode[1] == AX_FLEX || d.ax_mode[2] == AX_FLEX;
+}
 
 struct Graph {
   cudaGraphExec_t exec = nullptr;
@@ -438,7 +447,7 @@ void derive(gemsgpu_ctx* ctx, SysHost& h) {
 // into as the box moves
 int cells_needed(const SysHost& h) {
   if (!h.d.use_cells) return 0;
-  if (h.d.integ != IT_LGF) return h.d.ncell;
+  if (!moving_box(h.d)) return h.d.ncell;
   int64_t m = 1;
   for (int k = 0; k < 3; k++) m *= std::max(h.d.nc[k], (int)(1.15 * h.d.L[k] / h.d.rlist));
   return (int)std::min<int64_t>(m, 1 << 26);
@@ -513,7 +522,7 @@ int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, Blo
       if (!h.d.use_cells) continue;
       lo = h.cell_off;
       // a moving box re-plans its grid on the device within its allocation
-      hi = h.cell_off + (h.d.integ == IT_LGF ? h.cell_cap : h.d.ncell);
+      hi = h.cell_off + (moving_box(h.d) ? h.cell_cap : h.d.ncell);
     }
     blk0[s] = (int)bs.size();
     for (int a = lo; a < hi; a += apb) {
@@ -707,14 +716,14 @@ int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss,
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
   bool piston = false;
-  for (int s : ss) piston |= ctx->sys[s].d.integ == IT_LGF;
+  for (int s : ss) piston |= ctx->sys[s].d.integ == IT_LGF || ctx->sys[s].d.integ == IT_AXES;
   if (piston) {
     const int* sa;
     CHK(sys_array(ctx, ss, &sa));
     k_lgf_sys<<<((int)ss.size() + 127) / 128, 128, 0, ctx->stream>>>(ctx->A, sa, (int)ss.size());
     ++ctx->launches;
     for (int s : ss)
-      if (ctx->sys[s].d.integ == IT_LGF) ctx->sys[s].box_live = true;
+      if (moving_box(ctx->sys[s].d)) ctx->sys[s].box_live = true;
   }
   if (use_cond) k_step_a<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
   else k_step_a<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
@@ -1713,7 +1722,7 @@ int gemsgpu_set_box(gemsgpu_ctx* ctx, int sys, int boxed, const double L[3], con
     for (int k = 0; k < 3; k++)
       if (!(L[k] > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "set_box: L must be positive");
   }
-  if (h.d.integ == IT_LGF && !boxed) return fail(ctx, GEMSGPU_ERR_STATE, "set_box: a piston system keeps its box");
+  if (moving_box(h.d) && !boxed) return fail(ctx, GEMSGPU_ERR_STATE, "set_box: a piston system keeps its box");
   h.box_live = false;  // the given box replaces the one the pistons moved
   h.d.boxed = boxed ? 1 : 0;
   for (int k = 0; k < 3; k++) {
@@ -1759,7 +1768,7 @@ int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec) {
   CHK(check_sys(ctx, sys));
   if (prec != GEMSGPU_PREC_FP64 && prec != GEMSGPU_PREC_MIXED)
     return fail(ctx, GEMSGPU_ERR_ARG, "unknown precision %d", prec);
-  if (prec != GEMSGPU_PREC_FP64 && (ctx->sys[sys].d.integ == IT_LGF || ctx->sys[sys].d.virial))
+  if (prec != GEMSGPU_PREC_FP64 && (moving_box(ctx->sys[sys].d) || ctx->sys[sys].d.virial))
     return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: the virial and the piston are FP64 only");
   if (prec != GEMSGPU_PREC_FP64 && ctx->sys[sys].d.ff == FF_LJ)
     for (const PairP& P : ctx->sys[sys].prm)
@@ -2062,7 +2071,7 @@ int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on) {
   SysHost& h = ctx->sys[sys];
   if (on && h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "virial: pair potentials (lj, plj, slj) only");
   if (on && h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "virial: FP64 systems only");
-  if (!on && h.d.integ == IT_LGF) return fail(ctx, GEMSGPU_ERR_STATE, "virial: the piston needs it");
+  if (!on && moving_box(h.d)) return fail(ctx, GEMSGPU_ERR_STATE, "virial: the piston needs it");
   h.d.virial = on ? 1 : 0;
   h.has_forces = false;
   CHK(push_sys(ctx, sys));
@@ -2120,9 +2129,30 @@ int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
 int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals) {
   CHK(check_sys(ctx, sys));
   SysHost& h = ctx->sys[sys];
-  if (h.d.integ != IT_LGF) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf_normals: not a piston system");
+  if (h.d.integ != IT_LGF && h.d.integ != IT_AXES)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf_normals: not a piston or per-coordinate system");
   if (!normals) {
     h.d.use_ext_normals = 0;
+  } else if (h.d.integ == IT_AXES) {
+    // the pairs in draw order, scattered to (atom, coordinate) slots
+    std::vector<double> nrm(6 * (size_t)h.n, 0.0);
+    double pist[3] = {0, 0, 0};
+    const double* q = normals;
+    for (int d : h.ax_order) {
+      if (h.d.ax_mode[d] == AX_FLEX) {
+        pist[d] = q[0];
+        q += 2;
+      }
+      for (int i = 0; i < h.n; i++, q += 2) {
+        nrm[6 * (size_t)i + 2 * d] = q[0];
+        nrm[6 * (size_t)i + 2 * d + 1] = q[1];
+      }
+    }
+    CU(cudaMemcpyAsync(ctx->A.ext_normals + (size_t)6 * h.off, nrm.data(), nrm.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->A.st[sys].ax_ext, pist, sizeof(pist), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    h.d.use_ext_normals = 1;
   } else {
     CU(cudaMemcpyAsync(ctx->A.ext_normals + (size_t)6 * h.off, normals + 2, (size_t)6 * h.n * sizeof(double),
                        cudaMemcpyHostToDevice, ctx->stream));
@@ -2133,6 +2163,86 @@ int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals) {
   CHK(push_sys(ctx, sys));
   CU(cudaStreamSynchronize(ctx->stream));
   return 0;
+}
+
+// one per-coordinate integrator more (IT_AXES); a system that had another
+// integrator starts an empty set
+static int add_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt, int mode, const double p[8], uint64_t seed) {
+  SysHost& h = ctx->sys[sys];
+  SysDev& d = h.d;
+  if (d.integ != IT_AXES) {
+    d.integ = IT_AXES;
+    for (int k = 0; k < 3; k++) d.ax_mode[k] = AX_NONE;
+    h.ax_order.clear();
+    d.dt = dt;
+  }
+  if (d.ax_mode[axis] != AX_NONE)
+    return fail(ctx, GEMSGPU_ERR_STATE, "coordinate %d already has an integrator", axis);
+  if (dt != d.dt) return fail(ctx, GEMSGPU_ERR_ARG, "per-coordinate integrators share one dt");
+  d.ax_mode[axis] = mode;
+  for (int k = 0; k < 8; k++) d.ax_p[axis][k] = p[k];
+  h.ax_order.push_back(axis);
+  d.seed = seed;
+  d.use_ext_normals = 0;
+  if (mode == AX_FLEX) {
+    d.virial = 1;
+    h.has_forces = false;  // the first piston step needs the virial
+  }
+  CHK(push_sys(ctx, sys));
+  CHK(read_states(ctx));
+  SysState st = ctx->h_st[sys];
+  st.ax_phase[axis] = 0;
+  st.ax_pf[axis] = st.ax_pvel[axis] = st.ax_rangv[axis] = 0.0;
+  for (int k = 0; k < 3; k++) st.box_b[k] = d.L[k];
+  CU(cudaMemcpyAsync(ctx->A.st + sys, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+// set_lgf_flex (src/Integration.F90:652-696): a G-JF piston on one length
+int gemsgpu_add_lgf_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt, double temp, double press_atm,
+                         double pgama0, double pgamav, double pmass, uint64_t seed) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (axis < 0 || axis > 2) return fail(ctx, GEMSGPU_ERR_ARG, "add_lgf_axis: axis 0, 1 or 2");
+  if (!(dt > 0.0) || !(temp >= 0.0) || !(pgama0 >= 0.0) || !(pgamav >= 0.0) || !(pmass > 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "add_lgf_axis: dt>0, T>=0, gammas>=0, piston mass>0");
+  if (!h.d.boxed || !h.d.pbc[axis])
+    return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: the piston needs a box periodic along its axis");
+  if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: pair potentials (lj, plj, slj) only");
+  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: FP64 systems only");
+  double p[8];
+  p[0] = std::sqrt(2.0 * pgama0 * kB_ui * temp * dt);
+  p[1] = 0.5 * dt * pgama0;
+  p[2] = h.n * temp * kB_ui;
+  p[3] = press_atm * atm_ui();
+  p[4] = 1.0 / pmass;
+  p[5] = 1.0 / (1.0 + 0.5 * dt * p[4] * pgamav);
+  p[6] = std::sqrt(2.0 * pgamav * kB_ui * temp * dt);
+  p[7] = (1.0 - 0.5 * dt * p[4] * pgamav) * p[5];
+  return add_axis(ctx, sys, axis, dt, AX_FLEX, p, seed);
+}
+
+// set_ermak with a coordinate (src/Integration.F90:909-961): Ermak
+// dynamics of one coordinate
+int gemsgpu_add_ermak_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt, double gama, double temp,
+                           uint64_t seed) {
+  CHK(check_sys(ctx, sys));
+  if (axis < 0 || axis > 2) return fail(ctx, GEMSGPU_ERR_ARG, "add_ermak_axis: axis 0, 1 or 2");
+  if (!(dt > 0.0) || !(gama > 0.0) || !(temp >= 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "add_ermak_axis: dt>0, gamma>0, T>=0");
+  double p[8];
+  p[0] = std::exp(-dt * gama);
+  p[1] = (1.0 - p[0]) / gama;
+  p[2] = (1.0 - p[1] / dt) / gama;
+  p[3] = std::sqrt(dt / gama * (2.0 - (3.0 - 4.0 * p[0] + p[0] * p[0]) / (dt * gama)));
+  p[4] = std::sqrt(1.0 - p[0] * p[0]);
+  p[5] = (1.0 - p[0]) * (1.0 - p[0]) / (gama * p[3] * p[4]);
+  p[6] = std::sqrt(1.0 - (p[5] * p[5]));
+  p[7] = std::sqrt(kB_ui * temp);
+  return add_axis(ctx, sys, axis, dt, AX_ERMAK, p, seed);
 }
 
 int gemsgpu_get_box(gemsgpu_ctx* ctx, int sys, double L[3]) {
@@ -2690,7 +2800,7 @@ int gemsgpu_pool_set(gemsgpu_pool* P, const int* sys, int nsys) {
     if (s >= P->scap) return fail(ctx, GEMSGPU_ERR_FULL, "system id beyond the pool's capacity");
     if ((P->variant & 1) == 0 && ctx->sys[s].ntypes != 1)
       return fail(ctx, GEMSGPU_ERR_STATE, "pool variant %d needs single-species systems", P->variant);
-    if (ctx->sys[s].d.integ == IT_LGF || ctx->sys[s].d.virial)
+    if (moving_box(ctx->sys[s].d) || ctx->sys[s].d.virial)
       return fail(ctx, GEMSGPU_ERR_STATE, "pool_set: pools run fixed boxes without the virial");
     atoms += ctx->sys[s].n;
   }
@@ -2913,6 +3023,8 @@ struct ChpHeader {
   double box[3];
   double lgf_pf, lgf_pvel, lgf_rangv;
   int32_t lgf_phase, pad;
+  double ax_pf[3], ax_pvel[3], ax_rangv[3];
+  int32_t ax_phase[3], pad2;
 };
 }  // namespace
 
@@ -2932,7 +3044,7 @@ int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes) 
   const SysState& st = ctx->h_st[sys];
   ChpHeader hd{};
   memcpy(hd.magic, "GEMSGPU", 8);
-  hd.version = 2;
+  hd.version = 3;
   hd.n = h.n;
   hd.ff = h.d.ff;
   hd.integ = h.d.integ;
@@ -2949,6 +3061,12 @@ int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes) 
   hd.lgf_pvel = st.lgf_pvel;
   hd.lgf_rangv = st.lgf_rangv;
   hd.lgf_phase = st.lgf_phase;
+  for (int k = 0; k < 3; k++) {
+    hd.ax_pf[k] = st.ax_pf[k];
+    hd.ax_pvel[k] = st.ax_pvel[k];
+    hd.ax_rangv[k] = st.ax_rangv[k];
+    hd.ax_phase[k] = st.ax_phase[k];
+  }
   char* p = static_cast<char*>(buf);
   memcpy(p, &hd, sizeof(hd));
   double* x = reinterpret_cast<double*>(p + sizeof(hd));
@@ -2965,10 +3083,10 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   SysHost& h = ctx->sys[sys];
   ChpHeader hd;
   memcpy(&hd, buf, sizeof(hd));
-  if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || hd.version != 2)
+  if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || hd.version != 3)
     return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: not a checkpoint of this library");
   if (hd.n != h.n) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %d atoms, system has %d", hd.n, h.n);
-  if (h.d.boxed && (h.d.integ == IT_LGF || hd.integ == IT_LGF)) {
+  if (h.d.boxed && (moving_box(h.d) || hd.integ == IT_LGF || hd.integ == IT_AXES)) {
     // the box the piston had reached
     h.box_live = false;
     for (int k = 0; k < 3; k++) h.d.L[k] = hd.box[k];
@@ -2994,7 +3112,13 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   st.lgf_pvel = hd.lgf_pvel;
   st.lgf_rangv = hd.lgf_rangv;
   st.lgf_phase = hd.lgf_phase;
-  for (int k = 0; k < 3; k++) st.box_b[k] = h.d.L[k];
+  for (int k = 0; k < 3; k++) {
+    st.box_b[k] = h.d.L[k];
+    st.ax_pf[k] = hd.ax_pf[k];
+    st.ax_pvel[k] = hd.ax_pvel[k];
+    st.ax_rangv[k] = hd.ax_rangv[k];
+    st.ax_phase[k] = hd.ax_phase[k];
+  }
   st.status = 0;
   CU(cudaMemcpyAsync(ctx->A.st + sys, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
   BlockMap m;

@@ -1525,6 +1525,144 @@ __device__ __forceinline__ void lgf_b_atom(const SysDev& S, double om, const dou
   a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
 }
 
+// component D of a double4 (a compile-time index keeps it in registers)
+template <int D>
+__device__ __forceinline__ double& cmp(double4& v) {
+  if constexpr (D == 0) return v.x;
+  else if constexpr (D == 1) return v.y;
+  else return v.z;
+}
+template <int D>
+__device__ __forceinline__ double cmp(const double4& v) {
+  if constexpr (D == 0) return v.x;
+  else if constexpr (D == 1) return v.y;
+  else return v.z;
+}
+
+// Half step a of coordinate D under its own integrator (IT_AXES):
+// lgf_flex_stepa (src/Integration.F90:698-776) -- the same update as the
+// isotropic piston on this coordinate alone -- or ermak_a_x (:1033-1082);
+// r1, r2: this atom's normal pair for the coordinate.  pv receives the
+// piston's noise displacement or Ermak's velocity kick.
+template <int D>
+__device__ __forceinline__ void axis_a(const SysDev& S, const SysState& st, double om, double osm, double r1,
+                                       double r2, const double4& F, const double4& v, double4& a, double4& x,
+                                       double4& pv) {
+  const double* p = S.ax_p[D];
+  if (S.ax_mode[D] == AX_FLEX) {
+    const double b0 = 1.0 / (1.0 + p[1] * om);
+    cmp<D>(pv) = om * p[0] * r1;
+    cmp<D>(a) = cmp<D>(F) * om;
+    cmp<D>(x) = st.lgf_sc[D] * cmp<D>(x) +
+                st.lgf_f2[D] * b0 * S.dt * (cmp<D>(v) + 0.5 * S.dt * cmp<D>(a) + 0.5 * cmp<D>(pv));
+  } else if (S.ax_mode[D] == AX_ERMAK) {
+    const double f_lan = p[7] * osm;
+    const double pr = f_lan * p[3] * r1;
+    cmp<D>(pv) = f_lan * p[4] * (p[5] * r1 + p[6] * r2);
+    cmp<D>(x) = cmp<D>(x) + p[1] * cmp<D>(v) + p[2] * S.dt * cmp<D>(a) + pr;
+  }
+}
+
+// Half step b of coordinate D: lgf_flex_stepb (:778-830) or ermak_b_x
+// (:1084-1105); a coordinate without an integrator keeps its velocity
+template <int D>
+__device__ __forceinline__ void axis_b(const SysDev& S, double om, const double4& F, const double4& pv, double4& v,
+                                       double4& a) {
+  const double* p = S.ax_p[D];
+  if (S.ax_mode[D] == AX_FLEX) {
+    const double b0 = 1.0 / (1.0 + p[1] * om);
+    const double a0 = (1.0 - p[1] * om) * b0;
+    cmp<D>(v) = a0 * cmp<D>(v) + 0.5 * S.dt * (a0 * cmp<D>(a) + om * cmp<D>(F)) + b0 * cmp<D>(pv);
+    cmp<D>(a) = cmp<D>(F) * om;
+  } else if (S.ax_mode[D] == AX_ERMAK) {
+    cmp<D>(v) = p[0] * cmp<D>(v) + (p[1] - p[2]) * cmp<D>(a) + p[2] * cmp<D>(F) * om + cmp<D>(pv);
+    cmp<D>(a) = cmp<D>(F) * om;
+  }
+}
+
+__device__ __forceinline__ void axes_a_atom(const Arena& A, const SysDev& S, const SysState& st, int i,
+                                            double2 mi, const double4& F, const double4& v, double4& a,
+                                            double4& x, double4& pv) {
+  double r[6];
+  if (S.use_ext_normals) {
+#pragma unroll
+    for (int k = 0; k < 6; k++) r[k] = A.ext_normals[(size_t)6 * i + k];
+  } else {
+    normals6((uint32_t)(i - S.off), st.step, S.seed, r);
+  }
+  pv = make_double4(0, 0, 0, 0);
+  axis_a<0>(S, st, mi.x, mi.y, r[0], r[1], F, v, a, x, pv);
+  axis_a<1>(S, st, mi.x, mi.y, r[2], r[3], F, v, a, x, pv);
+  axis_a<2>(S, st, mi.x, mi.y, r[4], r[5], F, v, a, x, pv);
+}
+
+// re-plan a moving box's cell grid for its new lengths (intergroup_setcells,
+// cells no smaller than the list cut-off) within the cells allocated, with
+// fewer, larger cells where the allocation is short; below three cells a
+// dimension's stencil would visit a cell twice
+__device__ __forceinline__ void regrid(SysDev& S, SysState& st) {
+  if (!S.use_cells) return;
+  int nc[3];
+  for (int d = 0; d < 3; d++) nc[d] = (int)(S.L[d] / S.rlist);
+  while ((int64_t)nc[0] * nc[1] * nc[2] > S.cell_cap) {
+    int m = nc[1] > nc[0] ? 1 : 0;
+    if (nc[2] > nc[m]) m = 2;
+    nc[m]--;
+  }
+  if (nc[0] < 3 || nc[1] < 3 || nc[2] < 3) {
+    atomicOr(&st.status, ST_BOX);
+    return;
+  }
+  for (int d = 0; d < 3; d++) {
+    S.nc[d] = nc[d];
+    S.cell[d] = S.L[d] / nc[d];
+    S.inv_cell[d] = 1.0 / S.cell[d];
+  }
+  S.ncell = nc[0] * nc[1] * nc[2];
+}
+
+// Per-coordinate pistons (IT_AXES), one thread per system: each closes its
+// previous step (lgf_flex_stepb: pistonf from the virial's diagonal entry,
+// pvel with the factor V / L) and moves its length (lgf_flex_stepa)
+//   L' = L + b dt (pvel + (dt pistonf V / L + rangv) / (2 Q)),
+// every piston with the volume of the step's start, as the reference
+// updates the volume only once all of them have moved.
+__device__ __forceinline__ void axes_sys(SysDev& S, SysState& st) {
+  const double dt = S.dt;
+  const double vol0 = S.L[0] * S.L[1] * S.L[2];
+  double q[6];
+  if (!S.use_ext_normals) normals6((uint32_t)S.n, st.step, S.seed, q);
+  double Ln[3];
+  for (int d = 0; d < 3; d++) {
+    Ln[d] = S.L[d];
+    if (S.ax_mode[d] != AX_FLEX) continue;
+    const double* p = S.ax_p[d];
+    const double pf = (st.vir[d] + p[2]) / vol0 - p[3];
+    if (st.ax_phase[d] == 0) {
+      st.ax_phase[d] = 1;
+    } else {
+      st.ax_pvel[d] = p[7] * st.ax_pvel[d] + 0.5 * p[4] * dt * (p[7] * st.ax_pf[d] + pf) * vol0 / S.L[d] +
+                      p[5] * p[4] * st.ax_rangv[d];
+    }
+    st.ax_pf[d] = pf;
+    const double rangv = (S.use_ext_normals ? st.ax_ext[d] : q[d]) * p[6];
+    st.ax_rangv[d] = rangv;
+    Ln[d] = S.L[d] + p[5] * dt * (st.ax_pvel[d] + 0.5 * p[4] * (dt * pf * vol0 / S.L[d] + rangv));
+  }
+  for (int d = 0; d < 3; d++) {
+    if (!(Ln[d] > 0.0)) {
+      atomicOr(&st.status, ST_BOX);
+      Ln[d] = S.L[d];
+    }
+    const double Lo = S.L[d];
+    st.lgf_sc[d] = Ln[d] / Lo;
+    st.lgf_f2[d] = 2.0 * Ln[d] / (Lo + Ln[d]);
+    S.L[d] = Ln[d];
+    S.invL[d] = 1.0 / Ln[d];
+  }
+  regrid(S, st);
+}
+
 // The G-JF piston of each constant-pressure system (one thread per system),
 // ahead of the atoms' half step.  It first closes the previous step's
 // piston (lgf_stepb: pistonf from the virial of the last force evaluation
@@ -1542,6 +1680,10 @@ __global__ void k_lgf_sys(Arena A, const int* sys, int nsys) {
   if (s < 0) return;
   SysDev& S = A.sys[s];
   SysState& st = A.st[s];
+  if (S.integ == IT_AXES) {
+    axes_sys(S, st);
+    return;
+  }
   if (S.integ != IT_LGF) return;
   const double dt = S.dt;
   const double vol0 = S.L[0] * S.L[1] * S.L[2];
@@ -1578,28 +1720,7 @@ __global__ void k_lgf_sys(Arena A, const int* sys, int nsys) {
     S.L[d] = Ln;
     S.invL[d] = 1.0 / Ln;
   }
-  if (S.use_cells) {
-    // intergroup_setcells for the new box (cells no smaller than the list
-    // cut-off); fewer, larger cells where the allocation is short; below
-    // three cells a dimension's stencil would visit a cell twice
-    int nc[3];
-    for (int d = 0; d < 3; d++) nc[d] = (int)(S.L[d] / S.rlist);
-    while ((int64_t)nc[0] * nc[1] * nc[2] > S.cell_cap) {
-      int m = nc[1] > nc[0] ? 1 : 0;
-      if (nc[2] > nc[m]) m = 2;
-      nc[m]--;
-    }
-    if (nc[0] < 3 || nc[1] < 3 || nc[2] < 3) {
-      atomicOr(&st.status, ST_BOX);
-    } else {
-      for (int d = 0; d < 3; d++) {
-        S.nc[d] = nc[d];
-        S.cell[d] = S.L[d] / nc[d];
-        S.inv_cell[d] = 1.0 / S.cell[d];
-      }
-      S.ncell = nc[0] * nc[1] * nc[2];
-    }
-  }
+  regrid(S, st);
 }
 
 // the moved atom's outputs: position, fixed-point copy, skin displacement
@@ -1634,7 +1755,7 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
       // the change of its lengths since the build, on top of the atoms'
       // own displacements
       double box = 0.0;
-      if (PISTON && S.integ == IT_LGF)
+      if (PISTON && (S.integ == IT_LGF || S.integ == IT_AXES))
         box = fabs(S.L[0] - st.box_b[0]) + fabs(S.L[1] - st.box_b[1]) + fabs(S.L[2] - st.box_b[2]);
       int rb = __dadd_rn(__dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)), box) > S.skin;
       if (frozen) rb = 0;
@@ -1643,7 +1764,7 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
         atomicOr(A.any_rebuild, 1);
         if constexpr (COND) cudaGraphSetConditional(cond, 1u);
       }
-      if ((S.integ == IT_ERMAK || S.integ == IT_LGF) && !S.use_ext_normals) st.step++;
+      if ((S.integ == IT_ERMAK || S.integ == IT_LGF || S.integ == IT_AXES) && !S.use_ext_normals) st.step++;
       if (S.integ == IT_FIRE) st.fire_zero = 0;
     }
   }
@@ -1683,6 +1804,11 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
     } else if (S.integ == IT_LGF) {
       double4 pv;
       lgf_a_atom(A, S, st, i, mi.x, A.force[i], v, a, x, pv);
+      A.acel[i] = a;
+      A.vel_v[i] = pv;
+    } else if (S.integ == IT_AXES) {
+      double4 pv;
+      axes_a_atom(A, S, st, i, mi, A.force[i], v, a, x, pv);
       A.acel[i] = a;
       A.vel_v[i] = pv;
     }
@@ -1767,6 +1893,11 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
       ermak_b_atom(S, om, F, A.vel_v[i], v, a);
     } else if (S.integ == IT_LGF) {
       lgf_b_atom(S, om, F, A.vel_v[i], v, a);
+    } else if (S.integ == IT_AXES) {
+      const double4 pv = A.vel_v[i];
+      axis_b<0>(S, om, F, pv, v, a);
+      axis_b<1>(S, om, F, pv, v, a);
+      axis_b<2>(S, om, F, pv, v, a);
     }
     A.vel[i] = v;
     A.acel[i] = a;

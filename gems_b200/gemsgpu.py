@@ -65,6 +65,8 @@ _SIGS = {
     "gemsgpu_set_virial": (_i, [_p, _i, _i]),
     "gemsgpu_set_lgf": (_i, [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_set_lgf_normals": (_i, [_p, _i, _dp]),
+    "gemsgpu_add_lgf_axis": (_i, [_p, _i, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
+    "gemsgpu_add_ermak_axis": (_i, [_p, _i, _i, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_get_box": (_i, [_p, _i, _dp]),
     "gemsgpu_virial": (_i, [_p, _i, _dp]),
     "gemsgpu_pressure": (_i, [_p, _i, _dp]),
@@ -481,9 +483,11 @@ class System:
 
     # integrators -------------------------------------------------------------
     def set_vv(self, dt):
+        self._axes = []
         self._c(lib().gemsgpu_set_vv(self.ctx.h, self.sid, float(dt)))
 
     def set_ermak(self, dt, gama, temp, seed=12345):
+        self._axes = []
         self._c(lib().gemsgpu_set_ermak(self.ctx.h, self.sid, float(dt), float(gama), float(temp), int(seed)))
 
     def set_ermak_normals(self, nrm):
@@ -491,18 +495,38 @@ class System:
         self._c(lib().gemsgpu_set_ermak_normals(self.ctx.h, self.sid, _ptr(a)))
 
     def set_fire(self, dt0, dtmax):
+        self._axes = []
         self._c(lib().gemsgpu_set_fire(self.ctx.h, self.sid, float(dt0), float(dtmax)))
 
     def set_lgf(self, dt, temp, press_atm, pgama0, pgamav, pmass, seed=12345):
         """set_lgf (`evolve piston_lgf xyz*`): G-JF constant pressure and
         temperature; pressure in atm, frictions in 1/ps."""
+        self._axes = []
         self._c(lib().gemsgpu_set_lgf(self.ctx.h, self.sid, float(dt), float(temp), float(press_atm),
                                       float(pgama0), float(pgamav), float(pmass), int(seed)))
 
+    def add_lgf_axis(self, axis, dt, temp, press_atm, pgama0, pgamav, pmass, seed=12345):
+        """`evolve piston_lgf x|y|z`: a G-JF piston on one box length."""
+        self._c(lib().gemsgpu_add_lgf_axis(self.ctx.h, self.sid, int(axis), float(dt), float(temp),
+                                           float(press_atm), float(pgama0), float(pgamav), float(pmass),
+                                           int(seed)))
+        self._axes = getattr(self, "_axes", []) + ["lgf"]
+
+    def add_ermak_axis(self, axis, dt, gama, temp, seed=12345):
+        """`evolve ermak_x|y|z`: Ermak dynamics of one coordinate."""
+        self._c(lib().gemsgpu_add_ermak_axis(self.ctx.h, self.sid, int(axis), float(dt), float(gama),
+                                             float(temp), int(seed)))
+        self._axes = getattr(self, "_axes", []) + ["ermak"]
+
     def set_lgf_normals(self, nrm):
-        """Next step's normals: the piston's rang pair, then a pair per atom
-        coordinate (2 + 6 n values; None returns to the device stream)."""
-        a = None if nrm is None else _f64(nrm, 2 + 6 * self.n)
+        """Next step's normal pairs in the order the reference draws them:
+        isotropic piston -- the piston's pair, then a pair per atom
+        coordinate (2 + 6 n values); per-coordinate integrators -- for each
+        in order, a piston's pair and a pair per atom, or a pair per atom.
+        None returns to the device stream."""
+        axes = getattr(self, "_axes", [])
+        pairs = sum(1 + self.n if a == "lgf" else self.n for a in axes) if axes else 1 + 3 * self.n
+        a = None if nrm is None else _f64(nrm, 2 * pairs)
         self._c(lib().gemsgpu_set_lgf_normals(self.ctx.h, self.sid, _ptr(a)))
 
     def box_now(self):

@@ -205,11 +205,29 @@ int gemsgpu_set_fire(gemsgpu_ctx* ctx, int sys, double dt0, double dtmax);
 int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp,
                     double press_atm, double pgama0, double pgamav,
                     double pmass, uint64_t seed);
-/* Parity mode: the next step_a of a piston system consumes these normals,
- * 2 + 6 n values in the order rang() draws them in lgf_stepa
- * (Integration.F90:561-590): the piston's pair, then a pair per atom and
- * coordinate (the first value of each pair is used).  NULL returns to the
- * device stream. */
+/* One integrator per coordinate (`evolve piston_lgf x|y|z` and
+ * `evolve ermak_x|y|z`, Integration.F90:157-186): a G-JF piston on one box
+ * length (set_lgf_flex, :652-696; lgf_flex_stepa/b, :698-830; arguments as
+ * gemsgpu_set_lgf) or Ermak dynamics of one coordinate (set_ermak with a
+ * coordinate, :909-961; ermak_a_x/b_x, :1033-1105).  axis 0, 1, 2 = x, y,
+ * z; each call adds one integrator (a system that had another kind of
+ * integrator starts an empty set), all with the same dt, at most one per
+ * coordinate; a coordinate without one keeps its velocity.  The pistons
+ * move their lengths with the volume of the step's start, as the reference
+ * updates the volume after all of them.  Pistons need an FP64
+ * pair-potential system periodic along their axis. */
+int gemsgpu_add_lgf_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt,
+                         double temp, double press_atm, double pgama0,
+                         double pgamav, double pmass, uint64_t seed);
+int gemsgpu_add_ermak_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt,
+                           double gamma, double temp, uint64_t seed);
+/* Parity mode: the next step_a of a piston or per-coordinate system
+ * consumes these normal pairs, in the order rang() draws them.  Isotropic
+ * piston (lgf_stepa, Integration.F90:561-590): 2 + 6 n values, the
+ * piston's pair, then a pair per atom and coordinate (the first value of
+ * each pair is used).  Per-coordinate integrators, in the order they were
+ * added: a piston's pair then a pair per atom, or an Ermak coordinate's
+ * pair per atom.  NULL returns to the device stream. */
 int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals);
 /* The box lengths (A) as the device holds them (moved by a piston). */
 int gemsgpu_get_box(gemsgpu_ctx* ctx, int sys, double L[3]);

@@ -157,3 +157,70 @@ def test_lgf_cell_grid_follows_the_box(ctx):
     np.testing.assert_allclose(E1, E0, rtol=1e-8)
     np.testing.assert_allclose(V1, V0, rtol=1e-7, atol=1e-6)
     g.destroy()
+
+
+def _gpu_axes(ctx, d, seed=12345, pos=None):
+    g = gems.System(d["pos"] if pos is None else pos, d["mass"], ctx=ctx)
+    g.set_skin_mode(False)
+    decks.npt_axes_setup(g, d, seed)
+    return g
+
+
+@pytest.mark.parametrize("kind", ["flex", "x"])
+def test_per_coordinate_decks(ctx, kind):
+    """lgf_flex.gms (a piston on each length) and lgf_x.gms (a piston on x,
+    Ermak on y and z) on the GPU with the LCG normals fed in draw order:
+    the oracle's rows to 1e-9 and the golden files to their 7 digits."""
+    d = decks.npt_axes_deck(kind)
+    s = O.System(d["pos"], d["mass"])
+    rng_o = O.Rng(d["seed"])
+    decks.npt_axes_setup(s, d, rng_o)
+    B0 = []
+    E0, P0, V0 = decks.npt_run(s, d, rng_o, boxes=B0)
+    g = _gpu_axes(ctx, d)
+    B1 = []
+    E1, P1, V1 = decks.npt_run(g, d, O.Rng(d["seed"]), feed=_feed, boxes=B1)
+    np.testing.assert_allclose(E1, E0, rtol=1e-9)
+    np.testing.assert_allclose(P1, P0, rtol=1e-8, atol=1e-3)
+    np.testing.assert_allclose(np.array(B1), np.array(B0), rtol=1e-12)
+    E1[:, :3] *= O.UI_EV
+    np.testing.assert_allclose(E1, d["ref_energy"], rtol=2e-6)
+    np.testing.assert_allclose(P1, d["ref_press"], rtol=2e-6, atol=1e-2)
+    if d["ref_virial"] is not None:
+        np.testing.assert_allclose(V1, d["ref_virial"], rtol=2e-6, atol=1e-6)
+    if d["ref_box"] is not None:
+        np.testing.assert_allclose(np.array(B1), d["ref_box"], rtol=2e-7)
+    g.destroy()
+
+
+def test_per_coordinate_md_steps_and_resume(ctx):
+    """lgf_flex with the device's own noise: the captured loop equals
+    separate step calls bit for bit, and lgf_flex_a/b -- 60 steps,
+    checkpoint, a fresh system restored from it, 60 more -- ends where the
+    straight run does."""
+    d = decks.npt_axes_deck("flex")
+    a = _gpu_axes(ctx, d, seed=5)
+    b = _gpu_axes(ctx, d, seed=5)
+    a.interact()
+    b.interact()
+    a.md_steps(120)
+    for _ in range(120):
+        b.stepa()
+        b.interact()
+        b.stepb()
+    np.testing.assert_array_equal(a.pos, b.pos)
+    np.testing.assert_array_equal(a.vel, b.vel)
+    np.testing.assert_array_equal(a.box_now(), b.box_now())
+    L = a.box_now()
+    assert abs(L[0] - L[1]) > 1e-4 and abs(L[0] - d["box"][0]) > 1e-3  # three independent lengths
+    c = _gpu_axes(ctx, d, seed=5)
+    c.md_steps(60)
+    chp = c.checkpoint()
+    c.destroy()
+    e = _gpu_axes(ctx, d, seed=5, pos=np.zeros_like(d["pos"]))
+    e.restore(chp)
+    e.md_steps(60)
+    np.testing.assert_allclose(e.box_now(), L, rtol=1e-10)
+    np.testing.assert_allclose(e.pos, a.pos, rtol=0, atol=1e-8)
+    for g in (a, b, e):
+        g.destroy()
