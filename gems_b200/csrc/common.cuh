@@ -33,7 +33,7 @@ __device__ __forceinline__ void stencil(int k, int& dx, int& dy, int& dz) {
 }
 
 enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
-enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5 };
+enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6 };
 // IT_AXES: one integrator per coordinate -- a G-JF piston on that box length
 // (AX_FLEX) or Ermak dynamics of that coordinate (AX_ERMAK)
 enum AX : int { AX_NONE = 0, AX_FLEX = 1, AX_ERMAK = 2 };
@@ -103,6 +103,9 @@ struct SysDev {
   int ax_mode[3];
   int pad3;
   double ax_p[3][8];
+  // IT_LKD (set_lkd, Integration.F90:329-355): fac0, facv, target pressure,
+  // particle and piston frictions, piston mass
+  double lkd[6];
 };
 
 // Dynamic state of a system, written only by kernels (and reset by host).
@@ -134,6 +137,10 @@ struct SysState {
   double ax_pf[3], ax_pvel[3], ax_rangv[3], ax_ext[3];
   int ax_phase[3];
   int pad4;
+  // IT_LKD: the box at the step's start, after the half advance and final
+  // (the piston velocity is lgf_pvel; the fed piston normals of stepa and
+  // stepb are ax_ext[0] and ax_ext[1])
+  double lkd_bo[3], lkd_bh[3], lkd_bf[3];
 };
 
 // Block map: block b covers atoms [first[b], end[b]) of system sys[b];

@@ -61,7 +61,7 @@ struct SysHost {
 // a system whose box the device moves (a G-JF piston on the volume or on
 // a length)
 bool moving_box(const SysDev& d) {
-  if (d.integ == IT_LGF) return true;
+  if (d.integ == IT_LGF || d.integ == IT_LKD) return true;
   if (d.integ != IT_AXES) return false;
   return d.ax_mode[0] == AX_FLEX || d.ax_mode[1] == AX_FLEX || d.ax_mode[2] == AX_FLEX;
 }
@@ -715,8 +715,17 @@ int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss,
                   cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
-  bool piston = false;
-  for (int s : ss) piston |= ctx->sys[s].d.integ == IT_LGF || ctx->sys[s].d.integ == IT_AXES;
+  bool piston = false, lkd = false;
+  for (int s : ss) {
+    piston |= ctx->sys[s].d.integ == IT_LGF || ctx->sys[s].d.integ == IT_AXES;
+    lkd |= ctx->sys[s].d.integ == IT_LKD;
+  }
+  if (lkd) {
+    k_lkd_a<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+    ++ctx->launches;
+    for (int s : ss)
+      if (ctx->sys[s].d.integ == IT_LKD) ctx->sys[s].box_live = true;
+  }
   if (piston) {
     const int* sa;
     CHK(sys_array(ctx, ss, &sa));
@@ -2129,10 +2138,26 @@ int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
 int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals) {
   CHK(check_sys(ctx, sys));
   SysHost& h = ctx->sys[sys];
-  if (h.d.integ != IT_LGF && h.d.integ != IT_AXES)
+  if (h.d.integ != IT_LGF && h.d.integ != IT_AXES && h.d.integ != IT_LKD)
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf_normals: not a piston or per-coordinate system");
   if (!normals) {
     h.d.use_ext_normals = 0;
+  } else if (h.d.integ == IT_LKD) {
+    // stepa: a pair per atom coordinate, the piston's; stepb: the piston's,
+    // a pair per atom coordinate (first values used)
+    std::vector<double> nrm(6 * (size_t)h.n, 0.0);
+    const double* q = normals;
+    for (int i = 0; i < h.n; i++)
+      for (int k = 0; k < 3; k++, q += 2) nrm[6 * (size_t)i + 2 * k] = q[0];
+    double pist[3] = {q[0], q[2], 0.0};
+    q += 4;
+    for (int i = 0; i < h.n; i++)
+      for (int k = 0; k < 3; k++, q += 2) nrm[6 * (size_t)i + 2 * k + 1] = q[0];
+    CU(cudaMemcpyAsync(ctx->A.ext_normals + (size_t)6 * h.off, nrm.data(), nrm.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->A.st[sys].ax_ext, pist, sizeof(pist), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    h.d.use_ext_normals = 1;
   } else if (h.d.integ == IT_AXES) {
     // the pairs in draw order, scattered to (atom, coordinate) slots
     std::vector<double> nrm(6 * (size_t)h.n, 0.0);
@@ -2162,6 +2187,44 @@ int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals) {
   }
   CHK(push_sys(ctx, sys));
   CU(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+// set_lkd (src/Integration.F90:329-355): the Langevin piston of Kolb &
+// Dunweg
+int gemsgpu_set_lkd(gemsgpu_ctx* ctx, int sys, double dt, double temp, double press_atm, double pgama0,
+                    double pgamav, double pmass, uint64_t seed) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (!(dt > 0.0) || !(temp >= 0.0) || !(pgama0 >= 0.0) || !(pgamav >= 0.0) || !(pmass > 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_lkd: dt>0, T>=0, gammas>=0, piston mass>0");
+  if (!h.d.boxed || !h.d.pbc[0] || !h.d.pbc[1] || !h.d.pbc[2])
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: the piston needs a box periodic in x, y and z");
+  if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: pair potentials (lj, plj, slj) only");
+  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: FP64 systems only");
+  SysDev& d = h.d;
+  d.integ = IT_LKD;
+  d.dt = dt;
+  d.lkd[0] = std::sqrt(kB_ui * temp * dt * pgama0);
+  d.lkd[1] = std::sqrt(kB_ui * temp * dt * pgamav);
+  d.lkd[2] = press_atm * atm_ui();
+  d.lkd[3] = pgama0;
+  d.lkd[4] = pgamav;
+  d.lkd[5] = pmass;
+  d.virial = 1;
+  d.seed = seed;
+  d.use_ext_normals = 0;
+  h.temp = temp;
+  h.has_forces = false;  // the piston needs the virial
+  CHK(push_sys(ctx, sys));
+  CHK(read_states(ctx));
+  SysState st = ctx->h_st[sys];
+  st.lgf_pvel = 0.0;
+  for (int k = 0; k < 3; k++) st.box_b[k] = d.L[k];
+  CU(cudaMemcpyAsync(ctx->A.st + sys, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  invalidate(ctx);
+  drop_maps(ctx);
   return 0;
 }
 
@@ -3086,7 +3149,7 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || hd.version != 3)
     return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: not a checkpoint of this library");
   if (hd.n != h.n) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %d atoms, system has %d", hd.n, h.n);
-  if (h.d.boxed && (moving_box(h.d) || hd.integ == IT_LGF || hd.integ == IT_AXES)) {
+  if (h.d.boxed && (moving_box(h.d) || hd.integ == IT_LGF || hd.integ == IT_AXES || hd.integ == IT_LKD)) {
     // the box the piston had reached
     h.box_live = false;
     for (int k = 0; k < 3; k++) h.d.L[k] = hd.box[k];

@@ -1663,6 +1663,115 @@ __device__ __forceinline__ void axes_sys(SysDev& S, SysState& st) {
   regrid(S, st);
 }
 
+// ------------------------------------------------------------------ LKD
+// Block sums of three per-atom values; true in thread 0 of the system's
+// last block, which then holds the system's totals (added in block order).
+__device__ __forceinline__ bool sys3_close(Arena& A, const BlockMap& M, int s, const double w[3], double t[3]) {
+  double b[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) b[k] = block_sum(w[k]);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++) A.blk_red[8 * blockIdx.x + k] = b[k];
+  bool last = last_block(M, A.st, s, &A.st[s].ticket2);
+  if (!last || threadIdx.x >= 32) return false;
+  const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+  for (int k = 0; k < 3; k++) t[k] = 0.0;
+  for (int q = threadIdx.x; q < nb; q += 32)
+#pragma unroll
+    for (int k = 0; k < 3; k++) t[k] += __ldcg(&A.blk_red[8 * (b0 + q) + k]);
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    for (int o = 16; o; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+  return threadIdx.x == 0;
+}
+
+// the LKD velocity half kick (lkd_stepa :385-398 / lkd_stepb :470-481):
+// acel = F/m, v += dt/2 acel - dt/2 gamma0/m v + fac0/m r
+__device__ __forceinline__ void lkd_kick(const SysDev& S, double om, const double4& F, const double r[3], double4& v,
+                                         double4& a) {
+  const double hdt = 0.5 * S.dt;
+  const double c = om * S.lkd[0];
+  a.x = F.x * om; a.y = F.y * om; a.z = F.z * om;
+  v.x = v.x + hdt * a.x - hdt * S.lkd[3] * om * v.x + c * r[0];
+  v.y = v.y + hdt * a.y - hdt * S.lkd[3] * om * v.y + c * r[1];
+  v.z = v.z + hdt * a.z - hdt * S.lkd[3] * om * v.z + c * r[2];
+}
+
+// the LKD piston momentum step (lkd_stepa :400-411, lkd_stepb :458-468)
+// from the diagonal kinetic sums K of the current velocities:
+// P = mean_k (K_k + W_kk) / V, pvel += dt/2 (P - P0) - gammav dt/2 pvel/Q + facv r
+__device__ __forceinline__ void lkd_piston(const SysDev& S, SysState& st, const double K[3], double r) {
+  const double vol = S.L[0] * S.L[1] * S.L[2];
+  const double press = ((K[0] + st.vir[0]) / vol + (K[1] + st.vir[1]) / vol + (K[2] + st.vir[2]) / vol) / 3;
+  const double dt = S.dt;
+  st.lgf_pvel = st.lgf_pvel + 0.5 * dt * (press - S.lkd[2]) - S.lkd[4] * 0.5 * dt * st.lgf_pvel / S.lkd[5] +
+                S.lkd[1] * r;
+}
+
+// lkd_stepa, first part (Integration.F90:357-423): the velocity half kick
+// of every atom, then, in the system's last block, the piston momentum from
+// the pressure of the kicked velocities and the box's two half advances
+//   L_h = L (1 + dt/2 pvel / (Q V))^(1/3),  L' = L_h (1 + dt/2 pvel / (Q V_h))^(1/3)
+// (single-precision exponent 1./dd), which k_step_a applies to the atoms.
+__global__ void __launch_bounds__(BLOCK) k_lkd_a(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  SysDev& S = A.sys[s];
+  SysState& st = A.st[s];
+  if (S.integ != IT_LKD) return;  // uniform per block
+  const int i = M.first[blockIdx.x] + threadIdx.x;
+  double w[3] = {0, 0, 0};
+  if (i < M.end[blockIdx.x]) {
+    double r[3];
+    if (S.use_ext_normals) {
+      for (int k = 0; k < 3; k++) r[k] = A.ext_normals[(size_t)6 * i + 2 * k];
+    } else {
+      double q[6];
+      normals6((uint32_t)(i - S.off), st.step, S.seed, q);
+      r[0] = q[0], r[1] = q[2], r[2] = q[4];
+    }
+    double4 v = A.vel[i], a;
+    lkd_kick(S, A.minv[i].x, A.force[i], r, v, a);
+    A.vel[i] = v;
+    A.acel[i] = a;
+    const double m = A.mass[i];
+    w[0] = v.x * v.x * m;
+    w[1] = v.y * v.y * m;
+    w[2] = v.z * v.z * m;
+  }
+  double K[3];
+  if (!sys3_close(A, M, s, w, K)) return;
+  double rp;
+  if (S.use_ext_normals) {
+    rp = st.ax_ext[0];
+  } else {
+    double q[6];
+    normals6((uint32_t)S.n, st.step, S.seed, q);
+    rp = q[0];
+  }
+  lkd_piston(S, st, K, rp);
+  const double expo = (double)(1.0f / 3.0f);
+  const double dt = S.dt;
+  double vol = S.L[0] * S.L[1] * S.L[2];
+  for (int d = 0; d < 3; d++) {
+    st.lkd_bo[d] = S.L[d];
+    st.lkd_bh[d] = S.L[d] * pow(1.0 + 0.5 * dt * st.lgf_pvel / S.lkd[5] / vol, expo);
+  }
+  vol = st.lkd_bh[0] * st.lkd_bh[1] * st.lkd_bh[2];
+  const double g = 1.0 + 0.5 * dt * st.lgf_pvel / S.lkd[5] / vol;
+  if (!(vol > 0.0) || !(g > 0.0)) {
+    atomicOr(&st.status, ST_BOX);
+    for (int d = 0; d < 3; d++) st.lkd_bh[d] = st.lkd_bf[d] = st.lkd_bo[d];
+    return;
+  }
+  for (int d = 0; d < 3; d++) {
+    st.lkd_bf[d] = st.lkd_bh[d] * pow(g, expo);
+    S.L[d] = st.lkd_bf[d];
+    S.invL[d] = 1.0 / st.lkd_bf[d];
+  }
+  regrid(S, st);
+}
+
 // The G-JF piston of each constant-pressure system (one thread per system),
 // ahead of the atoms' half step.  It first closes the previous step's
 // piston (lgf_stepb: pistonf from the virial of the last force evaluation
@@ -1755,7 +1864,7 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
       // the change of its lengths since the build, on top of the atoms'
       // own displacements
       double box = 0.0;
-      if (PISTON && (S.integ == IT_LGF || S.integ == IT_AXES))
+      if (PISTON && (S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD))
         box = fabs(S.L[0] - st.box_b[0]) + fabs(S.L[1] - st.box_b[1]) + fabs(S.L[2] - st.box_b[2]);
       int rb = __dadd_rn(__dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)), box) > S.skin;
       if (frozen) rb = 0;
@@ -1764,7 +1873,9 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
         atomicOr(A.any_rebuild, 1);
         if constexpr (COND) cudaGraphSetConditional(cond, 1u);
       }
-      if ((S.integ == IT_ERMAK || S.integ == IT_LGF || S.integ == IT_AXES) && !S.use_ext_normals) st.step++;
+      if ((S.integ == IT_ERMAK || S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD) &&
+          !S.use_ext_normals)
+        st.step++;
       if (S.integ == IT_FIRE) st.fire_zero = 0;
     }
   }
@@ -1811,6 +1922,19 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
       axes_a_atom(A, S, st, i, mi, A.force[i], v, a, x, pv);
       A.acel[i] = a;
       A.vel_v[i] = pv;
+    } else if (S.integ == IT_LKD) {
+      // lkd_stepa (:423-436): drift with the half-advanced box, then scale
+      // positions and velocities to the final box (v was kicked by k_lkd_a)
+      x.x = x.x + v.x * S.dt * st.lkd_bo[0] * st.lkd_bo[0] / (st.lkd_bh[0] * st.lkd_bh[0]);
+      x.y = x.y + v.y * S.dt * st.lkd_bo[1] * st.lkd_bo[1] / (st.lkd_bh[1] * st.lkd_bh[1]);
+      x.z = x.z + v.z * S.dt * st.lkd_bo[2] * st.lkd_bo[2] / (st.lkd_bh[2] * st.lkd_bh[2]);
+      x.x = x.x * st.lkd_bf[0] / st.lkd_bo[0];
+      x.y = x.y * st.lkd_bf[1] / st.lkd_bo[1];
+      x.z = x.z * st.lkd_bf[2] / st.lkd_bo[2];
+      v.x = v.x * st.lkd_bo[0] / st.lkd_bf[0];
+      v.y = v.y * st.lkd_bo[1] / st.lkd_bf[1];
+      v.z = v.z * st.lkd_bo[2] / st.lkd_bf[2];
+      A.vel[i] = v;
     }
     wrap_atom(S, x);
     t.x = moved_atom(A, S, st, i, x, A.pos_old[i], A.type[i]);
@@ -1871,6 +1995,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
   bool act = i < M.end[blockIdx.x];
   bool frozen = S.integ == IT_FIRE && st.fire_done;
   double P = 0.0, f2max = 0.0;
+  double lkd_w[3] = {0, 0, 0};
   if (act && S.integ != IT_NONE && !frozen) {
     double4 v = A.vel[i], a = A.acel[i];
     const double4 F = A.force[i];
@@ -1898,9 +2023,40 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
       axis_b<0>(S, om, F, pv, v, a);
       axis_b<1>(S, om, F, pv, v, a);
       axis_b<2>(S, om, F, pv, v, a);
+    } else if (S.integ == IT_LKD) {
+      // lkd_stepb (:438-484): the pressure of the velocities as they come
+      // in (summed below), then the second half kick
+      const double m = A.mass[i];
+      lkd_w[0] = v.x * v.x * m;
+      lkd_w[1] = v.y * v.y * m;
+      lkd_w[2] = v.z * v.z * m;
+      double r[3];
+      if (S.use_ext_normals) {
+        for (int k = 0; k < 3; k++) r[k] = A.ext_normals[(size_t)6 * i + 2 * k + 1];
+      } else {
+        double q[6];
+        normals6((uint32_t)(i - S.off), st.step, S.seed, q);
+        r[0] = q[1], r[1] = q[3], r[2] = q[5];
+      }
+      lkd_kick(S, om, F, r, v, a);
     }
     A.vel[i] = v;
     A.acel[i] = a;
+  }
+  if (S.integ == IT_LKD) {  // uniform per block
+    double K[3];
+    if (sys3_close(A, M, s, lkd_w, K)) {
+      double rp;
+      if (S.use_ext_normals) {
+        rp = st.ax_ext[1];
+      } else {
+        double q[6];
+        normals6((uint32_t)S.n, st.step, S.seed, q);
+        rp = q[1];
+      }
+      lkd_piston(S, st, K, rp);
+    }
+    return;
   }
   if (S.integ != IT_FIRE) return;  // uniform per block
   double Pb = block_sum(P);

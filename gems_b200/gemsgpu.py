@@ -66,6 +66,7 @@ _SIGS = {
     "gemsgpu_set_lgf": (_i, [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_set_lgf_normals": (_i, [_p, _i, _dp]),
     "gemsgpu_add_lgf_axis": (_i, [_p, _i, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
+    "gemsgpu_set_lkd": (_i, [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_add_ermak_axis": (_i, [_p, _i, _i, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_get_box": (_i, [_p, _i, _dp]),
     "gemsgpu_virial": (_i, [_p, _i, _dp]),
@@ -505,8 +506,16 @@ class System:
         self._c(lib().gemsgpu_set_lgf(self.ctx.h, self.sid, float(dt), float(temp), float(press_atm),
                                       float(pgama0), float(pgamav), float(pmass), int(seed)))
 
+    def set_lkd(self, dt, temp, press_atm, pgama0, pgamav, pmass, seed=12345):
+        """set_lkd (`evolve piston_lkd`): the Langevin piston of Kolb & Dunweg."""
+        self._axes = ["lkd"]
+        self._c(lib().gemsgpu_set_lkd(self.ctx.h, self.sid, float(dt), float(temp), float(press_atm),
+                                      float(pgama0), float(pgamav), float(pmass), int(seed)))
+
     def add_lgf_axis(self, axis, dt, temp, press_atm, pgama0, pgamav, pmass, seed=12345):
         """`evolve piston_lgf x|y|z`: a G-JF piston on one box length."""
+        if getattr(self, "_axes", []) == ["lkd"]:
+            self._axes = []
         self._c(lib().gemsgpu_add_lgf_axis(self.ctx.h, self.sid, int(axis), float(dt), float(temp),
                                            float(press_atm), float(pgama0), float(pgamav), float(pmass),
                                            int(seed)))
@@ -514,6 +523,8 @@ class System:
 
     def add_ermak_axis(self, axis, dt, gama, temp, seed=12345):
         """`evolve ermak_x|y|z`: Ermak dynamics of one coordinate."""
+        if getattr(self, "_axes", []) == ["lkd"]:
+            self._axes = []
         self._c(lib().gemsgpu_add_ermak_axis(self.ctx.h, self.sid, int(axis), float(dt), float(gama),
                                              float(temp), int(seed)))
         self._axes = getattr(self, "_axes", []) + ["ermak"]
@@ -525,7 +536,10 @@ class System:
         in order, a piston's pair and a pair per atom, or a pair per atom.
         None returns to the device stream."""
         axes = getattr(self, "_axes", [])
-        pairs = sum(1 + self.n if a == "lgf" else self.n for a in axes) if axes else 1 + 3 * self.n
+        if axes == ["lkd"]:
+            pairs = 6 * self.n + 2
+        else:
+            pairs = sum(1 + self.n if a == "lgf" else self.n for a in axes) if axes else 1 + 3 * self.n
         a = None if nrm is None else _f64(nrm, 2 * pairs)
         self._c(lib().gemsgpu_set_lgf_normals(self.ctx.h, self.sid, _ptr(a)))
 

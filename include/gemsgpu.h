@@ -205,6 +205,13 @@ int gemsgpu_set_fire(gemsgpu_ctx* ctx, int sys, double dt0, double dtmax);
 int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp,
                     double press_atm, double pgama0, double pgamav,
                     double pmass, uint64_t seed);
+/* set_lkd (src/Integration.F90:329-355), `evolve piston_lkd`: the Langevin
+ * piston of Kolb & Dunweg (J. Chem. Phys. 111, 4453, 1999) as lkd_stepa /
+ * lkd_stepb (:357-484) state it; arguments and restrictions as
+ * gemsgpu_set_lgf. */
+int gemsgpu_set_lkd(gemsgpu_ctx* ctx, int sys, double dt, double temp,
+                    double press_atm, double pgama0, double pgamav,
+                    double pmass, uint64_t seed);
 /* One integrator per coordinate (`evolve piston_lgf x|y|z` and
  * `evolve ermak_x|y|z`, Integration.F90:157-186): a G-JF piston on one box
  * length (set_lgf_flex, :652-696; lgf_flex_stepa/b, :698-830; arguments as
@@ -227,7 +234,9 @@ int gemsgpu_add_ermak_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt,
  * piston's pair, then a pair per atom and coordinate (the first value of
  * each pair is used).  Per-coordinate integrators, in the order they were
  * added: a piston's pair then a pair per atom, or an Ermak coordinate's
- * pair per atom.  NULL returns to the device stream. */
+ * pair per atom.  LKD piston: 6 n + 2 pairs, stepa's pair per atom
+ * coordinate and piston pair, then stepb's piston pair and pair per atom
+ * coordinate.  NULL returns to the device stream. */
 int gemsgpu_set_lgf_normals(gemsgpu_ctx* ctx, int sys, const double* normals);
 /* The box lengths (A) as the device holds them (moved by a piston). */
 int gemsgpu_get_box(gemsgpu_ctx* ctx, int sys, double L[3]);

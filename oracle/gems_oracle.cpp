@@ -110,7 +110,7 @@ void rang(Lcg& s, double* r1, double* r2) {  // always draws a pair
 
 // ---------------------------------------------------------------- system
 enum FF { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3, FF_SLJ = 4 };
-enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5 };
+enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6 };
 
 // One integrator acting on one coordinate of every atom (integrate objects
 // set by `evolve piston_lgf x|y|z` and `evolve ermak_x|y|z`,
@@ -205,6 +205,9 @@ struct Sys {
          lgf_facv = 0, lgf_av = 0, lgf_rangv = 0, pvel = 0, pistonf = 0;
   bool lgf_first = true;
   std::vector<AxisInt> axes;  // IT_AXES: the per-coordinate integrators in order
+  // LKD piston (set_lkd, Integration.F90:329-355): noise amplitudes, target
+  // pressure (internal units), frictions and piston mass
+  double lkd_fac0 = 0, lkd_facv = 0, lkd_press = 0, lkd_g0 = 0, lkd_gv = 0, lkd_pmass = 0;
   int ext_used = 0;  // normals of the external stream used this step
   // FIRE state
   double fire_dt = 0, fire_dtmax = 0, fire_alpha = 0.1;
@@ -1091,6 +1094,91 @@ void axes_b(Sys& s) {
   }
 }
 
+// ------------------------------------------------------------------ LKD NPT
+// Langevin piston of Kolb & Dunweg (J. Chem. Phys. 111, 4453, 1999) as
+// lkd_stepa / lkd_stepb state it (Integration.F90:357-484): a half kick of
+// the velocities with friction and noise, the piston momentum from the
+// instantaneous pressure, the box moved in two half advances with the
+// positions drifted in between, then positions and velocities rescaled to
+// the final box.  Noise: stepa draws a pair per atom coordinate then the
+// piston's, stepb the piston's then a pair per atom coordinate.
+void set_lkd(Sys& s, double dt, double temp, double press, double pgama0, double pgamav, double pmass) {
+  s.integ = IT_LKD;
+  s.dt = dt;
+  s.temp = temp;
+  s.lkd_fac0 = std::sqrt(kB_ui * temp * dt * pgama0);
+  s.lkd_facv = std::sqrt(kB_ui * temp * dt * pgamav);
+  s.lkd_press = press;
+  s.lkd_g0 = pgama0;
+  s.lkd_gv = pgamav;
+  s.lkd_pmass = pmass;
+  s.pvel = 0.0;
+}
+
+// the mean of the pressure tensor's diagonal (inq_pressure,
+// Inq_Properties.F90:529-573), internal units, with the virial of the last
+// force evaluation
+double pressure_trace(const Sys& s) {
+  double K[3] = {0, 0, 0};
+  for (int i = 0; i < s.n; i++)
+    for (int a = 0; a < 3; a++) K[a] += s.vel[3 * i + a] * s.vel[3 * i + a] * s.mass[i];
+  const double vol = s.box[0] * s.box[1] * s.box[2];
+  return ((K[0] + s.virial[0]) / vol + (K[1] + s.virial[4]) / vol + (K[2] + s.virial[8]) / vol) / 3;
+}
+
+void lkd_kick(Sys& s) {
+  const double dt = s.dt;
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++) {
+      const int q = 3 * i + k;
+      double r1, r2;
+      rang(*s.rng, &r1, &r2);
+      s.acel[q] = s.force[q] * s.one_mass[i];
+      s.vel[q] = s.vel[q] + 0.5 * dt * s.acel[q] - 0.5 * dt * s.lkd_g0 * s.one_mass[i] * s.vel[q] +
+                 s.one_mass[i] * s.lkd_fac0 * r1;
+    }
+}
+
+void lkd_piston(Sys& s) {
+  const double dt = s.dt;
+  const double press = pressure_trace(s);
+  double r1, r2;
+  rang(*s.rng, &r1, &r2);
+  s.pvel = s.pvel + 0.5 * dt * (press - s.lkd_press) - s.lkd_gv * 0.5 * dt * s.pvel / s.lkd_pmass + s.lkd_facv * r1;
+}
+
+void lkd_a(Sys& s) {
+  const double dt = s.dt;
+  const double expo = (double)(1.0f / 3.0f);
+  double bo[3];
+  for (int k = 0; k < 3; k++) bo[k] = s.box[k];
+  lkd_kick(s);
+  lkd_piston(s);
+  double vol = s.box[0] * s.box[1] * s.box[2];
+  for (int k = 0; k < 3; k++) s.box[k] = s.box[k] * std::pow(1.0 + 0.5 * dt * s.pvel / s.lkd_pmass / vol, expo);
+  vol = s.box[0] * s.box[1] * s.box[2];
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++) {
+      const int q = 3 * i + k;
+      s.pos[q] = s.pos[q] + s.vel[q] * dt * bo[k] * bo[k] / (s.box[k] * s.box[k]);
+    }
+  for (int k = 0; k < 3; k++) {
+    s.box[k] = s.box[k] * std::pow(1.0 + 0.5 * dt * s.pvel / s.lkd_pmass / vol, expo);
+    s.one_box[k] = 1.0 / s.box[k];
+  }
+  for (int i = 0; i < s.n; i++)
+    for (int k = 0; k < 3; k++) {
+      const int q = 3 * i + k;
+      s.pos[q] = s.pos[q] * s.box[k] / bo[k];
+      s.vel[q] = s.vel[q] * bo[k] / s.box[k];
+    }
+}
+
+void lkd_b(Sys& s) {
+  lkd_piston(s);
+  lkd_kick(s);
+}
+
 void add_axis(Sys& s, const AxisInt& a) {
   if (s.integ != IT_AXES) s.axes.clear();
   s.integ = IT_AXES;
@@ -1104,6 +1192,7 @@ void stepa(Sys& s) {
   else if (s.integ == IT_ERMAK) ermak_a(s);
   else if (s.integ == IT_LGF) lgf_a(s);
   else if (s.integ == IT_AXES) axes_a(s);
+  else if (s.integ == IT_LKD) lkd_a(s);
   do_pbc(s);
 }
 
@@ -1112,6 +1201,7 @@ void stepb(Sys& s) {
   else if (s.integ == IT_ERMAK) ermak_b(s);
   else if (s.integ == IT_LGF) lgf_b(s);
   else if (s.integ == IT_AXES) axes_b(s);
+  else if (s.integ == IT_LKD) lkd_b(s);
   do_pbc(s);
   if (s.integ == IT_FIRE) fire_mix(s);
 }
@@ -1870,6 +1960,15 @@ void orc_add_lgf_axis(void* p, int d, double dt, double temp, double press_atm, 
   a.facv = std::sqrt(2.0 * pgamav * kB_ui * temp * dt);
   a.av = (1.0 - 0.5 * dt * a.ipm * pgamav) * a.bv;
   add_axis(*s, a);
+}
+
+// `evolve piston_lkd T gamma0 P gammav pmass` (Integration.F90:150-156),
+// press in atm
+void orc_set_lkd(void* p, double dt, double temp, double press_atm, double pgama0, double pgamav, double pmass,
+                 void* rng) {
+  Sys* s = (Sys*)p;
+  s->rng = (Lcg*)rng;
+  set_lkd(*s, dt, temp, press_atm * atm_ui, pgama0, pgamav, pmass);
 }
 
 // `evolve ermak_x|y|z T gamma` (Integration.F90:179-186; set_ermak with a

@@ -95,6 +95,7 @@ def lib():
         "orc_virial_ev": (None, [_p, _dp]),
         "orc_add_lgf_axis": (None, [_p, _i, _d, _d, _d, _d, _d, _d, _p]),
         "orc_add_ermak_axis": (None, [_p, _i, _d, _d, _d, _p]),
+        "orc_set_lkd": (None, [_p, _d, _d, _d, _d, _d, _d, _p]),
         "orc_pressure_atm": (None, [_p, _dp]),
         "orc_get_box": (None, [_p, _dp]),
         "orc_atm_ui": (_d, []),
@@ -385,6 +386,12 @@ class System:
         self._rng = rng
         lib().orc_set_lgf(self.h, float(dt), float(temp), float(press_atm), float(pgama0), float(pgamav),
                           float(pmass), rng.h if rng is not None else None)
+
+    def set_lkd(self, dt, temp, press_atm, pgama0, pgamav, pmass, rng):
+        """`evolve piston_lkd`: the Langevin piston of Kolb & Dunweg."""
+        self._rng = rng
+        lib().orc_set_lkd(self.h, float(dt), float(temp), float(press_atm), float(pgama0), float(pgamav),
+                          float(pmass), rng.h)
 
     def add_lgf_axis(self, axis, dt, temp, press_atm, pgama0, pgamav, pmass, rng):
         """`evolve piston_lgf x|y|z`: a G-JF piston on one box length."""

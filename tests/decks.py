@@ -251,6 +251,15 @@ def npt_axes_setup(s, d, rng):
             s.add_ermak_axis(a[1], d["dt"], a[3], a[2], rng)
 
 
+def npt_lkd_deck():
+    """The lgf.gms crystal, potential and targets under `evolve piston_lkd`
+    (piston friction 1e-4/tau, piston mass 1e-5).  The reference ships no
+    golden file for this integrator."""
+    d = npt_lgf_deck()
+    d["lkd"] = True
+    return d
+
+
 def npt_axes_pairs(d, n):
     """LCG pairs one step draws: a piston takes 1 + n, an Ermak coordinate n."""
     return sum(1 + n if a[0] == "lgf" else n for a in d["axes"])
@@ -259,7 +268,10 @@ def npt_axes_pairs(d, n):
 def npt_setup(s, d, rng):
     s.set_box(d["box"], (True, True, True))
     s.set_slj(*d["slj"])
-    s.set_lgf(d["dt"], d["temp"], d["press_atm"], d["pgama0"], d["pgamav"], d["pmass"], rng)
+    if d.get("lkd"):
+        s.set_lkd(d["dt"], d["temp"], d["press_atm"], d["pgama0"], d["pgamav"], d["pmass"], rng)
+    else:
+        s.set_lgf(d["dt"], d["temp"], d["press_atm"], d["pgama0"], d["pgamav"], d["pmass"], rng)
 
 
 def npt_run(s, d, rng, nsteps=None, each=None, feed=None, boxes=None):
@@ -274,7 +286,11 @@ def npt_run(s, d, rng, nsteps=None, each=None, feed=None, boxes=None):
     E, P, V = [], [], []
     for ns in range(1, nsteps + 1):
         if feed is not None:
-            feed(s, rng.rang_stream(npt_axes_pairs(d, s.n) if "axes" in d else 1 + 3 * s.n))
+            if "axes" in d:
+                pairs = npt_axes_pairs(d, s.n)
+            else:
+                pairs = 6 * s.n + 2 if d.get("lkd") else 1 + 3 * s.n
+            feed(s, rng.rang_stream(pairs))
         s.stepa()
         s.interact()
         s.stepb()

@@ -224,3 +224,36 @@ def test_per_coordinate_md_steps_and_resume(ctx):
     np.testing.assert_allclose(e.pos, a.pos, rtol=0, atol=1e-8)
     for g in (a, b, e):
         g.destroy()
+
+
+def test_lkd_trajectory_equals_oracle(ctx):
+    """piston_lkd (no golden file in the reference): 100 steps with the
+    oracle's normals fed in draw order, energies, pressure and box every
+    10th step; then the captured loop against separate step calls."""
+    d = decks.npt_lkd_deck()
+    s, rng_o = _oracle(d)
+    B0 = []
+    E0, P0, V0 = decks.npt_run(s, d, rng_o, boxes=B0)
+    g = gems.System(d["pos"], d["mass"], ctx=ctx)
+    g.set_skin_mode(False)
+    decks.npt_setup(g, d, 12345)
+    B1 = []
+    E1, P1, V1 = decks.npt_run(g, d, O.Rng(d["seed"]), feed=_feed, boxes=B1)
+    np.testing.assert_allclose(E1, E0, rtol=1e-9)
+    np.testing.assert_allclose(P1, P0, rtol=1e-8, atol=1e-3)
+    np.testing.assert_allclose(np.array(B1), np.array(B0), rtol=1e-12)
+    assert abs(B1[-1][0] - d["box"][0]) > 1e-3
+    g.destroy()
+    a, b = [gems.System(d["pos"], d["mass"], ctx=ctx) for _ in range(2)]
+    for x in (a, b):
+        decks.npt_setup(x, d, 3)
+        x.interact()
+    a.md_steps(120)
+    for _ in range(120):
+        b.stepa()
+        b.interact()
+        b.stepb()
+    np.testing.assert_array_equal(a.pos, b.pos)
+    np.testing.assert_array_equal(a.box_now(), b.box_now())
+    a.destroy()
+    b.destroy()
