@@ -122,6 +122,10 @@ struct SysState {
   double fmax2;     // max |F|^2 (internal units), FIRE convergence
   unsigned long long fmax2_bits;
   int maxnn, pad;
+  // the skin test's bound on how much closer any pair came since the list
+  // was built: the two largest displacements (+ the box's change of length
+  // for a moving box); 0 right after a build
+  double dmax;
   // pair virial W = sum_i r_i (x) F_i of the last force evaluation
   // (internal units; xx yy zz xy xz yz), kinetic tensor sum m v (x) v
   double vir[6], ktens[6];
@@ -181,6 +185,8 @@ struct Arena {
   int* flist;           // the same pairs sorted by distance at the rebuild
                         // (force kernels: a warp's atoms meet the same shell
                         // at the same slot, so the distance classes do not diverge)
+  uint4* ncut;          // per atom, eight 16-bit counts: flist entries built closer than
+                        // rcut + 1e-4 + k skin/7 (k = 0..7; see live_entries)
   int* cell_of;
   int* slot;
   int* cell_count;      // per cell, zero between rebuilds

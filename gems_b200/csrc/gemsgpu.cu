@@ -256,6 +256,7 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   CHK(dgrow(ctx, &A.mass, keep, nc));
   CHK(dgrow(ctx, &A.type, keep, nc));
   CHK(dgrow(ctx, &A.nn, keep, nc));
+  CHK(dgrow(ctx, &A.ncut, keep, nc));
   CHK(dgrow(ctx, &A.cell_of, keep, nc));
   CHK(dgrow(ctx, &A.slot, keep, nc));
   CHK(dgrow(ctx, &A.cell_atoms, keep, nc));
@@ -1537,7 +1538,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   drop_maps(ctx);
   Arena& A = ctx->A;
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.epot, A.band, A.eband,
-                  A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.list, A.flist, A.cell_of, A.slot,
+                  A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.ncut, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys};

@@ -242,8 +242,14 @@ __device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, i
     double2 v = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
       const SysDev& S = A.sys[s];
-      int rb = __dadd_rn(__dsqrt_rn(v.x), __dsqrt_rn(v.y)) > S.skin;
-      A.st[s].rebuild = rb;
+      SysState& st = A.st[s];
+      double box = 0.0;
+      if (S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD)
+        box = fabs(S.L[0] - st.box_b[0]) + fabs(S.L[1] - st.box_b[1]) + fabs(S.L[2] - st.box_b[2]);
+      const double D = __dadd_rn(__dadd_rn(__dsqrt_rn(v.x), __dsqrt_rn(v.y)), box);
+      int rb = D > S.skin;
+      st.dmax = D;
+      st.rebuild = rb;
       if (rb) atomicOr(A.any_rebuild, 1);
     }
   }
@@ -470,6 +476,42 @@ __device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
   atomicMax(&A.st[s].maxnn, m);
 }
 
+// flist holds an atom's entries sorted by their distance at the build, and
+// no pair has come closer since by more than the skin test's bound D
+// (SysState::dmax).  So the entries built at r >= rcut + 1e-4 + k skin/7
+// with k skin/7 >= D lie beyond every cut-off of the system now and add
+// nothing: the force kernels stop before them.  The counts are of entries
+// with (float) r^2 below the float of each threshold squared; the float
+// roundings move a distance by under 1e-6 A, inside the 1e-4 A margin.
+__device__ __forceinline__ void list_counts(const Arena& A, const SysDev& S, int i, int n, const float* rrow,
+                                            int ln) {
+  unsigned short c[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const double t = S.rcut + 1e-4 + k * (S.skin / 7.0);
+    const float T = (float)(t * t);
+    int cnt = 0;
+    for (int e0 = 0; e0 < n; e0 += 32) {
+      const int e = e0 + ln;
+      cnt += __popc(__ballot_sync(0xffffffffu, e < n && rrow[e] < T));
+    }
+    c[k] = (unsigned short)min(cnt, 65535);
+  }
+  if (ln == 0)
+    A.ncut[i] = make_uint4(c[0] | (unsigned)c[1] << 16, c[2] | (unsigned)c[3] << 16, c[4] | (unsigned)c[5] << 16,
+                           c[6] | (unsigned)c[7] << 16);
+}
+
+// the flist entries an atom's force loop must visit this step
+__device__ __forceinline__ int live_entries(const Arena& A, const SysDev& S, const SysState& st, int i, int nn) {
+  if (!(S.skin > 0.0) || !S.use_cells) return nn;  // O(N^2) lists are not distance-sorted
+  const double q = st.dmax * 7.0 / S.skin;
+  if (!(q <= 7.0)) return nn;
+  const int k = (int)ceil(q);
+  const unsigned w = __ldg(reinterpret_cast<const unsigned*>(A.ncut + i) + (k >> 1));
+  return min(nn, (int)((k & 1) ? (w >> 16) : (w & 0xffffu)));
+}
+
 // linkedcell_self / linkedcell_selfhalf (src/Neighbour.F90:991-1161): the
 // 27 (or 14) stencil cells in the reference's order with periodic cell
 // wrap (cell_pbc, :1350-1376); keep j if rd < (rcut+nb_dcut)^2 (strict).
@@ -605,6 +647,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
             }
             A.flist[(size_t)rank * A.cap + i] = row[e];
           }
+          list_counts(A, S, i, n, rrow, ln);
           if (ln == 0) list_done(A, s, i, m);
         }
         __syncwarp();
@@ -655,6 +698,7 @@ __global__ void k_count_rebuild(Arena A, const int* sys, int nsys, int in_graph)
   if (k < nsys && sys[k] >= 0 && A.st[sys[k]].rebuild) {
     SysState& st = A.st[sys[k]];
     st.nupd++;
+    st.dmax = 0.0;
     for (int d = 0; d < 3; d++) st.box_b[d] = A.sys[sys[k]].L[d];
   }
   if (in_graph && k == 0) atomicAdd(A.body_runs, 1ull);
@@ -757,7 +801,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
   if (act) {
     const double4 xi = A.pos[i];
     const int ti = A.type[i];
-    const int nn = min(A.nn[i], A.lcap);
+    const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const bool one = S.ntypes == 1;
     auto gat = [&](int j) { return A.pos[j]; };
     PAIR_LOOP_BEGIN(double4, gat)
@@ -808,7 +852,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
     const double4 xi = A.pos[i];
     const int ti = A.type[i];
     const double ebi = A.eband[i];
-    const int nn = min(A.nn[i], A.lcap);
+    const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const bool one = S.ntypes == 1;
     auto gat = [&](int j) { return A.pose[j]; };
     PAIR_LOOP_BEGIN(double4, gat)
@@ -930,7 +974,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
   double band = 0.0;
   if (act) {
     const int4 xi = A.fxp[i];
-    const int nn = min(A.nn[i], A.lcap);
+    const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
     int jn[UNR];
     list_group<K>(A, i, nn, lane, jn);
@@ -994,7 +1038,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
   if (act) {
     const int4 xi = A.fxp[i];
     const float ebi = A.ebandf[i];
-    const int nn = min(A.nn[i], A.lcap);
+    const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
     const float evui = (float)EV_UI;
     const int ti = xi.w;
@@ -1135,7 +1179,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
   if (act) {
     const double4 xi = A.pos[i];
     const int ti = A.type[i];
-    const int nn = min(A.nn[i], A.lcap);
+    const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     auto gat = [&](int j) { return A.pos[j]; };
     PAIR_LOOP_BEGIN(double4, gat)
       const PairP& P = A.prm[S.param_off + ti * S.ntypes + A.type[j]];
@@ -1203,7 +1247,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
   if (act) {
     const int4 xi = A.fxp[i];
-    const int nn = min(A.nn[i], A.lcap);
+    const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const float evui = (float)EV_UI;
     auto gat = [&](int j) { return A.fxp[j]; };
     PAIR_LOOP_BEGIN(int4, gat)
@@ -1866,7 +1910,9 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
       double box = 0.0;
       if (PISTON && (S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD))
         box = fabs(S.L[0] - st.box_b[0]) + fabs(S.L[1] - st.box_b[1]) + fabs(S.L[2] - st.box_b[2]);
-      int rb = __dadd_rn(__dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)), box) > S.skin;
+      const double D = __dadd_rn(__dadd_rn(__dsqrt_rn(w.x), __dsqrt_rn(w.y)), box);
+      int rb = D > S.skin;
+      st.dmax = D;
       if (frozen) rb = 0;
       st.rebuild = rb;
       if (rb) {

@@ -570,3 +570,42 @@ def test_fire_batch_equals_alone(ctx):
         np.testing.assert_array_equal(ga.pos, gb.pos)
         assert ga.energy()[0] == gb.energy()[0]
         ga.destroy()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_stale_list_pairs_entering_the_cutoff(ctx, prec):
+    """Between list builds the force kernels visit only the distance-sorted
+    entries that can have come within the cut-off (the skin test's bound on
+    how far pairs moved).  A periodic Au crystal is displaced by up to 0.24 A
+    per atom without a rebuild, so pairs built outside rce move inside it;
+    the forces still match the oracle's full-list sums."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=6)
+    L = np.array(w["L"])
+
+    def setup(s):
+        s.set_box(w["L"], (True, True, True))
+        s.set_smatb(*w["smatb"])
+    o, g = both(w["pos"], w["mass"], ctx, setup=setup)
+    g.set_precision(prec)
+    o.interact()
+    g.interact()
+    n0 = g.nupd
+    rng = np.random.default_rng(11)
+    step = rng.normal(size=w["pos"].shape)
+    step *= (0.24 * rng.random(len(step)) / np.linalg.norm(step, axis=1))[:, None]
+    moved = np.mod(w["pos"] + step, L)
+    rce = w["smatb"][6]
+    d0 = w["pos"][None, :, :] - w["pos"][:, None, :]
+    d1 = moved[None, :, :] - moved[:, None, :]
+    d0 -= L * np.round(d0 / L)
+    d1 -= L * np.round(d1 / L)
+    r0, r1 = np.linalg.norm(d0, axis=2), np.linalg.norm(d1, axis=2)
+    assert np.sum((r0 > rce) & (r1 < rce)) > 0  # pairs that entered the cut-off
+    o.set_pos(moved)
+    g.set_pos(moved)
+    o.interact()
+    g.interact()
+    assert g.nupd == n0  # no rebuild: the stale list was used
+    assert relrms(g.force, o.force) <= (RMS_FP64 if prec == 0 else RMS_MIXED)
+    g.destroy()
