@@ -153,6 +153,9 @@ struct SysState {
 struct BlockMap {
   int nblk;
   int apb;             // atoms per block
+  int base;            // index of block 0 in the per-block scratch (blk_top2, blk_red): a
+                       // system's blocks of a batch's map, launched on their own, keep
+                       // the batch's slots, so that concurrent launches do not share them
   const int* sys;
   const int* first;
   const int* end;

@@ -37,6 +37,7 @@ struct DevMap {
   BlockMap m{};
   int* buf = nullptr;  // device storage of the map arrays
   int nblk = 0;
+  std::vector<int> blk0, nblkv;  // host copies of sys_blk0 / sys_nblk
 };
 
 struct SysHost {
@@ -97,6 +98,10 @@ struct gemsgpu_ctx {
   int64_t body_nodes = 0;  // kernels in one captured rebuild chain
   unsigned long long body_seen = 0;  // body_runs already accounted
   int64_t pending = 0;   // kernels recorded by the capture in progress
+  // while a batched graph is captured as one branch per system: the batch;
+  // a one-system map then is that system's blocks of the batch's map
+  std::vector<int> view_set;
+  int64_t bodies = 0;    // conditional rebuild bodies in the graph being built
   std::map<std::string, DevMap> maps;
   std::map<std::string, Graph> graphs;
   // pinned scratch for small readbacks
@@ -503,9 +508,34 @@ int check_sys(gemsgpu_ctx* ctx, int s) {
 
 // ------------------------------------------------------------- block maps
 // kind 0: atoms, `apb` atoms per block; kind 1: cells, 256 cells per block.
-int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, BlockMap* out) {
+std::string map_key(const std::vector<int>& ss, int apb, int kind) {
   std::string key = std::to_string(kind) + ":" + std::to_string(apb) + ":";
   for (int s : ss) key += std::to_string(s) + ",";
+  return key;
+}
+
+int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, BlockMap* out) {
+  if (ss.size() == 1 && ctx->view_set.size() > 1 &&
+      std::find(ctx->view_set.begin(), ctx->view_set.end(), ss[0]) != ctx->view_set.end()) {
+    // a branch of a batched graph: the system's blocks of the batch's map
+    std::vector<int> full;
+    full.swap(ctx->view_set);
+    BlockMap fm;
+    int rc = get_map(ctx, full, apb, kind, &fm);
+    full.swap(ctx->view_set);
+    CHK(rc);
+    const DevMap& dm = ctx->maps[map_key(ctx->view_set, apb, kind)];
+    const int b0 = dm.blk0[ss[0]], nb = dm.nblkv[ss[0]];
+    BlockMap v = fm;
+    v.nblk = nb;
+    v.base = b0;
+    v.sys = fm.sys + b0;
+    v.first = fm.first + b0;
+    v.end = fm.end + b0;
+    *out = v;
+    return 0;
+  }
+  std::string key = map_key(ss, apb, kind);
   auto it = ctx->maps.find(key);
   if (it != ctx->maps.end()) {
     *out = it->second.m;
@@ -552,7 +582,10 @@ int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, Blo
   dm.m.end = dm.buf + 2 * nb;
   dm.m.sys_blk0 = dm.buf + 3 * nb;
   dm.m.sys_nblk = dm.buf + 3 * nb + ctx->scap;
+  dm.m.base = 0;
   dm.nblk = nb;
+  dm.blk0 = blk0;
+  dm.nblkv = nblk;
   ctx->maps[key] = dm;
   *out = dm.m;
   return 0;
@@ -947,6 +980,7 @@ int cap_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
   const int64_t before = ctx->launches;
   int rc = launch_rebuild(ctx, ss, 1);
   ctx->body_nodes = ctx->launches - before;
+  ctx->bodies++;
   return rc;
 }
 int cap_forces_b(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
@@ -960,46 +994,62 @@ int cap_plain(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
   return record_steps(ctx, ss, *(int*)arg);
 }
 
+// A batch of several systems is captured as one independent branch per
+// system: each system's steps, conditional rebuilds and force passes form
+// their own chain, so the GPU overlaps one system's list build or kernel
+// tail with the others' work.  The per-system launches use the batch's
+// block maps (views), so each block keeps its own per-block scratch slot.
 int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGraph_t* out) {
   cudaGraph_t g = nullptr;
   CU(cudaGraphCreate(&g, 0));
-  std::vector<cudaGraphNode_t> deps;
   int rc = 0;
   bool cond_ok = ctx->use_cond;
-  const bool fuse = can_fuse_steps(ctx, ss);
+  std::vector<std::vector<int>> sets;
+  if (ss.size() > 1)
+    for (int s : ss) sets.push_back({s});
+  else
+    sets.push_back(ss);
+  std::vector<std::vector<cudaGraphNode_t>> deps(sets.size());
+  if (sets.size() > 1) ctx->view_set = ss;
+  ctx->bodies = 0;
   for (int k = 0; k < nsteps && rc == 0 && cond_ok; k++) {
-    CondArg ca{};
-    if (cudaGraphConditionalHandleCreate(&ca.h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
-      cond_ok = false;
-      break;
+    for (size_t j = 0; j < sets.size() && rc == 0 && cond_ok; j++) {
+      const std::vector<int>& sj = sets[j];
+      const bool fuse = can_fuse_steps(ctx, sj);
+      CondArg ca{};
+      if (cudaGraphConditionalHandleCreate(&ca.h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+        cond_ok = false;
+        break;
+      }
+      rc = capture_into(ctx, g, deps[j], (k == 0 || !fuse) ? cap_step_a : cap_step_ba, sj, &ca);
+      if (rc) break;
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = ca.h;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cn;
+      if (cudaGraphAddNode(&cn, g, deps[j].data(), deps[j].size(), &cp) != cudaSuccess) {
+        cond_ok = false;
+        break;
+      }
+      std::vector<cudaGraphNode_t> none;
+      rc = capture_into(ctx, cp.conditional.phGraph_out[0], none, cap_rebuild, sj, nullptr);
+      if (rc) break;
+      deps[j].assign(1, cn);
+      rc = capture_into(ctx, g, deps[j], (fuse && k < nsteps - 1) ? cap_forces : cap_forces_b, sj, nullptr);
     }
-    rc = capture_into(ctx, g, deps, (k == 0 || !fuse) ? cap_step_a : cap_step_ba, ss, &ca);
-    if (rc) break;
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = ca.h;
-    cp.conditional.type = cudaGraphCondTypeIf;
-    cp.conditional.size = 1;
-    cudaGraphNode_t cn;
-    if (cudaGraphAddNode(&cn, g, deps.data(), deps.size(), &cp) != cudaSuccess) {
-      cond_ok = false;
-      break;
-    }
-    std::vector<cudaGraphNode_t> none;
-    rc = capture_into(ctx, cp.conditional.phGraph_out[0], none, cap_rebuild, ss, nullptr);
-    if (rc) break;
-    deps.assign(1, cn);
-    rc = capture_into(ctx, g, deps, (fuse && k < nsteps - 1) ? cap_forces : cap_forces_b, ss, nullptr);
   }
+  ctx->view_set.clear();
   cudaGetLastError();
   if (rc == 0 && !cond_ok) {
     // conditional nodes unavailable: plain capture, rebuild kernels exit early
     cudaGraphDestroy(g);
     ctx->use_cond = false;
     CU(cudaGraphCreate(&g, 0));
-    deps.clear();
+    std::vector<cudaGraphNode_t> none;
     int n = nsteps;
-    rc = capture_into(ctx, g, deps, cap_plain, ss, &n);
+    rc = capture_into(ctx, g, none, cap_plain, ss, &n);
   }
   if (rc) {
     cudaGraphDestroy(g);
@@ -1026,6 +1076,11 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
     CHK(get_map(ctx, ss, BLOCK / 32, 1, &m));
     CHK(get_map(ctx, ss, 1, 1, &m));
     CHK(sys_array(ctx, ss, &sa));
+    for (int s : ss) {
+      CHK(sys_array(ctx, {s}, &sa));
+      const SysHost& h = ctx->sys[s];
+      CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / h.lanes, 0, &m));
+    }
     std::map<std::tuple<int, int, int>, std::vector<int>> groups;
     for (int s : ss) {
       const SysHost& h = ctx->sys[s];
@@ -1044,7 +1099,7 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
   int rc = build_chunk_graph(ctx, ss, nsteps, &g);
   int64_t nodes = ctx->launches - before;
   const int64_t body = ctx->use_cond ? ctx->body_nodes : 0;
-  nodes -= body * nsteps;  // the bodies run only on rebuild steps
+  if (ctx->use_cond) nodes -= body * ctx->bodies;  // the bodies run only on rebuild steps
   ctx->launches = before;  // captured, not executed
   if (rc) {
     if (g) cudaGraphDestroy(g);
@@ -1220,6 +1275,7 @@ int pool_alloc(gemsgpu_pool* P) {
     m.end = P->dmap[k] + 2 * P->cap[k];
     m.sys_blk0 = P->dmap[k] + 3 * P->cap[k];
     m.sys_nblk = P->dmap[k] + 3 * P->cap[k] + P->scap;
+    m.base = 0;
   }
   CHK(dalloc(ctx, &P->dsys, P->max_systems));
   CHK(grow_blocks(ctx, *std::max_element(P->cap, P->cap + 5)));

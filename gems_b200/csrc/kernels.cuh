@@ -237,7 +237,7 @@ __device__ __forceinline__ double2 sys_top2(const Arena& A, const BlockMap& M, i
 // decides rebuild = sqrt(d1) + sqrt(d2) > nb_dcut (test_update).
 __device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, int s,
                                            double2 t) {
-  if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
+  if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
   if (last_block(M, A.st, s, &A.st[s].ticket) && threadIdx.x < 32) {
     double2 v = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
@@ -1116,7 +1116,7 @@ __device__ __forceinline__ void sys6_close(Arena& A, const BlockMap& M, int s, c
 #pragma unroll
   for (int k = 0; k < 6; k++) b[k] = block_sum(w[k]);
   if (threadIdx.x == 0)
-    for (int k = 0; k < 6; k++) A.blk_red[8 * blockIdx.x + k] = b[k];
+    for (int k = 0; k < 6; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = b[k];
   if (last_block(M, A.st, s, &A.st[s].ticket2) && threadIdx.x < 32) {
     const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
     double t[6] = {0, 0, 0, 0, 0, 0};
@@ -1715,7 +1715,7 @@ __device__ __forceinline__ bool sys3_close(Arena& A, const BlockMap& M, int s, c
 #pragma unroll
   for (int k = 0; k < 3; k++) b[k] = block_sum(w[k]);
   if (threadIdx.x == 0)
-    for (int k = 0; k < 3; k++) A.blk_red[8 * blockIdx.x + k] = b[k];
+    for (int k = 0; k < 3; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = b[k];
   bool last = last_block(M, A.st, s, &A.st[s].ticket2);
   if (!last || threadIdx.x >= 32) return false;
   const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
@@ -1900,7 +1900,7 @@ template <bool COND, bool PISTON = true>
 __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, const SysDev& S, SysState& st,
                                            bool frozen, double2 t, cudaGraphConditionalHandle cond) {
   t = block_top2(t);
-  if (threadIdx.x == 0) A.blk_top2[blockIdx.x] = t;
+  if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
   if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
     double2 w = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
@@ -2107,7 +2107,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
   if (S.integ != IT_FIRE) return;  // uniform per block
   double Pb = block_sum(P);
   double Fb = block_max(f2max);
-  if (threadIdx.x == 0) A.blk_red[2 * blockIdx.x] = Pb, A.blk_red[2 * blockIdx.x + 1] = Fb;
+  if (threadIdx.x == 0) A.blk_red[2 * (M.base + blockIdx.x)] = Pb, A.blk_red[2 * (M.base + blockIdx.x) + 1] = Fb;
   if (last_block(M, A.st, s, &st.ticket2) && threadIdx.x < 32) {
     const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
     double Pt = 0.0, Ft = 0.0;
