@@ -3250,6 +3250,242 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   return 0;
 }
 
+// ------------------------------------------------------------------ GEMS .chp
+// write_chp / read_chp (src/Checkpoint.F90:154-244) lay a checkpoint out as
+// Fortran unformatted sequential records, each framed by its byte length as
+// a 4-byte integer before and after (the gfortran layout):
+//   current, step, nsteps, nlocal            4 x int32
+//   tbox(3,3)                                9 x float64, column-major
+//   'lcg' | 'std', then the generator state  (write_chpseed, Random.F90:178-184)
+//   piston(3)                                3 x logical(4)
+//   ppos(i), pvel(i), pistonf(i)             one float64 record each, per piston i
+//   nframe, time, dm_steps, pnframe, ptime, frame   5 x float64 + int32
+//   per atom: pos, vel, acel, acel2, acel3, acel4    3 x float64 each
+// (write_chppiston / read_chppiston, Integration.F90:1488-1520).  The
+// library writes the 'lcg' form with the caller's generator state and zero
+// higher derivatives (acel2..4, the Nordsieck predictor's).
+namespace {
+struct ChpOut {
+  std::vector<unsigned char> b;
+  void raw(const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    b.insert(b.end(), c, c + n);
+  }
+  void rec(const void* p, size_t n) {
+    const int32_t m = (int32_t)n;
+    raw(&m, 4);
+    raw(p, n);
+    raw(&m, 4);
+  }
+};
+
+struct ChpIn {
+  const unsigned char* p;
+  size_t n, at = 0;
+  bool ok = true;
+  // the next record's payload (nullptr if the framing is broken)
+  const unsigned char* rec(size_t* len) {
+    int32_t m0, m1;
+    if (at + 4 > n) return ok = false, nullptr;
+    memcpy(&m0, p + at, 4);
+    if (m0 < 0 || at + 8 + (size_t)m0 > n) return ok = false, nullptr;
+    memcpy(&m1, p + at + 4 + m0, 4);
+    if (m1 != m0) return ok = false, nullptr;
+    const unsigned char* q = p + at + 4;
+    at += 8 + (size_t)m0;
+    *len = (size_t)m0;
+    return q;
+  }
+  bool getb(void* out, size_t size) {
+    size_t len = 0;
+    const unsigned char* q = rec(&len);
+    if (!q || len != size) return ok = false;
+    memcpy(out, q, len);
+    return true;
+  }
+  bool get(int32_t* out, size_t count) { return getb(out, 4 * count); }
+  bool get(double* out, size_t count) { return getb(out, 8 * count); }
+};
+
+// The piston values the reference holds after a step: the library closes a
+// G-JF piston step at the start of the next one (it needs the whole
+// system's virial), so the step just taken is closed here, as lgf_stepb /
+// lgf_flex_stepb (Integration.F90:600-650, 778-830) would have.
+void chp_pistons(const SysDev& d, const SysState& st, const double L[3], int flag[3], double pvel[3], double pf[3]) {
+  for (int k = 0; k < 3; k++) flag[k] = 0, pvel[k] = 0.0, pf[k] = 0.0;
+  const double vol = L[0] * L[1] * L[2];
+  if (d.integ == IT_LGF) {
+    for (int k = 0; k < 3; k++) flag[k] = 1;
+    if (st.lgf_phase) {
+      const double pfn = ((st.vir[0] + st.vir[1] + st.vir[2]) / 3 + d.lgf_kin) / vol - d.lgf_press;
+      pvel[0] = d.lgf_av * st.lgf_pvel + 0.5 * d.lgf_ipm * d.dt * (d.lgf_av * st.lgf_pf + pfn) +
+                d.lgf_bv * d.lgf_ipm * st.lgf_rangv;
+      pf[0] = pfn;
+    } else {
+      pvel[0] = st.lgf_pvel;
+    }
+  } else if (d.integ == IT_AXES) {
+    for (int k = 0; k < 3; k++) {
+      if (d.ax_mode[k] != AX_FLEX) continue;
+      const double* q = d.ax_p[k];
+      flag[k] = 1;
+      if (st.ax_phase[k]) {
+        const double pfn = (st.vir[k] + q[2]) / vol - q[3];
+        pvel[k] = q[7] * st.ax_pvel[k] + 0.5 * q[4] * d.dt * (q[7] * st.ax_pf[k] + pfn) * vol / L[k] +
+                  q[5] * q[4] * st.ax_rangv[k];
+        pf[k] = pfn;
+      } else {
+        pvel[k] = st.ax_pvel[k];
+      }
+    }
+  } else if (d.integ == IT_LKD) {
+    for (int k = 0; k < 3; k++) flag[k] = 1;
+    pvel[0] = st.lgf_pvel;
+  }
+}
+}  // namespace
+
+int gemsgpu_chp_write(gemsgpu_ctx* ctx, int sys, const gemsgpu_chp_info* info, void* buf, size_t bytes,
+                      size_t* written) {
+  CHK(check_sys(ctx, sys));
+  if (!info) return fail(ctx, GEMSGPU_ERR_ARG, "chp_write: info required");
+  const SysHost& h = ctx->sys[sys];
+  if (h.pos_dirty || !h.has_forces)
+    return fail(ctx, GEMSGPU_ERR_STATE, "chp_write: evaluate the forces at these positions first");
+  double L[3];
+  CHK(gemsgpu_get_box(ctx, sys, L));
+  CHK(read_states(ctx));
+  const SysState& st = ctx->h_st[sys];
+  std::vector<double> x(3 * (size_t)h.n), v(3 * (size_t)h.n), a(3 * (size_t)h.n);
+  CHK(get_d4(ctx, h, ctx->A.pos, x.data()));
+  CHK(get_d4(ctx, h, ctx->A.vel, v.data()));
+  CHK(get_d4(ctx, h, ctx->A.acel, a.data()));
+  ChpOut o;
+  const int32_t head[4] = {info->current, info->step, info->nsteps, h.n};
+  o.rec(head, sizeof(head));
+  double tbox[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < 3; k++) tbox[4 * k] = h.d.boxed ? L[k] : 0.0;
+  o.rec(tbox, sizeof(tbox));
+  o.rec("lcg", 3);
+  o.rec(info->rng, 3 * sizeof(int32_t));
+  int flag[3];
+  double pvel[3], pf[3];
+  chp_pistons(h.d, st, L, flag, pvel, pf);
+  const int32_t fl[3] = {flag[0], flag[1], flag[2]};
+  o.rec(fl, sizeof(fl));
+  for (int k = 0; k < 3; k++)
+    if (flag[k]) {
+      const double zero = 0.0;
+      o.rec(&zero, 8);
+      o.rec(&pvel[k], 8);
+      o.rec(&pf[k], 8);
+    }
+  const double fr[5] = {info->nframe, info->time, info->dm_steps, info->pnframe, info->ptime};
+  unsigned char frec[5 * 8 + 4];
+  memcpy(frec, fr, sizeof(fr));
+  memcpy(frec + sizeof(fr), &info->frame, 4);
+  o.rec(frec, sizeof(frec));
+  const double z3[3] = {0, 0, 0};
+  for (int i = 0; i < h.n; i++) {
+    o.rec(&x[3 * (size_t)i], 24);
+    o.rec(&v[3 * (size_t)i], 24);
+    o.rec(&a[3 * (size_t)i], 24);
+    for (int k = 0; k < 3; k++) o.rec(z3, 24);
+  }
+  if (written) *written = o.b.size();
+  if (!buf) return 0;  // size query
+  if (bytes < o.b.size()) return fail(ctx, GEMSGPU_ERR_ARG, "chp_write: buffer of %zu bytes needed", o.b.size());
+  memcpy(buf, o.b.data(), o.b.size());
+  return 0;
+}
+
+int gemsgpu_chp_read(gemsgpu_ctx* ctx, int sys, const void* buf, size_t bytes, gemsgpu_chp_info* info) {
+  CHK(check_sys(ctx, sys));
+  if (!buf) return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: NULL buffer");
+  SysHost& h = ctx->sys[sys];
+  ChpIn in{static_cast<const unsigned char*>(buf), bytes};
+  int32_t head[4];
+  double tbox[9];
+  if (!in.get(head, 4) || !in.get(tbox, 9)) return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: not a GEMS checkpoint");
+  if (head[3] != h.n)
+    return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: %d atoms in the checkpoint, %d in the system", head[3], h.n);
+  gemsgpu_chp_info got{};
+  got.current = head[0];
+  got.step = head[1];
+  got.nsteps = head[2];
+  size_t len = 0;
+  const unsigned char* tag = in.rec(&len);
+  if (!tag || len != 3) return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: generator record missing");
+  if (memcmp(tag, "lcg", 3) == 0) {
+    if (!in.get(got.rng, 3)) return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: lcg state");
+  } else if (memcmp(tag, "std", 3) == 0) {
+    int32_t sz = 0;
+    if (!in.get(&sz, 1) || sz < 0 || !in.rec(&len) || len != 4 * (size_t)sz)
+      return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: std seed");
+  } else {
+    return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: checkpoint file corrupted");
+  }
+  int32_t fl[3];
+  if (!in.get(fl, 3)) return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: piston flags");
+  double pvel[3] = {0, 0, 0};
+  for (int k = 0; k < 3; k++)
+    if (fl[k]) {
+      double ppos, pf;
+      if (!in.get(&ppos, 1) || !in.get(&pvel[k], 1) || !in.get(&pf, 1))
+        return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: piston %d", k);
+    }
+  size_t flen = 0;
+  const unsigned char* fr = in.rec(&flen);
+  if (!fr || flen != 44) return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: frame record");
+  double f5[5];
+  memcpy(f5, fr, 40);
+  memcpy(&got.frame, fr + 40, 4);
+  got.nframe = f5[0], got.time = f5[1], got.dm_steps = f5[2], got.pnframe = f5[3], got.ptime = f5[4];
+  std::vector<double> x(3 * (size_t)h.n), v(3 * (size_t)h.n), a(3 * (size_t)h.n), tmp(3);
+  for (int i = 0; i < h.n; i++) {
+    if (!in.get(&x[3 * (size_t)i], 3) || !in.get(&v[3 * (size_t)i], 3) || !in.get(&a[3 * (size_t)i], 3) ||
+        !in.get(tmp.data(), 3) || !in.get(tmp.data(), 3) || !in.get(tmp.data(), 3))
+      return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: atom %d", i);
+  }
+  // the box the checkpoint had reached (box_setvars after read(chpunit) tbox)
+  if (h.d.boxed) {
+    h.box_live = false;
+    for (int k = 0; k < 3; k++) h.d.L[k] = tbox[4 * k];
+    CHK(push_sys(ctx, sys));
+    drop_maps(ctx);
+    invalidate(ctx);
+  }
+  CHK(h2d_xyz(ctx, x.data(), ctx->A.pos + h.off, h.n));
+  CHK(h2d_xyz(ctx, v.data(), ctx->A.vel + h.off, h.n));
+  CHK(h2d_xyz(ctx, a.data(), ctx->A.acel + h.off, h.n));
+  CHK(read_states(ctx));
+  SysState st = ctx->h_st[sys];
+  // a piston resumes as the reference's does after read_chp: pvel from the
+  // file, pistonf from the virial of the first force evaluation
+  if (h.d.integ == IT_LGF || h.d.integ == IT_LKD) {
+    st.lgf_pvel = pvel[0];
+    st.lgf_phase = 0;
+  } else if (h.d.integ == IT_AXES) {
+    for (int k = 0; k < 3; k++)
+      if (h.d.ax_mode[k] == AX_FLEX) {
+        st.ax_pvel[k] = pvel[k];
+        st.ax_phase[k] = 0;
+      }
+  }
+  for (int k = 0; k < 3; k++) st.box_b[k] = h.d.L[k];
+  st.status = 0;
+  CU(cudaMemcpyAsync(ctx->A.st + sys, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+  BlockMap m;
+  CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
+  k_refresh_fx<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  CU(cudaStreamSynchronize(ctx->stream));
+  h.first = true;  // the resumed interact rebuilds the list, as read_chp's interact does
+  h.has_forces = false;
+  h.pos_dirty = false;
+  if (info) *info = got;
+  return 0;
+}
+
 // ------------------------------------------------------------------ L-BFGS
 // lbfgs_minimizator (src/Quasi_Newton.f90:77-160) for nsys systems at once;
 // the kernels and the method are in lbfgs.cuh.  Rounds of function

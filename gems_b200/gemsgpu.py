@@ -32,6 +32,15 @@ _d, _i, _p, _l = ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 
+
+class ChpInfo(ctypes.Structure):
+    """gemsgpu_chp_info: what a GEMS checkpoint holds beyond the system."""
+    _fields_ = [("current", ctypes.c_int32), ("step", ctypes.c_int32), ("nsteps", ctypes.c_int32),
+                ("rng", ctypes.c_int32 * 3), ("nframe", ctypes.c_double), ("time", ctypes.c_double),
+                ("dm_steps", ctypes.c_double), ("pnframe", ctypes.c_double), ("ptime", ctypes.c_double),
+                ("frame", ctypes.c_int32)]
+
+
 _SIGS = {
     "gemsgpu_version": (ctypes.c_char_p, []),
     "gemsgpu_create": (_i, [_i, _l, _i, ctypes.POINTER(_p)]),
@@ -65,6 +74,8 @@ _SIGS = {
     "gemsgpu_set_virial": (_i, [_p, _i, _i]),
     "gemsgpu_set_lgf": (_i, [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_set_lgf_normals": (_i, [_p, _i, _dp]),
+    "gemsgpu_chp_write": (_i, [_p, _i, ctypes.POINTER(ChpInfo), _p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "gemsgpu_chp_read": (_i, [_p, _i, _p, ctypes.c_size_t, ctypes.POINTER(ChpInfo)]),
     "gemsgpu_add_lgf_axis": (_i, [_p, _i, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_set_lkd": (_i, [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_add_ermak_axis": (_i, [_p, _i, _i, _d, _d, _d, ctypes.c_uint64]),
@@ -610,6 +621,28 @@ class System:
         """read_chp: resume from checkpoint bytes (the next interact rebuilds the list)."""
         buf = ctypes.create_string_buffer(data, len(data))
         self._c(lib().gemsgpu_checkpoint_load(self.ctx.h, self.sid, buf, len(data)))
+
+    def write_gems_chp(self, current=1, step=0, nsteps=0, rng=(0, 0, 0), **frame):
+        """write_chp: GEMS's checkpoint file as bytes (rng = lcg idum, iy, ix;
+        frame: nframe, time, dm_steps, pnframe, ptime, frame)."""
+        info = ChpInfo(current, step, nsteps, (ctypes.c_int32 * 3)(*rng), frame.get("nframe", 0.0),
+                       frame.get("time", 0.0), frame.get("dm_steps", 0.0), frame.get("pnframe", 0.0),
+                       frame.get("ptime", 0.0), frame.get("frame", 0))
+        n = ctypes.c_size_t()
+        self._c(lib().gemsgpu_chp_write(self.ctx.h, self.sid, ctypes.byref(info), None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        self._c(lib().gemsgpu_chp_write(self.ctx.h, self.sid, ctypes.byref(info), buf, n.value, ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    def read_gems_chp(self, data):
+        """read_chp: resume from GEMS checkpoint bytes; returns the file's
+        counters and generator state as a dict."""
+        buf = ctypes.create_string_buffer(data, len(data))
+        info = ChpInfo()
+        self._c(lib().gemsgpu_chp_read(self.ctx.h, self.sid, buf, len(data), ctypes.byref(info)))
+        return {"current": info.current, "step": info.step, "nsteps": info.nsteps, "rng": tuple(info.rng),
+                "nframe": info.nframe, "time": info.time, "dm_steps": info.dm_steps, "pnframe": info.pnframe,
+                "ptime": info.ptime, "frame": info.frame}
 
     def lbfgs(self, m=5, eps=1e-8, xtol=1e-15, itermax=1000):
         """lbfgs_minimizator: minimise in place; returns (status, iterations,

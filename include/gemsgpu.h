@@ -344,6 +344,31 @@ int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes);
 int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf,
                             size_t bytes);
 
+/* GEMS's own checkpoint file (write_chp / read_chp, src/Checkpoint.F90:
+ * 154-244): the Fortran unformatted records of the reference, so GEMS and
+ * this library resume each other's runs.  The caller supplies (write) or
+ * receives (read) what the file holds beyond the system's state: the
+ * algorithm index, step counters, the LCG generator state (idum, iy, ix of
+ * write_chpseed, src/Random.F90:178-184) and the output counters.
+ * gemsgpu_chp_write needs the forces at the current positions (the piston
+ * values it writes close the last step as lgf_stepb does); with buf NULL it
+ * only reports the size in *written.  gemsgpu_chp_read takes a system of the
+ * file's atom count, restores positions, velocities, accelerations, the box
+ * and the piston velocities; the next force evaluation rebuilds the list
+ * and a piston takes its force from that evaluation's virial, as the
+ * reference does after read_chp.  Higher derivatives are written as zero
+ * and ignored on reading. */
+typedef struct {
+  int32_t current, step, nsteps;
+  int32_t rng[3];   /* lcg idum, iy, ix */
+  double nframe, time, dm_steps, pnframe, ptime;
+  int32_t frame;
+} gemsgpu_chp_info;
+int gemsgpu_chp_write(gemsgpu_ctx* ctx, int sys, const gemsgpu_chp_info* info,
+                      void* buf, size_t bytes, size_t* written);
+int gemsgpu_chp_read(gemsgpu_ctx* ctx, int sys, const void* buf, size_t bytes,
+                     gemsgpu_chp_info* info);
+
 /* ------------------------------------------------------------ pools */
 
 /* A pool runs a changing set of systems (one force-field kind and precision)

@@ -1643,6 +1643,15 @@ void orc_rng_state(void* r, int* st) {
   Lcg* l = (Lcg*)r;
   st[0] = l->idum; st[1] = l->ix; st[2] = l->iy; st[3] = l->gaus_stored;
 }
+// lcg_read_chpseed (Random.F90:186-190): the state a checkpoint holds, in
+// its record order idum, iy, ix (no Gaussian is cached between rang pairs)
+void orc_rng_set_state(void* r, int idum, int iy, int ix) {
+  Lcg* l = (Lcg*)r;
+  l->idum = idum;
+  l->iy = iy;
+  l->ix = ix;
+  l->gaus_stored = false;
+}
 
 // create_fill (Select_Create.F90:64-135): random sequential addition in
 // [origin, origin+frame) with the reference's overlap rule rd < (s_a+s_b)^2.
@@ -1989,6 +1998,23 @@ void orc_add_ermak_axis(void* p, int d, double dt, double gama, double temp, voi
   a.crv2 = std::sqrt(1.0 - (a.crv1 * a.crv1));
   a.skt = std::sqrt(kB_ui * temp);
   add_axis(*s, a);
+}
+
+// pistonf(3), pvel(3) as the reference holds them after a step
+// (Integration.F90:66): the isotropic and LKD pistons use index 0
+void orc_piston_state(void* p, double* pf3, double* pvel3) {
+  Sys* s = (Sys*)p;
+  for (int k = 0; k < 3; k++) pf3[k] = pvel3[k] = 0.0;
+  if (s->integ == IT_LGF || s->integ == IT_LKD) {
+    pf3[0] = s->pistonf;
+    pvel3[0] = s->pvel;
+  } else if (s->integ == IT_AXES) {
+    for (const AxisInt& a : s->axes)
+      if (a.mode == AX_FLEX) {
+        pf3[a.d] = a.pf;
+        pvel3[a.d] = a.pvel;
+      }
+  }
 }
 
 void orc_virial_ev(void* p, double* out9) {

@@ -96,6 +96,8 @@ def lib():
         "orc_add_lgf_axis": (None, [_p, _i, _d, _d, _d, _d, _d, _d, _p]),
         "orc_add_ermak_axis": (None, [_p, _i, _d, _d, _d, _p]),
         "orc_set_lkd": (None, [_p, _d, _d, _d, _d, _d, _d, _p]),
+        "orc_rng_set_state": (None, [_p, _i, _i, _i]),
+        "orc_piston_state": (None, [_p, _dp, _dp]),
         "orc_pressure_atm": (None, [_p, _dp]),
         "orc_get_box": (None, [_p, _dp]),
         "orc_atm_ui": (_d, []),
@@ -156,6 +158,15 @@ class Rng:
         out = np.empty(2 * int(npairs), dtype=np.float64)
         lib().orc_rang_stream(self.h, int(npairs), _ptr(out))
         return out
+
+    def set_state(self, idum, iy, ix):
+        """lcg_read_chpseed: resume from a checkpoint's (idum, iy, ix)."""
+        lib().orc_rng_set_state(self.h, int(idum), int(iy), int(ix))
+
+    def chp_state(self):
+        """(idum, iy, ix) in the order write_chpseed stores them."""
+        st = self.state()
+        return int(st[0]), int(st[2]), int(st[1])
 
     def state(self):
         st = np.zeros(4, dtype=np.int32)
@@ -403,6 +414,12 @@ class System:
         """`evolve ermak_x|y|z`: Ermak dynamics of one coordinate."""
         self._rng = rng
         lib().orc_add_ermak_axis(self.h, int(axis), float(dt), float(gama), float(temp), rng.h)
+
+    def piston_state(self):
+        """(pistonf[3], pvel[3]) after the last step, internal units."""
+        pf, pv = np.zeros(3), np.zeros(3)
+        lib().orc_piston_state(self.h, _ptr(pf), _ptr(pv))
+        return pf, pv
 
     def virial_ev(self):
         out = np.zeros(9)

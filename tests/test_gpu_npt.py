@@ -257,3 +257,108 @@ def test_lkd_trajectory_equals_oracle(ctx):
     np.testing.assert_array_equal(a.box_now(), b.box_now())
     a.destroy()
     b.destroy()
+
+
+# ------------------------------------------------------------------ GEMS .chp
+def _records(data):
+    """Fortran unformatted sequential records (4-byte length before and after)."""
+    import struct
+    out, at = [], 0
+    while at < len(data):
+        (m,) = struct.unpack_from("<i", data, at)
+        (m2,) = struct.unpack_from("<i", data, at + 4 + m)
+        assert m == m2
+        out.append(data[at + 4:at + 4 + m])
+        at += 8 + m
+    return out
+
+
+def test_gems_checkpoint_file_flex_split_run(ctx):
+    """examples/test.sh's checkpoint case (lgf_flex_a.gms + lgf_flex_b.gms):
+    50 steps, GEMS's checkpoint file, a fresh system resumed from it with the
+    file's LCG state, 50 more; the concatenated energies are
+    Energy.lgf_flex.dat.  The file is checked record by record against the
+    layout of write_chp and the oracle's piston state after 50 steps."""
+    import struct
+    d = decks.npt_axes_deck("flex")
+    n = len(d["pos"])
+    g = _gpu_axes(ctx, d)
+    rng = O.Rng(d["seed"])
+    Ea, Pa, Va = decks.npt_run(g, d, rng, nsteps=50, feed=_feed)
+    state = rng.chp_state()
+    chp = g.write_gems_chp(current=1, step=50, nsteps=50, rng=state, time=50 * d["dt"], frame=5)
+    r = _records(chp)
+    assert struct.unpack("<4i", r[0]) == (1, 50, 50, n)
+    tbox = np.array(struct.unpack("<9d", r[1])).reshape(3, 3, order="F")
+    np.testing.assert_array_equal(np.diag(tbox), g.box_now())
+    assert r[2] == b"lcg" and struct.unpack("<3i", r[3]) == state
+    assert struct.unpack("<3i", r[4]) == (1, 1, 1)
+    s, rng_o = O.System(d["pos"], d["mass"]), O.Rng(d["seed"])
+    decks.npt_axes_setup(s, d, rng_o)
+    decks.npt_run(s, d, rng_o, nsteps=50)
+    pf, pv = s.piston_state()
+    for k in range(3):
+        ppos, pvel, pistonf = (struct.unpack("<d", r[5 + 3 * k + q])[0] for q in range(3))
+        assert ppos == 0.0
+        assert abs(pvel - pv[k]) <= 1e-9 * abs(pv[k]) and abs(pistonf - pf[k]) <= 1e-9 * abs(pf[k])
+    fr = struct.unpack("<5di", r[14])
+    assert fr[1] == 50 * d["dt"] and fr[5] == 5
+    atoms = r[15:]
+    assert len(atoms) == 6 * n
+    np.testing.assert_array_equal(np.array([struct.unpack("<3d", atoms[6 * i]) for i in range(n)]), g.pos)
+    g.destroy()
+    h = _gpu_axes(ctx, d, pos=np.zeros_like(d["pos"]))
+    info = h.read_gems_chp(chp)
+    assert info["step"] == 50 and info["rng"] == state and info["frame"] == 5
+    rng_b = O.Rng(1)
+    rng_b.set_state(*info["rng"])
+    Eb, Pb, Vb = decks.npt_run(h, d, rng_b, nsteps=50, feed=_feed)
+    E = np.vstack([Ea, Eb])
+    E[:, :3] *= O.UI_EV
+    np.testing.assert_allclose(E, d["ref_energy"], rtol=2e-6)
+    np.testing.assert_allclose(np.vstack([Pa, Pb]), d["ref_press"], rtol=2e-6, atol=1e-2)
+    h.destroy()
+
+
+def test_gems_checkpoint_file_from_gems(ctx):
+    """A file laid out as GEMS writes it (an 'std' generator record, no
+    piston) resumes an NVT system: positions, velocities, accelerations,
+    the box and the counters; a wrong atom count and a cut file are errors."""
+    import struct
+    d = decks.npt_lgf_deck()
+    n = len(d["pos"])
+    rng = np.random.default_rng(4)
+    x = np.mod(d["pos"] + rng.normal(0, 0.05, d["pos"].shape), d["box"][0] * 0.999)
+    v = rng.normal(0, 1.0, x.shape)
+    a = rng.normal(0, 1.0, x.shape)
+    L = np.array(d["box"]) * 0.999
+
+    def rec(b):
+        return struct.pack("<i", len(b)) + b + struct.pack("<i", len(b))
+    data = rec(struct.pack("<4i", 3, 700, 1000, n)) + rec(np.diag(L).flatten(order="F").tobytes())
+    data += rec(b"std") + rec(struct.pack("<i", 2)) + rec(struct.pack("<2i", 11, 12))
+    data += rec(struct.pack("<3i", 0, 0, 0)) + rec(struct.pack("<5di", 7.0, 1.4, 700.0, 0.0, 0.0, 7))
+    for i in range(n):
+        for arr in (x[i], v[i], a[i], np.zeros(3), np.zeros(3), np.zeros(3)):
+            data += rec(np.asarray(arr, dtype="<f8").tobytes())
+    g = gems.System(np.zeros_like(x), d["mass"], ctx=ctx)
+    g.set_box(d["box"], (True, True, True))
+    g.set_slj(*d["slj"])
+    g.set_ermak(d["dt"], 10.0, 300.0)
+    info = g.read_gems_chp(data)
+    assert (info["current"], info["step"], info["nsteps"], info["frame"]) == (3, 700, 1000, 7)
+    np.testing.assert_array_equal(g.pos, x)
+    np.testing.assert_array_equal(g.vel, v)
+    np.testing.assert_array_equal(g.acel, a)
+    np.testing.assert_array_equal(g.box_now(), L)
+    g.interact()
+    g.md_steps(5)
+    for bad in (data[:-10], data[:40]):
+        with pytest.raises(gems.GemsGpuError):
+            g.read_gems_chp(bad)
+    small = gems.System(x[:10], d["mass"], ctx=ctx)
+    small.set_box(d["box"], (True, True, True))
+    with pytest.raises(gems.GemsGpuError):
+        small.read_gems_chp(data)
+    g.destroy()
+    small.destroy()
