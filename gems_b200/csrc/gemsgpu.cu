@@ -514,10 +514,18 @@ std::string map_key(const std::vector<int>& ss, int apb, int kind) {
   return key;
 }
 
+// position of ss as a contiguous run inside the batch being captured, or -1
+int view_run(const gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  const std::vector<int>& vs = ctx->view_set;
+  if (vs.size() <= ss.size() || ss.empty()) return -1;
+  auto it = std::find(vs.begin(), vs.end(), ss[0]);
+  if (it == vs.end() || (size_t)(vs.end() - it) < ss.size()) return -1;
+  return std::equal(ss.begin(), ss.end(), it) ? (int)(it - vs.begin()) : -1;
+}
+
 int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, BlockMap* out) {
-  if (ss.size() == 1 && ctx->view_set.size() > 1 &&
-      std::find(ctx->view_set.begin(), ctx->view_set.end(), ss[0]) != ctx->view_set.end()) {
-    // a branch of a batched graph: the system's blocks of the batch's map
+  if (view_run(ctx, ss) >= 0) {
+    // a branch of a batched graph: its systems' blocks of the batch's map
     std::vector<int> full;
     full.swap(ctx->view_set);
     BlockMap fm;
@@ -525,7 +533,14 @@ int get_map(gemsgpu_ctx* ctx, const std::vector<int>& ss, int apb, int kind, Blo
     full.swap(ctx->view_set);
     CHK(rc);
     const DevMap& dm = ctx->maps[map_key(ctx->view_set, apb, kind)];
-    const int b0 = dm.blk0[ss[0]], nb = dm.nblkv[ss[0]];
+    int b0 = -1, b1 = 0;
+    for (int s : ss)
+      if (dm.nblkv[s] > 0) {
+        if (b0 < 0) b0 = dm.blk0[s];
+        b1 = dm.blk0[s] + dm.nblkv[s];
+      }
+    if (b0 < 0) b0 = b1 = 0;
+    const int nb = b1 - b0;
     BlockMap v = fm;
     v.nblk = nb;
     v.base = b0;
@@ -994,21 +1009,31 @@ int cap_plain(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
   return record_steps(ctx, ss, *(int*)arg);
 }
 
-// A batch of several systems is captured as one independent branch per
-// system: each system's steps, conditional rebuilds and force passes form
-// their own chain, so the GPU overlaps one system's list build or kernel
-// tail with the others' work.  The per-system launches use the batch's
-// block maps (views), so each block keeps its own per-block scratch slot.
+// A batch of several systems with one launch shape is captured as
+// independent branches -- one per system, or up to 16 runs of consecutive
+// systems for larger batches: each branch's steps, conditional rebuilds and
+// force passes form their own chain, so the GPU overlaps one system's list
+// build or kernel tail with the others' work.  A branch's launches use the
+// batch's block maps (views of its systems' blocks), so each block keeps
+// its own per-block scratch slot.
 int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGraph_t* out) {
   cudaGraph_t g = nullptr;
   CU(cudaGraphCreate(&g, 0));
   int rc = 0;
   bool cond_ok = ctx->use_cond;
+  // up to MAX_BRANCHES branches of consecutive systems
+  constexpr size_t MAX_BRANCHES = 16;
   std::vector<std::vector<int>> sets;
-  if (ss.size() > 1)
-    for (int s : ss) sets.push_back({s});
-  else
-    sets.push_back(ss);
+  bool uniform = true;
+  for (int s : ss) {
+    const SysHost& a = ctx->sys[s];
+    const SysHost& b = ctx->sys[ss[0]];
+    uniform &= a.d.ff == b.d.ff && a.d.prec == b.d.prec && a.lanes == b.lanes && a.variant == b.variant &&
+               a.d.virial == b.d.virial && (a.ntypes == 1) == (b.ntypes == 1);
+  }
+  const size_t nb = uniform ? std::min(ss.size(), MAX_BRANCHES) : 1;
+  for (size_t j = 0; j < nb; j++)
+    sets.emplace_back(ss.begin() + j * ss.size() / nb, ss.begin() + (j + 1) * ss.size() / nb);
   std::vector<std::vector<cudaGraphNode_t>> deps(sets.size());
   if (sets.size() > 1) ctx->view_set = ss;
   ctx->bodies = 0;
@@ -1076,8 +1101,11 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
     CHK(get_map(ctx, ss, BLOCK / 32, 1, &m));
     CHK(get_map(ctx, ss, 1, 1, &m));
     CHK(sys_array(ctx, ss, &sa));
+    const size_t nbr = std::min<size_t>(ss.size(), 16);
+    for (size_t j = 0; j < nbr && ss.size() > 1; j++)
+      CHK(sys_array(ctx, std::vector<int>(ss.begin() + j * ss.size() / nbr, ss.begin() + (j + 1) * ss.size() / nbr),
+                    &sa));
     for (int s : ss) {
-      CHK(sys_array(ctx, {s}, &sa));
       const SysHost& h = ctx->sys[s];
       CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / h.lanes, 0, &m));
     }

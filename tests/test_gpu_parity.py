@@ -643,3 +643,34 @@ def test_batched_graph_branches_equal_alone(ctx):
     assert len({g.nupd for g in a}) > 1 or all(g.nupd > 1 for g in a)
     for g in a + b:
         g.destroy()
+
+
+def test_large_batch_grouped_branches_equal_alone(ctx):
+    """Batches of more than 16 systems run as 16 branches of consecutive
+    systems; 18 uneven crystals, 100 batched Ermak steps, equal to each
+    system alone, bit for bit."""
+    from gems_b200 import workloads as W
+
+    def mk(nc, seed):
+        w = W.smatb_bulk(ncell=nc)
+        vel = W.maxwell(len(w["pos"]), w["mass"], 900.0, np.random.default_rng(seed))
+        g = gems.System(w["pos"], w["mass"], ctx=ctx, vel=vel)
+        g.set_box(w["L"], (True, True, True))
+        g.set_smatb(*w["smatb"])
+        g.set_precision(1)
+        g.set_lanes(4, 1)
+        g.set_ermak(w["dt"], w["gamma"], 900.0, seed=seed)
+        g.interact()
+        return g
+    sizes = [4, 5, 6] * 6
+    a = [mk(nc, 40 + k) for k, nc in enumerate(sizes)]
+    b = [mk(nc, 40 + k) for k, nc in enumerate(sizes)]
+    ctx.batch_md_steps(a, 100)
+    for g in b:
+        g.md_steps(100)
+    for ga, gb in zip(a, b):
+        np.testing.assert_array_equal(ga.pos, gb.pos)
+        np.testing.assert_array_equal(ga.vel, gb.vel)
+        assert ga.nupd == gb.nupd
+    for g in a + b:
+        g.destroy()
