@@ -402,7 +402,11 @@ inline double pow6(double x) {
 double lj_interact(Sys& s) {
   double etot = 0.0;
   const int n = s.n;
-#pragma omp parallel for schedule(static) reduction(+ : etot)
+  // the total is summed from the per-atom sums in atom order: the same
+  // bits for any thread count (an OpenMP reduction combines the threads'
+  // partial sums in an unspecified order)
+  std::vector<double> ea(n, 0.0);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
     int ti = s.type[i];
     double fx = 0, fy = 0, fz = 0, ep = 0;
@@ -427,7 +431,6 @@ double lj_interact(Sys& s) {
       p = p * ev_ui;
       f = f * ev_ui;
       ep = ep + p * 0.5;
-      etot = etot + p * 0.5;
       fx = fx - f * vd[0] / dr;
       fy = fy - f * vd[1] / dr;
       fz = fz - f * vd[2] / dr;
@@ -436,7 +439,9 @@ double lj_interact(Sys& s) {
     s.force[3 * i + 1] += fy;
     s.force[3 * i + 2] += fz;
     s.epot[i] += ep;
+    ea[i] = ep;
   }
+  for (int i = 0; i < n; i++) etot += ea[i];
   return etot;
 }
 
@@ -562,7 +567,8 @@ double smatb_interact(Sys& s) {
 
   const double lev_ui = ev_ui;
   double epot = 0.0;
-#pragma omp parallel for schedule(static) reduction(+ : epot)
+  std::vector<double> ea(n, 0.0);  // per-atom sums, added in atom order below
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
     int z1 = s.type[i];
     double f[3] = {0, 0, 0}, ep = 0.0;
@@ -594,14 +600,14 @@ double smatb_interact(Sys& s) {
       }
       for (int k = 0; k < 3; k++) f[k] = f[k] - factor * lev_ui * vd[k] / dr;
       ep = ep + repul * lev_ui;
-      epot = epot + repul * lev_ui;
     }
     double aux2 = std::sqrt(s.band[i]) * lev_ui;
     ep = ep - aux2;
-    epot = epot - aux2;
     for (int k = 0; k < 3; k++) s.force[3 * i + k] += f[k];
     s.epot[i] += ep;
+    ea[i] = ep;
   }
+  for (int i = 0; i < n; i++) epot += ea[i];
   return epot;
 }
 
@@ -639,7 +645,7 @@ double tersoff_interact(Sys& s) {
   nth = omp_get_max_threads();
 #endif
   std::vector<double> fbuf((size_t)nth * 3 * n, 0.0);
-#pragma omp parallel reduction(+ : etot)
+#pragma omp parallel
   {
     int tid = 0;
 #ifdef _OPENMP
@@ -695,7 +701,6 @@ double tersoff_interact(Sys& s) {
         }
         double e = 0.5 * fc * (vr + bij * va);
         s.epot[i] += e;
-        etot += e;
         // radial part: dE/dr_ij along u (u points i->j)
         double dV = 0.5 * (dfc * (vr + bij * va) + fc * (dvr + bij * dva));
         for (int k = 0; k < 3; k++) {
@@ -732,6 +737,7 @@ double tersoff_interact(Sys& s) {
   }
   for (int t = 0; t < nth; t++)
     for (size_t q = 0; q < (size_t)3 * n; q++) s.force[q] += fbuf[(size_t)t * 3 * n + q];
+  for (int i = 0; i < n; i++) etot += s.epot[i];  // atom order: the same bits for any thread count
   return etot;
 }
 
