@@ -629,7 +629,8 @@ int sys_array(gemsgpu_ctx* ctx, const std::vector<int>& ss, const int** out) {
 // (four 256-thread blocks); bit 2 with bit 1: the force pass capped at three
 // blocks instead (no spills, fewer warps).
 template <int K>
-void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, bool tight3, const BlockMap& m) {
+void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, bool tight3, bool vir,
+                  const BlockMap& m) {
   cudaStream_t st = ctx->stream;
   const Arena& A = ctx->A;
   if (prec == PREC_MIXED) {
@@ -648,7 +649,8 @@ void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, b
     }
   } else {
     if (pass == 0) k_smatb_rho_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m);
-    else k_smatb_force_fp64<K><<<m.nblk, BLOCK, 0, st>>>(A, m);
+    else if (vir) k_smatb_force_fp64<K, true><<<m.nblk, BLOCK, 0, st>>>(A, m);
+    else k_smatb_force_fp64<K, false><<<m.nblk, BLOCK, 0, st>>>(A, m);
   }
   ++ctx->launches;
 }
@@ -661,17 +663,18 @@ void lj_k(gemsgpu_ctx* ctx, int prec, bool vir, const BlockMap& m) {
   ++ctx->launches;
 }
 
-void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, int K, const BlockMap& m) {
+void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, int K, const BlockMap& m,
+                bool vir = false) {
   const bool regs = single && (variant & 1) == 0;
   const bool tight = (variant & 2) != 0;
   const bool tight3 = (variant & 4) != 0;
   switch (K) {
-    case 1: smatb_pass_k<1>(ctx, pass, prec, regs, tight, tight3, m); break;
-    case 2: smatb_pass_k<2>(ctx, pass, prec, regs, tight, tight3, m); break;
-    case 4: smatb_pass_k<4>(ctx, pass, prec, regs, tight, tight3, m); break;
-    case 8: smatb_pass_k<8>(ctx, pass, prec, regs, tight, tight3, m); break;
-    case 16: smatb_pass_k<16>(ctx, pass, prec, regs, tight, tight3, m); break;
-    default: smatb_pass_k<32>(ctx, pass, prec, regs, tight, tight3, m); break;
+    case 1: smatb_pass_k<1>(ctx, pass, prec, regs, tight, tight3, vir, m); break;
+    case 2: smatb_pass_k<2>(ctx, pass, prec, regs, tight, tight3, vir, m); break;
+    case 4: smatb_pass_k<4>(ctx, pass, prec, regs, tight, tight3, vir, m); break;
+    case 8: smatb_pass_k<8>(ctx, pass, prec, regs, tight, tight3, vir, m); break;
+    case 16: smatb_pass_k<16>(ctx, pass, prec, regs, tight, tight3, vir, m); break;
+    default: smatb_pass_k<32>(ctx, pass, prec, regs, tight, tight3, vir, m); break;
   }
 }
 
@@ -716,7 +719,7 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
     CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
     if (ff == FF_SMATB) {
       smatb_pass(ctx, 0, prec, variant, single, K, m);
-      smatb_pass(ctx, 1, prec, variant, single, K, m);
+      smatb_pass(ctx, 1, prec, variant, single, K, m, vir);
     } else if (ff == FF_LJ) {
       lj_pass(ctx, prec, K, vir, m);
     }
@@ -2163,7 +2166,8 @@ int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, doubl
 int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on) {
   CHK(check_sys(ctx, sys));
   SysHost& h = ctx->sys[sys];
-  if (on && h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "virial: pair potentials (lj, plj, slj) only");
+  if (on && h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
+    return fail(ctx, GEMSGPU_ERR_STATE, "virial: lj, plj, slj and SMA-TB systems only");
   if (on && h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "virial: FP64 systems only");
   if (!on && moving_box(h.d)) return fail(ctx, GEMSGPU_ERR_STATE, "virial: the piston needs it");
   h.d.virial = on ? 1 : 0;
@@ -2189,7 +2193,8 @@ int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
     return fail(ctx, GEMSGPU_ERR_ARG, "set_lgf: dt>0, T>=0, gammas>=0, piston mass>0");
   if (!h.d.boxed || !h.d.pbc[0] || !h.d.pbc[1] || !h.d.pbc[2])
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: the piston needs a box periodic in x, y and z");
-  if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: pair potentials (lj, plj, slj) only");
+  if (h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: lj, plj, slj and SMA-TB systems only");
   if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: FP64 systems only");
   SysDev& d = h.d;
   d.integ = IT_LGF;
@@ -2285,7 +2290,8 @@ int gemsgpu_set_lkd(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
     return fail(ctx, GEMSGPU_ERR_ARG, "set_lkd: dt>0, T>=0, gammas>=0, piston mass>0");
   if (!h.d.boxed || !h.d.pbc[0] || !h.d.pbc[1] || !h.d.pbc[2])
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: the piston needs a box periodic in x, y and z");
-  if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: pair potentials (lj, plj, slj) only");
+  if (h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: lj, plj, slj and SMA-TB systems only");
   if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: FP64 systems only");
   SysDev& d = h.d;
   d.integ = IT_LKD;
@@ -2359,7 +2365,8 @@ int gemsgpu_add_lgf_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt, double 
     return fail(ctx, GEMSGPU_ERR_ARG, "add_lgf_axis: dt>0, T>=0, gammas>=0, piston mass>0");
   if (!h.d.boxed || !h.d.pbc[axis])
     return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: the piston needs a box periodic along its axis");
-  if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: pair potentials (lj, plj, slj) only");
+  if (h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
+    return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: lj, plj, slj and SMA-TB systems only");
   if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: FP64 systems only");
   double p[8];
   p[0] = std::sqrt(2.0 * pgama0 * kB_ui * temp * dt);
@@ -2413,7 +2420,7 @@ int gemsgpu_virial(gemsgpu_ctx* ctx, int sys, double* out9) {
   CHK(check_sys(ctx, sys));
   if (!out9) return fail(ctx, GEMSGPU_ERR_ARG, "virial: NULL");
   const SysHost& h = ctx->sys[sys];
-  if (!h.d.virial || h.d.ff != FF_LJ || !h.has_forces)
+  if (!h.d.virial || (h.d.ff != FF_LJ && h.d.ff != FF_SMATB) || !h.has_forces)
     return fail(ctx, GEMSGPU_ERR_STATE, "virial: not computed (set_virial, forces)");
   CHK(read_states(ctx));
   sym9(ctx->h_st[sys].vir, UI_EV, out9);
@@ -2425,7 +2432,7 @@ int gemsgpu_pressure(gemsgpu_ctx* ctx, int sys, double* out9) {
   CHK(check_sys(ctx, sys));
   if (!out9) return fail(ctx, GEMSGPU_ERR_ARG, "pressure: NULL");
   const SysHost& h = ctx->sys[sys];
-  if (!h.d.virial || h.d.ff != FF_LJ || !h.has_forces)
+  if (!h.d.virial || (h.d.ff != FF_LJ && h.d.ff != FF_SMATB) || !h.has_forces)
     return fail(ctx, GEMSGPU_ERR_STATE, "pressure: virial not computed");
   if (!h.d.boxed) return fail(ctx, GEMSGPU_ERR_STATE, "pressure: no box");
   BlockMap m;

@@ -704,6 +704,58 @@ __global__ void k_count_rebuild(Arena A, const int* sys, int nsys, int in_graph)
   if (in_graph && k == 0) atomicAdd(A.body_runs, 1ull);
 }
 
+// ------------------------------------------------------------------ reductions
+// Six per-system sums (xx yy zz xy xz yz of a tensor): each block sums its
+// threads' values; the system's last block adds the block partials in
+// block order, so the result is the same bits on every run.
+__device__ __forceinline__ void sys6_close(Arena& A, const BlockMap& M, int s, const double w[6], double* dst) {
+  double b[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) b[k] = block_sum(w[k]);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 6; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = b[k];
+  if (last_block(M, A.st, s, &A.st[s].ticket2) && threadIdx.x < 32) {
+    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = threadIdx.x; q < nb; q += 32)
+#pragma unroll
+      for (int k = 0; k < 6; k++) t[k] += __ldcg(&A.blk_red[8 * (b0 + q) + k]);
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      for (int o = 16; o; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 6; k++) dst[k] = t[k];
+  }
+}
+
+// Pair virial W = sum_i r_i (x) F_i.  With minimum-image pairs it is half
+// the sum over the full list of vd (x) f vd / r (vd = r_j - r_i), the
+// virial inq_virial (Inq_Properties.F90:439-527) builds from local and
+// ghost atoms.
+__device__ __forceinline__ void virial_close(Arena& A, const BlockMap& M, int s, const double w[6]) {
+  sys6_close(A, M, s, w, A.st[s].vir);
+}
+
+// kinetic tensor sum_i m v (x) v of each system (inq_pressure,
+// Inq_Properties.F90:529-573), into SysState::ktens
+__global__ void k_kin_tensor(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  if (i < M.end[blockIdx.x]) {
+    const double4 v = A.vel[i];
+    const double m = A.mass[i];
+    w[0] = v.x * v.x * m;
+    w[1] = v.y * v.y * m;
+    w[2] = v.z * v.z * m;
+    w[3] = v.x * v.y * m;
+    w[4] = v.x * v.z * m;
+    w[5] = v.y * v.z * m;
+  }
+  sys6_close(A, M, s, w, A.st[s].ktens);
+}
+
 // ------------------------------------------------------------------ SMA-TB
 // Per species-pair constants of the FP64 kernels.
 struct SmFP64 {
@@ -837,7 +889,10 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
 //                       - xi^2/2 e^{-2q(r/r0-1)} (2q/r0)(eb_i + eb_j)
 //   tail     : factor = P P' (eb_i + eb_j) - 2 R'
 //   F_i -= factor * ev_ui * vd / r ;  e_i += repul ; e_i -= sqrt(rho_i)
-template <int K>
+// VIR: also the pair virial of the system (virial_close); SMA-TB forces are
+// central pair forces, F_i = -sum_j factor_ij vd / r, so W is the pair sum
+// (complete: the reference's TB.F90:548-564 omits the i-side term).
+template <int K, bool VIR>
 __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
@@ -848,6 +903,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
   if (act) {
     const double4 xi = A.pos[i];
     const int ti = A.type[i];
@@ -880,6 +936,15 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
       f1 -= fr * v1;
       f2 -= fr * v2;
       ep += repul;
+      if constexpr (VIR) {
+        const double h = 0.5 * fr;
+        w[0] += h * v0 * v0;
+        w[1] += h * v1 * v1;
+        w[2] += h * v2 * v2;
+        w[3] += h * v0 * v1;
+        w[4] += h * v0 * v2;
+        w[5] += h * v1 * v2;
+      }
     PAIR_LOOP_END
   }
   f0 = lane_sum<K>(f0);
@@ -890,6 +955,7 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
     A.force[i] = make_double4(f0, f1, f2, 0.0);
     A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
   }
+  if constexpr (VIR) virial_close(A, M, s, w);
 }
 
 // ---- mixed precision: FP32 pair math, FP64 accumulation.
@@ -1108,57 +1174,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
 }
 
 // ------------------------------------------------------------------ LJ
-// Six per-system sums (xx yy zz xy xz yz of a tensor): each block sums its
-// threads' values; the system's last block adds the block partials in
-// block order, so the result is the same bits on every run.
-__device__ __forceinline__ void sys6_close(Arena& A, const BlockMap& M, int s, const double w[6], double* dst) {
-  double b[6];
-#pragma unroll
-  for (int k = 0; k < 6; k++) b[k] = block_sum(w[k]);
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 6; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = b[k];
-  if (last_block(M, A.st, s, &A.st[s].ticket2) && threadIdx.x < 32) {
-    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
-    double t[6] = {0, 0, 0, 0, 0, 0};
-    for (int q = threadIdx.x; q < nb; q += 32)
-#pragma unroll
-      for (int k = 0; k < 6; k++) t[k] += __ldcg(&A.blk_red[8 * (b0 + q) + k]);
-#pragma unroll
-    for (int k = 0; k < 6; k++)
-      for (int o = 16; o; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
-    if (threadIdx.x == 0)
-      for (int k = 0; k < 6; k++) dst[k] = t[k];
-  }
-}
-
-// Pair virial W = sum_i r_i (x) F_i.  With minimum-image pairs it is half
-// the sum over the full list of vd (x) f vd / r (vd = r_j - r_i), the
-// virial inq_virial (Inq_Properties.F90:439-527) builds from local and
-// ghost atoms.
-__device__ __forceinline__ void virial_close(Arena& A, const BlockMap& M, int s, const double w[6]) {
-  sys6_close(A, M, s, w, A.st[s].vir);
-}
-
-// kinetic tensor sum_i m v (x) v of each system (inq_pressure,
-// Inq_Properties.F90:529-573), into SysState::ktens
-__global__ void k_kin_tensor(Arena A, BlockMap M) {
-  int s = blk_sys(M);
-  if (s < 0) return;  // padding block of a fixed-capacity map
-  int i = M.first[blockIdx.x] + threadIdx.x;
-  double w[6] = {0, 0, 0, 0, 0, 0};
-  if (i < M.end[blockIdx.x]) {
-    const double4 v = A.vel[i];
-    const double m = A.mass[i];
-    w[0] = v.x * v.x * m;
-    w[1] = v.y * v.y * m;
-    w[2] = v.z * v.z * m;
-    w[3] = v.x * v.y * m;
-    w[4] = v.x * v.z * m;
-    w[5] = v.y * v.z * m;
-  }
-  sys6_close(A, M, s, w, A.st[s].ktens);
-}
-
 // lj_interact / plj_interact (src/Pairs.F90:207-370), full list:
 //   s6 = (s/r)^6 ; p = 4e(s6^2 - s6) [- prc - frc (r - rc)] [- eshift]
 //   f = e(48 s6 - 24) s6 / r [+ frc] ; F_i -= f vd / r ; e_i += p/2

@@ -148,8 +148,10 @@ int gemsgpu_set_lj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
 int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
                     double sigma, double rs);
 /* Pair virial W = sum_i r_i (x) F_i (inq_virial, Inq_Properties.F90:439-527)
- * accumulated by the force kernels of an FP64 pair-potential system (on=1);
- * the G-JF piston switches it on. */
+ * accumulated by the force kernels of an FP64 lj/plj/slj or SMA-TB system
+ * (on=1; SMA-TB forces are central pair forces, and the library sums the
+ * complete virial where TB.F90:548-564 omits the i-side term); the pistons
+ * switch it on. */
 int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on);
 /* smatb_set (src/TB.F90:106-170): A, xi (eV), p, q, r0, rci, rce (A).  The
  * device derives the tail polynomial coefficients. */
@@ -200,8 +202,8 @@ int gemsgpu_set_fire(gemsgpu_ctx* ctx, int sys, double dt0, double dtmax);
  * volume.  dt (ps), T (K), target pressure (atm), particle friction pgama0
  * and piston friction pgamav (1/ps), piston mass pmass; lgf_stepa/stepb
  * (:527-650) per step.  The box moves on the device every step (its cell
- * grid re-planned within 15% growth); FP64 pair-potential systems in a box
- * periodic in x, y and z.  Production noise: Philox4x32-10 keyed by seed. */
+ * grid re-planned within 15% growth); FP64 lj/plj/slj or SMA-TB systems in
+ * a box periodic in x, y and z.  Production noise: Philox4x32-10 keyed by seed. */
 int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp,
                     double press_atm, double pgama0, double pgamav,
                     double pmass, uint64_t seed);
@@ -221,8 +223,8 @@ int gemsgpu_set_lkd(gemsgpu_ctx* ctx, int sys, double dt, double temp,
  * integrator starts an empty set), all with the same dt, at most one per
  * coordinate; a coordinate without one keeps its velocity.  The pistons
  * move their lengths with the volume of the step's start, as the reference
- * updates the volume after all of them.  Pistons need an FP64
- * pair-potential system periodic along their axis. */
+ * updates the volume after all of them.  Pistons need an FP64 lj/plj/slj or
+ * SMA-TB system periodic along their axis. */
 int gemsgpu_add_lgf_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt,
                          double temp, double press_atm, double pgama0,
                          double pgamav, double pmass, uint64_t seed);

@@ -568,10 +568,15 @@ double smatb_interact(Sys& s) {
   const double lev_ui = ev_ui;
   double epot = 0.0;
   std::vector<double> ea(n, 0.0);  // per-atom sums, added in atom order below
+  // pair virial W = 1/2 sum over the full list of vd (x) factor vd / r: the
+  // SMA-TB forces are central pair forces (the reference's TB.F90:548-564
+  // omits the i-side term; this is the complete sum)
+  std::vector<double> wa(9 * (size_t)n, 0.0);
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
     int z1 = s.type[i];
     double f[3] = {0, 0, 0}, ep = 0.0;
+    double* W = &wa[9 * (size_t)i];
     for (int l = 0; l < s.nn[i]; l++) {
       int j = s.list[(size_t)l * n + i];
       const SMp& P = s.sm[z1][s.type[j]];
@@ -598,7 +603,13 @@ double smatb_interact(Sys& s) {
                  2.0 * (5.0 * P.r1 * drm4 + 4.0 * P.r2 * drm3 + 3.0 * P.r3 * drm2);
         repul = P.r1 * drm5 + P.r2 * drm4 + P.r3 * drm3;
       }
-      for (int k = 0; k < 3; k++) f[k] = f[k] - factor * lev_ui * vd[k] / dr;
+      double f2[3];
+      for (int k = 0; k < 3; k++) {
+        f2[k] = factor * lev_ui * vd[k] / dr;
+        f[k] = f[k] - f2[k];
+      }
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) W[3 * a + b] += 0.5 * vd[a] * f2[b];
       ep = ep + repul * lev_ui;
     }
     double aux2 = std::sqrt(s.band[i]) * lev_ui;
@@ -608,6 +619,9 @@ double smatb_interact(Sys& s) {
     ea[i] = ep;
   }
   for (int i = 0; i < n; i++) epot += ea[i];
+  for (int k = 0; k < 9; k++) s.virial[k] = 0.0;
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 9; k++) s.virial[k] += wa[9 * (size_t)i + k];
   return epot;
 }
 

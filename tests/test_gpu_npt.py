@@ -362,3 +362,37 @@ def test_gems_checkpoint_file_from_gems(ctx):
         small.read_gems_chp(data)
     g.destroy()
     small.destroy()
+
+
+def test_smatb_virial_and_piston_equal_oracle(ctx):
+    """The pistons on a metal: the SMA-TB force pass sums the pair virial
+    (the complete sum of the central pair forces), and an Au crystal under
+    the isotropic G-JF piston at 1 atm follows the oracle for 100 steps with
+    the oracle's normals fed to the device."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=6)
+    rng = np.random.default_rng(9)
+    pos = np.mod(w["pos"] + rng.normal(0, 0.05, w["pos"].shape), w["L"])
+    s = O.System(pos, w["mass"])
+    s.set_box(w["L"], (True, True, True))
+    s.set_smatb(*w["smatb"])
+    g = gems.System(pos, w["mass"], ctx=ctx)
+    g.set_skin_mode(False)
+    g.set_box(w["L"], (True, True, True))
+    g.set_smatb(*w["smatb"])
+    g.set_virial(True)
+    s.interact()
+    g.interact()
+    np.testing.assert_allclose(g.virial_ev(), s.virial_ev(), rtol=1e-10, atol=1e-8)
+    d = dict(dt=w["dt"], nsteps=100, each=10)
+    s.set_lgf(w["dt"], 300.0, 1.0, 1.0, 1.0, 1e-3, O.Rng(7))
+    g.set_lgf(w["dt"], 300.0, 1.0, 1.0, 1.0, 1e-3)
+    rng_o = s._rng
+    B0, B1 = [], []
+    E0, P0, V0 = decks.npt_run(s, d, rng_o, boxes=B0)
+    E1, P1, V1 = decks.npt_run(g, d, O.Rng(7), feed=_feed, boxes=B1)
+    np.testing.assert_allclose(E1, E0, rtol=1e-9)
+    np.testing.assert_allclose(V1, V0, rtol=1e-8, atol=1e-6)
+    np.testing.assert_allclose(np.array(B1), np.array(B0), rtol=1e-12)
+    assert abs(B1[-1][0] - w["L"][0]) > 1e-4
+    g.destroy()
