@@ -639,6 +639,9 @@ void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, b
       else if (regs) k_smatb_rho_mixed<K, true, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else if (tight) k_smatb_rho_mixed<K, false, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else k_smatb_rho_mixed<K, false, 1><<<m.nblk, BLOCK, 0, st>>>(A, m);
+    } else if (vir) {  // the virial build: uncapped
+      if (regs) k_smatb_force_mixed<K, true, 1, true><<<m.nblk, BLOCK, 0, st>>>(A, m);
+      else k_smatb_force_mixed<K, false, 1, true><<<m.nblk, BLOCK, 0, st>>>(A, m);
     } else {
       if (regs && tight && tight3) k_smatb_force_mixed<K, true, 3><<<m.nblk, BLOCK, 0, st>>>(A, m);
       else if (regs && tight) k_smatb_force_mixed<K, true, 4><<<m.nblk, BLOCK, 0, st>>>(A, m);
@@ -657,7 +660,8 @@ void smatb_pass_k(gemsgpu_ctx* ctx, int pass, int prec, bool regs, bool tight, b
 
 template <int K>
 void lj_k(gemsgpu_ctx* ctx, int prec, bool vir, const BlockMap& m) {
-  if (prec == PREC_MIXED) k_lj_mixed<K><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  if (prec == PREC_MIXED && vir) k_lj_mixed<K, true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  else if (prec == PREC_MIXED) k_lj_mixed<K><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
   else if (vir) k_lj_fp64<K, true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
   else k_lj_fp64<K, false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
   ++ctx->launches;
@@ -1865,8 +1869,8 @@ int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec) {
   CHK(check_sys(ctx, sys));
   if (prec != GEMSGPU_PREC_FP64 && prec != GEMSGPU_PREC_MIXED)
     return fail(ctx, GEMSGPU_ERR_ARG, "unknown precision %d", prec);
-  if (prec != GEMSGPU_PREC_FP64 && (moving_box(ctx->sys[sys].d) || ctx->sys[sys].d.virial))
-    return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: the virial and the piston are FP64 only");
+  if (prec != GEMSGPU_PREC_FP64 && moving_box(ctx->sys[sys].d))
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: the pistons are FP64 only");
   if (prec != GEMSGPU_PREC_FP64 && ctx->sys[sys].d.ff == FF_LJ)
     for (const PairP& P : ctx->sys[sys].prm)
       if (P.v[8] != 0.0) return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: slj pairs are FP64 only");
@@ -2168,7 +2172,6 @@ int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on) {
   SysHost& h = ctx->sys[sys];
   if (on && h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
     return fail(ctx, GEMSGPU_ERR_STATE, "virial: lj, plj, slj and SMA-TB systems only");
-  if (on && h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "virial: FP64 systems only");
   if (!on && moving_box(h.d)) return fail(ctx, GEMSGPU_ERR_STATE, "virial: the piston needs it");
   h.d.virial = on ? 1 : 0;
   h.has_forces = false;

@@ -1090,7 +1090,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
   }
 }
 
-template <int K, bool ONE, int MINB>
+// VIR: also the pair virial, FP32 per pair and group, FP64 per atom and system.
+template <int K, bool ONE, int MINB, bool VIR = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
@@ -1101,6 +1102,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
   if (act) {
     const int4 xi = A.fxp[i];
     const float ebi = A.ebandf[i];
@@ -1124,6 +1126,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
         }
       list_group<K>(A, i, nn, m0 + UNR * K, jn);  // next group's ids, in flight meanwhile
       float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, ge = 0.0f;
+      float gw[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
       for (int u = 0; u < UNR; u++) {
         if (jj[u] < 0) continue;
@@ -1156,11 +1159,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
         g1 = fmaf(fr, v1, g1);
         g2 = fmaf(fr, v2, g2);
         ge += repul;
+        if constexpr (VIR) {
+          const float h = 0.5f * fr;
+          gw[0] += h * v0 * v0;
+          gw[1] += h * v1 * v1;
+          gw[2] += h * v2 * v2;
+          gw[3] += h * v0 * v1;
+          gw[4] += h * v0 * v2;
+          gw[5] += h * v1 * v2;
+        }
       }
       f0 -= (double)g0;
       f1 -= (double)g1;
       f2 -= (double)g2;
       ep += (double)ge;
+      if constexpr (VIR)
+        for (int k = 0; k < 6; k++) w[k] += (double)gw[k];
     }
   }
   f0 = lane_sum<K>(f0);
@@ -1171,6 +1185,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
     A.force[i] = make_double4(f0, f1, f2, 0.0);
     A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
   }
+  if constexpr (VIR) virial_close(A, M, s, w);
 }
 
 // ------------------------------------------------------------------ LJ
@@ -1251,7 +1266,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
   if constexpr (VIR) virial_close(A, M, s, w);
 }
 
-template <int K>
+template <int K, bool VIR = false>
 __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
@@ -1260,6 +1275,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
   if (act) {
     const int4 xi = A.fxp[i];
     const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
@@ -1292,6 +1308,15 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
       f1 -= (double)(fr * v1);
       f2 -= (double)(fr * v2);
       ep += (double)p;
+      if constexpr (VIR) {
+        const float h = 0.5f * fr;
+        w[0] += (double)(h * v0 * v0);
+        w[1] += (double)(h * v1 * v1);
+        w[2] += (double)(h * v2 * v2);
+        w[3] += (double)(h * v0 * v1);
+        w[4] += (double)(h * v0 * v2);
+        w[5] += (double)(h * v1 * v2);
+      }
     PAIR_LOOP_END
   }
   f0 = lane_sum<K>(f0);
@@ -1302,6 +1327,7 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
     A.force[i] = make_double4(f0, f1, f2, 0.0);
     A.epot[i] = ep * 0.5 * EV_UI;
   }
+  if constexpr (VIR) virial_close(A, M, s, w);
 }
 
 // ------------------------------------------------------------------ Tersoff

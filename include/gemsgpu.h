@@ -148,10 +148,10 @@ int gemsgpu_set_lj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
 int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
                     double sigma, double rs);
 /* Pair virial W = sum_i r_i (x) F_i (inq_virial, Inq_Properties.F90:439-527)
- * accumulated by the force kernels of an FP64 lj/plj/slj or SMA-TB system
- * (on=1; SMA-TB forces are central pair forces, and the library sums the
- * complete virial where TB.F90:548-564 omits the i-side term); the pistons
- * switch it on. */
+ * accumulated by the force kernels of an lj/plj/slj or SMA-TB system (on=1;
+ * FP64, or FP32 per pair with FP64 accumulation in mixed precision; SMA-TB
+ * forces are central pair forces, and the library sums the complete virial
+ * where TB.F90:548-564 omits the i-side term); the pistons switch it on. */
 int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on);
 /* smatb_set (src/TB.F90:106-170): A, xi (eV), p, q, r0, rci, rce (A).  The
  * device derives the tail polynomial coefficients. */

@@ -406,10 +406,14 @@ double lj_interact(Sys& s) {
   // bits for any thread count (an OpenMP reduction combines the threads'
   // partial sums in an unspecified order)
   std::vector<double> ea(n, 0.0);
+  // pair virial W = 1/2 sum over the full list of vd (x) f vd / r (complete;
+  // the reference's lj, Pairs.F90:254-272, omits the i-side term)
+  std::vector<double> wa(9 * (size_t)n, 0.0);
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
     int ti = s.type[i];
     double fx = 0, fy = 0, fz = 0, ep = 0;
+    double* W = &wa[9 * (size_t)i];
     for (int l = 0; l < s.nn[i]; l++) {
       int j = s.list[(size_t)l * n + i];
       const LJp& P = s.lj[ti][s.type[j]];
@@ -431,9 +435,12 @@ double lj_interact(Sys& s) {
       p = p * ev_ui;
       f = f * ev_ui;
       ep = ep + p * 0.5;
-      fx = fx - f * vd[0] / dr;
-      fy = fy - f * vd[1] / dr;
-      fz = fz - f * vd[2] / dr;
+      const double f2[3] = {f * vd[0] / dr, f * vd[1] / dr, f * vd[2] / dr};
+      fx = fx - f2[0];
+      fy = fy - f2[1];
+      fz = fz - f2[2];
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) W[3 * a + b] += 0.5 * vd[a] * f2[b];
     }
     s.force[3 * i] += fx;
     s.force[3 * i + 1] += fy;
@@ -442,6 +449,9 @@ double lj_interact(Sys& s) {
     ea[i] = ep;
   }
   for (int i = 0; i < n; i++) etot += ea[i];
+  for (int k = 0; k < 9; k++) s.virial[k] = 0.0;
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 9; k++) s.virial[k] += wa[9 * (size_t)i + k];
   return etot;
 }
 

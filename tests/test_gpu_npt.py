@@ -396,3 +396,31 @@ def test_smatb_virial_and_piston_equal_oracle(ctx):
     np.testing.assert_allclose(np.array(B1), np.array(B0), rtol=1e-12)
     assert abs(B1[-1][0] - w["L"][0]) > 1e-4
     g.destroy()
+
+
+@pytest.mark.parametrize("ff", ["smatb", "lj"])
+def test_mixed_precision_virial(ctx, ff):
+    """Mixed precision sums the pair virial in FP32 per pair and FP64 per
+    atom and system; its tensor matches the oracle's within the mixed
+    kernels' force tolerance (1e-5 of its largest component)."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=6)
+    rng = np.random.default_rng(12)
+    pos = np.mod(w["pos"] + rng.normal(0, 0.05, w["pos"].shape), w["L"])
+    s = O.System(pos, w["mass"])
+    g = gems.System(pos, w["mass"], ctx=ctx)
+    for x in (s, g):
+        x.set_box(w["L"], (True, True, True))
+        if ff == "smatb":
+            x.set_smatb(*w["smatb"])
+        else:
+            x.set_lj(0.2, 2.6, 6.0, shifted_force=True)
+    g.set_precision(1)
+    g.set_virial(True)
+    s.interact()
+    g.interact()
+    ref = s.virial_ev()
+    np.testing.assert_allclose(g.virial_ev(), ref, rtol=0, atol=1e-5 * np.abs(ref).max())
+    p = g.pressure_atm()
+    assert np.all(np.isfinite(p))
+    g.destroy()
