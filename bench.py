@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--arms", default="fp64,mixed,batched",
                     help="comma list of arms to run (profiling); the full line needs all three")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "next"],
                     help="c2 (default, the headline line) or one of the other configurations")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="c4: length of the Poisson arrival window (the full configuration is 120 s)")
@@ -655,6 +655,124 @@ def run_c4(args, gems, torch, ctx, ext):
           throughput_atom_steps_per_s=done_atoms_steps / wall)
 
 
+def run_next(args, gems, torch, ctx, ext):
+    """The rows after the hot path, measured beside their CPU restatement:
+    the G-JF constant-pressure piston on the 32k-atom Au bulk (FP64; one
+    system and a batch of 8), batched L-BFGS of 256 147-atom Au clusters, and
+    the NEB deck (30 images of a 72-atom Au slab with a Pt adatom, 20
+    iterations)."""
+    import sys
+    from gems_b200 import workloads as W
+    from oracle import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import decks
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    press_atm, pg0, pgv, pmass = 1.0, 1.0, 1.0, 1e-3
+
+    def npt_system(seed):
+        w = c2_replica(seed)
+        g = gems.System(w["pos"], w["mass"], ctx=ctx)
+        g.set_box(w["L"], (True, True, True))
+        g.set_smatb(*w["smatb"])
+        g.set_skin(w["skin"])
+        g.set_lanes(2, 1)
+        g.set_lgf(w["dt"], w["temp"], press_atm, pg0, pgv, pmass, seed=seed)
+        g.interact()
+        return g
+    out = {}
+    for name, nrep in (("npt_fp64", 1), ("npt_fp64_batch8", 8)):
+        ss = [npt_system(10 + k) for k in range(nrep)]
+        val, ms = _time_md(ctx, torch, ss, args.block, args.steps, args.warmup, ext)
+        out[name] = {"value": val, "unit": UNIT, "ms_per_block": ms, "atoms": sum(x.n for x in ss),
+                     "box_after": list(ss[0].box_now())}
+        for g in ss:
+            g.destroy()
+    w = c2_replica(10)
+    s = O.System(w["pos"], w["mass"])
+    s.set_box(w["L"], (True, True, True))
+    s.set_smatb(*w["smatb"])
+    s.set_skin(w["skin"])
+    s.set_lgf(w["dt"], w["temp"], press_atm, pg0, pgv, pmass, O.Rng(123456))
+    steps, el = _cpu_steps(s, args.cpu_seconds / 2)
+    out["npt_cpu"] = {"value": s.n * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+                      "sample": "%d G-JF steps of the 32000-atom workload" % steps}
+    # batched L-BFGS: atom-gradient evaluations per second
+    sm = W.smatb_bulk(ncell=2)["smatb"]
+    rng = np.random.default_rng(5)
+    cl = [W.cluster(147, rng, jitter=0.15) + 200.0 for _ in range(256)]
+    mass = W.smatb_bulk(ncell=2)["mass"]
+    warm = []
+    for _ in range(16):  # warm-up batch: workspace, maps and kernels loaded
+        g = gems.System(W.cluster(147, rng, jitter=0.15) + 200.0, mass, ctx=ctx)
+        g.set_smatb(*sm)
+        warm.append(g)
+    ctx.batch_lbfgs(warm)
+    for g in warm:
+        g.destroy()
+    gs = []
+    for p in cl:
+        g = gems.System(p, mass, ctx=ctx)
+        g.set_smatb(*sm)
+        gs.append(g)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    stt, its, nfs, _ = ctx.batch_lbfgs(gs)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    nfun = int(np.sum(nfs))
+    out["lbfgs_batch256"] = {"value": 147 * nfun / el, "unit": "atom-evaluations/s", "systems": 256,
+                             "evaluations": nfun, "iterations_max": int(np.max(its)), "seconds": el,
+                             "converged": int(np.sum(stt == 0))}
+    for g in gs:
+        g.destroy()
+    t0 = time.perf_counter()
+    nf = 0
+    for p in cl[:8]:
+        o = O.System(p, mass)
+        o.set_smatb(*sm)
+        st, it, nfo, em = o.lbfgs()
+        nf += nfo
+    el = time.perf_counter() - t0
+    out["lbfgs_cpu"] = {"value": 147 * nf / el, "unit": "atom-evaluations/s", "cores": cores, "kind": "port",
+                        "sample": "L-BFGS of the first 8 clusters"}
+    # NEB deck
+    d = decks.neb_deck()
+    g = gems.System(d["pos"], d["mass"], d["types"], 2, ctx=ctx)
+    decks.neb_setup(g, d)
+    imgs = decks.neb_fixed_images(g, d, lambda x: x.lbfgs())
+    g.destroy()
+    images = []
+    for k in range(d["nimg"]):
+        x = gems.System(imgs[k], d["mass"], d["types"], 2, ctx=ctx)
+        decks.neb_setup(x, d)
+        images.append(x)
+    ctx.neb(images, d["fixed"], d["k"], d["iters"])  # the deck's band (warm-up)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = 10
+    for _ in range(reps):  # the band continues from where it is
+        ctx.neb(images, d["fixed"], d["k"], d["iters"])
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    out["neb_deck"] = {"value": reps * d["nimg"] * d["iters"] / el, "unit": "image-iterations/s",
+                       "seconds": el, "repeats": reps}
+    for x in images:
+        x.destroy()
+    o = O.System(d["pos"], d["mass"], d["types"], 2)
+    decks.neb_setup(o, d)
+    oi = decks.neb_fixed_images(o, d, lambda x: x.lbfgs())
+    t0 = time.perf_counter()
+    o.neb(oi, d["fixed"], d["k"], d["iters"])
+    el = time.perf_counter() - t0
+    out["neb_cpu"] = {"value": d["nimg"] * d["iters"] / el, "unit": "image-iterations/s", "cores": cores,
+                      "kind": "port", "sample": "the whole band"}
+    _line("atom-steps/s (32000-atom Au bulk under the G-JF piston, FP64)", out["npt_fp64"]["value"], UNIT, args,
+          {"workload": "smatb_au_bulk_32000 G-JF NPT (300 K, 1 atm, gamma 1/ps, piston gamma 1/ps, mass 1e-3); "
+                       "lbfgs 256 x Au147; neb.gms", "md_steps_per_bench_step": args.block},
+          dtype="f64", rows=out, cpu_baseline=out["npt_cpu"])
+
+
 def main():
     global FIXED_TUNE
     args = parse()
@@ -682,7 +800,8 @@ def main():
         dev = torch.cuda.current_device()
         ctx = gems.Context(device=dev)
         ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
-        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args, gems, torch, ctx, ext)
+        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "next": run_next}[args.config](
+            args, gems, torch, ctx, ext)
         ctx.close()
         if world > 1:
             tdist.barrier()
