@@ -1016,6 +1016,8 @@ int cap_plain(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
   return record_steps(ctx, ss, *(int*)arg);
 }
 
+constexpr size_t MAX_BRANCHES = 16;  // branches of a batched MD graph
+
 // A batch of several systems with one launch shape is captured as
 // independent branches -- one per system, or up to 16 runs of consecutive
 // systems for larger batches: each branch's steps, conditional rebuilds and
@@ -1029,7 +1031,6 @@ int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, 
   int rc = 0;
   bool cond_ok = ctx->use_cond;
   // up to MAX_BRANCHES branches of consecutive systems
-  constexpr size_t MAX_BRANCHES = 16;
   std::vector<std::vector<int>> sets;
   bool uniform = true;
   for (int s : ss) {
@@ -1108,7 +1109,7 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
     CHK(get_map(ctx, ss, BLOCK / 32, 1, &m));
     CHK(get_map(ctx, ss, 1, 1, &m));
     CHK(sys_array(ctx, ss, &sa));
-    const size_t nbr = std::min<size_t>(ss.size(), 16);
+    const size_t nbr = std::min(ss.size(), MAX_BRANCHES);
     for (size_t j = 0; j < nbr && ss.size() > 1; j++)
       CHK(sys_array(ctx, std::vector<int>(ss.begin() + j * ss.size() / nbr, ss.begin() + (j + 1) * ss.size() / nbr),
                     &sa));
