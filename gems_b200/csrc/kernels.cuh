@@ -476,6 +476,35 @@ __device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
   atomicMax(&A.st[s].maxnn, m);
 }
 
+// Sort an atom's first n <= 64 list entries by (distance, slot) across a
+// warp: lane l holds entries l and l + 32 as 64-bit keys (the bits of the
+// non-negative float r^2 above the slot, so the integer order is the order
+// of the rank rule "closer first, then the earlier slot"), padding keys are
+// all ones.  Bitonic network (Batcher 1968) over the 64 positions
+// q = lane + 32 h; on return k0 / k1 hold the keys at positions lane and
+// lane + 32 of the sorted order.
+__device__ __forceinline__ void warp_sort64(const float* rrow, int n, int ln, unsigned long long& k0,
+                                            unsigned long long& k1) {
+  k0 = ln < n ? ((unsigned long long)__float_as_uint(rrow[ln]) << 32) | (unsigned)ln : ~0ull;
+  k1 = ln + 32 < n ? ((unsigned long long)__float_as_uint(rrow[ln + 32]) << 32) | (unsigned)(ln + 32) : ~0ull;
+  for (int size = 2; size <= 64; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride == 32) {  // partners in the same lane: positions lane and lane + 32
+        const unsigned long long lo = min(k0, k1), hi = max(k0, k1);
+        k0 = lo;  // size 64 sorts the whole sequence ascending
+        k1 = hi;
+        continue;
+      }
+      const unsigned long long p0 = __shfl_xor_sync(0xffffffffu, k0, stride);
+      const unsigned long long p1 = __shfl_xor_sync(0xffffffffu, k1, stride);
+      const bool lower = (ln & stride) == 0;
+      const bool up0 = (ln & size) == 0, up1 = ((ln + 32) & size) == 0;
+      k0 = (lower == up0) ? min(k0, p0) : max(k0, p0);
+      k1 = (lower == up1) ? min(k1, p1) : max(k1, p1);
+    }
+  }
+}
+
 // flist holds an atom's entries sorted by their distance at the build, and
 // no pair has come closer since by more than the skin test's bound D
 // (SysState::dmax).  So the entries built at r >= rcut + 1e-4 + k skin/7
@@ -636,16 +665,25 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
         __syncwarp();
         if (act) {
           const int n = min(m, A.lcap);
-          for (int e = ln; e < n; e += 32) {
-            A.list[(size_t)e * A.cap + i] = row[e];
-            // force order: rank by distance, ties by slot
-            const float re = rrow[e];
-            int rank = 0;
-            for (int f = 0; f < n; f++) {
-              const float rf = rrow[f];
-              rank += (rf < re) || (rf == re && f < e);
+          if (n <= 64) {
+            // force order by a warp bitonic sort of (distance, slot) keys
+            for (int e = ln; e < n; e += 32) A.list[(size_t)e * A.cap + i] = row[e];
+            unsigned long long k0, k1;
+            warp_sort64(rrow, n, ln, k0, k1);
+            if (ln < n) A.flist[(size_t)ln * A.cap + i] = row[(int)(k0 & 0xffffffffu)];
+            if (ln + 32 < n) A.flist[(size_t)(ln + 32) * A.cap + i] = row[(int)(k1 & 0xffffffffu)];
+          } else {
+            for (int e = ln; e < n; e += 32) {
+              A.list[(size_t)e * A.cap + i] = row[e];
+              // force order: rank by distance, ties by slot
+              const float re = rrow[e];
+              int rank = 0;
+              for (int f = 0; f < n; f++) {
+                const float rf = rrow[f];
+                rank += (rf < re) || (rf == re && f < e);
+              }
+              A.flist[(size_t)rank * A.cap + i] = row[e];
             }
-            A.flist[(size_t)rank * A.cap + i] = row[e];
           }
           list_counts(A, S, i, n, rrow, ln);
           if (ln == 0) list_done(A, s, i, m);
