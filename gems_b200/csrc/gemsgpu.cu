@@ -95,6 +95,7 @@ struct gemsgpu_ctx {
   uint64_t epoch = 1;  // bumps when device pointers or maps change
   int64_t launches = 0;  // kernels issued (graph replays add their node count)
   bool use_cond = true;  // conditional graph nodes guard the rebuild chain
+  bool fuse_forces = true;  // force pass + half steps in one kernel (GEMSGPU_NO_FUSED_FORCES=1: off)
   int64_t body_nodes = 0;  // kernels in one captured rebuild chain
   unsigned long long body_seen = 0;  // body_runs already accounted
   int64_t pending = 0;   // kernels recorded by the capture in progress
@@ -818,6 +819,68 @@ bool can_fuse_steps(const gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   return true;
 }
 
+// the force pass and the next half steps run as one kernel
+// (k_smatb_force_*_ba) when every system is a velocity-Verlet or Ermak SMA-TB
+// system without the virial, in FP64 or in mixed precision with the species
+// constants in registers
+bool can_fuse_forces(const gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  if (!ctx->fuse_forces || !can_fuse_steps(ctx, ss)) return false;
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    if (h.d.ff != FF_SMATB || h.d.virial || h.d.half) return false;
+    if (h.d.prec == PREC_MIXED && (h.ntypes != 1 || (h.variant & 1))) return false;
+  }
+  return true;
+}
+
+template <int K, int MINB>
+void force_mixed_ba(gemsgpu_ctx* ctx, const BlockMap& m, cudaGraphConditionalHandle cond, bool use_cond) {
+  if (use_cond) k_smatb_force_mixed_ba<K, true, MINB, true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, cond);
+  else k_smatb_force_mixed_ba<K, true, MINB, false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, cond);
+}
+
+template <int K>
+void force_ba_k(gemsgpu_ctx* ctx, int prec, int variant, const BlockMap& m, cudaGraphConditionalHandle cond,
+                bool use_cond) {
+  if (prec == PREC_MIXED) {
+    if ((variant & 2) && (variant & 4)) force_mixed_ba<K, 3>(ctx, m, cond, use_cond);
+    else if (variant & 2) force_mixed_ba<K, 4>(ctx, m, cond, use_cond);
+    else force_mixed_ba<K, 1>(ctx, m, cond, use_cond);
+  } else if (use_cond) {
+    k_smatb_force_fp64_ba<K, true><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, cond);
+  } else {
+    k_smatb_force_fp64_ba<K, false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, cond);
+  }
+  ++ctx->launches;
+}
+
+// the density pass, then the force pass fused with step_b of this step and
+// step_a of the next (which raises `cond` when a list must be rebuilt)
+int launch_forces_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss, cudaGraphConditionalHandle cond = 0,
+                     int use_cond = 0) {
+  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+  for (int s : ss) {
+    const SysHost& h = ctx->sys[s];
+    groups[{h.d.prec, h.lanes, h.variant}].push_back(s);
+  }
+  for (auto& kv : groups) {
+    const int prec = std::get<0>(kv.first), K = std::get<1>(kv.first), variant = std::get<2>(kv.first);
+    BlockMap m;
+    CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
+    smatb_pass(ctx, 0, prec, variant, true, K, m);
+    switch (K) {
+      case 1: force_ba_k<1>(ctx, prec, variant, m, cond, use_cond != 0); break;
+      case 2: force_ba_k<2>(ctx, prec, variant, m, cond, use_cond != 0); break;
+      case 4: force_ba_k<4>(ctx, prec, variant, m, cond, use_cond != 0); break;
+      case 8: force_ba_k<8>(ctx, prec, variant, m, cond, use_cond != 0); break;
+      case 16: force_ba_k<16>(ctx, prec, variant, m, cond, use_cond != 0); break;
+      default: force_ba_k<32>(ctx, prec, variant, m, cond, use_cond != 0); break;
+    }
+  }
+  CU(cudaGetLastError());
+  return 0;
+}
+
 int launch_step_b(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
@@ -950,6 +1013,21 @@ int reduce_sys(gemsgpu_ctx* ctx, const std::vector<int>& ss, std::vector<double>
 // n plain steps; with fusion, step k > 0 opens with step_b(k-1)+step_a(k)
 // and only the last step closes with its own step_b
 int record_steps(gemsgpu_ctx* ctx, const std::vector<int>& ss, int n) {
+  if (ss.size() == 1 && can_fuse_forces(ctx, ss)) {
+    // step_a, then per step: rebuild chain, density pass, force pass with
+    // step_b + the next step_a; the last step closes with its own step_b
+    CHK(launch_step_a(ctx, ss));
+    for (int k = 0; k < n; k++) {
+      CHK(launch_rebuild(ctx, ss));
+      if (k < n - 1) {
+        CHK(launch_forces_ba(ctx, ss));
+      } else {
+        CHK(launch_forces(ctx, ss));
+        CHK(launch_step_b(ctx, ss));
+      }
+    }
+    return 0;
+  }
   const bool fuse = can_fuse_steps(ctx, ss);
   for (int k = 0; k < n; k++) {
     if (k == 0 || !fuse) CHK(launch_step_a(ctx, ss));
@@ -1012,6 +1090,9 @@ int cap_forces_b(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
 int cap_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss, void*) {
   return launch_forces(ctx, ss);
 }
+int cap_forces_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
+  return launch_forces_ba(ctx, ss, ((CondArg*)arg)->h, 1);
+}
 int cap_plain(gemsgpu_ctx* ctx, const std::vector<int>& ss, void* arg) {
   return record_steps(ctx, ss, *(int*)arg);
 }
@@ -1045,8 +1126,62 @@ int build_chunk_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, 
   std::vector<std::vector<cudaGraphNode_t>> deps(sets.size());
   if (sets.size() > 1) ctx->view_set = ss;
   ctx->bodies = 0;
+  // the force pass fused with the half steps: [step_a] IF [rho, force+ba] IF ... [rho, force, step_b]
+  std::vector<CondArg> next(sets.size());
+  std::vector<char> fused(sets.size(), 0);
+  // (single systems only: in a batch, whose branches already overlap, the
+  // longer fused blocks measured 3 % slower; alone, fusion saves a launch
+  // and its tail per step, +7 % mixed, +4 % FP64)
+  for (size_t j = 0; j < sets.size(); j++) fused[j] = ss.size() == 1 && can_fuse_forces(ctx, sets[j]);
+  auto add_if = [&](size_t j, const CondArg& ca) -> int {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = ca.h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    if (cudaGraphAddNode(&cn, g, deps[j].data(), deps[j].size(), &cp) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> none;
+    int r = capture_into(ctx, cp.conditional.phGraph_out[0], none, cap_rebuild, sets[j], nullptr);
+    deps[j].assign(1, cn);
+    return r;
+  };
   for (int k = 0; k < nsteps && rc == 0 && cond_ok; k++) {
     for (size_t j = 0; j < sets.size() && rc == 0 && cond_ok; j++) {
+      if (!fused[j]) continue;
+      const std::vector<int>& sj = sets[j];
+      if (k == 0) {
+        CondArg ca{};
+        if (cudaGraphConditionalHandleCreate(&ca.h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+          cond_ok = false;
+          break;
+        }
+        if ((rc = capture_into(ctx, g, deps[j], cap_step_a, sj, &ca))) break;
+        if ((rc = add_if(j, ca)) < 0) {
+          cond_ok = false;
+          rc = 0;
+          break;
+        }
+        if (rc) break;
+      }
+      if (k < nsteps - 1) {
+        CondArg ca{};
+        if (cudaGraphConditionalHandleCreate(&ca.h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+          cond_ok = false;
+          break;
+        }
+        if ((rc = capture_into(ctx, g, deps[j], cap_forces_ba, sj, &ca))) break;
+        if ((rc = add_if(j, ca)) < 0) {
+          cond_ok = false;
+          rc = 0;
+          break;
+        }
+      } else {
+        rc = capture_into(ctx, g, deps[j], cap_forces_b, sj, nullptr);
+      }
+    }
+    for (size_t j = 0; j < sets.size() && rc == 0 && cond_ok; j++) {
+      if (fused[j]) continue;
       const std::vector<int>& sj = sets[j];
       const bool fuse = can_fuse_steps(ctx, sj);
       CondArg ca{};
@@ -1593,6 +1728,7 @@ int gemsgpu_create(int device, int64_t max_atoms, int max_systems, gemsgpu_ctx**
   // profilers cannot replay kernels of graphs with conditional nodes:
   // GEMSGPU_NO_COND=1 captures plain steps (rebuild kernels exit early)
   if (const char* e = getenv("GEMSGPU_NO_COND")) ctx->use_cond = !(e[0] == '1');
+  if (const char* e = getenv("GEMSGPU_NO_FUSED_FORCES")) ctx->fuse_forces = !(e[0] == '1');
   int rc = 0;
   do {
     if (cudaSetDevice(device) != cudaSuccess) { rc = GEMSGPU_ERR_CUDA; break; }

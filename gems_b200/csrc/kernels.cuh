@@ -927,19 +927,14 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
 //                       - xi^2/2 e^{-2q(r/r0-1)} (2q/r0)(eb_i + eb_j)
 //   tail     : factor = P P' (eb_i + eb_j) - 2 R'
 //   F_i -= factor * ev_ui * vd / r ;  e_i += repul ; e_i -= sqrt(rho_i)
+// The FP64 force pass for one thread's lane of atom i; lane 0 stores the
+// force and energy and returns the force in F.
 // VIR: also the pair virial of the system (virial_close); SMA-TB forces are
 // central pair forces, F_i = -sum_j factor_ij vd / r, so W is the pair sum
 // (complete: the reference's TB.F90:548-564 omits the i-side term).
 template <int K, bool VIR>
-__global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M) {
-  int s = blk_sys(M);
-  if (s < 0) return;  // padding block of a fixed-capacity map
-  const SysDev& S = A.sys[s];
-  __shared__ SmFP64 tab_sh[MAXT * MAXT];
-  const SmFP64* tab = sm_table(A, S, tab_sh);
-  int i = M.first[blockIdx.x] + threadIdx.x / K;
-  int lane = threadIdx.x % K;
-  bool act = i < M.end[blockIdx.x];
+__device__ __forceinline__ void force_fp64_body(Arena& A, const BlockMap& M, int s, const SysDev& S,
+                                                const SmFP64* tab, int i, int lane, bool act, double4& F) {
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
   double w[6] = {0, 0, 0, 0, 0, 0};
   if (act) {
@@ -990,10 +985,23 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M)
   f2 = lane_sum<K>(f2);
   ep = lane_sum<K>(ep);
   if (act && lane == 0) {
-    A.force[i] = make_double4(f0, f1, f2, 0.0);
+    F = make_double4(f0, f1, f2, 0.0);
+    A.force[i] = F;
     A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
   }
   if constexpr (VIR) virial_close(A, M, s, w);
+}
+
+template <int K, bool VIR>
+__global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  const SysDev& S = A.sys[s];
+  __shared__ SmFP64 tab_sh[MAXT * MAXT];
+  const SmFP64* tab = sm_table(A, S, tab_sh);
+  const int i = M.first[blockIdx.x] + threadIdx.x / K;
+  double4 F;
+  force_fp64_body<K, VIR>(A, M, s, S, tab, i, threadIdx.x % K, i < M.end[blockIdx.x], F);
 }
 
 // ---- mixed precision: FP32 pair math, FP64 accumulation.
@@ -1128,17 +1136,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
   }
 }
 
+// The force pass for one thread's lane of atom i (K lanes per atom); lane 0
+// stores the force and energy and returns the force in F.
 // VIR: also the pair virial, FP32 per pair and group, FP64 per atom and system.
-template <int K, bool ONE, int MINB, bool VIR = false>
-__global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, BlockMap M) {
-  int s = blk_sys(M);
-  if (s < 0) return;  // padding block of a fixed-capacity map
-  const SysDev& S = A.sys[s];
-  __shared__ SmF32 tab_sh[ONE ? 1 : MAXT * MAXT];
-  const SmF32* tab = smf_table<ONE>(A, S, tab_sh);
-  int i = M.first[blockIdx.x] + threadIdx.x / K;
-  int lane = threadIdx.x % K;
-  bool act = i < M.end[blockIdx.x];
+template <int K, bool ONE, bool VIR>
+__device__ __forceinline__ void force_mixed_body(Arena& A, const BlockMap& M, int s, const SysDev& S,
+                                                 const SmF32* tab, int i, int lane, bool act, double4& F) {
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
   double w[6] = {0, 0, 0, 0, 0, 0};
   if (act) {
@@ -1220,10 +1223,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
   f2 = lane_sum<K>(f2);
   ep = lane_sum<K>(ep);
   if (act && lane == 0) {
-    A.force[i] = make_double4(f0, f1, f2, 0.0);
+    F = make_double4(f0, f1, f2, 0.0);
+    A.force[i] = F;
     A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
   }
   if constexpr (VIR) virial_close(A, M, s, w);
+}
+
+template <int K, bool ONE, int MINB, bool VIR = false>
+__global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  const SysDev& S = A.sys[s];
+  __shared__ SmF32 tab_sh[ONE ? 1 : MAXT * MAXT];
+  const SmF32* tab = smf_table<ONE>(A, S, tab_sh);
+  const int i = M.first[blockIdx.x] + threadIdx.x / K;
+  double4 F;
+  force_mixed_body<K, ONE, VIR>(A, M, s, S, tab, i, threadIdx.x % K, i < M.end[blockIdx.x], F);
 }
 
 // ------------------------------------------------------------------ LJ
@@ -2067,6 +2083,34 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
   skin_close<COND>(A, M, s, S, st, frozen, t, cond);
 }
 
+// Atom i's step_b of one step and step_a of the next (velocity Verlet or
+// Ermak; other integrators leave the atom alone) given its force F: the
+// operations of k_step_b and k_step_a in their order.  Returns the squared
+// displacement since the list build (1e-16 when the atom did not move).
+__device__ __forceinline__ double ba_atom(Arena& A, const SysDev& S, SysState& st, int i, const double4& F) {
+  const int integ = S.integ;
+  if (integ != IT_VV && integ != IT_ERMAK) return 1.e-16;
+  // every input is loaded before the first store, so all loads are in flight together
+  double4 x = A.pos[i], v = A.vel[i], a = A.acel[i];
+  const double2 mi = A.minv[i];
+  const double4 xo = A.pos_old[i];
+  const int ty = A.type[i];
+  const double4 vv0 = integ == IT_ERMAK ? A.vel_v[i] : make_double4(0, 0, 0, 0);
+  if (integ == IT_VV) {
+    vv_b_atom(S.dt, mi.x, F, v, a);
+    vv_a_atom(S.dt, mi.x, F, x, v, a);
+  } else {
+    ermak_b_atom(S, mi.x, F, vv0, v, a);
+    double4 vv;
+    ermak_a_atom(A, S, st, i, mi, v, a, x, vv);
+    A.vel_v[i] = vv;
+  }
+  A.acel[i] = a;
+  A.vel[i] = v;
+  wrap_atom(S, x);
+  return moved_atom(A, S, st, i, x, xo, ty);
+}
+
 // step_b of one step fused with step_a of the next, for velocity Verlet and
 // Ermak systems (FIRE needs its system-wide P between the two and keeps the
 // split kernels).  Per atom it is exactly k_step_b followed by k_step_a:
@@ -2081,29 +2125,51 @@ __global__ void __launch_bounds__(BLOCK, 4) k_step_ba(Arena A, BlockMap M, cudaG
   int i = M.first[blockIdx.x] + threadIdx.x;
   bool act = i < M.end[blockIdx.x];
   double2 t = make_double2(1.e-16, 1.e-16);
-  const int integ = S.integ;
-  if (act && (integ == IT_VV || integ == IT_ERMAK)) {
-    // every input is loaded before the first store, so all loads are in flight together
-    double4 x = A.pos[i], v = A.vel[i], a = A.acel[i];
-    const double4 F = A.force[i];
-    const double2 mi = A.minv[i];
-    const double4 xo = A.pos_old[i];
-    const int ty = A.type[i];
-    const double4 vv0 = integ == IT_ERMAK ? A.vel_v[i] : make_double4(0, 0, 0, 0);
-    if (integ == IT_VV) {
-      vv_b_atom(S.dt, mi.x, F, v, a);
-      vv_a_atom(S.dt, mi.x, F, x, v, a);
-    } else {
-      ermak_b_atom(S, mi.x, F, vv0, v, a);
-      double4 vv;
-      ermak_a_atom(A, S, st, i, mi, v, a, x, vv);
-      A.vel_v[i] = vv;
-    }
-    A.acel[i] = a;
-    A.vel[i] = v;
-    wrap_atom(S, x);
-    t.x = moved_atom(A, S, st, i, x, xo, ty);
-  }
+  if (act) t.x = ba_atom(A, S, st, i, A.force[i]);
+  skin_close<COND, false>(A, M, s, S, st, false, t, cond);
+}
+
+// The force pass fused with the integrator: each atom's force, then its
+// step_b and the next step's step_a (ba_atom), then the skin test of the
+// system.  The force pass reads the neighbours' positions from the density
+// pass's gather records (fxe, pose), never from pos / fxp, so moving an atom
+// while others still gather is safe; the next density pass starts after
+// this launch.  Velocity Verlet and Ermak systems; the sums and the step are
+// those of the separate kernels, bit for bit.
+template <int K, bool ONE, int MINB, bool COND>
+__global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed_ba(Arena A, BlockMap M,
+                                                                       cudaGraphConditionalHandle cond) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  const SysDev& S = A.sys[s];
+  SysState& st = A.st[s];
+  __shared__ SmF32 tab_sh[ONE ? 1 : MAXT * MAXT];
+  const SmF32* tab = smf_table<ONE>(A, S, tab_sh);
+  const int i = M.first[blockIdx.x] + threadIdx.x / K;
+  const int lane = threadIdx.x % K;
+  const bool act = i < M.end[blockIdx.x];
+  double4 F;
+  force_mixed_body<K, ONE, false>(A, M, s, S, tab, i, lane, act, F);
+  double2 t = make_double2(1.e-16, 1.e-16);
+  if (act && lane == 0) t.x = ba_atom(A, S, st, i, F);
+  skin_close<COND, false>(A, M, s, S, st, false, t, cond);
+}
+
+template <int K, bool COND>
+__global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64_ba(Arena A, BlockMap M, cudaGraphConditionalHandle cond) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  const SysDev& S = A.sys[s];
+  SysState& st = A.st[s];
+  __shared__ SmFP64 tab_sh[MAXT * MAXT];
+  const SmFP64* tab = sm_table(A, S, tab_sh);
+  const int i = M.first[blockIdx.x] + threadIdx.x / K;
+  const int lane = threadIdx.x % K;
+  const bool act = i < M.end[blockIdx.x];
+  double4 F;
+  force_fp64_body<K, false>(A, M, s, S, tab, i, lane, act, F);
+  double2 t = make_double2(1.e-16, 1.e-16);
+  if (act && lane == 0) t.x = ba_atom(A, S, st, i, F);
   skin_close<COND, false>(A, M, s, S, st, false, t, cond);
 }
 
