@@ -1,7 +1,7 @@
 // gems_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
 //
 // CPU FP64 restatement of the GEMS force/neighbour hot path (alexispaz/GEMS,
-// Fortran 2003).  It is the checker for the CUDA path and the timed CPU
+// Fortran 2003).  The tests compare the CUDA path against it; it is the timed CPU
 // baseline ("port"): only tests/, __graft_entry__.smoke() and bench.py's
 // cpu_baseline / reference legs may load it.  The product library
 // (gems_b200/libgemsgpu.so) never links or calls it.

@@ -1,7 +1,7 @@
 """ctypes wrapper of the FP64 oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: a CPU restatement of the GEMS force/neighbour hot
-path used as the checker of the CUDA path and as the timed CPU baseline.  Only
+path that the tests compare the CUDA path against, and the timed CPU baseline.  Only
 tests/, __graft_entry__.smoke() and bench.py's CPU legs import this module;
 the product library never does.
 
