@@ -68,11 +68,12 @@ def xyz_deck():
 
 
 # --------------------------------------------------------------- LJ dimer
-def lj_dimer_deck():
-    """examples/LJ/lj.gms: dimer scan (251 states) then 1000 VV steps."""
+def lj_dimer_deck(kind="lj"):
+    """examples/LJ/lj.gms (mass 3) and slj.gms (H atoms, the slj form with
+    rs 1.108683): dimer scan (251 states) then 1000 VV steps."""
     g = golden()
     tau_ps = 0.01018
-    return dict(
+    d = dict(
         pos0=np.array([[1.0, 1.0, 1.0], [2.2, 1.0, 1.0]]),
         mass=3.0,
         box=(5.78, 5.78, 5.78),
@@ -80,6 +81,9 @@ def lj_dimer_deck():
         dt=0.002 * tau_ps,
         ref=np.array(g["lj_energy"]),
     )
+    if kind == "slj":
+        d.update(mass=MASS["H"], lj=None, slj=(1.0, 0.890898718140339, 1.108683), ref=np.array(g["slj_energy"]))
+    return d
 
 
 # --------------------------------------------------------------- SMA-TB bulk
@@ -329,13 +333,16 @@ def plj_params():
     }
 
 
-def lj_dimer_rows(sys_factory, ui_ev):
-    """Run the lj.gms deck on an engine; returns (rows, golden rows)."""
-    d = lj_dimer_deck()
+def lj_dimer_rows(sys_factory, ui_ev, kind="lj"):
+    """Run the lj.gms or slj.gms deck on an engine; returns (rows, golden rows)."""
+    d = lj_dimer_deck(kind)
     pos = d["pos0"].copy()
     s = sys_factory(pos, d["mass"])
     s.set_box(d["box"], (False, False, False))
-    s.set_lj(*d["lj"])
+    if d["lj"] is not None:
+        s.set_lj(*d["lj"])
+    else:
+        s.set_slj(*d["slj"])
     rows = []
 
     def state():

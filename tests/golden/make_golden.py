@@ -45,6 +45,7 @@ def main():
         "xyz_frames": xyz_frames("examples/XYZ/Pos.md.xyz"),
         "xyz_energy": rows("examples/XYZ/ref/Energy.readxyz.dat"),
         "lj_energy": rows("examples/LJ/ref/Energy.lj.dat"),
+        "slj_energy": rows("examples/LJ/ref/Energy.slj.dat"),
         "smatb_md_coords": xyz_frames("examples/SMA-TB/coords.xyz")[0],
         "smatb_md_energy": rows("examples/SMA-TB/ref/Energy.md.dat"),
         "smatb_bulk_energy": rows("examples/SMA-TB/ref/Energy.bulk.dat"),

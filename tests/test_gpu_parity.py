@@ -271,8 +271,10 @@ def test_gpu_xyz_frames(ctx):
     np.testing.assert_allclose(out, d["ref"], rtol=2e-7)
 
 
-def test_gpu_lj_dimer(ctx):
-    got, ref = decks.lj_dimer_rows(lambda p, m: gpu_ref_sys(p, m, ctx=ctx), gems.UI_EV)
+@pytest.mark.parametrize("kind", ["lj", "slj"])
+def test_gpu_lj_dimer(ctx, kind):
+    """lj.gms and slj.gms on the GPU (FP64)."""
+    got, ref = decks.lj_dimer_rows(lambda p, m: gpu_ref_sys(p, m, ctx=ctx), gems.UI_EV, kind)
     assert decks.gems_rule(ref[:, 0], got[:, 0]) < 1e-6
     np.testing.assert_allclose(got, ref, atol=2e-7, rtol=1e-6)
 

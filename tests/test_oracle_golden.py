@@ -54,9 +54,11 @@ def test_xyz_frames_lj_pbc():
     np.testing.assert_allclose(out, d["ref"], rtol=2e-7)
 
 
-def test_lj_dimer_scan_and_vv():
-    """examples/LJ/lj.gms: 251 dimer states + 1000 velocity-Verlet steps."""
-    got, ref = decks.lj_dimer_rows(O.System, 1.0 / O.lib().orc_ev_ui())
+@pytest.mark.parametrize("kind", ["lj", "slj"])
+def test_lj_dimer_scan_and_vv(kind):
+    """examples/LJ/lj.gms and slj.gms: 251 dimer states + 1000
+    velocity-Verlet steps."""
+    got, ref = decks.lj_dimer_rows(O.System, 1.0 / O.lib().orc_ev_ui(), kind)
     assert got.shape == ref.shape
     assert decks.gems_rule(ref[:, 0], got[:, 0]) < 1e-6
     np.testing.assert_allclose(got, ref, atol=1e-7, rtol=1e-6)
