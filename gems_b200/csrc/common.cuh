@@ -33,7 +33,7 @@ __device__ __forceinline__ void stencil(int k, int& dx, int& dy, int& dz) {
 }
 
 enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
-enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6 };
+enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6, IT_NORD = 7 };
 // IT_AXES: one integrator per coordinate -- a G-JF piston on that box length
 // (AX_FLEX) or Ermak dynamics of that coordinate (AX_ERMAK)
 enum AX : int { AX_NONE = 0, AX_FLEX = 1, AX_ERMAK = 2 };
@@ -173,6 +173,9 @@ struct Arena {
   double4* acel;
   double4* force;
   double4* vel_v;       // Ermak random velocity kick (ermak_a -> ermak_b)
+  double4* acel2;       // Nordsieck scaled derivatives (Atoms.F90:77-79); allocated
+  double4* acel3;       //   when a system first integrates with the predictor-corrector
+  double4* acel4;
   double* epot;         // per atom (internal units)
   double* band;         // SMA-TB density rho_i
   double* eband;        // 1/sqrt(rho_i)

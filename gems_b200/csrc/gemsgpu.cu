@@ -67,6 +67,20 @@ bool moving_box(const SysDev& d) {
   return d.ax_mode[0] == AX_FLEX || d.ax_mode[1] == AX_FLEX || d.ax_mode[2] == AX_FLEX;
 }
 
+// a pair of types that acts on one side only (`interact g1 feels g2`): its
+// forces are not a pair virial
+bool one_sided(const SysHost& h) {
+  auto on = [&](int a, int b) {
+    const PairP& P = h.prm[a * h.ntypes + b];
+    return P.v[0] != 0.0 || P.v[1] != 0.0;
+  };
+  if (h.d.ff != FF_LJ) return false;
+  for (int a = 0; a < h.ntypes; a++)
+    for (int b = 0; b < h.ntypes; b++)
+      if (on(a, b) != on(b, a)) return true;
+  return false;
+}
+
 struct Graph {
   cudaGraphExec_t exec = nullptr;
   uint64_t epoch = 0;
@@ -115,7 +129,8 @@ struct gemsgpu_ctx {
   double* stage = nullptr;      // 3 doubles per atom, host <-> device staging
   int64_t stage_cap = 0;
   int64_t snap_cap = 0;
-  double4* snap = nullptr;      // pos, vel, acel, force
+  double4* snap = nullptr;      // pos, vel, acel, force [, acel2, acel3, acel4]
+  int snap_arrays = 0;
   SysState* snap_st = nullptr;
   SysDev* snap_sys = nullptr;   // boxes moved by constant-pressure steps
 };
@@ -251,6 +266,11 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   CHK(dgrow(ctx, &A.acel, keep, nc));
   CHK(dgrow(ctx, &A.force, keep, nc));
   CHK(dgrow(ctx, &A.vel_v, keep, nc));
+  if (A.acel2) {
+    CHK(dgrow(ctx, &A.acel2, keep, nc));
+    CHK(dgrow(ctx, &A.acel3, keep, nc));
+    CHK(dgrow(ctx, &A.acel4, keep, nc));
+  }
   CHK(dgrow(ctx, &A.epot, keep, nc));
   CHK(dgrow(ctx, &A.band, keep, nc));
   CHK(dgrow(ctx, &A.eband, keep, nc));
@@ -884,7 +904,11 @@ int launch_forces_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss, cudaGraphCond
 int launch_step_b(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
-  k_step_b<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
+  bool nord = false;
+  for (int s : ss) nord |= ctx->sys[s].d.integ == IT_NORD;
+  if (nord) k_step_b<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+  else k_step_b<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+  ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
 }
@@ -1306,14 +1330,18 @@ int launch_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps) {
 
 int snapshot(gemsgpu_ctx* ctx, bool restore) {
   int64_t n = ctx->acap;
-  if (!restore && ctx->snap_cap < n) {
-    if (ctx->snap) cudaFree(ctx->snap);
-    CHK(dalloc(ctx, &ctx->snap, 4 * (size_t)n));
-    ctx->snap_cap = n;
-  }
   Arena& A = ctx->A;
-  double4* arr[4] = {A.pos, A.vel, A.acel, A.force};
-  for (int k = 0; k < 4; k++) {
+  // the Nordsieck derivatives, once a system has them
+  int na = A.acel2 ? 7 : 4;
+  if (restore) na = std::min(na, ctx->snap_arrays);
+  if (!restore && (ctx->snap_cap < n || ctx->snap_arrays < na)) {
+    if (ctx->snap) cudaFree(ctx->snap);
+    CHK(dalloc(ctx, &ctx->snap, na * (size_t)n));
+    ctx->snap_cap = n;
+    ctx->snap_arrays = na;
+  }
+  double4* arr[7] = {A.pos, A.vel, A.acel, A.force, A.acel2, A.acel3, A.acel4};
+  for (int k = 0; k < na; k++) {
     if (restore)
       CU(cudaMemcpyAsync(arr[k], ctx->snap + k * n, n * sizeof(double4), cudaMemcpyDeviceToDevice,
                          ctx->stream));
@@ -1553,7 +1581,7 @@ int pool_forces(gemsgpu_pool* P) {
 int pool_step_b(gemsgpu_pool* P) {
   gemsgpu_ctx* ctx = P->ctx;
   const BlockMap& m = P->maps[0];
-  k_step_b<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+  k_step_b<false><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
 }
@@ -1765,7 +1793,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   drop_graphs(ctx);
   drop_maps(ctx);
   Arena& A = ctx->A;
-  void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.epot, A.band, A.eband,
+  void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.acel2, A.acel3, A.acel4, A.epot, A.band, A.eband,
                   A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.ncut, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
@@ -1864,6 +1892,8 @@ int gemsgpu_upload(gemsgpu_ctx* ctx, int sys, const double* pos, const double* v
   CU(cudaMemcpyAsync(A.acel + h.off, z.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
   CU(cudaMemcpyAsync(A.force + h.off, z.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
   CU(cudaMemcpyAsync(A.vel_v + h.off, z.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+  for (double4* d : {A.acel2, A.acel3, A.acel4})
+    if (d) CU(cudaMemcpyAsync(d + h.off, z.data(), n * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
   std::vector<double2> mi(n);
   std::vector<int> t(n, 0);
   for (int i = 0; i < n; i++) {
@@ -2010,7 +2040,7 @@ int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec) {
     return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: the pistons are FP64 only");
   if (prec != GEMSGPU_PREC_FP64 && ctx->sys[sys].d.ff == FF_LJ)
     for (const PairP& P : ctx->sys[sys].prm)
-      if (P.v[8] != 0.0) return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: slj pairs are FP64 only");
+      if (P.v[8] != 0.0) return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: slj and sm1 pairs are FP64 only");
   ctx->sys[sys].d.prec = prec;
   CHK(push_sys(ctx, sys));
   BlockMap m;
@@ -2204,6 +2234,33 @@ int gemsgpu_set_vv(gemsgpu_ctx* ctx, int sys, double dt) {
   return 0;
 }
 
+// the Nordsieck derivative arrays, zero, on first use
+static int ensure_nord(gemsgpu_ctx* ctx) {
+  Arena& A = ctx->A;
+  if (A.acel2) return 0;
+  for (double4** d : {&A.acel2, &A.acel3, &A.acel4}) {
+    CHK(dalloc(ctx, d, (size_t)ctx->acap));
+    CU(cudaMemsetAsync(*d, 0, (size_t)ctx->acap * sizeof(double4), ctx->stream));
+  }
+  return 0;
+}
+
+// `evolve pred_corr_5` (src/Integration.F90:143-145): nordsieck_predictor
+// as step a, nordsieck_corrector as step b.  The derivatives acel..acel4
+// carry over as the reference's atoms keep them (zero for new atoms, or
+// from a .chp file).
+int gemsgpu_set_pred_corr(gemsgpu_ctx* ctx, int sys, double dt) {
+  CHK(check_sys(ctx, sys));
+  if (!(dt > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "dt must be > 0");
+  CHK(ensure_nord(ctx));
+  SysHost& h = ctx->sys[sys];
+  h.d.integ = IT_NORD;
+  h.d.dt = dt;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
 int gemsgpu_set_ermak(gemsgpu_ctx* ctx, int sys, double dt, double gama, double temp, uint64_t seed) {
   CHK(check_sys(ctx, sys));
   if (!(dt > 0.0) || !(gama > 0.0) || !(temp >= 0.0))
@@ -2304,11 +2361,68 @@ int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, doubl
   return 0;
 }
 
+// wca_set (src/Pairs.F90:495-506): LJ cut at 2**(1./6.) sigma, the
+// exponent a single-precision literal, shifted up by eps (wca_interact,
+// Pairs.F90:508-589)
+int gemsgpu_set_wca(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, double sigma) {
+  if (!(sigma > 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "set_wca: sigma must be positive");
+  return gemsgpu_set_lj(ctx, sys, ti, tj, eps, sigma, std::pow(2.0, (double)(1.0f / 6.0f)) * sigma, 0, -eps);
+}
+
+// sm1_set (src/Pairs.F90:916-923): a smooth step of depth eps (eV) from r1
+// to r2 = the cut-off (sm1_interact, Pairs.F90:925-1011)
+int gemsgpu_set_sm1(gemsgpu_ctx* ctx, int sys, int ti, int tj, double r1, double r2, double eps) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (ti < 0 || tj < 0 || ti >= h.ntypes || tj >= h.ntypes || !(r1 > 0.0) || !(r2 > r1))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_sm1: bad type pair or radii");
+  if (h.d.ff != FF_NONE && h.d.ff != FF_LJ)
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_sm1: system already has another force field");
+  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_sm1: FP64 systems only");
+  h.d.ff = FF_LJ;
+  PairP P{};
+  P.v[0] = eps;
+  P.v[1] = r1;
+  P.v[2] = r2;
+  P.v[3] = r2 * r2;
+  P.v[8] = 2.0;
+  P.v[11] = r1;
+  h.prm[ti * h.ntypes + tj] = P;
+  h.prm[tj * h.ntypes + ti] = P;
+  h.ff_set = true;
+  h.first = true;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
+// `interact g1 feels g2` (src/Interaction.f90:69-76, 128-131): half and
+// newton off, so only the atoms of g1 feel the pair; with one type per
+// group, the pair (ti, tj) keeps acting on type ti and stops acting on tj
+int gemsgpu_set_feels(gemsgpu_ctx* ctx, int sys, int ti, int tj) {
+  CHK(check_sys(ctx, sys));
+  SysHost& h = ctx->sys[sys];
+  if (ti < 0 || tj < 0 || ti >= h.ntypes || tj >= h.ntypes)
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_feels: bad type pair");
+  if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "set_feels: pair potentials only");
+  if (h.d.virial) return fail(ctx, GEMSGPU_ERR_STATE, "set_feels: one-sided pairs have no pair virial");
+  if (ti == tj) return 0;
+  h.prm[tj * h.ntypes + ti] = PairP{};
+  h.has_forces = false;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  drop_maps(ctx);
+  return 0;
+}
+
 int gemsgpu_set_virial(gemsgpu_ctx* ctx, int sys, int on) {
   CHK(check_sys(ctx, sys));
   SysHost& h = ctx->sys[sys];
   if (on && h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
     return fail(ctx, GEMSGPU_ERR_STATE, "virial: lj, plj, slj and SMA-TB systems only");
+  if (on && one_sided(h))
+    return fail(ctx, GEMSGPU_ERR_STATE, "virial: one-sided (feels) pairs have no pair virial");
   if (!on && moving_box(h.d)) return fail(ctx, GEMSGPU_ERR_STATE, "virial: the piston needs it");
   h.d.virial = on ? 1 : 0;
   h.has_forces = false;
@@ -2335,6 +2449,8 @@ int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: the piston needs a box periodic in x, y and z");
   if (h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: lj, plj, slj and SMA-TB systems only");
+  if (one_sided(h))
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: one-sided (feels) pairs have no pair virial");
   if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: FP64 systems only");
   SysDev& d = h.d;
   d.integ = IT_LGF;
@@ -2432,6 +2548,8 @@ int gemsgpu_set_lkd(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: the piston needs a box periodic in x, y and z");
   if (h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: lj, plj, slj and SMA-TB systems only");
+  if (one_sided(h))
+    return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: one-sided (feels) pairs have no pair virial");
   if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: FP64 systems only");
   SysDev& d = h.d;
   d.integ = IT_LKD;
@@ -2507,6 +2625,8 @@ int gemsgpu_add_lgf_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt, double 
     return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: the piston needs a box periodic along its axis");
   if (h.d.ff != FF_LJ && h.d.ff != FF_SMATB)
     return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: lj, plj, slj and SMA-TB systems only");
+  if (one_sided(h))
+    return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: one-sided (feels) pairs have no pair virial");
   if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: FP64 systems only");
   double p[8];
   p[0] = std::sqrt(2.0 * pgama0 * kB_ui * temp * dt);
@@ -3437,8 +3557,9 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
 //   nframe, time, dm_steps, pnframe, ptime, frame   5 x float64 + int32
 //   per atom: pos, vel, acel, acel2, acel3, acel4    3 x float64 each
 // (write_chppiston / read_chppiston, Integration.F90:1488-1520).  The
-// library writes the 'lcg' form with the caller's generator state and zero
-// higher derivatives (acel2..4, the Nordsieck predictor's).
+// library writes the 'lcg' form with the caller's generator state; the
+// higher derivatives acel2..4 are the Nordsieck predictor-corrector's (zero
+// until a system of the context has used it).
 namespace {
 struct ChpOut {
   std::vector<unsigned char> b;
@@ -3535,6 +3656,12 @@ int gemsgpu_chp_write(gemsgpu_ctx* ctx, int sys, const gemsgpu_chp_info* info, v
   CHK(get_d4(ctx, h, ctx->A.pos, x.data()));
   CHK(get_d4(ctx, h, ctx->A.vel, v.data()));
   CHK(get_d4(ctx, h, ctx->A.acel, a.data()));
+  std::vector<double> hi(ctx->A.acel2 ? 9 * (size_t)h.n : 0);
+  if (ctx->A.acel2) {
+    CHK(get_d4(ctx, h, ctx->A.acel2, hi.data()));
+    CHK(get_d4(ctx, h, ctx->A.acel3, hi.data() + 3 * (size_t)h.n));
+    CHK(get_d4(ctx, h, ctx->A.acel4, hi.data() + 6 * (size_t)h.n));
+  }
   ChpOut o;
   const int32_t head[4] = {info->current, info->step, info->nsteps, h.n};
   o.rec(head, sizeof(head));
@@ -3565,7 +3692,7 @@ int gemsgpu_chp_write(gemsgpu_ctx* ctx, int sys, const gemsgpu_chp_info* info, v
     o.rec(&x[3 * (size_t)i], 24);
     o.rec(&v[3 * (size_t)i], 24);
     o.rec(&a[3 * (size_t)i], 24);
-    for (int k = 0; k < 3; k++) o.rec(z3, 24);
+    for (int k = 0; k < 3; k++) o.rec(hi.empty() ? z3 : &hi[3 * ((size_t)k * h.n + i)], 24);
   }
   if (written) *written = o.b.size();
   if (!buf) return 0;  // size query
@@ -3616,12 +3743,15 @@ int gemsgpu_chp_read(gemsgpu_ctx* ctx, int sys, const void* buf, size_t bytes, g
   memcpy(f5, fr, 40);
   memcpy(&got.frame, fr + 40, 4);
   got.nframe = f5[0], got.time = f5[1], got.dm_steps = f5[2], got.pnframe = f5[3], got.ptime = f5[4];
-  std::vector<double> x(3 * (size_t)h.n), v(3 * (size_t)h.n), a(3 * (size_t)h.n), tmp(3);
+  std::vector<double> x(3 * (size_t)h.n), v(3 * (size_t)h.n), a(3 * (size_t)h.n), hi(9 * (size_t)h.n);
   for (int i = 0; i < h.n; i++) {
     if (!in.get(&x[3 * (size_t)i], 3) || !in.get(&v[3 * (size_t)i], 3) || !in.get(&a[3 * (size_t)i], 3) ||
-        !in.get(tmp.data(), 3) || !in.get(tmp.data(), 3) || !in.get(tmp.data(), 3))
+        !in.get(&hi[3 * (size_t)i], 3) || !in.get(&hi[3 * ((size_t)h.n + i)], 3) ||
+        !in.get(&hi[3 * (2 * (size_t)h.n + i)], 3))
       return fail(ctx, GEMSGPU_ERR_ARG, "chp_read: atom %d", i);
   }
+  bool any_hi = false;
+  for (double q : hi) any_hi |= q != 0.0;
   // the box the checkpoint had reached (box_setvars after read(chpunit) tbox)
   if (h.d.boxed) {
     h.box_live = false;
@@ -3633,6 +3763,12 @@ int gemsgpu_chp_read(gemsgpu_ctx* ctx, int sys, const void* buf, size_t bytes, g
   CHK(h2d_xyz(ctx, x.data(), ctx->A.pos + h.off, h.n));
   CHK(h2d_xyz(ctx, v.data(), ctx->A.vel + h.off, h.n));
   CHK(h2d_xyz(ctx, a.data(), ctx->A.acel + h.off, h.n));
+  if (any_hi) CHK(ensure_nord(ctx));
+  if (ctx->A.acel2) {
+    CHK(h2d_xyz(ctx, hi.data(), ctx->A.acel2 + h.off, h.n));
+    CHK(h2d_xyz(ctx, hi.data() + 3 * (size_t)h.n, ctx->A.acel3 + h.off, h.n));
+    CHK(h2d_xyz(ctx, hi.data() + 6 * (size_t)h.n, ctx->A.acel4 + h.off, h.n));
+  }
   CHK(read_states(ctx));
   SysState st = ctx->h_st[sys];
   // a piston resumes as the reference's does after read_chp: pvel from the

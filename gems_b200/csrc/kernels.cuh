@@ -23,6 +23,8 @@ __host__ __device__ constexpr double c_ui_ev() {
   return 1.0e2 * 1.0e2 * 1.6605402e-27 * (1.0 / 1.60219e-19);
 }
 #define EV_UI (1.0 / gg::c_ui_ev())
+// pi = 4 atan(1) (src/Constants.F90:71)
+#define PI_D 3.141592653589793
 
 __device__ __forceinline__ int blk_sys(const BlockMap& M) { return M.sys[blockIdx.x]; }
 
@@ -1249,6 +1251,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed(Arena A, Bloc
 // slj_interact (src/Pairs.F90:403-470) for pairs of the slj form:
 //   r < rs: p = 4e (s6 - 1) s6, f as LJ;  rs <= r <= rc, d = r - rc:
 //   p = sa4 d^4 + sa8 d^8, f = -(4 sa4 d^4 + 8 sa8 d^8) / d
+// sm1_interact (src/Pairs.F90:925-1011) for pairs of the sm1 form:
+//   r > r1: aux = pi (r - (r1 + rc)/2) / (rc - r1), p = e (1/2 + sin(aux)/2) - e,
+//   f = -e cos(aux) (pi/2) r / (rc - r1);  r <= r1: p = -e, f = 0
+// wca_interact (src/Pairs.F90:508-589) is LJ with eshift = -e
 // VIR: also the pair virial of the system (virial_close).
 template <int K, bool VIR>
 __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
@@ -1275,7 +1281,20 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
       if (dr > P.v[3]) continue;
       dr = sqrt(dr);
       double p, f;
-      if (P.v[8] != 0.0 && dr >= P.v[11]) {
+      if (P.v[8] == 2.0) {
+        // sm1: the reference's force carries a factor dr (Pairs.F90:957)
+        const double w = P.v[2] - P.v[11];
+        if (dr > P.v[11]) {
+          const double aux = PI_D * (dr - (P.v[11] + P.v[2]) * 0.5) / w;
+          double sn, cs;
+          sincos(aux, &sn, &cs);
+          p = (0.5 + 0.5 * sn) * e - e;
+          f = -(cs * (0.5 * PI_D) * dr / w) * e;
+        } else {
+          p = -e;
+          f = 0.0;
+        }
+      } else if (P.v[8] != 0.0 && dr >= P.v[11]) {
         const double d = dr - P.v[2];
         const double s4 = d * d * d * d;
         p = P.v[9] * s4 + P.v[10] * s4 * s4;
@@ -1293,7 +1312,8 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
           p = p - P.v[6];
         }
       }
-      double fr = f * EV_UI / dr;
+      // f == 0 (sm1 inside r1) adds nothing, also for coincident atoms
+      double fr = f != 0.0 ? f * EV_UI / dr : 0.0;
       f0 -= fr * v0;
       f1 -= fr * v1;
       f2 -= fr * v2;
@@ -1589,6 +1609,59 @@ __device__ __forceinline__ void vv_a_atom(double dt, double om, const double4& F
   v.x = v.x + adv * a.x;
   v.y = v.y + adv * a.y;
   v.z = v.z + adv * a.z;
+}
+
+// nordsieck_predictor (src/Integration.F90:1192-1228): the fifth-order Gear
+// predictor on the scaled derivatives (v dt, a = dt^2/2 F/m after a
+// correction, a2..a4 the higher ones), summed left to right as written
+__device__ __forceinline__ double nord_pred(double dt, double& x, double& v, double& a, double& a2, double& a3,
+                                            double a4) {
+  v = v * dt;
+  const double p1 = a, p2 = a2, p4 = a3, p7 = a4;
+  const double p3 = 3.0 * p2, p5 = 2.0 * p4, p6 = 2.0 * p5, p8 = 5.0 * p7, p9 = 2.0 * p8;
+  x = p7 + p4 + p2 + p1 + v + x;
+  v = p8 + p6 + p3 + p1 + p1 + v;
+  a = p9 + p6 + p5 + p3 + p1;
+  a2 = p9 + p6 + p2;
+  a3 = p8 + p4;
+  return x;
+}
+
+__device__ __forceinline__ void nord_a_atom(Arena& A, double dt, int i, double4& x, double4& v, double4& a) {
+  double4 a2 = A.acel2[i], a3 = A.acel3[i];
+  const double4 a4 = A.acel4[i];
+  nord_pred(dt, x.x, v.x, a.x, a2.x, a3.x, a4.x);
+  nord_pred(dt, x.y, v.y, a.y, a2.y, a3.y, a4.y);
+  nord_pred(dt, x.z, v.z, a.z, a2.z, a3.z, a4.z);
+  A.acel2[i] = a2;
+  A.acel3[i] = a3;
+}
+
+// nordsieck_corrector (src/Integration.F90:1230-1268), Allen & Tildesley's
+// coefficients for second-order equations: p = dt^2/2 F/m - a corrects
+// every derivative, then v returns to normal units
+__device__ __forceinline__ void nord_corr(double dt, double hm, double F, double& x, double& v, double& a,
+                                          double& a2, double& a3, double& a4) {
+  const double p = hm * F - a;
+  x = x + p * (3.0 / 20.0);
+  v = v + p * (251.0 / 360.0);
+  a = a + p;
+  a2 = a2 + p * (11.0 / 18.0);
+  a3 = a3 + p * (1.0 / 6.0);
+  a4 = a4 + p * (1.0 / 60.0);
+  v = v / dt;
+}
+
+__device__ __forceinline__ void nord_b_atom(Arena& A, double dt, double om, int i, const double4& F, double4& x,
+                                            double4& v, double4& a) {
+  double4 a2 = A.acel2[i], a3 = A.acel3[i], a4 = A.acel4[i];
+  const double hm = dt * dt / 2.0 * om;
+  nord_corr(dt, hm, F.x, x.x, v.x, a.x, a2.x, a3.x, a4.x);
+  nord_corr(dt, hm, F.y, x.y, v.y, a.y, a2.y, a3.y, a4.y);
+  nord_corr(dt, hm, F.z, x.z, v.z, a.z, a2.z, a3.z, a4.z);
+  A.acel2[i] = a2;
+  A.acel3[i] = a3;
+  A.acel4[i] = a4;
 }
 
 // ermak_a (src/Integration.F90:963-1011): position update and the velocity
@@ -2076,6 +2149,11 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
       v.y = v.y * st.lkd_bo[1] / st.lkd_bf[1];
       v.z = v.z * st.lkd_bo[2] / st.lkd_bf[2];
       A.vel[i] = v;
+    } else if (S.integ == IT_NORD) {
+      // between the predictor and the corrector v holds v dt
+      nord_a_atom(A, S.dt, i, x, v, a);
+      A.acel[i] = a;
+      A.vel[i] = v;
     }
     wrap_atom(S, x);
     t.x = moved_atom(A, S, st, i, x, A.pos_old[i], A.type[i]);
@@ -2174,9 +2252,14 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64_ba(Arena A, BlockMap
 }
 
 // integration_stepb (src/Integration.F90:264-301): velocity_verlet_b
-// (:1171-1186) or ermak_b (:1013-1031); FIRE adds P = sum v.F, the per-atom
+// (:1171-1186), ermak_b (:1013-1031), the pistons' second halves or the
+// Nordsieck corrector (:1230-1268); FIRE adds P = sum v.F, the per-atom
 // mixing v = (1-a) v + a |v| F/|F| (FIRE.f90:99-114, with |v|) and the
 // dt / alpha control (:116-131) in the system's last block.
+// NORD: the launch includes predictor-corrector systems (their corrector
+// holds three more derivative vectors; the other integrators' copy stays
+// leaner)
+template <bool NORD>
 __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
@@ -2230,6 +2313,13 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
         r[0] = q[1], r[1] = q[3], r[2] = q[5];
       }
       lkd_kick(S, om, F, r, v, a);
+    } else if (NORD && S.integ == IT_NORD) {
+      // the corrector moves the atom: do_pbc after integration_stepb
+      // (src/Integration.F90:275-280); the next step's skin test sees it
+      double4 x = A.pos[i];
+      nord_b_atom(A, S.dt, om, i, F, x, v, a);
+      wrap_atom(S, x);
+      moved_atom(A, S, st, i, x, A.pos_old[i], A.type[i]);
     }
     A.vel[i] = v;
     A.acel[i] = a;

@@ -71,6 +71,10 @@ _SIGS = {
     "gemsgpu_set_ermak_normals": (_i, [_p, _i, _dp]),
     "gemsgpu_set_fire": (_i, [_p, _i, _d, _d]),
     "gemsgpu_set_slj": (_i, [_p, _i, _i, _i, _d, _d, _d]),
+    "gemsgpu_set_wca": (_i, [_p, _i, _i, _i, _d, _d]),
+    "gemsgpu_set_pred_corr": (_i, [_p, _i, _d]),
+    "gemsgpu_set_sm1": (_i, [_p, _i, _i, _i, _d, _d, _d]),
+    "gemsgpu_set_feels": (_i, [_p, _i, _i, _i]),
     "gemsgpu_set_virial": (_i, [_p, _i, _i]),
     "gemsgpu_set_lgf": (_i, [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_set_lgf_normals": (_i, [_p, _i, _dp]),
@@ -451,6 +455,18 @@ class System:
         """slj_set: LJ core to rs, polynomial tail to the derived cut-off."""
         self._c(lib().gemsgpu_set_slj(self.ctx.h, self.sid, ti, tj, float(e), float(sg), float(rs)))
 
+    def set_wca(self, e, s, ti=0, tj=0):
+        """wca_set: LJ cut at its minimum and shifted up by e."""
+        self._c(lib().gemsgpu_set_wca(self.ctx.h, self.sid, ti, tj, float(e), float(s)))
+
+    def set_sm1(self, r1, r2, e, ti=0, tj=0):
+        """sm1_set: smooth step of depth e (eV) from r1 to r2."""
+        self._c(lib().gemsgpu_set_sm1(self.ctx.h, self.sid, ti, tj, float(r1), float(r2), float(e)))
+
+    def set_feels(self, ti, tj):
+        """`interact g1 feels g2`: the pair (ti, tj) acts on type ti only."""
+        self._c(lib().gemsgpu_set_feels(self.ctx.h, self.sid, int(ti), int(tj)))
+
     def set_virial(self, on=True):
         self._c(lib().gemsgpu_set_virial(self.ctx.h, self.sid, 1 if on else 0))
 
@@ -497,6 +513,11 @@ class System:
     def set_vv(self, dt):
         self._axes = []
         self._c(lib().gemsgpu_set_vv(self.ctx.h, self.sid, float(dt)))
+
+    def set_pred_corr(self, dt):
+        """`evolve pred_corr_5`: the fifth-order Nordsieck predictor-corrector."""
+        self._axes = []
+        self._c(lib().gemsgpu_set_pred_corr(self.ctx.h, self.sid, float(dt)))
 
     def set_ermak(self, dt, gama, temp, seed=12345):
         self._axes = []

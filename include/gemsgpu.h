@@ -147,6 +147,23 @@ int gemsgpu_set_lj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
  * mix lj, plj and slj (slj_interact, Pairs.F90:403-470); FP64 systems. */
 int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
                     double sigma, double rs);
+/* wca_set (src/Pairs.F90:495-506): Weeks-Chandler-Andersen, LJ cut at
+ * 2**(1./6.) sigma (the exponent a single-precision literal, as the
+ * reference evaluates it) and shifted up by eps (wca_interact,
+ * Pairs.F90:508-589).  Same as gemsgpu_set_lj with that cut-off and
+ * eshift = -eps. */
+int gemsgpu_set_wca(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps,
+                    double sigma);
+/* sm1_set (src/Pairs.F90:916-923): smooth step of depth eps (eV) that rises
+ * from -eps at r1 to 0 at r2 (A), the cut-off; the force keeps the factor r
+ * of sm1_interact (Pairs.F90:957).  FP64 systems. */
+int gemsgpu_set_sm1(gemsgpu_ctx* ctx, int sys, int ti, int tj, double r1,
+                    double r2, double eps);
+/* `interact g1 feels g2` (src/Interaction.f90:69-76, 128-131): after a pair
+ * setter for (ti, tj), the pair acts on the atoms of type ti only (give each
+ * group its own type).  Energies count the feeling side's half, as the
+ * reference's.  Not with the virial or a piston (no pair virial). */
+int gemsgpu_set_feels(gemsgpu_ctx* ctx, int sys, int ti, int tj);
 /* Pair virial W = sum_i r_i (x) F_i (inq_virial, Inq_Properties.F90:439-527)
  * accumulated by the force kernels of an lj/plj/slj or SMA-TB system (on=1;
  * FP64, or FP32 per pair with FP64 accumulation in mixed precision; SMA-TB
@@ -183,6 +200,12 @@ int gemsgpu_get_nupd(gemsgpu_ctx* ctx, int sys, int64_t* nupd);
 /* ------------------------------------------------------------ integrators */
 
 int gemsgpu_set_vv(gemsgpu_ctx* ctx, int sys, double dt);
+/* `evolve pred_corr_5` (src/Integration.F90:143-145): the fifth-order
+ * Nordsieck predictor-corrector, nordsieck_predictor as step a and
+ * nordsieck_corrector as step b (Integration.F90:1192-1268), on the scaled
+ * derivatives acel..acel4 that the atoms keep (zero for new atoms; read and
+ * written by gemsgpu_chp_read / gemsgpu_chp_write). */
+int gemsgpu_set_pred_corr(gemsgpu_ctx* ctx, int sys, double dt);
 /* set_ermak (src/Integration.F90:909-961): dt (ps), gamma (1/ps), T (K).
  * The device draws its normals from a counter-based Philox4x32-10 stream
  * keyed by seed (production mode). */

@@ -110,7 +110,7 @@ void rang(Lcg& s, double* r1, double* r2) {  // always draws a pair
 
 // ---------------------------------------------------------------- system
 enum FF { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3, FF_SLJ = 4 };
-enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6 };
+enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6, IT_NORD = 7 };
 
 // One integrator acting on one coordinate of every atom (integrate objects
 // set by `evolve piston_lgf x|y|z` and `evolve ermak_x|y|z`,
@@ -144,6 +144,8 @@ struct LJp {
   bool shifted_force = false;  // plj (Pairs.F90:282-370)
   double prc = 0, frc = 0;
   double eshift = 0;           // constant energy shift per pair (eV)
+  bool sm1 = false;            // sm1 (Pairs.F90:916-1011): smooth step from r1 to rc
+  double r1 = 0;
 };
 
 struct SLJp {  // slj (Pairs.F90:374-401): LJ with a splined tail from rs to rc
@@ -165,6 +167,7 @@ struct TSp {  // Tersoff 1988 parameter set (single species)
 struct Sys {
   int n = 0;
   std::vector<double> pos, vel, acel, force, pos_old, pos_v, vel_v;
+  std::vector<double> acel2, acel3, acel4;  // Nordsieck derivatives (Atoms.F90:77-79)
   std::vector<double> epot, mass, one_mass, one_sqrt_mass;
   std::vector<int> type;
   bool boxed = false;
@@ -425,7 +428,22 @@ double lj_interact(Sys& s) {
       dr = std::sqrt(dr);
       double s_dr = pow6(P.s / dr);
       double p, f;
-      if (P.shifted_force) {
+      if (P.sm1) {
+        // sm1_interact (Pairs.F90:925-1011): p = e (1/2 + 1/2 sin(aux)) - e
+        // beyond r1, -e inside; the reference's force carries a factor dr
+        // (Pairs.F90:957), kept; the sign flips into this loop's convention
+        // (F_i -= f vd / r, the reference's sm1 adds f vd / r)
+        if (dr > P.r1) {
+          const double aux = pi * (dr - (P.r1 + P.rc) * 0.5) / (P.rc - P.r1);
+          p = 0.5 + 0.5 * std::sin(aux);
+          f = std::cos(aux) * pio2 * dr / (P.rc - P.r1);
+          p = p * P.e - P.e;
+          f = -(f * P.e);
+        } else {
+          p = -P.e;
+          f = 0.0;
+        }
+      } else if (P.shifted_force) {
         p = 4.0 * P.e * (s_dr * s_dr - s_dr) - P.prc - P.frc * (dr - P.rc);
         f = P.e * (48.0 * s_dr - 24.0) * s_dr / dr + P.frc;
       } else {
@@ -435,6 +453,9 @@ double lj_interact(Sys& s) {
       p = p * ev_ui;
       f = f * ev_ui;
       ep = ep + p * 0.5;
+      // f == 0 (sm1 inside r1) adds nothing, also at dr == 0 where the
+      // reference's -0 vd / dr is not a number
+      if (f == 0.0) continue;
       const double f2[3] = {f * vd[0] / dr, f * vd[1] / dr, f * vd[2] / dr};
       fx = fx - f2[0];
       fy = fy - f2[1];
@@ -839,6 +860,43 @@ void vv_b(Sys& s) {
     }
 }
 
+// nordsieck_predictor (Integration.F90:1192-1228): the fifth-order Gear
+// predictor on the scaled derivatives (vel dt, acel = dt^2/2 F/m after a
+// correction, acel2..4 the higher ones); sums left to right as written
+void nord_a(Sys& s) {
+  for (int q = 0; q < 3 * s.n; q++) {
+    s.vel[q] = s.vel[q] * s.dt;
+    const double p1 = s.acel[q], p2 = s.acel2[q], p4 = s.acel3[q], p7 = s.acel4[q];
+    const double p3 = 3 * p2, p5 = 2 * p4, p6 = 2 * p5, p8 = 5 * p7, p9 = 2 * p8;
+    s.pos[q] = p7 + p4 + p2 + p1 + s.vel[q] + s.pos[q];
+    s.vel[q] = p8 + p6 + p3 + p1 + p1 + s.vel[q];
+    s.acel[q] = p9 + p6 + p5 + p3 + p1;
+    s.acel2[q] = p9 + p6 + p2;
+    s.acel3[q] = p8 + p4;
+  }
+}
+
+// nordsieck_corrector (Integration.F90:1230-1268): Allen & Tildesley's
+// coefficients for second-order equations (c0 = 3/20)
+void nord_b(Sys& s) {
+  const double c0 = 3.0 / 20.0, c1 = 251.0 / 360.0, c3 = 11.0 / 18.0, c4 = 1.0 / 6.0, c5 = 1.0 / 60.0;
+  const double dt2_2 = s.dt * s.dt / 2.0;
+  for (int i = 0; i < s.n; i++) {
+    const double half_mass = dt2_2 * s.one_mass[i];
+    for (int k = 0; k < 3; k++) {
+      const int q = 3 * i + k;
+      const double p = half_mass * s.force[q] - s.acel[q];
+      s.pos[q] = s.pos[q] + p * c0;
+      s.vel[q] = s.vel[q] + p * c1;
+      s.acel[q] = s.acel[q] + p;
+      s.acel2[q] = s.acel2[q] + p * c3;
+      s.acel3[q] = s.acel3[q] + p * c4;
+      s.acel4[q] = s.acel4[q] + p * c5;
+      s.vel[q] = s.vel[q] / s.dt;
+    }
+  }
+}
+
 // ermak_a (Integration.F90:963-1011).  Normals come from the LCG stream
 // (rang, one pair per dimension) or from an external stream of 6 per atom.
 void ermak_a(Sys& s) {
@@ -1223,6 +1281,7 @@ void stepa(Sys& s) {
   else if (s.integ == IT_LGF) lgf_a(s);
   else if (s.integ == IT_AXES) axes_a(s);
   else if (s.integ == IT_LKD) lkd_a(s);
+  else if (s.integ == IT_NORD) nord_a(s);
   do_pbc(s);
 }
 
@@ -1232,6 +1291,7 @@ void stepb(Sys& s) {
   else if (s.integ == IT_LGF) lgf_b(s);
   else if (s.integ == IT_AXES) axes_b(s);
   else if (s.integ == IT_LKD) lkd_b(s);
+  else if (s.integ == IT_NORD) nord_b(s);
   do_pbc(s);
   if (s.integ == IT_FIRE) fire_mix(s);
 }
@@ -1727,6 +1787,9 @@ void* orc_sys_new(int n) {
   s->force.assign(3 * n, 0.0);
   s->pos_v.assign(3 * n, 0.0);
   s->vel_v.assign(3 * n, 0.0);
+  s->acel2.assign(3 * n, 0.0);
+  s->acel3.assign(3 * n, 0.0);
+  s->acel4.assign(3 * n, 0.0);
   s->pos_old.assign(3 * n, 0.0);
   s->epot.assign(n, 0.0);
   s->mass.assign(n, 1.0);
@@ -1816,6 +1879,34 @@ void orc_set_lj(void* p, int ti, int tj, double e, double sg, double rc,
   recompute_rcut(s);
 }
 
+// wca_set (Pairs.F90:495-506): LJ cut at 2**(1./6.) sigma, where 1./6. is a
+// single-precision literal, and shifted up by e (wca_interact, :508-589)
+void orc_set_wca(void* p, int ti, int tj, double e, double sg) {
+  orc_set_lj(p, ti, tj, e, sg, std::pow(2.0, (double)(1.0f / 6.0f)) * sg, 0, -e);
+}
+
+// sm1_set (Pairs.F90:916-923): r1, r2 (A), e (eV; pair_cli reads it with
+// ev_ui, Pairs.F90:183-187)
+void orc_set_sm1(void* p, int ti, int tj, double r1, double r2, double e) {
+  Sys* s = (Sys*)p;
+  s->ff = FF_LJ;
+  LJp P;
+  P.on = true; P.sm1 = true; P.e = e; P.r1 = r1; P.rc = r2; P.rc2 = r2 * r2;
+  s->lj[ti][tj] = P;
+  s->lj[tj][ti] = P;
+  recompute_rcut(s);
+}
+
+// `interact g1 feels g2` (Interaction.f90:69-76, 128-131): half and newton
+// off, so only the atoms of g1 feel the pair.  With one type per group the
+// pair (ti, tj) then acts on the atoms of type ti only.
+void orc_set_feels(void* p, int ti, int tj) {
+  Sys* s = (Sys*)p;
+  if (ti == tj) return;
+  s->lj[tj][ti] = LJp();
+  s->slj[tj][ti] = SLJp();
+}
+
 void orc_set_smatb(void* p, int ti, int tj, double a, double eps, double pp,
                    double q, double r0, double rci, double rce) {
   Sys* s = (Sys*)p;
@@ -1866,6 +1957,19 @@ void orc_get_list(void* p, int* nn, int* list) {
 }
 
 void orc_set_vv(void* p, double dt) { Sys* s = (Sys*)p; s->integ = IT_VV; s->dt = dt; }
+// `evolve pred_corr_5` (Integration.F90:143-145)
+void orc_set_pred_corr(void* p, double dt) { Sys* s = (Sys*)p; s->integ = IT_NORD; s->dt = dt; }
+// acel, acel2, acel3, acel4 (3n each, atom-major) out of or into the system
+void orc_get_derivs(void* p, double* out) {
+  Sys* s = (Sys*)p;
+  const std::vector<double>* v[4] = {&s->acel, &s->acel2, &s->acel3, &s->acel4};
+  for (int k = 0; k < 4; k++) std::copy(v[k]->begin(), v[k]->end(), out + (size_t)k * 3 * s->n);
+}
+void orc_set_derivs(void* p, const double* in) {
+  Sys* s = (Sys*)p;
+  std::vector<double>* v[4] = {&s->acel, &s->acel2, &s->acel3, &s->acel4};
+  for (int k = 0; k < 4; k++) std::copy(in + (size_t)k * 3 * s->n, in + (size_t)(k + 1) * 3 * s->n, v[k]->begin());
+}
 void orc_set_ermak(void* p, double dt, double gama, double temp, void* rng) {
   Sys* s = (Sys*)p;
   set_ermak(*s, dt, gama, temp);

@@ -91,6 +91,12 @@ def lib():
         "orc_lbfgs": (_i, [_p, _i, _d, _d, _i, _ip, _ip, _dp]),
         "orc_neb": (_d, [_p, _i, _dp, _ip, _i, _d, _i]),
         "orc_set_slj": (None, [_p, _i, _i, _d, _d, _d]),
+        "orc_set_wca": (None, [_p, _i, _i, _d, _d]),
+        "orc_set_sm1": (None, [_p, _i, _i, _d, _d, _d]),
+        "orc_set_feels": (None, [_p, _i, _i]),
+        "orc_set_pred_corr": (None, [_p, _d]),
+        "orc_get_derivs": (None, [_p, _dp]),
+        "orc_set_derivs": (None, [_p, _dp]),
         "orc_set_lgf": (None, [_p, _d, _d, _d, _d, _d, _d, _p]),
         "orc_virial_ev": (None, [_p, _dp]),
         "orc_add_lgf_axis": (None, [_p, _i, _d, _d, _d, _d, _d, _d, _p]),
@@ -275,6 +281,32 @@ class System:
 
     def set_lj(self, e, s, rc, ti=0, tj=0, shifted_force=False, eshift=0.0):
         lib().orc_set_lj(self.h, ti, tj, e, s, rc, 1 if shifted_force else 0, eshift)
+
+    def set_pred_corr(self, dt):
+        """`evolve pred_corr_5`: the fifth-order Nordsieck predictor-corrector."""
+        lib().orc_set_pred_corr(self.h, float(dt))
+
+    def derivs(self):
+        """acel, acel2, acel3, acel4 as a (4, n, 3) array."""
+        out = np.empty((4, self.n, 3), dtype=np.float64)
+        lib().orc_get_derivs(self.h, _ptr(out))
+        return out
+
+    def set_derivs(self, d):
+        a = np.ascontiguousarray(d, dtype=np.float64).reshape(4, self.n, 3)
+        lib().orc_set_derivs(self.h, _ptr(a))
+
+    def set_wca(self, e, s, ti=0, tj=0):
+        """wca_set: LJ cut at its minimum and shifted up by e."""
+        lib().orc_set_wca(self.h, int(ti), int(tj), float(e), float(s))
+
+    def set_sm1(self, r1, r2, e, ti=0, tj=0):
+        """sm1_set: smooth step of depth e (eV) from r1 to r2."""
+        lib().orc_set_sm1(self.h, int(ti), int(tj), float(r1), float(r2), float(e))
+
+    def set_feels(self, ti, tj):
+        """`interact g1 feels g2`: the pair (ti, tj) acts on type ti only."""
+        lib().orc_set_feels(self.h, int(ti), int(tj))
 
     def set_smatb(self, A, xi, p, q, r0, rci, rce, ti=0, tj=0):
         lib().orc_set_smatb(self.h, ti, tj, A, xi, p, q, r0, rci, rce)

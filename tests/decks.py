@@ -366,6 +366,106 @@ def lj_dimer_rows(sys_factory, ui_ev, kind="lj"):
     return np.concatenate([np.array(rows), r[:, :3]]), d["ref"]
 
 
+# wca, sm1 and feels decks of examples/LJ (FP64 H atoms, mass 1.008)
+WCA_SIGMA = 0.890898718140339
+SLJ_PRM = (1.0, 0.890898718140339, 1.108683)
+
+
+def lj_family_rows(sys_factory, ui_ev, kind):
+    """Run examples/LJ/wca.gms, sm1.gms or feels.gms on an engine.
+
+    sys_factory(pos, mass, types, ntypes) makes the system; one atom type per
+    group of the deck, so that a one-sided `feels` pair is a pair of types.
+    Returns (rows of epot, ekin, etot in eV, golden rows)."""
+    g = golden()
+    rows = []
+    mass = MASS["H"]
+
+    def state(s, pos):
+        s.set_pos(pos)
+        s.interact()
+        ek, _ = s.kin()
+        ep = s.epot_sum()
+        rows.append([ep * ui_ev, ek * ui_ev, (ep + ek) * ui_ev])
+
+    if kind == "wca":
+        # group 2 = atom 2 feels group 3 = atom 1: `interact 2 feels 3 wca`
+        pos = np.array([[1.0, 1.0, 1.0], [2.2, 1.0, 1.0]])
+        s = sys_factory(pos.copy(), mass, np.array([0, 1]), 2)
+        s.set_box((5.78, 5.78, 5.78), (False, False, False))
+        s.set_wca(1.0, WCA_SIGMA, ti=1, tj=0)
+        s.set_feels(1, 0)
+        state(s, pos)
+        pos[1, 0] += -1.2
+        pos[1, 0] += WCA_SIGMA
+        state(s, pos)
+        pos[1, 0] += -WCA_SIGMA
+        pos[1, 0] += 0.9
+        for _ in range(250):
+            pos[1, 0] += 0.01
+            state(s, pos)
+        for mv in (-2.5, -0.9, 0.95):
+            pos[1, 0] += mv
+        s.set_pos(pos)
+        s.set_vv(0.002 * 0.01018)
+        r = s.dinamica(1000, 10)
+        ref = g["wca_energy"]
+    elif kind == "sm1":
+        # no box: the O(N^2) list; both atoms start on the same site
+        pos = np.array([[1.0, 1.0, 1.0], [1.0, 1.0, 1.0]])
+        s = sys_factory(pos.copy(), mass, np.array([0, 0]), 1)
+        s.set_sm1(1.0, 2.0, 0.01)
+        state(s, pos)
+        for _ in range(300):
+            pos[1, 0] += 0.01
+            state(s, pos)
+        pos[1, 0] += -2.0
+        s.set_pos(pos)
+        # set_cm_vel (Set_Properties.f90:981-997) of group 2 = atom 2
+        s.set_vel(np.array([[0.0, 0.0, 0.0], [10.0, 0.0, 0.0]]))
+        s.set_vv(0.001)
+        r = s.dinamica(1000, 1)
+        ref = g["sm1_energy"]
+    elif kind == "feels":
+        # types: 0 = atoms 1, 3; 1 = atoms 2, 4 (group 3); 2 = atom 5 (group 4)
+        pos = np.array([[1.0, 1.0, 1.0], [2.2, 1.0, 1.0], [1.0, 1.0, 5.0],
+                        [2.2, 1.0, 5.0], [3.4, 1.0, 1.0]])
+        s = sys_factory(pos.copy(), mass, np.array([0, 1, 0, 1, 2]), 3)
+        s.set_box((5.78, 5.78, 5.78), (False, False, False))
+        for a, b in ((0, 0), (0, 1), (1, 1)):   # interact 2 with 2 slj
+            s.set_slj(*SLJ_PRM, ti=a, tj=b)
+        s.set_slj(*SLJ_PRM, ti=2, tj=1)          # interact 4 feels 3 slj
+        s.set_feels(2, 1)
+        state(s, pos)
+        s.set_vv(0.002 * 0.01018)
+        r = s.dinamica(1000, 10)
+        ref = g["feels_energy"]
+    else:
+        raise ValueError(kind)
+    return np.concatenate([np.array(rows), r[:, :3]]), np.array(ref)
+
+
+def chp_records(data):
+    """Fortran unformatted sequential records (4-byte length before and after)."""
+    import struct
+    out, at = [], 0
+    while at < len(data):
+        (m,) = struct.unpack_from("<i", data, at)
+        (m2,) = struct.unpack_from("<i", data, at + 4 + m)
+        assert m == m2
+        out.append(data[at + 4:at + 4 + m])
+        at += 8 + m
+    return out
+
+
+def chp_atoms(data, n):
+    """The per-atom records of a GEMS .chp file as a (6, n, 3) array: pos,
+    vel, acel, acel2, acel3, acel4 (write_chp, Checkpoint.F90:175-184)."""
+    import struct
+    r = chp_records(data)[-6 * n:]
+    return np.array([[struct.unpack("<3d", r[6 * i + k]) for i in range(n)] for k in range(6)])
+
+
 def he_ne_setup(O):
     """NVE/NVT initial state from the oracle's stream (fill, box move,
     tempgdist 300); returns positions, velocities, types, masses, box, rng."""

@@ -46,10 +46,14 @@ def main():
         "xyz_energy": rows("examples/XYZ/ref/Energy.readxyz.dat"),
         "lj_energy": rows("examples/LJ/ref/Energy.lj.dat"),
         "slj_energy": rows("examples/LJ/ref/Energy.slj.dat"),
+        "wca_energy": rows("examples/LJ/ref/Energy.wca.dat"),
+        "sm1_energy": rows("examples/LJ/ref/Energy.sm1.dat"),
+        "feels_energy": rows("examples/LJ/ref/Energy.feels.dat"),
         "smatb_md_coords": xyz_frames("examples/SMA-TB/coords.xyz")[0],
         "smatb_md_energy": rows("examples/SMA-TB/ref/Energy.md.dat"),
         "smatb_bulk_energy": rows("examples/SMA-TB/ref/Energy.bulk.dat"),
         "nve_energy": rows("examples/NVE/ref/Energy.v_verlet.dat"),
+        "nve_pc5_energy": rows("examples/NVE/ref/Energy.pred_corr_5.dat"),
         "nvt_energy": rows("examples/NVT/ref/Energy.ermak.dat"),
         "repex_energy": [rows("examples/RepExchange/ref/Energy.lj.mpi%d.dat" % k) for k in range(4)],
         "neb_gold_cube": xyz_frames("examples/configs/ref/gold_cube.xyz")[0],

@@ -260,17 +260,7 @@ def test_lkd_trajectory_equals_oracle(ctx):
 
 
 # ------------------------------------------------------------------ GEMS .chp
-def _records(data):
-    """Fortran unformatted sequential records (4-byte length before and after)."""
-    import struct
-    out, at = [], 0
-    while at < len(data):
-        (m,) = struct.unpack_from("<i", data, at)
-        (m2,) = struct.unpack_from("<i", data, at + 4 + m)
-        assert m == m2
-        out.append(data[at + 4:at + 4 + m])
-        at += 8 + m
-    return out
+_records = decks.chp_records
 
 
 def test_gems_checkpoint_file_flex_split_run(ctx):

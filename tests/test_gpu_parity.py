@@ -279,6 +279,41 @@ def test_gpu_lj_dimer(ctx, kind):
     np.testing.assert_allclose(got, ref, atol=2e-7, rtol=1e-6)
 
 
+@pytest.mark.parametrize("kind", ["wca", "sm1", "feels"])
+def test_gpu_lj_family_decks(ctx, kind):
+    """wca.gms, sm1.gms and feels.gms on the GPU (FP64) against their golden
+    files, and row by row against the oracle."""
+    got, ref = decks.lj_family_rows(lambda p, m, t, nt: gpu_ref_sys(p, m, t, nt, ctx=ctx), gems.UI_EV, kind)
+    assert got.shape == ref.shape
+    assert decks.gems_rule(ref[:, 0], got[:, 0]) < 1e-6
+    np.testing.assert_allclose(got, ref, atol=6e-7, rtol=1e-6)
+    orc, _ = decks.lj_family_rows(O.System, 1.0 / O.lib().orc_ev_ui(), kind)
+    np.testing.assert_allclose(got, orc, atol=1e-12, rtol=1e-9)
+
+
+def test_gpu_feels_guards(ctx):
+    """One-sided pairs: forces on the feeling type only; no virial, no
+    piston; sm1 stays FP64."""
+    pos = np.array([[1.0, 1.0, 1.0], [2.0, 1.0, 1.0], [5.0, 5.0, 5.0]])
+    g = gpu_ref_sys(pos, 1.008, np.array([0, 1, 1]), 2, ctx=ctx)
+    g.set_box((10.0, 10.0, 10.0), (True, True, True))
+    g.set_wca(1.0, 0.95, ti=1, tj=0)
+    g.set_feels(1, 0)
+    g.interact()
+    f = g.force()
+    assert np.all(f[0] == 0.0) and f[1, 0] > 0.0 and np.all(f[2] == 0.0)
+    with pytest.raises(gems.GemsGpuError):
+        g.set_virial(True)
+    with pytest.raises(gems.GemsGpuError):
+        g.set_lgf(0.002, 300.0, 1.0, 1.0, 1.0, 10.0)
+    h = gpu_ref_sys(pos, 1.008, ctx=ctx)
+    h.set_sm1(1.0, 2.0, 0.01)
+    with pytest.raises(gems.GemsGpuError):
+        h.set_precision(gems.PREC_MIXED)
+    g.destroy()
+    h.destroy()
+
+
 def test_gpu_smatb_bulk_ermak_parity_stream(ctx):
     d = decks.bulk_deck()
     g = gpu_ref_sys(d["pos"], d["mass"], ctx=ctx)
@@ -300,6 +335,62 @@ def test_gpu_nve_plj(ctx):
     ref = np.array(decks.golden()["nve_energy"])
     assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
     np.testing.assert_allclose(r[:, 1:3], ref[:, 1:3], rtol=1e-5)
+
+
+def _he_ne_gpu(ctx):
+    pos, vel, types, mass, box, _ = decks.he_ne_setup(O)
+    g = gpu_ref_sys(pos, mass, types, 2, ctx=ctx, vel=vel)
+    g.set_box(box, (True, True, True))
+    decks.apply_plj(g)
+    return g
+
+
+def test_gpu_nve_pred_corr(ctx):
+    """pred_corr_5.gms on the GPU: the same gas under the fifth-order
+    Nordsieck predictor-corrector, against its golden file."""
+    g = _he_ne_gpu(ctx)
+    g.set_pred_corr(0.002)
+    r = g.dinamica(5000, 100)
+    ref = np.array(decks.golden()["nve_pc5_energy"])
+    assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
+    np.testing.assert_allclose(r[:, 1:3], ref[:, 1:3], rtol=1e-5)
+    g.destroy()
+
+
+def test_gpu_pred_corr_derivatives_and_resume(ctx):
+    """The predictor-corrector's derivatives acel..acel4 after 200 steps
+    match the oracle's, read from GEMS's .chp file; a system resumed from
+    the file written at step 100 continues the unbroken trajectory."""
+    pos, vel, types, mass, box, _ = decks.he_ne_setup(O)
+    n = len(pos)
+    s = O.System(pos, mass, types, 2)
+    s.set_box(box, (True, True, True))
+    s.set_vel(vel)
+    decks.apply_plj(s)
+    s.set_pred_corr(0.002)
+    s.dinamica(200, 100)
+    want = s.derivs()
+    g = _he_ne_gpu(ctx)
+    g.set_pred_corr(0.002)
+    g.dinamica(100, 100)
+    chp = g.write_gems_chp(step=100, nsteps=100)
+    g.dinamica(100, 100)
+    got = decks.chp_atoms(g.write_gems_chp(step=200, nsteps=200), n)
+    np.testing.assert_allclose(got[0], s.pos, rtol=0, atol=1e-9)
+    for k in range(4):
+        scale = np.abs(want[k]).max()
+        assert scale > 0.0
+        np.testing.assert_allclose(got[2 + k], want[k], rtol=1e-6, atol=1e-8 * scale)
+    h = gpu_ref_sys(np.zeros_like(pos), mass, types, 2, ctx=ctx)
+    h.set_box(box, (True, True, True))
+    decks.apply_plj(h)
+    h.set_pred_corr(0.002)
+    assert h.read_gems_chp(chp)["step"] == 100
+    h.dinamica(100, 100)
+    np.testing.assert_allclose(h.pos, g.pos, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(h.vel, g.vel, rtol=1e-9, atol=1e-12)
+    g.destroy()
+    h.destroy()
 
 
 def test_gpu_nvt_plj_parity_stream(ctx):

@@ -64,6 +64,17 @@ def test_lj_dimer_scan_and_vv(kind):
     np.testing.assert_allclose(got, ref, atol=1e-7, rtol=1e-6)
 
 
+@pytest.mark.parametrize("kind", ["wca", "sm1", "feels"])
+def test_lj_family_decks(kind):
+    """examples/LJ/wca.gms (one-sided WCA dimer), sm1.gms (smooth step, no
+    box, 1000 VV steps) and feels.gms (slj dimers plus one atom that feels
+    two of them): replayed against their golden files."""
+    got, ref = decks.lj_family_rows(O.System, 1.0 / O.lib().orc_ev_ui(), kind)
+    assert got.shape == ref.shape
+    assert decks.gems_rule(ref[:, 0], got[:, 0]) < 1e-6
+    np.testing.assert_allclose(got, ref, atol=6e-7, rtol=1e-6)
+
+
 def test_smatb_bulk_linked_cells_ermak():
     """examples/SMA-TB/bulk.gms: 4000 Ag, linked cells, Ermak 1500 K, LCG."""
     d = decks.bulk_deck()
@@ -131,6 +142,9 @@ def _he_ne(kind):
     if kind == "nve":
         s.set_vv(0.002)
         return s.dinamica(5000, 100), np.array(g["nve_energy"])
+    if kind == "pc5":
+        s.set_pred_corr(0.002)
+        return s.dinamica(5000, 100), np.array(g["nve_pc5_energy"])
     s.set_ermak(0.002, 10.0, 300.0, rng)
     return s.dinamica(10000, 100), np.array(g["nvt_energy"])
 
@@ -138,6 +152,15 @@ def _he_ne(kind):
 def test_nve_plj_fill_gdist_vv():
     """examples/NVE/v_verlet.gms: fill + tempgdist + 3 plj groups + VV."""
     r, ref = _he_ne("nve")
+    assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
+    np.testing.assert_allclose(r[:, 0], ref[:, 0], atol=2e-8)
+    np.testing.assert_allclose(r[:, 1:3], ref[:, 1:3], rtol=1e-6)
+
+
+def test_nve_plj_pred_corr_5():
+    """examples/NVE/pred_corr_5.gms: the same gas under the fifth-order
+    Nordsieck predictor-corrector (nordsieck_predictor/_corrector)."""
+    r, ref = _he_ne("pc5")
     assert decks.gems_rule(ref[:, 0], r[:, 0]) < 1e-6
     np.testing.assert_allclose(r[:, 0], ref[:, 0], atol=2e-8)
     np.testing.assert_allclose(r[:, 1:3], ref[:, 1:3], rtol=1e-6)
