@@ -33,7 +33,8 @@ __device__ __forceinline__ void stencil(int k, int& dx, int& dy, int& dz) {
 }
 
 enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
-enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6, IT_NORD = 7 };
+enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6, IT_NORD = 7,
+                IT_BROWN = 8 };
 // IT_AXES: one integrator per coordinate -- a G-JF piston on that box length
 // (AX_FLEX) or Ermak dynamics of that coordinate (AX_ERMAK)
 enum AX : int { AX_NONE = 0, AX_FLEX = 1, AX_ERMAK = 2 };
@@ -84,6 +85,7 @@ struct SysDev {
   // integrator
   double dt;
   double cc0, cc1, cc2, sdr, sdv, crv1, crv2, skt;
+  double bd_fac1, bd_fac2;  // set_cbrownian (Integration.F90:834-853): dt/gamma, sqrt(2 kB T dt/gamma)
   uint64_t seed;
   double fire_dtmax, fire_fmax;
   int fire_maxit, pad1;

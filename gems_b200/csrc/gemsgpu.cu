@@ -904,9 +904,9 @@ int launch_forces_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss, cudaGraphCond
 int launch_step_b(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
-  bool nord = false;
-  for (int s : ss) nord |= ctx->sys[s].d.integ == IT_NORD;
-  if (nord) k_step_b<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+  bool moves = false;
+  for (int s : ss) moves |= ctx->sys[s].d.integ == IT_NORD || ctx->sys[s].d.integ == IT_BROWN;
+  if (moves) k_step_b<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
   else k_step_b<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
   ++ctx->launches;
   CU(cudaGetLastError());
@@ -2256,6 +2256,26 @@ int gemsgpu_set_pred_corr(gemsgpu_ctx* ctx, int sys, double dt) {
   SysHost& h = ctx->sys[sys];
   h.d.integ = IT_NORD;
   h.d.dt = dt;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+// `evolve brownian temp gama` (src/Integration.F90:146-149): set_cbrownian
+// (:834-853); step a does nothing, step b is cbrownian (:855-882)
+int gemsgpu_set_brownian(gemsgpu_ctx* ctx, int sys, double dt, double temp, double gama, uint64_t seed) {
+  CHK(check_sys(ctx, sys));
+  if (!(dt > 0.0) || !(gama > 0.0) || !(temp >= 0.0))
+    return fail(ctx, GEMSGPU_ERR_ARG, "set_brownian: dt>0, gamma>0, T>=0");
+  SysHost& h = ctx->sys[sys];
+  SysDev& d = h.d;
+  d.integ = IT_BROWN;
+  d.dt = dt;
+  d.bd_fac1 = dt / gama;
+  d.bd_fac2 = std::sqrt(2.0 * kB_ui * temp * d.bd_fac1);
+  h.temp = temp;
+  d.seed = seed;
+  d.use_ext_normals = 0;
   CHK(push_sys(ctx, sys));
   invalidate(ctx);
   return 0;

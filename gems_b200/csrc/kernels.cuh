@@ -2087,7 +2087,8 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
         atomicOr(A.any_rebuild, 1);
         if constexpr (COND) cudaGraphSetConditional(cond, 1u);
       }
-      if ((S.integ == IT_ERMAK || S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD) &&
+      if ((S.integ == IT_ERMAK || S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD ||
+           S.integ == IT_BROWN) &&
           !S.use_ext_normals)
         st.step++;
       if (S.integ == IT_FIRE) st.fire_zero = 0;
@@ -2253,13 +2254,13 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64_ba(Arena A, BlockMap
 
 // integration_stepb (src/Integration.F90:264-301): velocity_verlet_b
 // (:1171-1186), ermak_b (:1013-1031), the pistons' second halves or the
-// Nordsieck corrector (:1230-1268); FIRE adds P = sum v.F, the per-atom
+// Nordsieck corrector (:1230-1268) or cbrownian (:855-882); FIRE adds P = sum v.F, the per-atom
 // mixing v = (1-a) v + a |v| F/|F| (FIRE.f90:99-114, with |v|) and the
 // dt / alpha control (:116-131) in the system's last block.
-// NORD: the launch includes predictor-corrector systems (their corrector
-// holds three more derivative vectors; the other integrators' copy stays
-// leaner)
-template <bool NORD>
+// MOVES: the launch includes systems whose step b moves the atoms (the
+// predictor-corrector, whose corrector also holds three more derivative
+// vectors, and Brownian dynamics); the other integrators' copy stays leaner
+template <bool MOVES>
 __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
@@ -2313,11 +2314,32 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
         r[0] = q[1], r[1] = q[3], r[2] = q[5];
       }
       lkd_kick(S, om, F, r, v, a);
-    } else if (NORD && S.integ == IT_NORD) {
-      // the corrector moves the atom: do_pbc after integration_stepb
+    } else if (MOVES && (S.integ == IT_NORD || S.integ == IT_BROWN)) {
+      // the step moves the atom: do_pbc after integration_stepb
       // (src/Integration.F90:275-280); the next step's skin test sees it
       double4 x = A.pos[i];
-      nord_b_atom(A, S.dt, om, i, F, x, v, a);
+      if (S.integ == IT_NORD) {
+        nord_b_atom(A, S.dt, om, i, F, x, v, a);
+      } else {
+        // cbrownian (:855-882): one normal per coordinate, the first of a
+        // rang pair (the parity stream's layout; Philox: the same slots)
+        double r[3];
+        if (S.use_ext_normals) {
+          for (int k = 0; k < 3; k++) r[k] = A.ext_normals[(size_t)6 * i + 2 * k];
+        } else {
+          double q[6];
+          normals6((uint32_t)(i - S.off), st.step, S.seed, q);
+          r[0] = q[0], r[1] = q[2], r[2] = q[4];
+        }
+        const double osm = A.minv[i].y;
+        const double4 xo = x;
+        x.x = xo.x + om * S.bd_fac1 * F.x + osm * r[0] * S.bd_fac2;
+        x.y = xo.y + om * S.bd_fac1 * F.y + osm * r[1] * S.bd_fac2;
+        x.z = xo.z + om * S.bd_fac1 * F.z + osm * r[2] * S.bd_fac2;
+        v.x = (x.x - xo.x) / S.dt;
+        v.y = (x.y - xo.y) / S.dt;
+        v.z = (x.z - xo.z) / S.dt;
+      }
       wrap_atom(S, x);
       moved_atom(A, S, st, i, x, A.pos_old[i], A.type[i]);
     }

@@ -73,6 +73,7 @@ _SIGS = {
     "gemsgpu_set_slj": (_i, [_p, _i, _i, _i, _d, _d, _d]),
     "gemsgpu_set_wca": (_i, [_p, _i, _i, _i, _d, _d]),
     "gemsgpu_set_pred_corr": (_i, [_p, _i, _d]),
+    "gemsgpu_set_brownian": (_i, [_p, _i, _d, _d, _d, ctypes.c_uint64]),
     "gemsgpu_set_sm1": (_i, [_p, _i, _i, _i, _d, _d, _d]),
     "gemsgpu_set_feels": (_i, [_p, _i, _i, _i]),
     "gemsgpu_set_virial": (_i, [_p, _i, _i]),
@@ -522,6 +523,11 @@ class System:
     def set_ermak(self, dt, gama, temp, seed=12345):
         self._axes = []
         self._c(lib().gemsgpu_set_ermak(self.ctx.h, self.sid, float(dt), float(gama), float(temp), int(seed)))
+
+    def set_brownian(self, dt, temp, gama, seed=12345):
+        """`evolve brownian temp gama`: overdamped Langevin (cbrownian)."""
+        self._axes = []
+        self._c(lib().gemsgpu_set_brownian(self.ctx.h, self.sid, float(dt), float(temp), float(gama), int(seed)))
 
     def set_ermak_normals(self, nrm):
         a = None if nrm is None else _f64(nrm, 6 * self.n)

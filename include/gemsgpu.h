@@ -211,9 +211,16 @@ int gemsgpu_set_pred_corr(gemsgpu_ctx* ctx, int sys, double dt);
  * keyed by seed (production mode). */
 int gemsgpu_set_ermak(gemsgpu_ctx* ctx, int sys, double dt, double gamma,
                       double temp, uint64_t seed);
-/* Parity mode: the next step_a of an Ermak system consumes these normals
- * (6 per atom: r1,r2 for x, y, z in atom order, as rang() draws them in
- * ermak_a, Integration.F90:988-993) instead of the device stream. */
+/* `evolve brownian temp gama` (src/Integration.F90:146-149, 834-882):
+ * overdamped Langevin steps x += F/m dt/gamma + r sqrt(2 kB T dt/gamma / m),
+ * v = (x - x_old)/dt, all in step b.  dt (ps), T (K), gamma (1/ps); normals
+ * from the Philox stream keyed by seed, or the parity stream below. */
+int gemsgpu_set_brownian(gemsgpu_ctx* ctx, int sys, double dt, double temp,
+                         double gamma, uint64_t seed);
+/* Parity mode: the next step of an Ermak (step a) or Brownian (step b)
+ * system consumes these normals (6 per atom: r1,r2 for x, y, z in atom
+ * order, as rang() draws them in ermak_a, Integration.F90:988-993; cbrownian
+ * uses each pair's r1) instead of the device stream. */
 int gemsgpu_set_ermak_normals(gemsgpu_ctx* ctx, int sys,
                               const double* normals);
 /* FIRE (Bitzek 2006) with the per-atom mixing of FIRE.f90:107-114: dt0,

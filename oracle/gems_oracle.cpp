@@ -110,7 +110,8 @@ void rang(Lcg& s, double* r1, double* r2) {  // always draws a pair
 
 // ---------------------------------------------------------------- system
 enum FF { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3, FF_SLJ = 4 };
-enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6, IT_NORD = 7 };
+enum INTEG { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6, IT_NORD = 7,
+             IT_BROWN = 8 };
 
 // One integrator acting on one coordinate of every atom (integrate objects
 // set by `evolve piston_lgf x|y|z` and `evolve ermak_x|y|z`,
@@ -202,6 +203,7 @@ struct Sys {
   double cc0 = 0, cc1 = 0, cc2 = 0, sdr = 0, sdv = 0, crv1 = 0, crv2 = 0,
          skt = 0, gama = 0, temp = 0;
   Lcg* rng = nullptr;
+  double bd_fac1 = 0, bd_fac2 = 0;  // set_cbrownian (Integration.F90:834-853)
   const double* ext_normals = nullptr;  // optional external normal stream
   // G-JF constant-pressure state (set_lgf, Integration.F90:486-525)
   double lgf_fac0 = 0, lgf_facg0 = 0, lgf_kinetic = 0, lgf_press = 0, lgf_inv_pmass = 0, lgf_bv = 0,
@@ -897,6 +899,25 @@ void nord_b(Sys& s) {
   }
 }
 
+// cbrownian (Integration.F90:855-882), the step b of `evolve brownian`
+// (step a does nothing): x += F/m dt/gamma + r sqrt(2 kT dt/gamma / m) with
+// r the first normal of a rang pair per coordinate; v = (x - x_old) / dt
+void brownian_b(Sys& s) {
+  for (int i = 0; i < s.n; i++)
+    for (int j = 0; j < 3; j++) {
+      double r1, r2;
+      if (s.ext_normals) {
+        r1 = s.ext_normals[6 * i + 2 * j];
+      } else {
+        rang(*s.rng, &r1, &r2);
+      }
+      const int q = 3 * i + j;
+      const double posold = s.pos[q];
+      s.pos[q] = posold + s.one_mass[i] * s.bd_fac1 * s.force[q] + s.one_sqrt_mass[i] * r1 * s.bd_fac2;
+      s.vel[q] = (s.pos[q] - posold) / s.dt;
+    }
+}
+
 // ermak_a (Integration.F90:963-1011).  Normals come from the LCG stream
 // (rang, one pair per dimension) or from an external stream of 6 per atom.
 void ermak_a(Sys& s) {
@@ -1292,6 +1313,7 @@ void stepb(Sys& s) {
   else if (s.integ == IT_AXES) axes_b(s);
   else if (s.integ == IT_LKD) lkd_b(s);
   else if (s.integ == IT_NORD) nord_b(s);
+  else if (s.integ == IT_BROWN) brownian_b(s);
   do_pbc(s);
   if (s.integ == IT_FIRE) fire_mix(s);
 }
@@ -1981,6 +2003,15 @@ void orc_ermak_consts(void* p, double* out8) {
   out8[4] = s->sdv; out8[5] = s->crv1; out8[6] = s->crv2; out8[7] = s->skt;
 }
 void orc_set_ext_normals(void* p, const double* nrm) { ((Sys*)p)->ext_normals = nrm; }
+// set_cbrownian (Integration.F90:834-853): `evolve brownian temp gama`
+void orc_set_brownian(void* p, double dt, double temp, double gama, void* rng) {
+  Sys* s = (Sys*)p;
+  s->integ = IT_BROWN;
+  s->dt = dt;
+  s->bd_fac1 = dt / gama;
+  s->bd_fac2 = std::sqrt(2.0 * kB_ui * temp * s->bd_fac1);
+  s->rng = (Lcg*)rng;
+}
 void orc_set_fire(void* p, double dt0, double dtmax) { fire_init(*(Sys*)p, dt0, dtmax); }
 double orc_fire_dt(void* p) { return ((Sys*)p)->fire_dt; }
 double orc_fmax(void* p) { return fmax_ev(*(Sys*)p); }

@@ -95,6 +95,7 @@ def lib():
         "orc_set_sm1": (None, [_p, _i, _i, _d, _d, _d]),
         "orc_set_feels": (None, [_p, _i, _i]),
         "orc_set_pred_corr": (None, [_p, _d]),
+        "orc_set_brownian": (None, [_p, _d, _d, _d, _p]),
         "orc_get_derivs": (None, [_p, _dp]),
         "orc_set_derivs": (None, [_p, _dp]),
         "orc_set_lgf": (None, [_p, _d, _d, _d, _d, _d, _d, _p]),
@@ -285,6 +286,11 @@ class System:
     def set_pred_corr(self, dt):
         """`evolve pred_corr_5`: the fifth-order Nordsieck predictor-corrector."""
         lib().orc_set_pred_corr(self.h, float(dt))
+
+    def set_brownian(self, dt, temp, gama, rng):
+        """`evolve brownian temp gama` (set_cbrownian / cbrownian)."""
+        self._rng = rng
+        lib().orc_set_brownian(self.h, float(dt), float(temp), float(gama), rng.h)
 
     def derivs(self):
         """acel, acel2, acel3, acel4 as a (4, n, 3) array."""

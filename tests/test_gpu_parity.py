@@ -393,6 +393,49 @@ def test_gpu_pred_corr_derivatives_and_resume(ctx):
     h.destroy()
 
 
+def test_gpu_brownian_parity_stream(ctx):
+    """examples/NVT/brownian.gms (the gas, tempgdist 300, `evolve brownian
+    300 10`) on the oracle's LCG stream: 500 steps on the device against
+    the oracle's own run, row by row."""
+    pos, vel, types, mass, box, rng_g = decks.he_ne_setup(O)
+    g = _he_ne_gpu(ctx)
+    g.set_brownian(0.002, 300.0, 10.0)
+    rows = decks.ermak_parity_run(g, rng_g, 500, 100)
+    _, _, _, _, _, rng_o = decks.he_ne_setup(O)
+    s = O.System(pos, mass, types, 2)
+    s.set_box(box, (True, True, True))
+    s.set_vel(vel)
+    decks.apply_plj(s)
+    s.set_brownian(0.002, 300.0, 10.0, rng_o)
+    want = s.dinamica(500, 100)
+    np.testing.assert_allclose(rows[:, :3] * gems.UI_EV, want[:, :3], rtol=1e-9)
+    np.testing.assert_allclose(rows[:, 3], want[:, 3], rtol=1e-9)
+    np.testing.assert_allclose(g.pos, s.pos, rtol=0, atol=1e-9)
+    g.destroy()
+
+
+def test_gpu_brownian_philox(ctx):
+    """Brownian dynamics on the device stream: the displacement noise of a
+    step has variance 2 kB T dt / (gamma m) per coordinate (force-free
+    atoms: a dilute gas far beyond the cut-off)."""
+    n = 4000
+    rng = np.random.default_rng(9)
+    pos = rng.uniform(0.0, 400.0, (n, 3))
+    g = gpu_ref_sys(pos, 4.0032, ctx=ctx)
+    g.set_box((400.0, 400.0, 400.0), (True, True, True))
+    g.set_lj(1e-6, 1.0, 1.5)
+    dt, temp, gama = 0.002, 300.0, 10.0
+    g.set_brownian(dt, temp, gama, seed=77)
+    g.dinamica(1, 1)
+    v = g.vel
+    d = v * dt
+    kB_ui = O.lib().orc_kB_ui()
+    var = 2.0 * kB_ui * temp * dt / gama / 4.0032
+    assert abs(d.var() / var - 1.0) < 0.05
+    assert abs(d.mean()) < 4.0 * np.sqrt(var / d.size)
+    g.destroy()
+
+
 def test_gpu_nvt_plj_parity_stream(ctx):
     pos, vel, types, mass, box, rng = decks.he_ne_setup(O)
     g = gpu_ref_sys(pos, mass, types, 2, ctx=ctx, vel=vel)

@@ -166,6 +166,36 @@ def test_nve_plj_pred_corr_5():
     np.testing.assert_allclose(r[:, 1:3], ref[:, 1:3], rtol=1e-6)
 
 
+def test_brownian_zero_temperature_descends():
+    """cbrownian at T = 0 is steepest descent, x += F/m dt/gamma: the
+    potential energy of the gas of brownian.gms falls step after step, and
+    v = (x - x_old)/dt."""
+    rng = O.Rng(123456)
+    pos, types, mass, box = decks.he_ne_gas(rng)
+    s = O.System(pos, mass, types, 2)
+    s.set_box(box, (True, True, True))
+    for (a, b), (e, sg) in decks.plj_params().items():
+        s.set_lj(e, sg, 10.0, a, b, shifted_force=True)
+    s.set_brownian(0.002, 0.0, 10.0, rng)
+    s.interact()
+    e_prev = s.epot_sum()
+    for _ in range(20):
+        x0 = s.pos.copy()
+        s.stepa()
+        s.interact()
+        f = s.force.copy()
+        s.stepb()
+        s.interact()
+        e = s.epot_sum()
+        assert e < e_prev
+        e_prev = e
+        dx = f / mass[:, None] * (0.002 / 10.0)
+        # (x - x_old)/dt cancels: |x| ~ 50 A against steps of ~1e-7 A
+        np.testing.assert_allclose(s.vel, dx / 0.002, rtol=1e-6, atol=1e-10)
+        wrapped = np.abs(s.pos - x0 - dx) > 1.0
+        np.testing.assert_allclose((s.pos - x0)[~wrapped], dx[~wrapped], rtol=1e-9, atol=1e-13)
+
+
 def test_nvt_plj_ermak():
     """examples/NVT/ermak.gms: same gas under Ermak (gamma=10/ps, 300 K)."""
     r, ref = _he_ne("nvt")
