@@ -300,7 +300,7 @@ def test_gpu_feels_guards(ctx):
     g.set_wca(1.0, 0.95, ti=1, tj=0)
     g.set_feels(1, 0)
     g.interact()
-    f = g.force()
+    f = g.force
     assert np.all(f[0] == 0.0) and f[1, 0] > 0.0 and np.all(f[2] == 0.0)
     with pytest.raises(gems.GemsGpuError):
         g.set_virial(True)
@@ -418,9 +418,8 @@ def test_gpu_brownian_philox(ctx):
     """Brownian dynamics on the device stream: the displacement noise of a
     step has variance 2 kB T dt / (gamma m) per coordinate (force-free
     atoms: a dilute gas far beyond the cut-off)."""
-    n = 4000
-    rng = np.random.default_rng(9)
-    pos = rng.uniform(0.0, 400.0, (n, 3))
+    k = np.arange(16) * 25.0 + 5.0
+    pos = np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 3)
     g = gpu_ref_sys(pos, 4.0032, ctx=ctx)
     g.set_box((400.0, 400.0, 400.0), (True, True, True))
     g.set_lj(1e-6, 1.0, 1.5)
