@@ -291,6 +291,36 @@ def test_gpu_lj_family_decks(ctx, kind):
     np.testing.assert_allclose(got, orc, atol=1e-12, rtol=1e-9)
 
 
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_gpu_wca_feels_fluid(ctx, prec, rms, etol):
+    """A dense two-species WCA fluid (2048 atoms, periodic, linked cells)
+    where species 1 feels species 0 one-sidedly and an sm1 well binds
+    species 1 to itself: forces and per-atom energies against the oracle
+    (FP64 and, without sm1, mixed)."""
+    rng = np.random.default_rng(21)
+    a = 1.6
+    k = np.arange(8) * a
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]]) * a
+    pos = (np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 1, 3) + base).reshape(-1, 3)
+    pos = pos + rng.normal(0.0, 0.05, pos.shape)
+    types = np.arange(len(pos)) % 2
+    L = 8 * a
+
+    def setup(s):
+        s.set_box((L, L, L), (True, True, True))
+        s.set_wca(1.0, 1.0, ti=0, tj=0)
+        s.set_wca(0.5, 1.05, ti=1, tj=0)
+        s.set_feels(1, 0)
+        if prec == 0:
+            s.set_sm1(1.0, 1.9, 0.2, ti=1, tj=1)
+        else:
+            s.set_wca(0.8, 0.95, ti=1, tj=1)
+    o, g = both(pos, 39.95, ctx, types, 2, setup=setup)
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+    g.destroy()
+
+
 def test_gpu_feels_guards(ctx):
     """One-sided pairs: forces on the feeling type only; no virial, no
     piston; sm1 stays FP64."""
