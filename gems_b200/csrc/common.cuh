@@ -33,6 +33,10 @@ __device__ __forceinline__ void stencil(int k, int& dx, int& dy, int& dz) {
 }
 
 enum FF : int { FF_NONE = 0, FF_LJ = 1, FF_SMATB = 2, FF_TERSOFF = 3 };
+// thermostats run after the integrator's step b (`evolve scalvel`,
+// `scalvel_after`, `andersen`)
+enum TH : int { TH_NONE = 0, TH_SCALVEL = 1, TH_SCALVEL_AFTER = 2, TH_ANDERSEN = 3 };
+
 enum IT : int { IT_NONE = 0, IT_VV = 1, IT_ERMAK = 2, IT_FIRE = 3, IT_LGF = 4, IT_AXES = 5, IT_LKD = 6, IT_NORD = 7,
                 IT_BROWN = 8 };
 // IT_AXES: one integrator per coordinate -- a G-JF piston on that box length
@@ -86,6 +90,11 @@ struct SysDev {
   double dt;
   double cc0, cc1, cc2, sdr, sdv, crv1, crv2, skt;
   double bd_fac1, bd_fac2;  // set_cbrownian (Integration.F90:834-853): dt/gamma, sqrt(2 kB T dt/gamma)
+  // thermostat: scalvel T0, soft = 0.5/steps, upto (scalvel_after), kB_ui;
+  // andersen sqrt(kB T)/(3N), nu
+  int thermo, pad_th;
+  double th[4];
+  uint64_t th_seed;
   uint64_t seed;
   double fire_dtmax, fire_fmax;
   int fire_maxit, pad1;
@@ -147,6 +156,7 @@ struct SysState {
   // (the piston velocity is lgf_pvel; the fed piston normals of stepa and
   // stepb are ax_ext[0] and ax_ext[1])
   double lkd_bo[3], lkd_bh[3], lkd_bf[3];
+  double th_factor;  // scalvel: this step's velocity factor
 };
 
 // Block map: block b covers atoms [first[b], end[b]) of system sys[b];

@@ -835,6 +835,7 @@ bool can_fuse_steps(const gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   for (int s : ss) {
     const int it = ctx->sys[s].d.integ;
     if (it != IT_VV && it != IT_ERMAK) return false;
+    if (ctx->sys[s].d.thermo != TH_NONE) return false;  // it runs between the two
   }
   return true;
 }
@@ -904,11 +905,25 @@ int launch_forces_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss, cudaGraphCond
 int launch_step_b(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   BlockMap ma;
   CHK(get_map(ctx, ss, BLOCK, 0, &ma));
-  bool moves = false;
-  for (int s : ss) moves |= ctx->sys[s].d.integ == IT_NORD || ctx->sys[s].d.integ == IT_BROWN;
+  bool moves = false, thermo = false, scal = false;
+  for (int s : ss) {
+    const SysDev& d = ctx->sys[s].d;
+    moves |= d.integ == IT_NORD || d.integ == IT_BROWN;
+    thermo |= d.thermo != TH_NONE;
+    scal |= d.thermo == TH_SCALVEL || d.thermo == TH_SCALVEL_AFTER;
+  }
   if (moves) k_step_b<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
   else k_step_b<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
   ++ctx->launches;
+  // the thermostats after the integrator's stepb
+  if (scal) {
+    k_thermo_sum<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+    ++ctx->launches;
+  }
+  if (thermo) {
+    k_thermo_apply<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+    ++ctx->launches;
+  }
   CU(cudaGetLastError());
   return 0;
 }
@@ -2256,6 +2271,51 @@ int gemsgpu_set_pred_corr(gemsgpu_ctx* ctx, int sys, double dt) {
   SysHost& h = ctx->sys[sys];
   h.d.integ = IT_NORD;
   h.d.dt = dt;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+// `evolve scalvel temp steps` and `evolve scalvel_after temp steps upto`
+// (src/Integration.F90:205-213, set_scalvel :1271-1298): after the system's
+// integrator, v *= (T0/T)^(0.5/steps) every step (scalvel_after: only while
+// |T - T0| > upto T0).  upto < 0 selects scalvel.
+int gemsgpu_set_scalvel(gemsgpu_ctx* ctx, int sys, double temp, int steps, double upto) {
+  CHK(check_sys(ctx, sys));
+  if (!(temp >= 0.0) || steps < 1) return fail(ctx, GEMSGPU_ERR_ARG, "set_scalvel: T >= 0, steps >= 1");
+  SysDev& d = ctx->sys[sys].d;
+  d.thermo = upto < 0.0 ? TH_SCALVEL : TH_SCALVEL_AFTER;
+  d.th[0] = temp;
+  d.th[1] = 0.5 / steps;
+  d.th[2] = upto;
+  d.th[3] = kB_ui;
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+// `evolve andersen temp [nu]` (src/Integration.F90:214-217, set_andersen
+// :1343-1364): after the system's integrator, each atom collides with
+// probability nu dt and takes new velocities of scale sqrt(kB T / (3N)^2)
+// / sqrt(m) (the reference's factor), from a Philox stream keyed by seed.
+int gemsgpu_set_andersen(gemsgpu_ctx* ctx, int sys, double temp, double nu, uint64_t seed) {
+  CHK(check_sys(ctx, sys));
+  if (!(temp >= 0.0) || !(nu >= 0.0)) return fail(ctx, GEMSGPU_ERR_ARG, "set_andersen: T >= 0, nu >= 0");
+  SysHost& h = ctx->sys[sys];
+  SysDev& d = h.d;
+  d.thermo = TH_ANDERSEN;
+  const double dof = 3.0 * h.n;
+  d.th[0] = std::sqrt(kB_ui * temp / (dof * dof));
+  d.th[1] = nu;
+  d.th_seed = seed ^ 0x9E3779B97F4A7C15ull;  // apart from the integrator's stream
+  CHK(push_sys(ctx, sys));
+  invalidate(ctx);
+  return 0;
+}
+
+int gemsgpu_clear_thermostat(gemsgpu_ctx* ctx, int sys) {
+  CHK(check_sys(ctx, sys));
+  ctx->sys[sys].d.thermo = TH_NONE;
   CHK(push_sys(ctx, sys));
   invalidate(ctx);
   return 0;

@@ -776,6 +776,87 @@ __device__ __forceinline__ void virial_close(Arena& A, const BlockMap& M, int s,
   sys6_close(A, M, s, w, A.st[s].vir);
 }
 
+// Thermostats after step b (integration_stepb runs every integrator's stepb
+// in the order the deck adds them, src/Integration.F90:264-275).
+// scalvel / scalvel_after (:1300-1340): the system's centre-of-mass-free
+// kinetic energy (inq_kin_energy / inq_temperature,
+// Inq_Properties.F90:399-434: sum m |v - v_cm|^2 = sum m v^2 - M |v_cm|^2)
+// gives T and the factor (T0/T)^soft, applied by k_thermo_apply; one atom
+// alone has no kinetic energy about its centre of mass and is not scaled.
+__global__ void k_thermo_sum(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  const SysDev& S = A.sys[s];
+  if (S.thermo != TH_SCALVEL && S.thermo != TH_SCALVEL_AFTER) return;  // the whole system's blocks
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  double w[5] = {0, 0, 0, 0, 0};
+  if (i < M.end[blockIdx.x]) {
+    const double4 v = A.vel[i];
+    const double m = A.mass[i];
+    w[0] = m;
+    w[1] = m * v.x;
+    w[2] = m * v.y;
+    w[3] = m * v.z;
+    w[4] = m * (v.x * v.x + v.y * v.y + v.z * v.z);
+  }
+  double b[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) b[k] = block_sum(w[k]);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 5; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = b[k];
+  if (last_block(M, A.st, s, &A.st[s].ticket2) && threadIdx.x < 32) {
+    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+    double t[5] = {0, 0, 0, 0, 0};
+    for (int q = threadIdx.x; q < nb; q += 32)
+#pragma unroll
+      for (int k = 0; k < 5; k++) t[k] += __ldcg(&A.blk_red[8 * (b0 + q) + k]);
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+      for (int o = 16; o; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+    if (threadIdx.x == 0) {
+      double ek = 0.0;
+      if (S.n > 1) ek = 0.5 * (t[4] - (t[1] * t[1] + t[2] * t[2] + t[3] * t[3]) / t[0]);
+      const double T = 2.0 * ek / (S.th[3] * (3 * S.n));
+      const double T0 = S.th[0];
+      double f = 1.0;
+      if (T != 0.0 && (S.thermo == TH_SCALVEL || fabs(T - T0) > S.th[2] * T0)) f = pow(T0 / T, S.th[1]);
+      A.st[s].th_factor = f;
+    }
+  }
+}
+
+// scalvel: v *= factor.  andersen (:1366-1395): each atom collides with
+// probability nu dt and takes v = th[0] / sqrt(m) r per coordinate, th[0]
+// the reference's sqrt(kB T / (3N)^2) (set_andersen, :1343-1364); the
+// uniform and the normals come from the thermostat's own Philox stream.
+__global__ void k_thermo_apply(Arena A, BlockMap M) {
+  int s = blk_sys(M);
+  if (s < 0) return;  // padding block of a fixed-capacity map
+  const SysDev& S = A.sys[s];
+  int i = M.first[blockIdx.x] + threadIdx.x;
+  if (S.thermo == TH_NONE || i >= M.end[blockIdx.x]) return;
+  if (S.thermo == TH_ANDERSEN) {
+    const uint64_t step = A.st[s].step;
+    const uint2 key = make_uint2((uint32_t)S.th_seed, (uint32_t)(S.th_seed >> 32));
+    const uint4 c = philox10(make_uint4((uint32_t)(i - S.off), (uint32_t)step, (uint32_t)(step >> 32), 7u), key);
+    const double u = ((double)(c.x >> 8) + 0.5) * 5.9604644775390625e-8;  // (0, 1)
+    if (u > S.th[1] * S.dt) return;
+    double r[6];
+    normals6((uint32_t)(i - S.off), step, S.th_seed, r);
+    const double vm = S.th[0] * A.minv[i].y;
+    A.vel[i] = make_double4(vm * r[0], vm * r[2], vm * r[4], 0.0);
+  } else {
+    const double f = A.st[s].th_factor;
+    if (f != 1.0) {
+      double4 v = A.vel[i];
+      v.x = v.x * f;
+      v.y = v.y * f;
+      v.z = v.z * f;
+      A.vel[i] = v;
+    }
+  }
+}
+
 // kinetic tensor sum_i m v (x) v of each system (inq_pressure,
 // Inq_Properties.F90:529-573), into SysState::ktens
 __global__ void k_kin_tensor(Arena A, BlockMap M) {
@@ -2087,9 +2168,10 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
         atomicOr(A.any_rebuild, 1);
         if constexpr (COND) cudaGraphSetConditional(cond, 1u);
       }
-      if ((S.integ == IT_ERMAK || S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD ||
-           S.integ == IT_BROWN) &&
-          !S.use_ext_normals)
+      if (((S.integ == IT_ERMAK || S.integ == IT_LGF || S.integ == IT_AXES || S.integ == IT_LKD ||
+            S.integ == IT_BROWN) &&
+           !S.use_ext_normals) ||
+          S.thermo == TH_ANDERSEN)
         st.step++;
       if (S.integ == IT_FIRE) st.fire_zero = 0;
     }

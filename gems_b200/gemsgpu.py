@@ -74,6 +74,9 @@ _SIGS = {
     "gemsgpu_set_wca": (_i, [_p, _i, _i, _i, _d, _d]),
     "gemsgpu_set_pred_corr": (_i, [_p, _i, _d]),
     "gemsgpu_set_brownian": (_i, [_p, _i, _d, _d, _d, ctypes.c_uint64]),
+    "gemsgpu_set_scalvel": (_i, [_p, _i, _d, _i, _d]),
+    "gemsgpu_set_andersen": (_i, [_p, _i, _d, _d, ctypes.c_uint64]),
+    "gemsgpu_clear_thermostat": (_i, [_p, _i]),
     "gemsgpu_set_sm1": (_i, [_p, _i, _i, _i, _d, _d, _d]),
     "gemsgpu_set_feels": (_i, [_p, _i, _i, _i]),
     "gemsgpu_set_virial": (_i, [_p, _i, _i]),
@@ -528,6 +531,19 @@ class System:
         """`evolve brownian temp gama`: overdamped Langevin (cbrownian)."""
         self._axes = []
         self._c(lib().gemsgpu_set_brownian(self.ctx.h, self.sid, float(dt), float(temp), float(gama), int(seed)))
+
+    def set_scalvel(self, temp, steps, upto=None):
+        """`evolve scalvel temp steps` (scalvel_after with upto), run after
+        the integrator's step b."""
+        self._c(lib().gemsgpu_set_scalvel(self.ctx.h, self.sid, float(temp), int(steps),
+                                          -1.0 if upto is None else float(upto)))
+
+    def set_andersen(self, temp, nu=20.0, seed=4242):
+        """`evolve andersen temp nu`, run after the integrator's step b."""
+        self._c(lib().gemsgpu_set_andersen(self.ctx.h, self.sid, float(temp), float(nu), int(seed)))
+
+    def clear_thermostat(self):
+        self._c(lib().gemsgpu_clear_thermostat(self.ctx.h, self.sid))
 
     def set_ermak_normals(self, nrm):
         a = None if nrm is None else _f64(nrm, 6 * self.n)

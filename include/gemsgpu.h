@@ -217,6 +217,20 @@ int gemsgpu_set_ermak(gemsgpu_ctx* ctx, int sys, double dt, double gamma,
  * from the Philox stream keyed by seed, or the parity stream below. */
 int gemsgpu_set_brownian(gemsgpu_ctx* ctx, int sys, double dt, double temp,
                          double gamma, uint64_t seed);
+/* Thermostats that run after the system's integrator, as a second `evolve`
+ * line does (integration_stepb, src/Integration.F90:264-275).  scalvel
+ * (set_scalvel :1271-1340): v *= (T0/T)^(0.5/steps) every step, T from the
+ * centre-of-mass-free kinetic energy; upto >= 0 selects scalvel_after,
+ * which scales only while |T - T0| > upto T0; upto < 0 selects scalvel. */
+int gemsgpu_set_scalvel(gemsgpu_ctx* ctx, int sys, double temp, int steps,
+                        double upto);
+/* andersen (set_andersen / andersen, :1343-1395): each atom collides with
+ * probability nu dt (nu in 1/ps; the deck's default is 20) and takes
+ * velocities of scale sqrt(kB T / (3N)^2) / sqrt(m), the reference's factor;
+ * Philox stream keyed by seed. */
+int gemsgpu_set_andersen(gemsgpu_ctx* ctx, int sys, double temp, double nu,
+                         uint64_t seed);
+int gemsgpu_clear_thermostat(gemsgpu_ctx* ctx, int sys);
 /* Parity mode: the next step of an Ermak (step a) or Brownian (step b)
  * system consumes these normals (6 per atom: r1,r2 for x, y, z in atom
  * order, as rang() draws them in ermak_a, Integration.F90:988-993; cbrownian

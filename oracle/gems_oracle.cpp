@@ -204,6 +204,10 @@ struct Sys {
          skt = 0, gama = 0, temp = 0;
   Lcg* rng = nullptr;
   double bd_fac1 = 0, bd_fac2 = 0;  // set_cbrownian (Integration.F90:834-853)
+  // thermostat run after the integrator's step b (integration_stepb runs
+  // every integrator's stepb in the order the deck adds them)
+  int thermo = 0;  // 0 none, 1 scalvel, 2 scalvel_after, 3 andersen
+  double th_temp = 0, th_soft = 0, th_upto = 0, th_factor = 0, th_nu = 0;
   const double* ext_normals = nullptr;  // optional external normal stream
   // G-JF constant-pressure state (set_lgf, Integration.F90:486-525)
   double lgf_fac0 = 0, lgf_facg0 = 0, lgf_kinetic = 0, lgf_press = 0, lgf_inv_pmass = 0, lgf_bv = 0,
@@ -918,6 +922,38 @@ void brownian_b(Sys& s) {
     }
 }
 
+void kin(const Sys& s, double* ekin, double* temp);
+
+// scalvel / scalvel_after (Integration.F90:1300-1340): v *= (T0/T)^soft
+// with T from the centre-of-mass-free kinetic energy (inq_temperature,
+// Inq_Properties.F90:424-434); scalvel_after only when |T - T0| > upto T0
+void scalvel(Sys& s) {
+  double ek, t;
+  kin(s, &ek, &t);
+  if (s.thermo == 2 && !(std::fabs(t - s.th_temp) > s.th_upto * s.th_temp)) return;
+  if (t == 0.0) return;
+  const double factor = std::pow(s.th_temp / t, s.th_soft);
+  for (int q = 0; q < 3 * s.n; q++) s.vel[q] = s.vel[q] * factor;
+}
+
+// andersen (Integration.F90:1366-1395): each atom collides with
+// probability nu dt (one ranu per atom) and takes v = factor / sqrt(m) r
+// per coordinate (r the first normal of a rang pair), with the reference's
+// factor = sqrt(kB T / (3N)^2) (set_andersen, :1343-1364)
+void andersen(Sys& s) {
+  const double nudt = s.th_nu * s.dt;
+  for (int i = 0; i < s.n; i++) {
+    const double r = lcg_ranu(*s.rng);
+    if (r > nudt) continue;
+    const double vel_med = s.th_factor * s.one_sqrt_mass[i];
+    for (int j = 0; j < 3; j++) {
+      double r1, r2;
+      rang(*s.rng, &r1, &r2);
+      s.vel[3 * i + j] = vel_med * r1;
+    }
+  }
+}
+
 // ermak_a (Integration.F90:963-1011).  Normals come from the LCG stream
 // (rang, one pair per dimension) or from an external stream of 6 per atom.
 void ermak_a(Sys& s) {
@@ -1314,6 +1350,8 @@ void stepb(Sys& s) {
   else if (s.integ == IT_LKD) lkd_b(s);
   else if (s.integ == IT_NORD) nord_b(s);
   else if (s.integ == IT_BROWN) brownian_b(s);
+  if (s.thermo == 1 || s.thermo == 2) scalvel(s);
+  else if (s.thermo == 3) andersen(s);
   do_pbc(s);
   if (s.integ == IT_FIRE) fire_mix(s);
 }
@@ -2003,6 +2041,25 @@ void orc_ermak_consts(void* p, double* out8) {
   out8[4] = s->sdv; out8[5] = s->crv1; out8[6] = s->crv2; out8[7] = s->skt;
 }
 void orc_set_ext_normals(void* p, const double* nrm) { ((Sys*)p)->ext_normals = nrm; }
+// `evolve scalvel temp steps` / `evolve scalvel_after temp steps upto`
+// (set_scalvel, Integration.F90:1271-1298); upto < 0 selects scalvel
+void orc_set_scalvel(void* p, double temp, int steps, double upto) {
+  Sys* s = (Sys*)p;
+  s->thermo = upto < 0.0 ? 1 : 2;
+  s->th_temp = temp;
+  s->th_soft = 0.5 / steps;
+  s->th_upto = upto;
+}
+// `evolve andersen temp [nu]` (set_andersen, Integration.F90:1343-1364)
+void orc_set_andersen(void* p, double temp, double nu, void* rng) {
+  Sys* s = (Sys*)p;
+  s->thermo = 3;
+  s->th_factor = std::sqrt(kB_ui * temp / ((s->n * 3.0) * (s->n * 3.0)));
+  s->th_nu = nu;
+  s->rng = (Lcg*)rng;
+}
+void orc_clear_thermostat(void* p) { ((Sys*)p)->thermo = 0; }
+
 // set_cbrownian (Integration.F90:834-853): `evolve brownian temp gama`
 void orc_set_brownian(void* p, double dt, double temp, double gama, void* rng) {
   Sys* s = (Sys*)p;

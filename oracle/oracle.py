@@ -96,6 +96,9 @@ def lib():
         "orc_set_feels": (None, [_p, _i, _i]),
         "orc_set_pred_corr": (None, [_p, _d]),
         "orc_set_brownian": (None, [_p, _d, _d, _d, _p]),
+        "orc_set_scalvel": (None, [_p, _d, _i, _d]),
+        "orc_set_andersen": (None, [_p, _d, _d, _p]),
+        "orc_clear_thermostat": (None, [_p]),
         "orc_get_derivs": (None, [_p, _dp]),
         "orc_set_derivs": (None, [_p, _dp]),
         "orc_set_lgf": (None, [_p, _d, _d, _d, _d, _d, _d, _p]),
@@ -291,6 +294,19 @@ class System:
         """`evolve brownian temp gama` (set_cbrownian / cbrownian)."""
         self._rng = rng
         lib().orc_set_brownian(self.h, float(dt), float(temp), float(gama), rng.h)
+
+    def set_scalvel(self, temp, steps, upto=None):
+        """`evolve scalvel temp steps` (or scalvel_after with upto), run
+        after the integrator's step b."""
+        lib().orc_set_scalvel(self.h, float(temp), int(steps), -1.0 if upto is None else float(upto))
+
+    def set_andersen(self, temp, nu, rng):
+        """`evolve andersen temp nu`, run after the integrator's step b."""
+        self._rng2 = rng
+        lib().orc_set_andersen(self.h, float(temp), float(nu), rng.h)
+
+    def clear_thermostat(self):
+        lib().orc_clear_thermostat(self.h)
 
     def derivs(self):
         """acel, acel2, acel3, acel4 as a (4, n, 3) array."""

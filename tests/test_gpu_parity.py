@@ -465,6 +465,56 @@ def test_gpu_brownian_philox(ctx):
     g.destroy()
 
 
+@pytest.mark.parametrize("upto", [None, 0.02])
+def test_gpu_scalvel_matches_oracle(ctx, upto):
+    """scalvel (and scalvel_after with a narrow band) after velocity Verlet
+    on the gas of v_verlet.gms, toward 250 K: the device's md_steps rows
+    against the oracle's."""
+    pos, vel, types, mass, box, _ = decks.he_ne_setup(O)
+    g = _he_ne_gpu(ctx)
+    g.set_vv(0.002)
+    g.set_scalvel(250.0, 10, upto)
+    rows = g.dinamica(400, 50)
+    s = O.System(pos, mass, types, 2)
+    s.set_box(box, (True, True, True))
+    s.set_vel(vel)
+    decks.apply_plj(s)
+    s.set_vv(0.002)
+    s.set_scalvel(250.0, 10, upto)
+    want = s.dinamica(400, 50)
+    np.testing.assert_allclose(rows[:, :4], want[:, :4], rtol=1e-8)
+    assert abs(rows[-1, 3] - 250.0) < 0.1 * 250.0
+    g.destroy()
+
+
+def test_gpu_andersen_statistics(ctx):
+    """andersen after velocity Verlet, force-free atoms: with nu dt = 1/4 a
+    quarter of the atoms collide per step; with nu dt = 1 every atom does
+    and m v^2 averages the reference's kB T / (3N)^2 per coordinate."""
+    k = np.arange(16) * 25.0 + 5.0
+    pos = np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 3)
+    n = len(pos)
+    vel = np.tile([1e-3, 2e-3, 3e-3], (n, 1))
+    g = gpu_ref_sys(pos, 4.0032, ctx=ctx, vel=vel)
+    g.set_box((400.0, 400.0, 400.0), (True, True, True))
+    g.set_lj(1e-6, 1.0, 1.5)
+    g.set_vv(0.002)
+    g.set_andersen(300.0, 0.25 / 0.002, seed=5)
+    g.dinamica(1, 1)
+    hit = np.any(g.vel != vel, axis=1)
+    assert abs(hit.mean() - 0.25) < 0.03
+    g.set_andersen(300.0, 1.0 / 0.002, seed=6)
+    kB_ui = O.lib().orc_kB_ui()
+    want = kB_ui * 300.0 / (3.0 * n) ** 2
+    m2 = []
+    for _ in range(3):
+        g.dinamica(1, 1)
+        m2.append((g.vel ** 2 * 4.0032).ravel())
+    assert abs(np.concatenate(m2).mean() / want - 1.0) < 0.05
+    g.clear_thermostat()
+    g.destroy()
+
+
 def test_gpu_nvt_plj_parity_stream(ctx):
     pos, vel, types, mass, box, rng = decks.he_ne_setup(O)
     g = gpu_ref_sys(pos, mass, types, 2, ctx=ctx, vel=vel)

@@ -196,6 +196,54 @@ def test_brownian_zero_temperature_descends():
         np.testing.assert_allclose((s.pos - x0)[~wrapped], dx[~wrapped], rtol=1e-9, atol=1e-13)
 
 
+def _gas_vv():
+    rng = O.Rng(123456)
+    pos, types, mass, box = decks.he_ne_gas(rng)
+    s = O.System(pos, mass, types, 2)
+    s.set_box(box, (True, True, True))
+    for (a, b), (e, sg) in decks.plj_params().items():
+        s.set_lj(e, sg, 10.0, a, b, shifted_force=True)
+    s.remove_cm()
+    s.gdist(rng, 300.0)
+    s.set_vv(0.002)
+    s.mass = mass
+    return s, rng
+
+
+def test_scalvel_thermostat():
+    """scalvel after velocity Verlet: with steps = 1 the factor is
+    sqrt(T0/T), so every step ends at T0; scalvel_after with a band wider
+    than the run's fluctuations never acts, leaving plain VV."""
+    s, _ = _gas_vv()
+    s.set_scalvel(250.0, 1)
+    r = s.dinamica(50, 10)
+    np.testing.assert_allclose(r[:, 3], 250.0, rtol=1e-12)
+    a, _ = _gas_vv()
+    b, _ = _gas_vv()
+    b.set_scalvel(300.0, 5, upto=0.9)
+    np.testing.assert_array_equal(a.dinamica(200, 50), b.dinamica(200, 50))
+    c, _ = _gas_vv()
+    c.set_scalvel(100.0, 5, upto=0.1)
+    rc = c.dinamica(200, 200)
+    assert abs(rc[-1, 3] - 100.0) <= 0.1 * 100.0 + 1e-9
+
+
+def test_andersen_thermostat():
+    """andersen with nu dt = 1: every atom collides every step and its new
+    velocity has m v^2 = kB T / (3N)^2 per coordinate on average (the
+    reference's factor), from the LCG stream."""
+    s, rng = _gas_vv()
+    s.set_andersen(300.0, 1.0 / 0.002, rng)
+    kB_ui = O.lib().orc_kB_ui()
+    want = kB_ui * 300.0 / (3.0 * s.n) ** 2
+    got = []
+    for _ in range(10):
+        s.dinamica(1, 1)
+        got.append((s.vel ** 2 * s.mass[:, None]).ravel())
+    got = np.concatenate(got)
+    assert abs(got.mean() / want - 1.0) < 0.08
+
+
 def test_nvt_plj_ermak():
     """examples/NVT/ermak.gms: same gas under Ermak (gamma=10/ps, 300 K)."""
     r, ref = _he_ne("nvt")
