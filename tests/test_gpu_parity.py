@@ -291,7 +291,9 @@ def test_gpu_lj_family_decks(ctx, kind):
     np.testing.assert_allclose(got, orc, atol=1e-12, rtol=1e-9)
 
 
-@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+# the compressed WCA core puts pair energies of several eV on an atom, of
+# which FP32 pair math carries about 6e-8: the mixed energy bound is 4e-6 eV
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, 4e-6)])
 def test_gpu_wca_feels_fluid(ctx, prec, rms, etol):
     """A dense two-species WCA fluid (2048 atoms, periodic, linked cells)
     where species 1 feels species 0 one-sidedly and an sm1 well binds
