@@ -3502,8 +3502,10 @@ int gemsgpu_server_forget(gemsgpu_server* S, int64_t id) {
 
 // ------------------------------------------------------------ checkpoints
 // write_chp / read_chp (src/Checkpoint.F90:154-244): the per-system state a
-// run resumes from -- positions, velocities, accelerations (GEMS layout), the
-// Ermak/Philox step counter, the FIRE state and the rebuild count.  Resuming
+// run resumes from -- positions, velocities, accelerations and the Nordsieck
+// derivatives acel2..acel4 (GEMS layout; version 3 files, without the
+// derivatives, still load), the Ermak/Philox step counter, the FIRE state and
+// the rebuild count.  Resuming
 // forces a neighbour rebuild, as the reference's interact does after
 // read_chp (src/Checkpoint.F90:232-241).
 namespace {
@@ -3526,7 +3528,7 @@ struct ChpHeader {
 int gemsgpu_checkpoint_size(gemsgpu_ctx* ctx, int sys, size_t* bytes) {
   CHK(check_sys(ctx, sys));
   if (!bytes) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_size: NULL");
-  *bytes = sizeof(ChpHeader) + 9 * sizeof(double) * (size_t)ctx->sys[sys].n;
+  *bytes = sizeof(ChpHeader) + 18 * sizeof(double) * (size_t)ctx->sys[sys].n;
   return 0;
 }
 
@@ -3539,7 +3541,7 @@ int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes) 
   const SysState& st = ctx->h_st[sys];
   ChpHeader hd{};
   memcpy(hd.magic, "GEMSGPU", 8);
-  hd.version = 3;
+  hd.version = 4;
   hd.n = h.n;
   hd.ff = h.d.ff;
   hd.integ = h.d.integ;
@@ -3568,19 +3570,28 @@ int gemsgpu_checkpoint_save(gemsgpu_ctx* ctx, int sys, void* buf, size_t bytes) 
   CHK(get_d4(ctx, h, ctx->A.pos, x));
   CHK(get_d4(ctx, h, ctx->A.vel, x + 3 * (size_t)h.n));
   CHK(get_d4(ctx, h, ctx->A.acel, x + 6 * (size_t)h.n));
+  if (ctx->A.acel2) {
+    CHK(get_d4(ctx, h, ctx->A.acel2, x + 9 * (size_t)h.n));
+    CHK(get_d4(ctx, h, ctx->A.acel3, x + 12 * (size_t)h.n));
+    CHK(get_d4(ctx, h, ctx->A.acel4, x + 15 * (size_t)h.n));
+  } else {
+    std::fill(x + 9 * (size_t)h.n, x + 18 * (size_t)h.n, 0.0);
+  }
   return 0;
 }
 
 int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t bytes) {
-  size_t need = 0;
-  CHK(gemsgpu_checkpoint_size(ctx, sys, &need));
-  if (!buf || bytes < need) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %zu bytes expected", need);
+  CHK(check_sys(ctx, sys));
+  if (!buf || bytes < sizeof(ChpHeader)) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: no header");
   SysHost& h = ctx->sys[sys];
   ChpHeader hd;
   memcpy(&hd, buf, sizeof(hd));
-  if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || hd.version != 3)
+  if (memcmp(hd.magic, "GEMSGPU", 8) != 0 || (hd.version != 3 && hd.version != 4))
     return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: not a checkpoint of this library");
   if (hd.n != h.n) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %d atoms, system has %d", hd.n, h.n);
+  const size_t per_atom = hd.version == 4 ? 18 : 9;
+  const size_t need = sizeof(ChpHeader) + per_atom * sizeof(double) * (size_t)h.n;
+  if (bytes < need) return fail(ctx, GEMSGPU_ERR_ARG, "checkpoint_load: %zu bytes expected", need);
   if (h.d.boxed && (moving_box(h.d) || hd.integ == IT_LGF || hd.integ == IT_AXES || hd.integ == IT_LKD)) {
     // the box the piston had reached
     h.box_live = false;
@@ -3593,6 +3604,16 @@ int gemsgpu_checkpoint_load(gemsgpu_ctx* ctx, int sys, const void* buf, size_t b
   CHK(h2d_xyz(ctx, x, ctx->A.pos + h.off, h.n));
   CHK(h2d_xyz(ctx, x + 3 * (size_t)h.n, ctx->A.vel + h.off, h.n));
   CHK(h2d_xyz(ctx, x + 6 * (size_t)h.n, ctx->A.acel + h.off, h.n));
+  std::vector<double> hi(9 * (size_t)h.n, 0.0);
+  if (hd.version == 4) std::copy(x + 9 * (size_t)h.n, x + 18 * (size_t)h.n, hi.begin());
+  bool any_hi = false;
+  for (double q : hi) any_hi |= q != 0.0;
+  if (any_hi) CHK(ensure_nord(ctx));
+  if (ctx->A.acel2) {
+    CHK(h2d_xyz(ctx, hi.data(), ctx->A.acel2 + h.off, h.n));
+    CHK(h2d_xyz(ctx, hi.data() + 3 * (size_t)h.n, ctx->A.acel3 + h.off, h.n));
+    CHK(h2d_xyz(ctx, hi.data() + 6 * (size_t)h.n, ctx->A.acel4 + h.off, h.n));
+  }
   CHK(read_states(ctx));
   SysState st = ctx->h_st[sys];
   st.step = hd.step;

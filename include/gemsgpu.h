@@ -378,8 +378,9 @@ int gemsgpu_neb(gemsgpu_ctx* ctx, const int* sys, int nimg, const int* fixed,
 /* ------------------------------------------------------------ checkpoints */
 
 /* Per-system checkpoint (write_chp / read_chp, src/Checkpoint.F90:154-244):
- * positions, velocities and accelerations in the GEMS layout plus the
- * integrator state (Philox step counter, FIRE dt/alpha/counters, the box
+ * positions, velocities, accelerations and the Nordsieck derivatives
+ * acel2..acel4 in the GEMS layout plus the integrator state (Philox step
+ * counter, FIRE dt/alpha/counters, the box
  * and the G-JF piston's force, velocity and last noise) and the
  * rebuild count, in a caller-owned host buffer of gemsgpu_checkpoint_size
  * bytes.  Loading into a system of the same size restores that state; the

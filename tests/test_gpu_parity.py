@@ -406,6 +406,7 @@ def test_gpu_pred_corr_derivatives_and_resume(ctx):
     g.set_pred_corr(0.002)
     g.dinamica(100, 100)
     chp = g.write_gems_chp(step=100, nsteps=100)
+    ck = g.checkpoint()
     g.dinamica(100, 100)
     got = decks.chp_atoms(g.write_gems_chp(step=200, nsteps=200), n)
     np.testing.assert_allclose(got[0], s.pos, rtol=0, atol=1e-9)
@@ -421,8 +422,17 @@ def test_gpu_pred_corr_derivatives_and_resume(ctx):
     h.dinamica(100, 100)
     np.testing.assert_allclose(h.pos, g.pos, rtol=0, atol=1e-9)
     np.testing.assert_allclose(h.vel, g.vel, rtol=1e-9, atol=1e-12)
+    # the library's own checkpoint carries the derivatives too
+    k = gpu_ref_sys(np.zeros_like(pos), mass, types, 2, ctx=ctx)
+    k.set_box(box, (True, True, True))
+    decks.apply_plj(k)
+    k.set_pred_corr(0.002)
+    k.restore(ck)
+    k.dinamica(100, 100)
+    np.testing.assert_allclose(k.pos, g.pos, rtol=0, atol=1e-9)
     g.destroy()
     h.destroy()
+    k.destroy()
 
 
 def test_gpu_brownian_parity_stream(ctx):
