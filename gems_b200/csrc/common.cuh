@@ -11,6 +11,13 @@
 
 namespace gg {
 
+// GEMS unit conversion (src/Constants.F90:101-127), fixed at compile time
+// in the same operation order as the reference.
+__host__ __device__ constexpr double c_ui_ev() {
+  return 1.0e2 * 1.0e2 * 1.6605402e-27 * (1.0 / 1.60219e-19);
+}
+#define EV_UI (1.0 / gg::c_ui_ev())
+
 constexpr int MAXT = 4;            // species per system
 constexpr int BLOCK = 256;         // threads per block of every kernel
 constexpr int NSTENCIL = 27;
@@ -47,7 +54,16 @@ enum PREC : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 // status bits of a system (SysState::status)
 // ST_BOX: a constant-pressure box shrank below three list cut-offs in a
 // dimension, or its volume collapsed
-enum ST : int { ST_OVERFLOW = 1, ST_LOST = 2, ST_NAN = 4, ST_BOX = 8 };
+// ST_BONDS: a Tersoff atom has more than TS_MAXB bonds, a bond beyond list
+// slot 63, or a bond its partner's list does not hold
+enum ST : int { ST_OVERFLOW = 1, ST_LOST = 2, ST_NAN = 4, ST_BOX = 8, ST_BONDS = 16 };
+// status bits that end a run with an error (an overflow is healed instead)
+constexpr int ST_FATAL = ST_NAN | ST_LOST | ST_BOX | ST_BONDS;
+
+// Tersoff gather formulation: bonds per atom, threads per atom of the bond
+// kernel (the system's "lanes"), atoms per block
+constexpr int TS_MAXB = 12;
+constexpr int TS_TPA = 4;
 
 // Parameters of one species pair.  LJ (Pairs.F90:198-291):
 //   v[0]=e v[1]=s v[2]=rc v[3]=rc2 v[4]=prc v[5]=frc v[6]=eshift
@@ -157,6 +173,7 @@ struct SysState {
   // stepb are ax_ext[0] and ax_ext[1])
   double lkd_bo[3], lkd_bh[3], lkd_bf[3];
   double th_factor;  // scalvel: this step's velocity factor
+  double th_vcm[3];  // scalvel: this step's centre-of-mass velocity
 };
 
 // Block map: block b covers atoms [first[b], end[b]) of system sys[b];
@@ -213,6 +230,13 @@ struct Arena {
   int* cell_start;      // absolute start in cell_atoms
   int* chunk_sum;       // per 256-cell chunk
   int* cell_atoms;      // atom ids sorted by cell (descending within a cell)
+  // Tersoff: rslot[m * cap + i] = the slot of i in the flist of its m-th
+  // neighbour (255: none), built with the list; per step, tsmask[i] marks
+  // the flist slots of i that are bonds and tsfb[a * cap + i] holds the force
+  // that centre i's energy puts on the partner of its a-th bond
+  unsigned char* rslot;
+  unsigned long long* tsmask;
+  double4* tsfb;
   double* ext_normals;  // parity-mode Ermak normals (6 per atom)
   double2* blk_top2;    // per-block top-2 displacement^2
   double* blk_red;      // per-block partial sums

@@ -52,6 +52,8 @@ struct SysHost {
   int variant = 1;          // 1: species table in shared memory, 0: constants in
                             //    registers (single-species mixed SMA-TB; autotuned)
   std::vector<PairP> prm;   // ntypes x ntypes
+  std::vector<char> deaf;   // ntypes x ntypes: [a][b] = 1 once set_feels(b, a) left
+                            //   type a deaf to type b (the pair acts on b only)
   SysDev d{};
   bool ff_set = false;
   double temp = 0.0;        // Ermak bath temperature (K)
@@ -69,6 +71,15 @@ bool moving_box(const SysDev& d) {
 
 // a pair of types that acts on one side only (`interact g1 feels g2`): its
 // forces are not a pair virial
+// write a pair's parameters both ways, except a direction set_feels
+// turned off: that stays off whatever pair setter is called later
+void put_pair(SysHost& h, int ti, int tj, const PairP& P) {
+  if (h.deaf.size() != h.prm.size()) h.deaf.assign(h.prm.size(), 0);
+  const int a = ti * h.ntypes + tj, b = tj * h.ntypes + ti;
+  if (!h.deaf[a]) h.prm[a] = P;
+  if (!h.deaf[b]) h.prm[b] = P;
+}
+
 bool one_sided(const SysHost& h) {
   auto on = [&](int a, int b) {
     const PairP& P = h.prm[a * h.ntypes + b];
@@ -133,6 +144,7 @@ struct gemsgpu_ctx {
   int snap_arrays = 0;
   SysState* snap_st = nullptr;
   SysDev* snap_sys = nullptr;   // boxes moved by constant-pressure steps
+  bool tersoff = false;         // a Tersoff system exists: rslot, tsmask, tsfb are kept
 };
 
 // A pool: a fixed-capacity batch of systems sharing one force-field kind and
@@ -254,6 +266,8 @@ void invalidate(gemsgpu_ctx* c) {
 }
 
 // ------------------------------------------------------------- arena
+int tersoff_records(gemsgpu_ctx* ctx);
+
 int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   if (need <= ctx->acap) return 0;
   int64_t nc = std::max<int64_t>(need, ctx->acap + ctx->acap / 2);
@@ -301,10 +315,42 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
       if (*lists[q]) CU(cudaFree(*lists[q]));
       *lists[q] = nl;
     }
+    if (A.rslot) {
+      unsigned char* nr = nullptr;
+      CHK(dalloc(ctx, &nr, (size_t)A.lcap * nc));
+      CU(cudaMemsetAsync(nr, 0xff, (size_t)A.lcap * nc, ctx->stream));
+      if (keep)
+        CU(cudaMemcpy2DAsync(nr, nc, A.rslot, keep, keep, A.lcap, cudaMemcpyDeviceToDevice, ctx->stream));
+      CU(cudaStreamSynchronize(ctx->stream));
+      CU(cudaFree(A.rslot));
+      A.rslot = nr;
+    }
   }
   ctx->acap = nc;
   A.cap = nc;
+  // the Tersoff bond records are rewritten by every force evaluation
+  if (ctx->tersoff) CHK(tersoff_records(ctx));
   invalidate(ctx);
+  return 0;
+}
+
+// Tersoff scratch: per-step bond masks and records (TS_MAXB rows of the
+// atom capacity), and the reverse list slots (one byte per list entry)
+int tersoff_records(gemsgpu_ctx* ctx) {
+  Arena& A = ctx->A;
+  const size_t n = (size_t)std::max<int64_t>(ctx->acap, 1);
+  CU(cudaStreamSynchronize(ctx->stream));
+  if (A.tsmask) CU(cudaFree(A.tsmask));
+  if (A.tsfb) CU(cudaFree(A.tsfb));
+  A.tsmask = nullptr;
+  A.tsfb = nullptr;
+  CHK(dalloc(ctx, &A.tsmask, n));
+  CU(cudaMemsetAsync(A.tsmask, 0, n * sizeof(unsigned long long), ctx->stream));
+  CHK(dalloc(ctx, &A.tsfb, (size_t)TS_MAXB * n));
+  if (!A.rslot && A.lcap > 0) {
+    CHK(dalloc(ctx, &A.rslot, (size_t)A.lcap * n));
+    CU(cudaMemsetAsync(A.rslot, 0xff, (size_t)A.lcap * n, ctx->stream));
+  }
   return 0;
 }
 
@@ -324,6 +370,16 @@ int grow_list(gemsgpu_ctx* ctx, int lcap) {
     CU(cudaStreamSynchronize(ctx->stream));
     if (*lists[q]) CU(cudaFree(*lists[q]));
     *lists[q] = nl;
+  }
+  if (ctx->tersoff) {
+    unsigned char* nr = nullptr;
+    CHK(dalloc(ctx, &nr, (size_t)lcap * ld));
+    CU(cudaMemsetAsync(nr, 0xff, (size_t)lcap * ld, ctx->stream));
+    if (A.rslot && A.lcap > 0)
+      CU(cudaMemcpyAsync(nr, A.rslot, (size_t)A.lcap * ld, cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (A.rslot) CU(cudaFree(A.rslot));
+    A.rslot = nr;
   }
   A.lcap = lcap;
   size_t smem = list_smem(lcap);
@@ -703,6 +759,15 @@ void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, 
   }
 }
 
+// Tersoff forces: bond records per centre atom, then the per-atom gather
+// (both on the TS_APB-atom map)
+void tersoff_pass(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
+  if (prec == PREC_MIXED) k_tsf_bonds<float><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  else k_tsf_bonds<double><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  ++ctx->launches;
+  k_tsf_gather<<<m.nblk, TS_APB, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+}
+
 void lj_pass(gemsgpu_ctx* ctx, int prec, int K, bool vir, const BlockMap& m) {
   switch (K) {
     case 2: lj_k<2>(ctx, prec, vir, m); break;
@@ -721,7 +786,7 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
     const SysHost& h = ctx->sys[s];
     if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no force field", s);
     if (h.d.half) return fail(ctx, GEMSGPU_ERR_STATE, "system %d: force kernels need full lists", s);
-    int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
+    int K = h.d.ff == FF_TERSOFF ? TS_TPA : h.lanes;
     int key = h.variant * 2 + (h.ntypes == 1 ? 1 : 0);
     groups[{h.d.ff, h.d.prec, K, key, h.d.virial}].push_back(s);
   }
@@ -731,17 +796,11 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
     const bool single = (std::get<3>(kv.first) & 1) != 0;
     const bool vir = std::get<4>(kv.first) != 0;
     BlockMap m;
+    CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
     if (ff == FF_TERSOFF) {
-      CHK(get_map(ctx, kv.second, BLOCK, 0, &m));
-      k_zero_force<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
-      if (prec == PREC_MIXED) {
-        k_tersoff<float><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
-      } else {
-        k_tersoff<double><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
-      }
+      tersoff_pass(ctx, prec, m);
       continue;
     }
-    CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
     if (ff == FF_SMATB) {
       smatb_pass(ctx, 0, prec, variant, single, K, m);
       smatb_pass(ctx, 1, prec, variant, single, K, m, vir);
@@ -782,6 +841,11 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 
   }
   if (n2) {
     k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  }
+  bool ts = false;
+  for (int s : ss) ts |= ctx->sys[s].d.ff == FF_TERSOFF;
+  if (ts) {
+    k_tsf_rslot<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   }
   k_count_rebuild<<<((int)ss.size() + 255) / 256, 256, 0, st>>>(A, sa, (int)ss.size(), in_graph); ++ctx->launches;
   CU(cudaGetLastError());
@@ -917,8 +981,9 @@ int launch_step_b(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   ++ctx->launches;
   // the thermostats after the integrator's stepb
   if (scal) {
-    k_thermo_sum<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
-    ++ctx->launches;
+    k_thermo_sum<0><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+    k_thermo_sum<1><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
+    ctx->launches += 2;
   }
   if (thermo) {
     k_thermo_apply<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
@@ -949,6 +1014,10 @@ int status_error(gemsgpu_ctx* ctx, int s, int st) {
   if (st & ST_NAN) return fail(ctx, GEMSGPU_ERR_NAN, "system %d: non-finite positions", s);
   if (st & ST_LOST)
     return fail(ctx, GEMSGPU_ERR_LOST, "system %d: atom outside the cell grid / fixed-point range", s);
+  if (st & ST_BONDS)
+    return fail(ctx, GEMSGPU_ERR_STATE,
+                "system %d: a Tersoff atom has more than %d bonds (r <= R+D), or a bond beyond list slot 63",
+                s, TS_MAXB);
   if (st & ST_OVERFLOW) return fail(ctx, GEMSGPU_ERR_OVERFLOW, "system %d: neighbour list overflow", s);
   if (st & ST_BOX)
     return fail(ctx, GEMSGPU_ERR_STATE,
@@ -1289,17 +1358,16 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
                     &sa));
     for (int s : ss) {
       const SysHost& h = ctx->sys[s];
-      CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / h.lanes, 0, &m));
+      CHK(get_map(ctx, ss, BLOCK / h.lanes, 0, &m));
     }
     std::map<std::tuple<int, int, int>, std::vector<int>> groups;
     for (int s : ss) {
       const SysHost& h = ctx->sys[s];
-      int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
-      groups[{h.d.ff, h.d.prec, K}].push_back(s);
+      groups[{h.d.ff, h.d.prec, h.lanes}].push_back(s);
     }
     for (auto& kv : groups) {
       int K = std::get<2>(kv.first);
-      CHK(get_map(ctx, kv.second, std::get<0>(kv.first) == FF_TERSOFF ? BLOCK : BLOCK / K, 0, &m));
+      CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
     }
     CU(cudaStreamSynchronize(ctx->stream));
   }
@@ -1403,7 +1471,7 @@ int md_group(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps) {
     for (int s : ss) {
       int st = ctx->h_st[s].status;
       if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
-      if (st & (ST_NAN | ST_LOST | ST_BOX)) { bad = st; bads = s; }
+      if (st & ST_FATAL) { bad = st; bads = s; }
     }
     if (bad) return status_error(ctx, bads, bad);
     if (grow > 0) {
@@ -1566,6 +1634,9 @@ int pool_rebuild(gemsgpu_pool* P, int in_graph) {
   k_list_cells<<<rebuild_grid(ctx, mc8.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc8);
   ++ctx->launches;
   k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  if (P->ff == FF_TERSOFF) {
+    k_tsf_rslot<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
+  }
   k_count_rebuild<<<(ns + 255) / 256, 256, 0, st>>>(A, P->dsys, ns, in_graph); ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
@@ -1574,7 +1645,6 @@ int pool_rebuild(gemsgpu_pool* P, int in_graph) {
 int pool_forces(gemsgpu_pool* P) {
   gemsgpu_ctx* ctx = P->ctx;
   const BlockMap& mk = P->maps[4];
-  const BlockMap& ma = P->maps[0];
   if (P->ff == FF_SMATB) {
     // the graph is captured once: the register variant (bit 0 clear) is only
     // allowed for single-species members (checked in gemsgpu_pool_set)
@@ -1584,10 +1654,7 @@ int pool_forces(gemsgpu_pool* P) {
   } else if (P->ff == FF_LJ) {
     lj_pass(ctx, P->prec, P->lanes, false, mk);
   } else if (P->ff == FF_TERSOFF) {
-    k_zero_force<<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma); ++ctx->launches;
-    if (P->prec == PREC_MIXED) k_tersoff<float><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
-    else k_tersoff<double><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma);
-    ++ctx->launches;
+    tersoff_pass(ctx, P->prec, mk);
   }
   CU(cudaGetLastError());
   return 0;
@@ -1718,7 +1785,7 @@ int pool_chunk(gemsgpu_pool* P) {
     int grow = 0;
     for (int s : P->active) {
       int st = ctx->h_st[s].status;
-      if (st & (ST_NAN | ST_LOST)) return status_error(ctx, s, st);
+      if (st & ST_FATAL) return status_error(ctx, s, st);
       if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
     }
     if (!grow) return 0;
@@ -1811,6 +1878,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.acel2, A.acel3, A.acel4, A.epot, A.band, A.eband,
                   A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.ncut, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
+                  A.rslot, A.tsmask, A.tsfb,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys};
   for (void* p : ptrs)
@@ -2090,8 +2158,7 @@ int gemsgpu_set_lj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, double
     P.v[7] = 1.0;
   }
   P.v[6] = eshift;
-  h.prm[ti * h.ntypes + tj] = P;
-  h.prm[tj * h.ntypes + ti] = P;
+  put_pair(h, ti, tj, P);
   h.ff_set = true;
   h.first = true;
   CHK(push_sys(ctx, sys));
@@ -2147,7 +2214,11 @@ int gemsgpu_set_tersoff(gemsgpu_ctx* ctx, int sys, const double prm[12]) {
   TersoffP& T = h.d.ts;
   T.A = prm[0]; T.B = prm[1]; T.l1 = prm[2]; T.l2 = prm[3]; T.beta = prm[4]; T.n = prm[5];
   T.c = prm[6]; T.d = prm[7]; T.h = prm[8]; T.R = prm[9]; T.D = prm[10]; T.chi = prm[11];
-  h.lanes = 1;
+  h.lanes = TS_TPA;
+  if (!ctx->tersoff) {
+    ctx->tersoff = true;
+    CHK(tersoff_records(ctx));
+  }
   h.ff_set = true;
   h.first = true;
   CHK(push_sys(ctx, sys));
@@ -2431,8 +2502,7 @@ int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, doubl
   P.v[9] = (8.0 * urs + d * dudrs) / (4 * d4);
   P.v[10] = -(4.0 * urs + d * dudrs) / (4 * (d4 * d4));
   P.v[11] = rs;
-  h.prm[ti * h.ntypes + tj] = P;
-  h.prm[tj * h.ntypes + ti] = P;
+  put_pair(h, ti, tj, P);
   h.ff_set = true;
   h.first = true;
   CHK(push_sys(ctx, sys));
@@ -2467,8 +2537,7 @@ int gemsgpu_set_sm1(gemsgpu_ctx* ctx, int sys, int ti, int tj, double r1, double
   P.v[3] = r2 * r2;
   P.v[8] = 2.0;
   P.v[11] = r1;
-  h.prm[ti * h.ntypes + tj] = P;
-  h.prm[tj * h.ntypes + ti] = P;
+  put_pair(h, ti, tj, P);
   h.ff_set = true;
   h.first = true;
   CHK(push_sys(ctx, sys));
@@ -2488,6 +2557,8 @@ int gemsgpu_set_feels(gemsgpu_ctx* ctx, int sys, int ti, int tj) {
   if (h.d.ff != FF_LJ) return fail(ctx, GEMSGPU_ERR_STATE, "set_feels: pair potentials only");
   if (h.d.virial) return fail(ctx, GEMSGPU_ERR_STATE, "set_feels: one-sided pairs have no pair virial");
   if (ti == tj) return 0;
+  if (h.deaf.size() != h.prm.size()) h.deaf.assign(h.prm.size(), 0);
+  h.deaf[tj * h.ntypes + ti] = 1;
   h.prm[tj * h.ntypes + ti] = PairP{};
   h.has_forces = false;
   CHK(push_sys(ctx, sys));
@@ -2917,7 +2988,7 @@ int gemsgpu_batch_fire(gemsgpu_ctx* ctx, const int* sys, int nsys, double fmax, 
       CHK(read_states(ctx));
       for (int s : ss) {
         int st = ctx->h_st[s].status;
-        if (st & (ST_NAN | ST_LOST)) return status_error(ctx, s, st);
+        if (st & ST_FATAL) return status_error(ctx, s, st);
         if (st & ST_OVERFLOW) {
           CHK(grow_list(ctx, ctx->h_st[s].maxnn + 16));
           const int* sa;
@@ -3058,7 +3129,7 @@ static int autotune_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, 
   if (!need.empty()) CHK(interact_group(ctx, need, true));
   std::vector<std::pair<int, int>> cand;
   if (h0.d.ff == FF_TERSOFF) {
-    cand.push_back({1, 1});
+    cand.push_back({TS_TPA, 1});
   } else {
     for (int K : {1, 2, 4, 8, 16, 32}) {
       cand.push_back({K, 1});
@@ -3098,7 +3169,7 @@ static int autotune_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, 
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (int s : ss) {
-    ctx->sys[s].lanes = ctx->sys[s].d.ff == FF_TERSOFF ? 1 : pick.first;
+    ctx->sys[s].lanes = ctx->sys[s].d.ff == FF_TERSOFF ? TS_TPA : pick.first;
     ctx->sys[s].variant = pick.second;
   }
   invalidate(ctx);
@@ -3259,7 +3330,7 @@ int gemsgpu_pool_create(gemsgpu_ctx* ctx, int max_systems, int64_t max_atoms, in
   P->max_cells = max_cells;
   P->ff = ff;
   P->prec = prec;
-  P->lanes = ff == FF_TERSOFF ? 1 : lanes;
+  P->lanes = ff == FF_TERSOFF ? TS_TPA : lanes;
   P->variant = (variant >= 0 && variant <= 7 && variant != 4 && variant != 5) ? variant : 1;
   P->chunk = chunk_steps;
   int rc = grow_systems(ctx, std::max((int)ctx->sys.size(), 0) + max_systems + 1);
@@ -3295,8 +3366,18 @@ int gemsgpu_pool_set(gemsgpu_pool* P, const int* sys, int nsys) {
     if (s >= P->scap) return fail(ctx, GEMSGPU_ERR_FULL, "system id beyond the pool's capacity");
     if ((P->variant & 1) == 0 && ctx->sys[s].ntypes != 1)
       return fail(ctx, GEMSGPU_ERR_STATE, "pool variant %d needs single-species systems", P->variant);
-    if (moving_box(ctx->sys[s].d) || ctx->sys[s].d.virial)
+    const SysDev& d = ctx->sys[s].d;
+    if (moving_box(d) || d.virial)
       return fail(ctx, GEMSGPU_ERR_STATE, "pool_set: pools run fixed boxes without the virial");
+    if (d.ff != P->ff || d.prec != P->prec)
+      return fail(ctx, GEMSGPU_ERR_STATE, "pool_set: system %d has another force field or precision", s);
+    // the pool's captured step runs k_step_a / k_step_b<false> and no
+    // thermostat kernels: velocity Verlet, Ermak and FIRE only
+    if (d.integ != IT_VV && d.integ != IT_ERMAK && d.integ != IT_FIRE)
+      return fail(ctx, GEMSGPU_ERR_STATE,
+                  "pool_set: system %d: pools run velocity Verlet, Ermak or FIRE systems only", s);
+    if (d.thermo != TH_NONE)
+      return fail(ctx, GEMSGPU_ERR_STATE, "pool_set: system %d has a thermostat; pools run none", s);
     atoms += ctx->sys[s].n;
   }
   if (atoms > P->max_atoms) return fail(ctx, GEMSGPU_ERR_FULL, "pool_set: %lld atoms > capacity", (long long)atoms);
@@ -3983,7 +4064,7 @@ int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m, doubl
     int grow = 0;
     for (int s : active) {
       const int st = ctx->h_st[s].status;
-      if (st & (ST_NAN | ST_LOST)) return fail_clean(status_error(ctx, s, st));
+      if (st & ST_FATAL) return fail_clean(status_error(ctx, s, st));
       if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
     }
     if (grow > 0) {
@@ -4121,7 +4202,7 @@ int gemsgpu_neb(gemsgpu_ctx* ctx, const int* sys, int nimg, const int* fixed, in
     int grow = 0;
     for (int s : inner) {
       const int st = ctx->h_st[s].status;
-      if (st & (ST_NAN | ST_LOST)) return bail(status_error(ctx, s, st));
+      if (st & ST_FATAL) return bail(status_error(ctx, s, st));
       if (st & ST_OVERFLOW) grow = std::max(grow, ctx->h_st[s].maxnn);
     }
     if (grow > 0) {  // the lists of this step would be truncated: grow and rebuild them
@@ -4177,11 +4258,11 @@ static int time_kernels_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int re
   for (int s : ss)
     if (ctx->sys[s].first || ctx->sys[s].pos_dirty || !ctx->sys[s].has_forces) need.push_back(s);
   if (!need.empty()) CHK(interact_group(ctx, need, true));
-  const int K = h.d.ff == FF_TERSOFF ? 1 : h.lanes;
+  const int K = h.lanes;
   bool single = true;
   for (int s : ss) single &= ctx->sys[s].ntypes == 1;
   BlockMap m;
-  CHK(get_map(ctx, ss, h.d.ff == FF_TERSOFF ? BLOCK : BLOCK / K, 0, &m));
+  CHK(get_map(ctx, ss, BLOCK / K, 0, &m));
   const int* sa;
   CHK(sys_array(ctx, ss, &sa));
   cudaEvent_t ev[4];

@@ -17,12 +17,6 @@
 
 namespace gg {
 
-// GEMS unit conversion (src/Constants.F90:101-127), fixed at compile time
-// in the same operation order as the reference.
-__host__ __device__ constexpr double c_ui_ev() {
-  return 1.0e2 * 1.0e2 * 1.6605402e-27 * (1.0 / 1.60219e-19);
-}
-#define EV_UI (1.0 / gg::c_ui_ev())
 // pi = 4 atan(1) (src/Constants.F90:71)
 #define PI_D 3.141592653589793
 
@@ -778,49 +772,66 @@ __device__ __forceinline__ void virial_close(Arena& A, const BlockMap& M, int s,
 
 // Thermostats after step b (integration_stepb runs every integrator's stepb
 // in the order the deck adds them, src/Integration.F90:264-275).
-// scalvel / scalvel_after (:1300-1340): the system's centre-of-mass-free
-// kinetic energy (inq_kin_energy / inq_temperature,
-// Inq_Properties.F90:399-434: sum m |v - v_cm|^2 = sum m v^2 - M |v_cm|^2)
-// gives T and the factor (T0/T)^soft, applied by k_thermo_apply; one atom
-// alone has no kinetic energy about its centre of mass and is not scaled.
+// scalvel / scalvel_after (:1300-1340) need the system's kinetic energy
+// about its centre of mass (inq_kin_energy / inq_temperature,
+// Inq_Properties.F90:399-434), summed as the reference sums it, over
+// m |v - v_cm|^2, in two passes: PASS 0 the centre-of-mass velocity, PASS 1
+// the sum, T and the factor (T0/T)^soft, applied by k_thermo_apply.  (The
+// one-pass form sum m v^2 - M |v_cm|^2 cancels digits when the centre of
+// mass drifts fast.)  One atom alone has no kinetic energy about its centre
+// of mass and is not scaled.
+template <int PASS>
 __global__ void k_thermo_sum(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   if (S.thermo != TH_SCALVEL && S.thermo != TH_SCALVEL_AFTER) return;  // the whole system's blocks
+  constexpr int NW = PASS == 0 ? 4 : 1;
   int i = M.first[blockIdx.x] + threadIdx.x;
-  double w[5] = {0, 0, 0, 0, 0};
+  double w[NW];
+#pragma unroll
+  for (int k = 0; k < NW; k++) w[k] = 0.0;
   if (i < M.end[blockIdx.x]) {
     const double4 v = A.vel[i];
     const double m = A.mass[i];
-    w[0] = m;
-    w[1] = m * v.x;
-    w[2] = m * v.y;
-    w[3] = m * v.z;
-    w[4] = m * (v.x * v.x + v.y * v.y + v.z * v.z);
+    if constexpr (PASS == 0) {
+      w[0] = m;
+      w[1] = m * v.x;
+      w[2] = m * v.y;
+      w[3] = m * v.z;
+    } else {
+      const double* c = A.st[s].th_vcm;
+      const double d0 = v.x - c[0], d1 = v.y - c[1], d2 = v.z - c[2];
+      w[0] = m * (d0 * d0 + d1 * d1 + d2 * d2);
+    }
   }
-  double b[5];
+  double b[NW];
 #pragma unroll
-  for (int k = 0; k < 5; k++) b[k] = block_sum(w[k]);
+  for (int k = 0; k < NW; k++) b[k] = block_sum(w[k]);
   if (threadIdx.x == 0)
-    for (int k = 0; k < 5; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = b[k];
+    for (int k = 0; k < NW; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = b[k];
   if (last_block(M, A.st, s, &A.st[s].ticket2) && threadIdx.x < 32) {
     const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
-    double t[5] = {0, 0, 0, 0, 0};
+    double t[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) t[k] = 0.0;
     for (int q = threadIdx.x; q < nb; q += 32)
 #pragma unroll
-      for (int k = 0; k < 5; k++) t[k] += __ldcg(&A.blk_red[8 * (b0 + q) + k]);
+      for (int k = 0; k < NW; k++) t[k] += __ldcg(&A.blk_red[8 * (b0 + q) + k]);
 #pragma unroll
-    for (int k = 0; k < 5; k++)
+    for (int k = 0; k < NW; k++)
       for (int o = 16; o; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
     if (threadIdx.x == 0) {
-      double ek = 0.0;
-      if (S.n > 1) ek = 0.5 * (t[4] - (t[1] * t[1] + t[2] * t[2] + t[3] * t[3]) / t[0]);
-      const double T = 2.0 * ek / (S.th[3] * (3 * S.n));
-      const double T0 = S.th[0];
-      double f = 1.0;
-      if (T != 0.0 && (S.thermo == TH_SCALVEL || fabs(T - T0) > S.th[2] * T0)) f = pow(T0 / T, S.th[1]);
-      A.st[s].th_factor = f;
+      if constexpr (PASS == 0) {
+        for (int k = 0; k < 3; k++) A.st[s].th_vcm[k] = t[0] > 0.0 ? t[1 + k] / t[0] : 0.0;
+      } else {
+        const double ek = S.n > 1 ? 0.5 * t[0] : 0.0;
+        const double T = 2.0 * ek / (S.th[3] * (3 * S.n));
+        const double T0 = S.th[0];
+        double f = 1.0;
+        if (T != 0.0 && (S.thermo == TH_SCALVEL || fabs(T - T0) > S.th[2] * T0)) f = pow(T0 / T, S.th[1]);
+        A.st[s].th_factor = f;
+      }
     }
   }
 }
@@ -1486,144 +1497,295 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
 }
 
 // ------------------------------------------------------------------ Tersoff
-// Tersoff 1988 with the functional form of src/Tersoff.f90:131-341 and the
-// cut-off of src/Algebra.F90:391-409, forces = exact gradient of
-// E = sum_i sum_j 1/2 fc(r_ij) [VR(r_ij) + b_ij VA(r_ij)].  One thread per
-// atom i gathers its bonds (r <= R+D) into registers and scatters the
-// three-body terms to j and k with FP64 atomics.  Bond geometry, the pair
-// terms fc, VR, VA and the bond order b_ij = chi (1 + beta^n zeta^n)^(-1/2n)
-// are FP64; the angular sums zeta_ij and their derivatives (the triplet
-// work) run in R = float for the mixed kernel, double for the FP64 kernel.
-constexpr int TS_MAXB = 12;
+// Tersoff 1988 with the functional form of src/Tersoff.f90:131-341 (chi
+// prefactor, no lambda3 term) and the cut-off fcut_dfcut of
+// src/Algebra.F90:391-409:
+//   E = sum_i E_i,  E_i = sum_{j bonded to i} 1/2 fc(r_ij) [VR(r_ij) + b_ij VA(r_ij)],
+//   VR = A e^{-l1 r},  VA = -B e^{-l2 r},  b_ij = chi (1 + (beta zeta_ij)^n)^{-1/2n},
+//   zeta_ij = sum_{k != j} fc(r_ik) g(cos theta_ijk),
+//   g = 1 + c^2/d^2 - c^2/(d^2 + (h - cos)^2),
+// with forces that are the exact gradient of E (the reference's missing
+// radial force on j and its unallocated gradb_k are not reproduced).
+//
+// Gather formulation: no atomics, so the forces are the same bits on every
+// run and in every batch.
+//  * k_tsf_bonds, per centre atom i (TS_TPA threads): i's bonds (r <= R+D)
+//    in flist order; per bond a = (i, j): zeta, b and the force that E_i puts
+//    on j, F_j(i) = -dE_i/dx_j, stored in the bond record tsfb[a cap + i].
+//    E_i is translation invariant, so the force it puts on i itself is
+//    -sum_a F_j(a).  tsmask[i] marks the flist slots that are bonds.
+//  * k_tsf_gather, per atom l: F_l = F_l(l) + the records its bond partners
+//    wrote for their bonds to l, in l's slot order.  rslot (built with the
+//    list) is l's slot in the partner's flist; the popcount of the partner's
+//    mask below that slot is the record's index.
+// Bond decisions are symmetric (the pair vector seen from j is the exact
+// negative of the one seen from i), so every record a gather looks for exists.
+//
+// R = double: the plain FP64 kernel.  R = float (mixed): geometry from the
+// fixed-point copies; the angular sums zeta, their gradients and the bond
+// order in FP32; VR, VA, fc and the energy in FP64.  b VA is formed as
+// chi VA - chi VA y with y = 1 - (1+x)^{-1/2n}, x = (beta zeta)^n, from log1p
+// and expm1, so the FP32 rounding of y costs y's relative error (y ~ 0.04 in
+// silicon), not b's.  A bond's triplet force terms are summed in FP32, the
+// bond records and the per-atom sums in FP64.
+constexpr int TS_APB = BLOCK / TS_TPA;  // atoms per block of the Tersoff kernels
 
-__device__ __forceinline__ double ts_fc(double r, double r1, double r2, double& dfc) {
-  if (r < r1) { dfc = 0.0; return 1.0; }
-  if (r > r2) { dfc = 0.0; return 0.0; }
-  const double pi = 3.14159265358979323846;
-  double aux = pi * (r - (r1 + r2) * 0.5) / (r2 - r1);
-  double sn, cs;
-  sincos(aux, &sn, &cs);
-  dfc = -cs * (pi * 0.5) / (r2 - r1);
-  return 0.5 - 0.5 * sn;
+template <typename R>
+__device__ __forceinline__ R ts_fc(R r, R r1, R r2, R& dfc) {
+  if (r < r1) { dfc = R(0); return R(1); }
+  if (r > r2) { dfc = R(0); return R(0); }
+  const R pi = R(3.14159265358979323846);
+  const R aux = pi * (r - (r1 + r2) * R(0.5)) / (r2 - r1);
+  R sn, cs;
+  if constexpr (sizeof(R) == 8) sincos(aux, &sn, &cs);
+  else sincosf(aux, &sn, &cs);
+  dfc = -cs * (pi * R(0.5)) / (r2 - r1);
+  return R(0.5) - R(0.5) * sn;
+}
+
+// bond order of one bond: b, b VA (FP64) and db/dzeta
+__device__ __forceinline__ void ts_border(const TersoffP& T, double z, double va, double& b, double& bva,
+                                          double& dbdz) {
+  if (z > 1.0e-15) {
+    const double zn = pow(z, T.n);
+    const double x = pow(T.beta, T.n) * zn;
+    const double aux = 1.0 / (1.0 + x);
+    b = T.chi * pow(aux, 0.5 / T.n);
+    dbdz = -0.5 * b * aux * x / z;
+  } else {
+    b = T.chi;
+    dbdz = 0.0;
+  }
+  bva = b * va;
+}
+__device__ __forceinline__ void ts_border(const TersoffP& T, float z, double va, double& b, double& bva,
+                                          float& dbdz) {
+  if (z > 1.0e-15f) {
+    const float x = exp2f((float)T.n * log2f((float)T.beta * z));
+    const float y = -expm1f((float)(-0.5 / T.n) * log1pf(x));
+    const double cva = T.chi * va;
+    b = T.chi - T.chi * (double)y;
+    bva = cva - cva * (double)y;
+    dbdz = -0.5f * (float)b * x / ((1.0f + x) * z);
+  } else {
+    b = T.chi;
+    bva = T.chi * va;
+    dbdz = 0.0f;
+  }
 }
 
 template <typename R>
-__global__ void __launch_bounds__(BLOCK) k_tersoff(Arena A, BlockMap M) {
-  int s = blk_sys(M);
+__global__ void __launch_bounds__(BLOCK) k_tsf_bonds(Arena A, BlockMap M) {
+  constexpr int NB = TS_APB * TS_MAXB;
+  constexpr bool MIXED = sizeof(R) == 4;
+  constexpr int PER = TS_MAXB / TS_TPA;  // bonds per thread
+  __shared__ R sux[NB], suy[NB], suz[NB], sr[NB], sfc[NB], sdfc[NB], spre[NB];
+  const int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
-  int i = M.first[blockIdx.x] + threadIdx.x;
-  if (i >= M.end[blockIdx.x]) return;
   const TersoffP& T = S.ts;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, q = threadIdx.x & (TS_TPA - 1), la = threadIdx.x / TS_TPA;
+  const int i = M.first[blockIdx.x] + la;
+  const bool act = i < M.end[blockIdx.x];
+  const int base = la * TS_MAXB;
   const double r1 = T.R - T.D, r2 = T.R + T.D;
-  const R c2 = R(T.c * T.c), d2 = R(T.d * T.d), h = R(T.h);
-  const R c2d2 = R(T.c * T.c / (T.d * T.d));
-  const double nexp = T.n;
-  const double btnp = pow(T.beta, T.n);
+  const int nl = act ? live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap)) : 0;
+
+  // ---- bonds in flist order: the atom's TS_TPA threads test TS_TPA slots
+  // at a time and a ballot ranks the bonds they found
+  double4 xi = make_double4(0, 0, 0, 0);
+  int4 qi = make_int4(0, 0, 0, 0);
+  if (act) {
+    if constexpr (MIXED) qi = A.fxp[i];
+    else xi = A.pos[i];
+  }
+  int cnt = 0, err = 0;
+  unsigned long long mask = 0ull;
+  const int tmax = __reduce_max_sync(FULL, (nl + TS_TPA - 1) / TS_TPA);
+  for (int t = 0; t < tmax; t++) {
+    const int m = t * TS_TPA + q;
+    bool bond = false;
+    R u0 = R(0), u1 = R(0), u2 = R(0), rr = R(0);
+    if (m < nl) {
+      const int j = A.flist[(size_t)m * A.cap + i];
+      if ((unsigned)j < (unsigned)A.cap) {
+        if constexpr (MIXED) {
+          float v0, v1, v2, ir;
+          vd_fx(S, qi, A.fxp[j], v0, v1, v2);
+          rr = sqrt_nr(v0 * v0 + v1 * v1 + v2 * v2, ir);
+          u0 = v0 * ir; u1 = v1 * ir; u2 = v2 * ir;
+          bond = rr <= (float)r2;
+        } else {
+          double v0, v1, v2;
+          vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+          rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+          u0 = v0 / rr; u1 = v1 / rr; u2 = v2 / rr;
+          bond = !(rr > r2);
+        }
+      }
+    }
+    const unsigned grp = (__ballot_sync(FULL, bond) >> (lane & ~(TS_TPA - 1))) & ((1u << TS_TPA) - 1u);
+    if (bond) {
+      const int idx = cnt + __popc(grp & ((1u << q) - 1u));
+      if (idx < TS_MAXB && m < 64) {
+        const int k = base + idx;
+        sux[k] = u0; suy[k] = u1; suz[k] = u2; sr[k] = rr;
+        R dfc;
+        sfc[k] = ts_fc<R>(rr, R(r1), R(r2), dfc);
+        sdfc[k] = dfc;
+        mask |= 1ull << m;
+      } else {
+        err = 1;
+      }
+    }
+    cnt += __popc(grp);
+  }
+  mask |= __shfl_xor_sync(FULL, mask, 1);
+  mask |= __shfl_xor_sync(FULL, mask, 2);
+  const int nb = min(cnt, TS_MAXB);
+  __syncthreads();
+
+  // ---- per bond: zeta, bond order, the pair part (FP64) and dE_i/dzeta
+  const R h = R(T.h), c2 = R(T.c * T.c), d2 = R(T.d * T.d), c2d2 = R(T.c * T.c / (T.d * T.d));
   const double Aa = T.A * EV_UI, Bb = T.B * EV_UI;
-  int bj[TS_MAXB];
-  double br[TS_MAXB], bfc[TS_MAXB];
-  R bu[TS_MAXB][3], bfcr[TS_MAXB], bdfcr[TS_MAXB];
-  int nb = 0;
-  const int nn = min(A.nn[i], A.lcap);
-  const double4 xi = A.pos[i];
-  for (int m = 0; m < nn; m++) {
-    int j = A.flist[(size_t)m * A.cap + i];
-    if ((unsigned)j >= (unsigned)A.cap) continue;  // never gather outside the arena
-    double v0, v1, v2;
-    vd_fp64(S, xi, A.pos[j], v0, v1, v2);
-    double rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-    if (rr > r2) continue;
-    if (nb == TS_MAXB) {
-      atomicOr(&A.st[s].status, ST_OVERFLOW);
-      break;
-    }
-    bj[nb] = j;
-    br[nb] = rr;
-    double ir = 1.0 / rr;
-    bu[nb][0] = R(v0 * ir); bu[nb][1] = R(v1 * ir); bu[nb][2] = R(v2 * ir);
-    double dfc;
-    bfc[nb] = ts_fc(rr, r1, r2, dfc);
-    bfcr[nb] = R(bfc[nb]);
-    bdfcr[nb] = R(dfc);
-    nb++;
-  }
   double ei = 0.0;
-  double fi0 = 0, fi1 = 0, fi2 = 0;
-  for (int a = 0; a < nb; a++) {
-    const double rij = br[a];
-    const R* u = bu[a];
-    R zij = R(0);
+  double dvs[PER];
+#pragma unroll
+  for (int t = 0; t < PER; t++) {
+    const int a = q + t * TS_TPA;
+    dvs[t] = 0.0;
+    if (a >= nb) continue;
+    const R ax = sux[base + a], ay = suy[base + a], az = suz[base + a];
+    R z = R(0);
     for (int b = 0; b < nb; b++) {
       if (b == a) continue;
-      R ct = u[0] * bu[b][0] + u[1] * bu[b][1] + u[2] * bu[b][2];
-      R hc = h - ct;
-      R hc2 = hc * hc;
-      R g = R(1) + c2d2 * hc2 / (d2 + hc2);  // = 1 + c2/d2 - c2/(d2+hc2), no cancellation
-      zij += bfcr[b] * g;
+      const R ct = ax * sux[base + b] + ay * suy[base + b] + az * suz[base + b];
+      const R hc = h - ct, hc2 = hc * hc;
+      z += sfc[base + b] * (R(1) + c2d2 * hc2 / (d2 + hc2));  // 1 + c2/d2 - c2/(d2+hc2), no cancellation
     }
-    double dfc_a;
-    const double fc_a = ts_fc(rij, r1, r2, dfc_a);
-    const double vr = Aa * exp(-T.l1 * rij), dvr = -T.l1 * vr;
-    const double va = -Bb * exp(-T.l2 * rij), dva = -T.l2 * va;
-    double bij, dbdz;
-    const double z = (double)zij;
-    if (z > 1.0e-15) {
-      double zn = pow(z, nexp);
-      double aux = 1.0 / (1.0 + btnp * zn);
-      bij = T.chi * pow(aux, 0.5 / nexp);
-      dbdz = -0.5 * bij * aux * btnp * zn / z;
-    } else {
-      bij = T.chi;
-      dbdz = 0.0;
-    }
-    ei += 0.5 * fc_a * (vr + bij * va);
-    const double dV = 0.5 * (dfc_a * (vr + bij * va) + fc_a * (dvr + bij * dva));
-    const double ua0 = (double)u[0], ua1 = (double)u[1], ua2 = (double)u[2];
-    double g0 = dV * ua0, g1 = dV * ua1, g2 = dV * ua2;
-    fi0 += g0; fi1 += g1; fi2 += g2;
-    double* fj = reinterpret_cast<double*>(&A.force[bj[a]]);
-    atomicAdd(fj + 0, -g0);
-    atomicAdd(fj + 1, -g1);
-    atomicAdd(fj + 2, -g2);
-    if (dbdz == 0.0) continue;
-    const R pre = R(0.5 * fc_a * va * dbdz);  // dE / dzeta
-    const R irij = R(1.0 / rij);
-    double gj0 = 0, gj1 = 0, gj2 = 0;
-    for (int b = 0; b < nb; b++) {
-      if (b == a) continue;
-      const R* w = bu[b];
-      const R irik = R(1.0 / br[b]);
-      R ct = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
-      R hc = h - ct;
-      R den = d2 + hc * hc;
-      R g = R(1) + c2d2 * (hc * hc) / den;
-      R dg = R(-2) * c2 * hc / (den * den);
-      R ka = pre * bfcr[b] * dg * irij;
-      R kb = pre * bfcr[b] * dg * irik;
-      R kc = pre * bdfcr[b] * g;
-      double gk0 = (double)(kb * (u[0] - ct * w[0]) + kc * w[0]);
-      double gk1 = (double)(kb * (u[1] - ct * w[1]) + kc * w[1]);
-      double gk2 = (double)(kb * (u[2] - ct * w[2]) + kc * w[2]);
-      gj0 += (double)(ka * (w[0] - ct * u[0]));
-      gj1 += (double)(ka * (w[1] - ct * u[1]));
-      gj2 += (double)(ka * (w[2] - ct * u[2]));
-      double* fk = reinterpret_cast<double*>(&A.force[bj[b]]);
-      atomicAdd(fk + 0, -gk0);
-      atomicAdd(fk + 1, -gk1);
-      atomicAdd(fk + 2, -gk2);
-      fi0 += gk0; fi1 += gk1; fi2 += gk2;
-    }
-    atomicAdd(fj + 0, -gj0);
-    atomicAdd(fj + 1, -gj1);
-    atomicAdd(fj + 2, -gj2);
-    fi0 += gj0; fi1 += gj1; fi2 += gj2;
+    const double rd = (double)sr[base + a];
+    double dfc;
+    const double fc = ts_fc<double>(rd, r1, r2, dfc);
+    const double vr = Aa * exp(-T.l1 * rd), va = -Bb * exp(-T.l2 * rd);
+    double b, bva;
+    R dbdz;
+    ts_border(T, z, va, b, bva, dbdz);
+    ei += 0.5 * fc * (vr + bva);
+    dvs[t] = 0.5 * (dfc * (vr + bva) + fc * (-T.l1 * vr - T.l2 * bva));
+    spre[base + a] = R(0.5 * fc * va) * dbdz;  // dE_i / dzeta_a
   }
-  double* f = reinterpret_cast<double*>(&A.force[i]);
-  atomicAdd(f + 0, fi0);
-  atomicAdd(f + 1, fi1);
-  atomicAdd(f + 2, fi2);
-  A.epot[i] = ei;
+  __syncthreads();
+
+  // ---- per bond a: F_j(i) = -dV_a u_a - sum_{b != a} [(pre_a fc_b + pre_b fc_a) g'(cos_ab)
+  //      (u_b - cos_ab u_a)/r_a + pre_b dfc_a g(cos_ab) u_a]; the triplet (a, b) enters
+  //      zeta_a through k = j_b and zeta_b through k = j_a with the same angle
+  double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+#pragma unroll
+  for (int t = 0; t < PER; t++) {
+    const int a = q + t * TS_TPA;
+    if (a >= nb) continue;
+    const R ax = sux[base + a], ay = suy[base + a], az = suz[base + a];
+    const R fca = sfc[base + a], dfca = sdfc[base + a], pa = spre[base + a];
+    const R ira = R(1) / sr[base + a];
+    R tx = R(0), ty = R(0), tz = R(0);
+    for (int b = 0; b < nb; b++) {
+      if (b == a) continue;
+      const R bx = sux[base + b], by = suy[base + b], bz = suz[base + b];
+      const R ct = ax * bx + ay * by + az * bz;
+      const R hc = h - ct, iden = R(1) / (d2 + hc * hc);
+      const R g = R(1) + c2d2 * (hc * hc) * iden;
+      const R dg = R(-2) * c2 * hc * iden * iden;  // dg / dcos
+      const R pb = spre[base + b];
+      const R coef = (pa * sfc[base + b] + pb * fca) * dg * ira;
+      const R kc = pb * dfca * g;
+      tx += coef * (bx - ct * ax) + kc * ax;
+      ty += coef * (by - ct * ay) + kc * ay;
+      tz += coef * (bz - ct * az) + kc * az;
+    }
+    const double dv = dvs[t];
+    const double4 fj = make_double4(-(dv * (double)ax + (double)tx), -(dv * (double)ay + (double)ty),
+                                    -(dv * (double)az + (double)tz), 0.0);
+    A.tsfb[(size_t)a * A.cap + i] = fj;
+    f0 -= fj.x;
+    f1 -= fj.y;
+    f2 -= fj.z;
+  }
+  // the atom's threads combine by a fixed xor tree (same bits in each)
+#pragma unroll
+  for (int o = 1; o < TS_TPA; o <<= 1) {
+    f0 += __shfl_xor_sync(FULL, f0, o);
+    f1 += __shfl_xor_sync(FULL, f1, o);
+    f2 += __shfl_xor_sync(FULL, f2, o);
+    ei += __shfl_xor_sync(FULL, ei, o);
+  }
+  if (act && q == 0) {
+    A.force[i] = make_double4(f0, f1, f2, 0.0);
+    A.epot[i] = ei;
+    A.tsmask[i] = mask;
+  }
+  if (act && err) atomicOr(&A.st[s].status, ST_BONDS);
+}
+
+// F_l += the bond records of l's partners for their bonds to l (slot order)
+__global__ void __launch_bounds__(TS_APB) k_tsf_gather(Arena A, BlockMap M) {
+  const int s = blk_sys(M);
+  if (s < 0) return;
+  const int i = M.first[blockIdx.x] + threadIdx.x;
+  if (i >= M.end[blockIdx.x]) return;
+  unsigned long long mk = A.tsmask[i];
+  double4 f = A.force[i];
+  bool bad = false;
+  while (mk) {
+    const int m = __ffsll((long long)mk) - 1;
+    mk &= mk - 1ull;
+    const size_t e = (size_t)m * A.cap + i;
+    const int j = A.flist[e];
+    const int r = A.rslot[e];
+    if ((unsigned)j >= (unsigned)A.cap || r >= 64) {
+      bad = true;
+      continue;
+    }
+    const unsigned long long mj = A.tsmask[j];
+    const int a = __popcll(mj & ((1ull << r) - 1ull));
+    if (!((mj >> r) & 1ull) || a >= TS_MAXB) {
+      bad = true;
+      continue;
+    }
+    const double4 b = A.tsfb[(size_t)a * A.cap + j];
+    f.x += b.x;
+    f.y += b.y;
+    f.z += b.z;
+  }
+  A.force[i] = f;
+  if (bad) atomicOr(&A.st[s].status, ST_BONDS);
+}
+
+// reverse slots of the Tersoff systems flagged for a rebuild: for each list
+// entry (i, m) with partner j, the slot of i in j's flist (255: none)
+__global__ void k_tsf_rslot(Arena A, BlockMap M) {
+  rebuild_items(M.nblk, [&](int b) {
+      const int s = M.sys[b];
+      return s >= 0 && A.st[s].rebuild && A.sys[s].ff == FF_TERSOFF;
+    }, [&](int b) {
+      const int i = M.first[b] + threadIdx.x;
+      if (i >= M.end[b]) return;
+      const int n = min(A.nn[i], A.lcap);
+      for (int m = 0; m < n; m++) {
+        const size_t e = (size_t)m * A.cap + i;
+        const int j = A.flist[e];
+        int r = 255;
+        if ((unsigned)j < (unsigned)A.cap) {
+          const int nj = min(min(A.nn[j], A.lcap), 255);
+          for (int k = 0; k < nj; k++)
+            if (A.flist[(size_t)k * A.cap + j] == i) {
+              r = k;
+              break;
+            }
+        }
+        A.rslot[e] = (unsigned char)r;
+      }
+    });
 }
 
 // interleaved [x1,y1,z1,...] staging <-> double4 arena slots

@@ -19,6 +19,7 @@
 #include <mutex>
 
 #include "../../include/gemsgpu.h"
+#include "common.cuh"
 
 namespace {
 
@@ -32,7 +33,11 @@ static __device__ __align__(256) double g_noalloc_scratch[2 * NA_MAX];
 
 // Device address of g_noalloc_scratch per device.  In host code the symbol
 // is only a host-side stand-in, so its device address is looked up once per
-// device (with that device current) and passed to the kernels.
+// device (with that device current) and passed to the kernels.  The cached
+// address belongs to the device's current context: after cudaDeviceReset
+// (or anything else that destroys and re-creates the primary context) the
+// module may load elsewhere, so a process that resets a device must not
+// call gemsgpu_smatb_forces_noalloc on it again.
 std::mutex g_na_mutex;
 double* g_na_addr[NA_MAXDEV] = {nullptr};
 
@@ -181,11 +186,18 @@ extern "C" int gemsgpu_smatb_forces_noalloc(const double* d_pos, int n, int boxe
   c.rce = rce;
   double* scratch = nullptr;
   if (scratch_address(&scratch) != cudaSuccess) return GEMSGPU_ERR_CUDA;
-  // GEMS internal energy unit (src/Constants.F90:101-127)
-  const double ev_ui = 1.0 / (1.0e2 * 1.0e2 * 1.6605402e-27 * (1.0 / 1.60219e-19));
+  double ev_ui = EV_UI;  // GEMS internal energy unit
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int grid = (n + NA_BLOCK - 1) / NA_BLOCK;
-  k_na_rho<<<grid, NA_BLOCK, 0, st>>>(d_pos, n, B, c, scratch);
-  k_na_force<<<grid, NA_BLOCK, 0, st>>>(d_pos, n, B, c, scratch, ev_ui, d_force, d_epot);
-  return cudaGetLastError() == cudaSuccess ? GEMSGPU_OK : GEMSGPU_ERR_CUDA;
+  const dim3 grid((n + NA_BLOCK - 1) / NA_BLOCK), block(NA_BLOCK);
+  // cudaLaunchKernel returns this launch's own status, so an error left
+  // behind by the caller's earlier work is not reported as this call's
+  void* rho_args[] = {(void*)&d_pos, (void*)&n, (void*)&B, (void*)&c, (void*)&scratch};
+  if (cudaLaunchKernel((const void*)k_na_rho, grid, block, rho_args, 0, st) != cudaSuccess)
+    return GEMSGPU_ERR_CUDA;
+  const double* scr = scratch;
+  void* force_args[] = {(void*)&d_pos, (void*)&n, (void*)&B, (void*)&c, (void*)&scr, (void*)&ev_ui,
+                        (void*)&d_force, (void*)&d_epot};
+  if (cudaLaunchKernel((const void*)k_na_force, grid, block, force_args, 0, st) != cudaSuccess)
+    return GEMSGPU_ERR_CUDA;
+  return GEMSGPU_OK;
 }

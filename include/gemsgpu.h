@@ -162,7 +162,9 @@ int gemsgpu_set_sm1(gemsgpu_ctx* ctx, int sys, int ti, int tj, double r1,
 /* `interact g1 feels g2` (src/Interaction.f90:69-76, 128-131): after a pair
  * setter for (ti, tj), the pair acts on the atoms of type ti only (give each
  * group its own type).  Energies count the feeling side's half, as the
- * reference's.  Not with the virial or a piston (no pair virial). */
+ * reference's.  Not with the virial or a piston (no pair virial).  The
+ * direction turned off stays off: a later set_lj / set_slj / set_wca /
+ * set_sm1 of the same pair changes its parameters on the feeling side only. */
 int gemsgpu_set_feels(gemsgpu_ctx* ctx, int sys, int ti, int tj);
 /* Pair virial W = sum_i r_i (x) F_i (inq_virial, Inq_Properties.F90:439-527)
  * accumulated by the force kernels of an lj/plj/slj or SMA-TB system (on=1;

@@ -176,6 +176,10 @@ struct Sys {
   int pbc[3] = {0, 0, 0};
   bool mic = true;  // Program_Types.F90:98
   double skin = 1.0;  // nb_dcut, Neighbour.F90:237
+  // skin test on minimum-image displacements (the device library's default):
+  // an atom wrapped by do_pbc then does not count as having moved a box
+  // length.  Forces are unchanged; the list is rebuilt less often.
+  bool skin_mic = false;
   bool half = false;  // OpenMP default: full lists (Neighbour.F90:160-171)
   // neighbour list, column-major like list(n1+100,mnb)
   int cap = 0;
@@ -385,7 +389,10 @@ bool test_update(Sys& s) {
   double d1 = 1.e-16, d2 = 1.e-16;
   for (int i = 0; i < s.n; i++) {
     double vd[3];
-    for (int l = 0; l < 3; l++) vd[l] = s.pos[3 * i + l] - s.pos_old[3 * i + l];
+    for (int l = 0; l < 3; l++) {
+      vd[l] = s.pos[3 * i + l] - s.pos_old[3 * i + l];
+      if (s.skin_mic && s.boxed && s.pbc[l]) vd[l] = vd[l] - s.box[l] * idnint(vd[l] * s.one_box[l]);
+    }
     double rd = dot3(vd);
     if (rd > d1) {
       d2 = d1;
@@ -1902,6 +1909,7 @@ void orc_set_box(void* p, int boxed, const double* L, const int* pbc) {
 }
 void orc_set_mic(void* p, int mic) { ((Sys*)p)->mic = mic != 0; }
 void orc_set_skin(void* p, double skin) { ((Sys*)p)->skin = skin; }
+void orc_set_skin_mode(void* p, int mic) { ((Sys*)p)->skin_mic = mic != 0; }
 void orc_set_half(void* p, int half) { ((Sys*)p)->half = half != 0; }
 void orc_set_capacity(void* p, int cap) { ensure_cap(*(Sys*)p, cap); }
 

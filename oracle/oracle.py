@@ -60,6 +60,7 @@ def lib():
         "orc_set_box": (None, [_p, _i, _dp, _ip]),
         "orc_set_mic": (None, [_p, _i]),
         "orc_set_skin": (None, [_p, _d]),
+        "orc_set_skin_mode": (None, [_p, _i]),
         "orc_set_half": (None, [_p, _i]),
         "orc_set_capacity": (None, [_p, _i]),
         "orc_set_lj": (None, [_p, _i, _i, _d, _d, _d, _i, _d]),
@@ -276,6 +277,11 @@ class System:
 
     def set_skin(self, skin):
         lib().orc_set_skin(self.h, float(skin))
+
+    def set_skin_mode(self, mic):
+        """True: skin test on minimum-image displacements (fewer rebuilds,
+        same forces); False: the reference's raw displacements (default)."""
+        lib().orc_set_skin_mode(self.h, 1 if mic else 0)
 
     def set_half(self, half):
         lib().orc_set_half(self.h, 1 if half else 0)

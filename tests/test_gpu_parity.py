@@ -234,20 +234,108 @@ def test_lj_fluid_forces(ctx, prec, rms, etol):
     check_forces(o, g, rms, etol)
 
 
-@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, 5e-5, 2e-6)])
-def test_tersoff_forces(ctx, prec, rms, etol):
+def _tersoff_crystal(ctx, ncell, sigma, seed):
+    """Diamond Si(C) of ncell^3 cells with N(0, sigma) displacements (A)."""
     from gems_b200 import workloads as W
-    rng = np.random.default_rng(5)
-    pos = W.diamond(4, 5.431)
-    L = 4 * 5.431
-    pos = np.mod(pos + rng.normal(0, 0.05, pos.shape), L)
+    rng = np.random.default_rng(seed)
+    L = ncell * 5.431
+    pos = np.mod(W.diamond(ncell, 5.431) + rng.normal(0, sigma, (8 * ncell ** 3, 3)), L)
 
     def setup(s):
         s.set_box((L, L, L), (True, True, True))
         s.set_tersoff(W.TERSOFF_SI)
-    o, g = both(pos, W.MASS["Si"], ctx, setup=setup)
+    return both(pos, W.MASS["Si"], ctx, setup=setup)
+
+
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_tersoff_forces(ctx, prec, rms, etol):
+    """512-atom diamond, displacements of 0.05 A."""
+    o, g = _tersoff_crystal(ctx, 4, 0.05, 5)
     g.set_precision(prec)
     check_forces(o, g, rms, etol)
+    g.destroy()
+
+
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_tersoff_forces_32k(ctx, prec, rms, etol):
+    """32768-atom diamond (16^3 cells) with thermal displacements of 0.1 A
+    (about the spread of silicon at 1000 K)."""
+    o, g = _tersoff_crystal(ctx, 16, 0.1, 6)
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+    g.destroy()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_tersoff_forces_reproducible(ctx, prec):
+    """The forces are gathered in a fixed order (no atomics): two evaluations
+    of the same state, and the same state in a second system, give the same
+    bits."""
+    _, g = _tersoff_crystal(ctx, 6, 0.1, 8)
+    _, h = _tersoff_crystal(ctx, 6, 0.1, 8)
+    for s in (g, h):
+        s.set_precision(prec)
+    g.interact()
+    f1, e1 = g.force, g.epot_atoms
+    g.set_pos(g.pos)          # dirty: the next call rebuilds and recomputes
+    g.interact()
+    np.testing.assert_array_equal(g.force, f1)
+    np.testing.assert_array_equal(g.epot_atoms, e1)
+    h.interact()
+    np.testing.assert_array_equal(h.force, f1)
+    g.destroy()
+    h.destroy()
+
+
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_tersoff_open_clusters(ctx, prec, rms, etol):
+    """No box (O(N^2) lists): an isolated atom (no bonds), a dimer (zeta = 0,
+    b = chi), a bent trimer, a bond in the cut-off region (R-D < r < R+D) and
+    a 40-atom random blob, as one system."""
+    from gems_b200 import workloads as W
+    rng = np.random.default_rng(9)
+    blob = W.diamond(2, 5.431)[:40] + rng.normal(0, 0.08, (40, 3))
+    parts = [np.array([[0.0, 0.0, 0.0]]),
+             np.array([[0.0, 0.0, 0.0], [2.3, 0.1, 0.0]]),
+             np.array([[0.0, 0.0, 0.0], [2.35, 0.0, 0.0], [-0.8, 2.2, 0.1]]),
+             np.array([[0.0, 0.0, 0.0], [2.88, 0.05, 0.0], [1.1, 2.1, 0.0]]),
+             blob]
+    pos = np.concatenate([p + 30.0 * k for k, p in enumerate(parts)])
+    o, g = both(pos, W.MASS["Si"], ctx, setup=lambda s: s.set_tersoff(W.TERSOFF_SI))
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+    assert np.all(g.force[0] == 0.0) and g.epot_atoms[0] == 0.0
+    g.destroy()
+
+
+def test_tersoff_batch_equals_alone(ctx):
+    """Tersoff crystals of three sizes, 200 NVE steps as one batch equal each
+    system's 200 steps alone, bit for bit (mixed precision, 1500 K)."""
+    from gems_b200 import workloads as W
+
+    def mk(nc, seed):
+        L = nc * 5.431
+        pos = W.diamond(nc, 5.431)
+        vel = W.maxwell(len(pos), W.MASS["Si"], 1500.0, np.random.default_rng(seed))
+        g = gems.System(pos, W.MASS["Si"], ctx=ctx, vel=vel)
+        g.set_box((L, L, L), (True, True, True))
+        g.set_tersoff(W.TERSOFF_SI)
+        g.set_precision(1)
+        g.set_vv(0.001)
+        g.interact()
+        return g
+    sizes = (4, 6, 5)
+    a = [mk(nc, 60 + k) for k, nc in enumerate(sizes)]
+    b = [mk(nc, 60 + k) for k, nc in enumerate(sizes)]
+    ctx.batch_md_steps(a, 200)
+    for g in b:
+        g.md_steps(200)
+    for ga, gb in zip(a, b):
+        np.testing.assert_array_equal(ga.pos, gb.pos)
+        np.testing.assert_array_equal(ga.vel, gb.vel)
+        assert ga.nupd == gb.nupd
+    for g in a + b:
+        g.destroy()
 
 
 # ------------------------------------------------------------------ golden decks
@@ -321,6 +409,33 @@ def test_gpu_wca_feels_fluid(ctx, prec, rms, etol):
     g.set_precision(prec)
     check_forces(o, g, rms, etol)
     g.destroy()
+
+
+def test_gpu_feels_survives_later_pair_setter(ctx):
+    """set_feels(1, 0) then set_wca of the same pair again (the reversed
+    order): the pair stays one-sided, so the forces equal those of the
+    setter-then-feels order, bit for bit."""
+    rng = np.random.default_rng(22)
+    pos = rng.uniform(0, 9.0, (400, 3))
+    pos = pos[np.all(np.linalg.norm(pos[:, None] - pos[None], axis=-1) + 9 * np.eye(400) > 0.9, axis=1)]
+    types = (np.arange(len(pos)) % 2).astype(np.int32)
+
+    def mk(again):
+        g = gems.System(pos, 39.95, types, 2, ctx=ctx)
+        g.set_box((9.0, 9.0, 9.0), (True, True, True))
+        g.set_wca(1.0, 1.0, ti=0, tj=0)
+        g.set_wca(0.5, 1.05, ti=1, tj=0)
+        g.set_feels(1, 0)
+        if again:
+            g.set_wca(0.5, 1.05, ti=1, tj=0)
+        g.set_wca(0.8, 0.95, ti=1, tj=1)
+        g.interact()
+        return g
+    a, b = mk(False), mk(True)
+    np.testing.assert_array_equal(b.force, a.force)
+    np.testing.assert_array_equal(b.epot_atoms, a.epot_atoms)
+    a.destroy()
+    b.destroy()
 
 
 def test_gpu_feels_guards(ctx):
@@ -478,12 +593,17 @@ def test_gpu_brownian_philox(ctx):
 
 
 @pytest.mark.parametrize("upto", [None, 0.02])
-def test_gpu_scalvel_matches_oracle(ctx, upto):
+@pytest.mark.parametrize("drift", [0.0, 500.0])
+def test_gpu_scalvel_matches_oracle(ctx, upto, drift):
     """scalvel (and scalvel_after with a narrow band) after velocity Verlet
     on the gas of v_verlet.gms, toward 250 K: the device's md_steps rows
-    against the oracle's."""
+    against the oracle's.  drift (A/ps, about 70 thermal speeds) is added to
+    every velocity: the temperature is the kinetic energy about the centre of
+    mass, which must not lose digits to the drift."""
     pos, vel, types, mass, box, _ = decks.he_ne_setup(O)
+    vel = vel + drift * np.array([0.6, -0.48, 0.64])
     g = _he_ne_gpu(ctx)
+    g.set_vel(vel)
     g.set_vv(0.002)
     g.set_scalvel(250.0, 10, upto)
     rows = g.dinamica(400, 50)

@@ -104,3 +104,35 @@ def test_server_admission_by_footprint(ctx):
     with pytest.raises(gems.GemsGpuError):
         srv.submit(np.zeros((1001, 3)), m, sm, gems.JOB_MD, 100)
     srv.close()
+
+
+def test_pool_refuses_what_its_step_does_not_run(ctx):
+    """A pool's captured step runs velocity Verlet, Ermak and FIRE and no
+    thermostat: a predictor-corrector, Brownian or thermostatted system, or
+    one of another force field or precision, is refused by pool_set rather
+    than advanced wrongly."""
+    from gems_b200 import workloads as W
+    sm, m = au()
+    pool = gems.Pool(ctx, 4, 2000, ff=gems.FF_SMATB, prec=gems.PREC_MIXED, lanes=4, variant=1, chunk=50)
+
+    def mk(setup, prec=gems.PREC_MIXED):
+        g = gems.System(W.cluster(40, np.random.default_rng(3)), m, ctx=ctx)
+        g.set_smatb(*sm)
+        g.set_precision(prec)
+        setup(g)
+        return g
+    ok = mk(lambda g: g.set_ermak(0.002, 1.0, 300.0))
+    pool.set([ok])
+    bad = [mk(lambda g: g.set_pred_corr(0.002)),
+           mk(lambda g: g.set_brownian(0.002, 300.0, 1.0)),
+           mk(lambda g: (g.set_vv(0.002), g.set_scalvel(300.0, 10))),
+           mk(lambda g: (g.set_vv(0.002), g.set_andersen(300.0))),
+           mk(lambda g: g.set_vv(0.002), prec=gems.PREC_FP64)]
+    for g in bad:
+        with pytest.raises(gems.GemsGpuError):
+            pool.set([ok, g])
+    pool.set([ok])
+    pool.run(1)
+    pool.close()
+    for g in bad + [ok]:
+        g.destroy()

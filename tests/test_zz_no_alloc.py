@@ -67,3 +67,38 @@ def test_noalloc_matches_context_entry_point():
 
     # sizes beyond the fixed scratch are refused before any launch
     assert call(16385) == -10     # GEMSGPU_ERR_FULL
+
+
+def test_noalloc_open_cluster_matches_oracle():
+    """boxed = 0: a free 600-atom Au cluster (no periodic dimension), two
+    calls in a row, against the FP64 oracle's smatb_interact directly."""
+    torch = pytest.importorskip("torch")
+    import gems_b200 as gems
+    from gems_b200 import workloads as W
+    from oracle import oracle as O
+
+    pos = W.cluster(600, np.random.default_rng(12))
+    n = len(pos)
+    o = O.System(pos, W.MASS["Au"])
+    o.set_smatb(*W.SMATB["Au"])
+    o.interact()
+    f_ref, e_ref = o.force, o.epot_atoms
+
+    fn = gems.lib().gemsgpu_smatb_forces_noalloc
+    dev = torch.device("cuda", 0)
+    d_pos = torch.tensor(pos.ravel(), dtype=torch.float64, device=dev)
+    d_force = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    d_epot = torch.empty(n, dtype=torch.float64, device=dev)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    for _ in range(2):
+        d_force.fill_(float("nan"))
+        d_epot.fill_(float("nan"))
+        rc = fn(ctypes.c_void_p(d_pos.data_ptr()), n, 0, None, None, *W.SMATB["Au"],
+                ctypes.c_void_p(d_force.data_ptr()), ctypes.c_void_p(d_epot.data_ptr()), stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+        f = d_force.cpu().numpy().reshape(n, 3)
+        e = d_epot.cpu().numpy()
+        rms = np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref)
+        assert rms <= RMS_FP64, rms
+        assert np.abs(e - e_ref).max() * gems.UI_EV <= E_FP64
