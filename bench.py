@@ -14,10 +14,14 @@ Arms measured in one run:
   mixed  : FP32 pair math with FP64 accumulation, one system;
   batched: the mixed kernels over --replicas independent 32k-atom replicas
            (different displacement / noise seeds) packed into one launch.
+  batched_fp64: the same replicas in the plain FP64 kernels (splits the
+           headline into batching and precision).
 `value` is the batched arm; every arm is reported.  `e2e` runs the batched
 arm through the C ABI with host buffers: each block uploads positions and
 velocities from pinned memory and reads positions, velocities and energies
-back.
+back.  `e2e_dropin_per_step` times the per-step drop-in path instead: a GEMS
+build that keeps its host integrator and calls gemsgpu_set_positions,
+gemsgpu_forces and gemsgpu_download every MD step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -51,6 +55,9 @@ def parse():
     ap.add_argument("--arms", default="fp64,mixed,batched",
                     help="comma list of arms to run (profiling); the full line needs all three")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--therm-steps", type=int, default=None,
+                    help="reference arm: untimed Ermak steps before timing (default: the GPU arms' %d)"
+                         % THERM_STEPS)
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "next"],
                     help="c2 (default, the headline line) or one of the other configurations")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
@@ -272,6 +279,81 @@ def timed_e2e(ctx, torch, systems, block, steps, warmup, flush, ext_stream):
     return times, h2d, d2h
 
 
+def ermak_consts(dt, gamma, temp):
+    """set_ermak (src/Integration.F90:909-961) for the host-side integrator
+    of the per-step drop-in arm."""
+    from gems_b200 import workloads as W
+    c0 = np.exp(-gamma * dt)
+    c1 = (1.0 - c0) / gamma
+    c2 = (1.0 - c1 / dt) / gamma
+    sdr = np.sqrt(dt / gamma * (2.0 - (3.0 - 4.0 * c0 + c0 * c0) / (gamma * dt)))
+    sdv = np.sqrt(1.0 - c0 * c0)
+    crv1 = (1.0 - c0) ** 2 / (gamma * sdr * sdv)
+    crv2 = np.sqrt(1.0 - crv1 * crv1)
+    return dict(dt=dt, c0=c0, c1=c1, c2=c2, sdr=sdr, sdv=sdv, crv1=crv1, crv2=crv2,
+                skt=np.sqrt(W.KB_UI * temp))
+
+
+def timed_dropin(gems, torch, ctx, ext, s, w, steps, warmup=5):
+    """The per-step drop-in path: a GEMS build that keeps its own (host)
+    integrator and swaps only the force field for the GPU one, through the
+    Fortran interact() shim.  Every MD step: ermak_a on the host, upload of
+    the positions (gemsgpu_set_positions), gemsgpu_forces, download of
+    forces and per-atom energies (gemsgpu_download), ermak_b on the host
+    (src/Integration.F90:963-1031, in numpy).  Timed with CUDA events on the
+    library's stream around `steps` MD steps, host work included."""
+    import ctypes
+    lib = gems.lib()
+    n = s.n
+    K = ermak_consts(w["dt"], w["gamma"], w["temp"])
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+    x, v, a, f, e = pin((n, 3)), pin((n, 3)), pin((n, 3)), pin((n, 3)), pin((n,))
+    x[:] = s.pos
+    v[:] = s.vel
+    a[:] = s.acel
+    m = float(w["mass"])
+    osm = 1.0 / np.sqrt(m)
+    L = np.asarray(w["L"], dtype=np.float64)
+    rng = np.random.default_rng(17)
+    ep = ctypes.c_double()
+    P = lambda arr: arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    px, pf, pe = P(x), P(f), P(e)
+    r = np.empty((2, n, 3))
+    vel_v = np.empty((n, 3))
+
+    def step():
+        rng.standard_normal(out=r)
+        fl = K["skt"] * osm
+        np.multiply(r[0], fl * K["sdr"], out=f)            # pos_v (f is free until the download)
+        x[:] += K["c1"] * v + (K["c2"] * K["dt"]) * a + f
+        np.subtract(x, L * np.floor(x / L), out=x)            # do_pbc
+        np.multiply(fl * K["sdv"], K["crv1"] * r[0] + K["crv2"] * r[1], out=vel_v)
+        ctx.check(lib.gemsgpu_set_positions(ctx.h, s.sid, px))
+        ctx.check(lib.gemsgpu_forces(ctx.h, s.sid, ctypes.byref(ep), None))
+        ctx.check(lib.gemsgpu_download(ctx.h, s.sid, None, None, pf, pe))
+        v[:] = K["c0"] * v + (K["c1"] - K["c2"]) * a + (K["c2"] / m) * f + vel_v
+        np.multiply(f, 1.0 / m, out=a)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(ext)
+    for _ in range(steps):
+        step()
+    e1.record(ext)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1)
+    return {"value": n * steps / (ms * 1e-3), "unit": UNIT, "md_steps": steps, "atoms": n,
+            "ms_per_md_step": ms / steps, "wall_ms_per_md_step": 1e3 * wall / steps,
+            "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 32 * n,
+            "path": "per MD step: host ermak_a, gemsgpu_set_positions, gemsgpu_forces, gemsgpu_download "
+                    "(forces, energies), host ermak_b"}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -404,6 +486,15 @@ def run_reference(args):
     s.set_skin(w["skin"])
     s.set_ermak(w["dt"], w["gamma"], w["temp"], O.Rng(123456))
     s.interact()
+    # the same start as the GPU arms: thermalised at 300 K, here by the CPU
+    # restatement's own Ermak steps (untimed)
+    nth = THERM_STEPS if args.therm_steps is None else max(0, args.therm_steps)
+    t_th = time.perf_counter()
+    for _ in range(nth):
+        s.stepa()
+        s.interact()
+        s.stepb()
+    t_th = time.perf_counter() - t_th
     per = max(1, min(args.block, 5))   # bounded sample per bench step
 
     def blk():
@@ -426,10 +517,13 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": "smatb_au_bulk_32000 (fcc 20^3, Ermak 300 K, dt 2 fs)",
-                       "md_steps_per_bench_step": per, "parallelism": "openmp"},
+                       "md_steps_per_bench_step": per, "parallelism": "openmp",
+                       "start": "thermalised: %d untimed Ermak steps (%.3g ps) from the 0 K lattice, "
+                                "by the CPU restatement itself (%.0f s)" % (nth, nth * w["dt"], t_th),
+                       "skin_test": "the reference's (raw displacements, src/Neighbour.F90:1320)"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "%d blocks of %d MD steps, 32000 atoms, from the 0 K lattice "
-                                       "(the CPU does not thermalise first)" % (args.steps, per)},
+                             "sample": "%d blocks of %d MD steps, 32000 atoms, from the thermalised "
+                                       "300 K state" % (args.steps, per)},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -502,7 +596,10 @@ def run_c5(args, gems, torch, ctx, ext):
     from gems_b200 import workloads as W
     w = W.tersoff_si()
     out = {}
+    want = set(args.arms.split(","))
     for name, prec in (("fp64", gems.PREC_FP64), ("mixed", gems.PREC_MIXED)):
+        if name not in want:
+            continue
         g = gems.System(w["pos"], w["mass"], ctx=ctx, vel=w["vel"])
         g.set_box(w["L"], (True, True, True))
         g.set_tersoff(w["tersoff"])
@@ -510,6 +607,7 @@ def run_c5(args, gems, torch, ctx, ext):
         g.set_precision(prec)
         g.set_vv(w["dt"])
         g.interact()
+        tuned = g.autotune(5)
         ep0, ek0, _ = g.energy()
         val, ms = _time_md(ctx, torch, [g], args.block, args.steps, args.warmup, ext)
         ep1, ek1, _ = g.energy()
@@ -517,9 +615,12 @@ def run_c5(args, gems, torch, ctx, ext):
         nsteps = args.block * (args.steps + args.warmup)
         out[name] = {"value": val, "ms_per_block": ms, "atoms": g.n, "steps_run": nsteps,
                      "etot_drift_ev_per_atom": ((ep1 + ek1) - (ep0 + ek0)) / g.n,
-                     "force_kernel_ms": kern[0], "rebuild_ms": kern[2]}
+                     "bonds_kernel_ms": kern[0], "gather_kernel_ms": kern[1],
+                     "force_kernel_ms": kern[0] + kern[1], "rebuild_ms": kern[2], "rebuilds": g.nupd,
+                     "lanes_variant": list(tuned[:2])}
         g.destroy()
-    _line("atom-steps/s (Tersoff Si 1M, NVE VV)", out["mixed"]["value"], UNIT, args,
+    head = out["mixed"] if "mixed" in out else out["fp64"]
+    _line("atom-steps/s (Tersoff Si 1M, NVE VV)", head["value"], UNIT, args,
           {"workload": "tersoff_si_1000000 (diamond 50^3, a=5.431, 1000 K, dt 1 fs, skin 1.0)",
            "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out,
           **({} if args.no_cpu else {"cpu_baseline": cpu_baseline_c5(args.cpu_seconds)}))
@@ -889,6 +990,29 @@ def main():
     arms["batched"] = {"value": natoms * blk * len(ts) / (sum(ts) * 1e-3), "ms_per_block": sum(ts) / len(ts),
                        "atoms": natoms, "replicas": len(reps), "launches": nl,
                        "lanes_variant": list(reps[0].tuned[:2])}
+    # --- batched FP64 arm: the same replicas in the plain FP64 kernels, so
+    # the headline splits into batching (batched_fp64 / fp64) and precision
+    # inside the batch (batched / batched_fp64)
+    reps64 = [make_system(gems, ctx, c2_replica(100 + k + 1000 * rank), gems.PREC_FP64, seed=100 + k,
+                          tune=(1, 1), therm=0) for k in range(args.replicas)]
+    ctx.batch_md_steps(reps64, THERM_STEPS)
+    if FIXED_TUNE is None:
+        ctx.batch_autotune(reps64, 10)
+    for s in reps64:
+        s.interact()
+    ts64, nl64 = timed_blocks(ctx, torch, reps64, blk, args.steps, args.warmup, flush, ext)
+    arms["batched_fp64"] = {"value": natoms * blk * len(ts64) / (sum(ts64) * 1e-3),
+                            "ms_per_block": sum(ts64) / len(ts64), "atoms": natoms, "replicas": len(reps64),
+                            "launches": nl64, "lanes_variant": list(reps64[0].tuned[:2])}
+    for s in reps64:
+        s.destroy()
+    # --- per-step drop-in e2e (forces on the GPU, integrator on the host)
+    dropin = {}
+    for name, prec in (("fp64", gems.PREC_FP64), ("mixed", gems.PREC_MIXED)):
+        s = make_system(gems, ctx, w, prec, seed=300 + rank, tune=tuple(arms[name]["lanes_variant"]))
+        s.interact()
+        dropin[name] = timed_dropin(gems, torch, ctx, ext, s, w, max(50, 10 * args.steps))
+        s.destroy()
     # --- e2e through the C ABI with host buffers
     te, h2d, d2h = timed_e2e(ctx, torch, reps, blk, args.steps, args.warmup, flush, ext)
     e2e_ms = max_over_ranks(sum(te), dist, "cuda")
@@ -938,7 +1062,11 @@ def main():
             "arms": arms,
             "speedup_batched_vs_fp64": arms["batched"]["value"] / arms["fp64"]["value"],
             "speedup_mixed_vs_fp64": arms["mixed"]["value"] / arms["fp64"]["value"],
-            "e2e": e2e, "roofline": roofline, "clocks": ck, "gpu_launches": nl}
+            "speedup_split": {"batching_fp64": arms["batched_fp64"]["value"] / arms["fp64"]["value"],
+                              "precision_in_batch": arms["batched"]["value"] / arms["batched_fp64"]["value"],
+                              "precision_single": arms["mixed"]["value"] / arms["fp64"]["value"]},
+            "e2e": e2e, "e2e_dropin_per_step": dropin,
+            "roofline": roofline, "clocks": ck, "gpu_launches": nl}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, therm_state)
     if rank == 0:

@@ -101,7 +101,7 @@ struct SysDev {
   float fx_inv[3];     // fixed-point unit (A), rounded to float ...
   float fx_inv_lo[3];  // ... and its rounding remainder (hi + lo = unit)
   int skin_mic;        // skin test on minimum-image displacements
-  int pad0;
+  int list_warp;       // cells of few atoms: the list kernel works one warp per cell
   // integrator
   double dt;
   double cc0, cc1, cc2, sdr, sdv, crv1, crv2, skt;
@@ -215,7 +215,8 @@ struct Arena {
   double2* minv;        // (1/m, 1/sqrt(m))
   double* mass;
   int* type;
-  int* nn;              // neighbours per atom
+  int* nn;              // neighbours per atom (flist entries: the full list)
+  int* hnn;             // half-list systems: entries of `list` (the half list)
   int* list;            // column-major: list[m * cap + i], the reference's order
   int* flist;           // the same pairs sorted by distance at the rebuild
                         // (force kernels: a warp's atoms meet the same shell
@@ -233,10 +234,12 @@ struct Arena {
   // Tersoff: rslot[m * cap + i] = the slot of i in the flist of its m-th
   // neighbour (255: none), built with the list; per step, tsmask[i] marks
   // the flist slots of i that are bonds and tsfb[a * cap + i] holds the force
-  // that centre i's energy puts on the partner of its a-th bond
+  // that centre i's energy puts on the partner of its a-th bond (tsfb32 in
+  // mixed precision)
   unsigned char* rslot;
   unsigned long long* tsmask;
-  double4* tsfb;
+  double4* tsfb;        // FP64 systems
+  float4* tsfb32;       // mixed systems
   double* ext_normals;  // parity-mode Ermak normals (6 per atom)
   double2* blk_top2;    // per-block top-2 displacement^2
   double* blk_red;      // per-block partial sums

@@ -296,6 +296,7 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   CHK(dgrow(ctx, &A.mass, keep, nc));
   CHK(dgrow(ctx, &A.type, keep, nc));
   CHK(dgrow(ctx, &A.nn, keep, nc));
+  CHK(dgrow(ctx, &A.hnn, keep, nc));
   CHK(dgrow(ctx, &A.ncut, keep, nc));
   CHK(dgrow(ctx, &A.cell_of, keep, nc));
   CHK(dgrow(ctx, &A.slot, keep, nc));
@@ -342,15 +343,30 @@ int tersoff_records(gemsgpu_ctx* ctx) {
   CU(cudaStreamSynchronize(ctx->stream));
   if (A.tsmask) CU(cudaFree(A.tsmask));
   if (A.tsfb) CU(cudaFree(A.tsfb));
+  if (A.tsfb32) CU(cudaFree(A.tsfb32));
   A.tsmask = nullptr;
   A.tsfb = nullptr;
+  A.tsfb32 = nullptr;
   CHK(dalloc(ctx, &A.tsmask, n));
   CU(cudaMemsetAsync(A.tsmask, 0, n * sizeof(unsigned long long), ctx->stream));
   CHK(dalloc(ctx, &A.tsfb, (size_t)TS_MAXB * n));
+  CHK(dalloc(ctx, &A.tsfb32, (size_t)TS_MAXB * n));
   if (!A.rslot && A.lcap > 0) {
     CHK(dalloc(ctx, &A.rslot, (size_t)A.lcap * n));
     CU(cudaMemsetAsync(A.rslot, 0xff, (size_t)A.lcap * n, ctx->stream));
   }
+  return 0;
+}
+
+// dynamic shared memory of the two cell-list kernels for list capacity lcap
+int list_smem_attr(gemsgpu_ctx* ctx, int lcap) {
+  const size_t smem = list_smem(lcap), smemw = listw_smem(lcap);
+  if (smem > 200 * 1024 || smemw > 200 * 1024)
+    return fail(ctx, GEMSGPU_ERR_ARG, "neighbour capacity %d too large", lcap);
+  if (smem > 48 * 1024)
+    CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smemw > 48 * 1024)
+    CU(cudaFuncSetAttribute(k_list_cells_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw));
   return 0;
 }
 
@@ -382,11 +398,7 @@ int grow_list(gemsgpu_ctx* ctx, int lcap) {
     A.rslot = nr;
   }
   A.lcap = lcap;
-  size_t smem = list_smem(lcap);
-  if (smem > 48 * 1024) {
-    if (smem > 200 * 1024) return fail(ctx, GEMSGPU_ERR_ARG, "neighbour capacity %d too large", lcap);
-    CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  }
+  CHK(list_smem_attr(ctx, lcap));
   invalidate(ctx);
   return 0;
 }
@@ -506,6 +518,8 @@ void derive(gemsgpu_ctx* ctx, SysHost& h) {
     }
   }
   d.ncell = d.use_cells ? d.nc[0] * d.nc[1] * d.nc[2] : 0;
+  // cells of fewer atoms than a CTA's warps: the warp-per-cell list kernel
+  d.list_warp = d.use_cells && (double)h.n < 6.0 * d.ncell ? 1 : 0;
   // fixed-point frame of the mixed kernels
   for (int k = 0; k < 3; k++) {
     bool per = d.boxed && d.pbc[k];
@@ -760,12 +774,29 @@ void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, 
 }
 
 // Tersoff forces: bond records per centre atom, then the per-atom gather
-// (both on the TS_APB-atom map)
-void tersoff_pass(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
-  if (prec == PREC_MIXED) k_tsf_bonds<float><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
-  else k_tsf_bonds<double><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+// (both on the TS_APB-atom map).  variant bit 1: the bond kernel built for
+// four blocks per SM (autotuned).
+void tersoff_bonds(gemsgpu_ctx* ctx, int prec, int variant, const BlockMap& m) {
+  const bool capped = (variant & 2) != 0;
+  if (prec == PREC_MIXED) {
+    if (capped) k_tsf_bonds<float, 4><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+    else k_tsf_bonds<float, 1><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  } else {
+    if (capped) k_tsf_bonds<double, 4><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+    else k_tsf_bonds<double, 1><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
+  }
   ++ctx->launches;
-  k_tsf_gather<<<m.nblk, TS_APB, 0, ctx->stream>>>(ctx->A, m); ++ctx->launches;
+}
+
+void tersoff_gather(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
+  if (prec == PREC_MIXED) k_tsf_gather<float><<<m.nblk, TS_APB, 0, ctx->stream>>>(ctx->A, m);
+  else k_tsf_gather<double><<<m.nblk, TS_APB, 0, ctx->stream>>>(ctx->A, m);
+  ++ctx->launches;
+}
+
+void tersoff_pass(gemsgpu_ctx* ctx, int prec, int variant, const BlockMap& m) {
+  tersoff_bonds(ctx, prec, variant, m);
+  tersoff_gather(ctx, prec, m);
 }
 
 void lj_pass(gemsgpu_ctx* ctx, int prec, int K, bool vir, const BlockMap& m) {
@@ -785,7 +816,6 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   for (int s : ss) {
     const SysHost& h = ctx->sys[s];
     if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no force field", s);
-    if (h.d.half) return fail(ctx, GEMSGPU_ERR_STATE, "system %d: force kernels need full lists", s);
     int K = h.d.ff == FF_TERSOFF ? TS_TPA : h.lanes;
     int key = h.variant * 2 + (h.ntypes == 1 ? 1 : 0);
     groups[{h.d.ff, h.d.prec, K, key, h.d.virial}].push_back(s);
@@ -798,7 +828,7 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
     BlockMap m;
     CHK(get_map(ctx, kv.second, BLOCK / K, 0, &m));
     if (ff == FF_TERSOFF) {
-      tersoff_pass(ctx, prec, m);
+      tersoff_pass(ctx, prec, variant, m);
       continue;
     }
     if (ff == FF_SMATB) {
@@ -836,8 +866,17 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 
     k_scan2<<<(int)ss.size(), BLOCK, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
     k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
     k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
-    k_list_cells<<<rebuild_grid(ctx, mc1.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc1);
-    ++ctx->launches;
+    bool wide = false, narrow = false;
+    for (int s : ss)
+      if (ctx->sys[s].d.use_cells) (ctx->sys[s].d.list_warp ? narrow : wide) = true;
+    if (wide) {
+      k_list_cells<<<rebuild_grid(ctx, mc1.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc1);
+      ++ctx->launches;
+    }
+    if (narrow) {
+      k_list_cells_w<<<rebuild_grid(ctx, mc8.nblk), BLOCK, listw_smem(A.lcap), st>>>(A, mc8);
+      ++ctx->launches;
+    }
   }
   if (n2) {
     k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
@@ -912,7 +951,7 @@ bool can_fuse_forces(const gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   if (!ctx->fuse_forces || !can_fuse_steps(ctx, ss)) return false;
   for (int s : ss) {
     const SysHost& h = ctx->sys[s];
-    if (h.d.ff != FF_SMATB || h.d.virial || h.d.half) return false;
+    if (h.d.ff != FF_SMATB || h.d.virial) return false;
     if (h.d.prec == PREC_MIXED && (h.ntypes != 1 || (h.variant & 1))) return false;
   }
   return true;
@@ -1097,23 +1136,33 @@ int interact_group(gemsgpu_ctx* ctx, const std::vector<int>& ss, bool sync_check
   return 0;
 }
 
+// Epot, Ekin, max |F|^2 and the status of each system of ss (4 doubles per
+// system, in the order of ss): two grid-wide passes over the atom map
 int reduce_sys(gemsgpu_ctx* ctx, const std::vector<int>& ss, std::vector<double>& out) {
-  int n = (int)ss.size();
-  if (n > ctx->h_red_cap) {
+  const int n = (int)ss.size();
+  const int sc = ctx->scap;
+  if (sc > ctx->h_red_cap) {
     if (ctx->h_red) cudaFreeHost(ctx->h_red);
     if (ctx->d_red) cudaFree(ctx->d_red);
-    CU(cudaMallocHost((void**)&ctx->h_red, 4 * sizeof(double) * n));
-    CHK(dalloc(ctx, &ctx->d_red, 4 * (size_t)n));
-    ctx->h_red_cap = n;
+    ctx->h_red = nullptr;
+    ctx->d_red = nullptr;
+    CU(cudaMallocHost((void**)&ctx->h_red, 4 * sizeof(double) * sc));
+    CHK(dalloc(ctx, &ctx->d_red, 7 * (size_t)sc));  // 4 results + the centre-of-mass velocity
+    ctx->h_red_cap = sc;
   }
-  const int* sa;
-  CHK(sys_array(ctx, ss, &sa));
-  k_sys_reduce<<<n, BLOCK, 0, ctx->stream>>>(ctx->A, sa, n, ctx->d_red); ++ctx->launches;
+  BlockMap m;
+  CHK(get_map(ctx, ss, BLOCK, 0, &m));
+  if (m.nblk > 0) {
+    k_sys_reduce<0><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, sc, ctx->d_red);
+    k_sys_reduce<1><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, sc, ctx->d_red);
+    ctx->launches += 2;
+  }
   CU(cudaGetLastError());
-  CU(cudaMemcpyAsync(ctx->h_red, ctx->d_red, 4 * sizeof(double) * n, cudaMemcpyDeviceToHost,
-                     ctx->stream));
+  CU(cudaMemcpyAsync(ctx->h_red, ctx->d_red, 4 * sizeof(double) * sc, cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
-  out.assign(ctx->h_red, ctx->h_red + 4 * n);
+  out.assign(4 * (size_t)n, 0.0);
+  for (int k = 0; k < n; k++)
+    for (int q = 0; q < 4; q++) out[4 * (size_t)k + q] = ctx->h_red[4 * (size_t)ss[k] + q];
   return 0;
 }
 
@@ -1632,7 +1681,8 @@ int pool_rebuild(gemsgpu_pool* P, int in_graph) {
   k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
   k_list_cells<<<rebuild_grid(ctx, mc8.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc8);
-  ++ctx->launches;
+  k_list_cells_w<<<rebuild_grid(ctx, mc8.nblk), BLOCK, listw_smem(A.lcap), st>>>(A, mc8);
+  ctx->launches += 2;
   k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   if (P->ff == FF_TERSOFF) {
     k_tsf_rslot<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
@@ -1654,7 +1704,7 @@ int pool_forces(gemsgpu_pool* P) {
   } else if (P->ff == FF_LJ) {
     lj_pass(ctx, P->prec, P->lanes, false, mk);
   } else if (P->ff == FF_TERSOFF) {
-    tersoff_pass(ctx, P->prec, mk);
+    tersoff_pass(ctx, P->prec, P->variant, mk);
   }
   CU(cudaGetLastError());
   return 0;
@@ -1793,9 +1843,7 @@ int pool_chunk(gemsgpu_pool* P) {
     // the fixed-point copies were left at the undone chunk's positions
     k_refresh_fx<<<P->maps[0].nblk, BLOCK, 0, ctx->stream>>>(ctx->A, P->maps[0]); ++ctx->launches;
     CHK(grow_list(ctx, grow + grow / 4 + 8));
-    if (list_smem(ctx->A.lcap) > 48 * 1024)
-      CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)list_smem(ctx->A.lcap)));
+    CHK(list_smem_attr(ctx, ctx->A.lcap));
     k_force_rebuild<<<(P->max_systems + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, P->dsys, P->max_systems);
     ++ctx->launches;
     k_clear_status<<<(P->max_systems + 255) / 256, 256, 0, ctx->stream>>>(ctx->A, P->dsys, P->max_systems);
@@ -1876,9 +1924,9 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   drop_maps(ctx);
   Arena& A = ctx->A;
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.acel2, A.acel3, A.acel4, A.epot, A.band, A.eband,
-                  A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.ncut, A.list, A.flist, A.cell_of, A.slot,
+                  A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.hnn, A.ncut, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
-                  A.rslot, A.tsmask, A.tsfb,
+                  A.rslot, A.tsmask, A.tsfb, A.tsfb32,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys};
   for (void* p : ptrs)
@@ -2280,8 +2328,10 @@ int gemsgpu_get_list(gemsgpu_ctx* ctx, int sys, int* nn, int* list, int cap, int
   CHK(check_sys(ctx, sys));
   const SysHost& h = ctx->sys[sys];
   std::vector<int> hn(h.n);
-  CU(cudaMemcpyAsync(hn.data(), ctx->A.nn + h.off, h.n * sizeof(int), cudaMemcpyDeviceToHost,
-                     ctx->stream));
+  // a half-list system's `list` holds the half list (hnn entries); flist
+  // holds the full list the force kernels use
+  CU(cudaMemcpyAsync(hn.data(), (h.d.half ? ctx->A.hnn : ctx->A.nn) + h.off, h.n * sizeof(int),
+                     cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   int mx = 0;
   for (int v : hn) mx = std::max(mx, v);
@@ -3130,6 +3180,7 @@ static int autotune_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, 
   std::vector<std::pair<int, int>> cand;
   if (h0.d.ff == FF_TERSOFF) {
     cand.push_back({TS_TPA, 1});
+    cand.push_back({TS_TPA, 3});
   } else {
     for (int K : {1, 2, 4, 8, 16, 32}) {
       cand.push_back({K, 1});
@@ -4267,12 +4318,15 @@ static int time_kernels_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int re
   CHK(sys_array(ctx, ss, &sa));
   cudaEvent_t ev[4];
   for (auto& e : ev) CU(cudaEventCreate(&e));
+  const bool ts = h.d.ff == FF_TERSOFF;
   auto first_kernel = [&]() {
     if (h.d.ff == FF_SMATB) smatb_pass(ctx, 0, h.d.prec, h.variant, single, K, m);
+    else if (ts) tersoff_bonds(ctx, h.d.prec, h.variant, m);
     else launch_forces(ctx, ss);
   };
   auto second_kernel = [&]() {
     if (h.d.ff == FF_SMATB) smatb_pass(ctx, 1, h.d.prec, h.variant, single, K, m);
+    else if (ts) tersoff_gather(ctx, h.d.prec, m);
   };
   first_kernel();
   second_kernel();
@@ -4287,6 +4341,8 @@ static int time_kernels_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int re
     CHK(launch_rebuild(ctx, ss));
   }
   CU(cudaEventRecord(ev[3], ctx->stream));
+  // the Tersoff gather adds to the forces: one untimed evaluation leaves them right
+  if (ts) tersoff_pass(ctx, h.d.prec, h.variant, m);
   CU(cudaEventSynchronize(ev[3]));
   float t[3];
   CU(cudaEventElapsedTime(&t[0], ev[0], ev[1]));

@@ -12,6 +12,7 @@
 //    operations (no FMA contraction) so they decide exactly as the reference.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 #include "common.cuh"
 
@@ -458,15 +459,16 @@ __global__ void k_sort_cells(Arena A, BlockMap C) {
 }
 
 // ------------------------------------------------------------------ lists
-__device__ __forceinline__ void list_put(const Arena& A, int i, int m, int j) {
-  if (m < A.lcap) {
-    A.list[(size_t)m * A.cap + i] = j;
-    A.flist[(size_t)m * A.cap + i] = j;  // O(N^2) lists keep index order for the forces too
-  }
-}
-
-__device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m) {
+// Every system's force kernels read `flist`, a full list (each pair from
+// both sides), with nn[i] entries.  `list` holds the reference's list, the
+// one gemsgpu_get_list returns: the same full list, or for a half-list
+// system (Newton on, src/Neighbour.F90:160-171) the half list with hnn[i]
+// entries.  A half list with the reaction added to j gives every atom the
+// same force, density and energy as the full list (src/TB.F90:432-441,
+// 542-552; src/Pairs.F90:248-252), so the force kernels need no half form.
+__device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m, int mh) {
   A.nn[i] = m;
+  A.hnn[i] = mh;
   A.pos_old[i] = A.pos[i];
   if (m > A.lcap) atomicOr(&A.st[s].status, ST_OVERFLOW);
   atomicMax(&A.st[s].maxnn, m);
@@ -537,6 +539,44 @@ __device__ __forceinline__ int live_entries(const Arena& A, const SysDev& S, con
   return min(nn, (int)((k & 1) ? (w >> 16) : (w & 0xffffu)));
 }
 
+// A warp's staged row of atom i (m accepted candidates in the reference's
+// order: ids, bit 31 set on the entries a half list leaves out, and r^2 as
+// float) out to the arena: `list` in the reference's order, `flist` ranked
+// by distance, the skip counts and nn / hnn.
+__device__ __forceinline__ void list_row_out(const Arena& A, const SysDev& S, int s, int i, int m,
+                                             const int* row, const float* rrow, int ln) {
+  const int n = min(m, A.lcap);
+  // the reference's list: the whole row, or its half-list entries in order
+  int mh = 0;
+  for (int e0 = 0; e0 < n; e0 += 32) {
+    const int e = e0 + ln;
+    const bool h = e < n && row[e] >= 0;
+    const unsigned hb = __ballot_sync(0xffffffffu, h);
+    if (h) A.list[(size_t)(mh + __popc(hb & ((1u << ln) - 1u))) * A.cap + i] = row[e];
+    mh += __popc(hb);
+  }
+  if (n <= 64) {
+    // force order by a warp bitonic sort of (distance, slot) keys
+    unsigned long long k0, k1;
+    warp_sort64(rrow, n, ln, k0, k1);
+    if (ln < n) A.flist[(size_t)ln * A.cap + i] = row[(int)(k0 & 0xffffffffu)] & 0x7fffffff;
+    if (ln + 32 < n) A.flist[(size_t)(ln + 32) * A.cap + i] = row[(int)(k1 & 0xffffffffu)] & 0x7fffffff;
+  } else {
+    for (int e = ln; e < n; e += 32) {
+      // force order: rank by distance, ties by slot
+      const float re = rrow[e];
+      int rank = 0;
+      for (int f = 0; f < n; f++) {
+        const float rf = rrow[f];
+        rank += (rf < re) || (rf == re && f < e);
+      }
+      A.flist[(size_t)rank * A.cap + i] = row[e] & 0x7fffffff;
+    }
+  }
+  list_counts(A, S, i, n, rrow, ln);
+  if (ln == 0) list_done(A, s, i, m, mh);
+}
+
 // linkedcell_self / linkedcell_selfhalf (src/Neighbour.F90:991-1161): the
 // 27 (or 14) stencil cells in the reference's order with periodic cell
 // wrap (cell_pbc, :1350-1376); keep j if rd < (rcut+nb_dcut)^2 (strict).
@@ -572,7 +612,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
   // over every CTA whatever the grid size
   auto live = [&](int w) {
     const int b = w % C.nblk, part = w / C.nblk;
-    if (!rebuild_block(A, C, b, true)) return false;
+    if (!rebuild_block(A, C, b, true) || A.sys[C.sys[b]].list_warp) return false;
     // one-cell blocks: is there an atom pass for this part?
     return C.end[b] - C.first[b] != 1 || part * LIST_ATOMS < A.cell_n[C.first[b]];
   };
@@ -580,7 +620,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
     const int b = w % C.nblk, part = w / C.nblk;
     const int s = C.sys[b];
     const SysDev& S = A.sys[s];
-    const int nst = S.half ? 14 : 27;
+    const int nst = 27;  // half lists: the first 14 stencil cells are the half stencil
     for (int c = C.first[b]; c < C.end[b]; c++) {
       const int cnt0 = A.cell_n[c];
       const int a_first = part * LIST_ATOMS;
@@ -609,6 +649,7 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
       __syncthreads();
       const int T = nb_pref[nst];     // candidates of every atom of the cell
       const int own = nb_pref[1];     // the first cell of the stencil is the cell itself
+      const int hend = nb_pref[14];   // end of the half stencil's candidates
       const int beg0 = nb_start[0];
       for (int a0 = a_first; a0 < cnt0; a0 += LIST_ATOMS * LIST_SPLIT) {
         const int a = a0 + warp;      // this warp's atom: chain position a of the cell
@@ -637,21 +678,23 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
             bool ok = false;
             int j = -1;
             double rd = 0.0;
+            bool in_half = true;
             if (act && q < tn) {
               const int g = t0 + q;
               j = cidx[q];
-              // half lists take only the atoms after i in its own cell's chain
-              const bool skip = (S.half && g < own) ? (g <= a) : (j == i);
-              if (!skip) {
+              if (j != i) {
                 rd = rd_exact(S, xi, cpos[q]);
                 ok = rd < S.rlist2;
               }
+              // the half list (linkedcell_selfhalf): the atoms after i in its
+              // own cell's chain, then the other 13 cells of the half stencil
+              if (S.half) in_half = g < own ? g > a : g < hend;
             }
             const unsigned bal = __ballot_sync(0xffffffffu, ok);
             if (ok) {
               const int mm = m + __popc(bal & ((1u << ln) - 1u));
               if (mm < A.lcap) {
-                row[mm] = j;
+                row[mm] = in_half ? j : (int)((unsigned)j | 0x80000000u);  // bit 31: full list only
                 rrow[mm] = (float)rd;
               }
             }
@@ -659,34 +702,124 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
           }
         }
         __syncwarp();
-        if (act) {
-          const int n = min(m, A.lcap);
-          if (n <= 64) {
-            // force order by a warp bitonic sort of (distance, slot) keys
-            for (int e = ln; e < n; e += 32) A.list[(size_t)e * A.cap + i] = row[e];
-            unsigned long long k0, k1;
-            warp_sort64(rrow, n, ln, k0, k1);
-            if (ln < n) A.flist[(size_t)ln * A.cap + i] = row[(int)(k0 & 0xffffffffu)];
-            if (ln + 32 < n) A.flist[(size_t)(ln + 32) * A.cap + i] = row[(int)(k1 & 0xffffffffu)];
-          } else {
-            for (int e = ln; e < n; e += 32) {
-              A.list[(size_t)e * A.cap + i] = row[e];
-              // force order: rank by distance, ties by slot
-              const float re = rrow[e];
-              int rank = 0;
-              for (int f = 0; f < n; f++) {
-                const float rf = rrow[f];
-                rank += (rf < re) || (rf == re && f < e);
-              }
-              A.flist[(size_t)rank * A.cap + i] = row[e];
-            }
-          }
-          list_counts(A, S, i, n, rrow, ln);
-          if (ln == 0) list_done(A, s, i, m);
-        }
+        if (act) list_row_out(A, S, s, i, m, row, rrow, ln);
         __syncwarp();
       }
       __syncthreads();  // nb_* and the tile are rewritten for the next cell
+    }
+  });
+}
+
+// The same lists for systems whose cells hold few atoms (Tersoff's 4 A
+// cells hold about three): one warp per cell, so no warp of a CTA idles.
+// Lanes 0..26 read the stencil cells' starts and counts and a warp scan
+// gives each cell's first candidate; a lane finds its candidate's stencil
+// cell by a binary search over the scan (shuffles) and stages id and
+// position in the warp's shared tile; the cell's atoms are then tested one
+// after another exactly as in k_list_cells.  Map: 8 cells per block (one per
+// warp).
+constexpr int LISTW_TILE = 128;  // candidates a warp stages at a time
+__host__ __device__ constexpr size_t listw_smem(int lcap) {
+  return (size_t)(BLOCK / 32) * (LISTW_TILE * (sizeof(double4) + sizeof(int)) + (size_t)lcap * (sizeof(int) + sizeof(float)));
+}
+
+__global__ void __launch_bounds__(BLOCK) k_list_cells_w(Arena A, BlockMap C) {
+  extern __shared__ __align__(32) unsigned char listw_sh[];
+  const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  unsigned char* mine = listw_sh + (size_t)warp * (LISTW_TILE * (sizeof(double4) + sizeof(int)) +
+                                                   (size_t)A.lcap * (sizeof(int) + sizeof(float)));
+  double4* cpos = reinterpret_cast<double4*>(mine);
+  int* cidx = reinterpret_cast<int*>(cpos + LISTW_TILE);
+  int* row = cidx + LISTW_TILE;
+  float* rrow = reinterpret_cast<float*>(row + A.lcap);
+  rebuild_items(C.nblk, [&](int b) { return rebuild_block(A, C, b, true) && A.sys[C.sys[b]].list_warp; },
+                [&](int b) {
+    const int c = C.first[b] + warp;
+    if (c >= C.end[b]) return;  // warp-uniform
+    const int s = C.sys[b];
+    const SysDev& S = A.sys[s];
+    const int cl = c - S.cell_off;
+    const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
+    int cs = 0, cn = 0;
+    if (ln < NSTENCIL) {
+      int dx, dy, dz;
+      stencil(ln, dx, dy, dz);
+      const int x = (cx + dx + S.nc[0]) % S.nc[0];
+      const int y = (cy + dy + S.nc[1]) % S.nc[1];
+      const int z = (cz + dz + S.nc[2]) % S.nc[2];
+      const int cid = S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
+      cs = A.cell_start[cid];
+      cn = A.cell_n[cid];
+    }
+    int inc = cn;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, inc, o);
+      if (ln >= o) inc += t;
+    }
+    const int ex = inc - cn;                          // first candidate of stencil cell ln
+    const int T = __shfl_sync(FULL, inc, NSTENCIL - 1);  // candidates of every atom of the cell
+    const int own = __shfl_sync(FULL, inc, 0);        // the cell itself: its atoms come first
+    const int hend = __shfl_sync(FULL, inc, 13);      // end of the half stencil's candidates
+    const int beg0 = __shfl_sync(FULL, cs, 0);
+    for (int a = 0; a < own; a++) {
+      const int i = A.cell_atoms[beg0 + a];
+      const double4 xi = A.pos[i];
+      int m = 0;
+      for (int t0 = 0; t0 < T; t0 += LISTW_TILE) {
+        const int tn = min(LISTW_TILE, T - t0);
+        if (T > LISTW_TILE || a == 0) {  // one tile stays staged for all the cell's atoms
+          __syncwarp();
+          for (int q0 = 0; q0 < tn; q0 += 32) {
+            const int q = q0 + ln;
+            const int g = t0 + q;
+            // the last stencil cell whose first candidate is <= g (an empty
+            // cell shares its first candidate with the next, non-empty one)
+            int k = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+              const int kk = min(k + step, NSTENCIL - 1);
+              const int e = __shfl_sync(FULL, ex, kk);
+              if (k + step < NSTENCIL && e <= g) k = kk;
+            }
+            const int st = __shfl_sync(FULL, cs, k), ek = __shfl_sync(FULL, ex, k);
+            if (q < tn) {
+              const int j = A.cell_atoms[st + (g - ek)];
+              cidx[q] = j;
+              cpos[q] = A.pos[j];
+            }
+          }
+          __syncwarp();
+        }
+        for (int q0 = 0; q0 < tn; q0 += 32) {
+          const int q = q0 + ln;
+          bool ok = false, in_half = true;
+          int j = -1;
+          double rd = 0.0;
+          if (q < tn) {
+            const int g = t0 + q;
+            j = cidx[q];
+            if (j != i) {
+              rd = rd_exact(S, xi, cpos[q]);
+              ok = rd < S.rlist2;
+            }
+            if (S.half) in_half = g < own ? g > a : g < hend;
+          }
+          const unsigned bal = __ballot_sync(FULL, ok);
+          if (ok) {
+            const int mm = m + __popc(bal & ((1u << ln) - 1u));
+            if (mm < A.lcap) {
+              row[mm] = in_half ? j : (int)((unsigned)j | 0x80000000u);
+              rrow[mm] = (float)rd;
+            }
+          }
+          m += __popc(bal);
+        }
+      }
+      __syncwarp();
+      list_row_out(A, S, s, i, m, row, rrow, ln);
+      __syncwarp();
     }
   });
 }
@@ -702,7 +835,7 @@ __global__ void k_list_n2(Arena A, BlockMap M) {
     int i = M.first[b] + threadIdx.x;
     bool act = i < M.end[b];
     double4 xi = act ? A.pos[i] : make_double4(0, 0, 0, 0);
-    int m = 0;
+    int m = 0, mh = 0;
     const int j0 = S.off, j1 = S.off + S.n;
     for (int base = j0; base < j1; base += BLOCK) {
       int j = base + threadIdx.x;
@@ -713,14 +846,21 @@ __global__ void k_list_n2(Arena A, BlockMap M) {
       if (act) {
         for (int t = 0; t < nt; t++) {
           int jj = base + t;
-          if (S.half ? (jj <= i) : (jj == i)) continue;
+          if (jj == i) continue;
           double rd = rd_exact(S, xi, tile[t]);
           if (rd > S.rlist2) continue;
-          list_put(A, i, m++, jj);
+          // flist: every pair in index order (O(N^2) lists are not
+          // distance-sorted); list: a half list keeps j > i only
+          if (m < A.lcap) A.flist[(size_t)m * A.cap + i] = jj;
+          m++;
+          if (!S.half || jj > i) {
+            if (mh < A.lcap) A.list[(size_t)mh * A.cap + i] = jj;
+            mh++;
+          }
         }
       }
     }
-    if (act) list_done(A, s, i, m);
+    if (act) list_done(A, s, i, m, mh);
     __syncthreads();  // the tile is reused by the next block
   });
 }
@@ -1561,7 +1701,10 @@ __device__ __forceinline__ void ts_border(const TersoffP& T, double z, double va
 __device__ __forceinline__ void ts_border(const TersoffP& T, float z, double va, double& b, double& bva,
                                           float& dbdz) {
   if (z > 1.0e-15f) {
-    const float x = exp2f((float)T.n * log2f((float)T.beta * z));
+    // x = (beta zeta)^n from the MUFU log2 / exp2: b's relative change per
+    // relative change of x is (1/2n) x/(1+x) (0.04 in silicon), so their
+    // ~2^-22 errors stay below 1e-8 in b; y needs log1p / expm1
+    const float x = ex2f((float)T.n * __log2f((float)T.beta * z));
     const float y = -expm1f((float)(-0.5 / T.n) * log1pf(x));
     const double cva = T.chi * va;
     b = T.chi - T.chi * (double)y;
@@ -1574,8 +1717,10 @@ __device__ __forceinline__ void ts_border(const TersoffP& T, float z, double va,
   }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(BLOCK) k_tsf_bonds(Arena A, BlockMap M) {
+// MINB > 1 asks for MINB blocks per SM (fewer registers, more warps to hide
+// the gathers; the autotuner tries it)
+template <typename R, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_tsf_bonds(Arena A, BlockMap M) {
   constexpr int NB = TS_APB * TS_MAXB;
   constexpr bool MIXED = sizeof(R) == 4;
   constexpr int PER = TS_MAXB / TS_TPA;  // bonds per thread
@@ -1603,43 +1748,61 @@ __global__ void __launch_bounds__(BLOCK) k_tsf_bonds(Arena A, BlockMap M) {
   int cnt = 0, err = 0;
   unsigned long long mask = 0ull;
   const int tmax = __reduce_max_sync(FULL, (nl + TS_TPA - 1) / TS_TPA);
-  for (int t = 0; t < tmax; t++) {
-    const int m = t * TS_TPA + q;
-    bool bond = false;
-    R u0 = R(0), u1 = R(0), u2 = R(0), rr = R(0);
-    if (m < nl) {
-      const int j = A.flist[(size_t)m * A.cap + i];
-      if ((unsigned)j < (unsigned)A.cap) {
+  constexpr int TB = MIXED ? 4 : 2;  // slot rounds whose loads are issued together
+  using P = typename std::conditional<MIXED, int4, double4>::type;
+  for (int t0 = 0; t0 < tmax; t0 += TB) {
+    int jj[TB];
+    P xj[TB];
+#pragma unroll
+    for (int u = 0; u < TB; u++) {
+      const int m = (t0 + u) * TS_TPA + q;
+      jj[u] = m < nl ? A.flist[(size_t)m * A.cap + i] : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < TB; u++) {
+      if ((unsigned)jj[u] < (unsigned)A.cap) {
+        if constexpr (MIXED) xj[u] = A.fxp[jj[u]];
+        else xj[u] = A.pos[jj[u]];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < TB; u++) {
+      if (t0 + u < tmax) {  // uniform across the warp
+      const int m = (t0 + u) * TS_TPA + q;
+      bool bond = false;
+      R u0 = R(0), u1 = R(0), u2 = R(0), rr = R(0);
+      if ((unsigned)jj[u] < (unsigned)A.cap) {
         if constexpr (MIXED) {
           float v0, v1, v2, ir;
-          vd_fx(S, qi, A.fxp[j], v0, v1, v2);
+          vd_fx(S, qi, xj[u], v0, v1, v2);
           rr = sqrt_nr(v0 * v0 + v1 * v1 + v2 * v2, ir);
           u0 = v0 * ir; u1 = v1 * ir; u2 = v2 * ir;
           bond = rr <= (float)r2;
         } else {
           double v0, v1, v2;
-          vd_fp64(S, xi, A.pos[j], v0, v1, v2);
+          vd_fp64(S, xi, xj[u], v0, v1, v2);
           rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
           u0 = v0 / rr; u1 = v1 / rr; u2 = v2 / rr;
           bond = !(rr > r2);
         }
       }
-    }
-    const unsigned grp = (__ballot_sync(FULL, bond) >> (lane & ~(TS_TPA - 1))) & ((1u << TS_TPA) - 1u);
-    if (bond) {
-      const int idx = cnt + __popc(grp & ((1u << q) - 1u));
-      if (idx < TS_MAXB && m < 64) {
-        const int k = base + idx;
-        sux[k] = u0; suy[k] = u1; suz[k] = u2; sr[k] = rr;
-        R dfc;
-        sfc[k] = ts_fc<R>(rr, R(r1), R(r2), dfc);
-        sdfc[k] = dfc;
-        mask |= 1ull << m;
-      } else {
-        err = 1;
+      const unsigned grp = (__ballot_sync(FULL, bond) >> (lane & ~(TS_TPA - 1))) & ((1u << TS_TPA) - 1u);
+      if (bond) {
+        const int idx = cnt + __popc(grp & ((1u << q) - 1u));
+        if (idx < TS_MAXB && m < 64) {
+          const int k = base + idx;
+          sux[k] = u0; suy[k] = u1; suz[k] = u2; sr[k] = rr;
+          R dfc;
+          sfc[k] = ts_fc<R>(rr, R(r1), R(r2), dfc);
+          sdfc[k] = dfc;
+          mask |= 1ull << m;
+        } else {
+          err = 1;
+        }
+      }
+      cnt += __popc(grp);
       }
     }
-    cnt += __popc(grp);
   }
   mask |= __shfl_xor_sync(FULL, mask, 1);
   mask |= __shfl_xor_sync(FULL, mask, 2);
@@ -1706,10 +1869,21 @@ __global__ void __launch_bounds__(BLOCK) k_tsf_bonds(Arena A, BlockMap M) {
     const double dv = dvs[t];
     const double4 fj = make_double4(-(dv * (double)ax + (double)tx), -(dv * (double)ay + (double)ty),
                                     -(dv * (double)az + (double)tz), 0.0);
-    A.tsfb[(size_t)a * A.cap + i] = fj;
-    f0 -= fj.x;
-    f1 -= fj.y;
-    f2 -= fj.z;
+    if constexpr (MIXED) {
+      // the record travels in FP32 (7 digits of one bond's force); the
+      // partner adds it to its FP64 sum, and the centre subtracts the
+      // same rounded value, so the forces still sum to zero
+      const float4 f4 = make_float4((float)fj.x, (float)fj.y, (float)fj.z, 0.0f);
+      A.tsfb32[(size_t)a * A.cap + i] = f4;
+      f0 -= (double)f4.x;
+      f1 -= (double)f4.y;
+      f2 -= (double)f4.z;
+    } else {
+      A.tsfb[(size_t)a * A.cap + i] = fj;
+      f0 -= fj.x;
+      f1 -= fj.y;
+      f2 -= fj.z;
+    }
   }
   // the atom's threads combine by a fixed xor tree (same bits in each)
 #pragma unroll
@@ -1728,6 +1902,7 @@ __global__ void __launch_bounds__(BLOCK) k_tsf_bonds(Arena A, BlockMap M) {
 }
 
 // F_l += the bond records of l's partners for their bonds to l (slot order)
+template <typename R>
 __global__ void __launch_bounds__(TS_APB) k_tsf_gather(Arena A, BlockMap M) {
   const int s = blk_sys(M);
   if (s < 0) return;
@@ -1752,10 +1927,17 @@ __global__ void __launch_bounds__(TS_APB) k_tsf_gather(Arena A, BlockMap M) {
       bad = true;
       continue;
     }
-    const double4 b = A.tsfb[(size_t)a * A.cap + j];
-    f.x += b.x;
-    f.y += b.y;
-    f.z += b.z;
+    if constexpr (sizeof(R) == 4) {
+      const float4 b = A.tsfb32[(size_t)a * A.cap + j];
+      f.x += (double)b.x;
+      f.y += (double)b.y;
+      f.z += (double)b.z;
+    } else {
+      const double4 b = A.tsfb[(size_t)a * A.cap + j];
+      f.x += b.x;
+      f.y += b.y;
+      f.z += b.z;
+    }
   }
   A.force[i] = f;
   if (bad) atomicOr(&A.st[s].status, ST_BONDS);
@@ -2644,46 +2826,81 @@ __global__ void __launch_bounds__(BLOCK) k_step_b(Arena A, BlockMap M) {
 }
 
 // ------------------------------------------------------------------ reductions
-// Per-system sums in a fixed order (one block per system): Epot, sum m v,
-// total mass, then Ekin with the centre-of-mass velocity removed
-// (inq_kin_energy, src/Inq_Properties.F90:399-422) and max |F|^2.
-__global__ void k_sys_reduce(Arena A, const int* sys, int nsys, double* out) {
-  int s = sys[blockIdx.x];
+// Per-system inquiry sums (inq_kin_energy / inq_temperature,
+// src/Inq_Properties.F90:399-437) over the system's blocks of an atom map;
+// each block's partials go to blk_red and the system's last block adds them
+// in block order, so the sums are the same bits on every run.
+//  PASS 0: Epot, the total mass and momentum (-> the centre-of-mass velocity),
+//          max |F|^2 and the status: out[4s+0], out[4s+2], out[4s+3], and
+//          v_cm in out[4 scap + 3s ..];
+//  PASS 1: Ekin = 1/2 sum m |v - v_cm|^2 (the reference's sum, which keeps
+//          its digits when the centre of mass drifts): out[4s+1].
+template <int PASS>
+__global__ void k_sys_reduce(Arena A, BlockMap M, int scap, double* out) {
+  const int s = blk_sys(M);
+  if (s < 0) return;
   const SysDev& S = A.sys[s];
-  double ep = 0, mx = 0, my = 0, mz = 0, mt = 0, f2 = 0;
-  for (int i = S.off + threadIdx.x; i < S.off + S.n; i += BLOCK) {
-    ep += A.epot[i];
-    double m = A.mass[i];
-    double4 v = A.vel[i];
-    mx += m * v.x; my += m * v.y; mz += m * v.z; mt += m;
-    double4 F = A.force[i];
-    f2 = fmax(f2, F.x * F.x + F.y * F.y + F.z * F.z);
-  }
-  ep = block_sum(ep);
-  __shared__ double cm[4];
-  double bx = block_sum(mx), by = block_sum(my), bz = block_sum(mz), bm = block_sum(mt);
-  double bf = block_max(f2);
-  if (threadIdx.x == 0) {
-    if (S.n == 1) {
-      double4 v = A.vel[S.off];
-      cm[0] = v.x; cm[1] = v.y; cm[2] = v.z;
+  const int i = M.first[blockIdx.x] + threadIdx.x;
+  const bool act = i < M.end[blockIdx.x];
+  constexpr int NW = PASS == 0 ? 6 : 1;
+  double w[NW];
+#pragma unroll
+  for (int k = 0; k < NW; k++) w[k] = 0.0;
+  if (act) {
+    const double4 v = A.vel[i];
+    const double m = A.mass[i];
+    if constexpr (PASS == 0) {
+      const double4 F = A.force[i];
+      w[0] = A.epot[i];
+      w[1] = m;
+      w[2] = m * v.x;
+      w[3] = m * v.y;
+      w[4] = m * v.z;
+      w[5] = F.x * F.x + F.y * F.y + F.z * F.z;
     } else {
-      cm[0] = bx / bm; cm[1] = by / bm; cm[2] = bz / bm;
+      const double* c = out + 4 * (size_t)scap + 3 * (size_t)s;
+      const double a = v.x - c[0], b = v.y - c[1], d = v.z - c[2];
+      w[0] = (a * a + b * b + d * d) * m;
     }
   }
-  __syncthreads();
-  double ek = 0.0;
-  for (int i = S.off + threadIdx.x; i < S.off + S.n; i += BLOCK) {
-    double4 v = A.vel[i];
-    double a = v.x - cm[0], b = v.y - cm[1], c = v.z - cm[2];
-    ek += (a * a + b * b + c * c) * A.mass[i];
-  }
-  ek = block_sum(ek);
-  if (threadIdx.x == 0) {
-    out[4 * blockIdx.x + 0] = ep;
-    out[4 * blockIdx.x + 1] = ek * 0.5;
-    out[4 * blockIdx.x + 2] = bf;
-    out[4 * blockIdx.x + 3] = (double)A.st[s].status;
+  double bsum[NW];
+#pragma unroll
+  for (int k = 0; k < NW; k++) bsum[k] = (PASS == 0 && k == 5) ? block_max(w[k]) : block_sum(w[k]);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NW; k++) A.blk_red[8 * (M.base + blockIdx.x) + k] = bsum[k];
+  if (last_block(M, A.st, s, &A.st[s].ticket2) && threadIdx.x < 32) {
+    const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+    double t[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) t[k] = 0.0;
+    for (int q = threadIdx.x; q < nb; q += 32)
+#pragma unroll
+      for (int k = 0; k < NW; k++) {
+        const double x = __ldcg(&A.blk_red[8 * (b0 + q) + k]);
+        t[k] = (PASS == 0 && k == 5) ? fmax(t[k], x) : t[k] + x;
+      }
+#pragma unroll
+    for (int k = 0; k < NW; k++)
+      for (int o = 16; o; o >>= 1) {
+        const double x = __shfl_xor_sync(0xffffffffu, t[k], o);
+        t[k] = (PASS == 0 && k == 5) ? fmax(t[k], x) : t[k] + x;
+      }
+    if (threadIdx.x == 0) {
+      if constexpr (PASS == 0) {
+        out[4 * (size_t)s + 0] = t[0];
+        out[4 * (size_t)s + 2] = t[5];
+        out[4 * (size_t)s + 3] = (double)A.st[s].status;
+        double* c = out + 4 * (size_t)scap + 3 * (size_t)s;
+        if (S.n == 1) {
+          const double4 v = A.vel[S.off];
+          c[0] = v.x; c[1] = v.y; c[2] = v.z;
+        } else {
+          c[0] = t[2] / t[1]; c[1] = t[3] / t[1]; c[2] = t[4] / t[1];
+        }
+      } else {
+        out[4 * (size_t)s + 1] = 0.5 * t[0];
+      }
+    }
   }
 }
 

@@ -129,9 +129,12 @@ int gemsgpu_set_skin(gemsgpu_ctx* ctx, int sys, double skin);
  * wrapped into the box by do_pbc triggers a rebuild; mic=1 (default) takes
  * the minimum image and skips those rebuilds (same forces, fewer rebuilds). */
 int gemsgpu_set_skin_mode(gemsgpu_ctx* ctx, int sys, int mic);
-/* 0 = full list, newton off (OpenMP default); 1 = half list
- * (src/Neighbour.F90:160-171).  Half lists are built for export/parity;
- * force kernels require full lists. */
+/* 0 = full list, newton off (OpenMP default); 1 = half list, newton on
+ * (the serial default, src/Neighbour.F90:160-171).  gemsgpu_get_list returns
+ * the list of the chosen mode in the reference's order.  The force kernels
+ * always sum over the full list: with the reaction added to j, a half list
+ * gives every atom the same force, density and energy (src/TB.F90:432-441,
+ * 542-552; src/Pairs.F90:248-252), up to summation order. */
 int gemsgpu_set_list_mode(gemsgpu_ctx* ctx, int sys, int half);
 int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec);
 
@@ -517,8 +520,11 @@ int gemsgpu_retemper(gemsgpu_ctx* ctx, int nsys, const int* sys,
  * the library holds until exit.  n > GEMSGPU_NOALLOC_MAX_ATOMS returns
  * GEMSGPU_ERR_FULL without launching.  The first call on a device looks up
  * the array's device address, so make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (two
- * streams, or two host threads) race; calls ordered on one stream do not. */
+ * capture.  That address is kept for the life of the process: after
+ * cudaDeviceReset (or anything else that destroys the device's primary
+ * context) do not call this function on that device again.  All calls share
+ * the array: calls that overlap on the GPU (two streams, or two host
+ * threads) race; calls ordered on one stream do not. */
 int gemsgpu_smatb_forces_noalloc(const double* d_pos, int n, int boxed,
                                  const double L[3], const int pbc[3],
                                  double A, double xi, double p, double q,
@@ -554,8 +560,9 @@ int gemsgpu_get_stream(gemsgpu_ctx* ctx, void** stream);
 int gemsgpu_get_launch_count(gemsgpu_ctx* ctx, int64_t* launches);
 /* Time the force kernels of `sys` on the context's stream with CUDA events:
  * reps back-to-back evaluations after one warm-up; out_ms[0] = mean time of
- * the first force kernel (density pass for SMA-TB), out_ms[1] = mean time of
- * the second (force pass; 0 if none), out_ms[2] = mean list rebuild time.
+ * the first force kernel (density pass for SMA-TB, bond records for
+ * Tersoff), out_ms[1] = mean time of the second (force pass; Tersoff's
+ * gather; 0 if none), out_ms[2] = mean list rebuild time.
  * Replaces timer_dump's per-step wall time (src/Errors.f90:128-172). */
 int gemsgpu_time_kernels(gemsgpu_ctx* ctx, int sys, int reps, double* out_ms);
 /* The same for nsys systems launched together (one launch shape). */

@@ -42,7 +42,8 @@ def test_reference_arm_two_ranks_prints_once():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--block", "1"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--block", "1",
+           "--therm-steps", "5"]
     env = dict(os.environ, OMP_NUM_THREADS="2")
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stderr[-2000:]

@@ -91,6 +91,29 @@ def test_list_cells_pbc_32k(ctx, half):
     compare_lists(o, g)
 
 
+@pytest.mark.parametrize("half", [False, True])
+def test_list_cells_small_cells(ctx, half):
+    """Cells of about three atoms (a thermal Tersoff diamond, 4.1 A cells)
+    go to the warp-per-cell list kernel: the lists equal the oracle's, entry
+    by entry, full and half."""
+    from gems_b200 import workloads as W
+    rng = np.random.default_rng(31)
+    L = 10 * 5.431
+    pos = np.mod(W.diamond(10, 5.431) + rng.normal(0, 0.1, (8000, 3)), L)
+
+    def setup(s):
+        s.set_box((L, L, L), (True, True, True))
+        s.set_tersoff(W.TERSOFF_SI)
+        s.set_half(half)
+
+    o, g = both(pos, W.MASS["Si"], ctx, setup=setup)
+    o.update()
+    g.update()
+    assert o.uses_cells() == (True, (13, 13, 13))
+    compare_lists(o, g)
+    g.destroy()
+
+
 def test_list_cells_batch_rebuild(ctx):
     """A batch of periodic cell-list systems rebuilt together (the force
     rebuild of a kernel timing call, then md steps that rebuild each system
@@ -232,6 +255,97 @@ def test_lj_fluid_forces(ctx, prec, rms, etol):
     o, g = both(pos, 1.0, ctx, setup=setup)
     g.set_precision(prec)
     check_forces(o, g, rms, etol)
+
+
+# ------------------------------------------------------------------ half lists
+@pytest.mark.parametrize("prec,rms,etol", [(0, RMS_FP64, E_FP64), (1, RMS_MIXED, E_MIXED)])
+def test_half_list_forces_32k(ctx, prec, rms, etol):
+    """A half-list system (Newton on, the serial build's default): its list is
+    the reference's half list, entry by entry, and its forces and per-atom
+    energies are the full-list oracle's (with the reaction added to j a half
+    list gives every atom the same force, density and energy)."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk()
+
+    def setup(s):
+        s.set_box(w["L"], (True, True, True))
+        s.set_smatb(*w["smatb"])
+    o, g = both(w["pos"], w["mass"], ctx, setup=setup)
+    g.set_half(True)
+    g.set_precision(prec)
+    check_forces(o, g, rms, etol)
+    oh = O.System(w["pos"], w["mass"])
+    setup(oh)
+    oh.set_half(True)
+    oh.update()
+    compare_lists(oh, g)
+    g.destroy()
+
+
+@pytest.mark.parametrize("kind", ["lj", "tersoff", "open_cluster"])
+def test_half_list_forces_other_fields(ctx, kind):
+    """Half lists under LJ (linked cells), Tersoff (which needs the full set
+    of bonds) and an open SMA-TB cluster (O(N^2) lists): FP64 forces against
+    the oracle, and the half list against the oracle's."""
+    from gems_b200 import workloads as W
+    if kind == "lj":
+        w = W.lj_fluid()
+        rng = np.random.default_rng(3)
+        pos, mass = np.mod(w["pos"] + rng.normal(0, 0.05, w["pos"].shape), w["L"][0]), 1.0
+
+        def setup(s):
+            s.set_box(w["L"], (True, True, True))
+            e, sg, rc, sh = w["lj"]
+            s.set_lj(e, sg, rc, eshift=sh)
+            s.set_skin(w["skin"])
+    elif kind == "tersoff":
+        rng = np.random.default_rng(4)
+        L = 6 * 5.431
+        pos = np.mod(W.diamond(6, 5.431) + rng.normal(0, 0.08, (1728, 3)), L)
+        mass = W.MASS["Si"]
+
+        def setup(s):
+            s.set_box((L, L, L), (True, True, True))
+            s.set_tersoff(W.TERSOFF_SI)
+    else:
+        pos, mass = W.cluster(300, np.random.default_rng(8)), W.MASS["Au"]
+
+        def setup(s):
+            s.set_smatb(*W.SMATB["Au"])
+    o, g = both(pos, mass, ctx, setup=setup)
+    g.set_half(True)
+    check_forces(o, g, RMS_FP64, E_FP64)
+    oh = O.System(pos, mass)
+    setup(oh)
+    oh.set_half(True)
+    oh.update()
+    compare_lists(oh, g)
+    g.destroy()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_half_list_md_equals_full_list_md(ctx, prec):
+    """The force kernels read the same full list in both list modes, so 200
+    Ermak steps of a half-list system equal those of a full-list one, bit for
+    bit."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=6)
+
+    def mk(half):
+        g = gems.System(w["pos"], w["mass"], ctx=ctx)
+        g.set_box(w["L"], (True, True, True))
+        g.set_smatb(*w["smatb"])
+        g.set_half(half)
+        g.set_precision(prec)
+        g.set_ermak(0.002, 1.0, 600.0, seed=3)
+        g.interact()
+        g.md_steps(200)
+        return g
+    a, b = mk(False), mk(True)
+    np.testing.assert_array_equal(b.pos, a.pos)
+    np.testing.assert_array_equal(b.vel, a.vel)
+    a.destroy()
+    b.destroy()
 
 
 def _tersoff_crystal(ctx, ncell, sigma, seed):
