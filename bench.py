@@ -758,8 +758,8 @@ def run_c4(args, gems, torch, ctx, ext):
 
 def run_next(args, gems, torch, ctx, ext):
     """The rows after the hot path, measured beside their CPU restatement:
-    the G-JF constant-pressure piston on the 32k-atom Au bulk (FP64; one
-    system and a batch of 8), batched L-BFGS of 256 147-atom Au clusters, and
+    the G-JF constant-pressure piston on the 32k-atom Au bulk (FP64 and
+    mixed; one system and a batch of 8), batched L-BFGS of 256 147-atom Au clusters, and
     the NEB deck (30 images of a 72-atom Au slab with a Pt adatom, 20
     iterations)."""
     import sys
@@ -771,19 +771,21 @@ def run_next(args, gems, torch, ctx, ext):
     O.set_threads(cores)
     press_atm, pg0, pgv, pmass = 1.0, 1.0, 1.0, 1e-3
 
-    def npt_system(seed):
+    def npt_system(seed, prec):
         w = c2_replica(seed)
         g = gems.System(w["pos"], w["mass"], ctx=ctx)
         g.set_box(w["L"], (True, True, True))
         g.set_smatb(*w["smatb"])
         g.set_skin(w["skin"])
+        g.set_precision(prec)
         g.set_lanes(2, 1)
         g.set_lgf(w["dt"], w["temp"], press_atm, pg0, pgv, pmass, seed=seed)
         g.interact()
         return g
     out = {}
-    for name, nrep in (("npt_fp64", 1), ("npt_fp64_batch8", 8)):
-        ss = [npt_system(10 + k) for k in range(nrep)]
+    for name, nrep, prec in (("npt_fp64", 1, gems.PREC_FP64), ("npt_fp64_batch8", 8, gems.PREC_FP64),
+                             ("npt_mixed", 1, gems.PREC_MIXED), ("npt_mixed_batch8", 8, gems.PREC_MIXED)):
+        ss = [npt_system(10 + k, prec) for k in range(nrep)]
         val, ms = _time_md(ctx, torch, ss, args.block, args.steps, args.warmup, ext)
         out[name] = {"value": val, "unit": UNIT, "ms_per_block": ms, "atoms": sum(x.n for x in ss),
                      "box_after": list(ss[0].box_now())}

@@ -237,6 +237,7 @@ struct Arena {
   // that centre i's energy puts on the partner of its a-th bond (tsfb32 in
   // mixed precision)
   unsigned char* rslot;
+  unsigned char* tidx;  // [m cap + l]: the index of the record l's m-th partner wrote for l
   unsigned long long* tsmask;
   double4* tsfb;        // FP64 systems
   float4* tsfb32;       // mixed systems

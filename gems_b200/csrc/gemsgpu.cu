@@ -316,15 +316,16 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
       if (*lists[q]) CU(cudaFree(*lists[q]));
       *lists[q] = nl;
     }
-    if (A.rslot) {
+    unsigned char** bytes[2] = {&A.rslot, &A.tidx};
+    for (auto pp : bytes) {
+      if (!*pp) continue;
       unsigned char* nr = nullptr;
       CHK(dalloc(ctx, &nr, (size_t)A.lcap * nc));
       CU(cudaMemsetAsync(nr, 0xff, (size_t)A.lcap * nc, ctx->stream));
-      if (keep)
-        CU(cudaMemcpy2DAsync(nr, nc, A.rslot, keep, keep, A.lcap, cudaMemcpyDeviceToDevice, ctx->stream));
+      if (keep) CU(cudaMemcpy2DAsync(nr, nc, *pp, keep, keep, A.lcap, cudaMemcpyDeviceToDevice, ctx->stream));
       CU(cudaStreamSynchronize(ctx->stream));
-      CU(cudaFree(A.rslot));
-      A.rslot = nr;
+      CU(cudaFree(*pp));
+      *pp = nr;
     }
   }
   ctx->acap = nc;
@@ -354,6 +355,8 @@ int tersoff_records(gemsgpu_ctx* ctx) {
   if (!A.rslot && A.lcap > 0) {
     CHK(dalloc(ctx, &A.rslot, (size_t)A.lcap * n));
     CU(cudaMemsetAsync(A.rslot, 0xff, (size_t)A.lcap * n, ctx->stream));
+    CHK(dalloc(ctx, &A.tidx, (size_t)A.lcap * n));
+    CU(cudaMemsetAsync(A.tidx, 0xff, (size_t)A.lcap * n, ctx->stream));
   }
   return 0;
 }
@@ -388,14 +391,17 @@ int grow_list(gemsgpu_ctx* ctx, int lcap) {
     *lists[q] = nl;
   }
   if (ctx->tersoff) {
-    unsigned char* nr = nullptr;
-    CHK(dalloc(ctx, &nr, (size_t)lcap * ld));
-    CU(cudaMemsetAsync(nr, 0xff, (size_t)lcap * ld, ctx->stream));
-    if (A.rslot && A.lcap > 0)
-      CU(cudaMemcpyAsync(nr, A.rslot, (size_t)A.lcap * ld, cudaMemcpyDeviceToDevice, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
-    if (A.rslot) CU(cudaFree(A.rslot));
-    A.rslot = nr;
+    unsigned char** bytes[2] = {&A.rslot, &A.tidx};
+    for (auto pp : bytes) {
+      unsigned char* nr = nullptr;
+      CHK(dalloc(ctx, &nr, (size_t)lcap * ld));
+      CU(cudaMemsetAsync(nr, 0xff, (size_t)lcap * ld, ctx->stream));
+      if (*pp && A.lcap > 0)
+        CU(cudaMemcpyAsync(nr, *pp, (size_t)A.lcap * ld, cudaMemcpyDeviceToDevice, ctx->stream));
+      CU(cudaStreamSynchronize(ctx->stream));
+      if (*pp) CU(cudaFree(*pp));
+      *pp = nr;
+    }
   }
   A.lcap = lcap;
   CHK(list_smem_attr(ctx, lcap));
@@ -773,24 +779,51 @@ void smatb_pass(gemsgpu_ctx* ctx, int pass, int prec, int variant, bool single, 
   }
 }
 
-// Tersoff forces: bond records per centre atom, then the per-atom gather
-// (both on the TS_APB-atom map).  variant bit 1: the bond kernel built for
-// four blocks per SM (autotuned).
+// Tersoff forces: bond records per centre atom, then the per-atom gather,
+// both on the system's map of BLOCK / lanes atoms per block (lanes = threads
+// per atom of the bond kernel: 4, or 2 in mixed precision).  variant bit 1:
+// the bond kernel built for four blocks per SM, with bit 2 for three
+// (autotuned).
+template <typename R, int TPA>
+void tersoff_bonds_t(gemsgpu_ctx* ctx, int variant, const BlockMap& m) {
+  const size_t sh = tsf_smem<R, TPA>();
+  if ((variant & 6) == 6) k_tsf_bonds<R, 3, TPA><<<m.nblk, BLOCK, sh, ctx->stream>>>(ctx->A, m);
+  else if (variant & 2) k_tsf_bonds<R, 4, TPA><<<m.nblk, BLOCK, sh, ctx->stream>>>(ctx->A, m);
+  else k_tsf_bonds<R, 1, TPA><<<m.nblk, BLOCK, sh, ctx->stream>>>(ctx->A, m);
+}
+
+// the bond kernels' dynamic shared memory may exceed the default 48 KB
+template <typename R, int TPA>
+int tersoff_smem_attr_t() {
+  const int sh = (int)tsf_smem<R, TPA>();
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tsf_bonds<R, 1, TPA>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tsf_bonds<R, 3, TPA>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tsf_bonds<R, 4, TPA>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh);
+  return e == cudaSuccess ? 0 : 1;
+}
+
+int tersoff_smem_attr(gemsgpu_ctx* ctx) {
+  if (tersoff_smem_attr_t<float, 2>() || tersoff_smem_attr_t<float, 4>() || tersoff_smem_attr_t<double, 4>())
+    return fail(ctx, GEMSGPU_ERR_CUDA, "Tersoff kernels: shared-memory size refused");
+  return 0;
+}
+
 void tersoff_bonds(gemsgpu_ctx* ctx, int prec, int variant, const BlockMap& m) {
-  const bool capped = (variant & 2) != 0;
-  if (prec == PREC_MIXED) {
-    if (capped) k_tsf_bonds<float, 4><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
-    else k_tsf_bonds<float, 1><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
-  } else {
-    if (capped) k_tsf_bonds<double, 4><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
-    else k_tsf_bonds<double, 1><<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m);
-  }
+  // two threads per atom: float only (the FP64 bond arrays of 128 atoms
+  // exceed the static shared memory)
+  if (prec == PREC_MIXED && m.apb == BLOCK / 2) tersoff_bonds_t<float, 2>(ctx, variant, m);
+  else if (prec == PREC_MIXED) tersoff_bonds_t<float, 4>(ctx, variant, m);
+  else tersoff_bonds_t<double, 4>(ctx, variant, m);
   ++ctx->launches;
 }
 
 void tersoff_gather(gemsgpu_ctx* ctx, int prec, const BlockMap& m) {
-  if (prec == PREC_MIXED) k_tsf_gather<float><<<m.nblk, TS_APB, 0, ctx->stream>>>(ctx->A, m);
-  else k_tsf_gather<double><<<m.nblk, TS_APB, 0, ctx->stream>>>(ctx->A, m);
+  if (prec == PREC_MIXED) k_tsf_gather<float><<<m.nblk, m.apb, 0, ctx->stream>>>(ctx->A, m);
+  else k_tsf_gather<double><<<m.nblk, m.apb, 0, ctx->stream>>>(ctx->A, m);
   ++ctx->launches;
 }
 
@@ -810,13 +843,19 @@ void lj_pass(gemsgpu_ctx* ctx, int prec, int K, bool vir, const BlockMap& m) {
   }
 }
 
+// threads per atom of a Tersoff system's bond kernel: its tuned lanes if
+// valid for its precision, else TS_TPA
+int tersoff_lanes(const SysHost& h) {
+  return (h.lanes == 2 && h.d.prec == PREC_MIXED) ? 2 : TS_TPA;
+}
+
 // group systems by (ff, prec, lanes) and launch the force kernels
 int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
   std::map<std::tuple<int, int, int, int, int>, std::vector<int>> groups;
   for (int s : ss) {
     const SysHost& h = ctx->sys[s];
     if (h.d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "system %d has no force field", s);
-    int K = h.d.ff == FF_TERSOFF ? TS_TPA : h.lanes;
+    int K = h.d.ff == FF_TERSOFF ? tersoff_lanes(h) : h.lanes;
     int key = h.variant * 2 + (h.ntypes == 1 ? 1 : 0);
     groups[{h.d.ff, h.d.prec, K, key, h.d.virial}].push_back(s);
   }
@@ -1926,7 +1965,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.acel2, A.acel3, A.acel4, A.epot, A.band, A.eband,
                   A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.hnn, A.ncut, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
-                  A.rslot, A.tsmask, A.tsfb, A.tsfb32,
+                  A.rslot, A.tidx, A.tsmask, A.tsfb, A.tsfb32,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys};
   for (void* p : ptrs)
@@ -2167,12 +2206,11 @@ int gemsgpu_set_precision(gemsgpu_ctx* ctx, int sys, int prec) {
   CHK(check_sys(ctx, sys));
   if (prec != GEMSGPU_PREC_FP64 && prec != GEMSGPU_PREC_MIXED)
     return fail(ctx, GEMSGPU_ERR_ARG, "unknown precision %d", prec);
-  if (prec != GEMSGPU_PREC_FP64 && moving_box(ctx->sys[sys].d))
-    return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: the pistons are FP64 only");
   if (prec != GEMSGPU_PREC_FP64 && ctx->sys[sys].d.ff == FF_LJ)
     for (const PairP& P : ctx->sys[sys].prm)
-      if (P.v[8] != 0.0) return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: slj and sm1 pairs are FP64 only");
+      if (P.v[8] == 2.0) return fail(ctx, GEMSGPU_ERR_STATE, "set_precision: sm1 pairs are FP64 only");
   ctx->sys[sys].d.prec = prec;
+  if (ctx->sys[sys].d.ff == FF_TERSOFF) ctx->sys[sys].lanes = TS_TPA;  // two lanes are mixed-only
   CHK(push_sys(ctx, sys));
   BlockMap m;
   CHK(get_map(ctx, {sys}, BLOCK, 0, &m));
@@ -2265,6 +2303,7 @@ int gemsgpu_set_tersoff(gemsgpu_ctx* ctx, int sys, const double prm[12]) {
   h.lanes = TS_TPA;
   if (!ctx->tersoff) {
     ctx->tersoff = true;
+    CHK(tersoff_smem_attr(ctx));
     CHK(tersoff_records(ctx));
   }
   h.ff_set = true;
@@ -2535,7 +2574,6 @@ int gemsgpu_set_slj(gemsgpu_ctx* ctx, int sys, int ti, int tj, double eps, doubl
     return fail(ctx, GEMSGPU_ERR_ARG, "set_slj: bad type pair, sigma or rs");
   if (h.d.ff != FF_NONE && h.d.ff != FF_LJ)
     return fail(ctx, GEMSGPU_ERR_STATE, "set_slj: system already has another force field");
-  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_slj: FP64 systems only");
   const double x = sigma / rs, x3 = x * x * x, s_dr = x3 * x3;
   const double urs = 4.0 * eps * (s_dr * s_dr - s_dr);
   const double dudrs = -eps * (48.0 * s_dr - 24.0) * s_dr / rs;
@@ -2652,7 +2690,6 @@ int gemsgpu_set_lgf(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: lj, plj, slj and SMA-TB systems only");
   if (one_sided(h))
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: one-sided (feels) pairs have no pair virial");
-  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lgf: FP64 systems only");
   SysDev& d = h.d;
   d.integ = IT_LGF;
   d.dt = dt;
@@ -2751,7 +2788,6 @@ int gemsgpu_set_lkd(gemsgpu_ctx* ctx, int sys, double dt, double temp, double pr
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: lj, plj, slj and SMA-TB systems only");
   if (one_sided(h))
     return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: one-sided (feels) pairs have no pair virial");
-  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "set_lkd: FP64 systems only");
   SysDev& d = h.d;
   d.integ = IT_LKD;
   d.dt = dt;
@@ -2828,7 +2864,6 @@ int gemsgpu_add_lgf_axis(gemsgpu_ctx* ctx, int sys, int axis, double dt, double 
     return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: lj, plj, slj and SMA-TB systems only");
   if (one_sided(h))
     return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: one-sided (feels) pairs have no pair virial");
-  if (h.d.prec != PREC_FP64) return fail(ctx, GEMSGPU_ERR_STATE, "add_lgf_axis: FP64 systems only");
   double p[8];
   p[0] = std::sqrt(2.0 * pgama0 * kB_ui * temp * dt);
   p[1] = 0.5 * dt * pgama0;
@@ -3179,8 +3214,12 @@ static int autotune_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, 
   if (!need.empty()) CHK(interact_group(ctx, need, true));
   std::vector<std::pair<int, int>> cand;
   if (h0.d.ff == FF_TERSOFF) {
-    cand.push_back({TS_TPA, 1});
-    cand.push_back({TS_TPA, 3});
+    for (int K : {TS_TPA, 2}) {
+      if (K == 2 && h0.d.prec != PREC_MIXED) continue;
+      cand.push_back({K, 1});
+      cand.push_back({K, 3});
+      cand.push_back({K, 7});
+    }
   } else {
     for (int K : {1, 2, 4, 8, 16, 32}) {
       cand.push_back({K, 1});
@@ -3220,7 +3259,7 @@ static int autotune_set(gemsgpu_ctx* ctx, const std::vector<int>& ss, int reps, 
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (int s : ss) {
-    ctx->sys[s].lanes = ctx->sys[s].d.ff == FF_TERSOFF ? TS_TPA : pick.first;
+    ctx->sys[s].lanes = pick.first;
     ctx->sys[s].variant = pick.second;
   }
   invalidate(ctx);
@@ -3250,7 +3289,9 @@ int gemsgpu_set_lanes(gemsgpu_ctx* ctx, int sys, int lanes, int variant) {
   if (variant < 0 || variant > 7 || variant == 4 || variant == 5)
     return fail(ctx, GEMSGPU_ERR_ARG, "variant must be 0..3, 6 or 7");
   SysHost& h = ctx->sys[sys];
-  if (h.d.ff != FF_TERSOFF) h.lanes = lanes;
+  if (h.d.ff == FF_TERSOFF && lanes != TS_TPA && !(lanes == 2 && h.d.prec == PREC_MIXED))
+    return fail(ctx, GEMSGPU_ERR_ARG, "Tersoff: lanes 4, or 2 in mixed precision");
+  h.lanes = lanes;
   h.variant = variant;
   invalidate(ctx);
   return 0;

@@ -503,6 +503,24 @@ __device__ __forceinline__ void warp_sort64(const float* rrow, int n, int ln, un
   }
 }
 
+// The same rank rule for n <= 32 entries, one key per lane: a bitonic
+// network over 32 positions (15 compare-exchange stages of one shuffle each,
+// against 21 stages of two for warp_sort64).  On return k0 holds the key at
+// position lane of the sorted order.
+__device__ __forceinline__ void warp_sort32(const float* rrow, int n, int ln, unsigned long long& k0) {
+  k0 = ln < n ? ((unsigned long long)__float_as_uint(rrow[ln]) << 32) | (unsigned)ln : ~0ull;
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const unsigned long long p0 = __shfl_xor_sync(0xffffffffu, k0, stride);
+      const bool lower = (ln & stride) == 0;
+      const bool up = (ln & size) == 0 || size == 32;
+      k0 = (lower == up) ? min(k0, p0) : max(k0, p0);
+    }
+  }
+}
+
 // flist holds an atom's entries sorted by their distance at the build, and
 // no pair has come closer since by more than the skin test's bound D
 // (SysState::dmax).  So the entries built at r >= rcut + 1e-4 + k skin/7
@@ -555,8 +573,12 @@ __device__ __forceinline__ void list_row_out(const Arena& A, const SysDev& S, in
     if (h) A.list[(size_t)(mh + __popc(hb & ((1u << ln) - 1u))) * A.cap + i] = row[e];
     mh += __popc(hb);
   }
-  if (n <= 64) {
+  if (n <= 32) {
     // force order by a warp bitonic sort of (distance, slot) keys
+    unsigned long long k0;
+    warp_sort32(rrow, n, ln, k0);
+    if (ln < n) A.flist[(size_t)ln * A.cap + i] = row[(int)(k0 & 0xffffffffu)] & 0x7fffffff;
+  } else if (n <= 64) {
     unsigned long long k0, k1;
     warp_sort64(rrow, n, ln, k0, k1);
     if (ln < n) A.flist[(size_t)ln * A.cap + i] = row[(int)(k0 & 0xffffffffu)] & 0x7fffffff;
@@ -1602,7 +1624,18 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
       float s6 = t2 * t2 * t2;
       float p = 4.0f * e * (s6 * s6 - s6);
       float fr = e * (48.0f * s6 - 24.0f) * s6 * ir2;  // f / r
-      if (P.v[7] != 0.0) {
+      if (P.v[8] != 0.0) {
+        // slj (Pairs.F90:403-470): plain LJ inside rs, the quartic-octic
+        // spline sa4 d^4 + sa8 d^8 (d = r - rc) from rs to rc
+        const float rs = (float)P.v[11];
+        if (r2 >= rs * rs) {
+          const float dr = sqrtf(r2), d = dr - (float)P.v[2];
+          const float s4 = d * d * d * d;
+          const float a4 = (float)P.v[9], a8 = (float)P.v[10];
+          p = a4 * s4 + a8 * s4 * s4;
+          fr = -(4.0f * a4 * s4 + 8.0f * a8 * s4 * s4) / (d * dr);
+        }
+      } else if (P.v[7] != 0.0) {
         float dr = sqrtf(r2);
         p = p - (float)P.v[4] - (float)P.v[5] * (dr - (float)P.v[2]);
         fr = fr + (float)P.v[5] / dr;
@@ -1649,15 +1682,16 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
 //
 // Gather formulation: no atomics, so the forces are the same bits on every
 // run and in every batch.
-//  * k_tsf_bonds, per centre atom i (TS_TPA threads): i's bonds (r <= R+D)
+//  * k_tsf_bonds, per centre atom i (2 or 4 threads): i's bonds (r <= R+D)
 //    in flist order; per bond a = (i, j): zeta, b and the force that E_i puts
 //    on j, F_j(i) = -dE_i/dx_j, stored in the bond record tsfb[a cap + i].
 //    E_i is translation invariant, so the force it puts on i itself is
 //    -sum_a F_j(a).  tsmask[i] marks the flist slots that are bonds.
 //  * k_tsf_gather, per atom l: F_l = F_l(l) + the records its bond partners
 //    wrote for their bonds to l, in l's slot order.  rslot (built with the
-//    list) is l's slot in the partner's flist; the popcount of the partner's
-//    mask below that slot is the record's index.
+//    list) is l's slot in the partner's flist: centre j writes the index of
+//    its record for l to tidx at that slot of l, so l reads it from its own
+//    row.
 // Bond decisions are symmetric (the pair vector seen from j is the exact
 // negative of the one seen from i), so every record a gather looks for exists.
 //
@@ -1668,7 +1702,6 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
 // and expm1, so the FP32 rounding of y costs y's relative error (y ~ 0.04 in
 // silicon), not b's.  A bond's triplet force terms are summed in FP32, the
 // bond records and the per-atom sums in FP64.
-constexpr int TS_APB = BLOCK / TS_TPA;  // atoms per block of the Tersoff kernels
 
 template <typename R>
 __device__ __forceinline__ R ts_fc(R r, R r1, R r2, R& dfc) {
@@ -1718,27 +1751,45 @@ __device__ __forceinline__ void ts_border(const TersoffP& T, float z, double va,
 }
 
 // MINB > 1 asks for MINB blocks per SM (fewer registers, more warps to hide
-// the gathers; the autotuner tries it)
-template <typename R, int MINB>
+// the gathers).  TPA threads per atom (4 or 2; BLOCK / TPA atoms per block):
+// each thread carries the atom's bonds q, q + TPA, ... two at a time, so with
+// TPA = 2 a crystal's four bonds give every thread two independent chains.
+// The autotuner picks MINB and TPA.
+template <typename R, int TPA>
+__host__ __device__ constexpr size_t tsf_smem() {
+  return (size_t)8 * (BLOCK / TPA) * TS_MAXB * sizeof(R);  // eight per-bond arrays
+}
+
+template <typename R, int MINB, int TPA>
 __global__ void __launch_bounds__(BLOCK, MINB) k_tsf_bonds(Arena A, BlockMap M) {
-  constexpr int NB = TS_APB * TS_MAXB;
+  constexpr int APB = BLOCK / TPA;
+  constexpr int NB = APB * TS_MAXB;
   constexpr bool MIXED = sizeof(R) == 4;
-  constexpr int PER = TS_MAXB / TS_TPA;  // bonds per thread
-  __shared__ R sux[NB], suy[NB], suz[NB], sr[NB], sfc[NB], sdfc[NB], spre[NB];
+  constexpr int PER = TS_MAXB / TPA;  // bonds per thread at most
+  constexpr int CH = TPA == 2 ? 2 : 1;  // bonds a thread carries at once
+  extern __shared__ __align__(16) unsigned char tsf_sh[];
+  R* sux = reinterpret_cast<R*>(tsf_sh);
+  R* suy = sux + NB;
+  R* suz = suy + NB;
+  R* sr = suz + NB;
+  R* sfc = sr + NB;
+  R* sdfc = sfc + NB;
+  R* spre = sdfc + NB;
+  R* sdv = spre + NB;  // the radial pair derivative dV of each bond (its owner's)
   const int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   const TersoffP& T = S.ts;
   const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, q = threadIdx.x & (TS_TPA - 1), la = threadIdx.x / TS_TPA;
+  const int lane = threadIdx.x & 31, q = threadIdx.x & (TPA - 1), la = threadIdx.x / TPA;
   const int i = M.first[blockIdx.x] + la;
   const bool act = i < M.end[blockIdx.x];
   const int base = la * TS_MAXB;
   const double r1 = T.R - T.D, r2 = T.R + T.D;
   const int nl = act ? live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap)) : 0;
 
-  // ---- bonds in flist order: the atom's TS_TPA threads test TS_TPA slots
-  // at a time and a ballot ranks the bonds they found
+  // ---- bonds in flist order: the atom's TPA threads test TPA slots at a
+  // time and a ballot ranks the bonds they found
   double4 xi = make_double4(0, 0, 0, 0);
   int4 qi = make_int4(0, 0, 0, 0);
   if (act) {
@@ -1747,16 +1798,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_tsf_bonds(Arena A, BlockMap M) 
   }
   int cnt = 0, err = 0;
   unsigned long long mask = 0ull;
-  const int tmax = __reduce_max_sync(FULL, (nl + TS_TPA - 1) / TS_TPA);
+  const int tmax = __reduce_max_sync(FULL, (nl + TPA - 1) / TPA);
   constexpr int TB = MIXED ? 4 : 2;  // slot rounds whose loads are issued together
   using P = typename std::conditional<MIXED, int4, double4>::type;
   for (int t0 = 0; t0 < tmax; t0 += TB) {
-    int jj[TB];
+    int jj[TB], rs[TB];
     P xj[TB];
 #pragma unroll
     for (int u = 0; u < TB; u++) {
-      const int m = (t0 + u) * TS_TPA + q;
+      const int m = (t0 + u) * TPA + q;
       jj[u] = m < nl ? A.flist[(size_t)m * A.cap + i] : -1;
+      rs[u] = m < nl ? A.rslot[(size_t)m * A.cap + i] : 255;
     }
 #pragma unroll
     for (int u = 0; u < TB; u++) {
@@ -1768,75 +1820,92 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_tsf_bonds(Arena A, BlockMap M) 
 #pragma unroll
     for (int u = 0; u < TB; u++) {
       if (t0 + u < tmax) {  // uniform across the warp
-      const int m = (t0 + u) * TS_TPA + q;
-      bool bond = false;
-      R u0 = R(0), u1 = R(0), u2 = R(0), rr = R(0);
-      if ((unsigned)jj[u] < (unsigned)A.cap) {
-        if constexpr (MIXED) {
-          float v0, v1, v2, ir;
-          vd_fx(S, qi, xj[u], v0, v1, v2);
-          rr = sqrt_nr(v0 * v0 + v1 * v1 + v2 * v2, ir);
-          u0 = v0 * ir; u1 = v1 * ir; u2 = v2 * ir;
-          bond = rr <= (float)r2;
-        } else {
-          double v0, v1, v2;
-          vd_fp64(S, xi, xj[u], v0, v1, v2);
-          rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-          u0 = v0 / rr; u1 = v1 / rr; u2 = v2 / rr;
-          bond = !(rr > r2);
+        const int m = (t0 + u) * TPA + q;
+        bool bond = false;
+        R u0 = R(0), u1 = R(0), u2 = R(0), rr = R(0);
+        if ((unsigned)jj[u] < (unsigned)A.cap) {
+          if constexpr (MIXED) {
+            float v0, v1, v2, ir;
+            vd_fx(S, qi, xj[u], v0, v1, v2);
+            rr = sqrt_nr(v0 * v0 + v1 * v1 + v2 * v2, ir);
+            u0 = v0 * ir; u1 = v1 * ir; u2 = v2 * ir;
+            bond = rr <= (float)r2;
+          } else {
+            double v0, v1, v2;
+            vd_fp64(S, xi, xj[u], v0, v1, v2);
+            rr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+            u0 = v0 / rr; u1 = v1 / rr; u2 = v2 / rr;
+            bond = !(rr > r2);
+          }
         }
-      }
-      const unsigned grp = (__ballot_sync(FULL, bond) >> (lane & ~(TS_TPA - 1))) & ((1u << TS_TPA) - 1u);
-      if (bond) {
-        const int idx = cnt + __popc(grp & ((1u << q) - 1u));
-        if (idx < TS_MAXB && m < 64) {
-          const int k = base + idx;
-          sux[k] = u0; suy[k] = u1; suz[k] = u2; sr[k] = rr;
-          R dfc;
-          sfc[k] = ts_fc<R>(rr, R(r1), R(r2), dfc);
-          sdfc[k] = dfc;
-          mask |= 1ull << m;
-        } else {
-          err = 1;
+        const unsigned grp = (__ballot_sync(FULL, bond) >> (lane & ~(TPA - 1))) & ((1u << TPA) - 1u);
+        if (bond) {
+          const int idx = cnt + __popc(grp & ((1u << q) - 1u));
+          if (idx < TS_MAXB && m < 64 && rs[u] < 64) {
+            const int k = base + idx;
+            sux[k] = u0; suy[k] = u1; suz[k] = u2; sr[k] = rr;
+            R dfc;
+            sfc[k] = ts_fc<R>(rr, R(r1), R(r2), dfc);
+            sdfc[k] = dfc;
+            mask |= 1ull << m;
+            A.tidx[(size_t)rs[u] * A.cap + jj[u]] = (unsigned char)idx;  // where j finds this record
+          } else {
+            err = 1;
+          }
         }
-      }
-      cnt += __popc(grp);
+        cnt += __popc(grp);
       }
     }
   }
-  mask |= __shfl_xor_sync(FULL, mask, 1);
-  mask |= __shfl_xor_sync(FULL, mask, 2);
+#pragma unroll
+  for (int o = 1; o < TPA; o <<= 1) mask |= __shfl_xor_sync(FULL, mask, o);
   const int nb = min(cnt, TS_MAXB);
   __syncthreads();
 
-  // ---- per bond: zeta, bond order, the pair part (FP64) and dE_i/dzeta
+  // ---- per bond: zeta, bond order, the pair part (FP64) and dE_i/dzeta.
+  // Two of the thread's bonds at a time, each partner bond b read once for both.
   const R h = R(T.h), c2 = R(T.c * T.c), d2 = R(T.d * T.d), c2d2 = R(T.c * T.c / (T.d * T.d));
   const double Aa = T.A * EV_UI, Bb = T.B * EV_UI;
   double ei = 0.0;
-  double dvs[PER];
 #pragma unroll
-  for (int t = 0; t < PER; t++) {
-    const int a = q + t * TS_TPA;
-    dvs[t] = 0.0;
-    if (a >= nb) continue;
-    const R ax = sux[base + a], ay = suy[base + a], az = suz[base + a];
-    R z = R(0);
-    for (int b = 0; b < nb; b++) {
-      if (b == a) continue;
-      const R ct = ax * sux[base + b] + ay * suy[base + b] + az * suz[base + b];
-      const R hc = h - ct, hc2 = hc * hc;
-      z += sfc[base + b] * (R(1) + c2d2 * hc2 / (d2 + hc2));  // 1 + c2/d2 - c2/(d2+hc2), no cancellation
+  for (int c = 0; c < PER; c += CH) {
+    const int a0 = q + c * TPA, a1 = q + (c + 1) * TPA;
+    const bool h0 = a0 < nb, h1 = CH == 2 && c + 1 < PER && a1 < nb;
+    if (!h0) continue;
+    const int k1 = h1 ? a1 : a0;
+    R ax[CH], ay[CH], az[CH], z[CH];
+#pragma unroll
+    for (int e = 0; e < CH; e++) {
+      const int a = e ? k1 : a0;
+      ax[e] = sux[base + a]; ay[e] = suy[base + a]; az[e] = suz[base + a];
+      z[e] = R(0);
     }
-    const double rd = (double)sr[base + a];
-    double dfc;
-    const double fc = ts_fc<double>(rd, r1, r2, dfc);
-    const double vr = Aa * exp(-T.l1 * rd), va = -Bb * exp(-T.l2 * rd);
-    double b, bva;
-    R dbdz;
-    ts_border(T, z, va, b, bva, dbdz);
-    ei += 0.5 * fc * (vr + bva);
-    dvs[t] = 0.5 * (dfc * (vr + bva) + fc * (-T.l1 * vr - T.l2 * bva));
-    spre[base + a] = R(0.5 * fc * va) * dbdz;  // dE_i / dzeta_a
+    for (int b = 0; b < nb; b++) {
+      const R bx = sux[base + b], by = suy[base + b], bz = suz[base + b], fcb = sfc[base + b];
+#pragma unroll
+      for (int e = 0; e < CH; e++) {
+        if (b == (e ? a1 : a0) || (e == 1 && !h1)) continue;
+        const R ct = ax[e] * bx + ay[e] * by + az[e] * bz;
+        const R hc = h - ct, hq = hc * hc;
+        z[e] += fcb * (R(1) + c2d2 * hq / (d2 + hq));  // 1 + c2/d2 - c2/(d2+hc2), no cancellation
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < CH; e++) {
+      if (e == 1 && !h1) break;
+      const int a = e ? a1 : a0;
+      const double rd = (double)sr[base + a];
+      double dfc;
+      const double fc = ts_fc<double>(rd, r1, r2, dfc);
+      const double vr = Aa * exp(-T.l1 * rd), va = -Bb * exp(-T.l2 * rd);
+      double bo, bva;
+      R dbdz;
+      ts_border(T, z[e], va, bo, bva, dbdz);
+      ei += 0.5 * fc * (vr + bva);
+      // in mixed precision dV travels in FP32 like the record it ends in
+      sdv[base + a] = R(0.5 * (dfc * (vr + bva) + fc * (-T.l1 * vr - T.l2 * bva)));
+      spre[base + a] = R(0.5 * fc * va) * dbdz;  // dE_i / dzeta_a
+    }
   }
   __syncthreads();
 
@@ -1845,49 +1914,64 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_tsf_bonds(Arena A, BlockMap M) 
   //      zeta_a through k = j_b and zeta_b through k = j_a with the same angle
   double f0 = 0.0, f1 = 0.0, f2 = 0.0;
 #pragma unroll
-  for (int t = 0; t < PER; t++) {
-    const int a = q + t * TS_TPA;
-    if (a >= nb) continue;
-    const R ax = sux[base + a], ay = suy[base + a], az = suz[base + a];
-    const R fca = sfc[base + a], dfca = sdfc[base + a], pa = spre[base + a];
-    const R ira = R(1) / sr[base + a];
-    R tx = R(0), ty = R(0), tz = R(0);
-    for (int b = 0; b < nb; b++) {
-      if (b == a) continue;
-      const R bx = sux[base + b], by = suy[base + b], bz = suz[base + b];
-      const R ct = ax * bx + ay * by + az * bz;
-      const R hc = h - ct, iden = R(1) / (d2 + hc * hc);
-      const R g = R(1) + c2d2 * (hc * hc) * iden;
-      const R dg = R(-2) * c2 * hc * iden * iden;  // dg / dcos
-      const R pb = spre[base + b];
-      const R coef = (pa * sfc[base + b] + pb * fca) * dg * ira;
-      const R kc = pb * dfca * g;
-      tx += coef * (bx - ct * ax) + kc * ax;
-      ty += coef * (by - ct * ay) + kc * ay;
-      tz += coef * (bz - ct * az) + kc * az;
+  for (int c = 0; c < PER; c += CH) {
+    const int a0 = q + c * TPA, a1 = q + (c + 1) * TPA;
+    const bool h0 = a0 < nb, h1 = CH == 2 && c + 1 < PER && a1 < nb;
+    if (!h0) continue;
+    const int k1 = h1 ? a1 : a0;
+    R ax[CH], ay[CH], az[CH], fca[CH], dfca[CH], pa[CH], ira[CH], tx[CH], ty[CH], tz[CH];
+#pragma unroll
+    for (int e = 0; e < CH; e++) {
+      const int a = e ? k1 : a0;
+      ax[e] = sux[base + a]; ay[e] = suy[base + a]; az[e] = suz[base + a];
+      fca[e] = sfc[base + a]; dfca[e] = sdfc[base + a]; pa[e] = spre[base + a];
+      ira[e] = R(1) / sr[base + a];
+      tx[e] = ty[e] = tz[e] = R(0);
     }
-    const double dv = dvs[t];
-    const double4 fj = make_double4(-(dv * (double)ax + (double)tx), -(dv * (double)ay + (double)ty),
-                                    -(dv * (double)az + (double)tz), 0.0);
-    if constexpr (MIXED) {
-      // the record travels in FP32 (7 digits of one bond's force); the
-      // partner adds it to its FP64 sum, and the centre subtracts the
-      // same rounded value, so the forces still sum to zero
-      const float4 f4 = make_float4((float)fj.x, (float)fj.y, (float)fj.z, 0.0f);
-      A.tsfb32[(size_t)a * A.cap + i] = f4;
-      f0 -= (double)f4.x;
-      f1 -= (double)f4.y;
-      f2 -= (double)f4.z;
-    } else {
-      A.tsfb[(size_t)a * A.cap + i] = fj;
-      f0 -= fj.x;
-      f1 -= fj.y;
-      f2 -= fj.z;
+    for (int b = 0; b < nb; b++) {
+      const R bx = sux[base + b], by = suy[base + b], bz = suz[base + b];
+      const R fcb = sfc[base + b], pb = spre[base + b];
+#pragma unroll
+      for (int e = 0; e < CH; e++) {
+        if (b == (e ? a1 : a0) || (e == 1 && !h1)) continue;
+        const R ct = ax[e] * bx + ay[e] * by + az[e] * bz;
+        const R hc = h - ct, iden = R(1) / (d2 + hc * hc);
+        const R g = R(1) + c2d2 * (hc * hc) * iden;
+        const R dg = R(-2) * c2 * hc * iden * iden;  // dg / dcos
+        const R coef = (pa[e] * fcb + pb * fca[e]) * dg * ira[e];
+        const R kc = pb * dfca[e] * g;
+        tx[e] += coef * (bx - ct * ax[e]) + kc * ax[e];
+        ty[e] += coef * (by - ct * ay[e]) + kc * ay[e];
+        tz[e] += coef * (bz - ct * az[e]) + kc * az[e];
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < CH; e++) {
+      if (e == 1 && !h1) break;
+      const int a = e ? a1 : a0;
+      const double dv = (double)sdv[base + a];
+      const double4 fj = make_double4(-(dv * (double)ax[e] + (double)tx[e]), -(dv * (double)ay[e] + (double)ty[e]),
+                                      -(dv * (double)az[e] + (double)tz[e]), 0.0);
+      if constexpr (MIXED) {
+        // the record travels in FP32 (7 digits of one bond's force); the
+        // partner adds it to its FP64 sum, and the centre subtracts the
+        // same rounded value, so the forces still sum to zero
+        const float4 f4 = make_float4((float)fj.x, (float)fj.y, (float)fj.z, 0.0f);
+        A.tsfb32[(size_t)a * A.cap + i] = f4;
+        f0 -= (double)f4.x;
+        f1 -= (double)f4.y;
+        f2 -= (double)f4.z;
+      } else {
+        A.tsfb[(size_t)a * A.cap + i] = fj;
+        f0 -= fj.x;
+        f1 -= fj.y;
+        f2 -= fj.z;
+      }
     }
   }
   // the atom's threads combine by a fixed xor tree (same bits in each)
 #pragma unroll
-  for (int o = 1; o < TS_TPA; o <<= 1) {
+  for (int o = 1; o < TPA; o <<= 1) {
     f0 += __shfl_xor_sync(FULL, f0, o);
     f1 += __shfl_xor_sync(FULL, f1, o);
     f2 += __shfl_xor_sync(FULL, f2, o);
@@ -1903,7 +1987,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_tsf_bonds(Arena A, BlockMap M) 
 
 // F_l += the bond records of l's partners for their bonds to l (slot order)
 template <typename R>
-__global__ void __launch_bounds__(TS_APB) k_tsf_gather(Arena A, BlockMap M) {
+__global__ void __launch_bounds__(BLOCK / 2) k_tsf_gather(Arena A, BlockMap M) {
   const int s = blk_sys(M);
   if (s < 0) return;
   const int i = M.first[blockIdx.x] + threadIdx.x;
@@ -1916,14 +2000,8 @@ __global__ void __launch_bounds__(TS_APB) k_tsf_gather(Arena A, BlockMap M) {
     mk &= mk - 1ull;
     const size_t e = (size_t)m * A.cap + i;
     const int j = A.flist[e];
-    const int r = A.rslot[e];
-    if ((unsigned)j >= (unsigned)A.cap || r >= 64) {
-      bad = true;
-      continue;
-    }
-    const unsigned long long mj = A.tsmask[j];
-    const int a = __popcll(mj & ((1ull << r) - 1ull));
-    if (!((mj >> r) & 1ull) || a >= TS_MAXB) {
+    const int a = A.tidx[e];
+    if ((unsigned)j >= (unsigned)A.cap || a >= TS_MAXB) {
       bad = true;
       continue;
     }
@@ -2237,7 +2315,22 @@ __device__ __forceinline__ void axes_a_atom(const Arena& A, const SysDev& S, con
 // cells no smaller than the list cut-off) within the cells allocated, with
 // fewer, larger cells where the allocation is short; below three cells a
 // dimension's stencil would visit a cell twice
+// the fixed-point frame of the mixed kernels follows the box: periodic
+// dimensions map [0, L) onto the 32-bit ring for the current L (the same
+// arithmetic as the host's set-up), and the step kernel that moves every atom
+// into the new box rewrites the fixed-point copies in it
+__device__ __forceinline__ void fx_frame(SysDev& S) {
+  for (int d = 0; d < 3; d++)
+    if (S.fx_per[d]) {
+      S.fx_scale[d] = 4294967296.0 / S.L[d];
+      const double u = S.L[d] / 4294967296.0;
+      S.fx_inv[d] = (float)u;
+      S.fx_inv_lo[d] = (float)(u - (double)S.fx_inv[d]);
+    }
+}
+
 __device__ __forceinline__ void regrid(SysDev& S, SysState& st) {
+  fx_frame(S);
   if (!S.use_cells) return;
   int nc[3];
   for (int d = 0; d < 3; d++) nc[d] = (int)(S.L[d] / S.rlist);

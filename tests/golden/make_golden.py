@@ -1,7 +1,7 @@
 """Extract the reference's golden vectors into tests/golden/golden.json.
 
-Run once in a checkout that has the reference tree (default path below or
-$GEMS_REF); the resulting JSON is committed so the tests never read the
+Run once where the reference tree exists, giving its path as the argument
+or in $GEMS_REF; the resulting JSON is committed so the tests never read the
 reference at run time.  It collects the regression outputs that pin the
 force/neighbour path (examples/*/ref/Energy.*.dat, the test rule of
 examples/test.sh) and the input coordinates those decks read.
@@ -12,7 +12,9 @@ import json
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GEMS_REF", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GEMS_REF")
+if not REF:
+    sys.exit("usage: make_golden.py /path/to/GEMS   (or set GEMS_REF)")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
 
 

@@ -59,6 +59,26 @@ def test_slj_forces_and_virial_equal_oracle(ctx):
     g.destroy()
 
 
+def test_slj_mixed_forces_and_virial(ctx):
+    """slj in mixed precision (FP32 pair math with the quartic-octic tail,
+    FP64 accumulation): forces to 1e-5 relative RMS, energy to 1e-6 eV per
+    atom and the virial to 1e-5 of its largest component against the oracle."""
+    d = decks.npt_lgf_deck()
+    rng = np.random.default_rng(6)
+    pos = d["pos"] + rng.normal(0.0, 0.05, d["pos"].shape)
+    s, _ = _oracle(d, pos)
+    s.interact()
+    g = _gpu(ctx, d, pos)
+    g.set_precision(1)
+    g.interact()
+    f_ref = s.force
+    assert np.linalg.norm(g.force - f_ref) / np.linalg.norm(f_ref) <= 1e-5
+    assert abs(g.epot_sum() - s.epot_sum()) * O.UI_EV / len(pos) <= 1e-6
+    ref = s.virial_ev()
+    np.testing.assert_allclose(g.virial_ev(), ref, rtol=0, atol=1e-5 * np.abs(ref).max())
+    g.destroy()
+
+
 def test_lgf_trajectory_equals_oracle(ctx):
     """100 piston steps with the oracle's normals fed to the device: energy,
     pressure, virial and box at every 10th step."""
@@ -88,13 +108,17 @@ def test_lgf_deck_golden(ctx):
     g.destroy()
 
 
-def test_lgf_md_steps_equals_stepwise(ctx):
+@pytest.mark.parametrize("prec", [0, 1])
+def test_lgf_md_steps_equals_stepwise(ctx, prec):
     """The captured md_steps loop (piston kernel, half steps, conditional
     rebuilds) gives the trajectory of separate step calls bit for bit, with
-    the device's own noise."""
+    the device's own noise, in FP64 and in mixed precision (where the
+    fixed-point frame follows the moving box)."""
     d = decks.npt_lgf_deck()
     a = _gpu(ctx, d, seed=7)
     b = _gpu(ctx, d, seed=7)
+    a.set_precision(prec)
+    b.set_precision(prec)
     a.interact()
     b.interact()
     a.md_steps(120)
@@ -413,4 +437,62 @@ def test_mixed_precision_virial(ctx, ff):
     np.testing.assert_allclose(g.virial_ev(), ref, rtol=0, atol=1e-5 * np.abs(ref).max())
     p = g.pressure_atm()
     assert np.all(np.isfinite(p))
+    g.destroy()
+
+
+# Mixed precision under the pistons: the fixed-point frame of the mixed kernels
+# follows the box the device moves, so the constant-pressure integrators run
+# the FP32-math / FP64-accumulation kernels.  Measured against the oracle's
+# FP64 rows over these runs: energies within 3.1e-7 eV/atom, pressure and
+# virial within 5e-6 of their largest component, box lengths within 1.5e-7 A.
+E_MIXED = 1e-6        # eV per atom (the mixed kernels' energy bar)
+P_MIXED = 2e-5        # of the largest pressure / virial component
+BOX_MIXED = 1e-6      # relative box length
+
+
+def _mixed_rows_close(n, E1, P1, V1, E0, P0, V0):
+    assert np.abs(E1[:, :3] - E0[:, :3]).max() * O.UI_EV / n <= E_MIXED
+    assert np.abs(P1 - P0).max() <= P_MIXED * np.abs(P0).max()
+    assert np.abs(V1 - V0).max() <= P_MIXED * np.abs(V0).max()
+
+
+def test_lgf_deck_mixed_precision(ctx):
+    """lgf.gms (864 slj atoms, isotropic G-JF piston, 100 steps) in mixed
+    precision, the oracle's normals fed in, against the oracle's FP64 rows."""
+    d = decks.npt_lgf_deck()
+    s, rng_o = _oracle(d)
+    E0, P0, V0 = decks.npt_run(s, d, rng_o)
+    g = _gpu(ctx, d)
+    g.set_precision(1)
+    E1, P1, V1 = decks.npt_run(g, d, O.Rng(d["seed"]), feed=_feed)
+    _mixed_rows_close(len(d["pos"]), E1, P1, V1, E0, P0, V0)
+    np.testing.assert_allclose(g.box_now(), s.box_now(), rtol=BOX_MIXED)
+    g.destroy()
+
+
+def test_smatb_piston_mixed_precision(ctx):
+    """An Au crystal (864 atoms) under the isotropic G-JF piston at 1 atm,
+    100 steps in mixed precision, against the oracle's FP64 rows and boxes."""
+    from gems_b200 import workloads as W
+    w = W.smatb_bulk(ncell=6)
+    rng = np.random.default_rng(9)
+    pos = np.mod(w["pos"] + rng.normal(0, 0.05, w["pos"].shape), w["L"])
+    s = O.System(pos, w["mass"])
+    s.set_box(w["L"], (True, True, True))
+    s.set_smatb(*w["smatb"])
+    g = gems.System(pos, w["mass"], ctx=ctx)
+    g.set_skin_mode(False)
+    g.set_box(w["L"], (True, True, True))
+    g.set_smatb(*w["smatb"])
+    g.set_virial(True)
+    g.set_precision(1)
+    d = dict(dt=w["dt"], nsteps=100, each=10)
+    s.set_lgf(w["dt"], 300.0, 1.0, 1.0, 1.0, 1e-3, O.Rng(7))
+    g.set_lgf(w["dt"], 300.0, 1.0, 1.0, 1.0, 1e-3)
+    B0, B1 = [], []
+    E0, P0, V0 = decks.npt_run(s, d, s._rng, boxes=B0)
+    E1, P1, V1 = decks.npt_run(g, d, O.Rng(7), feed=_feed, boxes=B1)
+    _mixed_rows_close(len(pos), E1, P1, V1, E0, P0, V0)
+    np.testing.assert_allclose(np.array(B1), np.array(B0), rtol=BOX_MIXED)
+    assert abs(B1[-1][0] - w["L"][0]) > 1e-4      # the box did move
     g.destroy()

@@ -1072,6 +1072,49 @@ def test_stale_list_pairs_entering_the_cutoff(ctx, prec):
     g.destroy()
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_tersoff_stale_list_bonds_entering_the_cutoff(ctx, prec):
+    """The Tersoff bond scan stops at the entries that can have come within
+    R+D (the skin test's bound on how far pairs moved).  A diamond with its
+    second shell squeezed to just beyond R+D is displaced
+    without a rebuild (a few atoms by 0.45 A, the rest by up to 0.12 A) so
+    that second-shell pairs become bonds; the forces still match the oracle's
+    fresh full-list sums."""
+    from gems_b200 import workloads as W
+    a = 4.45          # second shell at a/sqrt(2) = 3.15 A, first at 1.93 A
+    L = 6 * a
+    rng = np.random.default_rng(12)
+    pos0 = np.mod(W.diamond(6, a) + rng.normal(0, 0.01, (1728, 3)), L)
+
+    def setup(s):
+        s.set_box((L, L, L), (True, True, True))
+        s.set_tersoff(W.TERSOFF_SI)
+        s.set_skin(1.0)
+    o, g = both(pos0, W.MASS["Si"], ctx, setup=setup)
+    g.set_precision(prec)
+    o.interact()
+    g.interact()
+    n0 = g.nupd
+    step = rng.normal(size=pos0.shape)
+    mag = 0.12 * rng.random(len(step))
+    mag[rng.choice(len(step), 8, replace=False)] = 0.45
+    step *= (mag / np.linalg.norm(step, axis=1))[:, None]
+    moved = np.mod(pos0 + step, L)
+    d0 = pos0[None, :, :] - pos0[:, None, :]
+    d1 = moved[None, :, :] - moved[:, None, :]
+    d0 -= L * np.round(d0 / L)
+    d1 -= L * np.round(d1 / L)
+    r0, r1 = np.linalg.norm(d0, axis=2), np.linalg.norm(d1, axis=2)
+    assert np.sum((r0 > 3.0) & (r1 <= 3.0)) > 0   # pairs that became bonds
+    o.set_pos(moved)
+    g.set_pos(moved)
+    o.interact()
+    g.interact()
+    assert g.nupd == n0  # no rebuild: the stale list was used
+    check_forces(o, g, RMS_FP64 if prec == 0 else RMS_MIXED, E_FP64 if prec == 0 else E_MIXED)
+    g.destroy()
+
+
 def test_batched_graph_branches_equal_alone(ctx):
     """A batch runs as one graph branch per system (its own steps,
     conditional rebuilds and force passes), so systems overlap on the GPU.
