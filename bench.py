@@ -591,6 +591,29 @@ def run_c1(args, gems, torch, ctx, ext):
           **({} if args.no_cpu else {"cpu_baseline": cpu_baseline_c1(args.cpu_seconds)}))
 
 
+def tersoff_counts(g, L, R_plus_D):
+    """Bonds (r <= R+D) and ordered bond pairs (triplets) per system from its
+    current list, and the algorithmic counts of one Tersoff evaluation:
+      bytes: own position 16 (fixed point) + list 4 n + force 32 + energy 8
+             per atom (the force-kernel row of the byte model, float4 reads);
+      FP32 flops: per bond ~30 (geometry, cut-off, bond order), per triplet
+             ~45 (zeta term, its gradients for i, j and k);
+      MUFU: per bond 2 exponentials (FP64 here), per triplet 1 reciprocal."""
+    nn, lst = g.neighbour_list()
+    x = g.pos
+    i = np.repeat(np.arange(g.n), nn)
+    j = np.concatenate([lst[:c, a] for a, c in enumerate(nn)]).astype(np.int64)
+    d = x[j] - x[i]
+    Lv = np.asarray(L, dtype=np.float64)
+    d -= Lv * np.round(d / Lv)
+    bond = np.sqrt((d * d).sum(1)) <= R_plus_D
+    nb = np.bincount(i[bond], minlength=g.n)
+    bonds, trip = int(nb.sum()), int((nb * (nb - 1)).sum())
+    return {"atoms": g.n, "list_entries": int(nn.sum()), "bonds": bonds, "triplets": trip,
+            "bytes": g.n * (16 + 32 + 8) + 4 * int(nn.sum()),
+            "flops": 30 * bonds + 45 * trip, "mufu": 2 * bonds + trip}
+
+
 def run_c5(args, gems, torch, ctx, ext):
     """Tersoff Si(C), 1,000,000 atoms on a diamond lattice, NVE VV dt=1 fs."""
     from gems_b200 import workloads as W
@@ -618,11 +641,34 @@ def run_c5(args, gems, torch, ctx, ext):
                      "bonds_kernel_ms": kern[0], "gather_kernel_ms": kern[1],
                      "force_kernel_ms": kern[0] + kern[1], "rebuild_ms": kern[2], "rebuilds": g.nupd,
                      "lanes_variant": list(tuned[:2])}
+        if name == "mixed":
+            cts = tersoff_counts(g, w["L"], w["tersoff"][9] + w["tersoff"][10])
+            hbm, kind = measured_peaks()
+            pk = gems.measure_peaks(torch.cuda.current_device())
+            t_ms = kern[0] + kern[1]
+            roofs = {"hbm_us": cts["bytes"] / (hbm * 1e9) * 1e6,
+                     "fp32_us": cts["flops"] / (pk["fp32_tflops"] * 1e12) * 1e6,
+                     "mufu_us": cts["mufu"] / (pk["ex2_gops"] * 1e9) * 1e6}
+            bind = max(roofs, key=roofs.get)
+            traffic = None
+            tpath = os.path.join(ROOT, "profiles", "traffic.json")
+            if os.path.exists(tpath):
+                with open(tpath) as f:
+                    tj = json.load(f)
+                if "k_tsf_bonds" in tj and "k_tsf_gather" in tj:
+                    traffic = (tj["k_tsf_bonds"]["dram_bytes_per_atom"] +
+                               tj["k_tsf_gather"]["dram_bytes_per_atom"]) * g.n
+            roof = {"bound": "hbm", "achieved": cts["bytes"] / (t_ms * 1e-3) / 1e9, "peak": hbm,
+                    "unit": "GB/s", "frac": cts["bytes"] / (t_ms * 1e-3) / 1e9 / hbm, "traffic": traffic,
+                    "peak_source": kind, "kernel": "k_tsf_bonds + k_tsf_gather (one 1M-atom evaluation)",
+                    "ms_per_launch": t_ms, "counts": cts, "roof_times_us": roofs, "binding": bind.replace("_us", ""),
+                    "frac_of_binding_roof": roofs[bind] / (t_ms * 1e3), "compute_peaks": pk}
         g.destroy()
     head = out["mixed"] if "mixed" in out else out["fp64"]
+    extra = {"roofline": roof} if "mixed" in out else {}
     _line("atom-steps/s (Tersoff Si 1M, NVE VV)", head["value"], UNIT, args,
           {"workload": "tersoff_si_1000000 (diamond 50^3, a=5.431, 1000 K, dt 1 fs, skin 1.0)",
-           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out,
+           "md_steps_per_bench_step": args.block}, dtype="f32+f64acc", arms=out, **extra,
           **({} if args.no_cpu else {"cpu_baseline": cpu_baseline_c5(args.cpu_seconds)}))
 
 

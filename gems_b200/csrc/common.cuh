@@ -122,6 +122,7 @@ struct SysDev {
   int virial;          // force kernels accumulate the pair virial
   int cell_cap;        // cells allocated (a moving box may re-grid within them)
   double rlist;        // rcut + skin
+  float ncut_r2[8];    // the list's skip-count thresholds (rcut + 1e-4 + k skin/7)^2, k = 0..7
   double lgf_fac0, lgf_facg0, lgf_kin, lgf_press, lgf_ipm, lgf_bv, lgf_facv, lgf_av;
   // IT_AXES, per coordinate: the mode and its constants --
   // AX_FLEX (set_lgf_flex, Integration.F90:652-696):

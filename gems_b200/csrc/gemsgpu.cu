@@ -501,6 +501,10 @@ void derive(gemsgpu_ctx* ctx, SysHost& h) {
   double rl = rc + d.skin;
   d.rlist = rl;
   d.rlist2 = rl * rl;
+  for (int k = 0; k < 8; k++) {
+    const double t = rc + 1e-4 + k * (d.skin / 7.0);
+    d.ncut_r2[k] = (float)(t * t);
+  }
   // intergroup_setcells (src/Neighbour.F90:587-664)
   d.use_cells = 0;
   for (int k = 0; k < 3; k++) {

@@ -533,8 +533,7 @@ __device__ __forceinline__ void list_counts(const Arena& A, const SysDev& S, int
   unsigned short c[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    const double t = S.rcut + 1e-4 + k * (S.skin / 7.0);
-    const float T = (float)(t * t);
+    const float T = S.ncut_r2[k];
     int cnt = 0;
     for (int e0 = 0; e0 < n; e0 += 32) {
       const int e = e0 + ln;
