@@ -145,6 +145,12 @@ struct gemsgpu_ctx {
   SysState* snap_st = nullptr;
   SysDev* snap_sys = nullptr;   // boxes moved by constant-pressure steps
   bool tersoff = false;         // a Tersoff system exists: rslot, tsmask, tsfb are kept
+  // the L-BFGS workspace, kept between calls (freeing device memory can stall
+  // for a long time, so a minimisation does not allocate and free its own)
+  gg::LbWork lbw{};
+  int lbw_m = 0, lbw_scap = 0;
+  double* d_fac = nullptr;      // per-system velocity factors of gemsgpu_retemper
+  int d_fac_cap = 0;
 };
 
 // A pool: a fixed-capacity batch of systems sharing one force-field kind and
@@ -1971,7 +1977,9 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
                   A.rslot, A.tidx, A.tsmask, A.tsfb, A.tsfb32,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
-                  ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys};
+                  ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys,
+                  ctx->lbw.x0, ctx->lbw.g, ctx->lbw.gold, ctx->lbw.d, ctx->lbw.S, ctx->lbw.Y, ctx->lbw.st,
+                  ctx->d_fac};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
@@ -3368,14 +3376,18 @@ int gemsgpu_retemper(gemsgpu_ctx* ctx, int nsys, const int* sys, const double* t
     }
   }
   if (any) {
-    double* dfac = nullptr;
-    CHK(dalloc(ctx, &dfac, ctx->scap));
-    CU(cudaMemcpyAsync(dfac, fac.data(), ctx->scap * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->d_fac_cap < ctx->scap) {
+      CU(cudaStreamSynchronize(ctx->stream));
+      if (ctx->d_fac) cudaFree(ctx->d_fac);
+      ctx->d_fac = nullptr;
+      CHK(dalloc(ctx, &ctx->d_fac, ctx->scap));
+      ctx->d_fac_cap = ctx->scap;
+    }
+    CU(cudaMemcpyAsync(ctx->d_fac, fac.data(), ctx->scap * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     BlockMap m;
     CHK(get_map(ctx, ss, BLOCK, 0, &m));
-    k_scale_vel<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, dfac); ++ctx->launches;
-    CU(cudaStreamSynchronize(ctx->stream));
-    cudaFree(dfac);
+    k_scale_vel<<<m.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, m, ctx->d_fac); ++ctx->launches;
+    CU(cudaStreamSynchronize(ctx->stream));  // the host vector `fac` is released on return
   }
   return 0;
 }
@@ -4082,6 +4094,32 @@ int gemsgpu_chp_read(gemsgpu_ctx* ctx, int sys, const void* buf, size_t bytes, g
 // phases, drops finished systems from the launches, and heals a list
 // overflow by growing the list and restarting the affected searches from
 // their current points (the L-BFGS history is then discarded).
+// (re)allocate the context's L-BFGS workspace for the current arena and
+// system capacity and at least m history pairs
+int lbfgs_workspace(gemsgpu_ctx* ctx, int m) {
+  LbWork& W = ctx->lbw;
+  CU(cudaStreamSynchronize(ctx->stream));
+  void* old[7] = {W.x0, W.g, W.gold, W.d, W.S, W.Y, W.st};
+  for (void* p : old)
+    if (p) cudaFree(p);
+  W = LbWork{};
+  ctx->lbw_m = 0;
+  ctx->lbw_scap = 0;
+  const int64_t cap = ctx->acap;
+  const int mm = std::max(m, 5);  // at least GEMS's default history, so a later m = 5 call reuses it
+  CHK(dalloc(ctx, &W.x0, cap));
+  CHK(dalloc(ctx, &W.g, cap));
+  CHK(dalloc(ctx, &W.gold, cap));
+  CHK(dalloc(ctx, &W.d, cap));
+  CHK(dalloc(ctx, &W.S, (size_t)mm * cap));
+  CHK(dalloc(ctx, &W.Y, (size_t)mm * cap));
+  CHK(dalloc(ctx, &W.st, ctx->scap));
+  W.cap = cap;
+  ctx->lbw_m = mm;
+  ctx->lbw_scap = ctx->scap;
+  return 0;
+}
+
 int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m, double eps, double xtol, int itermax,
                         int* iters, int* nfun, int* status, double* emin_ev) {
   std::vector<int> ss;
@@ -4091,31 +4129,12 @@ int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m, doubl
   for (int s : ss)
     if (ctx->sys[s].d.ff == FF_NONE) return fail(ctx, GEMSGPU_ERR_STATE, "lbfgs: system %d has no force field", s);
   cudaSetDevice(ctx->device);
-  // workspace, indexed like the arena
+  // workspace, indexed like the arena: the context's, grown when the arena,
+  // the history length or the system capacity outgrew it
   const int64_t cap = ctx->acap;
-  LbWork W{};
-  W.cap = cap;
-  std::vector<void*> bufs;
-  auto take = [&](double4** p, size_t n) -> int {
-    CHK(dalloc(ctx, p, n));
-    bufs.push_back(*p);
-    return 0;
-  };
-  auto release = [&]() {
-    for (void* b : bufs) cudaFree(b);
-    bufs.clear();
-  };
   int rc = 0;
-  if ((rc = take(&W.x0, cap)) || (rc = take(&W.g, cap)) || (rc = take(&W.gold, cap)) || (rc = take(&W.d, cap)) ||
-      (rc = take(&W.S, (size_t)m * cap)) || (rc = take(&W.Y, (size_t)m * cap))) {
-    release();
-    return rc;
-  }
-  if ((rc = dalloc(ctx, &W.st, ctx->scap))) {
-    release();
-    return rc;
-  }
-  bufs.push_back(W.st);
+  if (cap > ctx->lbw.cap || m > ctx->lbw_m || ctx->scap > ctx->lbw_scap) CHK(lbfgs_workspace(ctx, m));
+  const LbWork W = ctx->lbw;
   std::vector<LbState> hs(ctx->scap);
   for (auto& L : hs) {
     L = LbState{};
@@ -4125,10 +4144,7 @@ int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m, doubl
     L.xtol = xtol;
     L.itermax = itermax;
   }
-  auto fail_clean = [&](int code) {
-    release();
-    return code;
-  };
+  auto fail_clean = [&](int code) { return code; };
   if (cudaMemcpyAsync(W.st, hs.data(), hs.size() * sizeof(LbState), cudaMemcpyHostToDevice, ctx->stream) !=
       cudaSuccess)
     return fail_clean(fail(ctx, GEMSGPU_ERR_CUDA, "lbfgs: state upload"));
@@ -4191,7 +4207,6 @@ int gemsgpu_batch_lbfgs(gemsgpu_ctx* ctx, const int* sys, int nsys, int m, doubl
     if (status) status[k] = L.phase == LB_DONE ? 0 : (L.phase == LB_FAIL ? -1 : 1);
     if (emin_ev) emin_ev[k] = L.f;
   }
-  release();
   return 0;
 }
 
