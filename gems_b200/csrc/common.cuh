@@ -101,7 +101,9 @@ struct SysDev {
   float fx_inv[3];     // fixed-point unit (A), rounded to float ...
   float fx_inv_lo[3];  // ... and its rounding remainder (hi + lo = unit)
   int skin_mic;        // skin test on minimum-image displacements
-  int list_warp;       // cells of few atoms: the list kernel works one warp per cell
+  int list_warp;       // list kernel: 0 one CTA per cell, 1 / 2 one warp per cell (128 / 512-candidate tile)
+  int list_img;        // list build in the image frame (every periodic dim has >= 3 cells)
+  int pad_list;
   // integrator
   double dt;
   double cc0, cc1, cc2, sdr, sdv, crv1, crv2, skt;
@@ -123,6 +125,7 @@ struct SysDev {
   int cell_cap;        // cells allocated (a moving box may re-grid within them)
   double rlist;        // rcut + skin
   float ncut_r2[8];    // the list's skip-count thresholds (rcut + 1e-4 + k skin/7)^2, k = 0..7
+  float nsplit_r2;     // force-order split below ncut_r2[0]: the inner regime (SMA-TB rci^2, Tersoff (R-D)^2)
   double lgf_fac0, lgf_facg0, lgf_kin, lgf_press, lgf_ipm, lgf_bv, lgf_facv, lgf_av;
   // IT_AXES, per coordinate: the mode and its constants --
   // AX_FLEX (set_lgf_flex, Integration.F90:652-696):

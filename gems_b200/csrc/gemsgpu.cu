@@ -369,15 +369,22 @@ int tersoff_records(gemsgpu_ctx* ctx) {
 
 // dynamic shared memory of the two cell-list kernels for list capacity lcap
 int list_smem_attr(gemsgpu_ctx* ctx, int lcap) {
-  const size_t smem = list_smem(lcap), smemw = listw_smem(lcap);
-  if (smem > 200 * 1024 || smemw > 200 * 1024)
+  const size_t smem = list_smem(lcap), smemw = listw_smem<128>(lcap), smemw4 = listw_smem<512>(lcap);
+  if (smem > 200 * 1024 || smemw > 200 * 1024 || smemw4 > 200 * 1024)
     return fail(ctx, GEMSGPU_ERR_ARG, "neighbour capacity %d too large", lcap);
   if (smem > 48 * 1024)
     CU(cudaFuncSetAttribute(k_list_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  if (smemw > 48 * 1024)
-    CU(cudaFuncSetAttribute(k_list_cells_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw));
+  if (smemw > 48 * 1024) {
+    CU(cudaFuncSetAttribute(k_list_cells_w<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw));
+    CU(cudaFuncSetAttribute(k_list_cells_w<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw));
+  }
+  if (smemw4 > 48 * 1024) {
+    CU(cudaFuncSetAttribute(k_list_cells_w<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw4));
+    CU(cudaFuncSetAttribute(k_list_cells_w<512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw4));
+  }
   return 0;
 }
+
 
 int grow_list(gemsgpu_ctx* ctx, int lcap) {
   Arena& A = ctx->A;
@@ -511,6 +518,15 @@ void derive(gemsgpu_ctx* ctx, SysHost& h) {
     const double t = rc + 1e-4 + k * (d.skin / 7.0);
     d.ncut_r2[k] = (float)(t * t);
   }
+  // the force order puts a pair potential's inner regime first (SMA-TB
+  // r <= rci, Tersoff r <= R - D), so a warp's lanes meet the same branch
+  // at the same slot; it only orders entries, so any value <= ncut_r2[0] is right
+  double rin = 0.0;
+  if (d.ff == FF_SMATB)
+    for (auto& p : h.prm)
+      if (p.v[13] != 0.0) rin = std::max(rin, p.v[5]);
+  if (d.ff == FF_TERSOFF) rin = d.ts.R - d.ts.D;
+  d.nsplit_r2 = std::min((float)(rin * rin), d.ncut_r2[0]);
   // intergroup_setcells (src/Neighbour.F90:587-664)
   d.use_cells = 0;
   for (int k = 0; k < 3; k++) {
@@ -534,8 +550,16 @@ void derive(gemsgpu_ctx* ctx, SysHost& h) {
     }
   }
   d.ncell = d.use_cells ? d.nc[0] * d.nc[1] * d.nc[2] : 0;
-  // cells of fewer atoms than a CTA's warps: the warp-per-cell list kernel
-  d.list_warp = d.use_cells && (double)h.n < 6.0 * d.ncell ? 1 : 0;
+  // list kernel: one warp per cell with a 128-candidate tile for cells of
+  // about three atoms or fewer, a 512-candidate tile up to sixteen, else one
+  // CTA per cell
+  const double per_cell = d.use_cells ? (double)h.n / d.ncell : 0.0;
+  d.list_warp = !d.use_cells ? 0 : per_cell < 3.5 ? 1 : per_cell <= 16.0 ? 2 : 0;
+  // the list build's FP32 frame: stencil images when every periodic dim
+  // has three cells or more (a constant-pressure box never shrinks below)
+  d.list_img = 1;
+  for (int k = 0; k < 3; k++)
+    if (d.use_cells && d.pbc[k] && d.nc[k] < 3) d.list_img = 0;
   // fixed-point frame of the mixed kernels
   for (int k = 0; k < 3; k++) {
     bool per = d.boxed && d.pbc[k];
@@ -896,6 +920,21 @@ int launch_forces(gemsgpu_ctx* ctx, const std::vector<int>& ss) {
 // grid of the rebuild kernels that visit only flagged systems' blocks
 int rebuild_grid(const gemsgpu_ctx* ctx, int nblk) { return std::max(1, std::min(nblk, 8 * ctx->nsm)); }
 
+// the warp-per-cell list kernels for the systems of each tile size
+// (t128 / t512) and frame ([0] integer, [1] image)
+int launch_list_w(gemsgpu_ctx* ctx, const BlockMap& mc8, const bool* t128, const bool* t512) {
+  cudaStream_t st = ctx->stream;
+  const Arena& A = ctx->A;
+  const int g = rebuild_grid(ctx, mc8.nblk);
+  if (t128[1]) k_list_cells_w<128, true><<<g, BLOCK, listw_smem<128>(A.lcap), st>>>(A, mc8);
+  if (t128[0]) k_list_cells_w<128, false><<<g, BLOCK, listw_smem<128>(A.lcap), st>>>(A, mc8);
+  if (t512[1]) k_list_cells_w<512, true><<<g, BLOCK, listw_smem<512>(A.lcap), st>>>(A, mc8);
+  if (t512[0]) k_list_cells_w<512, false><<<g, BLOCK, listw_smem<512>(A.lcap), st>>>(A, mc8);
+  ctx->launches += t128[0] + t128[1] + t512[0] + t512[1];
+  CU(cudaGetLastError());
+  return 0;
+}
+
 int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 0) {
   BlockMap ma, mc, mc8, mc1;
   const int* sa;
@@ -915,17 +954,14 @@ int launch_rebuild(gemsgpu_ctx* ctx, const std::vector<int>& ss, int in_graph = 
     k_scan2<<<(int)ss.size(), BLOCK, 0, st>>>(A, sa, (int)ss.size()); ++ctx->launches;
     k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
     k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
-    bool wide = false, narrow = false;
+    bool kind[3][2] = {};
     for (int s : ss)
-      if (ctx->sys[s].d.use_cells) (ctx->sys[s].d.list_warp ? narrow : wide) = true;
-    if (wide) {
+      if (ctx->sys[s].d.use_cells) kind[ctx->sys[s].d.list_warp][ctx->sys[s].d.list_img] = true;
+    if (kind[0][0] || kind[0][1]) {
       k_list_cells<<<rebuild_grid(ctx, mc1.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc1);
       ++ctx->launches;
     }
-    if (narrow) {
-      k_list_cells_w<<<rebuild_grid(ctx, mc8.nblk), BLOCK, listw_smem(A.lcap), st>>>(A, mc8);
-      ++ctx->launches;
-    }
+    CHK(launch_list_w(ctx, mc8, kind[1], kind[2]));
   }
   if (n2) {
     k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
@@ -1730,8 +1766,9 @@ int pool_rebuild(gemsgpu_pool* P, int in_graph) {
   k_scatter<<<ma.nblk, BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   k_sort_cells<<<rebuild_grid(ctx, mc8.nblk), BLOCK, 0, st>>>(A, mc8); ++ctx->launches;
   k_list_cells<<<rebuild_grid(ctx, mc8.nblk * LIST_SPLIT), BLOCK, list_smem(A.lcap), st>>>(A, mc8);
-  k_list_cells_w<<<rebuild_grid(ctx, mc8.nblk), BLOCK, listw_smem(A.lcap), st>>>(A, mc8);
-  ctx->launches += 2;
+  ++ctx->launches;
+  const bool all[2] = {true, true};
+  CHK(launch_list_w(ctx, mc8, all, all));
   k_list_n2<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;
   if (P->ff == FF_TERSOFF) {
     k_tsf_rslot<<<rebuild_grid(ctx, ma.nblk), BLOCK, 0, st>>>(A, ma); ++ctx->launches;

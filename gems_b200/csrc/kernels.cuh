@@ -474,81 +474,81 @@ __device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m, i
   atomicMax(&A.st[s].maxnn, m);
 }
 
-// Sort an atom's first n <= 64 list entries by (distance, slot) across a
-// warp: lane l holds entries l and l + 32 as 64-bit keys (the bits of the
-// non-negative float r^2 above the slot, so the integer order is the order
-// of the rank rule "closer first, then the earlier slot"), padding keys are
-// all ones.  Bitonic network (Batcher 1968) over the 64 positions
-// q = lane + 32 h; on return k0 / k1 hold the keys at positions lane and
-// lane + 32 of the sorted order.
-__device__ __forceinline__ void warp_sort64(const float* rrow, int n, int ln, unsigned long long& k0,
-                                            unsigned long long& k1) {
-  k0 = ln < n ? ((unsigned long long)__float_as_uint(rrow[ln]) << 32) | (unsigned)ln : ~0ull;
-  k1 = ln + 32 < n ? ((unsigned long long)__float_as_uint(rrow[ln + 32]) << 32) | (unsigned)(ln + 32) : ~0ull;
-  for (int size = 2; size <= 64; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      if (stride == 32) {  // partners in the same lane: positions lane and lane + 32
-        const unsigned long long lo = min(k0, k1), hi = max(k0, k1);
-        k0 = lo;  // size 64 sorts the whole sequence ascending
-        k1 = hi;
-        continue;
-      }
-      const unsigned long long p0 = __shfl_xor_sync(0xffffffffu, k0, stride);
-      const unsigned long long p1 = __shfl_xor_sync(0xffffffffu, k1, stride);
-      const bool lower = (ln & stride) == 0;
-      const bool up0 = (ln & size) == 0, up1 = ((ln + 32) & size) == 0;
-      k0 = (lower == up0) ? min(k0, p0) : max(k0, p0);
-      k1 = (lower == up1) ? min(k1, p1) : max(k1, p1);
-    }
-  }
-}
-
-// The same rank rule for n <= 32 entries, one key per lane: a bitonic
-// network over 32 positions (15 compare-exchange stages of one shuffle each,
-// against 21 stages of two for warp_sort64).  On return k0 holds the key at
-// position lane of the sorted order.
-__device__ __forceinline__ void warp_sort32(const float* rrow, int n, int ln, unsigned long long& k0) {
-  k0 = ln < n ? ((unsigned long long)__float_as_uint(rrow[ln]) << 32) | (unsigned)ln : ~0ull;
-#pragma unroll
-  for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      const unsigned long long p0 = __shfl_xor_sync(0xffffffffu, k0, stride);
-      const bool lower = (ln & stride) == 0;
-      const bool up = (ln & size) == 0 || size == 32;
-      k0 = (lower == up) ? min(k0, p0) : max(k0, p0);
-    }
-  }
-}
-
-// flist holds an atom's entries sorted by their distance at the build, and
-// no pair has come closer since by more than the skin test's bound D
-// (SysState::dmax).  So the entries built at r >= rcut + 1e-4 + k skin/7
+// The force order: an atom's entries grouped by distance band at the build,
+// slot order within a band.  Band 0 holds the inner regime of the pair
+// potential (staged r^2 below nsplit_r2: SMA-TB r <= rci, Tersoff r <= R-D),
+// so the lanes of a warp, one atom each, take the same branch at the same
+// slot; band 1 the rest below T_0; band b >= 2 the entries that reach b - 1
+// of the skip thresholds T_k = (rcut + 1e-4 + k skin/7)^2, k = 0..7.  The
+// first ncut[k] entries are then exactly those with staged r^2 below T_k.
+//
+// Between builds no pair has come closer by more than the skin test's bound
+// D (SysState::dmax), so the entries built at r >= rcut + 1e-4 + k skin/7
 // with k skin/7 >= D lie beyond every cut-off of the system now and add
-// nothing: the force kernels stop before them.  The counts are of entries
-// with (float) r^2 below the float of each threshold squared; the float
-// roundings move a distance by under 1e-6 A, inside the 1e-4 A margin.
-__device__ __forceinline__ void list_counts(const Arena& A, const SysDev& S, int i, int n, const float* rrow,
-                                            int ln) {
-  unsigned short c[8];
+// nothing: the force kernels stop before them.  The staged r^2 is within
+// err of the exact one (err: the list build's FP32 error bound), so the
+// thresholds are raised by err: an entry counts above T_k only if its exact
+// r^2 is; the float roundings of r^2 and of the thresholds move a distance
+// by under 1e-6 A, inside the 1e-4 A margin.
+//
+// A warp writes the row of atom i: the first pass counts the entries below
+// each threshold (one ballot per threshold and 32 entries), the second
+// places each entry at its band's next free position (a match over the
+// lanes' bands ranks lanes of one band, and the band's first lane advances
+// the band's offset in boff, a 10-entry per-warp scratch).
+__device__ __forceinline__ void list_force_order(const Arena& A, const SysDev& S, int i, int n, const int* row,
+                                                 const float* rrow, float err, int* boff, int ln) {
+  const unsigned FULL = 0xffffffffu, lt = (1u << ln) - 1u;
+  float T[8];
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const float T = S.ncut_r2[k];
-    int cnt = 0;
-    for (int e0 = 0; e0 < n; e0 += 32) {
-      const int e = e0 + ln;
-      cnt += __popc(__ballot_sync(0xffffffffu, e < n && rrow[e] < T));
-    }
-    c[k] = (unsigned short)min(cnt, 65535);
+  for (int k = 0; k < 8; k++) T[k] = __fadd_ru(S.ncut_r2[k], err);
+  const float Ts = S.nsplit_r2;  // <= ncut_r2[0]
+  int c[8], cs = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) c[k] = 0;
+  for (int e0 = 0; e0 < n; e0 += 32) {
+    const int e = e0 + ln;
+    const float r = e < n ? rrow[e] : __int_as_float(0x7f800000);  // +inf is below no threshold
+    cs += __popc(__ballot_sync(FULL, r < Ts));
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] += __popc(__ballot_sync(FULL, r < T[k]));
   }
-  if (ln == 0)
-    A.ncut[i] = make_uint4(c[0] | (unsigned)c[1] << 16, c[2] | (unsigned)c[3] << 16, c[4] | (unsigned)c[5] << 16,
-                           c[6] | (unsigned)c[7] << 16);
+  if (ln == 0) {
+    unsigned short h[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) h[k] = (unsigned short)min(c[k], 65535);
+    A.ncut[i] = make_uint4(h[0] | (unsigned)h[1] << 16, h[2] | (unsigned)h[3] << 16, h[4] | (unsigned)h[5] << 16,
+                           h[6] | (unsigned)h[7] << 16);
+  }
+  if (ln < 10) {  // band b starts after the entries of the bands below it
+    int v = ln == 1 ? cs : 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      if (ln == k + 2) v = c[k];
+    boff[ln] = v;
+  }
+  __syncwarp();
+  for (int e0 = 0; e0 < n; e0 += 32) {
+    const int e = e0 + ln;
+    const bool v = e < n;
+    int b = 10;  // lanes past the row share a band of their own
+    if (v) {
+      const float r = rrow[e];
+      b = r >= Ts;
+#pragma unroll
+      for (int k = 0; k < 8; k++) b += r >= T[k];
+    }
+    const unsigned M = __match_any_sync(FULL, b);
+    if (v) A.flist[(size_t)(boff[b] + __popc(M & lt)) * A.cap + i] = row[e] & 0x7fffffff;
+    __syncwarp();
+    if (v && (M & lt) == 0) boff[b] += __popc(M);
+    __syncwarp();
+  }
 }
 
 // the flist entries an atom's force loop must visit this step
 __device__ __forceinline__ int live_entries(const Arena& A, const SysDev& S, const SysState& st, int i, int nn) {
-  if (!(S.skin > 0.0) || !S.use_cells) return nn;  // O(N^2) lists are not distance-sorted
+  if (!(S.skin > 0.0) || !S.use_cells) return nn;  // O(N^2) lists are not grouped by band
   const double q = st.dmax * 7.0 / S.skin;
   if (!(q <= 7.0)) return nn;
   const int k = (int)ceil(q);
@@ -558,10 +558,10 @@ __device__ __forceinline__ int live_entries(const Arena& A, const SysDev& S, con
 
 // A warp's staged row of atom i (m accepted candidates in the reference's
 // order: ids, bit 31 set on the entries a half list leaves out, and r^2 as
-// float) out to the arena: `list` in the reference's order, `flist` ranked
-// by distance, the skip counts and nn / hnn.
+// float, within err of the exact r^2) out to the arena: `list` in the
+// reference's order, `flist` in the force order, the skip counts and nn / hnn.
 __device__ __forceinline__ void list_row_out(const Arena& A, const SysDev& S, int s, int i, int m,
-                                             const int* row, const float* rrow, int ln) {
+                                             const int* row, const float* rrow, float err, int* boff, int ln) {
   const int n = min(m, A.lcap);
   // the reference's list: the whole row, or its half-list entries in order
   int mh = 0;
@@ -572,30 +572,167 @@ __device__ __forceinline__ void list_row_out(const Arena& A, const SysDev& S, in
     if (h) A.list[(size_t)(mh + __popc(hb & ((1u << ln) - 1u))) * A.cap + i] = row[e];
     mh += __popc(hb);
   }
-  if (n <= 32) {
-    // force order by a warp bitonic sort of (distance, slot) keys
-    unsigned long long k0;
-    warp_sort32(rrow, n, ln, k0);
-    if (ln < n) A.flist[(size_t)ln * A.cap + i] = row[(int)(k0 & 0xffffffffu)] & 0x7fffffff;
-  } else if (n <= 64) {
-    unsigned long long k0, k1;
-    warp_sort64(rrow, n, ln, k0, k1);
-    if (ln < n) A.flist[(size_t)ln * A.cap + i] = row[(int)(k0 & 0xffffffffu)] & 0x7fffffff;
-    if (ln + 32 < n) A.flist[(size_t)(ln + 32) * A.cap + i] = row[(int)(k1 & 0xffffffffu)] & 0x7fffffff;
-  } else {
-    for (int e = ln; e < n; e += 32) {
-      // force order: rank by distance, ties by slot
-      const float re = rrow[e];
-      int rank = 0;
-      for (int f = 0; f < n; f++) {
-        const float rf = rrow[f];
-        rank += (rf < re) || (rf == re && f < e);
-      }
-      A.flist[(size_t)rank * A.cap + i] = row[e] & 0x7fffffff;
-    }
-  }
-  list_counts(A, S, i, n, rrow, ln);
+  list_force_order(A, S, i, n, row, rrow, err, boff, ln);
   if (ln == 0) list_done(A, s, i, m, mh);
+}
+
+// ---- the candidate test of the cell-list builds
+// A candidate's r^2 is first computed in FP32 from a 16-byte record staged
+// per candidate (float4: three coordinates and the atom id as int bits), in
+// one of two frames:
+//  * image frame (every periodic dim has >= 3 cells, SysDev::list_img):
+//    coordinates relative to the cell's origin, each candidate shifted by
+//    its stencil cell's periodic image.  With >= 3 cells a periodic dim's
+//    three stencil cells are distinct, so an atom appears once in the
+//    stencil, at the one image within a cell of the home cell; an image
+//    within rlist (<= a cell) of the atom must be that one, so this r^2 is
+//    the minimum-image one for every pair within rlist.  Open dims use the
+//    plain difference, as rd_exact does.  Components are within 2^-24 of
+//    3 cells + rlist (open dims: of L + 3 cells + rlist, atoms lie in the
+//    box) per rounding.
+//  * integer frame (a periodic dim has fewer cells): integer coordinates, a
+//    periodic dim mapping [0, L) onto the 32-bit ring (the wrapped int32
+//    difference is the minimum image), an open dim 2^30 units per
+//    max(L, rlist) (a difference that wraps is one of more than 2 rlist).
+//    The difference shifted right by 10 bits (|v| < 2^21) converts to float
+//    exactly through the 1.5 * 2^23 bias, so a component is off by under
+//    1025 units plus two float roundings.
+// err bounds |r2f - r^2| for pairs near rlist.  r2f < lo (rlist^2 - err)
+// is inside the exact test's strict rlist^2 and r2f >= hi (rlist^2 + err)
+// outside it; only candidates between take the exact FP64 test (rd_exact,
+// the reference's arithmetic).  The lists are therefore the ones the exact
+// test over every candidate gives.
+struct ListFrame {
+  double ls[3];   // integer frame: integer units per Angstrom
+  float unit[3];  // integer frame: Angstrom per filter unit (1024 integer units)
+  float lo, hi;   // r2f < lo: inside rlist; r2f >= hi: outside
+  float err;      // bound on |r2f - r^2| for r^2 < hi
+  int img;        // 1: image frame, 0: integer frame
+};
+
+__device__ __forceinline__ ListFrame list_frame(const SysDev& S) {
+  ListFrame f;
+  f.img = S.list_img;
+  double sd = 0.0, sd2 = 0.0, dm = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double dk;
+    if (f.img) {
+      const double span = (S.pbc[k] ? 3.0 * S.cell[k] : S.L[k] + 3.0 * S.cell[k]) + S.rlist;
+      dk = 4.0 * 5.9604644775390625e-8 * span;
+      f.ls[k] = 0.0;
+      f.unit[k] = 0.0f;
+    } else {
+      const double M = S.pbc[k] ? S.L[k] : 4.0 * fmax(S.L[k], S.rlist);  // Angstrom per 2^32 units
+      f.ls[k] = 4294967296.0 / M;
+      f.unit[k] = (float)(M * 2.384185791015625e-07);  // M / 2^22
+      dk = 1025.0 * M * 2.3283064365386963e-10 + 2.4e-7 * S.rlist;
+    }
+    sd += dk;
+    sd2 += dk * dk;
+    dm = fmax(dm, dk);
+  }
+  const double err = 2.0 * (S.rlist + dm) * sd + sd2 + 1e-6 * S.rlist2;
+  f.err = __double2float_ru(err);
+  f.lo = __double2float_rd(S.rlist2 - err);
+  f.hi = __double2float_ru(S.rlist2 + err);
+  return f;
+}
+
+// integer-frame record of a position (atom id in w)
+__device__ __forceinline__ float4 list_coords(const ListFrame& f, double4 p, int id) {
+  return make_float4(__int_as_float((int)(unsigned)(unsigned long long)__double2ll_rn(p.x * f.ls[0])),
+                     __int_as_float((int)(unsigned)(unsigned long long)__double2ll_rn(p.y * f.ls[1])),
+                     __int_as_float((int)(unsigned)(unsigned long long)__double2ll_rn(p.z * f.ls[2])),
+                     __int_as_float(id));
+}
+
+// one integer-frame component in Angstrom
+__device__ __forceinline__ float list_comp(float a, float b, float unit) {
+  const int v = (int)((unsigned)__float_as_int(b) - (unsigned)__float_as_int(a)) >> 10;
+  return (__int_as_float(0x4B400000 + v) - 12582912.0f) * unit;
+}
+
+template <bool IMG>
+__device__ __forceinline__ float list_r2(const ListFrame& f, float4 a, float4 b) {
+  float x, y, z;
+  if (IMG) {
+    x = b.x - a.x;
+    y = b.y - a.y;
+    z = b.z - a.z;
+  } else {
+    x = list_comp(a.x, b.x, f.unit[0]);
+    y = list_comp(a.y, b.y, f.unit[1]);
+    z = list_comp(a.z, b.z, f.unit[2]);
+  }
+  return fmaf(z, z, fmaf(y, y, x * x));
+}
+
+// the staged record of candidate p (id j) of a stencil cell with periodic
+// shift sh, for a home cell with origin o
+template <bool IMG>
+__device__ __forceinline__ float4 list_record(const ListFrame& f, double4 p, int j, double3 sh, double3 o) {
+  if (IMG)
+    return make_float4((float)(p.x + sh.x - o.x), (float)(p.y + sh.y - o.y), (float)(p.z + sh.z - o.z),
+                       __int_as_float(j));
+  return list_coords(f, p, j);
+}
+
+// stencil cell k of home cell (cx, cy, cz): its id and the periodic shift
+// that takes its atoms to the image next to the home cell (open dims: none)
+__device__ __forceinline__ int stencil_cell(const SysDev& S, int k, int cx, int cy, int cz, double3& sh) {
+  int dx, dy, dz;
+  stencil(k, dx, dy, dz);
+  const int ux = cx + dx, uy = cy + dy, uz = cz + dz;
+  const int x = (ux + S.nc[0]) % S.nc[0];
+  const int y = (uy + S.nc[1]) % S.nc[1];
+  const int z = (uz + S.nc[2]) % S.nc[2];
+  sh = make_double3(S.pbc[0] ? (ux - x) * S.cell[0] : 0.0, S.pbc[1] ? (uy - y) * S.cell[1] : 0.0,
+                    S.pbc[2] ? (uz - z) * S.cell[2] : 0.0);
+  return S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
+}
+
+// One warp tests atom i (chain position a of its cell, staged record ri)
+// against the staged candidates t0 .. t0 + tn - 1 (records cf[0 .. tn-1]),
+// 32 at a time, and appends the accepted ones to the row in candidate
+// order: ids (bit 31 on those a half list leaves out) and r^2 as float.
+// m counts the accepted candidates, lcap or more.
+template <bool IMG>
+__device__ __forceinline__ void list_scan_tile(const Arena& A, const SysDev& S, const ListFrame& f, const float4* cf,
+                                               int t0, int tn, int i, int a, float4 ri, bool half, int own, int hend,
+                                               int* row, float* rrow, int lcap, int& m, int ln) {
+  const unsigned FULL = 0xffffffffu, lt = (1u << ln) - 1u;
+  for (int q0 = 0; q0 < tn; q0 += 32) {
+    const int q = q0 + ln;
+    bool in = false, maybe = false;
+    int j = -1;
+    float r2 = 0.0f;
+    if (q < tn) {
+      const float4 c = cf[q];
+      j = __float_as_int(c.w);
+      r2 = list_r2<IMG>(f, ri, c);
+      in = r2 < f.lo && j != i;
+      maybe = r2 >= f.lo && r2 < f.hi && j != i;
+    }
+    if (__any_sync(FULL, maybe) && maybe) {  // within the error bound of rlist: the exact test
+      const double rd = rd_exact(S, A.pos[i], A.pos[j]);
+      in = rd < S.rlist2;
+      r2 = (float)rd;
+    }
+    const unsigned bal = __ballot_sync(FULL, in);
+    if (in) {
+      const int mm = m + __popc(bal & lt);
+      if (mm < lcap) {
+        // the half list (linkedcell_selfhalf): the atoms after i in its own
+        // cell's chain, then the other 13 cells of the half stencil
+        const int g = t0 + q;
+        const bool in_half = !half || (g < own ? g > a : g < hend);
+        row[mm] = in_half ? j : (int)((unsigned)j | 0x80000000u);  // bit 31: full list only
+        rrow[mm] = r2;
+      }
+    }
+    m += __popc(bal);
+  }
 }
 
 // linkedcell_self / linkedcell_selfhalf (src/Neighbour.F90:991-1161): the
@@ -603,29 +740,122 @@ __device__ __forceinline__ void list_row_out(const Arena& A, const SysDev& S, in
 // wrap (cell_pbc, :1350-1376); keep j if rd < (rcut+nb_dcut)^2 (strict).
 // For every atom of a cell the candidates are the same sequence: the
 // stencil cells of that cell in stencil order, each in its chain order.  So
-// one CTA takes one cell: it stages that sequence in shared memory
-// (LIST_TILE candidates at a time) and its warps test the cell's atoms
-// against it, one atom per warp; the lanes test 32 consecutive candidates
-// and a ballot keeps the accepted ones in candidate order, so each list
-// comes out in the reference's order.  A warp stages its atom's row (ids
-// and distances), then writes it to `list` as it is and to `flist` ranked
-// by distance.
+// one CTA takes one cell: warp 0 scans the stencil cells' counts, the CTA
+// stages that sequence's records in shared memory (LIST_TILE candidates at
+// a time) and its warps test the cell's atoms against it, one atom per warp
+// (list_scan_tile), so each list comes out in the reference's order.  The
+// home cell's atoms are the sequence's first candidates, so an atom's own
+// record comes from the tile.  A warp stages its atom's row (ids and
+// distances), then writes it to `list` as it is and to `flist` in the force
+// order.
 constexpr int LIST_ATOMS = BLOCK / 32;  // atoms per pass: one per warp
-constexpr int LIST_TILE = 1024;         // candidates staged at a time
+constexpr int LIST_TILE = 512;          // candidates staged at a time
 constexpr int LIST_SPLIT = 4;           // CTAs that may share one cell's atoms
 __host__ __device__ constexpr size_t list_smem(int lcap) {
-  return (size_t)LIST_TILE * (sizeof(double4) + sizeof(int)) +
-         (size_t)LIST_ATOMS * lcap * (sizeof(int) + sizeof(float));
+  return (size_t)LIST_TILE * sizeof(float4) + (size_t)LIST_ATOMS * lcap * (sizeof(int) + sizeof(float));
+}
+
+template <bool IMG>
+__device__ __forceinline__ void list_cells_item(const Arena& A, const BlockMap& C, int b, int part, float4* cf,
+                                                int* stage, float* stage_rd, int* nb_start, int* nb_pref,
+                                                double3* nb_sh, int* boff) {
+  const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  const int s = C.sys[b];
+  const SysDev& S = A.sys[s];
+  const ListFrame f = list_frame(S);
+  const bool half = S.half != 0;
+  for (int c = C.first[b]; c < C.end[b]; c++) {
+    const int cnt0 = A.cell_n[c];
+    const int a_first = part * LIST_ATOMS;
+    if (a_first >= cnt0) continue;  // uniform per CTA
+    const int cl = c - S.cell_off;
+    const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
+    const double3 o = make_double3(cx * S.cell[0], cy * S.cell[1], cz * S.cell[2]);
+    if (warp == 0) {  // the stencil cells' starts, shifts and first candidates (a warp scan)
+      int cn = 0, cs = 0;
+      double3 sh = make_double3(0, 0, 0);
+      if (ln < NSTENCIL) {
+        const int cid = stencil_cell(S, ln, cx, cy, cz, sh);
+        cs = A.cell_start[cid];
+        cn = A.cell_n[cid];
+      }
+      int inc = cn;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int t = __shfl_up_sync(FULL, inc, d);
+        if (ln >= d) inc += t;
+      }
+      if (ln < NSTENCIL) {
+        nb_start[ln] = cs;
+        nb_pref[ln] = inc - cn;
+        nb_sh[ln] = sh;
+      }
+      if (ln == NSTENCIL - 1) nb_pref[NSTENCIL] = inc;
+    }
+    __syncthreads();
+    const int T = nb_pref[NSTENCIL];  // candidates of every atom of the cell
+    const int own = nb_pref[1];       // the first cell of the stencil is the cell itself
+    const int hend = nb_pref[14];     // end of the half stencil's candidates
+    auto stage_tile = [&](int t0, int tn) {
+      for (int q = threadIdx.x; q < tn; q += BLOCK) {
+        const int g = t0 + q;
+        int k = 0;  // the last stencil cell whose first candidate is <= g
+#pragma unroll
+        for (int step = 16; step; step >>= 1)
+          if (k + step < NSTENCIL && nb_pref[k + step] <= g) k += step;
+        const int j = A.cell_atoms[nb_start[k] + (g - nb_pref[k])];
+        cf[q] = list_record<IMG>(f, A.pos[j], j, nb_sh[k], o);
+      }
+    };
+    const bool one = T <= LIST_TILE;  // one tile stays staged for all this CTA's passes
+    if (one) {
+      stage_tile(0, T);
+      __syncthreads();
+    }
+    for (int a0 = a_first; a0 < cnt0; a0 += LIST_ATOMS * LIST_SPLIT) {
+      const int a = a0 + warp;  // this warp's atom: chain position a of the cell
+      const bool act = a < cnt0;
+      int i = -1;
+      float4 ri = make_float4(0, 0, 0, 0);
+      if (act) {
+        if (one) {
+          ri = cf[a];  // the home cell's atoms come first, with no shift
+          i = __float_as_int(ri.w);
+        } else {
+          i = A.cell_atoms[nb_start[0] + a];
+          ri = list_record<IMG>(f, A.pos[i], i, make_double3(0, 0, 0), o);
+        }
+      }
+      int* row = stage + warp * A.lcap;
+      float* rrow = stage_rd + warp * A.lcap;
+      int m = 0;
+      for (int t0 = 0; t0 < T; t0 += LIST_TILE) {
+        const int tn = min(LIST_TILE, T - t0);
+        if (!one) {
+          __syncthreads();
+          stage_tile(t0, tn);
+          __syncthreads();
+        }
+        if (act) list_scan_tile<IMG>(A, S, f, cf, t0, tn, i, a, ri, half, own, hend, row, rrow, A.lcap, m, ln);
+      }
+      __syncwarp();
+      if (act) list_row_out(A, S, s, i, m, row, rrow, f.err, boff, ln);
+      __syncwarp();
+    }
+    __syncthreads();  // nb_* and the tile are rewritten for the next cell
+  }
 }
 
 __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
-  extern __shared__ __align__(32) unsigned char list_sh[];
-  double4* cpos = reinterpret_cast<double4*>(list_sh);                      // LIST_TILE positions
-  int* cidx = reinterpret_cast<int*>(cpos + LIST_TILE);                     // LIST_TILE atom ids
-  int* stage = cidx + LIST_TILE;                                            // LIST_ATOMS x lcap ids
-  float* stage_rd = reinterpret_cast<float*>(stage + LIST_ATOMS * A.lcap);  // and their rd
-  __shared__ int nb_start[27], nb_cnt[27], nb_pref[28];
-  const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  extern __shared__ __align__(16) unsigned char list_sh[];
+  float4* cf = reinterpret_cast<float4*>(list_sh);                          // LIST_TILE records
+  int* stage = reinterpret_cast<int*>(cf + LIST_TILE);                      // LIST_ATOMS x lcap ids
+  float* stage_rd = reinterpret_cast<float*>(stage + LIST_ATOMS * A.lcap);  // and their r^2
+  __shared__ int nb_start[NSTENCIL], nb_pref[NSTENCIL + 1];
+  __shared__ double3 nb_sh[NSTENCIL];
+  __shared__ int boff_sh[LIST_ATOMS][16];
+  const int warp = threadIdx.x >> 5;
   // work item w = (map block w % nblk, part w / nblk): the part
   // takes atom passes part, part + LIST_SPLIT, ... of each of the block's
   // cells, so a cell of many atoms is shared by up to LIST_SPLIT CTAs
@@ -639,210 +869,157 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
   };
   rebuild_items(C.nblk * LIST_SPLIT, live, [&](int w) {
     const int b = w % C.nblk, part = w / C.nblk;
-    const int s = C.sys[b];
-    const SysDev& S = A.sys[s];
-    const int nst = 27;  // half lists: the first 14 stencil cells are the half stencil
-    for (int c = C.first[b]; c < C.end[b]; c++) {
-      const int cnt0 = A.cell_n[c];
-      const int a_first = part * LIST_ATOMS;
-      if (a_first >= cnt0) continue;  // uniform per CTA
-      const int cl = c - S.cell_off;
-      const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
-      if ((int)threadIdx.x < nst) {
-        int dx, dy, dz;
-        stencil(threadIdx.x, dx, dy, dz);
-        const int x = (cx + dx + S.nc[0]) % S.nc[0];
-        const int y = (cy + dy + S.nc[1]) % S.nc[1];
-        const int z = (cz + dz + S.nc[2]) % S.nc[2];
-        const int cid = S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
-        nb_start[threadIdx.x] = A.cell_start[cid];
-        nb_cnt[threadIdx.x] = A.cell_n[cid];
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int k = 0; k < nst; k++) {
-          nb_pref[k] = acc;
-          acc += nb_cnt[k];
-        }
-        nb_pref[nst] = acc;
-      }
-      __syncthreads();
-      const int T = nb_pref[nst];     // candidates of every atom of the cell
-      const int own = nb_pref[1];     // the first cell of the stencil is the cell itself
-      const int hend = nb_pref[14];   // end of the half stencil's candidates
-      const int beg0 = nb_start[0];
-      for (int a0 = a_first; a0 < cnt0; a0 += LIST_ATOMS * LIST_SPLIT) {
-        const int a = a0 + warp;      // this warp's atom: chain position a of the cell
-        const bool act = a < cnt0;
-        const int i = act ? A.cell_atoms[beg0 + a] : -1;
-        const double4 xi = act ? A.pos[i] : make_double4(0, 0, 0, 0);
-        int* row = stage + warp * A.lcap;
-        float* rrow = stage_rd + warp * A.lcap;
-        int m = 0;
-        for (int t0 = 0; t0 < T; t0 += LIST_TILE) {
-          const int tn = min(LIST_TILE, T - t0);
-          if (T > LIST_TILE || a0 == a_first) {  // one tile stays staged for all this CTA's passes
-            __syncthreads();
-            for (int q = threadIdx.x; q < tn; q += BLOCK) {
-              const int g = t0 + q;
-              int k = 0;
-              while (nb_pref[k + 1] <= g) k++;
-              const int j = A.cell_atoms[nb_start[k] + (g - nb_pref[k])];
-              cidx[q] = j;
-              cpos[q] = A.pos[j];
-            }
-            __syncthreads();
-          }
-          for (int q0 = 0; q0 < tn; q0 += 32) {
-            const int q = q0 + ln;
-            bool ok = false;
-            int j = -1;
-            double rd = 0.0;
-            bool in_half = true;
-            if (act && q < tn) {
-              const int g = t0 + q;
-              j = cidx[q];
-              if (j != i) {
-                rd = rd_exact(S, xi, cpos[q]);
-                ok = rd < S.rlist2;
-              }
-              // the half list (linkedcell_selfhalf): the atoms after i in its
-              // own cell's chain, then the other 13 cells of the half stencil
-              if (S.half) in_half = g < own ? g > a : g < hend;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, ok);
-            if (ok) {
-              const int mm = m + __popc(bal & ((1u << ln) - 1u));
-              if (mm < A.lcap) {
-                row[mm] = in_half ? j : (int)((unsigned)j | 0x80000000u);  // bit 31: full list only
-                rrow[mm] = (float)rd;
-              }
-            }
-            m += __popc(bal);
-          }
-        }
-        __syncwarp();
-        if (act) list_row_out(A, S, s, i, m, row, rrow, ln);
-        __syncwarp();
-      }
-      __syncthreads();  // nb_* and the tile are rewritten for the next cell
-    }
+    if (A.sys[C.sys[b]].list_img)
+      list_cells_item<true>(A, C, b, part, cf, stage, stage_rd, nb_start, nb_pref, nb_sh, boff_sh[warp]);
+    else
+      list_cells_item<false>(A, C, b, part, cf, stage, stage_rd, nb_start, nb_pref, nb_sh, boff_sh[warp]);
   });
 }
 
-// The same lists for systems whose cells hold few atoms (Tersoff's 4 A
-// cells hold about three): one warp per cell, so no warp of a CTA idles.
-// Lanes 0..26 read the stencil cells' starts and counts and a warp scan
-// gives each cell's first candidate; a lane finds its candidate's stencil
-// cell by a binary search over the scan (shuffles) and stages id and
-// position in the warp's shared tile; the cell's atoms are then tested one
-// after another exactly as in k_list_cells.  Map: 8 cells per block (one per
-// warp).
-constexpr int LISTW_TILE = 128;  // candidates a warp stages at a time
+// The same lists one warp per cell, so no warp idles on cells of few atoms
+// and each SM keeps many cells' memory chains in flight (the CTA kernel
+// above keeps one per CTA).  Lanes 0..26 read the stencil cells' starts,
+// counts and shifts and a warp scan gives each cell's first candidate; the
+// warp stages the candidates' records in its shared tile in two passes (ids,
+// then positions, four loads in flight per lane), finding a candidate's
+// stencil cell by a binary search over the scan (shuffles); the cell's
+// atoms are then tested one after another exactly as in k_list_cells.
+// TILE = 128 for cells of about three atoms (Tersoff's 4 A cells), 512 for
+// cells of up to about sixteen (a cell with more candidates than TILE is
+// staged again for each atom).  Map: 8 cells per block (one per warp).
+template <int TILE>
+__host__ __device__ constexpr size_t listw_warp_bytes(int lcap) {
+  return (size_t)TILE * sizeof(float4) + (size_t)lcap * (sizeof(int) + sizeof(float)) + 16 * sizeof(int);
+}
+template <int TILE>
 __host__ __device__ constexpr size_t listw_smem(int lcap) {
-  return (size_t)(BLOCK / 32) * (LISTW_TILE * (sizeof(double4) + sizeof(int)) + (size_t)lcap * (sizeof(int) + sizeof(float)));
+  return (size_t)(BLOCK / 32) * listw_warp_bytes<TILE>(lcap);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_list_cells_w(Arena A, BlockMap C) {
-  extern __shared__ __align__(32) unsigned char listw_sh[];
+template <bool IMG, int TILE>
+__device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap& C, int b, float4* cf, int* boff,
+                                                  int* row, float* rrow) {
+  constexpr int U = 2;  // loads in flight per lane while staging
   const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
-  unsigned char* mine = listw_sh + (size_t)warp * (LISTW_TILE * (sizeof(double4) + sizeof(int)) +
-                                                   (size_t)A.lcap * (sizeof(int) + sizeof(float)));
-  double4* cpos = reinterpret_cast<double4*>(mine);
-  int* cidx = reinterpret_cast<int*>(cpos + LISTW_TILE);
-  int* row = cidx + LISTW_TILE;
-  float* rrow = reinterpret_cast<float*>(row + A.lcap);
-  rebuild_items(C.nblk, [&](int b) { return rebuild_block(A, C, b, true) && A.sys[C.sys[b]].list_warp; },
-                [&](int b) {
-    const int c = C.first[b] + warp;
-    if (c >= C.end[b]) return;  // warp-uniform
-    const int s = C.sys[b];
-    const SysDev& S = A.sys[s];
-    const int cl = c - S.cell_off;
-    const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
-    int cs = 0, cn = 0;
-    if (ln < NSTENCIL) {
-      int dx, dy, dz;
-      stencil(ln, dx, dy, dz);
-      const int x = (cx + dx + S.nc[0]) % S.nc[0];
-      const int y = (cy + dy + S.nc[1]) % S.nc[1];
-      const int z = (cz + dz + S.nc[2]) % S.nc[2];
-      const int cid = S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
-      cs = A.cell_start[cid];
-      cn = A.cell_n[cid];
-    }
-    int inc = cn;
+  const int c = C.first[b] + warp;
+  if (c >= C.end[b]) return;  // warp-uniform
+  const int s = C.sys[b];
+  const SysDev& S = A.sys[s];
+  const ListFrame f = list_frame(S);
+  const bool half = S.half != 0;
+  const int cl = c - S.cell_off;
+  const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
+  const double3 o = make_double3(cx * S.cell[0], cy * S.cell[1], cz * S.cell[2]);
+  int cs = 0, cn = 0;
+  double3 sh = make_double3(0, 0, 0);
+  if (ln < NSTENCIL) {
+    const int cid = stencil_cell(S, ln, cx, cy, cz, sh);
+    cs = A.cell_start[cid];
+    cn = A.cell_n[cid];
+  }
+  int inc = cn;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(FULL, inc, o);
-      if (ln >= o) inc += t;
-    }
-    const int ex = inc - cn;                          // first candidate of stencil cell ln
-    const int T = __shfl_sync(FULL, inc, NSTENCIL - 1);  // candidates of every atom of the cell
-    const int own = __shfl_sync(FULL, inc, 0);        // the cell itself: its atoms come first
-    const int hend = __shfl_sync(FULL, inc, 13);      // end of the half stencil's candidates
-    const int beg0 = __shfl_sync(FULL, cs, 0);
-    for (int a = 0; a < own; a++) {
-      const int i = A.cell_atoms[beg0 + a];
-      const double4 xi = A.pos[i];
-      int m = 0;
-      for (int t0 = 0; t0 < T; t0 += LISTW_TILE) {
-        const int tn = min(LISTW_TILE, T - t0);
-        if (T > LISTW_TILE || a == 0) {  // one tile stays staged for all the cell's atoms
-          __syncwarp();
-          for (int q0 = 0; q0 < tn; q0 += 32) {
-            const int q = q0 + ln;
-            const int g = t0 + q;
-            // the last stencil cell whose first candidate is <= g (an empty
-            // cell shares its first candidate with the next, non-empty one)
-            int k = 0;
+  for (int d = 1; d < 32; d <<= 1) {
+    const int t = __shfl_up_sync(FULL, inc, d);
+    if (ln >= d) inc += t;
+  }
+  const int ex = inc - cn;                             // first candidate of stencil cell ln
+  const int T = __shfl_sync(FULL, inc, NSTENCIL - 1);  // candidates of every atom of the cell
+  const int own = __shfl_sync(FULL, inc, 0);           // the cell itself: its atoms come first
+  const int hend = __shfl_sync(FULL, inc, 13);         // end of the half stencil's candidates
+  const int beg0 = __shfl_sync(FULL, cs, 0);
+  const bool one = T <= TILE;  // one tile stays staged for all the cell's atoms
+  auto stage_tile = [&](int t0, int tn) {
+    __syncwarp();
+    // pass 1: each candidate's stencil cell and atom id (into .x / .w)
+    for (int q0 = 0; q0 < tn; q0 += 32 * U) {
+      int jv[U], kv[U];
 #pragma unroll
-            for (int step = 16; step; step >>= 1) {
-              const int kk = min(k + step, NSTENCIL - 1);
-              const int e = __shfl_sync(FULL, ex, kk);
-              if (k + step < NSTENCIL && e <= g) k = kk;
-            }
-            const int st = __shfl_sync(FULL, cs, k), ek = __shfl_sync(FULL, ex, k);
-            if (q < tn) {
-              const int j = A.cell_atoms[st + (g - ek)];
-              cidx[q] = j;
-              cpos[q] = A.pos[j];
-            }
-          }
-          __syncwarp();
+      for (int u = 0; u < U; u++) {
+        const int q = q0 + 32 * u + ln;
+        const int g = t0 + q;
+        // the last stencil cell whose first candidate is <= g (an empty
+        // cell shares its first candidate with the next, non-empty one)
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step; step >>= 1) {
+          const int kk = min(k + step, NSTENCIL - 1);
+          const int e = __shfl_sync(FULL, ex, kk);
+          if (k + step < NSTENCIL && e <= g) k = kk;
         }
-        for (int q0 = 0; q0 < tn; q0 += 32) {
-          const int q = q0 + ln;
-          bool ok = false, in_half = true;
-          int j = -1;
-          double rd = 0.0;
-          if (q < tn) {
-            const int g = t0 + q;
-            j = cidx[q];
-            if (j != i) {
-              rd = rd_exact(S, xi, cpos[q]);
-              ok = rd < S.rlist2;
-            }
-            if (S.half) in_half = g < own ? g > a : g < hend;
-          }
-          const unsigned bal = __ballot_sync(FULL, ok);
-          if (ok) {
-            const int mm = m + __popc(bal & ((1u << ln) - 1u));
-            if (mm < A.lcap) {
-              row[mm] = in_half ? j : (int)((unsigned)j | 0x80000000u);
-              rrow[mm] = (float)rd;
-            }
-          }
-          m += __popc(bal);
-        }
+        const int st = __shfl_sync(FULL, cs, k), ek = __shfl_sync(FULL, ex, k);
+        kv[u] = k;
+        jv[u] = q < tn ? A.cell_atoms[st + (g - ek)] : -1;
       }
-      __syncwarp();
-      list_row_out(A, S, s, i, m, row, rrow, ln);
-      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int q = q0 + 32 * u + ln;
+        if (q < tn) cf[q] = make_float4(__int_as_float(kv[u]), 0.0f, 0.0f, __int_as_float(jv[u]));
+      }
     }
-  });
+    __syncwarp();
+    // pass 2: the records
+    for (int q0 = 0; q0 < tn; q0 += 32 * U) {
+      double4 p[U];
+      int jv[U], kv[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int q = q0 + 32 * u + ln;
+        const float4 e = q < tn ? cf[q] : make_float4(0, 0, 0, __int_as_float(-1));
+        kv[u] = __float_as_int(e.x);
+        jv[u] = __float_as_int(e.w);
+        if (jv[u] >= 0) p[u] = A.pos[jv[u]];
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int q = q0 + 32 * u + ln;
+        double3 shk = make_double3(0, 0, 0);
+        if (IMG)
+          shk = make_double3(__shfl_sync(FULL, sh.x, kv[u]), __shfl_sync(FULL, sh.y, kv[u]),
+                             __shfl_sync(FULL, sh.z, kv[u]));
+        if (q < tn) cf[q] = list_record<IMG>(f, p[u], jv[u], shk, o);
+      }
+    }
+    __syncwarp();
+  };
+  if (one) stage_tile(0, T);
+  for (int a = 0; a < own; a++) {
+    int m = 0, i;
+    float4 ri;
+    if (one) {
+      ri = cf[a];  // the home cell's atoms come first, with no shift
+      i = __float_as_int(ri.w);
+    } else {
+      i = A.cell_atoms[beg0 + a];
+      ri = list_record<IMG>(f, A.pos[i], i, make_double3(0, 0, 0), o);
+    }
+    for (int t0 = 0; t0 < T; t0 += TILE) {
+      const int tn = min(TILE, T - t0);
+      if (!one) stage_tile(t0, tn);
+      list_scan_tile<IMG>(A, S, f, cf, t0, tn, i, a, ri, half, own, hend, row, rrow, A.lcap, m, ln);
+    }
+    __syncwarp();
+    list_row_out(A, S, s, i, m, row, rrow, f.err, boff, ln);
+    __syncwarp();
+  }
+}
+
+template <int TILE, bool IMG>
+__global__ void __launch_bounds__(BLOCK) k_list_cells_w(Arena A, BlockMap C) {
+  extern __shared__ __align__(16) unsigned char listw_sh[];
+  const int warp = threadIdx.x >> 5;
+  unsigned char* mine = listw_sh + (size_t)warp * listw_warp_bytes<TILE>(A.lcap);
+  float4* cf = reinterpret_cast<float4*>(mine);
+  int* boff = reinterpret_cast<int*>(cf + TILE);
+  int* row = boff + 16;
+  float* rrow = reinterpret_cast<float*>(row + A.lcap);
+  constexpr int KIND = TILE == 128 ? 1 : 2;  // SysDev::list_warp of the systems this kernel builds
+  rebuild_items(C.nblk, [&](int b) {
+      if (!rebuild_block(A, C, b, true)) return false;
+      const SysDev& S = A.sys[C.sys[b]];
+      return S.list_warp == KIND && (S.list_img != 0) == IMG;
+    }, [&](int b) { list_cells_w_item<IMG, TILE>(A, C, b, cf, boff, row, rrow); });
 }
 
 // verlet_self / verlet_selfhalf (src/Neighbour.F90:676-811): O(N^2) over the
@@ -1183,11 +1360,12 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_rho_fp64(Arena A, BlockMap M) {
 //   tail     : factor = P P' (eb_i + eb_j) - 2 R'
 //   F_i -= factor * ev_ui * vd / r ;  e_i += repul ; e_i -= sqrt(rho_i)
 // The FP64 force pass for one thread's lane of atom i; lane 0 stores the
-// force and energy and returns the force in F.
+// force and energy and returns the force in F (STORE=false: stores
+// nothing and returns the energy in F.w, for the caller to store).
 // VIR: also the pair virial of the system (virial_close); SMA-TB forces are
 // central pair forces, F_i = -sum_j factor_ij vd / r, so W is the pair sum
 // (complete: the reference's TB.F90:548-564 omits the i-side term).
-template <int K, bool VIR>
+template <int K, bool VIR, bool STORE = true>
 __device__ __forceinline__ void force_fp64_body(Arena& A, const BlockMap& M, int s, const SysDev& S,
                                                 const SmFP64* tab, int i, int lane, bool act, double4& F) {
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
@@ -1240,9 +1418,14 @@ __device__ __forceinline__ void force_fp64_body(Arena& A, const BlockMap& M, int
   f2 = lane_sum<K>(f2);
   ep = lane_sum<K>(ep);
   if (act && lane == 0) {
-    F = make_double4(f0, f1, f2, 0.0);
-    A.force[i] = F;
-    A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
+    const double e = (ep - sqrt(A.band[i])) * EV_UI;
+    if constexpr (STORE) {
+      F = make_double4(f0, f1, f2, 0.0);
+      A.force[i] = F;
+      A.epot[i] = e;
+    } else {
+      F = make_double4(f0, f1, f2, e);
+    }
   }
   if constexpr (VIR) virial_close(A, M, s, w);
 }
@@ -1392,9 +1575,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
 }
 
 // The force pass for one thread's lane of atom i (K lanes per atom); lane 0
-// stores the force and energy and returns the force in F.
+// stores the force and energy and returns the force in F (STORE=false:
+// stores nothing and returns the energy in F.w, for the caller to store).
 // VIR: also the pair virial, FP32 per pair and group, FP64 per atom and system.
-template <int K, bool ONE, bool VIR>
+template <int K, bool ONE, bool VIR, bool STORE = true>
 __device__ __forceinline__ void force_mixed_body(Arena& A, const BlockMap& M, int s, const SysDev& S,
                                                  const SmF32* tab, int i, int lane, bool act, double4& F) {
   double f0 = 0, f1 = 0, f2 = 0, ep = 0;
@@ -1478,9 +1662,14 @@ __device__ __forceinline__ void force_mixed_body(Arena& A, const BlockMap& M, in
   f2 = lane_sum<K>(f2);
   ep = lane_sum<K>(ep);
   if (act && lane == 0) {
-    F = make_double4(f0, f1, f2, 0.0);
-    A.force[i] = F;
-    A.epot[i] = (ep - sqrt(A.band[i])) * EV_UI;
+    const double e = (ep - sqrt(A.band[i])) * EV_UI;
+    if constexpr (STORE) {
+      F = make_double4(f0, f1, f2, 0.0);
+      A.force[i] = F;
+      A.epot[i] = e;
+    } else {
+      F = make_double4(f0, f1, f2, e);
+    }
   }
   if constexpr (VIR) virial_close(A, M, s, w);
 }
@@ -2681,31 +2870,54 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
 }
 
 // Atom i's step_b of one step and step_a of the next (velocity Verlet or
-// Ermak; other integrators leave the atom alone) given its force F: the
-// operations of k_step_b and k_step_a in their order.  Returns the squared
-// displacement since the list build (1e-16 when the atom did not move).
-__device__ __forceinline__ double ba_atom(Arena& A, const SysDev& S, SysState& st, int i, const double4& F) {
+// Ermak; other integrators leave the atom alone) given its force F, in
+// registers: the operations of k_step_b and k_step_a in their order.
+// ba_store writes the result.  The fused kernels store after the system's
+// skin test, so the fence before a block's ticket waits on no atom stores.
+struct BaAtom {
+  double4 x, v, a, vv;
+  double d;  // squared displacement since the list build (1e-16: not moved)
+  int ty;
+  bool on;   // velocity Verlet or Ermak
+};
+
+__device__ __forceinline__ void ba_calc(const Arena& A, const SysDev& S, const SysState& st, int i, const double4& F,
+                                        BaAtom& b) {
   const int integ = S.integ;
-  if (integ != IT_VV && integ != IT_ERMAK) return 1.e-16;
-  // every input is loaded before the first store, so all loads are in flight together
-  double4 x = A.pos[i], v = A.vel[i], a = A.acel[i];
+  b.on = integ == IT_VV || integ == IT_ERMAK;
+  b.d = 1.e-16;
+  if (!b.on) return;
+  // every input is loaded before the first use, so all loads are in flight together
+  b.x = A.pos[i];
+  b.v = A.vel[i];
+  b.a = A.acel[i];
   const double2 mi = A.minv[i];
   const double4 xo = A.pos_old[i];
-  const int ty = A.type[i];
+  b.ty = A.type[i];
   const double4 vv0 = integ == IT_ERMAK ? A.vel_v[i] : make_double4(0, 0, 0, 0);
   if (integ == IT_VV) {
-    vv_b_atom(S.dt, mi.x, F, v, a);
-    vv_a_atom(S.dt, mi.x, F, x, v, a);
+    vv_b_atom(S.dt, mi.x, F, b.v, b.a);
+    vv_a_atom(S.dt, mi.x, F, b.x, b.v, b.a);
   } else {
-    ermak_b_atom(S, mi.x, F, vv0, v, a);
-    double4 vv;
-    ermak_a_atom(A, S, st, i, mi, v, a, x, vv);
-    A.vel_v[i] = vv;
+    ermak_b_atom(S, mi.x, F, vv0, b.v, b.a);
+    ermak_a_atom(A, S, st, i, mi, b.v, b.a, b.x, b.vv);
   }
-  A.acel[i] = a;
-  A.vel[i] = v;
-  wrap_atom(S, x);
-  return moved_atom(A, S, st, i, x, xo, ty);
+  wrap_atom(S, b.x);
+  b.d = disp2(S, b.x, xo);
+}
+
+__device__ __forceinline__ void ba_store(Arena& A, const SysDev& S, SysState& st, int i, const BaAtom& b) {
+  if (!b.on) return;
+  if (S.integ == IT_ERMAK) A.vel_v[i] = b.vv;
+  A.acel[i] = b.a;
+  A.vel[i] = b.v;
+  A.pos[i] = b.x;
+  if (S.prec == PREC_MIXED || S.ff == FF_TERSOFF) {
+    int bad = 0;
+    write_fx(A, S, i, b.x, b.ty, bad);
+    if (bad) atomicOr(&st.status, ST_LOST);
+  }
+  if (!(b.d == b.d)) atomicOr(&st.status, ST_NAN);
 }
 
 // step_b of one step fused with step_a of the next, for velocity Verlet and
@@ -2722,12 +2934,18 @@ __global__ void __launch_bounds__(BLOCK, 4) k_step_ba(Arena A, BlockMap M, cudaG
   int i = M.first[blockIdx.x] + threadIdx.x;
   bool act = i < M.end[blockIdx.x];
   double2 t = make_double2(1.e-16, 1.e-16);
-  if (act) t.x = ba_atom(A, S, st, i, A.force[i]);
+  BaAtom b;
+  b.on = false;
+  if (act) {
+    ba_calc(A, S, st, i, A.force[i], b);
+    t.x = b.d;
+  }
   skin_close<COND, false>(A, M, s, S, st, false, t, cond);
+  if (act) ba_store(A, S, st, i, b);
 }
 
 // The force pass fused with the integrator: each atom's force, then its
-// step_b and the next step's step_a (ba_atom), then the skin test of the
+// step_b and the next step's step_a (ba_calc), then the skin test of the
 // system.  The force pass reads the neighbours' positions from the density
 // pass's gather records (fxe, pose), never from pos / fxp, so moving an atom
 // while others still gather is safe; the next density pass starts after
@@ -2746,10 +2964,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed_ba(Arena A, B
   const int lane = threadIdx.x % K;
   const bool act = i < M.end[blockIdx.x];
   double4 F;
-  force_mixed_body<K, ONE, false>(A, M, s, S, tab, i, lane, act, F);
+  force_mixed_body<K, ONE, false, false>(A, M, s, S, tab, i, lane, act, F);
   double2 t = make_double2(1.e-16, 1.e-16);
-  if (act && lane == 0) t.x = ba_atom(A, S, st, i, F);
+  BaAtom b;
+  b.on = false;
+  if (act && lane == 0) {
+    ba_calc(A, S, st, i, make_double4(F.x, F.y, F.z, 0.0), b);
+    t.x = b.d;
+  }
   skin_close<COND, false>(A, M, s, S, st, false, t, cond);
+  if (act && lane == 0) {
+    A.force[i] = make_double4(F.x, F.y, F.z, 0.0);
+    A.epot[i] = F.w;
+    ba_store(A, S, st, i, b);
+  }
 }
 
 template <int K, bool COND>
@@ -2764,10 +2992,20 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64_ba(Arena A, BlockMap
   const int lane = threadIdx.x % K;
   const bool act = i < M.end[blockIdx.x];
   double4 F;
-  force_fp64_body<K, false>(A, M, s, S, tab, i, lane, act, F);
+  force_fp64_body<K, false, false>(A, M, s, S, tab, i, lane, act, F);
   double2 t = make_double2(1.e-16, 1.e-16);
-  if (act && lane == 0) t.x = ba_atom(A, S, st, i, F);
+  BaAtom b;
+  b.on = false;
+  if (act && lane == 0) {
+    ba_calc(A, S, st, i, make_double4(F.x, F.y, F.z, 0.0), b);
+    t.x = b.d;
+  }
   skin_close<COND, false>(A, M, s, S, st, false, t, cond);
+  if (act && lane == 0) {
+    A.force[i] = make_double4(F.x, F.y, F.z, 0.0);
+    A.epot[i] = F.w;
+    ba_store(A, S, st, i, b);
+  }
 }
 
 // integration_stepb (src/Integration.F90:264-301): velocity_verlet_b

@@ -43,9 +43,15 @@ def both(pos, mass, ctx, types=None, ntypes=1, setup=None):
     return o, g
 
 
-def compare_lists(o, g):
+def compare_lists(o, g, drop_self=False):
     no, lo = o.neighbour_list()
     ng, lg = g.neighbour_list()
+    if drop_self:  # leave out the reference's self entries (test_list_cells_thin_slab)
+        rows = [[j for j in lo[: no[i], i] if j != i] for i in range(len(no))]
+        no = np.array([len(r) for r in rows])
+        lo = np.zeros_like(lo)
+        for i, r in enumerate(rows):
+            lo[: len(r), i] = r
     np.testing.assert_array_equal(ng, no)
     m = int(no.max()) if len(no) else 0
     for k in range(m):
@@ -181,6 +187,69 @@ def test_list_boundary_ties(ctx):
         g.update()
         assert o.uses_cells()[0] == boxed
         compare_lists(o, g)
+
+
+@pytest.mark.parametrize("pbc", [(True, True, True), (True, True, False)])
+@pytest.mark.parametrize("half", [False, True])
+def test_list_cells_thin_slab(ctx, pbc, half):
+    """A slab one cell thick (6 x 5 x 1 cells): the stencil visits the one
+    z-cell three times, so a periodic slab lists a neighbour once per visit,
+    as the reference does; the lists equal the oracle's, entry by entry.
+    One deliberate difference: the reference's half-list loop
+    (linkedcell_selfhalf, src/Neighbour.F90:1117-1149) has no i /= j test, so
+    in a periodic slab one cell thick a half-stencil cell that wraps onto the
+    atom's own cell lists the atom as its own neighbour (at distance 0, which
+    the force loops would then evaluate).  The GPU lists never hold an atom
+    itself; the half-list comparison leaves those entries out.  (The stencil
+    wraps cells in every dim, periodic or not, as cell_pbc does, so the
+    slab's open z takes the same path.)"""
+    rng = np.random.default_rng(5)
+    L = (40.0, 33.0, 7.5)
+    pos = rng.random((600, 3)) * np.array(L)
+
+    def setup(s):
+        s.set_box(L, pbc)
+        s.set_smatb(0.2061, 1.79, 10.229, 4.036, 2.884, 4.4, 5.0)
+        s.set_half(half)
+
+    o, g = both(pos, 196.97, ctx, setup=setup)
+    o.update()
+    g.update()
+    assert o.uses_cells() == (True, (6, 5, 1))
+    compare_lists(o, g, drop_self=half)
+    g.destroy()
+
+
+def test_list_cells_pairs_at_rlist_large_box(ctx):
+    """Pairs 1e-12 relative inside and outside rlist, across the periodic
+    faces of a 400 A box in every direction: the cell lists keep exactly the
+    inside ones, as the oracle does."""
+    rl = 5.0 + 1.0
+    L = 400.0
+    rng = np.random.default_rng(17)
+    pts = []
+    for k in range(40):
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        a = rng.random(3) * L
+        d = k % 3  # near a face in dim d
+        a[d] = rng.random() * 3.0 + (0.1 if rng.random() < 0.5 else L - 3.1)
+        r = rl * (1.0 - 1e-12 if k % 2 == 0 else 1.0 + 1e-12)
+        pts += [a, np.mod(a + r * u, L)]
+    pos = np.array(pts)
+
+    def setup(s):
+        s.set_box((L, L, L), (True, True, True))
+        s.set_smatb(0.2061, 1.79, 10.229, 4.036, 2.884, 4.4, 5.0)
+
+    o, g = both(pos, 196.97, ctx, setup=setup)
+    o.update()
+    g.update()
+    assert o.uses_cells()[0]
+    no, _ = o.neighbour_list()
+    assert no.sum() == 40  # the 20 inside pairs, both ways
+    compare_lists(o, g)
+    g.destroy()
 
 
 def test_list_single_atom_and_cluster(ctx):
