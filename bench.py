@@ -95,6 +95,7 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.samples = []
+        self.mark = 0
         self.proc = None
         self.thread = None
 
@@ -109,6 +110,12 @@ class Clocks:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi takes a while to print its first line: wait for it, so
+        # that the samples kept (from here on) cover the timed region
+        t_end = time.time() + 5.0
+        while not self.samples and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.mark = len(self.samples)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -118,6 +125,11 @@ class Clocks:
 
     def stop(self):
         if self.proc:
+            # one more sample at the end of the timed region (100 ms period)
+            n = len(self.samples)
+            t_end = time.time() + 0.3
+            while len(self.samples) == n and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -125,6 +137,7 @@ class Clocks:
                 self.proc.kill()
         if self.thread:
             self.thread.join(timeout=5)
+        self.samples = self.samples[self.mark:] or self.samples[-1:]
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]

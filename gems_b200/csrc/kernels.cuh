@@ -1268,10 +1268,10 @@ constexpr int UNR = 4;
 
 // list slots m0, m0+K, ... (UNR of them) of atom i; slots past nn, and ids
 // outside the arena (never gather outside it), read as -1
-template <int K>
-__device__ __forceinline__ void list_group(const Arena& A, int i, int nn, int m0, int (&jj)[UNR]) {
+template <int K, int N>
+__device__ __forceinline__ void list_group(const Arena& A, int i, int nn, int m0, int (&jj)[N]) {
 #pragma unroll
-  for (int u = 0; u < UNR; u++) {
+  for (int u = 0; u < N; u++) {
     int m = m0 + u * K;
     int j = m < nn ? __ldg(&A.flist[(size_t)m * A.cap + i]) : -1;
     jj[u] = (unsigned)j < (unsigned)A.cap ? j : -1;
@@ -1496,8 +1496,12 @@ __device__ __forceinline__ float sqrt_nr(float r2, float& rinv) {
   return fmaf(0.5f * rinv, fmaf(-r, r, r2), r);
 }
 
-// Mixed kernels sum the FP32 pair terms of one UNR group in FP32 and add the
-// group sums to FP64 per-atom accumulators (one conversion per group).
+// Mixed kernels sum the FP32 pair terms of one group (UNR_R pairs in the
+// density pass, UNR_F in the force pass, whose pairs hold more registers)
+// in FP32 and add the group sums to FP64 per-atom accumulators (one
+// conversion per group).
+constexpr int UNR_R = 4;
+constexpr int UNR_F = 2;
 // ONE: single-species system, constants held in registers; otherwise the
 // species-pair table sits in shared memory and is read per pair.
 template <bool ONE>
@@ -1526,38 +1530,38 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
     const int4 xi = A.fxp[i];
     const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
-    int jn[UNR];
+    int jn[UNR_R];
     list_group<K>(A, i, nn, lane, jn);
-    for (int m0 = lane; m0 < nn; m0 += UNR * K) {
-      int jj[UNR];
+    for (int m0 = lane; m0 < nn; m0 += UNR_R * K) {
+      int jj[UNR_R];
 #pragma unroll
-      for (int u = 0; u < UNR; u++) jj[u] = jn[u];
-      int4 gj[UNR];
+      for (int u = 0; u < UNR_R; u++) jj[u] = jn[u];
+      int4 gj[UNR_R];
 #pragma unroll
-      for (int u = 0; u < UNR; u++)
+      for (int u = 0; u < UNR_R; u++) {
+        gj[u] = xi;  // an empty slot: a zero pair vector, masked below
         if (jj[u] >= 0) gj[u] = A.fxp[jj[u]];
-      list_group<K>(A, i, nn, m0 + UNR * K, jn);  // next group's ids, in flight meanwhile
+      }
+      list_group<K>(A, i, nn, m0 + UNR_R * K, jn);  // next group's ids, in flight meanwhile
       float grp = 0.0f;
+      // branch-free: both regimes are evaluated and selected, so the
+      // group's pairs interleave (a warp's lanes would run both anyway)
 #pragma unroll
-      for (int u = 0; u < UNR; u++) {
-        if (jj[u] < 0) continue;
+      for (int u = 0; u < UNR_R; u++) {
         const int4 xj = gj[u];
         const SmF32& c = ONE ? c1 : tab[xi.w * S.ntypes + xj.w];
         float v0, v1, v2;
         vd_fx(S, xi, xj, v0, v1, v2);
-        float r2 = v0 * v0 + v1 * v1 + v2 * v2;
-        if (r2 > c.rce2) continue;
+        const float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+        const bool ok = jj[u] >= 0 && !(r2 > c.rce2);
         float rinv;
-        float dr = sqrt_nr(r2, rinv);
-        float banda;
-        if (dr < c.rci) {
-          banda = c.eps2 * ex2f(c.kq * (c.r0 - dr));
-        } else {
-          float d = dr - c.rce, d2 = d * d, d3 = d2 * d;
-          banda = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
-          banda = banda * banda;
-        }
-        grp += banda;
+        const float dr = sqrt_nr(ok ? r2 : c.rce2, rinv);
+        const float bin = c.eps2 * ex2f(c.kq * (c.r0 - dr));
+        const float d = dr - c.rce, d2 = d * d, d3 = d2 * d;
+        float bt = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+        bt = bt * bt;
+        const float banda = dr < c.rci ? bin : bt;
+        grp += ok ? banda : 0.0f;
       }
       band += (double)grp;
     }
@@ -1590,51 +1594,50 @@ __device__ __forceinline__ void force_mixed_body(Arena& A, const BlockMap& M, in
     const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
     const float evui = (float)EV_UI;
     const int ti = xi.w;
-    int jn[UNR];
+    int jn[UNR_F];
     list_group<K>(A, i, nn, lane, jn);
-    for (int m0 = lane; m0 < nn; m0 += UNR * K) {
-      int jj[UNR];
+    for (int m0 = lane; m0 < nn; m0 += UNR_F * K) {
+      int jj[UNR_F];
 #pragma unroll
-      for (int u = 0; u < UNR; u++) jj[u] = jn[u];
-      int4 gj[UNR];
-      int tj[UNR];
+      for (int u = 0; u < UNR_F; u++) jj[u] = jn[u];
+      int4 gj[UNR_F];
+      int tj[UNR_F];
 #pragma unroll
-      for (int u = 0; u < UNR; u++)
+      for (int u = 0; u < UNR_F; u++) {
+        gj[u] = make_int4(xi.x, xi.y, xi.z, 0);  // an empty slot: a zero pair vector, masked below
+        tj[u] = 0;
         if (jj[u] >= 0) {
           gj[u] = A.fxe[jj[u]];
           if (!ONE) tj[u] = A.type[jj[u]];
         }
-      list_group<K>(A, i, nn, m0 + UNR * K, jn);  // next group's ids, in flight meanwhile
+      }
+      list_group<K>(A, i, nn, m0 + UNR_F * K, jn);  // next group's ids, in flight meanwhile
       float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, ge = 0.0f;
       float gw[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+      // branch-free: both regimes are evaluated and selected, so the
+      // group's pairs interleave (a warp's lanes would run both anyway)
 #pragma unroll
-      for (int u = 0; u < UNR; u++) {
-        if (jj[u] < 0) continue;
+      for (int u = 0; u < UNR_F; u++) {
         const int4 xj = gj[u];
         const SmF32& c = ONE ? c1 : tab[ti * S.ntypes + tj[u]];
         float v0, v1, v2;
         vd_fx(S, xi, xj, v0, v1, v2);
-        float r2 = v0 * v0 + v1 * v1 + v2 * v2;
-        if (r2 > c.rce2) continue;
+        const float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+        const bool ok = jj[u] >= 0 && !(r2 > c.rce2);
         float rinv;
-        float dr = sqrt_nr(r2, rinv);
-        float ebs = ebi + __int_as_float(xj.w);
-        float factor, repul;
-        if (dr <= c.rci) {
-          float x = c.r0 - dr;
-          float e1 = ex2f(c.kp * x);
-          float e2 = ex2f(c.kq * x);
-          repul = c.A * e1;
-          factor = c.c1 * e1 - c.c2 * e2 * ebs;
-        } else {
-          float d = dr - c.rce, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
-          float P = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
-          float dP = 5.0f * c.b1 * d4 + 4.0f * c.b2 * d3 + 3.0f * c.b3 * d2;
-          float dR = 5.0f * c.r1 * d4 + 4.0f * c.r2 * d3 + 3.0f * c.r3 * d2;
-          factor = P * dP * ebs - 2.0f * dR;
-          repul = (c.r1 * d2 + c.r2 * d + c.r3) * d3;
-        }
-        float fr = factor * evui * rinv;
+        const float dr = sqrt_nr(ok ? r2 : c.rce2, rinv);
+        const float ebs = ebi + __int_as_float(xj.w);
+        const float x = c.r0 - dr;
+        const float e1 = ex2f(c.kp * x);
+        const float e2 = ex2f(c.kq * x);
+        const float d = dr - c.rce, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
+        const float P = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+        const float dP = 5.0f * c.b1 * d4 + 4.0f * c.b2 * d3 + 3.0f * c.b3 * d2;
+        const float dR = 5.0f * c.r1 * d4 + 4.0f * c.r2 * d3 + 3.0f * c.r3 * d2;
+        const bool inner = dr <= c.rci;
+        const float factor = inner ? c.c1 * e1 - c.c2 * e2 * ebs : P * dP * ebs - 2.0f * dR;
+        const float repul = ok ? (inner ? c.A * e1 : (c.r1 * d2 + c.r2 * d + c.r3) * d3) : 0.0f;
+        const float fr = ok ? factor * evui * rinv : 0.0f;
         g0 = fmaf(fr, v0, g0);
         g1 = fmaf(fr, v1, g1);
         g2 = fmaf(fr, v2, g2);
