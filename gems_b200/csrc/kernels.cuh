@@ -230,14 +230,47 @@ __device__ __forceinline__ double2 sys_top2(const Arena& A, const BlockMap& M, i
 }
 
 // ------------------------------------------------------------------ skin test
-// Per-block top-2 of |pos - pos_old|^2; the last block of each system
-// decides rebuild = sqrt(d1) + sqrt(d2) > nb_dcut (test_update).
+// The system's two largest squared displacements (test_update,
+// src/Neighbour.F90:1305-1346), one warp at a time, with no block barrier:
+// every warp of the system's blocks calls this once per launch with its
+// lanes' top-2.  The warp's pair enters the system's through two atomic
+// maxima of the bit patterns (ordered as the non-negative doubles are):
+// atomicMax on top1 returns the previous maximum, and the smaller of that
+// and the warp's maximum is a candidate for second place, as is the warp's
+// own second value; every value but the final maximum is so offered to
+// top2, which ends as the system's second largest.  A ticket counts the
+// system's warps; in lane 0 of the last one the function returns true with
+// the system's pair in top, having reset the pair and the ticket for the
+// next launch.
+__device__ __forceinline__ bool warp_top2_close(SysState& st, const BlockMap& M, int s, double2 t, double2& top) {
+  const unsigned FULL = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    double2 w;
+    w.x = __shfl_xor_sync(FULL, t.x, o);
+    w.y = __shfl_xor_sync(FULL, t.y, o);
+    t = top2_merge(t, w);
+  }
+  if ((threadIdx.x & 31) != 0) return false;
+  const unsigned long long b1 = (unsigned long long)__double_as_longlong(t.x);
+  const unsigned long long b2 = (unsigned long long)__double_as_longlong(t.y);
+  const unsigned long long old = atomicMax(&st.top1, b1);
+  atomicMax(&st.top2, max(b2, min(old, b1)));
+  __threadfence();  // the maxima before the ticket
+  if (atomicAdd(&st.wticket, 1) != M.sys_nblk[s] * (BLOCK / 32) - 1) return false;
+  __threadfence();
+  top.x = __longlong_as_double((long long)atomicExch(&st.top1, 0ull));
+  top.y = __longlong_as_double((long long)atomicExch(&st.top2, 0ull));
+  st.wticket = 0;
+  return true;
+}
+
+// decides rebuild = sqrt(d1) + sqrt(d2) > nb_dcut for the system
 __device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, int s,
                                            double2 t) {
-  if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
-  if (last_block(M, A.st, s, &A.st[s].ticket) && threadIdx.x < 32) {
-    double2 v = sys_top2(A, M, s);
-    if (threadIdx.x == 0) {
+  double2 v;
+  if (warp_top2_close(A.st[s], M, s, t, v)) {
+    {
       const SysDev& S = A.sys[s];
       SysState& st = A.st[s];
       double box = 0.0;
@@ -258,7 +291,6 @@ __global__ void k_skin(Arena A, BlockMap M) {
   int i = M.first[blockIdx.x] + threadIdx.x;
   double2 t = make_double2(1.e-16, 1.e-16);
   if (i < M.end[blockIdx.x]) t.x = disp2(A.sys[s], A.pos[i], A.pos_old[i]);
-  t = block_top2(t);
   skin_finish(A, M, s, t);
 }
 
@@ -1451,6 +1483,9 @@ struct SmF32 {
   float A, eps2, c1, c2;
   float rci, rce, rci2, rce2;
   float b1, b2, b3, r1, r2, r3;
+  // the force pass's constants with the unit ev_ui folded in: c1, c2; the
+  // tail derivatives' coefficients 5 b1, 4 b2, 3 b3 and 2 (5 r1, 4 r2, 3 r3)
+  float c1e, c2e, dp5, dp4, dp3, dr5, dr4, dr3;
 };
 __device__ __forceinline__ SmF32 smf_load(const PairP& P) {
   const double log2e = 1.4426950408889634;
@@ -1469,6 +1504,11 @@ __device__ __forceinline__ SmF32 smf_load(const PairP& P) {
   c.rce2 = (float)(P.v[6] * P.v[6]);
   c.b1 = (float)P.v[7]; c.b2 = (float)P.v[8]; c.b3 = (float)P.v[9];
   c.r1 = (float)P.v[10]; c.r2 = (float)P.v[11]; c.r3 = (float)P.v[12];
+  const double e = EV_UI;
+  c.c1e = (float)(2.0 * A * p / r0 * e);
+  c.c2e = (float)(xi * xi * q / r0 * e);
+  c.dp5 = (float)(5.0 * P.v[7] * e); c.dp4 = (float)(4.0 * P.v[8] * e); c.dp3 = (float)(3.0 * P.v[9] * e);
+  c.dr5 = (float)(10.0 * P.v[10] * e); c.dr4 = (float)(8.0 * P.v[11] * e); c.dr3 = (float)(6.0 * P.v[12] * e);
   return c;
 }
 
@@ -1557,8 +1597,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_rho_mixed(Arena A, BlockM
         float rinv;
         const float dr = sqrt_nr(ok ? r2 : c.rce2, rinv);
         const float bin = c.eps2 * ex2f(c.kq * (c.r0 - dr));
-        const float d = dr - c.rce, d2 = d * d, d3 = d2 * d;
-        float bt = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
+        const float d = dr - c.rce, d3 = d * d * d;
+        float bt = fmaf(fmaf(c.b1, d, c.b2), d, c.b3) * d3;
         bt = bt * bt;
         const float banda = dr < c.rci ? bin : bt;
         grp += ok ? banda : 0.0f;
@@ -1592,7 +1632,6 @@ __device__ __forceinline__ void force_mixed_body(Arena& A, const BlockMap& M, in
     const float ebi = A.ebandf[i];
     const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const SmF32 c1 = ONE ? smf_load(A.prm[S.param_off]) : SmF32{};
-    const float evui = (float)EV_UI;
     const int ti = xi.w;
     int jn[UNR_F];
     list_group<K>(A, i, nn, lane, jn);
@@ -1630,14 +1669,15 @@ __device__ __forceinline__ void force_mixed_body(Arena& A, const BlockMap& M, in
         const float x = c.r0 - dr;
         const float e1 = ex2f(c.kp * x);
         const float e2 = ex2f(c.kq * x);
-        const float d = dr - c.rce, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
-        const float P = (c.b1 * d2 + c.b2 * d + c.b3) * d3;
-        const float dP = 5.0f * c.b1 * d4 + 4.0f * c.b2 * d3 + 3.0f * c.b3 * d2;
-        const float dR = 5.0f * c.r1 * d4 + 4.0f * c.r2 * d3 + 3.0f * c.r3 * d2;
+        // the tail polynomials in Horner form; factor carries ev_ui
+        const float d = dr - c.rce, d2 = d * d, d3 = d2 * d;
+        const float P = fmaf(fmaf(c.b1, d, c.b2), d, c.b3) * d3;
+        const float dPe = fmaf(fmaf(c.dp5, d, c.dp4), d, c.dp3) * d2;  // ev_ui P'
+        const float dRe = fmaf(fmaf(c.dr5, d, c.dr4), d, c.dr3) * d2;  // 2 ev_ui R'
         const bool inner = dr <= c.rci;
-        const float factor = inner ? c.c1 * e1 - c.c2 * e2 * ebs : P * dP * ebs - 2.0f * dR;
-        const float repul = ok ? (inner ? c.A * e1 : (c.r1 * d2 + c.r2 * d + c.r3) * d3) : 0.0f;
-        const float fr = ok ? factor * evui * rinv : 0.0f;
+        const float factor = inner ? c.c1e * e1 - c.c2e * e2 * ebs : P * dPe * ebs - dRe;
+        const float repul = ok ? (inner ? c.A * e1 : fmaf(fmaf(c.r1, d, c.r2), d, c.r3) * d3) : 0.0f;
+        const float fr = ok ? factor * rinv : 0.0f;
         g0 = fmaf(fr, v0, g0);
         g1 = fmaf(fr, v1, g1);
         g2 = fmaf(fr, v2, g2);
@@ -2776,11 +2816,9 @@ __device__ __forceinline__ double moved_atom(Arena& A, const SysDev& S, SysState
 template <bool COND, bool PISTON = true>
 __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, const SysDev& S, SysState& st,
                                            bool frozen, double2 t, cudaGraphConditionalHandle cond) {
-  t = block_top2(t);
-  if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
-  if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
-    double2 w = sys_top2(A, M, s);
-    if (threadIdx.x == 0) {
+  double2 w;
+  if (warp_top2_close(st, M, s, t, w)) {
+    {
       // a moving box (constant pressure) shifts periodic images by up to
       // the change of its lengths since the build, on top of the atoms'
       // own displacements
