@@ -178,10 +178,6 @@ struct SysState {
   double lkd_bo[3], lkd_bh[3], lkd_bf[3];
   double th_factor;  // scalvel: this step's velocity factor
   double th_vcm[3];  // scalvel: this step's centre-of-mass velocity
-  // the skin test's running top-2 of squared displacements (bit patterns of
-  // the non-negative doubles) and its warp ticket; 0 between launches
-  unsigned long long top1, top2;
-  int wticket, pad6;
 };
 
 // Block map: block b covers atoms [first[b], end[b]) of system sys[b];

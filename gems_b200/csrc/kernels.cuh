@@ -230,47 +230,14 @@ __device__ __forceinline__ double2 sys_top2(const Arena& A, const BlockMap& M, i
 }
 
 // ------------------------------------------------------------------ skin test
-// The system's two largest squared displacements (test_update,
-// src/Neighbour.F90:1305-1346), one warp at a time, with no block barrier:
-// every warp of the system's blocks calls this once per launch with its
-// lanes' top-2.  The warp's pair enters the system's through two atomic
-// maxima of the bit patterns (ordered as the non-negative doubles are):
-// atomicMax on top1 returns the previous maximum, and the smaller of that
-// and the warp's maximum is a candidate for second place, as is the warp's
-// own second value; every value but the final maximum is so offered to
-// top2, which ends as the system's second largest.  A ticket counts the
-// system's warps; in lane 0 of the last one the function returns true with
-// the system's pair in top, having reset the pair and the ticket for the
-// next launch.
-__device__ __forceinline__ bool warp_top2_close(SysState& st, const BlockMap& M, int s, double2 t, double2& top) {
-  const unsigned FULL = 0xffffffffu;
-#pragma unroll
-  for (int o = 16; o; o >>= 1) {
-    double2 w;
-    w.x = __shfl_xor_sync(FULL, t.x, o);
-    w.y = __shfl_xor_sync(FULL, t.y, o);
-    t = top2_merge(t, w);
-  }
-  if ((threadIdx.x & 31) != 0) return false;
-  const unsigned long long b1 = (unsigned long long)__double_as_longlong(t.x);
-  const unsigned long long b2 = (unsigned long long)__double_as_longlong(t.y);
-  const unsigned long long old = atomicMax(&st.top1, b1);
-  atomicMax(&st.top2, max(b2, min(old, b1)));
-  __threadfence();  // the maxima before the ticket
-  if (atomicAdd(&st.wticket, 1) != M.sys_nblk[s] * (BLOCK / 32) - 1) return false;
-  __threadfence();
-  top.x = __longlong_as_double((long long)atomicExch(&st.top1, 0ull));
-  top.y = __longlong_as_double((long long)atomicExch(&st.top2, 0ull));
-  st.wticket = 0;
-  return true;
-}
-
-// decides rebuild = sqrt(d1) + sqrt(d2) > nb_dcut for the system
+// Per-block top-2 of |pos - pos_old|^2; the last block of each system
+// decides rebuild = sqrt(d1) + sqrt(d2) > nb_dcut (test_update).
 __device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, int s,
                                            double2 t) {
-  double2 v;
-  if (warp_top2_close(A.st[s], M, s, t, v)) {
-    {
+  if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
+  if (last_block(M, A.st, s, &A.st[s].ticket) && threadIdx.x < 32) {
+    double2 v = sys_top2(A, M, s);
+    if (threadIdx.x == 0) {
       const SysDev& S = A.sys[s];
       SysState& st = A.st[s];
       double box = 0.0;
@@ -291,6 +258,7 @@ __global__ void k_skin(Arena A, BlockMap M) {
   int i = M.first[blockIdx.x] + threadIdx.x;
   double2 t = make_double2(1.e-16, 1.e-16);
   if (i < M.end[blockIdx.x]) t.x = disp2(A.sys[s], A.pos[i], A.pos_old[i]);
+  t = block_top2(t);
   skin_finish(A, M, s, t);
 }
 
@@ -2816,9 +2784,11 @@ __device__ __forceinline__ double moved_atom(Arena& A, const SysDev& S, SysState
 template <bool COND, bool PISTON = true>
 __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, const SysDev& S, SysState& st,
                                            bool frozen, double2 t, cudaGraphConditionalHandle cond) {
-  double2 w;
-  if (warp_top2_close(st, M, s, t, w)) {
-    {
+  t = block_top2(t);
+  if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
+  if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
+    double2 w = sys_top2(A, M, s);
+    if (threadIdx.x == 0) {
       // a moving box (constant pressure) shifts periodic images by up to
       // the change of its lengths since the build, on top of the atoms'
       // own displacements
