@@ -466,10 +466,12 @@ __global__ void k_sort_cells(Arena A, BlockMap C) {
 // entries.  A half list with the reaction added to j gives every atom the
 // same force, density and energy as the full list (src/TB.F90:432-441,
 // 542-552; src/Pairs.F90:248-252), so the force kernels need no half form.
-__device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m, int mh) {
+// (the cell-list kernels store pos_old while they stage the home cell's
+// atoms, whose positions they load anyway; the O(N^2) kernel here)
+__device__ __forceinline__ void list_done(const Arena& A, int s, int i, int m, int mh, bool pos_old) {
   A.nn[i] = m;
   A.hnn[i] = mh;
-  A.pos_old[i] = A.pos[i];
+  if (pos_old) A.pos_old[i] = A.pos[i];
   if (m > A.lcap) atomicOr(&A.st[s].status, ST_OVERFLOW);
   atomicMax(&A.st[s].maxnn, m);
 }
@@ -573,7 +575,7 @@ __device__ __forceinline__ void list_row_out(const Arena& A, const SysDev& S, in
     mh += __popc(hb);
   }
   list_force_order(A, S, i, n, row, rrow, err, boff, ln);
-  if (ln == 0) list_done(A, s, i, m, mh);
+  if (ln == 0) list_done(A, s, i, m, mh, false);
 }
 
 // ---- the candidate test of the cell-list builds
@@ -805,7 +807,9 @@ __device__ __forceinline__ void list_cells_item(const Arena& A, const BlockMap& 
         for (int step = 16; step; step >>= 1)
           if (k + step < NSTENCIL && nb_pref[k + step] <= g) k += step;
         const int j = A.cell_atoms[nb_start[k] + (g - nb_pref[k])];
-        cf[q] = list_record<IMG>(f, A.pos[j], j, nb_sh[k], o);
+        const double4 p = A.pos[j];
+        cf[q] = list_record<IMG>(f, p, j, nb_sh[k], o);
+        if (g < own) A.pos_old[j] = p;  // the home cell's atoms: the list's reference positions
       }
     };
     const bool one = T <= LIST_TILE;  // one tile stays staged for all this CTA's passes
@@ -978,7 +982,10 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
         if (IMG)
           shk = make_double3(__shfl_sync(FULL, sh.x, kv[u]), __shfl_sync(FULL, sh.y, kv[u]),
                              __shfl_sync(FULL, sh.z, kv[u]));
-        if (q < tn) cf[q] = list_record<IMG>(f, p[u], jv[u], shk, o);
+        if (q < tn) {
+          cf[q] = list_record<IMG>(f, p[u], jv[u], shk, o);
+          if (t0 + q < own) A.pos_old[jv[u]] = p[u];  // the home cell's atoms: the list's reference positions
+        }
       }
     }
     __syncwarp();
@@ -1006,7 +1013,7 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
 }
 
 template <int TILE, bool IMG>
-__global__ void __launch_bounds__(BLOCK) k_list_cells_w(Arena A, BlockMap C) {
+__global__ void __launch_bounds__(BLOCK, TILE == 128 ? 3 : 1) k_list_cells_w(Arena A, BlockMap C) {
   extern __shared__ __align__(16) unsigned char listw_sh[];
   const int warp = threadIdx.x >> 5;
   unsigned char* mine = listw_sh + (size_t)warp * listw_warp_bytes<TILE>(A.lcap);
@@ -1058,7 +1065,7 @@ __global__ void k_list_n2(Arena A, BlockMap M) {
         }
       }
     }
-    if (act) list_done(A, s, i, m, mh);
+    if (act) list_done(A, s, i, m, mh, true);
     __syncthreads();  // the tile is reused by the next block
   });
 }
@@ -2236,11 +2243,15 @@ __global__ void k_tsf_rslot(Arena A, BlockMap M) {
         int r = 255;
         if ((unsigned)j < (unsigned)A.cap) {
           const int nj = min(min(A.nn[j], A.lcap), 255);
-          for (int k = 0; k < nj; k++)
-            if (A.flist[(size_t)k * A.cap + j] == i) {
-              r = k;
-              break;
-            }
+          // the first slot of j's list that holds i, four loads in flight at a time
+          for (int k0 = 0; k0 < nj && r == 255; k0 += 4) {
+            int v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) v[u] = k0 + u < nj ? A.flist[(size_t)(k0 + u) * A.cap + j] : -1;
+#pragma unroll
+            for (int u = 3; u >= 0; u--)
+              if (v[u] == i) r = k0 + u;
+          }
         }
         A.rslot[e] = (unsigned char)r;
       }
