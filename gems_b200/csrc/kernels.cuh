@@ -1012,8 +1012,10 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
   }
 }
 
+// register bounds measured best: three blocks per SM for the 128 tile, two
+// for the 512 tile (its 72 KB of tiles fit three; more registers win)
 template <int TILE, bool IMG>
-__global__ void __launch_bounds__(BLOCK, TILE == 128 ? 3 : 1) k_list_cells_w(Arena A, BlockMap C) {
+__global__ void __launch_bounds__(BLOCK, TILE == 128 ? 3 : 2) k_list_cells_w(Arena A, BlockMap C) {
   extern __shared__ __align__(16) unsigned char listw_sh[];
   const int warp = threadIdx.x >> 5;
   unsigned char* mine = listw_sh + (size_t)warp * listw_warp_bytes<TILE>(A.lcap);
