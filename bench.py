@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--replicas", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--arms", default="fp64,mixed,batched",
-                    help="comma list of arms to run (profiling); the full line needs all three")
+                    help="comma list of arms to run (profiling; 'rebuild' times the batch's list "
+                         "rebuild alone); the full line needs fp64,mixed,batched")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--therm-steps", type=int, default=None,
                     help="reference arm: untimed Ermak steps before timing (default: the GPU arms' %d)"
@@ -865,7 +866,7 @@ def run_next(args, gems, torch, ctx, ext):
     cl = [W.cluster(147, rng, jitter=0.15) + 200.0 for _ in range(256)]
     mass = W.smatb_bulk(ncell=2)["mass"]
     warm = []
-    for _ in range(16):  # warm-up batch: workspace, maps and kernels loaded
+    for _ in range(256):  # warm-up batch of the same size: workspace, maps and kernels loaded
         g = gems.System(W.cluster(147, rng, jitter=0.15) + 200.0, mass, ctx=ctx)
         g.set_smatb(*sm)
         warm.append(g)
@@ -1007,6 +1008,20 @@ def main():
             ts, nl = timed_blocks(ctx, torch, ss, blk, args.steps, args.warmup, flush, ext)
             out[name] = {"atom_steps_per_s": sum(x.n for x in ss) * blk * len(ts) / (sum(ts) * 1e-3),
                          "launches": nl}
+            for s_ in ss:
+                s_.destroy()
+        if "rebuild" in want:
+            # the list rebuild of the batch on its own (for ncu): replicas of the
+            # lattice displaced by N(0, 0.1 A), one list build each, then three
+            # forced rebuilds of all of them together
+            ss = []
+            for k in range(args.replicas):
+                wk = c2_replica(100 + k)
+                wk["pos"] = np.mod(wk["pos"] + np.random.default_rng(k).normal(0.0, 0.1, wk["pos"].shape),
+                                   np.asarray(wk["L"], dtype=np.float64))
+                ss.append(make_system(gems, ctx, wk, gems.PREC_MIXED, seed=100 + k, tune=(1, 2), therm=0))
+            kb = ctx.batch_time_kernels(ss, 3)
+            out["rebuild"] = {"atoms": sum(x.n for x in ss), "rebuild_ms": float(kb[2])}
             for s_ in ss:
                 s_.destroy()
         print(json.dumps({"profile_arms": out}), flush=True)
