@@ -2896,8 +2896,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_a(Arena A, BlockMap M, cudaGraph
 // Atom i's step_b of one step and step_a of the next (velocity Verlet or
 // Ermak; other integrators leave the atom alone) given its force F, in
 // registers: the operations of k_step_b and k_step_a in their order.
-// ba_store writes the result.  The fused kernels store after the system's
-// skin test, so the fence before a block's ticket waits on no atom stores.
+// ba_store writes the result.
 struct BaAtom {
   double4 x, v, a, vv;
   double d;  // squared displacement since the list build (1e-16: not moved)
@@ -2963,9 +2962,9 @@ __global__ void __launch_bounds__(BLOCK, 4) k_step_ba(Arena A, BlockMap M, cudaG
   if (act) {
     ba_calc(A, S, st, i, A.force[i], b);
     t.x = b.d;
+    ba_store(A, S, st, i, b);
   }
   skin_close<COND, false>(A, M, s, S, st, false, t, cond);
-  if (act) ba_store(A, S, st, i, b);
 }
 
 // The force pass fused with the integrator: each atom's force, then its
@@ -2993,15 +2992,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_smatb_force_mixed_ba(Arena A, B
   BaAtom b;
   b.on = false;
   if (act && lane == 0) {
-    ba_calc(A, S, st, i, make_double4(F.x, F.y, F.z, 0.0), b);
-    t.x = b.d;
-  }
-  skin_close<COND, false>(A, M, s, S, st, false, t, cond);
-  if (act && lane == 0) {
     A.force[i] = make_double4(F.x, F.y, F.z, 0.0);
     A.epot[i] = F.w;
+    ba_calc(A, S, st, i, make_double4(F.x, F.y, F.z, 0.0), b);
+    t.x = b.d;
     ba_store(A, S, st, i, b);
   }
+  skin_close<COND, false>(A, M, s, S, st, false, t, cond);
 }
 
 template <int K, bool COND>
@@ -3021,15 +3018,13 @@ __global__ void __launch_bounds__(BLOCK) k_smatb_force_fp64_ba(Arena A, BlockMap
   BaAtom b;
   b.on = false;
   if (act && lane == 0) {
-    ba_calc(A, S, st, i, make_double4(F.x, F.y, F.z, 0.0), b);
-    t.x = b.d;
-  }
-  skin_close<COND, false>(A, M, s, S, st, false, t, cond);
-  if (act && lane == 0) {
     A.force[i] = make_double4(F.x, F.y, F.z, 0.0);
     A.epot[i] = F.w;
+    ba_calc(A, S, st, i, make_double4(F.x, F.y, F.z, 0.0), b);
+    t.x = b.d;
     ba_store(A, S, st, i, b);
   }
+  skin_close<COND, false>(A, M, s, S, st, false, t, cond);
 }
 
 // integration_stepb (src/Integration.F90:264-301): velocity_verlet_b
