@@ -680,15 +680,33 @@ __device__ __forceinline__ float4 list_record(const ListFrame& f, double4 p, int
   return list_coords(f, p, j);
 }
 
+// a / b for 0 <= a < 2^31, b >= 1 by a double reciprocal and one
+// correction (the estimate is off by one at most)
+__device__ __forceinline__ int div_small(int a, int b) {
+  int q = (int)((double)a * __drcp_rn((double)b));
+  const int r = a - q * b;
+  q += (r >= b) - (r < 0);
+  return q;
+}
+
+// the grid coordinates of a system's cell cl (x fastest)
+__device__ __forceinline__ void cell_xyz(const SysDev& S, int cl, int& cx, int& cy, int& cz) {
+  const int yz = div_small(cl, S.nc[0]);
+  cx = cl - yz * S.nc[0];
+  cz = div_small(yz, S.nc[1]);
+  cy = yz - cz * S.nc[1];
+}
+
 // stencil cell k of home cell (cx, cy, cz): its id and the periodic shift
 // that takes its atoms to the image next to the home cell (open dims: none)
 __device__ __forceinline__ int stencil_cell(const SysDev& S, int k, int cx, int cy, int cz, double3& sh) {
   int dx, dy, dz;
   stencil(k, dx, dy, dz);
   const int ux = cx + dx, uy = cy + dy, uz = cz + dz;
-  const int x = (ux + S.nc[0]) % S.nc[0];
-  const int y = (uy + S.nc[1]) % S.nc[1];
-  const int z = (uz + S.nc[2]) % S.nc[2];
+  // ux is in [-1, nc]: one wrap at most
+  const int x = ux < 0 ? ux + S.nc[0] : ux >= S.nc[0] ? ux - S.nc[0] : ux;
+  const int y = uy < 0 ? uy + S.nc[1] : uy >= S.nc[1] ? uy - S.nc[1] : uy;
+  const int z = uz < 0 ? uz + S.nc[2] : uz >= S.nc[2] ? uz - S.nc[2] : uz;
   sh = make_double3(S.pbc[0] ? (ux - x) * S.cell[0] : 0.0, S.pbc[1] ? (uy - y) * S.cell[1] : 0.0,
                     S.pbc[2] ? (uz - z) * S.cell[2] : 0.0);
   return S.cell_off + x + S.nc[0] * (y + S.nc[1] * z);
@@ -772,7 +790,8 @@ __device__ __forceinline__ void list_cells_item(const Arena& A, const BlockMap& 
     const int a_first = part * LIST_ATOMS;
     if (a_first >= cnt0) continue;  // uniform per CTA
     const int cl = c - S.cell_off;
-    const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
+    int cx, cy, cz;
+    cell_xyz(S, cl, cx, cy, cz);
     const double3 o = make_double3(cx * S.cell[0], cy * S.cell[1], cz * S.cell[2]);
     if (warp == 0) {  // the stencil cells' starts, shifts and first candidates (a warp scan)
       int cn = 0, cs = 0;
@@ -913,7 +932,8 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
   const ListFrame f = list_frame(S);
   const bool half = S.half != 0;
   const int cl = c - S.cell_off;
-  const int cx = cl % S.nc[0], cy = (cl / S.nc[0]) % S.nc[1], cz = cl / (S.nc[0] * S.nc[1]);
+  int cx, cy, cz;
+  cell_xyz(S, cl, cx, cy, cz);
   const double3 o = make_double3(cx * S.cell[0], cy * S.cell[1], cz * S.cell[2]);
   int cs = 0, cn = 0;
   double3 sh = make_double3(0, 0, 0);
