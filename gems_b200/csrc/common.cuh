@@ -222,9 +222,10 @@ struct Arena {
   int* nn;              // neighbours per atom (flist entries: the full list)
   int* hnn;             // half-list systems: entries of `list` (the half list)
   int* list;            // column-major: list[m * cap + i], the reference's order
-  int* flist;           // the same pairs sorted by distance at the rebuild
-                        // (force kernels: a warp's atoms meet the same shell
-                        // at the same slot, so the distance classes do not diverge)
+  int* flist;           // the same pairs in the force order: the potential's inner
+                        // regime, the rest of the cut-off, then the skin bands (list
+                        // order within each), so a warp's atoms take the same branch
+                        // at the same slot and the skip counts cut a prefix
   uint4* ncut;          // per atom, eight 16-bit counts: flist entries built closer than
                         // rcut + 1e-4 + k skin/7 (k = 0..7; see live_entries)
   int* cell_of;

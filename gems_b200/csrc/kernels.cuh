@@ -1082,7 +1082,7 @@ __global__ void k_list_n2(Arena A, BlockMap M) {
           double rd = rd_exact(S, xi, tile[t]);
           if (rd > S.rlist2) continue;
           // flist: every pair in index order (O(N^2) lists are not
-          // distance-sorted); list: a half list keeps j > i only
+          // grouped by band); list: a half list keeps j > i only
           if (m < A.lcap) A.flist[(size_t)m * A.cap + i] = jj;
           m++;
           if (!S.half || jj > i) {

@@ -1104,7 +1104,7 @@ def test_fire_batch_equals_alone(ctx):
 
 @pytest.mark.parametrize("prec", [0, 1])
 def test_stale_list_pairs_entering_the_cutoff(ctx, prec):
-    """Between list builds the force kernels visit only the distance-sorted
+    """Between list builds the force kernels visit only the band-ordered
     entries that can have come within the cut-off (the skin test's bound on
     how far pairs moved).  A periodic Au crystal is displaced by up to 0.24 A
     per atom without a rebuild, so pairs built outside rce move inside it;
