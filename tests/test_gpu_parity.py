@@ -189,9 +189,10 @@ def test_list_boundary_ties(ctx):
         compare_lists(o, g)
 
 
+@pytest.mark.parametrize("natoms", [600, 300, 90])
 @pytest.mark.parametrize("pbc", [(True, True, True), (True, True, False)])
 @pytest.mark.parametrize("half", [False, True])
-def test_list_cells_thin_slab(ctx, pbc, half):
+def test_list_cells_thin_slab(ctx, pbc, half, natoms):
     """A slab one cell thick (6 x 5 x 1 cells): the stencil visits the one
     z-cell three times, so a periodic slab lists a neighbour once per visit,
     as the reference does; the lists equal the oracle's, entry by entry.
@@ -202,10 +203,13 @@ def test_list_cells_thin_slab(ctx, pbc, half):
     the force loops would then evaluate).  The GPU lists never hold an atom
     itself; the half-list comparison leaves those entries out.  (The stencil
     wraps cells in every dim, periodic or not, as cell_pbc does, so the
-    slab's open z takes the same path.)"""
+    slab's open z takes the same path.)  600, 300 and 90 atoms (20, 10 and 3
+    per cell) reach the three list kernels (a CTA per cell, a warp per cell
+    with a 512- and a 128-candidate tile) in the integer frame that a
+    periodic dimension of fewer than three cells needs."""
     rng = np.random.default_rng(5)
     L = (40.0, 33.0, 7.5)
-    pos = rng.random((600, 3)) * np.array(L)
+    pos = rng.random((natoms, 3)) * np.array(L)
 
     def setup(s):
         s.set_box(L, pbc)
