@@ -434,16 +434,11 @@ __global__ void k_sort_cells(Arena A, BlockMap C) {
         int v0 = ln < n ? a[ln] : -1;
         int v1 = ln + 32 < n ? a[ln + 32] : -1;
         int r0 = 0, r1 = 0;
-        // rank = entries greater than mine; empty slots (-1) are greater than none
-        for (int k = 0; k < min(n, 32); k++) {
-          const int w0 = __shfl_sync(0xffffffffu, v0, k);
-          r0 += w0 > v0;
-          r1 += w0 > v1;
-        }
-        for (int k = 0; k < n - 32; k++) {
-          const int w1 = __shfl_sync(0xffffffffu, v1, k);
-          r0 += w1 > v0;
-          r1 += w1 > v1;
+        for (int k = 0; k < 32; k++) {
+          int w0 = __shfl_sync(0xffffffffu, v0, k);
+          int w1 = __shfl_sync(0xffffffffu, v1, k);
+          r0 += (w0 > v0) + (w1 > v0);
+          r1 += (w0 > v1) + (w1 > v1);
         }
         __syncwarp();
         if (ln < n) a[r0] = v0;
