@@ -1822,11 +1822,43 @@ __global__ void __launch_bounds__(BLOCK) k_lj_fp64(Arena A, BlockMap M) {
   if constexpr (VIR) virial_close(A, M, s, w);
 }
 
+// The float constants of one LJ species pair, in a per-block table: 4e,
+// 48e, 24e, sigma^2, rc^2, and by form -- 0: truncated and shifted (the
+// shift), 1: shifted force (prc, frc, rc), 2: slj (rs^2, sa4, sa8, rc).
+struct LjF32 {
+  float e4, e48, e24, sg2, rc2, sh, frc, rc, rs2, sa4, sa8;
+  int form, on;
+};
+__device__ __forceinline__ LjF32 ljf_load(const PairP& P) {
+  LjF32 c;
+  const double e = P.v[0], sg = P.v[1];
+  c.e4 = (float)(4.0 * e);
+  c.e48 = (float)(48.0 * e);
+  c.e24 = (float)(24.0 * e);
+  c.sg2 = (float)(sg * sg);
+  c.rc2 = (float)P.v[3];
+  c.rc = (float)P.v[2];
+  c.form = P.v[8] != 0.0 ? 2 : P.v[7] != 0.0 ? 1 : 0;
+  c.sh = (float)(c.form == 1 ? P.v[4] : P.v[6]);
+  c.frc = (float)P.v[5];
+  c.rs2 = (float)(P.v[11] * P.v[11]);
+  c.sa4 = (float)P.v[9];
+  c.sa8 = (float)P.v[10];
+  c.on = (float)e != 0.0f;
+  return c;
+}
+
+// Mixed LJ: FP32 pair math from the fixed-point geometry, the species
+// table in shared memory, the FP32 terms of each group of UNR pairs summed
+// and the group sums accumulated per atom in FP64.
 template <int K, bool VIR = false>
 __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
+  __shared__ LjF32 tab[MAXT * MAXT];
+  for (int t = threadIdx.x; t < S.ntypes * S.ntypes; t += BLOCK) tab[t] = ljf_load(A.prm[S.param_off + t]);
+  __syncthreads();
   int i = M.first[blockIdx.x] + threadIdx.x / K;
   int lane = threadIdx.x % K;
   bool act = i < M.end[blockIdx.x];
@@ -1836,55 +1868,73 @@ __global__ void __launch_bounds__(BLOCK) k_lj_mixed(Arena A, BlockMap M) {
     const int4 xi = A.fxp[i];
     const int nn = live_entries(A, S, A.st[s], i, min(A.nn[i], A.lcap));
     const float evui = (float)EV_UI;
-    auto gat = [&](int j) { return A.fxp[j]; };
-    PAIR_LOOP_BEGIN(int4, gat)
-      const int4 xj = gj[u];
-      const PairP& P = A.prm[S.param_off + xi.w * S.ntypes + xj.w];
-      float e = (float)P.v[0];
-      float rc2 = (float)P.v[3];
-      float v0, v1, v2;
-      vd_fx(S, xi, xj, v0, v1, v2);
-      float r2 = v0 * v0 + v1 * v1 + v2 * v2;
-      if (r2 > rc2 || e == 0.0f) continue;
-      float sg = (float)P.v[1];
-      float ir2 = 1.0f / r2;
-      float t2 = sg * sg * ir2;
-      float s6 = t2 * t2 * t2;
-      float p = 4.0f * e * (s6 * s6 - s6);
-      float fr = e * (48.0f * s6 - 24.0f) * s6 * ir2;  // f / r
-      if (P.v[8] != 0.0) {
-        // slj (Pairs.F90:403-470): plain LJ inside rs, the quartic-octic
-        // spline sa4 d^4 + sa8 d^8 (d = r - rc) from rs to rc
-        const float rs = (float)P.v[11];
-        if (r2 >= rs * rs) {
-          const float dr = sqrtf(r2), d = dr - (float)P.v[2];
-          const float s4 = d * d * d * d;
-          const float a4 = (float)P.v[9], a8 = (float)P.v[10];
-          p = a4 * s4 + a8 * s4 * s4;
-          fr = -(4.0f * a4 * s4 + 8.0f * a8 * s4 * s4) / (d * dr);
+    const LjF32* row = tab + xi.w * S.ntypes;
+    int jn[UNR];
+    list_group<K>(A, i, nn, lane, jn);
+    for (int m0 = lane; m0 < nn; m0 += UNR * K) {
+      int jj[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; u++) jj[u] = jn[u];
+      int4 gj[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        gj[u] = xi;  // an empty slot: a zero pair vector, masked below
+        if (jj[u] >= 0) gj[u] = A.fxp[jj[u]];
+      }
+      list_group<K>(A, i, nn, m0 + UNR * K, jn);  // next group's ids, in flight meanwhile
+      float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, ge = 0.0f;
+      float gw[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        const int4 xj = gj[u];
+        const LjF32& c = row[xj.w];
+        float v0, v1, v2;
+        vd_fx(S, xi, xj, v0, v1, v2);
+        const float r2 = v0 * v0 + v1 * v1 + v2 * v2;
+        const bool ok = jj[u] >= 0 && !(r2 > c.rc2) && c.on;
+        const float ir2 = __frcp_rn(ok ? r2 : c.rc2);
+        const float t2 = c.sg2 * ir2;
+        const float s6 = t2 * t2 * t2;
+        float p = c.e4 * (s6 * s6 - s6);
+        float fr = (c.e48 * s6 - c.e24) * s6 * ir2;  // f / r
+        if (c.form == 2) {
+          // slj (Pairs.F90:403-470): plain LJ inside rs, the quartic-octic
+          // spline sa4 d^4 + sa8 d^8 (d = r - rc) from rs to rc
+          if (ok && r2 >= c.rs2) {
+            const float dr = sqrtf(r2), d = dr - c.rc;
+            const float s4 = d * d * d * d;
+            p = c.sa4 * s4 + c.sa8 * s4 * s4;
+            fr = -(4.0f * c.sa4 * s4 + 8.0f * c.sa8 * s4 * s4) / (d * dr);
+          }
+        } else if (c.form == 1) {  // shifted force (plj, Pairs.F90:282-370)
+          const float dr = sqrtf(ok ? r2 : c.rc2);
+          p = p - c.sh - c.frc * (dr - c.rc);
+          fr = fr + c.frc / dr;
+        } else {
+          p = p - c.sh;
         }
-      } else if (P.v[7] != 0.0) {
-        float dr = sqrtf(r2);
-        p = p - (float)P.v[4] - (float)P.v[5] * (dr - (float)P.v[2]);
-        fr = fr + (float)P.v[5] / dr;
-      } else {
-        p = p - (float)P.v[6];
+        fr = ok ? fr * evui : 0.0f;
+        g0 = fmaf(fr, v0, g0);
+        g1 = fmaf(fr, v1, g1);
+        g2 = fmaf(fr, v2, g2);
+        ge += ok ? p : 0.0f;
+        if constexpr (VIR) {
+          const float h = 0.5f * fr;
+          gw[0] += h * v0 * v0;
+          gw[1] += h * v1 * v1;
+          gw[2] += h * v2 * v2;
+          gw[3] += h * v0 * v1;
+          gw[4] += h * v0 * v2;
+          gw[5] += h * v1 * v2;
+        }
       }
-      fr = fr * evui;
-      f0 -= (double)(fr * v0);
-      f1 -= (double)(fr * v1);
-      f2 -= (double)(fr * v2);
-      ep += (double)p;
-      if constexpr (VIR) {
-        const float h = 0.5f * fr;
-        w[0] += (double)(h * v0 * v0);
-        w[1] += (double)(h * v1 * v1);
-        w[2] += (double)(h * v2 * v2);
-        w[3] += (double)(h * v0 * v1);
-        w[4] += (double)(h * v0 * v2);
-        w[5] += (double)(h * v1 * v2);
-      }
-    PAIR_LOOP_END
+      f0 -= (double)g0;
+      f1 -= (double)g1;
+      f2 -= (double)g2;
+      ep += (double)ge;
+      if constexpr (VIR)
+        for (int k = 0; k < 6; k++) w[k] += (double)gw[k];
+    }
   }
   f0 = lane_sum<K>(f0);
   f1 = lane_sum<K>(f1);
