@@ -236,6 +236,7 @@ struct Arena {
   int* cell_start;      // absolute start in cell_atoms
   int* chunk_sum;       // per 256-cell chunk
   int* cell_atoms;      // atom ids sorted by cell (descending within a cell)
+  double4* cell_pos;    // their positions, in the same order (written with it at a rebuild)
   // Tersoff: rslot[m * cap + i] = the slot of i in the flist of its m-th
   // neighbour (255: none), built with the list; per step, tsmask[i] marks
   // the flist slots of i that are bonds and tsfb[a * cap + i] holds the force

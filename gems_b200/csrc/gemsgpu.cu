@@ -307,6 +307,7 @@ int grow_atoms(gemsgpu_ctx* ctx, int64_t need) {
   CHK(dgrow(ctx, &A.cell_of, keep, nc));
   CHK(dgrow(ctx, &A.slot, keep, nc));
   CHK(dgrow(ctx, &A.cell_atoms, keep, nc));
+  CHK(dgrow(ctx, &A.cell_pos, keep, nc));
   CHK(dgrow(ctx, &A.ext_normals, 6 * keep, 6 * nc));
   // the lists' leading dimension is the atom capacity: re-lay them out
   if (A.lcap > 0) {
@@ -2011,7 +2012,7 @@ int gemsgpu_destroy(gemsgpu_ctx* ctx) {
   void* ptrs[] = {A.pos, A.pos_old, A.vel, A.acel, A.force, A.vel_v, A.acel2, A.acel3, A.acel4, A.epot, A.band, A.eband,
                   A.ebandf, A.fxp, A.pose, A.fxe, A.minv, A.mass, A.type, A.nn, A.hnn, A.ncut, A.list, A.flist, A.cell_of, A.slot,
                   A.cell_count, A.cell_n, A.cell_loc, A.cell_start, A.chunk_sum, A.cell_atoms,
-                  A.rslot, A.tidx, A.tsmask, A.tsfb, A.tsfb32,
+                  A.cell_pos, A.rslot, A.tidx, A.tsmask, A.tsfb, A.tsfb32,
                   A.ext_normals, A.blk_top2, A.blk_red, A.sys, A.st, A.prm, A.any_rebuild, A.body_runs,
                   ctx->d_red, ctx->snap, ctx->snap_st, ctx->snap_sys, ctx->d_sys,
                   ctx->lbw.x0, ctx->lbw.g, ctx->lbw.gold, ctx->lbw.d, ctx->lbw.S, ctx->lbw.Y, ctx->lbw.st,

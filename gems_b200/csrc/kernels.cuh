@@ -434,15 +434,27 @@ __global__ void k_sort_cells(Arena A, BlockMap C) {
         int v0 = ln < n ? a[ln] : -1;
         int v1 = ln + 32 < n ? a[ln + 32] : -1;
         int r0 = 0, r1 = 0;
-        for (int k = 0; k < 32; k++) {
-          int w0 = __shfl_sync(0xffffffffu, v0, k);
-          int w1 = __shfl_sync(0xffffffffu, v1, k);
-          r0 += (w0 > v0) + (w1 > v0);
-          r1 += (w0 > v1) + (w1 > v1);
+        // rank = entries greater than mine; empty slots (-1) are greater than none
+        for (int k = 0; k < min(n, 32); k++) {
+          const int w0 = __shfl_sync(0xffffffffu, v0, k);
+          r0 += w0 > v0;
+          r1 += w0 > v1;
+        }
+        for (int k = 0; k < n - 32; k++) {
+          const int w1 = __shfl_sync(0xffffffffu, v1, k);
+          r0 += w1 > v0;
+          r1 += w1 > v1;
         }
         __syncwarp();
-        if (ln < n) a[r0] = v0;
-        if (ln + 32 < n) a[r1] = v1;
+        // each lane places its own atoms (id and position) at their ranks
+        if (ln < n) {
+          a[r0] = v0;
+          A.cell_pos[start + r0] = A.pos[v0];
+        }
+        if (ln + 32 < n) {
+          a[r1] = v1;
+          A.cell_pos[start + r1] = A.pos[v1];
+        }
       } else if (ln == 0) {
         for (int x = 1; x < n; x++) {
           int v = a[x];
@@ -453,6 +465,7 @@ __global__ void k_sort_cells(Arena A, BlockMap C) {
           }
           a[y + 1] = v;
         }
+        for (int x = 0; x < n; x++) A.cell_pos[start + x] = A.pos[a[x]];  // the lane's own writes
       }
     }
     });
@@ -825,8 +838,9 @@ __device__ __forceinline__ void list_cells_item(const Arena& A, const BlockMap& 
 #pragma unroll
         for (int step = 16; step; step >>= 1)
           if (k + step < NSTENCIL && nb_pref[k + step] <= g) k += step;
-        const int j = A.cell_atoms[nb_start[k] + (g - nb_pref[k])];
-        const double4 p = A.pos[j];
+        const int idx = nb_start[k] + (g - nb_pref[k]);
+        const int j = A.cell_atoms[idx];
+        const double4 p = A.cell_pos[idx];
         cf[q] = list_record<IMG>(f, p, j, nb_sh[k], o);
         if (g < own) A.pos_old[j] = p;  // the home cell's atoms: the list's reference positions
       }
@@ -847,7 +861,7 @@ __device__ __forceinline__ void list_cells_item(const Arena& A, const BlockMap& 
           i = __float_as_int(ri.w);
         } else {
           i = A.cell_atoms[nb_start[0] + a];
-          ri = list_record<IMG>(f, A.pos[i], i, make_double3(0, 0, 0), o);
+          ri = list_record<IMG>(f, A.cell_pos[nb_start[0] + a], i, make_double3(0, 0, 0), o);
         }
       }
       int* row = stage + warp * A.lcap;
@@ -903,8 +917,8 @@ __global__ void __launch_bounds__(BLOCK) k_list_cells(Arena A, BlockMap C) {
 // and each SM keeps many cells' memory chains in flight (the CTA kernel
 // above keeps one per CTA).  Lanes 0..26 read the stencil cells' starts,
 // counts and shifts and a warp scan gives each cell's first candidate; the
-// warp stages the candidates' records in its shared tile in two passes (ids,
-// then positions, four loads in flight per lane), finding a candidate's
+// warp stages the candidates' records in its shared tile (ids and positions
+// from the cell-ordered arrays, two rounds in flight per lane), finding a candidate's
 // stencil cell by a binary search over the scan (shuffles); the cell's
 // atoms are then tested one after another exactly as in k_list_cells.
 // TILE = 128 for cells of about three atoms (Tersoff's 4 A cells), 512 for
@@ -956,8 +970,10 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
   const bool one = T <= TILE;  // one tile stays staged for all the cell's atoms
   auto stage_tile = [&](int t0, int tn) {
     __syncwarp();
-    // pass 1: each candidate's stencil cell and atom id (into .x / .w)
+    // the records: ids and positions from the cell-ordered arrays (one
+    // index, two independent loads), U rounds of candidates in flight
     for (int q0 = 0; q0 < tn; q0 += 32 * U) {
+      double4 p[U];
       int jv[U], kv[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
@@ -974,26 +990,11 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
         }
         const int st = __shfl_sync(FULL, cs, k), ek = __shfl_sync(FULL, ex, k);
         kv[u] = k;
-        jv[u] = q < tn ? A.cell_atoms[st + (g - ek)] : -1;
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int q = q0 + 32 * u + ln;
-        if (q < tn) cf[q] = make_float4(__int_as_float(kv[u]), 0.0f, 0.0f, __int_as_float(jv[u]));
-      }
-    }
-    __syncwarp();
-    // pass 2: the records
-    for (int q0 = 0; q0 < tn; q0 += 32 * U) {
-      double4 p[U];
-      int jv[U], kv[U];
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int q = q0 + 32 * u + ln;
-        const float4 e = q < tn ? cf[q] : make_float4(0, 0, 0, __int_as_float(-1));
-        kv[u] = __float_as_int(e.x);
-        jv[u] = __float_as_int(e.w);
-        if (jv[u] >= 0) p[u] = A.pos[jv[u]];
+        jv[u] = -1;
+        if (q < tn) {
+          jv[u] = A.cell_atoms[st + (g - ek)];
+          p[u] = A.cell_pos[st + (g - ek)];
+        }
       }
 #pragma unroll
       for (int u = 0; u < U; u++) {
@@ -1019,7 +1020,7 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
       i = __float_as_int(ri.w);
     } else {
       i = A.cell_atoms[beg0 + a];
-      ri = list_record<IMG>(f, A.pos[i], i, make_double3(0, 0, 0), o);
+      ri = list_record<IMG>(f, A.cell_pos[beg0 + a], i, make_double3(0, 0, 0), o);
     }
     for (int t0 = 0; t0 < T; t0 += TILE) {
       const int tn = min(TILE, T - t0);
