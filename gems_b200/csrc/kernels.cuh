@@ -216,17 +216,23 @@ __device__ __forceinline__ bool last_block(const BlockMap& M, SysState* st, int 
 }
 
 // warp 0 of a system's last block: top-2 over that system's block results
+// The system's top-2 over its blocks' partial results, merged by the whole
+// last block: each thread takes every BLOCK-th partial, four loads in flight
+// (a 1M-atom system has about 4000 blocks), then the block's tree.  The
+// top-2 of a set does not depend on the merge order.  Valid in thread 0.
 __device__ __forceinline__ double2 sys_top2(const Arena& A, const BlockMap& M, int s) {
   double2 w = make_double2(1.e-16, 1.e-16);
   const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
-  for (int b = threadIdx.x; b < nb; b += 32) w = top2_merge(w, __ldcg(&A.blk_top2[b0 + b]));
-  for (int o = 16; o; o >>= 1) {
-    double2 q;
-    q.x = __shfl_xor_sync(0xffffffffu, w.x, o);
-    q.y = __shfl_xor_sync(0xffffffffu, w.y, o);
-    w = top2_merge(w, q);
+  int b = threadIdx.x;
+  for (; b + 3 * BLOCK < nb; b += 4 * BLOCK) {
+    double2 q[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) q[u] = __ldcg(&A.blk_top2[b0 + b + u * BLOCK]);
+#pragma unroll
+    for (int u = 0; u < 4; u++) w = top2_merge(w, q[u]);
   }
-  return w;
+  for (; b < nb; b += BLOCK) w = top2_merge(w, __ldcg(&A.blk_top2[b0 + b]));
+  return block_top2(w);
 }
 
 // ------------------------------------------------------------------ skin test
@@ -235,7 +241,7 @@ __device__ __forceinline__ double2 sys_top2(const Arena& A, const BlockMap& M, i
 __device__ __forceinline__ void skin_finish(const Arena& A, const BlockMap& M, int s,
                                            double2 t) {
   if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
-  if (last_block(M, A.st, s, &A.st[s].ticket) && threadIdx.x < 32) {
+  if (last_block(M, A.st, s, &A.st[s].ticket)) {
     double2 v = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
       const SysDev& S = A.sys[s];
@@ -1033,10 +1039,11 @@ __device__ __forceinline__ void list_cells_w_item(const Arena& A, const BlockMap
   }
 }
 
-// register bounds measured best: three blocks per SM for the 128 tile, two
-// for the 512 tile (its 72 KB of tiles fit three; more registers win)
+// register bounds measured best: two blocks per SM for both tiles (three
+// blocks of the 128 tile spill the staging's positions; the 512 tile's
+// 72 KB of tiles fit three, but more registers win)
 template <int TILE, bool IMG>
-__global__ void __launch_bounds__(BLOCK, TILE == 128 ? 3 : 2) k_list_cells_w(Arena A, BlockMap C) {
+__global__ void __launch_bounds__(BLOCK, 2) k_list_cells_w(Arena A, BlockMap C) {
   extern __shared__ __align__(16) unsigned char listw_sh[];
   const int warp = threadIdx.x >> 5;
   unsigned char* mine = listw_sh + (size_t)warp * listw_warp_bytes<TILE>(A.lcap);
@@ -2870,7 +2877,7 @@ __device__ __forceinline__ void skin_close(Arena& A, const BlockMap& M, int s, c
                                            bool frozen, double2 t, cudaGraphConditionalHandle cond) {
   t = block_top2(t);
   if (threadIdx.x == 0) A.blk_top2[M.base + blockIdx.x] = t;
-  if (last_block(M, A.st, s, &st.ticket) && threadIdx.x < 32) {
+  if (last_block(M, A.st, s, &st.ticket)) {
     double2 w = sys_top2(A, M, s);
     if (threadIdx.x == 0) {
       // a moving box (constant pressure) shifts periodic images by up to
