@@ -1007,12 +1007,34 @@ int launch_step_a(gemsgpu_ctx* ctx, const std::vector<int>& ss,
   return 0;
 }
 
+// atoms per thread of the fused integrator step: STEP_APT for launches of
+// four or more full waves of one-atom blocks (four blocks per SM), else one
+#ifndef STEP_APT
+#define STEP_APT 2
+#endif
+int step_apt(const gemsgpu_ctx* ctx, const std::vector<int>& ss) {
+  // a branch of a batched graph uses the batch's map: the batch decides
+  const std::vector<int>& all = view_run(ctx, ss) >= 0 ? ctx->view_set : ss;
+  int64_t n = 0;
+  for (int s : all) n += ctx->sys[s].n;
+  return n >= (int64_t)4 * 4 * BLOCK * ctx->nsm ? STEP_APT : 1;
+}
+
 int launch_step_ba(gemsgpu_ctx* ctx, const std::vector<int>& ss,
                    cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
   BlockMap ma;
-  CHK(get_map(ctx, ss, BLOCK, 0, &ma));
-  if (use_cond) k_step_ba<true><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
-  else k_step_ba<false><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  const int apt = step_apt(ctx, ss);
+  CHK(get_map(ctx, ss, apt * BLOCK, 0, &ma));
+  if (apt == 4) {
+    if (use_cond) k_step_ba<true, 4><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+    else k_step_ba<false, 4><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  } else if (apt == 2) {
+    if (use_cond) k_step_ba<true, 2><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+    else k_step_ba<false, 2><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  } else {
+    if (use_cond) k_step_ba<true, 1><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+    else k_step_ba<false, 1><<<ma.nblk, BLOCK, 0, ctx->stream>>>(ctx->A, ma, cond);
+  }
   ++ctx->launches;
   CU(cudaGetLastError());
   return 0;
@@ -1482,6 +1504,7 @@ int get_graph(gemsgpu_ctx* ctx, const std::vector<int>& ss, int nsteps, cudaGrap
     BlockMap m;
     const int* sa;
     CHK(get_map(ctx, ss, BLOCK, 0, &m));
+    CHK(get_map(ctx, ss, step_apt(ctx, ss) * BLOCK, 0, &m));
     CHK(get_map(ctx, ss, 256, 1, &m));
     CHK(get_map(ctx, ss, BLOCK / 32, 1, &m));
     CHK(get_map(ctx, ss, 1, 1, &m));

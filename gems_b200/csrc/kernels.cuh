@@ -216,13 +216,26 @@ __device__ __forceinline__ bool last_block(const BlockMap& M, SysState* st, int 
 }
 
 // warp 0 of a system's last block: top-2 over that system's block results
-// The system's top-2 over its blocks' partial results, merged by the whole
-// last block: each thread takes every BLOCK-th partial, four loads in flight
-// (a 1M-atom system has about 4000 blocks), then the block's tree.  The
-// top-2 of a set does not depend on the merge order.  Valid in thread 0.
+// The system's top-2 over its blocks' partial results, called by the whole
+// last block.  Up to 128 partials one warp merges them; more (a 1M-atom
+// system has about 4000 blocks) the whole block does, each thread taking
+// every BLOCK-th partial with four loads in flight, then the block's tree.
+// The top-2 of a set does not depend on the merge order.  Valid in thread 0.
 __device__ __forceinline__ double2 sys_top2(const Arena& A, const BlockMap& M, int s) {
   double2 w = make_double2(1.e-16, 1.e-16);
   const int b0 = M.sys_blk0[s], nb = M.sys_nblk[s];
+  if (nb <= 128) {  // uniform across the block
+    if (threadIdx.x < 32) {
+      for (int b = threadIdx.x; b < nb; b += 32) w = top2_merge(w, __ldcg(&A.blk_top2[b0 + b]));
+      for (int o = 16; o; o >>= 1) {
+        double2 q;
+        q.x = __shfl_xor_sync(0xffffffffu, w.x, o);
+        q.y = __shfl_xor_sync(0xffffffffu, w.y, o);
+        w = top2_merge(w, q);
+      }
+    }
+    return w;
+  }
   int b = threadIdx.x;
   for (; b + 3 * BLOCK < nb; b += 4 * BLOCK) {
     double2 q[4];
@@ -3026,21 +3039,26 @@ __device__ __forceinline__ void ba_store(Arena& A, const SysDev& S, SysState& st
 // split kernels).  Per atom it is exactly k_step_b followed by k_step_a:
 // the same operations in the same order, with each array read and written
 // once instead of twice.
-template <bool COND>
+// APT atoms per thread (blocks of APT * BLOCK atoms, one after another):
+// a large system's blocks then pay the skin test's block merge and ticket
+// once per APT * BLOCK atoms.
+template <bool COND, int APT>
 __global__ void __launch_bounds__(BLOCK, 4) k_step_ba(Arena A, BlockMap M, cudaGraphConditionalHandle cond) {
   int s = blk_sys(M);
   if (s < 0) return;  // padding block of a fixed-capacity map
   const SysDev& S = A.sys[s];
   SysState& st = A.st[s];
-  int i = M.first[blockIdx.x] + threadIdx.x;
-  bool act = i < M.end[blockIdx.x];
   double2 t = make_double2(1.e-16, 1.e-16);
-  BaAtom b;
-  b.on = false;
-  if (act) {
-    ba_calc(A, S, st, i, A.force[i], b);
-    t.x = b.d;
-    ba_store(A, S, st, i, b);
+#pragma unroll 1
+  for (int k = 0; k < APT; k++) {
+    const int i = M.first[blockIdx.x] + threadIdx.x + k * BLOCK;
+    if (i < M.end[blockIdx.x]) {
+      BaAtom b;
+      b.on = false;
+      ba_calc(A, S, st, i, A.force[i], b);
+      t = top2_merge(t, make_double2(b.d, 1.e-16));
+      ba_store(A, S, st, i, b);
+    }
   }
   skin_close<COND, false>(A, M, s, S, st, false, t, cond);
 }

@@ -880,6 +880,39 @@ def test_md_steps_equals_stepwise(ctx, integ, prec):
         g.destroy()
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_md_steps_equals_stepwise_large_tersoff(ctx, prec):
+    """A 636,056-atom Tersoff Si crystal (43^3 diamond cells, 1000 K): on a
+    system this large the captured loop's integrator kernel takes two atoms
+    per thread and merges the skin test over half as many blocks; the
+    trajectory equals that of separate step_a / interact / step_b calls bit
+    for bit over 60 velocity-Verlet steps, list rebuilds included."""
+    from gems_b200 import workloads as W
+    pos = W.diamond(43, 5.431)
+    L = 43 * 5.431
+    vel = W.maxwell(len(pos), W.MASS["Si"], 1000.0, np.random.default_rng(4))
+    sys = []
+    for _ in range(2):
+        g = gems.System(pos, W.MASS["Si"], ctx=ctx, vel=vel)
+        g.set_box((L, L, L), (True, True, True))
+        g.set_tersoff(W.TERSOFF_SI)
+        g.set_skin(1.0)
+        g.set_precision(prec)
+        g.set_vv(0.001)
+        g.interact()
+        sys.append(g)
+    sys[0].md_steps(60)
+    for _ in range(60):
+        sys[1].stepa()
+        sys[1].interact()
+        sys[1].stepb()
+    np.testing.assert_array_equal(sys[0].pos, sys[1].pos)
+    np.testing.assert_array_equal(sys[0].vel, sys[1].vel)
+    assert sys[0].nupd == sys[1].nupd >= 2
+    for g in sys:
+        g.destroy()
+
+
 def test_batch_state_transfer_equals_per_system_calls(ctx):
     """gemsgpu_batch_set_state / _get_state move the same bytes as the
     per-system calls, and a run after a batched upload equals one after
